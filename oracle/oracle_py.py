@@ -1,0 +1,192 @@
+"""ctypes front-end to the CPU oracle (liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py as the checker.  The product path never imports
+this module.  Parity status of the oracle: unpinned (no Fortran compiler, no
+reference golden vectors); see oracle/oracle.h.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+
+NMAX = 64
+RMAX = 512
+
+
+class OrcMech(ctypes.Structure):
+    _fields_ = [
+        ("n_species", ctypes.c_int),
+        ("n_reactions", ctypes.c_int),
+        ("species_names", (ctypes.c_char * 21) * (NMAX + 1)),
+        ("reaction_type", ctypes.c_int * RMAX),
+        ("coeffs", ((ctypes.c_int * 4) * RMAX) * 2),
+        ("A", ctypes.c_double * RMAX),
+        ("beta", ctypes.c_double * RMAX),
+        ("E_act", ctypes.c_double * RMAX),
+        ("A_low", ctypes.c_double * RMAX),
+        ("beta_low", ctypes.c_double * RMAX),
+        ("E_act_low", ctypes.c_double * RMAX),
+        ("troe", (ctypes.c_double * 4) * RMAX),
+        ("eff", (ctypes.c_double * NMAX) * RMAX),
+        ("a_coeffs", ((ctypes.c_double * 7) * 2) * NMAX),
+        ("molar_mass", ctypes.c_double * NMAX),
+    ]
+
+
+class OrcCounters(ctypes.Structure):
+    _fields_ = [("nstate", ctypes.c_int), ("nstep", ctypes.c_int),
+                ("nfe", ctypes.c_int), ("nje", ctypes.c_int)]
+
+
+_lib = None
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        dp = ctypes.POINTER(ctypes.c_double)
+        L.orc_load_mechanism.argtypes = [ctypes.c_char_p] * 3 + [ctypes.c_double, ctypes.c_char_p,
+                                                                 ctypes.POINTER(OrcMech)]
+        L.orc_load_mechanism.restype = ctypes.c_int
+        L.orc_chem_step_mx.argtypes = [ctypes.POINTER(OrcMech), ctypes.c_long, ctypes.c_double,
+                                       dp, dp, dp, ctypes.c_void_p, dp, dp, dp,
+                                       ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+        L.orc_chem_step_mx.restype = ctypes.c_int
+        L.orc_temperature_after.argtypes = [ctypes.POINTER(OrcMech), ctypes.c_long, ctypes.c_double,
+                                            dp, dp, dp, dp, dp, dp, ctypes.c_int]
+        L.orc_rate_constants.argtypes = [ctypes.POINTER(OrcMech), ctypes.c_double, dp, dp, dp]
+        L.orc_rate_constants.restype = None
+        L.orc_rhs.argtypes = [ctypes.POINTER(OrcMech), dp, dp, dp, dp, dp]
+        L.orc_rhs.restype = None
+        for f in ("orc_specie_enthalpy", "orc_specie_entropy", "orc_specie_cp"):
+            getattr(L, f).argtypes = [ctypes.POINTER(OrcMech), ctypes.c_double, ctypes.c_int]
+            getattr(L, f).restype = ctypes.c_double
+        L.orc_dnrm2.argtypes = [ctypes.c_int, dp, ctypes.c_int]
+        L.orc_dnrm2.restype = ctypes.c_double
+        L.orc_ddcst.argtypes = [ctypes.c_int, dp, dp]
+        L.orc_ddcst.restype = None
+        _lib = L
+    return _lib
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Mechanism:
+    """Parsed mechanism held by the oracle."""
+
+    def __init__(self, mech_path, thermo_path, molar_path, eff_default=1.0, eact_units="cal.mol"):
+        self.m = OrcMech()
+        rc = lib().orc_load_mechanism(mech_path.encode(), thermo_path.encode(), molar_path.encode(),
+                                      float(eff_default), eact_units.encode(), ctypes.byref(self.m))
+        if rc != 0:
+            raise RuntimeError(f"oracle mechanism load failed: {rc}")
+
+    @property
+    def n_species(self):
+        return self.m.n_species
+
+    @property
+    def n_reactions(self):
+        return self.m.n_reactions
+
+    def species(self):
+        return [self.m.species_names[i].value.decode() for i in range(self.m.n_species + 1)]
+
+    def tables(self) -> dict:
+        """Constant tables as numpy arrays (reference layouts)."""
+        N, R = self.m.n_species, self.m.n_reactions
+        m = self.m
+        coeffs = np.array([[list(m.coeffs[s][r]) for r in range(R)] for s in range(2)], dtype=np.int32)
+        return dict(
+            species=self.species(),
+            reaction_type=np.array(m.reaction_type[:R], dtype=np.int32),
+            coeffs=coeffs,
+            A=np.array(m.A[:R]), beta=np.array(m.beta[:R]), E_act=np.array(m.E_act[:R]),
+            A_low=np.array(m.A_low[:R]), beta_low=np.array(m.beta_low[:R]),
+            E_act_low=np.array(m.E_act_low[:R]),
+            troe=np.array([list(m.troe[r]) for r in range(R)]),
+            eff=np.array([list(m.eff[r])[:N] for r in range(R)]),
+            a_coeffs=np.array([[list(m.a_coeffs[k][s]) for s in range(2)] for k in range(N)]),
+            molar_mass=np.array(m.molar_mass[:N]),
+        )
+
+    def chem_step(self, dt, T, rho, Y, bc=None, threads=0, mxstep=10000, Y_prod2_init=None):
+        """Y is (N, n) SoA.  Returns dict of outputs and per-cell counters."""
+        n = T.shape[0]
+        N = self.m.n_species
+        T = np.ascontiguousarray(T, dtype=np.float64)
+        rho = np.ascontiguousarray(rho, dtype=np.float64)
+        Y = np.ascontiguousarray(Y, dtype=np.float64).reshape(N, n)
+        Yp = np.zeros((N, n))
+        Yp2 = np.zeros((N, n)) if Y_prod2_init is None else np.array(Y_prod2_init, dtype=np.float64)
+        Ef = np.zeros(n)
+        cnt = (OrcCounters * n)()
+        bcp = None
+        if bc is not None:
+            bc = np.ascontiguousarray(bc, dtype=np.int8)
+            bcp = bc.ctypes.data_as(ctypes.c_void_p)
+        lib().orc_chem_step_mx(ctypes.byref(self.m), n, float(dt), _dp(T), _dp(rho), _dp(Y), bcp,
+                               _dp(Yp), _dp(Yp2), _dp(Ef), ctypes.cast(cnt, ctypes.c_void_p),
+                               int(threads), int(mxstep))
+        c = np.frombuffer(cnt, dtype=np.int32).reshape(n, 4)
+        return dict(Y_prod=Yp, Y_prod2=Yp2, E_f_prod=Ef, nstate=c[:, 0].copy(), nstep=c[:, 1].copy(),
+                    nfe=c[:, 2].copy(), nje=c[:, 3].copy())
+
+    def temperature_after(self, dt, T, rho, Y, Y_prod, E_f_prod, threads=0):
+        n = T.shape[0]
+        out = np.zeros(n)
+        args = [np.ascontiguousarray(a, dtype=np.float64) for a in (T, rho, Y, Y_prod, E_f_prod)]
+        lib().orc_temperature_after(ctypes.byref(self.m), n, float(dt), *[_dp(a) for a in args],
+                                    _dp(out), int(threads))
+        return out
+
+    def rate_constants(self, T, mix_conc):
+        R = self.m.n_reactions
+        mc = np.ascontiguousarray(mix_conc, dtype=np.float64)
+        kf = np.zeros(R)
+        kr = np.zeros(R)
+        lib().orc_rate_constants(ctypes.byref(self.m), float(T), _dp(mc), _dp(kf), _dp(kr))
+        return kf, kr
+
+    def rhs(self, kf, kr, mix_conc, Z):
+        out = np.zeros(self.m.n_species)
+        a = [np.ascontiguousarray(x, dtype=np.float64) for x in (kf, kr, mix_conc, Z)]
+        lib().orc_rhs(ctypes.byref(self.m), *[_dp(x) for x in a], _dp(out))
+        return out
+
+    def enthalpy(self, T, k):
+        return lib().orc_specie_enthalpy(ctypes.byref(self.m), float(T), int(k))
+
+    def entropy(self, T, k):
+        return lib().orc_specie_entropy(ctypes.byref(self.m), float(T), int(k))
+
+    def cp(self, T, k):
+        return lib().orc_specie_cp(ctypes.byref(self.m), float(T), int(k))
+
+
+def dnrm2(x) -> float:
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    return lib().orc_dnrm2(x.shape[0], _dp(x), 1)
+
+
+def ddcst(maxord=5):
+    el = np.zeros(13 * 12)
+    tq = np.zeros(3 * 12)
+    lib().orc_ddcst(maxord, _dp(el), _dp(tq))
+    return el.reshape(12, 13).T, tq.reshape(12, 3).T
