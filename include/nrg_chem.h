@@ -1,0 +1,166 @@
+/*
+ * nrg_chem.h -- C ABI of the B200 chemistry step for NRG.
+ *
+ * Drop-in boundary for the operator-split chemistry source term of NRG
+ * (module chemical_kinetics_solver_class,
+ *  computing_module/src/current_build/chemical_kinetics_solver.f90).
+ * Plain pointers and sizes only; every function returns an int status
+ * (NRG_OK = 0, negative = error, see nrg_chem_last_error) and never exits the
+ * process.  One handle owns one CUDA stream on the device that was current at
+ * creation; a handle is not re-entrant across host threads.
+ */
+#ifndef NRG_CHEM_H
+#define NRG_CHEM_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NRG_MAX_SPECIES 16
+
+#if defined(__GNUC__)
+#define NRG_API __attribute__((visibility("default")))
+#else
+#define NRG_API
+#endif
+
+enum nrg_status {
+  NRG_OK = 0,
+  NRG_ERR_ARG = -1,         /* bad argument (null pointer, bad size, bad bounds) */
+  NRG_ERR_IO = -2,          /* mechanism / thermo / molar-mass deck unreadable */
+  NRG_ERR_CUDA = -3,        /* CUDA runtime error (message in nrg_chem_last_error) */
+  NRG_ERR_UNSUPPORTED = -4, /* mechanism size without a compiled kernel */
+  NRG_ERR_STATE = -5        /* call not valid in the current state */
+};
+
+/* Activation-energy units of the deck (reference E_act_units,
+ * chemical_properties_class.f90:165-174). */
+enum nrg_eact_units { NRG_EACT_J_MOL = 0, NRG_EACT_KJ_MOL = 1, NRG_EACT_CAL_MOL = 2, NRG_EACT_KCAL_MOL = 3 };
+
+/* Integration modes. */
+enum nrg_mode {
+  NRG_MODE_REFERENCE = 0, /* FP64, finite-difference Jacobian exactly as the reference (DDPST MITER=2) */
+  NRG_MODE_FAST = 1,      /* FP64, analytic Jacobian */
+  NRG_MODE_MIXED = 2,     /* analytic Jacobian, FP32 LU + FP64 residual and refinement */
+  NRG_MODE_SURROGATE = 3  /* gated BF16 MLP surrogate with FP64 fallback (needs a trained model) */
+};
+
+/* Per-cell status byte (nrg_chem_step_device status output). */
+enum nrg_cell_status {
+  NRG_CELL_SKIPPED = 0,   /* T < 305 K or bc_markers /= 0: zero sources, Y_prod2 untouched */
+  NRG_CELL_OK = 1,
+  NRG_CELL_MXSTEP = 2,    /* MXSTEP steps without reaching dt (reference NSTATE = 3) */
+  NRG_CELL_FATAL = 3,     /* step size vanished or 50 retries (reference stops the program) */
+  NRG_CELL_NONFINITE = 4,
+  NRG_CELL_SURROGATE = 5  /* surrogate prediction accepted by the gate */
+};
+
+typedef struct nrg_chem nrg_chem;
+
+/* Host field block in the reference layout: every array is a Fortran
+ * column-major 3-D array cells(lb(1):ub(1), lb(2):ub(2), lb(3):ub(3)) with the
+ * ghost layer included (field_scalar_class.f90:68-73); Y, Y_prod and Y_prod2
+ * hold one array per species (field_vector_class.f90:61-80).  lo/hi are the
+ * interior bounds the reference loops over (get_local_inner_cells_bounds,
+ * computational_domain_class.f90:492-503). */
+typedef struct {
+  int lb[3], ub[3];
+  int lo[3], hi[3];
+  const double* T;
+  const double* p; /* read by the reference, unused by its arithmetic; may be NULL */
+  const double* rho;
+  const double* Y[NRG_MAX_SPECIES];
+  double* Y_prod[NRG_MAX_SPECIES];
+  double* Y_prod2[NRG_MAX_SPECIES];
+  double* E_f_prod;
+  const signed char* bc_markers; /* int8 markers; NULL = all interior */
+} nrg_field_desc;
+
+typedef struct {
+  long long cells;           /* cells in the call */
+  long long cells_active;    /* cells integrated (not skipped) */
+  long long cells_bad;       /* MXSTEP / fatal / non-finite cells */
+  long long cells_surrogate; /* cells answered by the surrogate */
+  long long cells_fallback;  /* active cells sent to the FP64 integrator by the gate */
+  long long steps, rhs_evals, jacobians, solves;
+  double device_ms;          /* device time of the step (CUDA events) */
+} nrg_chem_stats;
+
+/* Replaces chemical_kinetics_solver_c(manager) (chemical_kinetics_solver.f90:
+ * 111-173) together with the mechanism set-up it relies on
+ * (chemical_properties%set_properties, chemical_properties_class.f90:117-181;
+ * thermophysical_properties%set_properties, thermophysical_properties_class.f90:
+ * 137-210).  Paths name the three input decks. */
+NRG_API int nrg_chem_create(const char* mechanism_path, const char* thermo_path, const char* molar_masses_path,
+                    double default_enhanced_efficiencies, int eact_units, nrg_chem** out);
+
+/* Releases the handle and its device memory (never the caller's arrays). */
+NRG_API int nrg_chem_destroy(nrg_chem* h);
+
+/* Replaces call this%solve_chemical_kinetics(time_step)
+ * (chemical_kinetics_solver.f90:175-358) on host arrays in the reference
+ * layout: gathers the interior, runs the step on the GPU and scatters
+ * Y_prod / Y_prod2 / E_f_prod back.  stats may be NULL. */
+NRG_API int nrg_chem_step(nrg_chem* h, double time_step, const nrg_field_desc* fields, nrg_chem_stats* stats);
+
+/* Same step on device-resident species-major arrays: element (k, c) at
+ * [k*ld + c], ld >= n.  T_after (temperature after the energy closure),
+ * status and bc may be NULL.  stream is the caller's cudaStream_t (NULL: the
+ * legacy default stream): the step is ordered after work already queued there
+ * and the call returns when the step has finished. */
+NRG_API int nrg_chem_step_device(nrg_chem* h, double time_step, long n, long ld, const double* T,
+                         const double* rho, const double* Y, const signed char* bc, double* Y_prod,
+                         double* Y_prod2, double* E_f_prod, double* T_after, unsigned char* status,
+                         void* stream, nrg_chem_stats* stats);
+
+/* Mode (enum nrg_mode).  The reference's ODE_solver selector
+ * (chemical_kinetics_solver.f90:91,309-316) has no GPU counterpart for
+ * 'table_approximated'. */
+NRG_API int nrg_chem_set_mode(nrg_chem* h, int mode);
+
+/* Launch shape: persistent work-queue kernel or one thread per cell, threads
+ * per block, persistent grid (0 = one block per SM), cells per queue fetch. */
+NRG_API int nrg_chem_set_launch(nrg_chem* h, int persistent, int block, int grid, int chunk);
+NRG_API int nrg_chem_get_launch(nrg_chem* h, int* persistent, int* block, int* grid, int* chunk);
+
+/* Times candidate launch shapes on the given device-resident inputs (outputs
+ * are scratch) and keeps the fastest for this handle.  ms_best may be NULL. */
+NRG_API int nrg_chem_autotune(nrg_chem* h, double time_step, long n, long ld, const double* T,
+                      const double* rho, const double* Y, const signed char* bc, double* Y_prod,
+                      double* Y_prod2, double* E_f_prod, double* ms_best);
+
+/* Capture the step in a CUDA graph (1) or launch directly (0). */
+NRG_API int nrg_chem_set_graph(nrg_chem* h, int enable);
+
+/* Mechanism size and parsed tables (for checks against the reference decks).
+ * Arrays may be NULL; sizes follow n_species (N) and n_reactions (R):
+ * reaction_type[R], coeffs[2*R*4] ([side][r][count,i1,i2,i3], 1-based, N+1 = M),
+ * arrhenius[R*9] (A, beta, E, A_low, beta_low, E_low, troe0..2), troe3[R],
+ * eff[R*N], a_coeffs[N*2*7] (times R), molar_mass[N]. */
+NRG_API int nrg_chem_info(nrg_chem* h, int* n_species, int* n_reactions);
+NRG_API int nrg_chem_tables(nrg_chem* h, int* reaction_type, int* coeffs, double* arrhenius, double* troe3,
+                    double* eff, double* a_coeffs, double* molar_mass);
+NRG_API int nrg_chem_species_name(nrg_chem* h, int k, char* buf, int buflen);
+
+/* Host-only parse of the three decks (no CUDA call): fills n_species /
+ * n_reactions and, when non-NULL, the tables in the nrg_chem_tables layout.
+ * Call once with NULL arrays to size them. */
+NRG_API int nrg_mech_tables(const char* mechanism_path, const char* thermo_path,
+                            const char* molar_masses_path, double default_enhanced_efficiencies,
+                            int eact_units, int* n_species, int* n_reactions, int* reaction_type,
+                            int* coeffs, double* arrhenius, double* troe3, double* eff,
+                            double* a_coeffs, double* molar_mass);
+
+/* Message of the last failing call on this handle (or of the last failing
+ * nrg_chem_create when h is NULL). */
+NRG_API const char* nrg_chem_last_error(nrg_chem* h);
+
+/* Measured dependent-FMA FP64 throughput of the current device, TFLOP/s. */
+NRG_API int nrg_fp64_peak_tflops(double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

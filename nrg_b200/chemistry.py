@@ -1,0 +1,304 @@
+"""Host-side mirror of NRG's chemistry operator over the libnrg_chem C ABI.
+
+Reference interface (computing_module/src/current_build/
+chemical_kinetics_solver.f90):
+
+    type(chemical_kinetics_solver) function chemical_kinetics_solver_c(manager)   ! :111-173
+    subroutine solve_chemical_kinetics(this, time_step)                           ! :175-358
+
+The constructor finds 'temperature', 'pressure', 'density' and
+'specie_mass_fraction' in the data manager and creates
+'energy_production_chemistry', 'specie_production_chemistry' and
+'specie_production_chemistry2' (:121-138).  This module keeps those names and
+that behaviour; the arithmetic runs in libnrg_chem.so on the GPU.  There is no
+CPU fallback: a missing library or GPU raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libnrg_chem.so")
+NRG_MAX_SPECIES = 16
+
+MODES = {"reference": 0, "fast": 1, "mixed": 2, "surrogate": 3}
+EACT_UNITS = {"J.mol": 0, "kJ.mol": 1, "cal.mol": 2, "kcal.mol": 3}
+CELL_STATUS = {0: "skipped", 1: "ok", 2: "mxstep", 3: "fatal", 4: "nonfinite", 5: "surrogate"}
+
+
+class NrgError(RuntimeError):
+    pass
+
+
+class FieldDesc(ctypes.Structure):
+    _fields_ = [
+        ("lb", ctypes.c_int * 3), ("ub", ctypes.c_int * 3),
+        ("lo", ctypes.c_int * 3), ("hi", ctypes.c_int * 3),
+        ("T", ctypes.c_void_p), ("p", ctypes.c_void_p), ("rho", ctypes.c_void_p),
+        ("Y", ctypes.c_void_p * NRG_MAX_SPECIES),
+        ("Y_prod", ctypes.c_void_p * NRG_MAX_SPECIES),
+        ("Y_prod2", ctypes.c_void_p * NRG_MAX_SPECIES),
+        ("E_f_prod", ctypes.c_void_p),
+        ("bc_markers", ctypes.c_void_p),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("cells", ctypes.c_longlong), ("cells_active", ctypes.c_longlong),
+        ("cells_bad", ctypes.c_longlong), ("cells_surrogate", ctypes.c_longlong),
+        ("cells_fallback", ctypes.c_longlong),
+        ("steps", ctypes.c_longlong), ("rhs_evals", ctypes.c_longlong),
+        ("jacobians", ctypes.c_longlong), ("solves", ctypes.c_longlong),
+        ("device_ms", ctypes.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+# every symbol include/nrg_chem.h declares, with its ctypes signature
+_VP, _I, _D, _L, _CP = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_long, ctypes.c_char_p
+SIGNATURES = {
+    "nrg_chem_create": (_I, [_CP, _CP, _CP, _D, _I, ctypes.POINTER(_VP)]),
+    "nrg_chem_destroy": (_I, [_VP]),
+    "nrg_chem_step": (_I, [_VP, _D, ctypes.POINTER(FieldDesc), ctypes.POINTER(Stats)]),
+    "nrg_chem_step_device": (_I, [_VP, _D, _L, _L, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP,
+                                  ctypes.POINTER(Stats)]),
+    "nrg_chem_set_mode": (_I, [_VP, _I]),
+    "nrg_chem_set_launch": (_I, [_VP, _I, _I, _I, _I]),
+    "nrg_chem_get_launch": (_I, [_VP] + [ctypes.POINTER(_I)] * 4),
+    "nrg_chem_autotune": (_I, [_VP, _D, _L, _L, _VP, _VP, _VP, _VP, _VP, _VP, _VP, ctypes.POINTER(_D)]),
+    "nrg_chem_set_graph": (_I, [_VP, _I]),
+    "nrg_chem_info": (_I, [_VP, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
+    "nrg_chem_tables": (_I, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "nrg_chem_species_name": (_I, [_VP, _I, ctypes.c_char_p, _I]),
+    "nrg_mech_tables": (_I, [_CP, _CP, _CP, _D, _I, ctypes.POINTER(_I), ctypes.POINTER(_I)] + [_VP] * 7),
+    "nrg_chem_last_error": (ctypes.c_char_p, [_VP]),
+    "nrg_fp64_peak_tflops": (_I, [ctypes.POINTER(_D)]),
+}
+
+_lib = None
+
+
+def lib():
+    """Loads libnrg_chem.so; raises if it is missing (no fallback path)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise NrgError(f"{LIB_PATH} not built: run __graft_entry__.build() or python nrg_b200/build.py")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _ptr(a) -> int | None:
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    return a.ctypes.data
+
+
+def _check(rc: int, h=None) -> None:
+    if rc != 0:
+        msg = lib().nrg_chem_last_error(h)
+        raise NrgError(f"libnrg_chem error {rc}: {msg.decode() if msg else ''}")
+
+
+def mechanism_tables(mechanism, thermo, molar_masses, default_enhanced_efficiencies=1.0,
+                     E_act_units="cal.mol") -> dict:
+    """Parsed constant tables (host only, no GPU)."""
+    L = lib()
+    n, r = ctypes.c_int(), ctypes.c_int()
+    args = [str(mechanism).encode(), str(thermo).encode(), str(molar_masses).encode(),
+            float(default_enhanced_efficiencies), EACT_UNITS[E_act_units]]
+    _check(L.nrg_mech_tables(*args, ctypes.byref(n), ctypes.byref(r), *([None] * 7)))
+    N, R = n.value, r.value
+    t = dict(reaction_type=np.zeros(R, np.int32), coeffs=np.zeros((2, R, 4), np.int32),
+             arrhenius=np.zeros((R, 9)), troe3=np.zeros(R), eff=np.zeros((R, N)),
+             a_coeffs=np.zeros((N, 2, 7)), molar_mass=np.zeros(N))
+    _check(L.nrg_mech_tables(*args, ctypes.byref(n), ctypes.byref(r),
+                             *[_ptr(t[k]) for k in ("reaction_type", "coeffs", "arrhenius", "troe3",
+                                                    "eff", "a_coeffs", "molar_mass")]))
+    t["n_species"], t["n_reactions"] = N, R
+    return t
+
+
+@dataclass
+class DataManager:
+    """Named Fortran-layout fields of one block: cells(lb:ub) per axis, ghost
+    layer included, column-major (data_manager_class.f90:55-68)."""
+
+    lb: tuple
+    ub: tuple
+    lo: tuple
+    hi: tuple
+    fields: dict = field(default_factory=dict)
+
+    @classmethod
+    def block(cls, nx: int, ny: int, nz: int = 1, ghost: int = 1) -> "DataManager":
+        lb = (1 - ghost, 1 - ghost, 1 - ghost if nz > 1 else 1)
+        ub = (nx + ghost, ny + ghost, nz + ghost if nz > 1 else 1)
+        return cls(lb, ub, (1, 1, 1), (nx, ny, nz))
+
+    @property
+    def shape(self):
+        return tuple(u - l + 1 for l, u in zip(self.lb, self.ub))
+
+    def create_scalar_field(self, name: str) -> np.ndarray:
+        self.fields[name] = np.zeros(self.shape, order="F")
+        return self.fields[name]
+
+    def create_vector_field(self, name: str, n: int) -> list:
+        self.fields[name] = [np.zeros(self.shape, order="F") for _ in range(n)]
+        return self.fields[name]
+
+    def get_field_pointer_by_name(self, name: str):
+        return self.fields[name]
+
+    def interior(self, a: np.ndarray) -> np.ndarray:
+        sl = tuple(slice(lo - l, hi - l + 1) for lo, hi, l in zip(self.lo, self.hi, self.lb))
+        return a[sl]
+
+
+class ChemicalKineticsSolver:
+    """GPU chemistry operator with the reference's constructor and step."""
+
+    def __init__(self, manager: DataManager | None, mechanism, thermo, molar_masses,
+                 default_enhanced_efficiencies: float = 1.0, E_act_units: str = "cal.mol",
+                 mode: str = "fast"):
+        L = lib()
+        h = ctypes.c_void_p()
+        _check(L.nrg_chem_create(str(mechanism).encode(), str(thermo).encode(), str(molar_masses).encode(),
+                                 float(default_enhanced_efficiencies), EACT_UNITS[E_act_units],
+                                 ctypes.byref(h)))
+        self._h = h
+        n, r = ctypes.c_int(), ctypes.c_int()
+        _check(L.nrg_chem_info(h, ctypes.byref(n), ctypes.byref(r)), h)
+        self.species_number, self.reactions_number = n.value, r.value
+        buf = ctypes.create_string_buffer(32)
+        self.species_names = []
+        for k in range(self.species_number):
+            _check(L.nrg_chem_species_name(h, k, buf, 32), h)
+            self.species_names.append(buf.value.decode())
+        self.set_mode(mode)
+        self.manager = manager
+        if manager is not None:
+            for name in ("temperature", "density", "specie_mass_fraction"):
+                if name not in manager.fields:
+                    raise NrgError(f"field '{name}' not registered in the data manager")
+            manager.create_scalar_field("energy_production_chemistry")
+            manager.create_vector_field("specie_production_chemistry", self.species_number)
+            manager.create_vector_field("specie_production_chemistry2", self.species_number)
+
+    # -- lifecycle ---------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().nrg_chem_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- options -----------------------------------------------------------
+    def set_mode(self, mode: str) -> None:
+        _check(lib().nrg_chem_set_mode(self._h, MODES[mode]), self._h)
+        self.mode = mode
+
+    def set_launch(self, persistent=True, block=128, grid=0, chunk=1) -> None:
+        _check(lib().nrg_chem_set_launch(self._h, int(persistent), block, grid, chunk), self._h)
+
+    def get_launch(self) -> dict:
+        v = [ctypes.c_int() for _ in range(4)]
+        _check(lib().nrg_chem_get_launch(self._h, *[ctypes.byref(x) for x in v]), self._h)
+        return dict(zip(("persistent", "block", "grid", "chunk"), [x.value for x in v]))
+
+    def set_graph(self, enable: bool) -> None:
+        _check(lib().nrg_chem_set_graph(self._h, int(enable)), self._h)
+
+    @property
+    def handle(self):
+        return self._h
+
+    # -- the reference step on host fields -------------------------------------
+    def solve_chemical_kinetics(self, time_step: float) -> dict:
+        m = self.manager
+        if m is None:
+            raise NrgError("no data manager attached")
+        N = self.species_number
+        d = FieldDesc()
+        for i in range(3):
+            d.lb[i], d.ub[i], d.lo[i], d.hi[i] = m.lb[i], m.ub[i], m.lo[i], m.hi[i]
+        keep = []
+
+        def fptr(a):
+            if not (a.flags.f_contiguous and a.dtype == np.float64):
+                raise NrgError("fields must be float64 Fortran-ordered arrays")
+            keep.append(a)
+            return a.ctypes.data
+
+        f = m.fields
+        d.T = fptr(f["temperature"])
+        d.rho = fptr(f["density"])
+        d.p = fptr(f["pressure"]) if "pressure" in f else None
+        for k in range(N):
+            d.Y[k] = fptr(f["specie_mass_fraction"][k])
+            d.Y_prod[k] = fptr(f["specie_production_chemistry"][k])
+            d.Y_prod2[k] = fptr(f["specie_production_chemistry2"][k])
+        d.E_f_prod = fptr(f["energy_production_chemistry"])
+        if "bc_markers" in f:
+            bc = f["bc_markers"]
+            if bc.dtype != np.int8 or not bc.flags.f_contiguous:
+                raise NrgError("bc_markers must be int8 Fortran-ordered")
+            keep.append(bc)
+            d.bc_markers = bc.ctypes.data
+        st = Stats()
+        _check(lib().nrg_chem_step(self._h, float(time_step), ctypes.byref(d), ctypes.byref(st)), self._h)
+        return st.as_dict()
+
+    # -- device-resident step (torch CUDA tensors) ---------------------------
+    def step_device(self, time_step, T, rho, Y, Y_prod, Y_prod2, E_f_prod, bc=None, T_after=None,
+                    status=None, stream=None) -> dict:
+        """Species-major device arrays: Y has shape (N, ld) with cells in the
+        first n = T.numel() columns."""
+        n = T.numel()
+        ld = Y.shape[1]
+        if stream is None and hasattr(T, "device"):
+            import torch
+            stream = torch.cuda.current_stream(T.device).cuda_stream
+        st = Stats()
+        _check(lib().nrg_chem_step_device(
+            self._h, float(time_step), n, ld, _ptr(T), _ptr(rho), _ptr(Y), _ptr(bc), _ptr(Y_prod),
+            _ptr(Y_prod2), _ptr(E_f_prod), _ptr(T_after), _ptr(status),
+            ctypes.c_void_p(stream) if stream else None, ctypes.byref(st)), self._h)
+        return st.as_dict()
+
+    def autotune(self, time_step, T, rho, Y, Y_prod, Y_prod2, E_f_prod, bc=None) -> float:
+        ms = ctypes.c_double()
+        _check(lib().nrg_chem_autotune(self._h, float(time_step), T.numel(), Y.shape[1], _ptr(T), _ptr(rho),
+                                       _ptr(Y), _ptr(bc), _ptr(Y_prod), _ptr(Y_prod2), _ptr(E_f_prod),
+                                       ctypes.byref(ms)), self._h)
+        return ms.value
+
+
+def chemical_kinetics_solver_c(manager: DataManager, mechanism, thermo, molar_masses, **kw) -> ChemicalKineticsSolver:
+    """Constructor with the reference's name (chemical_kinetics_solver.f90:105-107)."""
+    return ChemicalKineticsSolver(manager, mechanism, thermo, molar_masses, **kw)
+
+
+def fp64_peak_tflops() -> float:
+    v = ctypes.c_double()
+    _check(lib().nrg_fp64_peak_tflops(ctypes.byref(v)))
+    return v.value

@@ -1,0 +1,642 @@
+// C ABI implementation (include/nrg_chem.h): handle, mechanism upload,
+// host-layout gather/scatter, CUDA-graph capture and the launch autotuner.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/nrg_chem.h"
+#include "chem_device.cuh"
+#include "chem_kernels.hpp"
+#include "mechanism.hpp"
+#include "surrogate.hpp"
+
+using nrg::DevMech;
+using nrg::LaunchCfg;
+using nrg::StepArgs;
+
+static thread_local std::string g_create_error;
+
+struct nrg_chem {
+  nrg::Mechanism mech;
+  DevMech dm;
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  int mode = NRG_MODE_FAST;
+  LaunchCfg cfg;
+  bool use_graph = true;
+  int* d_queue = nullptr;
+  unsigned long long* d_counters = nullptr;
+  unsigned long long* h_counters = nullptr;  // pinned
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_in = nullptr;
+  // host-path staging
+  size_t cap = 0;
+  double *d_T = nullptr, *d_rho = nullptr, *d_Y = nullptr, *d_Yp = nullptr, *d_Yp2 = nullptr,
+         *d_Ef = nullptr;
+  int8_t* d_bc = nullptr;
+  uint8_t* d_status = nullptr;
+  double *h_T = nullptr, *h_rho = nullptr, *h_Y = nullptr, *h_Yp = nullptr, *h_Yp2 = nullptr,
+         *h_Ef = nullptr;
+  int8_t* h_bc = nullptr;
+  uint8_t* h_status = nullptr;
+  // graph cache
+  cudaGraphExec_t gexec = nullptr;
+  // surrogate state (owned by surrogate.cu)
+  nrg::Surrogate* sur = nullptr;
+  std::string err;
+};
+
+namespace {
+
+int fail(nrg_chem* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  else g_create_error = msg;
+  return code;
+}
+
+int cuda_fail(nrg_chem* h, cudaError_t e, const char* where) {
+  return fail(h, NRG_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(h, call)                                        \
+  do {                                                     \
+    cudaError_t e_ = (call);                               \
+    if (e_ != cudaSuccess) return cuda_fail(h, e_, #call); \
+  } while (0)
+
+// Gear coefficients EL(13,12), TQ(3,12) (ddcst.f90:35-106, MINT = 2).
+void gear_coefficients(double* el, double* tq) {
+  const int maxord = nrg::kMaxOrd;
+  double fact[13];
+  fact[0] = 1.0;
+  for (int i = 2; i <= maxord; ++i) fact[i - 1] = (double)i * fact[i - 2];
+  auto E = [&](int i, int j) -> double& { return el[(j - 1) * 13 + (i - 1)]; };
+  auto Q = [&](int i, int j) -> double& { return tq[(j - 1) * 3 + (i - 1)]; };
+  std::fill(el, el + 13 * 12, 0.0);
+  std::fill(tq, tq + 3 * 12, 0.0);
+  E(1, 1) = 1.0;
+  E(2, 1) = 1.0;
+  for (int j = 2; j <= maxord; ++j) {
+    E(1, j) = fact[j - 1];
+    for (int i = 2; i <= j; ++i) E(i, j) = (double)j * E(i, j - 1) + E(i - 1, j - 1);
+    E(j + 1, j) = 1.0;
+  }
+  double sum = 1.0;
+  for (int j = 2; j <= maxord; ++j) {
+    sum = sum + 1.0 / (double)j;
+    for (int i = 1; i <= j + 1; ++i) E(i, j) = E(i, j) / (fact[j - 1] * sum);
+  }
+  for (int j = 1; j <= maxord; ++j) {
+    if (j > 1) Q(1, j) = 1.0 / fact[j - 2];
+    Q(2, j) = (double)(j + 1) / E(1, j);
+    Q(3, j) = (double)(j + 2) / E(1, j);
+  }
+}
+
+// Atom counts of H, O, N from a species formula such as "H2O2".
+void formula_elements(const std::string& name, double out[3]) {
+  out[0] = out[1] = out[2] = 0.0;
+  size_t i = 0;
+  while (i < name.size()) {
+    char c = name[i++];
+    int idx = c == 'H' ? 0 : c == 'O' ? 1 : c == 'N' ? 2 : -1;
+    int cnt = 0;
+    while (i < name.size() && std::isdigit((unsigned char)name[i])) cnt = cnt * 10 + (name[i++] - '0');
+    if (cnt == 0) cnt = 1;
+    if (idx >= 0) out[idx] += cnt;
+  }
+}
+
+std::string build_dev_mech(const nrg::Mechanism& m, DevMech* d) {
+  const int N = m.n(), R = m.r();
+  if (N > nrg::kMaxSpecies || R > nrg::kMaxReactions) return "mechanism larger than the compiled tables";
+  std::memset(d, 0, sizeof(DevMech));
+  d->N = N;
+  d->R = R;
+  for (int r = 0; r < R; ++r) {
+    const nrg::Reaction& rx = m.reactions[r];
+    d->type[r] = rx.type;
+    d->nl[r] = rx.n_left;
+    d->nr[r] = rx.n_right;
+    for (int i = 0; i < 3; ++i) {
+      d->left[r][i] = (i < rx.n_left) ? (rx.left[i] == N + 1 ? -1 : rx.left[i] - 1) : -1;
+      d->right[r][i] = (i < rx.n_right) ? (rx.right[i] == N + 1 ? -1 : rx.right[i] - 1) : -1;
+    }
+    int u = 0;
+    for (int k = 1; k <= N; ++k) {
+      for (int i = 0; i < rx.n_left; ++i)
+        if (rx.left[i] == k) { d->upd_k[r][u] = k - 1; d->upd_prod[r][u] = 0; ++u; }
+      for (int i = 0; i < rx.n_right; ++i)
+        if (rx.right[i] == k) { d->upd_k[r][u] = k - 1; d->upd_prod[r][u] = 1; ++u; }
+    }
+    d->nupd[r] = u;
+    d->A[r] = rx.A;
+    d->beta[r] = rx.beta;
+    d->E[r] = rx.E;
+    d->A_low[r] = rx.A_low;
+    d->beta_low[r] = rx.beta_low;
+    d->E_low[r] = rx.E_low;
+    for (int q = 0; q < 4; ++q) d->troe[r][q] = rx.troe[q];
+    d->dnu[r] = (double)(rx.n_right - rx.n_left);
+    for (int k = 0; k < N; ++k) d->eff[r][k] = m.eff[(size_t)r * N + k];
+  }
+  for (int k = 0; k < N; ++k) {
+    for (int s = 0; s < 2; ++s)
+      for (int i = 0; i < 7; ++i) d->a[k][s][i] = m.a_coeffs[((size_t)k * 2 + s) * 7 + i];
+    d->W[k] = m.molar_mass[k];
+    if (d->W[k] == 0.0) return "zero molar mass for species " + m.species[k];
+    d->invW[k] = 1.0 / d->W[k];
+    d->h_ref[k] = nrg::specie_enthalpy(m, nrg::kTRef, k);
+    double e[3];
+    formula_elements(m.species[k], e);
+    for (int q = 0; q < 3; ++q) d->elem[q][k] = e[q];
+  }
+  gear_coefficients(d->el, d->tq);
+  d->eps = 1.0e-9;
+  d->ewt = 1.0e-4;
+  d->hmax = (double)1.0E-7f;  // single-precision literal in the reference
+  d->uround = DBL_EPSILON;
+  d->sqrt_uround = std::sqrt(DBL_EPSILON);
+  d->br = std::pow(DBL_EPSILON, 0.875);
+  d->bl = std::pow(DBL_EPSILON, 0.75);
+  d->bp = std::pow(DBL_EPSILON, -0.15);
+  d->facmin = std::pow(DBL_EPSILON, 0.78);
+  return "";
+}
+
+void free_staging(nrg_chem* h) {
+  cudaFree(h->d_T); cudaFree(h->d_rho); cudaFree(h->d_Y); cudaFree(h->d_Yp); cudaFree(h->d_Yp2);
+  cudaFree(h->d_Ef); cudaFree(h->d_bc); cudaFree(h->d_status);
+  cudaFreeHost(h->h_T); cudaFreeHost(h->h_rho); cudaFreeHost(h->h_Y); cudaFreeHost(h->h_Yp);
+  cudaFreeHost(h->h_Yp2); cudaFreeHost(h->h_Ef); cudaFreeHost(h->h_bc); cudaFreeHost(h->h_status);
+  h->d_T = h->d_rho = h->d_Y = h->d_Yp = h->d_Yp2 = h->d_Ef = nullptr;
+  h->h_T = h->h_rho = h->h_Y = h->h_Yp = h->h_Yp2 = h->h_Ef = nullptr;
+  h->d_bc = h->h_bc = nullptr;
+  h->d_status = h->h_status = nullptr;
+  h->cap = 0;
+}
+
+int ensure_staging(nrg_chem* h, size_t n) {
+  if (n <= h->cap) return NRG_OK;
+  free_staging(h);
+  const size_t N = (size_t)h->mech.n();
+  CK(h, cudaMalloc(&h->d_T, n * 8));
+  CK(h, cudaMalloc(&h->d_rho, n * 8));
+  CK(h, cudaMalloc(&h->d_Y, N * n * 8));
+  CK(h, cudaMalloc(&h->d_Yp, N * n * 8));
+  CK(h, cudaMalloc(&h->d_Yp2, N * n * 8));
+  CK(h, cudaMalloc(&h->d_Ef, n * 8));
+  CK(h, cudaMalloc(&h->d_bc, n));
+  CK(h, cudaMalloc(&h->d_status, n));
+  CK(h, cudaMallocHost(&h->h_T, n * 8));
+  CK(h, cudaMallocHost(&h->h_rho, n * 8));
+  CK(h, cudaMallocHost(&h->h_Y, N * n * 8));
+  CK(h, cudaMallocHost(&h->h_Yp, N * n * 8));
+  CK(h, cudaMallocHost(&h->h_Yp2, N * n * 8));
+  CK(h, cudaMallocHost(&h->h_Ef, n * 8));
+  CK(h, cudaMallocHost(&h->h_bc, n));
+  CK(h, cudaMallocHost(&h->h_status, n));
+  h->cap = n;
+  return NRG_OK;
+}
+
+int jac_of(int mode) { return mode == NRG_MODE_REFERENCE ? 0 : 1; }
+
+// Enqueue the plain integrator (no surrogate) on stream s.
+cudaError_t enqueue_integrator(nrg_chem* h, const StepArgs& a, const LaunchCfg& cfg, cudaStream_t s) {
+  cudaError_t e = cudaSuccess;
+  if (cfg.persistent) {
+    e = cudaMemsetAsync(h->d_queue, 0, sizeof(int), s);
+    if (e != cudaSuccess) return e;
+  }
+  LaunchCfg c = cfg;
+  if (c.persistent && c.grid <= 0) c.grid = h->num_sms;
+  return nrg::launch_chem(h->mech.n(), h->mech.r(), jac_of(h->mode), h->mode == NRG_MODE_MIXED, a, c,
+                          h->d_queue, h->d_counters, s);
+}
+
+cudaError_t enqueue_step(nrg_chem* h, const StepArgs& a, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(h->d_counters, 0, sizeof(unsigned long long) * 8, s);
+  if (e != cudaSuccess) return e;
+  if (h->mode == NRG_MODE_SURROGATE) return nrg::surrogate_step(h->sur, a, h->cfg, h->d_queue, h->d_counters, s,
+                                                                 [h](const StepArgs& fa, cudaStream_t fs) {
+                                                                   LaunchCfg c = h->cfg;
+                                                                   c.persistent = true;
+                                                                   return enqueue_integrator(h, fa, c, fs);
+                                                                 });
+  return enqueue_integrator(h, a, h->cfg, s);
+}
+
+// Runs the step on stream s, through a CUDA graph when enabled.
+int run_step(nrg_chem* h, const StepArgs& a, cudaStream_t s, nrg_chem_stats* stats) {
+  if (h->mode == NRG_MODE_SURROGATE && !nrg::surrogate_ready(h->sur))
+    return fail(h, NRG_ERR_STATE, "surrogate mode selected but no trained model is loaded");
+  CK(h, cudaEventRecord(h->ev0, s));
+  if (h->use_graph) {
+    cudaGraph_t g = nullptr;
+    CK(h, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = enqueue_step(h, a, s);
+    cudaError_t e2 = cudaStreamEndCapture(s, &g);
+    if (e != cudaSuccess) { if (g) cudaGraphDestroy(g); return cuda_fail(h, e, "enqueue_step"); }
+    if (e2 != cudaSuccess) return cuda_fail(h, e2, "cudaStreamEndCapture");
+    bool updated = false;
+    if (h->gexec) {
+      cudaGraphExecUpdateResultInfo info;
+      updated = cudaGraphExecUpdate(h->gexec, g, &info) == cudaSuccess;
+      if (!updated) {
+        cudaGetLastError();
+        cudaGraphExecDestroy(h->gexec);
+        h->gexec = nullptr;
+      }
+    }
+    if (!h->gexec) {
+      e = cudaGraphInstantiate(&h->gexec, g, 0);
+      if (e != cudaSuccess) { cudaGraphDestroy(g); return cuda_fail(h, e, "cudaGraphInstantiate"); }
+    }
+    cudaGraphDestroy(g);
+    CK(h, cudaGraphLaunch(h->gexec, s));
+  } else {
+    cudaError_t e = enqueue_step(h, a, s);
+    if (e != cudaSuccess) return cuda_fail(h, e, "enqueue_step");
+  }
+  CK(h, cudaEventRecord(h->ev1, s));
+  CK(h, cudaMemcpyAsync(h->h_counters, h->d_counters, sizeof(unsigned long long) * 8,
+                        cudaMemcpyDeviceToHost, s));
+  CK(h, cudaStreamSynchronize(s));
+  if (stats) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    std::memset(stats, 0, sizeof(*stats));
+    stats->cells = a.n;
+    stats->cells_active = (long long)h->h_counters[0];
+    stats->steps = (long long)h->h_counters[1];
+    stats->rhs_evals = (long long)h->h_counters[2];
+    stats->jacobians = (long long)h->h_counters[3];
+    stats->solves = (long long)h->h_counters[4];
+    stats->cells_bad = (long long)h->h_counters[5];
+    stats->cells_surrogate = (long long)h->h_counters[6];
+    stats->cells_fallback = (long long)h->h_counters[7];
+    if (h->mode == NRG_MODE_SURROGATE) stats->cells_active += stats->cells_surrogate;
+    stats->device_ms = ms;
+  }
+  return NRG_OK;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ API
+extern "C" int nrg_chem_create(const char* mechanism_path, const char* thermo_path,
+                               const char* molar_masses_path, double default_enhanced_efficiencies,
+                               int eact_units, nrg_chem** out) {
+  if (!mechanism_path || !thermo_path || !molar_masses_path || !out)
+    return fail(nullptr, NRG_ERR_ARG, "null argument to nrg_chem_create");
+  if (eact_units < 0 || eact_units > 3) return fail(nullptr, NRG_ERR_ARG, "unknown eact_units");
+  *out = nullptr;
+  nrg_chem* h = new nrg_chem();
+  std::string e = nrg::load_mechanism(mechanism_path, thermo_path, molar_masses_path,
+                                      default_enhanced_efficiencies, (nrg::EactUnits)eact_units, &h->mech);
+  if (!e.empty()) { delete h; return fail(nullptr, NRG_ERR_IO, e); }
+  e = build_dev_mech(h->mech, &h->dm);
+  if (!e.empty()) { delete h; return fail(nullptr, NRG_ERR_UNSUPPORTED, e); }
+  if (!(h->mech.n() == 9 && h->mech.r() == 24)) {
+    std::string msg = "no compiled kernel for " + std::to_string(h->mech.n()) + " species / " +
+                      std::to_string(h->mech.r()) + " reactions";
+    delete h;
+    return fail(nullptr, NRG_ERR_UNSUPPORTED, msg);
+  }
+  cudaError_t ce;
+  if ((ce = cudaGetDevice(&h->device)) != cudaSuccess ||
+      (ce = cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device)) != cudaSuccess ||
+      (ce = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+      (ce = cudaMalloc(&h->d_queue, sizeof(int) * 4)) != cudaSuccess ||
+      (ce = cudaMalloc(&h->d_counters, sizeof(unsigned long long) * 8)) != cudaSuccess ||
+      (ce = cudaMallocHost(&h->h_counters, sizeof(unsigned long long) * 8)) != cudaSuccess ||
+      (ce = cudaEventCreate(&h->ev0)) != cudaSuccess || (ce = cudaEventCreate(&h->ev1)) != cudaSuccess ||
+      (ce = cudaEventCreateWithFlags(&h->ev_in, cudaEventDisableTiming)) != cudaSuccess) {
+    std::string msg = std::string("CUDA initialisation failed: ") + cudaGetErrorString(ce);
+    nrg_chem_destroy(h);
+    return fail(nullptr, NRG_ERR_CUDA, msg);
+  }
+  nrg::upload_mechanism(h->dm, h->stream);
+  if ((ce = cudaStreamSynchronize(h->stream)) != cudaSuccess) {
+    std::string msg = std::string("mechanism upload failed: ") + cudaGetErrorString(ce);
+    nrg_chem_destroy(h);
+    return fail(nullptr, NRG_ERR_CUDA, msg);
+  }
+  h->cfg.persistent = true;
+  h->cfg.block = 128;
+  h->cfg.grid = 0;
+  h->cfg.chunk = 1;
+  h->sur = nrg::surrogate_create(h->dm);
+  *out = h;
+  return NRG_OK;
+}
+
+extern "C" int nrg_chem_destroy(nrg_chem* h) {
+  if (!h) return NRG_ERR_ARG;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->gexec) cudaGraphExecDestroy(h->gexec);
+  nrg::surrogate_destroy(h->sur);
+  free_staging(h);
+  cudaFree(h->d_queue);
+  cudaFree(h->d_counters);
+  cudaFreeHost(h->h_counters);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->ev_in) cudaEventDestroy(h->ev_in);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return NRG_OK;
+}
+
+extern "C" int nrg_chem_set_mode(nrg_chem* h, int mode) {
+  if (!h) return NRG_ERR_ARG;
+  if (mode < NRG_MODE_REFERENCE || mode > NRG_MODE_SURROGATE) return fail(h, NRG_ERR_ARG, "unknown mode");
+  h->mode = mode;
+  return NRG_OK;
+}
+
+extern "C" int nrg_chem_set_launch(nrg_chem* h, int persistent, int block, int grid, int chunk) {
+  if (!h) return NRG_ERR_ARG;
+  if (block < 32 || block > 256 || (block % 32) || chunk < 1 || chunk > 64 || grid < 0)
+    return fail(h, NRG_ERR_ARG, "launch shape out of range (block 32..256 step 32, chunk 1..64)");
+  h->cfg.persistent = persistent != 0;
+  h->cfg.block = block;
+  h->cfg.grid = grid;
+  h->cfg.chunk = chunk;
+  return NRG_OK;
+}
+
+extern "C" int nrg_chem_get_launch(nrg_chem* h, int* persistent, int* block, int* grid, int* chunk) {
+  if (!h) return NRG_ERR_ARG;
+  if (persistent) *persistent = h->cfg.persistent;
+  if (block) *block = h->cfg.block;
+  if (grid) *grid = h->cfg.grid;
+  if (chunk) *chunk = h->cfg.chunk;
+  return NRG_OK;
+}
+
+extern "C" int nrg_chem_set_graph(nrg_chem* h, int enable) {
+  if (!h) return NRG_ERR_ARG;
+  h->use_graph = enable != 0;
+  return NRG_OK;
+}
+
+extern "C" int nrg_chem_step_device(nrg_chem* h, double time_step, long n, long ld, const double* T,
+                                    const double* rho, const double* Y, const signed char* bc,
+                                    double* Y_prod, double* Y_prod2, double* E_f_prod, double* T_after,
+                                    unsigned char* status, void* stream, nrg_chem_stats* stats) {
+  if (!h) return NRG_ERR_ARG;
+  if (n < 0 || ld < n) return fail(h, NRG_ERR_ARG, "need 0 <= n <= ld");
+  if (!(time_step > 0.0) || !std::isfinite(time_step)) return fail(h, NRG_ERR_ARG, "time_step must be > 0");
+  if (n > 0 && (!T || !rho || !Y || !Y_prod || !Y_prod2 || !E_f_prod))
+    return fail(h, NRG_ERR_ARG, "null field pointer");
+  if (n > 0x7fffffffL / 2) return fail(h, NRG_ERR_ARG, "too many cells for one call");
+  CK(h, cudaSetDevice(h->device));
+  StepArgs a;
+  a.n = n;
+  a.ld = ld;
+  a.dt = time_step;
+  a.T = T;
+  a.rho = rho;
+  a.Y = Y;
+  a.bc = (const int8_t*)bc;
+  a.Y_prod = Y_prod;
+  a.Y_prod2 = Y_prod2;
+  a.E_f_prod = E_f_prod;
+  a.T_after = T_after;
+  a.status = status;
+  a.mxstep = 10000;
+  if (n == 0) {
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    return NRG_OK;
+  }
+  // Work runs on the handle's own (capturable) stream, ordered after
+  // everything already queued on the caller's stream (legacy default included).
+  CK(h, cudaEventRecord(h->ev_in, (cudaStream_t)stream));
+  CK(h, cudaStreamWaitEvent(h->stream, h->ev_in, 0));
+  return run_step(h, a, h->stream, stats);
+}
+
+extern "C" int nrg_chem_step(nrg_chem* h, double time_step, const nrg_field_desc* f, nrg_chem_stats* stats) {
+  if (!h || !f) return NRG_ERR_ARG;
+  const int N = h->mech.n();
+  long ext[3], cnt[3];
+  for (int d = 0; d < 3; ++d) {
+    ext[d] = (long)f->ub[d] - f->lb[d] + 1;
+    if (ext[d] <= 0 || f->lo[d] < f->lb[d] || f->hi[d] > f->ub[d])
+      return fail(h, NRG_ERR_ARG, "field bounds inconsistent (need lb <= lo, hi <= ub)");
+    cnt[d] = f->hi[d] >= f->lo[d] ? (long)f->hi[d] - f->lo[d] + 1 : 0;
+  }
+  if (!f->T || !f->rho || !f->E_f_prod) return fail(h, NRG_ERR_ARG, "null T, rho or E_f_prod");
+  for (int k = 0; k < N; ++k)
+    if (!f->Y[k] || !f->Y_prod[k] || !f->Y_prod2[k]) return fail(h, NRG_ERR_ARG, "null species array");
+  const long n = cnt[0] * cnt[1] * cnt[2];
+  if (n == 0) {
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    return NRG_OK;
+  }
+  int rc = ensure_staging(h, (size_t)n);
+  if (rc) return rc;
+  // gather the interior (i fastest, as the reference's collapse(3) loop)
+  auto lin = [&](int i, int j, int k) {
+    return ((long)(k - f->lb[2]) * ext[1] + (j - f->lb[1])) * ext[0] + (i - f->lb[0]);
+  };
+  long c = 0;
+  for (int k = f->lo[2]; k <= f->hi[2]; ++k)
+    for (int j = f->lo[1]; j <= f->hi[1]; ++j)
+      for (int i = f->lo[0]; i <= f->hi[0]; ++i, ++c) {
+        long L = lin(i, j, k);
+        h->h_T[c] = f->T[L];
+        h->h_rho[c] = f->rho[L];
+        h->h_bc[c] = f->bc_markers ? f->bc_markers[L] : 0;
+        for (int s = 0; s < N; ++s) h->h_Y[(size_t)s * n + c] = f->Y[s][L];
+      }
+  cudaStream_t s = h->stream;
+  CK(h, cudaMemcpyAsync(h->d_T, h->h_T, n * 8, cudaMemcpyHostToDevice, s));
+  CK(h, cudaMemcpyAsync(h->d_rho, h->h_rho, n * 8, cudaMemcpyHostToDevice, s));
+  CK(h, cudaMemcpyAsync(h->d_Y, h->h_Y, (size_t)N * n * 8, cudaMemcpyHostToDevice, s));
+  CK(h, cudaMemcpyAsync(h->d_bc, h->h_bc, n, cudaMemcpyHostToDevice, s));
+  StepArgs a;
+  a.n = n;
+  a.ld = n;
+  a.dt = time_step;
+  a.T = h->d_T;
+  a.rho = h->d_rho;
+  a.Y = h->d_Y;
+  a.bc = h->d_bc;
+  a.Y_prod = h->d_Yp;
+  a.Y_prod2 = h->d_Yp2;
+  a.E_f_prod = h->d_Ef;
+  a.T_after = nullptr;
+  a.status = h->d_status;
+  a.mxstep = 10000;
+  if (!(time_step > 0.0)) return fail(h, NRG_ERR_ARG, "time_step must be > 0");
+  rc = run_step(h, a, s, stats);
+  if (rc) return rc;
+  CK(h, cudaMemcpyAsync(h->h_Yp, h->d_Yp, (size_t)N * n * 8, cudaMemcpyDeviceToHost, s));
+  CK(h, cudaMemcpyAsync(h->h_Yp2, h->d_Yp2, (size_t)N * n * 8, cudaMemcpyDeviceToHost, s));
+  CK(h, cudaMemcpyAsync(h->h_Ef, h->d_Ef, n * 8, cudaMemcpyDeviceToHost, s));
+  CK(h, cudaMemcpyAsync(h->h_status, h->d_status, n, cudaMemcpyDeviceToHost, s));
+  CK(h, cudaStreamSynchronize(s));
+  c = 0;
+  for (int k = f->lo[2]; k <= f->hi[2]; ++k)
+    for (int j = f->lo[1]; j <= f->hi[1]; ++j)
+      for (int i = f->lo[0]; i <= f->hi[0]; ++i, ++c) {
+        long L = lin(i, j, k);
+        f->E_f_prod[L] = h->h_Ef[c];
+        const bool touched = h->h_status[c] != NRG_CELL_SKIPPED;
+        for (int sp = 0; sp < N; ++sp) {
+          f->Y_prod[sp][L] = h->h_Yp[(size_t)sp * n + c];
+          if (touched) f->Y_prod2[sp][L] = h->h_Yp2[(size_t)sp * n + c];  // reference leaves it
+        }
+      }
+  return NRG_OK;
+}
+
+extern "C" int nrg_chem_autotune(nrg_chem* h, double time_step, long n, long ld, const double* T,
+                                 const double* rho, const double* Y, const signed char* bc, double* Y_prod,
+                                 double* Y_prod2, double* E_f_prod, double* ms_best) {
+  if (!h) return NRG_ERR_ARG;
+  if (n <= 0 || ld < n || !T || !rho || !Y || !Y_prod || !Y_prod2 || !E_f_prod)
+    return fail(h, NRG_ERR_ARG, "autotune needs device inputs with n > 0");
+  CK(h, cudaSetDevice(h->device));
+  StepArgs a;
+  a.n = n; a.ld = ld; a.dt = time_step; a.T = T; a.rho = rho; a.Y = Y; a.bc = (const int8_t*)bc;
+  a.Y_prod = Y_prod; a.Y_prod2 = Y_prod2; a.E_f_prod = E_f_prod; a.T_after = nullptr; a.status = nullptr;
+  a.mxstep = 10000;
+  std::vector<LaunchCfg> cands;
+  for (int block : {64, 128, 256})
+    for (int per_sm : {1, 2, 3, 4})
+      for (int chunk : {1, 2, 4}) {
+        if (block * per_sm > 1024) continue;
+        LaunchCfg c;
+        c.persistent = true;
+        c.block = block;
+        c.grid = per_sm * h->num_sms;
+        c.chunk = chunk;
+        cands.push_back(c);
+      }
+  {
+    LaunchCfg c;
+    c.persistent = false;
+    c.block = 128;
+    cands.push_back(c);
+  }
+  cudaStream_t s = h->stream;
+  float best = 1e30f;
+  LaunchCfg best_cfg = h->cfg;
+  for (const LaunchCfg& c : cands) {
+    CK(h, cudaMemsetAsync(h->d_counters, 0, sizeof(unsigned long long) * 8, s));
+    CK(h, cudaEventRecord(h->ev0, s));
+    cudaError_t e = enqueue_integrator(h, a, c, s);
+    if (e != cudaSuccess) return cuda_fail(h, e, "autotune launch");
+    CK(h, cudaEventRecord(h->ev1, s));
+    CK(h, cudaStreamSynchronize(s));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    if (ms < best) { best = ms; best_cfg = c; }
+  }
+  h->cfg = best_cfg;
+  if (ms_best) *ms_best = best;
+  return NRG_OK;
+}
+
+extern "C" int nrg_chem_info(nrg_chem* h, int* n_species, int* n_reactions) {
+  if (!h) return NRG_ERR_ARG;
+  if (n_species) *n_species = h->mech.n();
+  if (n_reactions) *n_reactions = h->mech.r();
+  return NRG_OK;
+}
+
+static void fill_tables(const nrg::Mechanism& m, int* reaction_type, int* coeffs, double* arrhenius,
+                        double* troe3, double* eff, double* a_coeffs, double* molar_mass) {
+  const int N = m.n(), R = m.r();
+  for (int r = 0; r < R; ++r) {
+    const nrg::Reaction& rx = m.reactions[r];
+    if (reaction_type) reaction_type[r] = rx.type;
+    if (coeffs) {
+      int* L = coeffs + (0 * R + r) * 4;
+      int* P = coeffs + (1 * R + r) * 4;
+      L[0] = rx.n_left; P[0] = rx.n_right;
+      for (int i = 0; i < 3; ++i) { L[1 + i] = rx.left[i]; P[1 + i] = rx.right[i]; }
+    }
+    if (arrhenius) {
+      double* A = arrhenius + r * 9;
+      A[0] = rx.A; A[1] = rx.beta; A[2] = rx.E; A[3] = rx.A_low; A[4] = rx.beta_low; A[5] = rx.E_low;
+      A[6] = rx.troe[0]; A[7] = rx.troe[1]; A[8] = rx.troe[2];
+    }
+    if (troe3) troe3[r] = rx.troe[3];
+  }
+  if (eff) std::memcpy(eff, m.eff.data(), sizeof(double) * (size_t)R * N);
+  if (a_coeffs) std::memcpy(a_coeffs, m.a_coeffs.data(), sizeof(double) * (size_t)N * 14);
+  if (molar_mass) std::memcpy(molar_mass, m.molar_mass.data(), sizeof(double) * (size_t)N);
+}
+
+extern "C" int nrg_chem_tables(nrg_chem* h, int* reaction_type, int* coeffs, double* arrhenius, double* troe3,
+                               double* eff, double* a_coeffs, double* molar_mass) {
+  if (!h) return NRG_ERR_ARG;
+  fill_tables(h->mech, reaction_type, coeffs, arrhenius, troe3, eff, a_coeffs, molar_mass);
+  return NRG_OK;
+}
+
+extern "C" int nrg_mech_tables(const char* mechanism_path, const char* thermo_path,
+                               const char* molar_masses_path, double default_enhanced_efficiencies,
+                               int eact_units, int* n_species, int* n_reactions, int* reaction_type,
+                               int* coeffs, double* arrhenius, double* troe3, double* eff,
+                               double* a_coeffs, double* molar_mass) {
+  if (!mechanism_path || !thermo_path || !molar_masses_path)
+    return fail(nullptr, NRG_ERR_ARG, "null path");
+  if (eact_units < 0 || eact_units > 3) return fail(nullptr, NRG_ERR_ARG, "unknown eact_units");
+  nrg::Mechanism m;
+  std::string e = nrg::load_mechanism(mechanism_path, thermo_path, molar_masses_path,
+                                      default_enhanced_efficiencies, (nrg::EactUnits)eact_units, &m);
+  if (!e.empty()) return fail(nullptr, NRG_ERR_IO, e);
+  if (n_species) *n_species = m.n();
+  if (n_reactions) *n_reactions = m.r();
+  fill_tables(m, reaction_type, coeffs, arrhenius, troe3, eff, a_coeffs, molar_mass);
+  return NRG_OK;
+}
+
+extern "C" int nrg_chem_species_name(nrg_chem* h, int k, char* buf, int buflen) {
+  if (!h || !buf || buflen <= 0 || k < 0 || k > h->mech.n()) return NRG_ERR_ARG;
+  std::string s = k == h->mech.n() ? std::string("M") : h->mech.species[k];
+  std::snprintf(buf, (size_t)buflen, "%s", s.c_str());
+  return NRG_OK;
+}
+
+extern "C" const char* nrg_chem_last_error(nrg_chem* h) {
+  return h ? h->err.c_str() : g_create_error.c_str();
+}
+
+extern "C" int nrg_fp64_peak_tflops(double* tflops) {
+  if (!tflops) return NRG_ERR_ARG;
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return NRG_ERR_CUDA;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  double* out = nullptr;
+  if (cudaMalloc(&out, 8) != cudaSuccess) return NRG_ERR_CUDA;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int blocks = sms * 8, threads = 256, iters = 4096;
+  nrg::launch_fp64_peak(out, blocks, threads, 64, nullptr);  // warm-up
+  cudaEventRecord(e0);
+  nrg::launch_fp64_peak(out, blocks, threads, iters, nullptr);
+  cudaEventRecord(e1);
+  cudaError_t e = cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  if (e != cudaSuccess) return NRG_ERR_CUDA;
+  const double flops = 2.0 * 8 * 16 * (double)iters * blocks * threads;
+  *tflops = flops / (ms * 1e-3) / 1e12;
+  return NRG_OK;
+}

@@ -1,0 +1,57 @@
+// Device-side mechanism tables and per-cell chemistry for the NRG step.
+//
+// Layout: one thread integrates one cell.  Mechanism constants live in
+// __constant__ memory: every lane of a warp walks the same reaction at the same
+// time, so each table read is a broadcast.  Cell fields are SoA in HBM
+// (species-major, cell-minor) so a warp's loads/stores of one species are
+// coalesced 256-byte transactions.
+#pragma once
+
+#include <cstdint>
+
+namespace nrg {
+
+constexpr int kMaxSpecies = 16;
+constexpr int kMaxReactions = 64;
+constexpr int kMaxOrd = 5;  // MXORD for Gear (MINT = 2)
+
+// Per-reaction update list entry: species (0-based) and whether the
+// occurrence is a reactant (Zdot -= f, += r) or a product (Zdot -= r, += f).
+// Entries are ordered species-major, reactants before products, which is the
+// accumulation order of the reference RHS (chemical_kinetics_solver.f90:528-535).
+struct DevMech {
+  int N, R;
+  int type[kMaxReactions];
+  int nl[kMaxReactions], nr[kMaxReactions];
+  int left[kMaxReactions][3], right[kMaxReactions][3];  // 0-based, -1 = M
+  int nupd[kMaxReactions];
+  int upd_k[kMaxReactions][6];
+  int upd_prod[kMaxReactions][6];
+  double A[kMaxReactions], beta[kMaxReactions], E[kMaxReactions];
+  double A_low[kMaxReactions], beta_low[kMaxReactions], E_low[kMaxReactions];
+  double troe[kMaxReactions][4];
+  double dnu[kMaxReactions];
+  double eff[kMaxReactions][kMaxSpecies];
+  double a[kMaxSpecies][2][7];  // NASA-7 times R
+  double W[kMaxSpecies];
+  double invW[kMaxSpecies];
+  double h_ref[kMaxSpecies];   // h_k(T_ref)
+  // integrator constants (host-computed so host and device agree bit-for-bit)
+  double el[13 * 12], tq[3 * 12];
+  double eps, ewt, hmax, uround;
+  double sqrt_uround, br, bl, bp, facmin;
+  // element composition for conservation checks (H, O, N) in atoms/molecule
+  double elem[3][kMaxSpecies];
+};
+
+// Per-cell status byte written by the integrator.
+enum CellStatus : uint8_t {
+  kCellSkipped = 0,   // T < 305 K or bc /= 0: zero sources (reference rule)
+  kCellOk = 1,
+  kCellMxstep = 2,    // MXSTEP reached; state at the current T returned
+  kCellFatal = 3,     // step size vanished / too many retries / singular
+  kCellNonfinite = 4, // non-finite input or output
+  kCellSurrogate = 5  // accepted surrogate prediction (gated path)
+};
+
+}  // namespace nrg

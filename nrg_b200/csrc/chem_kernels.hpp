@@ -1,0 +1,47 @@
+// Host-visible declarations of the chemistry kernels' launch interface.
+#pragma once
+
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+namespace nrg {
+
+struct DevMech;
+
+// Arguments of one chemistry step over n cells.  Species arrays are
+// species-major: element (k, c) lives at [k * ld + c].
+struct StepArgs {
+  long n;
+  long ld;
+  double dt;
+  const double* T;
+  const double* rho;
+  const double* Y;
+  const int8_t* bc;   // may be null: every cell interior
+  double* Y_prod;
+  double* Y_prod2;
+  double* E_f_prod;
+  double* T_after;    // may be null
+  uint8_t* status;    // may be null
+  int mxstep;
+};
+
+struct LaunchCfg {
+  bool persistent = true;  // work-queue kernel (else one thread per cell)
+  int block = 128;         // threads per block
+  int grid = 0;            // persistent grid size (0: one block per SM)
+  int chunk = 1;           // cells a lane reserves per queue fetch
+};
+
+void upload_mechanism(const DevMech& m, cudaStream_t s);
+
+// jac: 0 finite-difference (reference DDPST), 1 analytic.  mixed: float LU.
+// queue must point at a zeroed device int when cfg.persistent.
+cudaError_t launch_chem(int n_species, int n_reactions, int jac, bool mixed, const StepArgs& a,
+                        const LaunchCfg& cfg, int* queue, unsigned long long* counters,
+                        cudaStream_t s);
+
+cudaError_t launch_fp64_peak(double* out, int blocks, int threads, int iters, cudaStream_t s);
+
+}  // namespace nrg

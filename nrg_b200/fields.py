@@ -1,0 +1,141 @@
+"""Seeded synthetic cell fields for the chemistry-step workloads.
+
+Composition model (as the reference's H2/air set-ups,
+package_interface/src/tests/classic_tests/1D_laminar_velocity.f90:269-271,
+477-480): stoichiometric H2/air reactants H2:O2:N2 = 2:1:3.762 (mole), products
+H2O:N2 = 2:3.762, blended in mass by a progress variable c, radicals
+H, O, OH, HO2, H2O2 set separately, renormalised; rho = p W / (R T).
+Species order is the mechanism's (KEROMNES: H2 O2 N2 O H OH H2O HO2 H2O2).
+Arrays are species-major: Y[k, cell].
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+R_GAS = 8.31446261815324
+P_ATM = 101325.0
+SPECIES = ["H2", "O2", "N2", "O", "H", "OH", "H2O", "HO2", "H2O2"]
+RADICALS = ["H", "O", "OH", "HO2", "H2O2"]
+# Frozen-temperature ignition temperature of the stoichiometric mixture at
+# 1 atm for which the time of peak OH production is 1e-5 s (oracle bisection,
+# tests/golden/make_ignition_temperature.py).
+T_IGNITION_1E5 = 1586.9
+
+
+@dataclass
+class Field:
+    name: str
+    T: np.ndarray       # (n,)
+    rho: np.ndarray     # (n,)
+    p: np.ndarray       # (n,)
+    Y: np.ndarray       # (N, n)
+    dt: float
+    shape: tuple
+    dt_cells: np.ndarray | None = None  # per-cell dt (training pairs)
+
+    @property
+    def n(self) -> int:
+        return self.T.shape[0]
+
+
+def _stoich(W: np.ndarray):
+    idx = {s: i for i, s in enumerate(SPECIES)}
+    Xr = np.zeros(len(SPECIES))
+    Xr[idx["H2"]], Xr[idx["O2"]], Xr[idx["N2"]] = 2.0, 1.0, 3.762
+    Xp = np.zeros(len(SPECIES))
+    Xp[idx["H2O"]], Xp[idx["N2"]] = 2.0, 3.762
+    Yr = Xr * W / np.sum(Xr * W)
+    Yp = Xp * W / np.sum(Xp * W)
+    return Yr, Yp, idx
+
+
+def _finish(name, T, p, Y, W, dt, shape, dt_cells=None) -> Field:
+    Y = Y / Y.sum(axis=0, keepdims=True)
+    Wmix = 1.0 / np.sum(Y / W[:, None], axis=0)
+    rho = p * Wmix / (R_GAS * T)
+    return Field(name, np.ascontiguousarray(T), np.ascontiguousarray(rho), np.ascontiguousarray(p),
+                 np.ascontiguousarray(Y), dt, shape, dt_cells)
+
+
+def random_state(n: int, rng: np.random.Generator, W: np.ndarray, T_lo: float, T_hi: float,
+                 p_lo: float = 1.0, p_hi: float = 1.0):
+    Yr, Yp, idx = _stoich(W)
+    T = rng.uniform(T_lo, T_hi, n)
+    c = rng.uniform(0.0, 1.0, n)
+    p = P_ATM * (rng.uniform(p_lo, p_hi, n) if p_hi > p_lo else np.full(n, p_lo))
+    Y = (1.0 - c)[None, :] * Yr[:, None] + c[None, :] * Yp[:, None]
+    for s in RADICALS:
+        Y[idx[s]] = 10.0 ** rng.uniform(-8.0, -3.0, n)
+    return T, p, Y
+
+
+def config0(W: np.ndarray, n_side: int = 64) -> Field:
+    """4,096 cells, T ~ U[1000, 2400] K, p = 1 atm, dt = 1e-6 s."""
+    rng = np.random.Generator(np.random.PCG64(0))
+    n = n_side * n_side
+    T, p, Y = random_state(n, rng, W, 1000.0, 2400.0)
+    return _finish("config0", T, p, Y, W, 1e-6, (n_side, n_side))
+
+
+def config1(W: np.ndarray, n_side: int = 512) -> Field:
+    """262,144 cells, dt = 1e-5 s; 20 % of cells within +-50 K of the
+    temperature whose ignition delay is 1e-5 s (uneven substep counts)."""
+    rng = np.random.Generator(np.random.PCG64(1))
+    n = n_side * n_side
+    T, p, Y = random_state(n, rng, W, 1000.0, 2400.0)
+    hot = rng.uniform(0.0, 1.0, n) < 0.2
+    T[hot] = T_IGNITION_1E5 + rng.uniform(-50.0, 50.0, int(hot.sum()))
+    return _finish("config1", T, p, Y, W, 1e-5, (n_side, n_side))
+
+
+def config2(W: np.ndarray, n_side: int = 1024, seed: int = 2) -> Field:
+    """1,048,576 cells, T ~ U[800, 2600] K, p ~ U[0.5, 5] atm, dt = 1e-5 s."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    n = n_side * n_side
+    T, p, Y = random_state(n, rng, W, 800.0, 2600.0, 0.5, 5.0)
+    return _finish("config2", T, p, Y, W, 1e-5, (n_side, n_side))
+
+
+def config3_pairs(W: np.ndarray, n: int, seed: int = 3) -> Field:
+    """Training states: the config-2 distribution with dt ~ log-U[1e-7, 1e-5]."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    T, p, Y = random_state(n, rng, W, 800.0, 2600.0, 0.5, 5.0)
+    dts = 10.0 ** rng.uniform(-7.0, -5.0, n)
+    return _finish("config3", T, p, Y, W, float("nan"), (n,), dts)
+
+
+def config4(W: np.ndarray, n_side: int = 2048, seed: int = 4) -> Field:
+    """Premixed-flame-like field: 2048 x 2048 cells of 10 um, tanh front
+    (delta = 0.5 mm) from 300 K to 2400 K along x, front position perturbed in
+    y by 8 seeded sinusoids of amplitude 0.2 mm, radicals Gaussian at the front
+    with peak mass fraction 1e-3, p = 1 atm, dt = 1e-6 s."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    dx = 10e-6
+    delta = 0.5e-3
+    L = n_side * dx
+    x = (np.arange(n_side) + 0.5) * dx
+    y = (np.arange(n_side) + 0.5) * dx
+    modes = rng.integers(1, 17, 8)
+    phases = rng.uniform(0.0, 2.0 * np.pi, 8)
+    xf = 0.5 * L + np.sum(0.2e-3 * np.sin(2.0 * np.pi * modes[:, None] * y[None, :] / L + phases[:, None]), axis=0)
+    # cell (i, j) with i along x fastest: flat index j * n_side + i
+    s = (x[None, :] - xf[:, None]) / delta
+    c = 0.5 * (1.0 + np.tanh(s))
+    T = 300.0 + 2100.0 * c
+    Yr, Yp, idx = _stoich(W)
+    cf = c.reshape(-1)
+    Y = (1.0 - cf)[None, :] * Yr[:, None] + cf[None, :] * Yp[:, None]
+    g = np.exp(-0.5 * (s.reshape(-1)) ** 2)
+    for sp in RADICALS:
+        Y[idx[sp]] = 1e-3 * g
+    n = n_side * n_side
+    return _finish("config4", T.reshape(-1), np.full(n, P_ATM), Y, W, 1e-6, (n_side, n_side))
+
+
+def slice_field(f: Field, n: int, stride: int = 1, offset: int = 0) -> Field:
+    sel = np.arange(offset, offset + n * stride, stride) % f.n
+    return Field(f.name + f"[{n}]", f.T[sel].copy(), f.rho[sel].copy(), f.p[sel].copy(),
+                 np.ascontiguousarray(f.Y[:, sel]), f.dt, (n,),
+                 None if f.dt_cells is None else f.dt_cells[sel].copy())

@@ -1,0 +1,40 @@
+"""The C-ABI library loads and exports every symbol include/nrg_chem.h declares."""
+import os
+import re
+
+from nrg_b200 import chemistry
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    out = set()
+    for f in os.listdir(os.path.join(ROOT, "include")):
+        if f.endswith(".h"):
+            src = open(os.path.join(ROOT, "include", f)).read()
+            out |= set(re.findall(r"NRG_API\s+[\w\s\*]+?\b(nrg_\w+)\s*\(", src))
+    return out
+
+
+def test_every_declared_symbol_is_exported():
+    names = declared_symbols()
+    assert len(names) >= 15
+    L = chemistry.lib()
+    for n in sorted(names):
+        assert hasattr(L, n), n
+
+
+def test_bindings_cover_the_header():
+    assert declared_symbols() <= set(chemistry.SIGNATURES)
+
+
+def test_create_error_is_reported_without_gpu(decks, tmp_path):
+    import ctypes
+    import pytest
+    L = chemistry.lib()
+    h = ctypes.c_void_p()
+    rc = L.nrg_chem_create(str(tmp_path / "missing.txt").encode(), decks[1].encode(), decks[2].encode(),
+                           1.0, 2, ctypes.byref(h))
+    assert rc == -2 and b"cannot open" in L.nrg_chem_last_error(None)
+    with pytest.raises(chemistry.NrgError):
+        chemistry.ChemicalKineticsSolver(None, str(tmp_path / "missing.txt"), *decks[1:])

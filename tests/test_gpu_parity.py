@@ -1,0 +1,131 @@
+"""Parity of the CUDA integrator with the CPU oracle, through the C ABI.
+
+Tolerances (from the task statement for the plain FP64 form):
+|dY| <= 1e-9 (mass fraction after the step) and |dT|/T <= 1e-6, where T is
+the temperature after the reference energy closure."""
+import numpy as np
+import pytest
+
+from nrg_b200 import fields
+from tests.gpu_util import dY, run_device
+
+pytestmark = pytest.mark.gpu
+
+TOL_Y = 1e-9
+TOL_T = 1e-6
+
+
+@pytest.fixture(scope="module")
+def solver(decks):
+    from nrg_b200.chemistry import ChemicalKineticsSolver
+    s = ChemicalKineticsSolver(None, *decks, mode="reference")
+    yield s
+    s.close()
+
+
+def oracle_run(oracle_mech, f, bc=None):
+    o = oracle_mech.chem_step(f.dt, f.T, f.rho, f.Y, bc=bc)
+    o["T_after"] = oracle_mech.temperature_after(f.dt, f.T, f.rho, f.Y, o["Y_prod"], o["E_f_prod"])
+    return o
+
+
+def check_parity(g, o, f, active):
+    err_y = np.max(np.abs(dY(g, f)[:, active] - dY(o, f)[:, active]))
+    err_t = np.max(np.abs(g["T_after"][active] - o["T_after"][active]) / f.T[active])
+    assert err_y <= TOL_Y, f"max |dY| = {err_y:.3e}"
+    assert err_t <= TOL_T, f"max |dT|/T = {err_t:.3e}"
+    return err_y, err_t
+
+
+@pytest.mark.parametrize("mode", ["reference", "fast"])
+def test_config0_parity(solver, oracle_mech, W, mode):
+    f = fields.config0(W)
+    o = oracle_run(oracle_mech, f)
+    g, st = run_device(solver, f, mode)
+    assert np.all(g["status"] == 1)
+    check_parity(g, o, f, np.ones(f.n, bool))
+    assert st["cells_active"] == f.n
+    if mode == "reference":
+        # same algorithm, same decisions: the work counters agree closely
+        assert abs(st["steps"] - o["nstep"].sum()) <= 0.01 * o["nstep"].sum()
+        assert abs(st["rhs_evals"] - o["nfe"].sum()) <= 0.01 * o["nfe"].sum()
+
+
+def test_config1_sample_parity(solver, oracle_mech, W):
+    f = fields.slice_field(fields.config1(W, n_side=128), 2048, stride=7)
+    o = oracle_run(oracle_mech, f)
+    for mode in ("reference", "fast"):
+        g, _ = run_device(solver, f, mode)
+        check_parity(g, o, f, np.ones(f.n, bool))
+
+
+def test_launch_shapes_and_graph_agree(solver, W):
+    f = fields.config0(W)
+    base, _ = run_device(solver, f, "fast", launch=dict(persistent=False, block=128))
+    for launch in (dict(persistent=True, block=128, grid=0, chunk=1),
+                   dict(persistent=True, block=64, grid=296, chunk=4),
+                   dict(persistent=True, block=256, grid=148, chunk=2)):
+        for graph in (True, False):
+            g, _ = run_device(solver, f, "fast", launch=launch, graph=graph)
+            for k in ("Y_prod", "Y_prod2", "E_f_prod", "T_after"):
+                np.testing.assert_array_equal(g[k], base[k])
+    solver.set_launch(persistent=True, block=128, grid=0, chunk=1)
+
+
+def test_skip_rule_bc_and_untouched_y_prod2(solver, oracle_mech, W):
+    f = fields.slice_field(fields.config0(W), 1024)
+    f.T[:32] = 300.0
+    bc = np.zeros(f.n, np.int8)
+    bc[32:64] = 1
+    init2 = np.full((9, f.n), 3.25)
+    g, st = run_device(solver, f, "reference", bc=bc, y_prod2_init=init2)
+    o = oracle_run(oracle_mech, f, bc=bc)
+    assert np.all(g["status"][:64] == 0) and np.all(g["status"][64:] == 1)
+    assert np.all(g["Y_prod"][:, :64] == 0.0) and np.all(g["E_f_prod"][:64] == 0.0)
+    assert np.all(g["Y_prod2"][:, :64] == 3.25)
+    assert st["cells_active"] == f.n - 64
+    act = np.arange(f.n) >= 64
+    check_parity(g, o, f, act)
+
+
+def test_empty_and_nonfinite_inputs(solver, W):
+    import torch
+    f = fields.slice_field(fields.config0(W), 256)
+    z = torch.zeros((9, 0), dtype=torch.float64, device="cuda")
+    e = torch.zeros(0, dtype=torch.float64, device="cuda")
+    st = solver.step_device(1e-6, e, e, z, z, z, e)
+    assert st["cells"] == 0
+    f.Y[4, :16] = np.nan
+    g, st = run_device(solver, f, "fast")
+    assert np.all(g["status"][:16] == 4) and np.all(g["status"][16:] == 1)
+    assert st["cells_bad"] >= 16
+
+
+def test_host_layout_drop_in(decks, oracle_mech, W):
+    """solve_chemical_kinetics on Fortran-layout host arrays with ghost cells."""
+    from nrg_b200.chemistry import DataManager, chemical_kinetics_solver_c
+    f = fields.config0(W)
+    nx, ny = f.shape
+    m = DataManager.block(nx, ny)
+    T = m.create_scalar_field("temperature")
+    m.create_scalar_field("pressure")
+    rho = m.create_scalar_field("density")
+    Y = m.create_vector_field("specie_mass_fraction", 9)
+    bc = np.zeros(m.shape, np.int8, order="F")
+    m.fields["bc_markers"] = bc
+    m.interior(T)[...] = f.T.reshape(ny, nx).T[:, :, None]
+    m.interior(rho)[...] = f.rho.reshape(ny, nx).T[:, :, None]
+    for k in range(9):
+        m.interior(Y[k])[...] = f.Y[k].reshape(ny, nx).T[:, :, None]
+    T[0, :, :] = 2000.0  # ghost cells hold data that must not be touched or read
+    s = chemical_kinetics_solver_c(m, *decks, mode="reference")
+    for k in range(9):
+        m.fields["specie_production_chemistry2"][k][...] = -1.0
+    st = s.solve_chemical_kinetics(f.dt)
+    assert st["cells"] == f.n
+    o = oracle_mech.chem_step(f.dt, f.T, f.rho, f.Y)
+    yp = np.stack([m.interior(a)[:, :, 0].T.reshape(-1) for a in m.fields["specie_production_chemistry"]])
+    np.testing.assert_allclose(yp * f.dt / f.rho, o["Y_prod"] * f.dt / f.rho, rtol=0, atol=TOL_Y)
+    # ghost layer untouched
+    assert np.all(m.fields["specie_production_chemistry2"][0][0, :, :] == -1.0)
+    s.close()
