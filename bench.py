@@ -1,0 +1,350 @@
+#!/usr/bin/env python
+"""Chemistry-step throughput on B200 (cell-updates/s), one JSON line.
+
+Workload (default): the 2048 x 2048 premixed-flame field (4,194,304 cells,
+dt = 1e-6 s, p = 1 atm) of the H2/air KEROMNES mechanism, synthetic and seeded
+(nrg_b200/fields.py: config4).  A step is one chemistry step over the whole
+field.  Inputs (370 MB of FP64 state) are larger than the 126 MB L2, so no
+flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--mode surrogate|fast|reference|mixed]
+  python bench.py --impl reference ...   # CPU restatement of the reference path
+
+Multi-GPU (torchrun): every rank integrates its own full field (weak scaling,
+no collective on the data path); time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "chem cell-updates/s: surrogate+fallback vs plain FP64, same GPU, |ΔT|≤1 K"
+UNIT = "cell-updates/s"
+H2D_BYTES_PER_CELL = 11 * 8 + 1   # T, rho, 9 Y, bc
+D2H_BYTES_PER_CELL = 19 * 8 + 1   # 9 Y_prod, 9 Y_prod2, E_f_prod, status
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--mode", default="auto", choices=["auto", "surrogate", "fast", "reference", "mixed"])
+    p.add_argument("--n-side", type=int, default=2048)
+    p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+# --------------------------------------------------------------- helpers
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.rows = []
+        self._p = None
+        self._t = None
+
+    def __enter__(self):
+        try:
+            self._p = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                        "--format=csv,noheader,nounits", "-lms", "200"],
+                                       stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self._p = None
+        return self
+
+    def _read(self):
+        for line in self._p.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self._p:
+            self._p.terminate()
+            try:
+                self._p.wait(timeout=5)
+            except Exception:
+                self._p.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for i, nm in enumerate(names):
+                    if r[5 + i].lower().startswith("active"):
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def flop_model(tables: dict, mode: str) -> dict:
+    """Algorithmic FP64 flops per counted event (reference formulation).
+
+    rhs   : per reaction, one multiply per reactant and product factor and two
+            adds per species update (chemical_kinetics_solver.f90:509-536)
+    lu    : DGEFA on N x N: sum_k (N-k) + 2 (N-k)^2
+    solve : DGESL: N(N-1) forward + N + N(N-1) backward, plus the corrector's
+            residual and weighted norm (6N)
+    jac   : FD (reference): 2N^2 to form columns and the matrix (its N right-hand
+            sides are counted as rhs); analytic: partial products and updates
+    step  : predictor, Nordsieck update, error weights and norms (~30N)
+    setup : 9 NASA-7 species x 40 + 24 reactions x 30 (transcendentals as 1)
+    """
+    co = tables["coeffs"]
+    N, R = tables["n_species"], tables["n_reactions"]
+    f_rhs = 0
+    f_jac = 0
+    for r in range(R):
+        nl, nr = co[0][r][0], co[1][r][0]
+        left = [x for x in co[0][r][1:1 + nl] if x != N + 1]
+        right = [x for x in co[1][r][1:1 + nr] if x != N + 1]
+        nupd = len(left) + len(right)
+        f_rhs += nl + nr + 2 * nupd
+        for side in (left, right):
+            f_jac += len(side) * (max(len(side) - 1, 0) + 1 + nupd)
+    f_lu = sum((N - k) + 2 * (N - k) ** 2 for k in range(1, N))
+    f_sol = N * (N - 1) + N + N * (N - 1) + 6 * N
+    f_jacform = 2 * N * N if mode == "reference" else f_jac + N * N
+    return dict(rhs=f_rhs, lu=f_lu, solve=f_sol, jac=f_jacform + f_lu, step=30 * N,
+                setup=9 * 40 + 24 * 30)
+
+
+def algorithmic_flops(st: dict, fm: dict) -> float:
+    return (st["cells_active"] * fm["setup"] + st["rhs_evals"] * fm["rhs"] + st["jacobians"] * fm["jac"]
+            + st["solves"] * fm["solve"] + st["steps"] * fm["step"])
+
+
+def load_peaks() -> dict:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return json.load(fh)
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "fallback": True}
+
+
+def cpu_baseline(field, W, decks, seconds: float) -> dict:
+    """CPU restatement of the reference path (oracle, all host cores) on a
+    strided sample of the same field, sized to about `seconds` of work."""
+    from oracle import oracle_py as op
+    from nrg_b200 import fields as F
+    m = op.Mechanism(*decks, 1.0, "cal.mol")
+    cores = os.cpu_count() or 1
+    n0 = 2048
+    probe = F.slice_field(field, n0, stride=max(1, field.n // n0), offset=1)
+    t0 = time.perf_counter()
+    m.chem_step(probe.dt, probe.T, probe.rho, probe.Y, threads=cores)
+    rate = n0 / max(time.perf_counter() - t0, 1e-6)
+    n = int(min(field.n, max(n0, rate * seconds)))
+    samp = F.slice_field(field, n, stride=max(1, field.n // n), offset=7)
+    t0 = time.perf_counter()
+    m.chem_step(samp.dt, samp.T, samp.rho, samp.Y, threads=cores)
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{n} cells, every {max(1, field.n // n)}th cell of the {field.name} field "
+                      f"({dt:.1f} s, OpenMP dynamic schedule)"}
+
+
+# ------------------------------------------------------------ reference arm
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from nrg_b200 import fields as F, keromnes_paths
+    from nrg_b200.chemistry import mechanism_tables
+    decks = keromnes_paths()
+    W = mechanism_tables(*decks)["molar_mass"]
+    field = F.config4(W, n_side=args.n_side)
+    from oracle import oracle_py as op
+    m = op.Mechanism(*decks, 1.0, "cal.mol")
+    cores = os.cpu_count() or 1
+    # sample sized so that a step takes ~ cpu-seconds
+    n0 = 2048
+    probe = F.slice_field(field, n0, stride=max(1, field.n // n0), offset=1)
+    t0 = time.perf_counter()
+    m.chem_step(probe.dt, probe.T, probe.rho, probe.Y, threads=cores)
+    rate = n0 / max(time.perf_counter() - t0, 1e-6)
+    n = int(min(field.n, max(n0, rate * args.cpu_seconds)))
+    samp = F.slice_field(field, n, stride=max(1, field.n // n), offset=7)
+    for _ in range(args.warmup):
+        m.chem_step(samp.dt, samp.T, samp.rho, samp.Y, threads=cores)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        m.chem_step(samp.dt, samp.T, samp.rho, samp.Y, threads=cores)
+    el = time.perf_counter() - t0
+    value = args.steps * n / el
+    sample = (f"{n} cells per step, every {max(1, field.n // n)}th cell of the {args.n_side}x{args.n_side} flame field; "
+              f"C restatement of the reference Fortran + SLATEC DDRIV3 path (no Fortran compiler on the box)")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": f"flame field {args.n_side}x{args.n_side} ({field.n:,} cells), "
+                                                    "dt=1e-6 s, p=1 atm, KEROMNES H2/air; CPU sample"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ our arm
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    from nrg_b200 import fields as F, keromnes_paths
+    from nrg_b200.chemistry import ChemicalKineticsSolver, DataManager, fp64_peak_tflops, mechanism_tables
+    decks = keromnes_paths()
+    tables = mechanism_tables(*decks)
+    W = tables["molar_mass"]
+    field = F.config4(W, n_side=args.n_side)
+    n = field.n
+    mode = args.mode
+    solver = ChemicalKineticsSolver(None, *decks, mode="fast")
+    if mode == "auto":
+        mode = "fast"
+    solver.set_mode(mode)
+    dev = torch.device("cuda", local)
+    T, rho, Y = (torch.tensor(a, device=dev) for a in (field.T, field.rho, field.Y))
+    Yp, Yp2 = torch.zeros_like(Y), torch.zeros_like(Y)
+    Ef = torch.zeros_like(T)
+    # launch shape: autotuned on a strided sample of the field
+    samp = F.slice_field(field, 131072, stride=32, offset=3)
+    sT, sr, sY = (torch.tensor(a, device=dev) for a in (samp.T, samp.rho, samp.Y))
+    solver.autotune(samp.dt, sT, sr, sY, torch.zeros_like(sY), torch.zeros_like(sY), torch.zeros_like(sT))
+    launch = solver.get_launch()
+    del sT, sr, sY
+    peak_fp64 = fp64_peak_tflops()
+
+    def step():
+        return solver.step_device(field.dt, T, rho, Y, Yp, Yp2, Ef)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    stats = []
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            stats.append(step())
+        e1.record()
+        torch.cuda.synchronize()
+    el_ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([el_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        el_ms = float(t.item())
+        dist.barrier()
+    value = args.steps * n * world / (el_ms * 1e-3)
+
+    # end-to-end: the drop-in host path (Fortran-layout host arrays with a
+    # ghost layer, copies in both directions inside the timed region)
+    e2e = None
+    if not args.no_e2e:
+        nx, ny = field.shape
+        m = DataManager.block(nx, ny)
+        for name in ("temperature", "pressure", "density"):
+            m.create_scalar_field(name)
+        m.create_vector_field("specie_mass_fraction", 9)
+        m.interior(m.fields["temperature"])[...] = field.T.reshape(ny, nx).T[:, :, None]
+        m.interior(m.fields["density"])[...] = field.rho.reshape(ny, nx).T[:, :, None]
+        for k in range(9):
+            m.interior(m.fields["specie_mass_fraction"][k])[...] = field.Y[k].reshape(ny, nx).T[:, :, None]
+        host = ChemicalKineticsSolver(m, *decks, mode=mode)
+        host.set_launch(**{k: v for k, v in launch.items()})
+        host.solve_chemical_kinetics(field.dt)
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            host.solve_chemical_kinetics(field.dt)
+        el2 = time.perf_counter() - t0
+        if world > 1:
+            t = torch.tensor([el2], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            el2 = float(t.item())
+        e2e = {"value": args.steps * n * world / el2, "unit": UNIT,
+               "h2d_bytes_per_step": n * H2D_BYTES_PER_CELL, "d2h_bytes_per_step": n * D2H_BYTES_PER_CELL,
+               "path": "nrg_chem_step (host Fortran-layout arrays, gather/H2D/step/D2H/scatter)"}
+        host.close()
+
+    if rank == 0:
+        st = stats[-1]
+        fm = flop_model(tables, mode)
+        flops = algorithmic_flops(st, fm)
+        kern_ms = float(np.median([s["device_ms"] for s in stats]))
+        achieved = flops / (kern_ms * 1e-3) / 1e12
+        peaks = load_peaks()
+        cpu = cpu_baseline(field, W, decks, args.cpu_seconds)
+        clocks = clk.summary()
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": el_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"flame field {args.n_side}x{args.n_side} ({n:,} cells), dt=1e-6 s, p=1 atm, "
+                                   f"KEROMNES H2/air (9 species, 24 reactions)",
+                       "path": {"fast": "plain FP64 integrator, analytic Jacobian",
+                                "reference": "plain FP64 integrator, reference FD Jacobian",
+                                "mixed": "FP32 LU + FP64 residual/refinement",
+                                "surrogate": "BF16 MLP surrogate + gated FP64 fallback"}[mode],
+                       "launch": launch, "l2": "inputs (370 MB) larger than L2; no flush",
+                       "active_cells": st["cells_active"], "cells_fallback": st["cells_fallback"],
+                       "cells_surrogate": st["cells_surrogate"],
+                       "steps_per_active_cell": st["steps"] / max(1, st["cells_active"])},
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak_fp64, "unit": "TFLOP/s",
+                         "frac": achieved / peak_fp64, "traffic": None,
+                         "kernel": "k_chem_queue (persistent BDF integrator)",
+                         "peak_source": "measured live: dependent-FMA FP64 probe (MEASURED_PEAKS.json has no FP64 figure)",
+                         "flops_per_step": flops, "flop_model": fm},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": args.steps * 1,
+            "clocks": clocks,
+            "peaks_file": {k: peaks.get(k) for k in ("hbm_gbs", "bf16_tflops", "bf16_tflops_sustained")},
+        }
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -121,7 +121,8 @@ NRG_API int nrg_chem_step_device(nrg_chem* h, double time_step, long n, long ld,
 NRG_API int nrg_chem_set_mode(nrg_chem* h, int mode);
 
 /* Launch shape: persistent work-queue kernel or one thread per cell, threads
- * per block, persistent grid (0 = one block per SM), cells per queue fetch. */
+ * per block (64 or 128: each cell keeps ~1.7 KB of state in shared memory),
+ * persistent grid (0 = one block per SM), cells per queue fetch (1..64). */
 NRG_API int nrg_chem_set_launch(nrg_chem* h, int persistent, int block, int grid, int chunk);
 NRG_API int nrg_chem_get_launch(nrg_chem* h, int* persistent, int* block, int* grid, int* chunk);
 

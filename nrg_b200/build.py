@@ -18,7 +18,10 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 # Per-file flags: the integrator keeps the reference's operation order (no
 # FMA contraction); the MLP kernels use the default contraction.
 SOURCES = {
-    "chem_kernels.cu": ["--fmad=false"],
+    "chem_k_ref.cu": ["--fmad=false"],
+    "chem_k_fast.cu": ["--fmad=false"],
+    "chem_k_mixed.cu": ["--fmad=false"],
+    "chem_kernels.cu": [],
     "capi.cu": [],
     "surrogate.cu": [],
     "mechanism.cpp": [],

@@ -363,8 +363,8 @@ extern "C" int nrg_chem_set_mode(nrg_chem* h, int mode) {
 
 extern "C" int nrg_chem_set_launch(nrg_chem* h, int persistent, int block, int grid, int chunk) {
   if (!h) return NRG_ERR_ARG;
-  if (block < 32 || block > 256 || (block % 32) || chunk < 1 || chunk > 64 || grid < 0)
-    return fail(h, NRG_ERR_ARG, "launch shape out of range (block 32..256 step 32, chunk 1..64)");
+  if ((block != 64 && block != 128) || chunk < 1 || chunk > 64 || grid < 0)
+    return fail(h, NRG_ERR_ARG, "launch shape out of range (block 64 or 128, chunk 1..64, grid >= 0)");
   h->cfg.persistent = persistent != 0;
   h->cfg.block = block;
   h->cfg.grid = grid;
@@ -511,10 +511,12 @@ extern "C" int nrg_chem_autotune(nrg_chem* h, double time_step, long n, long ld,
   a.Y_prod = Y_prod; a.Y_prod2 = Y_prod2; a.E_f_prod = E_f_prod; a.T_after = nullptr; a.status = nullptr;
   a.mxstep = 10000;
   std::vector<LaunchCfg> cands;
-  for (int block : {64, 128, 256})
-    for (int per_sm : {1, 2, 3, 4})
+  // one cell holds ~1.7 KB of shared memory, so 128-thread blocks fit once
+  // per SM and 64-thread blocks twice
+  for (int block : {64, 128})
+    for (int per_sm : {1, 2})
       for (int chunk : {1, 2, 4}) {
-        if (block * per_sm > 1024) continue;
+        if (block * per_sm > 128) continue;
         LaunchCfg c;
         c.persistent = true;
         c.block = block;

@@ -24,6 +24,7 @@
 
 #include <cmath>
 #include <cstdint>
+#include <type_traits>
 
 #include "chem_device.cuh"
 #include "chem_kernels.hpp"
@@ -36,18 +37,61 @@ static __constant__ DevMech c_mech;
 
 enum JacMode { kJacFD = 0, kJacAnalytic = 1 };
 
-template <int N, int R, typename LUT>
-struct CellState {
-  double yh[kMaxOrd + 1][N];
-  LUT a[N][N];  // column-major: a[j][i] = A(i+1, j+1)
-  double ywt[N], s1[N], s2[N], fac[N], y[N];
-  double kf[R], kr[R], mc[R];
-  double conc_in[N];
-  int ipvt[N];
+// ------------------------------------------------------------ storage
+// Per-cell arrays live in shared memory in an [element][thread] layout: for
+// element e, the BS threads of a block touch BS consecutive words, so every
+// warp access is bank-conflict free.  Vectors that are only ever indexed by
+// unrolled loops (y, YWT, SAVE1, SAVE2, FAC) stay in registers; the pivot
+// vector is packed into one 64-bit register (4 bits per row).
+template <int N, int R, typename LUT, int BS>
+struct SmemStore {
+  static constexpr int kYH = 0;
+  static constexpr int kKF = (kMaxOrd + 1) * N;
+  static constexpr int kKR = kKF + R;
+  static constexpr int kZ = kKR + R;
+  static constexpr int kZD = kZ + N;
+  static constexpr int kW = kZD + N;
+  static constexpr int kDoubles = kW + N;
+  static constexpr int kBytesPerThread = kDoubles * 8 + N * N * (int)sizeof(LUT);
+  double* d;
+  LUT* f;
+  __device__ __forceinline__ void bind(char* smem, int tid) {
+    d = reinterpret_cast<double*>(smem) + tid;
+    f = reinterpret_cast<LUT*>(smem + (size_t)kDoubles * 8 * BS) + tid;
+  }
+  __device__ __forceinline__ double& yh(int j, int i) { return d[(kYH + j * N + i) * BS]; }
+  __device__ __forceinline__ double& kf(int r) { return d[(kKF + r) * BS]; }
+  __device__ __forceinline__ double& kr(int r) { return d[(kKR + r) * BS]; }
+  __device__ __forceinline__ double& z(int k) { return d[(kZ + k) * BS]; }
+  __device__ __forceinline__ double& zd(int k) { return d[(kZD + k) * BS]; }
+  __device__ __forceinline__ double& w(int k) { return d[(kW + k) * BS]; }
+  __device__ __forceinline__ LUT& a(int j, int i) { return f[(j * N + i) * BS]; }  // A(i+1, j+1)
+};
+
+template <int N, int R, typename LUT, int BS>
+struct CellState : SmemStore<N, R, LUT, BS> {
+  double y[N], ywt[N], s1[N], s2[N], fac[N];
+  unsigned long long piv;  // ipvt, 4 bits per row
   double h, t, tout, rc, rmax, trend, eps;
   int nq, nwait, jtask, nstep, nfe, nje, nsolve, jstepl, nstepl, convrg, ier;
-  int refine;  // iterative-refinement sweeps taken (mixed mode)
+  __device__ __forceinline__ int ipvt(int k) const { return (int)((piv >> (4 * k)) & 15ull); }
 };
+
+// Register-array element with a runtime index (select chain, no local memory).
+template <int N>
+__device__ __forceinline__ double sel(const double (&v)[N], int j) {
+  double r = v[0];
+#pragma unroll
+  for (int i = 1; i < N; ++i)
+    if (i == j) r = v[i];
+  return r;
+}
+template <int N>
+__device__ __forceinline__ void put(double (&v)[N], int j, double x) {
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+    if (i == j) v[i] = x;
+}
 
 #define NRG_FMAX(a, b) ((a) >= (b) ? (a) : (b))
 #define NRG_FMIN(a, b) ((a) <= (b) ? (a) : (b))
@@ -98,56 +142,56 @@ __device__ __forceinline__ double int_pow(double x, double dnu) {
   return pow(x, dnu);
 }
 
-// calculate_rate_constants (chemical_kinetics_solver.f90:360-493)
-template <int N, int R>
-__device__ void rate_constants(double Tin, const double* mc, double* kf, double* kr) {
+// calculate_rate_constants (chemical_kinetics_solver.f90:360-493).  The
+// frozen third-body concentration [M] of reactions written with M is folded
+// into the rate constant here (k_f [M] and k_r [M]), so the right-hand side
+// multiplies concentrations only.  Expects the third-body sums in c.kr(r).
+template <int N, int R, class CS>
+__device__ void rate_constants(CS& c, double Tin) {
   const double RG = 8.31446261815324, PATM = 101325.0;
-  double T = NRG_FMIN(Tin, 10000.0);
-  double tt = NRG_FMIN(T, 6000.0);
-  double logt = log(tt);
-  double s[N], h[N];
+  const double T = NRG_FMIN(Tin, 10000.0);
+  const double logt = log(NRG_FMIN(T, 6000.0));
 #pragma unroll
   for (int k = 0; k < N; ++k) {
-    s[k] = d_entropy(T, k, logt);
-    h[k] = d_enthalpy(T, k);
+    c.z(k) = d_entropy(T, k, logt);
+    c.zd(k) = d_enthalpy(T, k);
   }
-  const double inv_RT = 1.0 / RG / T;  // only used through the reference order below
-  (void)inv_RT;
   const double conc_ref = PATM / RG / T;
+#pragma unroll 1
   for (int r = 0; r < R; ++r) {
+    const double mc = c.kr(r);
     double d_s = 0.0, d_h = 0.0;
+    bool m_left = false, m_right = false;
     for (int i = 0; i < c_mech.nr[r]; ++i) {
       int sp = c_mech.right[r][i];
-      if (sp < 0) continue;
-#pragma unroll
-      for (int k = 0; k < N; ++k)
-        if (k == sp) { d_s = d_s + s[k]; d_h = d_h + h[k]; }
+      if (sp < 0) { m_right = true; continue; }
+      d_s = d_s + c.z(sp);
+      d_h = d_h + c.zd(sp);
     }
     for (int i = 0; i < c_mech.nl[r]; ++i) {
       int sp = c_mech.left[r][i];
-      if (sp < 0) continue;
-#pragma unroll
-      for (int k = 0; k < N; ++k)
-        if (k == sp) { d_s = d_s - s[k]; d_h = d_h - h[k]; }
+      if (sp < 0) { m_left = true; continue; }
+      d_s = d_s - c.z(sp);
+      d_h = d_h - c.zd(sp);
     }
     const int type = c_mech.type[r];
-    double kinf = c_mech.A[r] * pow(T, c_mech.beta[r]) * exp(-(c_mech.E[r] / RG / T));
+    const double kinf = c_mech.A[r] * pow(T, c_mech.beta[r]) * exp(-(c_mech.E[r] / RG / T));
     double k = kinf;
     if (type == 2 || type == 3 || type == 7) {
-      double k0 = c_mech.A_low[r] * pow(T, c_mech.beta_low[r]) * exp(-(c_mech.E_low[r] / RG / T));
-      double rp = k0 * mc[r] / kinf;
+      const double k0 = c_mech.A_low[r] * pow(T, c_mech.beta_low[r]) * exp(-(c_mech.E_low[r] / RG / T));
+      const double rp = k0 * mc / kinf;
       k = kinf * (rp / (1.0 + rp));
       if (type == 3) {
         const double al = c_mech.troe[r][0];
-        double Fc = (1.0 - al) * exp(-(T / c_mech.troe[r][1])) + al * exp(-(T / c_mech.troe[r][2])) +
-                    exp(-(c_mech.troe[r][3] / T));
-        double lf = log10(Fc);
-        double c = -0.4 - 0.67 * lf;
-        double nn = 0.75 - 1.27 * lf;
+        const double Fc = (1.0 - al) * exp(-(T / c_mech.troe[r][1])) + al * exp(-(T / c_mech.troe[r][2])) +
+                          exp(-(c_mech.troe[r][3] / T));
+        const double lf = log10(Fc);
+        const double cc = -0.4 - 0.67 * lf;
+        const double nn = 0.75 - 1.27 * lf;
         double blend;
         if (rp != 0.0) {
-          double lr = log10(rp);
-          double x = (lr + c) / (nn - 0.14 * (lr + c));
+          const double lr = log10(rp);
+          const double x = (lr + cc) / (nn - 0.14 * (lr + cc));
           blend = pow(Fc, 1.0 / (1.0 + x * x));
         } else {
           blend = pow(Fc, -1.0 / 0.14);
@@ -155,226 +199,271 @@ __device__ void rate_constants(double Tin, const double* mc, double* kf, double*
         k = k * blend;
       }
     }
-    kf[r] = k;
-    if (type >= 5) {
-      kr[r] = 0.0;
-    } else {
-      double Kp = exp(d_s / RG - d_h / RG / T);
-      double Kc = Kp * int_pow(conc_ref, c_mech.dnu[r]);
-      kr[r] = k / Kc;
+    double kr = 0.0;
+    if (type < 5) {
+      const double Kp = exp(d_s / RG - d_h / RG / T);
+      kr = k / (Kp * int_pow(conc_ref, c_mech.dnu[r]));
     }
+    c.kf(r) = m_left ? k * mc : k;
+    c.kr(r) = m_right ? kr * mc : kr;
   }
 }
 
-// fun (chemical_kinetics_solver.f90:495-540); zd accumulated in the
-// reference order (reaction-major, then the species-ordered update list).
-template <int N, int R, typename CS>
-__device__ __forceinline__ void rhs(const CS& c, const double* z, double* zd) {
+// fun (chemical_kinetics_solver.f90:495-540): zd = dC/dt at z (both in the
+// cell's shared scratch), accumulated per reaction as the net rate f - b.
+template <int N, int R, class CS>
+__device__ __forceinline__ void rhs(CS& c) {
 #pragma unroll
-  for (int k = 0; k < N; ++k) zd[k] = 0.0;
+  for (int k = 0; k < N; ++k) c.zd(k) = 0.0;
+#pragma unroll 4
   for (int r = 0; r < R; ++r) {
-    double f = c.kf[r];
+    double f = c.kf(r);
     for (int i = 0; i < c_mech.nl[r]; ++i) {
-      int sp = c_mech.left[r][i];
-      f = f * (sp < 0 ? c.mc[r] : z[sp]);
+      const int sp = c_mech.left[r][i];
+      if (sp >= 0) f = f * c.z(sp);
     }
-    double b = c.kr[r];
+    double b = c.kr(r);
     for (int i = 0; i < c_mech.nr[r]; ++i) {
-      int sp = c_mech.right[r][i];
-      b = b * (sp < 0 ? c.mc[r] : z[sp]);
+      const int sp = c_mech.right[r][i];
+      if (sp >= 0) b = b * c.z(sp);
     }
+    const double q = f - b;
     for (int u = 0; u < c_mech.nupd[r]; ++u) {
-      int k = c_mech.upd_k[r][u];
-      if (c_mech.upd_prod[r][u]) zd[k] = zd[k] - b + f;
-      else zd[k] = zd[k] - f + b;
+      const int k = c_mech.upd_k[r][u];
+      if (c_mech.upd_prod[r][u]) c.zd(k) += q;
+      else c.zd(k) -= q;
     }
   }
 }
 
-// dZdot/dZ of the mass-action RHS.  jac is column-major (jac[j][i] =
-// dZdot_i/dZ_j) and is overwritten.
-template <int N, int R, typename CS>
-__device__ void analytic_jacobian(const CS& c, const double* z, double jac[N][N]) {
+// Right-hand side at the register vector v, result into the register vector out.
+template <int N, int R, class CS>
+__device__ __forceinline__ void rhs_at(CS& c, const double (&v)[N], double (&out)[N]) {
+#pragma unroll
+  for (int k = 0; k < N; ++k) c.z(k) = v[k];
+  rhs<N, R>(c);
+#pragma unroll
+  for (int k = 0; k < N; ++k) out[k] = c.zd(k);
+}
+
+// Iteration matrix I + factor * J with J = dZdot/dZ of the mass-action rates
+// at z, written straight into the LU storage.
+template <int N, int R, class CS>
+__device__ void analytic_iteration_matrix(CS& c, double factor) {
 #pragma unroll
   for (int j = 0; j < N; ++j)
 #pragma unroll
-    for (int i = 0; i < N; ++i) jac[j][i] = 0.0;
+    for (int i = 0; i < N; ++i) c.a(j, i) = 0;
+#pragma unroll 1
   for (int r = 0; r < R; ++r) {
-    const int nl = c_mech.nl[r], nr = c_mech.nr[r];
-    double fac_l[3], fac_r[3];
-    for (int i = 0; i < 3; ++i) {
-      int sl = i < nl ? c_mech.left[r][i] : -2;
-      int sr = i < nr ? c_mech.right[r][i] : -2;
-      fac_l[i] = sl == -2 ? 1.0 : (sl < 0 ? c.mc[r] : z[sl]);
-      fac_r[i] = sr == -2 ? 1.0 : (sr < 0 ? c.mc[r] : z[sr]);
-    }
-    const int nu = c_mech.nupd[r];
-    // forward partials
-    for (int p = 0; p < nl; ++p) {
-      int sp = c_mech.left[r][p];
-      if (sp < 0) continue;
-      double d = c.kf[r];
-      for (int q = 0; q < 3; ++q)
-        if (q != p) d = d * fac_l[q];
-      for (int u = 0; u < nu; ++u) {
-        int k = c_mech.upd_k[r][u];
-        if (c_mech.upd_prod[r][u]) jac[sp][k] += d;
-        else jac[sp][k] -= d;
+    const int nl = c_mech.nl[r], nr = c_mech.nr[r], nu = c_mech.nupd[r];
+    for (int side = 0; side < 2; ++side) {
+      const int cnt = side ? nr : nl;
+      const double k = side ? c.kr(r) : c.kf(r);
+      const double sgn = side ? -factor : factor;  // d(f - b)
+      for (int p = 0; p < cnt; ++p) {
+        const int sp = side ? c_mech.right[r][p] : c_mech.left[r][p];
+        if (sp < 0) continue;
+        double d = k;
+        for (int q = 0; q < cnt; ++q) {
+          if (q == p) continue;
+          const int sq = side ? c_mech.right[r][q] : c_mech.left[r][q];
+          if (sq >= 0) d = d * c.z(sq);
+        }
+        d = d * sgn;
+        for (int u = 0; u < nu; ++u) {
+          const int k2 = c_mech.upd_k[r][u];
+          if (c_mech.upd_prod[r][u]) c.a(sp, k2) += d;
+          else c.a(sp, k2) -= d;
+        }
       }
     }
-    // reverse partials
-    for (int p = 0; p < nr; ++p) {
-      int sp = c_mech.right[r][p];
-      if (sp < 0) continue;
-      double d = c.kr[r];
-      for (int q = 0; q < 3; ++q)
-        if (q != p) d = d * fac_r[q];
-      for (int u = 0; u < nu; ++u) {
-        int k = c_mech.upd_k[r][u];
-        if (c_mech.upd_prod[r][u]) jac[sp][k] -= d;
-        else jac[sp][k] += d;
+  }
+#pragma unroll
+  for (int i = 0; i < N; ++i) c.a(i, i) += 1;
+}
+
+// out = J v at z (analytic; used for the FP64 residual of the mixed solve).
+// v is read from c.w, out accumulated into c.zd.
+template <int N, int R, class CS>
+__device__ void jac_vec(CS& c) {
+#pragma unroll
+  for (int k = 0; k < N; ++k) c.zd(k) = 0.0;
+#pragma unroll 1
+  for (int r = 0; r < R; ++r) {
+    const int nl = c_mech.nl[r], nr = c_mech.nr[r], nu = c_mech.nupd[r];
+    double dq = 0.0;
+    for (int side = 0; side < 2; ++side) {
+      const int cnt = side ? nr : nl;
+      const double k = side ? -c.kr(r) : c.kf(r);
+      for (int p = 0; p < cnt; ++p) {
+        const int sp = side ? c_mech.right[r][p] : c_mech.left[r][p];
+        if (sp < 0) continue;
+        double d = k;
+        for (int q = 0; q < cnt; ++q) {
+          if (q == p) continue;
+          const int sq = side ? c_mech.right[r][q] : c_mech.left[r][q];
+          if (sq >= 0) d = d * c.z(sq);
+        }
+        dq = dq + d * c.w(sp);
       }
+    }
+    for (int u = 0; u < nu; ++u) {
+      const int k2 = c_mech.upd_k[r][u];
+      if (c_mech.upd_prod[r][u]) c.zd(k2) += dq;
+      else c.zd(k2) -= dq;
     }
   }
 }
 
-// dnrm2.f90:75-162 -- Lawson-Hanson scaled two-norm (sequential phases)
+// dnrm2.f90:75-162, Lawson-Hanson scaled two-norm, restated as a per-element
+// state machine over an unrolled loop (phases 1-4 of the reference's
+// ASSIGN/GO TO form: zero, small-scaled, mid-range, large-scaled).
 template <int N>
-__device__ double dnrm2(const double* dx) {
+__device__ __forceinline__ double dnrm2(const double (&dx)[N]) {
   const double cutlo = 8.232e-11, cuthi = 1.304e19;
-  double sum = 0.0, xmax = 0.0;
-  int next = 30, i = 0, j = 0;
-L20:
-  if (next == 30) goto L30;
-  if (next == 50) goto L50;
-  if (next == 70) goto L70;
-  goto L110;
-L30:
-  if (fabs(dx[i]) > cutlo) goto L85;
-  next = 50;
-  xmax = 0.0;
-L50:
-  if (dx[i] == 0.0) goto L200;
-  if (fabs(dx[i]) > cutlo) goto L85;
-  next = 70;
-  goto L105;
-L100:
-  i = j;
-  next = 110;
-  sum = (sum / dx[i]) / dx[i];
-L105:
-  xmax = fabs(dx[i]);
-  goto L115;
-L70:
-  if (fabs(dx[i]) > cutlo) goto L75;
-L110:
-  if (fabs(dx[i]) <= xmax) goto L115;
-  {
-    double q = xmax / dx[i];
-    sum = 1.0 + sum * (q * q);
-  }
-  xmax = fabs(dx[i]);
-  goto L200;
-L115: {
-  double q = dx[i] / xmax;
-  sum = sum + q * q;
-}
-  goto L200;
-L75:
-  sum = (sum * xmax) * xmax;
-L85: {
   const double hitest = cuthi / (double)N;
-  for (j = i; j < N; ++j) {
-    if (fabs(dx[j]) >= hitest) goto L100;
-    sum = sum + dx[j] * dx[j];
+  enum { S30, S50, S70, S85, S110 };
+  int st = S30;
+  double sum = 0.0, xmax = 0.0;
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    const double x = dx[i], ax = fabs(x);
+    if (st == S30) {
+      if (ax > cutlo) st = S85;
+      else { st = S50; xmax = 0.0; }
+    }
+    if (st == S50) {
+      if (x == 0.0) continue;
+      if (ax > cutlo) {
+        st = S85;
+      } else {
+        st = S70;
+        xmax = ax;
+        const double q = x / xmax;
+        sum = sum + q * q;
+        continue;
+      }
+    }
+    if (st == S70) {
+      if (ax > cutlo) {
+        sum = (sum * xmax) * xmax;
+        st = S85;
+      }
+    }
+    if (st == S70 || st == S110) {
+      if (ax <= xmax) {
+        const double q = x / xmax;
+        sum = sum + q * q;
+      } else {
+        const double q = xmax / x;
+        sum = 1.0 + sum * (q * q);
+        xmax = ax;
+      }
+      continue;
+    }
+    // S85: mid-range, unscaled
+    if (ax >= hitest) {
+      sum = (sum / x) / x;
+      xmax = ax;
+      const double q = x / xmax;
+      sum = sum + q * q;
+      st = S110;
+    } else {
+      sum = sum + x * x;
+    }
   }
-}
-  return sqrt(sum);
-L200:
-  i = i + 1;
-  if (i < N) goto L20;
-  return xmax * sqrt(sum);
+  return st == S85 ? sqrt(sum) : xmax * sqrt(sum);
 }
 
-// dgefa.f90:60-117 on the column-major matrix a (element type LUT)
-template <int N, typename LUT>
-__device__ int dgefa(LUT a[N][N], int* ipvt) {
+// dgefa.f90:60-117 on the shared-memory matrix (column-major a(j, i) = A(i, j))
+template <int N, class CS>
+__device__ int dgefa(CS& c) {
+  using LUT = typename std::remove_reference<decltype(c.a(0, 0))>::type;
   int info = 0;
+  unsigned long long piv = 0;
+#pragma unroll 1
   for (int k = 0; k < N - 1; ++k) {
-    // idamax over a[k][k..N-1]
     int l = k;
-    LUT dmax = fabs(a[k][k]);
+    LUT dmax = fabs(c.a(k, k));
     for (int i = k + 1; i < N; ++i) {
-      LUT xm = fabs(a[k][i]);
+      const LUT xm = fabs(c.a(k, i));
       if (xm > dmax) { l = i; dmax = xm; }
     }
-    ipvt[k] = l;
-    if (a[k][l] == (LUT)0) { info = k + 1; continue; }
+    piv |= (unsigned long long)l << (4 * k);
+    if (c.a(k, l) == (LUT)0) { info = k + 1; continue; }
     if (l != k) {
-      LUT t = a[k][l];
-      a[k][l] = a[k][k];
-      a[k][k] = t;
+      const LUT t = c.a(k, l);
+      c.a(k, l) = c.a(k, k);
+      c.a(k, k) = t;
     }
-    LUT t = (LUT)-1 / a[k][k];
-    for (int i = k + 1; i < N; ++i) a[k][i] = t * a[k][i];
+    const LUT t = (LUT)-1 / c.a(k, k);
+    for (int i = k + 1; i < N; ++i) c.a(k, i) = t * c.a(k, i);
     for (int j = k + 1; j < N; ++j) {
-      LUT tj = a[j][l];
+      const LUT tj = c.a(j, l);
       if (l != k) {
-        a[j][l] = a[j][k];
-        a[j][k] = tj;
+        c.a(j, l) = c.a(j, k);
+        c.a(j, k) = tj;
       }
       if (tj != (LUT)0)
-        for (int i = k + 1; i < N; ++i) a[j][i] = a[j][i] + tj * a[k][i];
+        for (int i = k + 1; i < N; ++i) c.a(j, i) = c.a(j, i) + tj * c.a(k, i);
     }
   }
-  ipvt[N - 1] = N - 1;
-  if (a[N - 1][N - 1] == (LUT)0) info = N;
+  piv |= (unsigned long long)(N - 1) << (4 * (N - 1));
+  c.piv = piv;
+  if (c.a(N - 1, N - 1) == (LUT)0) info = N;
   return info;
 }
 
-// dgesl.f90:71-131, JOB = 0 (b overwritten with the solution)
-template <int N, typename LUT, typename VT>
-__device__ void dgesl(const LUT a[N][N], const int* ipvt, VT* b) {
+// dgesl.f90:71-131, JOB = 0, on the register vector b
+template <int N, class CS>
+__device__ __forceinline__ void dgesl(CS& c, double (&b)[N]) {
+#pragma unroll
   for (int k = 0; k < N - 1; ++k) {
-    int l = ipvt[k];
-    VT t = b[l];
+    const int l = c.ipvt(k);
+    const double t = sel(b, l);
     if (l != k) {
-      b[l] = b[k];
+      put(b, l, b[k]);
       b[k] = t;
     }
-    if (t != (VT)0)
-      for (int i = k + 1; i < N; ++i) b[i] = b[i] + t * (VT)a[k][i];
+    if (t != 0.0) {
+#pragma unroll
+      for (int i = k + 1; i < N; ++i) b[i] = b[i] + t * (double)c.a(k, i);
+    }
   }
+#pragma unroll
   for (int k = N - 1; k >= 0; --k) {
-    b[k] = b[k] / (VT)a[k][k];
-    VT t = -b[k];
-    if (t != (VT)0)
-      for (int i = 0; i < k; ++i) b[i] = b[i] + t * (VT)a[k][i];
+    b[k] = b[k] / (double)c.a(k, k);
+    const double t = -b[k];
+    if (t != 0.0) {
+#pragma unroll
+      for (int i = 0; i < k; ++i) b[i] = b[i] + t * (double)c.a(k, i);
+    }
   }
 }
 
 // --------------------------------------------------------- SLATEC pieces
-template <int N, typename CS>
+template <int N, class CS>
 __device__ __forceinline__ void ddpsc(int ksgn, CS& c) {
   const int nq = c.nq;
   for (int j1 = 1; j1 <= nq; ++j1)
     for (int j2 = j1; j2 <= nq; ++j2) {
-      int j = nq - j2 + j1;  // 1-based column
+      const int j = nq - j2 + j1;  // 1-based column
       if (ksgn > 0) {
 #pragma unroll
-        for (int i = 0; i < N; ++i) c.yh[j - 1][i] = c.yh[j - 1][i] + c.yh[j][i];
+        for (int i = 0; i < N; ++i) c.yh(j - 1, i) = c.yh(j - 1, i) + c.yh(j, i);
       } else {
 #pragma unroll
-        for (int i = 0; i < N; ++i) c.yh[j - 1][i] = c.yh[j - 1][i] - c.yh[j][i];
+        for (int i = 0; i < N; ++i) c.yh(j - 1, i) = c.yh(j - 1, i) - c.yh(j, i);
       }
     }
 }
 
-template <int N, typename CS>
+template <int N, class CS>
 __device__ __forceinline__ void ddscl(CS& c, double rh) {
   const double hmax = c_mech.hmax;
   if (c.h < 1.0) {
-    double ah = fabs(c.h);
+    const double ah = fabs(c.h);
     rh = NRG_FMIN(NRG_FMIN(ah * rh, ah * c.rmax), hmax) / ah;
   } else {
     rh = NRG_FMIN(NRG_FMIN(rh, c.rmax), hmax / fabs(c.h));
@@ -383,7 +472,7 @@ __device__ __forceinline__ void ddscl(CS& c, double rh) {
   for (int j = 1; j <= c.nq; ++j) {
     r1 = r1 * rh;
 #pragma unroll
-    for (int i = 0; i < N; ++i) c.yh[j][i] = c.yh[j][i] * r1;
+    for (int i = 0; i < N; ++i) c.yh(j, i) = c.yh(j, i) * r1;
   }
   c.h = c.h * rh;
   c.rc = c.rc * rh;
@@ -392,7 +481,7 @@ __device__ __forceinline__ void ddscl(CS& c, double rh) {
 #define EL(i, j) c_mech.el[((j)-1) * 13 + ((i)-1)]
 #define TQ(i, j) c_mech.tq[((j)-1) * 3 + ((i)-1)]
 
-template <int N, int R, typename CS>
+template <int N, int R, class CS>
 __device__ void ddntl(CS& c) {
   c.ier = 0;
   if (c.jtask == 0) c.rmax = 10000.0;
@@ -401,20 +490,20 @@ __device__ void ddntl(CS& c) {
   c.trend = 1.0;
   c.nq = 1;
   c.nwait = 3;
-  rhs<N, R>(c, c.y, c.s2);
+  rhs_at<N, R>(c, c.y, c.s2);
   c.nfe += 1;
 #pragma unroll
   for (int i = 0; i < N; ++i) c.s1[i] = c.s2[i] / NRG_FMAX(1.0, c.ywt[i]);
-  double sum = dnrm2<N>(c.s1) / sqrt((double)N);
+  const double sum = dnrm2<N>(c.s1) / sqrt((double)N);
   if (sum > c.eps / fabs(c.h)) c.h = copysign(c.eps / sum, c.h);
 #pragma unroll
-  for (int i = 0; i < N; ++i) c.yh[1][i] = c.h * c.s2[i];
+  for (int i = 0; i < N; ++i) c.yh(1, i) = c.h * c.s2[i];
 #pragma unroll
   for (int i = 0; i < N; ++i) c.fac[i] = c_mech.sqrt_uround;
 }
 
-// Iteration matrix I - h*l0*J and its LU (DDPST MITER=2 or analytic J).
-template <int N, int R, int JAC, typename CS>
+// Iteration matrix I - h*l0*J and its LU (DDPST, ddpst.f90:52-142).
+template <int N, int R, int JAC, class CS>
 __device__ void ddpst(CS& c) {
   c.nje += 1;
   c.ier = 0;
@@ -422,84 +511,99 @@ __device__ void ddpst(CS& c) {
   if (JAC == kJacFD) {
     const double FACMAX = 0.5, BU = 0.5;
     const double br = c_mech.br, bl = c_mech.bl, bp = c_mech.bp, facmin = c_mech.facmin;
+#pragma unroll
+    for (int k = 0; k < N; ++k) c.z(k) = c.y[k];
+#pragma unroll 1
     for (int j = 0; j < N; ++j) {
-      double ys = NRG_FMAX(fabs(c.ywt[j]), fabs(c.y[j]));
+      const double yj = sel(c.y, j);
+      const double ys = NRG_FMAX(fabs(sel(c.ywt, j)), fabs(yj));
+      double fj = sel(c.fac, j);
       double dy;
       for (;;) {
-        dy = c.fac[j] * ys;
+        dy = fj * ys;
         if (dy == 0.0) {
-          if (c.fac[j] < FACMAX) {
-            c.fac[j] = NRG_FMIN(100.0 * c.fac[j], FACMAX);
+          if (fj < FACMAX) {
+            fj = NRG_FMIN(100.0 * fj, FACMAX);
             continue;
           }
           dy = ys;
         }
         break;
       }
-      dy = (c.nq == 1) ? copysign(dy, c.s2[j]) : copysign(dy, c.yh[2][j]);
-      dy = (c.y[j] + dy) - c.y[j];
-      double yj = c.y[j];
-      c.y[j] = c.y[j] + dy;
-      rhs<N, R>(c, c.y, c.s1);
-      c.y[j] = yj;
-      double factor = -(el1h / dy);
+      dy = (c.nq == 1) ? copysign(dy, sel(c.s2, j)) : copysign(dy, c.yh(2, j));
+      dy = (yj + dy) - yj;
+      c.z(j) = yj + dy;
+      rhs<N, R>(c);
+      c.z(j) = yj;
+      const double factor = -(el1h / dy);
+      double diff = -1.0, s2m = 0.0, s1m = 0.0;
 #pragma unroll
-      for (int i = 0; i < N; ++i) c.a[j][i] = (c.s1[i] - c.s2[i]) * factor;
-      double diff = fabs(c.s2[0] - c.s1[0]);
-      int imax = 0;
-#pragma unroll
-      for (int i = 1; i < N; ++i) {
-        double di = fabs(c.s2[i] - c.s1[i]);
-        if (di > diff) { imax = i; diff = di; }
+      for (int i = 0; i < N; ++i) {
+        const double f1 = c.zd(i);
+        c.a(j, i) = (f1 - c.s2[i]) * factor;
+        const double di = fabs(c.s2[i] - f1);
+        if (di > diff) { diff = di; s2m = fabs(c.s2[i]); s1m = fabs(f1); }
       }
-      double s2m = 0.0, s1m = 0.0;
-#pragma unroll
-      for (int i = 0; i < N; ++i)
-        if (i == imax) { s2m = fabs(c.s2[i]); s1m = fabs(c.s1[i]); }
       if (NRG_FMIN(s2m, s1m) > 0.0) {
-        double scale = NRG_FMAX(s2m, s1m);
-        if (diff > BU * scale) c.fac[j] = NRG_FMAX(facmin, c.fac[j] * 0.5);
-        else if (br * scale <= diff && diff <= bl * scale) c.fac[j] = NRG_FMIN(c.fac[j] * 2.0, FACMAX);
-        else if (diff < br * scale) c.fac[j] = NRG_FMIN(bp * c.fac[j], FACMAX);
+        const double scale = NRG_FMAX(s2m, s1m);
+        if (diff > BU * scale) fj = NRG_FMAX(facmin, fj * 0.5);
+        else if (br * scale <= diff && diff <= bl * scale) fj = NRG_FMIN(fj * 2.0, FACMAX);
+        else if (diff < br * scale) fj = NRG_FMIN(bp * fj, FACMAX);
       }
+      put(c.fac, j, fj);
     }
     c.nfe += N;
+#pragma unroll
+    for (int i = 0; i < N; ++i) c.a(i, i) += 1;
   } else {
-    double jac[N][N];
-    analytic_jacobian<N, R>(c, c.y, jac);
-    const double factor = -el1h;
 #pragma unroll
-    for (int j = 0; j < N; ++j)
-#pragma unroll
-      for (int i = 0; i < N; ++i) c.a[j][i] = factor * jac[j][i];
+    for (int k = 0; k < N; ++k) c.z(k) = c.y[k];
+    analytic_iteration_matrix<N, R>(c, -el1h);
   }
-#pragma unroll
-  for (int i = 0; i < N; ++i) c.a[i][i] = c.a[i][i] + 1.0;
-  int info = dgefa<N>(c.a, c.ipvt);
+  const int info = dgefa<N>(c);
   if (info != 0) c.ier = 1;
 }
 
-// Corrector solve (DDCOR MITER=2, IMPL=0).  With float LU factors the
-// correction is refined: r = rhs - M x is formed in double with M rebuilt
-// from its definition (I - h l0 J applied through a Jacobian-vector product
-// would need J; instead the refinement uses the stored double residual of the
-// Newton system, see mixed_solve).
-template <int N, typename CS>
+// Corrector solve (DDCOR MITER=2, IMPL=0, ddcor.f90:61-107).  With float LU
+// factors the solve is followed by one step of iterative refinement whose
+// residual b - (I - h l0 J) x is formed in FP64 with an analytic J v.
+template <int N, int R, typename LUT, class CS>
 __device__ double ddcor(CS& c) {
+  double b[N];
 #pragma unroll
-  for (int i = 0; i < N; ++i) c.s2[i] = c.h * c.s2[i] - c.yh[1][i] - c.s1[i];
-  dgesl<N>(c.a, c.ipvt, c.s2);
+  for (int i = 0; i < N; ++i) b[i] = c.h * c.s2[i] - c.yh(1, i) - c.s1[i];
+  double x[N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) x[i] = b[i];
+  dgesl<N>(c, x);
+  if (sizeof(LUT) == 4) {
+    const double el1h = EL(1, c.nq) * c.h;
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      c.z(k) = c.y[k];
+      c.w(k) = x[k];
+    }
+    jac_vec<N, R>(c);
+    double r[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) r[i] = b[i] - (x[i] - el1h * c.zd(i));
+    dgesl<N>(c, r);
+#pragma unroll
+    for (int i = 0; i < N; ++i) x[i] = x[i] + r[i];
+    c.nsolve += 1;
+  }
   c.nsolve += 1;
 #pragma unroll
   for (int i = 0; i < N; ++i) {
-    c.s1[i] = c.s1[i] + c.s2[i];
-    c.s2[i] = c.s2[i] / NRG_FMAX(fabs(c.y[i]), c.ywt[i]);
+    c.s1[i] = c.s1[i] + x[i];
+    c.s2[i] = x[i] / NRG_FMAX(fabs(c.y[i]), c.ywt[i]);
   }
   return dnrm2<N>(c.s2) / sqrt((double)N);
 }
 
-// One DDSTP call; returns JSTATE (1 ok, 2 h vanished, 3 MXTRY, 4 singular).
-template <int N, int R, int JAC, typename CS>
+// One DDSTP call (ddstp.f90:72-459); returns JSTATE (1 ok, 2 h vanished,
+// 3 MXTRY retries, 4 singular).
+template <int N, int R, int JAC, typename LUT, class CS>
 __device__ int ddstp(CS& c) {
   const double BIAS1 = 1.3, BIAS2 = 1.2, BIAS3 = 1.4, RCTEST = 0.3, RMFAIL = 2.0, RMNORM = 10.0,
                TRSHLD = 1.0;
@@ -524,8 +628,8 @@ L100:
 L110:
   iter = 0;
 #pragma unroll
-  for (int i = 0; i < N; ++i) c.y[i] = c.yh[0][i];
-  rhs<N, R>(c, c.y, c.s2);
+  for (int i = 0; i < N; ++i) c.y[i] = c.yh(0, i);
+  rhs_at<N, R>(c, c.y, c.s2);
   c.nfe += 1;
   if (evaljc || c.ier) {
     ddpst<N, R, JAC>(c);
@@ -537,7 +641,7 @@ L110:
 #pragma unroll
   for (int i = 0; i < N; ++i) c.s1[i] = 0.0;
 L130:
-  d = ddcor<N>(c);
+  d = ddcor<N, R, LUT>(c);
   if (iter > 0) c.trend = NRG_FMAX(0.9 * c.trend, d / d1);
   d1 = d;
   ctest = NRG_FMIN(2.0 * c.trend, 1.0) * d;
@@ -546,8 +650,8 @@ L130:
   if (iter < MXITER) {
     const double el1 = EL(1, c.nq);
 #pragma unroll
-    for (int i = 0; i < N; ++i) c.y[i] = c.yh[0][i] + el1 * c.s1[i];
-    rhs<N, R>(c, c.y, c.s2);
+    for (int i = 0; i < N; ++i) c.y[i] = c.yh(0, i) + el1 * c.s1[i];
+    rhs_at<N, R>(c, c.y, c.s2);
     c.nfe += 1;
     goto L130;
   }
@@ -575,12 +679,12 @@ L170:
     nfail = nfail + 1;
     if (nfail < MXFAIL || c.nq == 1) {
       if (c.jtask != 0 && c.jtask != 2) c.rmax = RMFAIL;
-      double rh2 = 1.0 / (BIAS2 * pow(etest / eps, 1.0 / (double)(c.nq + 1)));
+      const double rh2 = 1.0 / (BIAS2 * pow(etest / eps, 1.0 / (double)(c.nq + 1)));
       if (c.nq > 1) {
 #pragma unroll
-        for (int i = 0; i < N; ++i) c.s2[i] = c.yh[c.nq][i] / NRG_FMAX(fabs(c.y[i]), c.ywt[i]);
-        double erdn = dnrm2<N>(c.s2) / (TQ(1, c.nq) * sqn);
-        double rh1 = 1.0 / NRG_FMAX(1.0, BIAS1 * pow(erdn / eps, 1.0 / (double)c.nq));
+        for (int i = 0; i < N; ++i) c.s2[i] = c.yh(c.nq, i) / NRG_FMAX(fabs(c.y[i]), c.ywt[i]);
+        const double erdn = dnrm2<N>(c.s2) / (TQ(1, c.nq) * sqn);
+        const double rh1 = 1.0 / NRG_FMAX(1.0, BIAS1 * pow(erdn / eps, 1.0 / (double)c.nq));
         if (rh2 < rh1) {
           c.nq = c.nq - 1;
           c.rc = c.rc * EL(1, c.nq) / EL(1, c.nq + 1);
@@ -599,7 +703,7 @@ L170:
     nfail = 0;
     c.jtask = 2;
 #pragma unroll
-    for (int i = 0; i < N; ++i) c.y[i] = c.yh[0][i];
+    for (int i = 0; i < N; ++i) c.y[i] = c.yh(0, i);
     ddntl<N, R>(c);
     c.rmax = RMNORM;
     if (c.h == 0.0) goto L400;
@@ -610,10 +714,10 @@ L170:
   for (int j = 0; j <= c.nq; ++j) {
     const double e = EL(j + 1, c.nq);
 #pragma unroll
-    for (int i = 0; i < N; ++i) c.yh[j][i] = c.yh[j][i] + e * c.s1[i];
+    for (int i = 0; i < N; ++i) c.yh(j, i) = c.yh(j, i) + e * c.s1[i];
   }
 #pragma unroll
-  for (int i = 0; i < N; ++i) c.y[i] = c.yh[0][i];
+  for (int i = 0; i < N; ++i) c.y[i] = c.yh(0, i);
   if (c.jtask == 0 || c.jtask == 2) {
     rh = 1.0 / NRG_FMAX(uround, BIAS2 * pow(etest / eps, 1.0 / (double)(c.nq + 1)));
     if (rh > TRSHLD) ddscl<N>(c, rh);
@@ -621,7 +725,7 @@ L170:
     c.nwait = c.nwait - 1;
     if (c.nwait == 1 && c.nq < kMaxOrd) {
 #pragma unroll
-      for (int i = 0; i < N; ++i) c.yh[kMaxOrd][i] = c.s1[i];
+      for (int i = 0; i < N; ++i) c.yh(kMaxOrd, i) = c.s1[i];
     }
   } else {
     double rh1, rh2, rh3;
@@ -629,8 +733,8 @@ L170:
       rh1 = 0.0;
     } else {
 #pragma unroll
-      for (int i = 0; i < N; ++i) c.s2[i] = c.yh[c.nq][i] / NRG_FMAX(fabs(c.y[i]), c.ywt[i]);
-      double erdn = dnrm2<N>(c.s2) / (TQ(1, c.nq) * sqn);
+      for (int i = 0; i < N; ++i) c.s2[i] = c.yh(c.nq, i) / NRG_FMAX(fabs(c.y[i]), c.ywt[i]);
+      const double erdn = dnrm2<N>(c.s2) / (TQ(1, c.nq) * sqn);
       rh1 = 1.0 / NRG_FMAX(uround, BIAS1 * pow(erdn / eps, 1.0 / (double)c.nq));
     }
     rh2 = 1.0 / NRG_FMAX(uround, BIAS2 * pow(etest / eps, 1.0 / (double)(c.nq + 1)));
@@ -639,8 +743,8 @@ L170:
     } else {
 #pragma unroll
       for (int i = 0; i < N; ++i)
-        c.s2[i] = (c.s1[i] - c.yh[kMaxOrd][i]) / NRG_FMAX(fabs(c.y[i]), c.ywt[i]);
-      double erup = dnrm2<N>(c.s2) / (TQ(3, c.nq) * sqn);
+        c.s2[i] = (c.s1[i] - c.yh(kMaxOrd, i)) / NRG_FMAX(fabs(c.y[i]), c.ywt[i]);
+      const double erup = dnrm2<N>(c.s2) / (TQ(3, c.nq) * sqn);
       rh3 = 1.0 / NRG_FMAX(uround, BIAS3 * pow(erup / eps, 1.0 / (double)(c.nq + 2)));
     }
     if (rh1 > rh2 && rh1 >= rh3) {
@@ -656,7 +760,7 @@ L170:
       if (rh <= TRSHLD) goto L380;
       const double e = EL(c.nq + 1, c.nq);
 #pragma unroll
-      for (int i = 0; i < N; ++i) c.yh[c.nq + 1][i] = c.s1[i] * e / (double)(c.nq + 1);
+      for (int i = 0; i < N; ++i) c.yh(c.nq + 1, i) = c.s1[i] * e / (double)(c.nq + 1);
       c.nq = c.nq + 1;
       c.rc = c.rc * EL(1, c.nq) / EL(1, c.nq - 1);
     }
@@ -668,7 +772,7 @@ L170:
   return 1;
 L400:
 #pragma unroll
-  for (int i = 0; i < N; ++i) c.y[i] = c.yh[0][i];
+  for (int i = 0; i < N; ++i) c.y[i] = c.yh(0, i);
   return 2;
 L410:
   return 3;
@@ -677,11 +781,10 @@ L420:
 }
 
 // ----------------------------------------------------------- cell driver
-enum CellPhase { kPhaseRunning = 0, kPhaseDone = 1 };
-
-// Cell set-up: skip rule, third-body sums, rate constants, DDRIV3 init.
+// Cell set-up: skip rule (chemical_kinetics_solver.f90:228-231), third-body
+// sums (:238-248), rate constants (:251), DDRIV3 init (ddriv3.f90:930-978).
 // Returns false when the cell is passed through (outputs already written).
-template <int N, int R, typename CS>
+template <int N, int R, class CS>
 __device__ bool cell_begin(CS& c, const StepArgs& a, long cid) {
   const double Tc = a.T[cid];
   const bool active = (Tc >= 305.0) && (a.bc == nullptr || a.bc[cid] == 0);
@@ -696,23 +799,23 @@ __device__ bool cell_begin(CS& c, const StepArgs& a, long cid) {
   double yk[N];
 #pragma unroll
   for (int k = 0; k < N; ++k) yk[k] = a.Y[k * a.ld + cid];
+#pragma unroll 1
   for (int r = 0; r < R; ++r) {
     double s = 0.0;
 #pragma unroll
     for (int k = 0; k < N; ++k) s = s + yk[k] * rho / c_mech.W[k] * c_mech.eff[r][k];
-    c.mc[r] = s;
+    c.kr(r) = s;  // third-body sum, consumed by rate_constants
   }
-  rate_constants<N, R>(Tc, c.mc, c.kf, c.kr);
+  rate_constants<N, R>(c, Tc);
 #pragma unroll
   for (int k = 0; k < N; ++k) {
-    c.conc_in[k] = yk[k] * rho / c_mech.W[k];
-    c.yh[0][k] = c.conc_in[k];
-    c.y[k] = c.conc_in[k];
+    const double ci = yk[k] * rho / c_mech.W[k];
+    c.yh(0, k) = ci;
+    c.y[k] = ci;
   }
-  // ddriv3.f90:930-978 (NSTATE = 1)
   c.tout = a.dt;
   c.t = 0.0;
-  double h = (c.tout - c.t) * (1.0 - 4.0 * c_mech.uround);
+  const double h = (c.tout - c.t) * (1.0 - 4.0 * c_mech.uround);
   c.h = copysign(NRG_FMIN(fabs(h), c_mech.hmax), h);
   c.eps = c_mech.eps;
   c.jtask = 0;
@@ -724,64 +827,67 @@ __device__ bool cell_begin(CS& c, const StepArgs& a, long cid) {
   c.nsolve = 0;
   c.convrg = 0;
   c.ier = 0;
-  c.refine = 0;
   c.nq = 1;
+  c.rc = 0.0;
+  c.rmax = 10000.0;
+  c.trend = 1.0;
+  c.nwait = 3;
+  c.piv = 0;
   return true;
 }
 
-// One pass of the DDRIV3 loop (label 260): error weights, accuracy and
-// MXSTEP checks, one DDSTP step, and on reaching TOUT the interpolation.
-// Returns 0 while running, else a CellStatus.
-template <int N, int R, int JAC, typename CS>
+// One pass of the DDRIV3 loop (label 260, ddriv3.f90:1292-1448): error
+// weights, accuracy and MXSTEP checks, one DDSTP step and, on reaching TOUT,
+// the Nordsieck interpolation (DDNTP).  Returns 0 while running, else a
+// CellStatus.
+template <int N, int R, int JAC, typename LUT, class CS>
 __device__ int cell_advance(CS& c, int mxstep) {
 #pragma unroll
   for (int i = 0; i < N; ++i) c.ywt[i] = NRG_FMAX(c_mech.ewt, fabs(c.y[i]));
 #pragma unroll
   for (int i = 0; i < N; ++i) c.s2[i] = c.y[i] / c.ywt[i];
-  double sum = NRG_FMAX(1.0, dnrm2<N>(c.s2) / sqrt((double)N));
+  const double sum = NRG_FMAX(1.0, dnrm2<N>(c.s2) / sqrt((double)N));
   if (c.eps < sum * c_mech.uround) {
     c.eps = sum * c_mech.uround * (1.0 + 10.0 * c_mech.uround);
 #pragma unroll
-    for (int i = 0; i < N; ++i) c.y[i] = c.yh[0][i];
-    return kCellOk;  // NSTATE = 4: state at current T returned
+    for (int i = 0; i < N; ++i) c.y[i] = c.yh(0, i);
+    return kCellOk;  // NSTATE = 4: the state at the current T is returned
   }
   if (c.nstep - c.nstepl == mxstep) {
 #pragma unroll
-    for (int i = 0; i < N; ++i) c.y[i] = c.yh[0][i];
+    for (int i = 0; i < N; ++i) c.y[i] = c.yh(0, i);
     return kCellMxstep;
   }
-  int js = ddstp<N, R, JAC>(c);
+  const int js = ddstp<N, R, JAC, LUT>(c);
   if (js != 1) {
 #pragma unroll
-    for (int i = 0; i < N; ++i) c.y[i] = c.yh[0][i];
+    for (int i = 0; i < N; ++i) c.y[i] = c.yh(0, i);
     return kCellFatal;
   }
   c.jtask = 1;
   if (c.t < c.tout) return 0;
-  // ddntp.f90 K = 0
 #pragma unroll
-  for (int i = 0; i < N; ++i) c.y[i] = c.yh[c.nq][i];
+  for (int i = 0; i < N; ++i) c.y[i] = c.yh(c.nq, i);
   const double r = (c.tout - c.t) / c.h;
   for (int jj = 1; jj <= c.nq; ++jj) {
-    int j = c.nq - jj;  // 0-based column nq-jj
+    const int j = c.nq - jj;
 #pragma unroll
-    for (int i = 0; i < N; ++i) c.y[i] = c.yh[j][i] + r * c.y[i];
+    for (int i = 0; i < N; ++i) c.y[i] = c.yh(j, i) + r * c.y[i];
   }
   return kCellOk;
 }
 
-// Energy closure at constant density (the temperature the reference EOS
-// would compute after adding the sources: cpm_solver.f90:517,549 ->
-// table_approximated_real_gas.f90:404-440 -> calculate_temperature
+// Energy closure at constant density: the temperature the reference EOS
+// computes after the sources are added (cpm_solver.f90:517,549 ->
+// table_approximated_real_gas.f90:404-440 -> calculate_temperature,
 // thermophysical_properties_class.f90:409-452).
 template <int N>
-__device__ double temperature_after(double T0, double rho, const double* Y0, const double* dY,
-                                    double dE /* E_f_prod*dt/rho */) {
+__device__ double temperature_after(double T0, const double (&Y0)[N], const double (&dY)[N], double dE) {
   const double RG = 8.31446261815324;
   double X[N], avg = 0.0;
 #pragma unroll
   for (int k = 0; k < N; ++k) avg = avg + Y0[k] / c_mech.W[k];
-  double W0 = 1.0 / avg;
+  const double W0 = 1.0 / avg;
   double e0 = 0.0, h0 = 0.0;
 #pragma unroll
   for (int k = 0; k < N; ++k) {
@@ -790,7 +896,7 @@ __device__ double temperature_after(double T0, double rho, const double* Y0, con
   }
 #pragma unroll
   for (int k = 0; k < N; ++k) h0 = h0 + c_mech.h_ref[k] * X[k];
-  double e1 = (e0 - h0) / W0 + dE;
+  const double e1 = (e0 - h0) / W0 + dE;
   avg = 0.0;
   double Y1[N];
 #pragma unroll
@@ -798,7 +904,7 @@ __device__ double temperature_after(double T0, double rho, const double* Y0, con
     Y1[k] = Y0[k] + dY[k];
     avg = avg + Y1[k] / c_mech.W[k];
   }
-  double W1 = 1.0 / avg;
+  const double W1 = 1.0 / avg;
   double hc = 0.0, cp = 0.0;
   double temp = NRG_FMIN(T0, 6000.0);
 #pragma unroll
@@ -808,40 +914,40 @@ __device__ double temperature_after(double T0, double rho, const double* Y0, con
     cp = cp + d_cp(temp, k) * X[k];
   }
   const double ei = e1 * W1;
-  const double tol = (double)1e-08f;
+  const double tol = (double)1e-08f;  // single-precision literal in the reference
   for (int it = 0; it < 1000; ++it) {
     double e = 0.0;
 #pragma unroll
     for (int k = 0; k < N; ++k) e = e + (d_enthalpy(temp, k) - RG * temp) * X[k];
-    double res = (ei - (e - hc)) / cp;
+    const double res = (ei - (e - hc)) / cp;
     temp = temp + res;
     if (fabs(res) < tol) break;
   }
   return temp;
 }
 
-// Outputs for a finished cell (chemical_kinetics_solver.f90:318-340).
-template <int N, typename CS>
+// Outputs of a finished cell (chemical_kinetics_solver.f90:318-340).
+template <int N, class CS>
 __device__ void cell_finish(const CS& c, const StepArgs& a, long cid, int st) {
   const double dt = a.dt;
+  const double rho = a.rho[cid];
   double E = 0.0;
   bool finite = true;
-  double dYm[N], Y0[N];
-  const double rho = a.rho[cid];
+  double Y0[N], dYm[N];
 #pragma unroll
   for (int k = 0; k < N; ++k) {
-    double dc = c.y[k] - c.conc_in[k];
+    Y0[k] = a.Y[k * a.ld + cid];
+    const double ci = Y0[k] * rho / c_mech.W[k];
+    const double dc = c.y[k] - ci;
     finite = finite && isfinite(dc);
-    a.Y_prod[k * a.ld + cid] = dc * c_mech.W[k] / dt;
+    const double yp = dc * c_mech.W[k] / dt;
+    a.Y_prod[k * a.ld + cid] = yp;
     a.Y_prod2[k * a.ld + cid] = dc;
     E = E - c_mech.h_ref[k] * dc / dt;
-    if (a.T_after) {
-      Y0[k] = a.Y[k * a.ld + cid];
-      dYm[k] = dc * c_mech.W[k] / dt * dt / rho;
-    }
+    dYm[k] = yp * dt / rho;
   }
   a.E_f_prod[cid] = E;
-  if (a.T_after) a.T_after[cid] = temperature_after<N>(a.T[cid], rho, Y0, dYm, E * dt / rho);
+  if (a.T_after) a.T_after[cid] = temperature_after<N>(a.T[cid], Y0, dYm, E * dt / rho);
   if (a.status) a.status[cid] = finite ? (uint8_t)st : (uint8_t)kCellNonfinite;
 }
 

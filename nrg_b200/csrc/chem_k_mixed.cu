@@ -1,0 +1,15 @@
+// Chemistry-step kernels, variant "mixed": analytic Jacobian, FP32 LU with FP64 residual refinement.
+#include "chem_kernels.cuh"
+
+namespace nrg {
+
+void upload_mechanism_mixed(const DevMech& m, cudaStream_t s) {
+  cudaMemcpyToSymbolAsync(c_mech, &m, sizeof(DevMech), 0, cudaMemcpyHostToDevice, s);
+}
+
+cudaError_t launch_chem_mixed(const StepArgs& a, const LaunchCfg& cfg, int* queue,
+                              unsigned long long* counters, cudaStream_t s) {
+  return launch_variant<9, 24, kJacAnalytic, float>(a, cfg, queue, counters, s);
+}
+
+}  // namespace nrg

@@ -1,105 +1,18 @@
-// CUDA kernels for the NRG chemistry step (sm_100a).
-//
-//   k_chem_plain  -- one thread per cell, grid covers all cells (K1).
-//   k_chem_queue  -- persistent grid; every lane pulls cells from a device
-//                    work queue and is refilled as soon as its cell reaches
-//                    t = dt, so lanes never wait for the slowest cell of a
-//                    warp (K4).  Block size, blocks per SM and the number of
-//                    cells a lane reserves per queue fetch are autotuned on
-//                    the host.
-//   k_fp64_peak   -- dependent-FMA chains used to measure the FP64 pipe peak
-//                    (the roofline denominator for the integrator).
-#include <cooperative_groups.h>
+// Dispatch of the chemistry-step kernel variants, mechanism upload and the
+// FP64 peak probe (the roofline denominator for the integrator).
 #include <cuda_runtime.h>
 
 #include "chem_bdf.cuh"
 #include "chem_kernels.hpp"
 
-namespace cg = cooperative_groups;
-
 namespace nrg {
 
-// Counter slots (unsigned long long): cells integrated, steps, RHS
-// evaluations, Jacobians, linear solves, cells not ok.
-enum { kCntCells = 0, kCntSteps, kCntRhs, kCntJac, kCntSolve, kCntBad, kCntSlots };
-
-template <int N, int R, int JAC, typename LUT>
-__device__ __forceinline__ void block_flush_counters(unsigned long long* counters,
-                                                     unsigned long long v[kCntSlots]) {
-  __shared__ unsigned long long s_cnt[kCntSlots];
-  if (threadIdx.x < kCntSlots) s_cnt[threadIdx.x] = 0;
-  __syncthreads();
-#pragma unroll
-  for (int i = 0; i < kCntSlots; ++i) {
-    unsigned long long x = v[i];
-    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-    if ((threadIdx.x & 31) == 0 && x) atomicAdd(&s_cnt[i], x);
-  }
-  __syncthreads();
-  if (threadIdx.x < kCntSlots && s_cnt[threadIdx.x]) atomicAdd(&counters[threadIdx.x], s_cnt[threadIdx.x]);
-}
-
-template <int N, int R, int JAC, typename LUT>
-__global__ void __launch_bounds__(256) k_chem_plain(StepArgs a, unsigned long long* counters) {
-  long cid = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  unsigned long long v[kCntSlots] = {0, 0, 0, 0, 0, 0};
-  if (cid < a.n) {
-    CellState<N, R, LUT> c;
-    if (cell_begin<N, R>(c, a, cid)) {
-      int st;
-      while ((st = cell_advance<N, R, JAC>(c, a.mxstep)) == 0) {
-      }
-      cell_finish<N>(c, a, cid, st);
-      v[kCntCells] = 1;
-      v[kCntSteps] = c.nstep;
-      v[kCntRhs] = c.nfe;
-      v[kCntJac] = c.nje;
-      v[kCntSolve] = c.nsolve;
-      v[kCntBad] = st != kCellOk;
-    }
-  }
-  if (counters) block_flush_counters<N, R, JAC, LUT>(counters, v);
-}
-
-template <int N, int R, int JAC, typename LUT>
-__global__ void __launch_bounds__(256) k_chem_queue(StepArgs a, int* queue, int chunk,
-                                                    unsigned long long* counters) {
-  unsigned long long v[kCntSlots] = {0, 0, 0, 0, 0, 0};
-  CellState<N, R, LUT> c;
-  long cur = 0, left = 0;  // current cell and cells still reserved by this lane
-  bool have = false;
-  for (;;) {
-    if (!have) {
-      if (left == 0) {
-        // warp-aggregated reservation of `chunk` cells per requesting lane
-        cg::coalesced_group g = cg::coalesced_threads();
-        long base = 0;
-        if (g.thread_rank() == 0) base = (long)atomicAdd(queue, (int)(g.size() * chunk));
-        base = g.shfl(base, 0);
-        cur = base + (long)g.thread_rank() * chunk;
-        left = chunk;
-      } else {
-        ++cur;
-      }
-      --left;
-      if (cur >= a.n) break;
-      have = cell_begin<N, R>(c, a, cur);
-      if (!have) continue;
-    }
-    int st = cell_advance<N, R, JAC>(c, a.mxstep);
-    if (st) {
-      cell_finish<N>(c, a, cur, st);
-      v[kCntCells] += 1;
-      v[kCntSteps] += c.nstep;
-      v[kCntRhs] += c.nfe;
-      v[kCntJac] += c.nje;
-      v[kCntSolve] += c.nsolve;
-      v[kCntBad] += st != kCellOk;
-      have = false;
-    }
-  }
-  if (counters) block_flush_counters<N, R, JAC, LUT>(counters, v);
-}
+void upload_mechanism_ref(const DevMech& m, cudaStream_t s);
+void upload_mechanism_fast(const DevMech& m, cudaStream_t s);
+void upload_mechanism_mixed(const DevMech& m, cudaStream_t s);
+cudaError_t launch_chem_ref(const StepArgs&, const LaunchCfg&, int*, unsigned long long*, cudaStream_t);
+cudaError_t launch_chem_fast(const StepArgs&, const LaunchCfg&, int*, unsigned long long*, cudaStream_t);
+cudaError_t launch_chem_mixed(const StepArgs&, const LaunchCfg&, int*, unsigned long long*, cudaStream_t);
 
 __global__ void k_fp64_peak(double* out, int iters) {
   double a0 = threadIdx.x * 1e-9, a1 = a0 + 1.0, a2 = a0 + 2.0, a3 = a0 + 3.0;
@@ -118,34 +31,25 @@ __global__ void k_fp64_peak(double* out, int iters) {
 
 // ------------------------------------------------------------ launchers
 void upload_mechanism(const DevMech& m, cudaStream_t s) {
+  // every translation unit holding kernels keeps its own copy of the tables
   cudaMemcpyToSymbolAsync(c_mech, &m, sizeof(DevMech), 0, cudaMemcpyHostToDevice, s);
-}
-
-template <int N, int R, int JAC, typename LUT>
-static cudaError_t launch_t(const StepArgs& a, const LaunchCfg& cfg, int* queue,
-                            unsigned long long* counters, cudaStream_t s) {
-  if (cfg.persistent) {
-    int grid = cfg.grid > 0 ? cfg.grid : 148;
-    k_chem_queue<N, R, JAC, LUT><<<grid, cfg.block, 0, s>>>(a, queue, cfg.chunk, counters);
-  } else {
-    long grid = (a.n + cfg.block - 1) / cfg.block;
-    if (grid > 0) k_chem_plain<N, R, JAC, LUT><<<(unsigned)grid, cfg.block, 0, s>>>(a, counters);
-  }
-  return cudaGetLastError();
+  upload_mechanism_ref(m, s);
+  upload_mechanism_fast(m, s);
+  upload_mechanism_mixed(m, s);
 }
 
 cudaError_t launch_chem(int n_species, int n_reactions, int jac, bool mixed, const StepArgs& a,
                         const LaunchCfg& cfg, int* queue, unsigned long long* counters,
                         cudaStream_t s) {
-  if (n_species == 9 && n_reactions == 24) {
-    if (mixed) {
-      return jac == kJacFD ? launch_t<9, 24, kJacFD, float>(a, cfg, queue, counters, s)
-                           : launch_t<9, 24, kJacAnalytic, float>(a, cfg, queue, counters, s);
-    }
-    return jac == kJacFD ? launch_t<9, 24, kJacFD, double>(a, cfg, queue, counters, s)
-                         : launch_t<9, 24, kJacAnalytic, double>(a, cfg, queue, counters, s);
-  }
-  return cudaErrorNotSupported;
+  if (n_species != 9 || n_reactions != 24) return cudaErrorNotSupported;
+  if (mixed) return launch_chem_mixed(a, cfg, queue, counters, s);
+  return jac == kJacFD ? launch_chem_ref(a, cfg, queue, counters, s) : launch_chem_fast(a, cfg, queue, counters, s);
+}
+
+int smem_bytes_per_cell(int n_species, int n_reactions, bool mixed) {
+  if (n_species == 9 && n_reactions == 24)
+    return mixed ? SmemStore<9, 24, float, 32>::kBytesPerThread : SmemStore<9, 24, double, 32>::kBytesPerThread;
+  return 0;
 }
 
 cudaError_t launch_fp64_peak(double* out, int blocks, int threads, int iters, cudaStream_t s) {

@@ -1,0 +1,140 @@
+// Kernel templates of the chemistry step (included by the per-variant
+// translation units chem_k_*.cu, which instantiate them).
+//
+//   k_chem_plain  -- one thread per cell, grid covers all cells.
+//   k_chem_queue  -- persistent grid; every lane pulls cells from a device
+//                    work queue and is refilled as soon as its cell reaches
+//                    t = dt, so lanes never wait for the slowest cell of a
+//                    warp.  Block size, blocks per SM and the number of cells
+//                    a lane reserves per queue fetch are autotuned on the host.
+#pragma once
+
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include "chem_bdf.cuh"
+#include "chem_kernels.hpp"
+
+namespace nrg {
+
+namespace cg = cooperative_groups;
+
+// Counter slots (unsigned long long): cells integrated, steps, RHS
+// evaluations, Jacobians, linear solves, cells not ok.
+enum { kCntCells = 0, kCntSteps, kCntRhs, kCntJac, kCntSolve, kCntBad, kCntSlots };
+
+__device__ __forceinline__ void block_flush_counters(unsigned long long* counters,
+                                                     unsigned long long v[kCntSlots]) {
+  __shared__ unsigned long long s_cnt[kCntSlots];
+  if (threadIdx.x < kCntSlots) s_cnt[threadIdx.x] = 0;
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < kCntSlots; ++i) {
+    unsigned long long x = v[i];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if ((threadIdx.x & 31) == 0 && x) atomicAdd(&s_cnt[i], x);
+  }
+  __syncthreads();
+  if (threadIdx.x < kCntSlots && s_cnt[threadIdx.x]) atomicAdd(&counters[threadIdx.x], s_cnt[threadIdx.x]);
+}
+
+template <int N, int R, int JAC, typename LUT, int BS>
+__global__ void __launch_bounds__(BS, 1) k_chem_plain(StepArgs a, unsigned long long* counters) {
+  extern __shared__ __align__(16) char smem[];
+  const long cid = (long)blockIdx.x * BS + threadIdx.x;
+  unsigned long long v[kCntSlots] = {0, 0, 0, 0, 0, 0};
+  CellState<N, R, LUT, BS> c;
+  c.bind(smem, threadIdx.x);
+  if (cid < a.n) {
+    if (cell_begin<N, R>(c, a, cid)) {
+      int st;
+      while ((st = cell_advance<N, R, JAC, LUT>(c, a.mxstep)) == 0) {
+      }
+      cell_finish<N>(c, a, cid, st);
+      v[kCntCells] = 1;
+      v[kCntSteps] = c.nstep;
+      v[kCntRhs] = c.nfe;
+      v[kCntJac] = c.nje;
+      v[kCntSolve] = c.nsolve;
+      v[kCntBad] = st != kCellOk;
+    }
+  }
+  if (counters) block_flush_counters(counters, v);
+}
+
+template <int N, int R, int JAC, typename LUT, int BS>
+__global__ void __launch_bounds__(BS, 1) k_chem_queue(StepArgs a, int* queue, int chunk,
+                                                       unsigned long long* counters) {
+  extern __shared__ __align__(16) char smem[];
+  unsigned long long v[kCntSlots] = {0, 0, 0, 0, 0, 0};
+  CellState<N, R, LUT, BS> c;
+  c.bind(smem, threadIdx.x);
+  long cur = 0, left = 0;  // current cell and cells still reserved by this lane
+  bool have = false;
+  for (;;) {
+    if (!have) {
+      if (left == 0) {
+        // warp-aggregated reservation of `chunk` cells per requesting lane
+        cg::coalesced_group g = cg::coalesced_threads();
+        long base = 0;
+        if (g.thread_rank() == 0) base = (long)atomicAdd(queue, (int)(g.size() * chunk));
+        base = g.shfl(base, 0);
+        cur = base + (long)g.thread_rank() * chunk;
+        left = chunk;
+      } else {
+        ++cur;
+      }
+      --left;
+      if (cur >= a.n) break;
+      have = cell_begin<N, R>(c, a, cur);
+      if (!have) continue;
+    }
+    const int st = cell_advance<N, R, JAC, LUT>(c, a.mxstep);
+    if (st) {
+      cell_finish<N>(c, a, cur, st);
+      v[kCntCells] += 1;
+      v[kCntSteps] += c.nstep;
+      v[kCntRhs] += c.nfe;
+      v[kCntJac] += c.nje;
+      v[kCntSolve] += c.nsolve;
+      v[kCntBad] += st != kCellOk;
+      have = false;
+    }
+  }
+  if (counters) block_flush_counters(counters, v);
+}
+
+template <int N, int R, int JAC, typename LUT, int BS>
+static cudaError_t launch_bs(const StepArgs& a, const LaunchCfg& cfg, int* queue,
+                             unsigned long long* counters, cudaStream_t s) {
+  const size_t smem = (size_t)BS * SmemStore<N, R, LUT, BS>::kBytesPerThread;
+  cudaError_t e;
+  if (cfg.persistent) {
+    e = cudaFuncSetAttribute(k_chem_queue<N, R, JAC, LUT, BS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+    if (e != cudaSuccess) return e;
+    const int grid = cfg.grid > 0 ? cfg.grid : 148;
+    k_chem_queue<N, R, JAC, LUT, BS><<<grid, BS, smem, s>>>(a, queue, cfg.chunk, counters);
+  } else {
+    e = cudaFuncSetAttribute(k_chem_plain<N, R, JAC, LUT, BS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+    if (e != cudaSuccess) return e;
+    const long grid = (a.n + BS - 1) / BS;
+    if (grid > 0) k_chem_plain<N, R, JAC, LUT, BS><<<(unsigned)grid, BS, smem, s>>>(a, counters);
+  }
+  return cudaGetLastError();
+}
+
+
+// Launches one (JAC, LUT) variant with a runtime block size.
+template <int N, int R, int JAC, typename LUT>
+static cudaError_t launch_variant(const StepArgs& a, const LaunchCfg& cfg, int* queue,
+                                  unsigned long long* counters, cudaStream_t s) {
+  switch (cfg.block) {
+    case 64: return launch_bs<N, R, JAC, LUT, 64>(a, cfg, queue, counters, s);
+    case 128: return launch_bs<N, R, JAC, LUT, 128>(a, cfg, queue, counters, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace nrg

@@ -42,6 +42,9 @@ cudaError_t launch_chem(int n_species, int n_reactions, int jac, bool mixed, con
                         const LaunchCfg& cfg, int* queue, unsigned long long* counters,
                         cudaStream_t s);
 
+// Shared memory one cell of the given mechanism size occupies.
+int smem_bytes_per_cell(int n_species, int n_reactions, bool mixed);
+
 cudaError_t launch_fp64_peak(double* out, int blocks, int threads, int iters, cudaStream_t s);
 
 }  // namespace nrg

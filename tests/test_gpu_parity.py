@@ -64,7 +64,7 @@ def test_launch_shapes_and_graph_agree(solver, W):
     base, _ = run_device(solver, f, "fast", launch=dict(persistent=False, block=128))
     for launch in (dict(persistent=True, block=128, grid=0, chunk=1),
                    dict(persistent=True, block=64, grid=296, chunk=4),
-                   dict(persistent=True, block=256, grid=148, chunk=2)):
+                   dict(persistent=False, block=64)):
         for graph in (True, False):
             g, _ = run_device(solver, f, "fast", launch=launch, graph=graph)
             for k in ("Y_prod", "Y_prod2", "E_f_prod", "T_after"):
