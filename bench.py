@@ -329,7 +329,7 @@ def main():
                        "steps_per_active_cell": st["steps"] / max(1, st["cells_active"])},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak_fp64, "unit": "TFLOP/s",
                          "frac": achieved / peak_fp64, "traffic": None,
-                         "kernel": "k_chem_queue (persistent BDF integrator)",
+                         "kernel": "k_chem_warp (warp-per-cell BDF integrator)" if launch["kernel"] == "warp_queue" else "k_chem_queue/k_chem_plain (thread-per-cell BDF integrator)",
                          "peak_source": "measured live: dependent-FMA FP64 probe (MEASURED_PEAKS.json has no FP64 figure)",
                          "flops_per_step": flops, "flop_model": fm},
             "cpu_baseline": cpu,

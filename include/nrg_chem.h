@@ -120,11 +120,14 @@ NRG_API int nrg_chem_step_device(nrg_chem* h, double time_step, long n, long ld,
  * 'table_approximated'. */
 NRG_API int nrg_chem_set_mode(nrg_chem* h, int mode);
 
-/* Launch shape: persistent work-queue kernel or one thread per cell, threads
- * per block (64 or 128: each cell keeps ~1.7 KB of state in shared memory),
- * persistent grid (0 = one block per SM), cells per queue fetch (1..64). */
-NRG_API int nrg_chem_set_launch(nrg_chem* h, int persistent, int block, int grid, int chunk);
-NRG_API int nrg_chem_get_launch(nrg_chem* h, int* persistent, int* block, int* grid, int* chunk);
+/* Launch shape.  kernel: 0 = one thread per cell over a grid covering the
+ * cells, 1 = one thread per cell pulling cells from a device work queue,
+ * 2 = one warp per cell pulling cells from the work queue (default).  block:
+ * 64 for kernels 0/1 (each cell keeps ~1.7 KB in shared memory), 128 or 256
+ * for kernel 2.  grid: persistent grid size (0 = fill the GPU).  chunk: cells
+ * reserved per queue fetch (1..64). */
+NRG_API int nrg_chem_set_launch(nrg_chem* h, int kernel, int block, int grid, int chunk);
+NRG_API int nrg_chem_get_launch(nrg_chem* h, int* kernel, int* block, int* grid, int* chunk);
 
 /* Times candidate launch shapes on the given device-resident inputs (outputs
  * are scratch) and keeps the fastest for this handle.  ms_best may be NULL. */

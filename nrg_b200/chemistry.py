@@ -217,13 +217,20 @@ class ChemicalKineticsSolver:
         _check(lib().nrg_chem_set_mode(self._h, MODES[mode]), self._h)
         self.mode = mode
 
-    def set_launch(self, persistent=True, block=128, grid=0, chunk=1) -> None:
-        _check(lib().nrg_chem_set_launch(self._h, int(persistent), block, grid, chunk), self._h)
+    KERNELS = {"thread": 0, "thread_queue": 1, "warp_queue": 2}
+
+    def set_launch(self, kernel="warp_queue", block=256, grid=0, chunk=1) -> None:
+        """kernel: 'thread' (one thread per cell), 'thread_queue' (thread per
+        cell with a work queue) or 'warp_queue' (warp per cell, work queue)."""
+        k = self.KERNELS[kernel] if isinstance(kernel, str) else int(kernel)
+        _check(lib().nrg_chem_set_launch(self._h, k, block, grid, chunk), self._h)
 
     def get_launch(self) -> dict:
         v = [ctypes.c_int() for _ in range(4)]
         _check(lib().nrg_chem_get_launch(self._h, *[ctypes.byref(x) for x in v]), self._h)
-        return dict(zip(("persistent", "block", "grid", "chunk"), [x.value for x in v]))
+        d = dict(zip(("kernel", "block", "grid", "chunk"), [x.value for x in v]))
+        d["kernel"] = {v: k for k, v in self.KERNELS.items()}[d["kernel"]]
+        return d
 
     def set_graph(self, enable: bool) -> None:
         _check(lib().nrg_chem_set_graph(self._h, int(enable)), self._h)

@@ -143,6 +143,13 @@ std::string build_dev_mech(const nrg::Mechanism& m, DevMech* d) {
     d->E_low[r] = rx.E_low;
     for (int q = 0; q < 4; ++q) d->troe[r][q] = rx.troe[q];
     d->dnu[r] = (double)(rx.n_right - rx.n_left);
+    for (int uu = 0; uu < u; ++uu) {
+      const int k = d->upd_k[r][uu];
+      if (d->sp_n[k] >= nrg::kMaxSpecUpd) return "species appears in too many reactions";
+      d->sp_r[k][d->sp_n[k]] = r;
+      d->sp_sgn[k][d->sp_n[k]] = d->upd_prod[r][uu] ? 1 : -1;
+      d->sp_n[k] += 1;
+    }
     for (int k = 0; k < N; ++k) d->eff[r][k] = m.eff[(size_t)r * N + k];
   }
   for (int k = 0; k < N; ++k) {
@@ -210,12 +217,12 @@ int jac_of(int mode) { return mode == NRG_MODE_REFERENCE ? 0 : 1; }
 // Enqueue the plain integrator (no surrogate) on stream s.
 cudaError_t enqueue_integrator(nrg_chem* h, const StepArgs& a, const LaunchCfg& cfg, cudaStream_t s) {
   cudaError_t e = cudaSuccess;
-  if (cfg.persistent) {
+  if (cfg.kernel != nrg::kKernelThreadGrid) {
     e = cudaMemsetAsync(h->d_queue, 0, sizeof(int), s);
     if (e != cudaSuccess) return e;
   }
   LaunchCfg c = cfg;
-  if (c.persistent && c.grid <= 0) c.grid = h->num_sms;
+  if (c.kernel == nrg::kKernelThreadQueue && c.grid <= 0) c.grid = h->num_sms;
   return nrg::launch_chem(h->mech.n(), h->mech.r(), jac_of(h->mode), h->mode == NRG_MODE_MIXED, a, c,
                           h->d_queue, h->d_counters, s);
 }
@@ -226,7 +233,6 @@ cudaError_t enqueue_step(nrg_chem* h, const StepArgs& a, cudaStream_t s) {
   if (h->mode == NRG_MODE_SURROGATE) return nrg::surrogate_step(h->sur, a, h->cfg, h->d_queue, h->d_counters, s,
                                                                  [h](const StepArgs& fa, cudaStream_t fs) {
                                                                    LaunchCfg c = h->cfg;
-                                                                   c.persistent = true;
                                                                    return enqueue_integrator(h, fa, c, fs);
                                                                  });
   return enqueue_integrator(h, a, h->cfg, s);
@@ -328,8 +334,8 @@ extern "C" int nrg_chem_create(const char* mechanism_path, const char* thermo_pa
     nrg_chem_destroy(h);
     return fail(nullptr, NRG_ERR_CUDA, msg);
   }
-  h->cfg.persistent = true;
-  h->cfg.block = 128;
+  h->cfg.kernel = nrg::kKernelWarpQueue;
+  h->cfg.block = 256;
   h->cfg.grid = 0;
   h->cfg.chunk = 1;
   h->sur = nrg::surrogate_create(h->dm);
@@ -361,20 +367,23 @@ extern "C" int nrg_chem_set_mode(nrg_chem* h, int mode) {
   return NRG_OK;
 }
 
-extern "C" int nrg_chem_set_launch(nrg_chem* h, int persistent, int block, int grid, int chunk) {
+extern "C" int nrg_chem_set_launch(nrg_chem* h, int kernel, int block, int grid, int chunk) {
   if (!h) return NRG_ERR_ARG;
-  if ((block != 64 && block != 128) || chunk < 1 || chunk > 64 || grid < 0)
-    return fail(h, NRG_ERR_ARG, "launch shape out of range (block 64 or 128, chunk 1..64, grid >= 0)");
-  h->cfg.persistent = persistent != 0;
+  const bool ok_kernel = kernel >= 0 && kernel <= 2;
+  const bool ok_block = kernel == 2 ? (block == 128 || block == 256) : block == 64;
+  if (!ok_kernel || !ok_block || chunk < 1 || chunk > 64 || grid < 0)
+    return fail(h, NRG_ERR_ARG,
+                "launch shape out of range (kernel 0/1: block 64; kernel 2: block 128 or 256; chunk 1..64)");
+  h->cfg.kernel = kernel;
   h->cfg.block = block;
   h->cfg.grid = grid;
   h->cfg.chunk = chunk;
   return NRG_OK;
 }
 
-extern "C" int nrg_chem_get_launch(nrg_chem* h, int* persistent, int* block, int* grid, int* chunk) {
+extern "C" int nrg_chem_get_launch(nrg_chem* h, int* kernel, int* block, int* grid, int* chunk) {
   if (!h) return NRG_ERR_ARG;
-  if (persistent) *persistent = h->cfg.persistent;
+  if (kernel) *kernel = h->cfg.kernel;
   if (block) *block = h->cfg.block;
   if (grid) *grid = h->cfg.grid;
   if (chunk) *chunk = h->cfg.chunk;
@@ -511,23 +520,29 @@ extern "C" int nrg_chem_autotune(nrg_chem* h, double time_step, long n, long ld,
   a.Y_prod = Y_prod; a.Y_prod2 = Y_prod2; a.E_f_prod = E_f_prod; a.T_after = nullptr; a.status = nullptr;
   a.mxstep = 10000;
   std::vector<LaunchCfg> cands;
-  // one cell holds ~1.7 KB of shared memory, so 128-thread blocks fit once
-  // per SM and 64-thread blocks twice
-  for (int block : {64, 128})
-    for (int per_sm : {1, 2})
-      for (int chunk : {1, 2, 4}) {
-        if (block * per_sm > 128) continue;
+  for (int block : {128, 256})
+    for (int per_sm : {0, 1, 2, 4})
+      for (int chunk : {1, 4}) {
         LaunchCfg c;
-        c.persistent = true;
+        c.kernel = nrg::kKernelWarpQueue;
         c.block = block;
-        c.grid = per_sm * h->num_sms;
+        c.grid = per_sm * h->num_sms;  // 0: occupancy-derived
         c.chunk = chunk;
         cands.push_back(c);
       }
+  for (int per_sm : {1, 2})
+    for (int chunk : {1, 2}) {
+      LaunchCfg c;
+      c.kernel = nrg::kKernelThreadQueue;
+      c.block = 64;
+      c.grid = per_sm * h->num_sms;
+      c.chunk = chunk;
+      cands.push_back(c);
+    }
   {
     LaunchCfg c;
-    c.persistent = false;
-    c.block = 128;
+    c.kernel = nrg::kKernelThreadGrid;
+    c.block = 64;
     cands.push_back(c);
   }
   cudaStream_t s = h->stream;

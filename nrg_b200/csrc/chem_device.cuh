@@ -14,6 +14,7 @@ namespace nrg {
 constexpr int kMaxSpecies = 16;
 constexpr int kMaxReactions = 64;
 constexpr int kMaxOrd = 5;  // MXORD for Gear (MINT = 2)
+constexpr int kMaxSpecUpd = 64;  // reactions touching one species
 
 // Per-reaction update list entry: species (0-based) and whether the
 // occurrence is a reactant (Zdot -= f, += r) or a product (Zdot -= r, += f).
@@ -40,6 +41,11 @@ struct DevMech {
   double el[13 * 12], tq[3 * 12];
   double eps, ewt, hmax, uround;
   double sqrt_uround, br, bl, bp, facmin;
+  // per-species update lists in reaction order: reaction index and sign of
+  // the net rate (+1 product occurrence, -1 reactant occurrence)
+  int sp_n[kMaxSpecies];
+  int sp_r[kMaxSpecies][kMaxSpecUpd];
+  int sp_sgn[kMaxSpecies][kMaxSpecUpd];
   // element composition for conservation checks (H, O, N) in atoms/molecule
   double elem[3][kMaxSpecies];
 };

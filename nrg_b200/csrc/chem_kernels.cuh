@@ -14,6 +14,7 @@
 
 #include "chem_bdf.cuh"
 #include "chem_kernels.hpp"
+#include "chem_warp.cuh"
 
 namespace nrg {
 
@@ -109,7 +110,7 @@ static cudaError_t launch_bs(const StepArgs& a, const LaunchCfg& cfg, int* queue
                              unsigned long long* counters, cudaStream_t s) {
   const size_t smem = (size_t)BS * SmemStore<N, R, LUT, BS>::kBytesPerThread;
   cudaError_t e;
-  if (cfg.persistent) {
+  if (cfg.kernel == kKernelThreadQueue) {
     e = cudaFuncSetAttribute(k_chem_queue<N, R, JAC, LUT, BS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem);
     if (e != cudaSuccess) return e;
@@ -126,15 +127,74 @@ static cudaError_t launch_bs(const StepArgs& a, const LaunchCfg& cfg, int* queue
 }
 
 
-// Launches one (JAC, LUT) variant with a runtime block size.
+// Warp-per-cell persistent kernel: every warp pulls `chunk` cells at a time
+// from the work queue and integrates them one after the other.
+template <int N, int R, int JAC, typename LUT, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) k_chem_warp(StepArgs a, int* queue, int chunk,
+                                                         unsigned long long* counters) {
+  __shared__ WarpSmem<N, R, LUT> sm[WARPS];
+  unsigned long long v[kCntSlots] = {0, 0, 0, 0, 0, 0};
+  WarpCell<N, R, LUT> c;
+  c.lane = threadIdx.x & 31;
+  c.sm = &sm[threadIdx.x >> 5];
+  long cur = 0, left = 0;
+  for (;;) {
+    if (left == 0) {
+      int base = 0;
+      if (c.lane == 0) base = atomicAdd(queue, chunk);
+      cur = __shfl_sync(kFullMask, base, 0);
+      left = chunk;
+    } else {
+      ++cur;
+    }
+    --left;
+    if (cur >= a.n) break;
+    if (!warp_cell_begin(c, a, cur)) continue;
+    int st;
+    while ((st = warp_cell_advance<N, R, JAC>(c, a.mxstep)) == 0) {
+    }
+    warp_cell_finish(c, a, cur, st);
+    if (c.lane == 0) {
+      v[kCntCells] += 1;
+      v[kCntSteps] += c.nstep;
+      v[kCntRhs] += c.nfe;
+      v[kCntJac] += c.nje;
+      v[kCntSolve] += c.nsolve;
+      v[kCntBad] += st != kCellOk;
+    }
+  }
+  if (counters) block_flush_counters(counters, v);
+}
+
+template <int N, int R, int JAC, typename LUT, int WARPS>
+static cudaError_t launch_warp(const StepArgs& a, const LaunchCfg& cfg, int* queue,
+                               unsigned long long* counters, cudaStream_t s) {
+  int grid = cfg.grid;
+  if (grid <= 0) {
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_chem_warp<N, R, JAC, LUT, WARPS>, WARPS * 32, 0);
+    grid = sms * (per_sm > 0 ? per_sm : 1);
+  }
+  k_chem_warp<N, R, JAC, LUT, WARPS><<<grid, WARPS * 32, 0, s>>>(a, queue, cfg.chunk, counters);
+  return cudaGetLastError();
+}
+
+// Launches one (JAC, LUT) variant: cfg.kernel selects thread-per-cell (grid
+// or work queue, 64-thread blocks) or warp-per-cell (128- or 256-thread blocks).
 template <int N, int R, int JAC, typename LUT>
 static cudaError_t launch_variant(const StepArgs& a, const LaunchCfg& cfg, int* queue,
                                   unsigned long long* counters, cudaStream_t s) {
-  switch (cfg.block) {
-    case 64: return launch_bs<N, R, JAC, LUT, 64>(a, cfg, queue, counters, s);
-    case 128: return launch_bs<N, R, JAC, LUT, 128>(a, cfg, queue, counters, s);
-    default: return cudaErrorInvalidValue;
+  if (cfg.kernel == kKernelWarpQueue) {
+    switch (cfg.block) {
+      case 128: return launch_warp<N, R, JAC, LUT, 4>(a, cfg, queue, counters, s);
+      case 256: return launch_warp<N, R, JAC, LUT, 8>(a, cfg, queue, counters, s);
+      default: return cudaErrorInvalidValue;
+    }
   }
+  if (cfg.block != 64) return cudaErrorInvalidValue;
+  return launch_bs<N, R, JAC, LUT, 64>(a, cfg, queue, counters, s);
 }
 
 }  // namespace nrg

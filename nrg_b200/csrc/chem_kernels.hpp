@@ -27,17 +27,19 @@ struct StepArgs {
   int mxstep;
 };
 
+enum KernelKind { kKernelThreadGrid = 0, kKernelThreadQueue = 1, kKernelWarpQueue = 2 };
+
 struct LaunchCfg {
-  bool persistent = true;  // work-queue kernel (else one thread per cell)
-  int block = 128;         // threads per block
-  int grid = 0;            // persistent grid size (0: one block per SM)
-  int chunk = 1;           // cells a lane reserves per queue fetch
+  int kernel = kKernelWarpQueue;  // KernelKind
+  int block = 256;                // threads per block
+  int grid = 0;                   // persistent grid (0: fill the GPU)
+  int chunk = 1;                  // cells reserved per queue fetch (per lane or per warp)
 };
 
 void upload_mechanism(const DevMech& m, cudaStream_t s);
 
 // jac: 0 finite-difference (reference DDPST), 1 analytic.  mixed: float LU.
-// queue must point at a zeroed device int when cfg.persistent.
+// queue must point at a zeroed device int for the work-queue kernels.
 cudaError_t launch_chem(int n_species, int n_reactions, int jac, bool mixed, const StepArgs& a,
                         const LaunchCfg& cfg, int* queue, unsigned long long* counters,
                         cudaStream_t s);

@@ -61,15 +61,25 @@ def test_config1_sample_parity(solver, oracle_mech, W):
 
 def test_launch_shapes_and_graph_agree(solver, W):
     f = fields.config0(W)
-    base, _ = run_device(solver, f, "fast", launch=dict(persistent=False, block=128))
-    for launch in (dict(persistent=True, block=128, grid=0, chunk=1),
-                   dict(persistent=True, block=64, grid=296, chunk=4),
-                   dict(persistent=False, block=64)):
+    base, _ = run_device(solver, f, "fast", launch=dict(kernel="warp_queue", block=256))
+    for launch in (dict(kernel="warp_queue", block=128, grid=0, chunk=1),
+                   dict(kernel="warp_queue", block=256, grid=296, chunk=4),
+                   dict(kernel="warp_queue", block=128, grid=148, chunk=7)):
         for graph in (True, False):
             g, _ = run_device(solver, f, "fast", launch=launch, graph=graph)
             for k in ("Y_prod", "Y_prod2", "E_f_prod", "T_after"):
                 np.testing.assert_array_equal(g[k], base[k])
-    solver.set_launch(persistent=True, block=128, grid=0, chunk=1)
+    solver.set_launch(kernel="warp_queue", block=256, grid=0, chunk=1)
+
+
+@pytest.mark.parametrize("kernel", ["thread", "thread_queue"])
+def test_thread_per_cell_kernels_parity(solver, oracle_mech, W, kernel):
+    f = fields.slice_field(fields.config0(W), 1024)
+    o = oracle_run(oracle_mech, f)
+    for mode in ("reference", "fast"):
+        g, _ = run_device(solver, f, mode, launch=dict(kernel=kernel, block=64, grid=0, chunk=1))
+        check_parity(g, o, f, np.ones(f.n, bool))
+    solver.set_launch(kernel="warp_queue", block=256, grid=0, chunk=1)
 
 
 def test_skip_rule_bc_and_untouched_y_prod2(solver, oracle_mech, W):
