@@ -114,8 +114,8 @@ def flop_model(tables: dict, mode: str) -> dict:
     step  : predictor, Nordsieck update, error weights and norms (~30N)
     setup : 9 NASA-7 species x 40 + 24 reactions x 30 (transcendentals as 1)
     """
-    co = tables["coeffs"]
-    N, R = tables["n_species"], tables["n_reactions"]
+    co = tables["coeffs"].tolist()
+    N, R = int(tables["n_species"]), int(tables["n_reactions"])
     f_rhs = 0
     f_jac = 0
     for r in range(R):
@@ -134,6 +134,7 @@ def flop_model(tables: dict, mode: str) -> dict:
 
 
 def algorithmic_flops(st: dict, fm: dict) -> float:
+    st = {k: float(v) for k, v in st.items()}
     return (st["cells_active"] * fm["setup"] + st["rhs_evals"] * fm["rhs"] + st["jacobians"] * fm["jac"]
             + st["solves"] * fm["solve"] + st["steps"] * fm["step"])
 
