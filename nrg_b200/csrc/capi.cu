@@ -31,6 +31,7 @@ struct nrg_chem {
   LaunchCfg cfg;
   bool use_graph = true;
   int* d_queue = nullptr;
+  DevMech* d_mech = nullptr;  // global copy of the tables for kernels that stage them in shared memory
   unsigned long long* d_counters = nullptr;
   unsigned long long* h_counters = nullptr;  // pinned
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_in = nullptr;
@@ -320,6 +321,8 @@ extern "C" int nrg_chem_create(const char* mechanism_path, const char* thermo_pa
       (ce = cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device)) != cudaSuccess ||
       (ce = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess ||
       (ce = cudaMalloc(&h->d_queue, sizeof(int) * 4)) != cudaSuccess ||
+      (ce = cudaMalloc(&h->d_mech, sizeof(DevMech))) != cudaSuccess ||
+      (ce = cudaMemcpy(h->d_mech, &h->dm, sizeof(DevMech), cudaMemcpyHostToDevice)) != cudaSuccess ||
       (ce = cudaMalloc(&h->d_counters, sizeof(unsigned long long) * 8)) != cudaSuccess ||
       (ce = cudaMallocHost(&h->h_counters, sizeof(unsigned long long) * 8)) != cudaSuccess ||
       (ce = cudaEventCreate(&h->ev0)) != cudaSuccess || (ce = cudaEventCreate(&h->ev1)) != cudaSuccess ||
@@ -350,6 +353,7 @@ extern "C" int nrg_chem_destroy(nrg_chem* h) {
   nrg::surrogate_destroy(h->sur);
   free_staging(h);
   cudaFree(h->d_queue);
+  cudaFree(h->d_mech);
   cudaFree(h->d_counters);
   cudaFreeHost(h->h_counters);
   if (h->ev0) cudaEventDestroy(h->ev0);
@@ -421,6 +425,7 @@ extern "C" int nrg_chem_step_device(nrg_chem* h, double time_step, long n, long 
   a.T_after = T_after;
   a.status = status;
   a.mxstep = 10000;
+  a.mech = h->d_mech;
   if (n == 0) {
     if (stats) std::memset(stats, 0, sizeof(*stats));
     return NRG_OK;
@@ -485,6 +490,7 @@ extern "C" int nrg_chem_step(nrg_chem* h, double time_step, const nrg_field_desc
   a.T_after = nullptr;
   a.status = h->d_status;
   a.mxstep = 10000;
+  a.mech = h->d_mech;
   if (!(time_step > 0.0)) return fail(h, NRG_ERR_ARG, "time_step must be > 0");
   rc = run_step(h, a, s, stats);
   if (rc) return rc;
@@ -519,6 +525,7 @@ extern "C" int nrg_chem_autotune(nrg_chem* h, double time_step, long n, long ld,
   a.n = n; a.ld = ld; a.dt = time_step; a.T = T; a.rho = rho; a.Y = Y; a.bc = (const int8_t*)bc;
   a.Y_prod = Y_prod; a.Y_prod2 = Y_prod2; a.E_f_prod = E_f_prod; a.T_after = nullptr; a.status = nullptr;
   a.mxstep = 10000;
+  a.mech = h->d_mech;
   std::vector<LaunchCfg> cands;
   for (int block : {128, 256})
     for (int per_sm : {0, 1, 2, 4})

@@ -133,8 +133,18 @@ template <int N, int R, int JAC, typename LUT, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) k_chem_warp(StepArgs a, int* queue, int chunk,
                                                          unsigned long long* counters) {
   __shared__ WarpSmem<N, R, LUT> sm[WARPS];
+  __shared__ __align__(16) DevMech sM;
+  {
+    // lanes read per-reaction and per-species entries at different addresses,
+    // which __constant__ memory would serialize: work from a shared copy
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(a.mech);
+    unsigned long long* dst = reinterpret_cast<unsigned long long*>(&sM);
+    for (int i = threadIdx.x; i < (int)(sizeof(DevMech) / 8); i += WARPS * 32) dst[i] = src[i];
+    __syncthreads();
+  }
   unsigned long long v[kCntSlots] = {0, 0, 0, 0, 0, 0};
   WarpCell<N, R, LUT> c;
+  c.M = &sM;
   c.lane = threadIdx.x & 31;
   c.sm = &sm[threadIdx.x >> 5];
   long cur = 0, left = 0;

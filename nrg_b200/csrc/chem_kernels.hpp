@@ -25,6 +25,7 @@ struct StepArgs {
   double* T_after;    // may be null
   uint8_t* status;    // may be null
   int mxstep;
+  const DevMech* mech;  // device copy of the mechanism tables (global memory)
 };
 
 enum KernelKind { kKernelThreadGrid = 0, kKernelThreadQueue = 1, kKernelWarpQueue = 2 };

@@ -35,6 +35,7 @@ struct WarpSmem {
 
 template <int N, int R, typename LUT>
 struct WarpCell {
+  const DevMech* M;  // block-shared copy of the mechanism tables
   WarpSmem<N, R, LUT>* sm;
   int lane;
   double yh[kMaxOrd + 1];  // Nordsieck row `lane`
@@ -73,8 +74,11 @@ __device__ __forceinline__ void yh_set(double (&yh)[kMaxOrd + 1], int j, double 
 }
 
 // First index of the largest value over lanes (IDAMAX tie rule); lanes that
-// do not take part pass v = -1.
+// do not take part pass v = -1.  A NaN ranks below every number of a lane
+// that takes part, so (value, index) is a strict total order and every lane
+// ends with the same participating index.
 __device__ __forceinline__ int warp_argmax(double v, int idx, double* vmax) {
+  if (v != v) v = -0.5;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     const double v2 = __shfl_xor_sync(kFullMask, v, o);
@@ -97,40 +101,52 @@ __device__ void warp_rate_constants(WarpCell<N, R, LUT>& c, double Tin, const do
   const double T = NRG_FMIN(Tin, 10000.0);
   if (c.lane < N) {
     const double logt = log(NRG_FMIN(T, 6000.0));
-    c.sm->th_s[c.lane] = d_entropy(T, c.lane, logt);
-    c.sm->th_h[c.lane] = d_enthalpy(T, c.lane);
+    const double t = NRG_FMIN(T, 6000.0);
+    const double* ak = c.M->a[c.lane][nasa_set(t)];
+    double sv = ak[4] / 4.0;
+    sv = sv * t + ak[3] / 3.0;
+    sv = sv * t + ak[2] / 2.0;
+    sv = sv * t + ak[1] / 1.0;
+    c.sm->th_s[c.lane] = sv * t + ak[6] + ak[0] * logt;
+    double hv = ak[4] / 5.0;
+    hv = hv * t + ak[3] / 4.0;
+    hv = hv * t + ak[2] / 3.0;
+    hv = hv * t + ak[1] / 2.0;
+    hv = hv * t + ak[0] / 1.0;
+    hv = hv + ak[5] / t;
+    c.sm->th_h[c.lane] = hv * t;
   }
   __syncwarp();
   const double conc_ref = PATM / RG / T;
   for (int r = c.lane; r < R; r += 32) {
     double mc = 0.0;
 #pragma unroll
-    for (int k = 0; k < N; ++k) mc = mc + yc[k] * c_mech.eff[r][k];
+    for (int k = 0; k < N; ++k) mc = mc + yc[k] * c.M->eff[r][k];
     double d_s = 0.0, d_h = 0.0;
     bool m_left = false, m_right = false;
-    for (int i = 0; i < c_mech.nr[r]; ++i) {
-      const int sp = c_mech.right[r][i];
+    for (int i = 0; i < c.M->nr[r]; ++i) {
+      const int sp = c.M->right[r][i];
       if (sp < 0) { m_right = true; continue; }
       d_s = d_s + c.sm->th_s[sp];
       d_h = d_h + c.sm->th_h[sp];
     }
-    for (int i = 0; i < c_mech.nl[r]; ++i) {
-      const int sp = c_mech.left[r][i];
+    for (int i = 0; i < c.M->nl[r]; ++i) {
+      const int sp = c.M->left[r][i];
       if (sp < 0) { m_left = true; continue; }
       d_s = d_s - c.sm->th_s[sp];
       d_h = d_h - c.sm->th_h[sp];
     }
-    const int type = c_mech.type[r];
-    const double kinf = c_mech.A[r] * pow(T, c_mech.beta[r]) * exp(-(c_mech.E[r] / RG / T));
+    const int type = c.M->type[r];
+    const double kinf = c.M->A[r] * pow(T, c.M->beta[r]) * exp(-(c.M->E[r] / RG / T));
     double k = kinf;
     if (type == 2 || type == 3 || type == 7) {
-      const double k0 = c_mech.A_low[r] * pow(T, c_mech.beta_low[r]) * exp(-(c_mech.E_low[r] / RG / T));
+      const double k0 = c.M->A_low[r] * pow(T, c.M->beta_low[r]) * exp(-(c.M->E_low[r] / RG / T));
       const double rp = k0 * mc / kinf;
       k = kinf * (rp / (1.0 + rp));
       if (type == 3) {
-        const double al = c_mech.troe[r][0];
-        const double Fc = (1.0 - al) * exp(-(T / c_mech.troe[r][1])) + al * exp(-(T / c_mech.troe[r][2])) +
-                          exp(-(c_mech.troe[r][3] / T));
+        const double al = c.M->troe[r][0];
+        const double Fc = (1.0 - al) * exp(-(T / c.M->troe[r][1])) + al * exp(-(T / c.M->troe[r][2])) +
+                          exp(-(c.M->troe[r][3] / T));
         const double lf = log10(Fc);
         const double cc = -0.4 - 0.67 * lf;
         const double nn = 0.75 - 1.27 * lf;
@@ -148,7 +164,7 @@ __device__ void warp_rate_constants(WarpCell<N, R, LUT>& c, double Tin, const do
     double kr = 0.0;
     if (type < 5) {
       const double Kp = exp(d_s / RG - d_h / RG / T);
-      kr = k / (Kp * int_pow(conc_ref, c_mech.dnu[r]));
+      kr = k / (Kp * int_pow(conc_ref, c.M->dnu[r]));
     }
     c.sm->kf[r] = m_left ? k * mc : k;
     c.sm->kr[r] = m_right ? kr * mc : kr;
@@ -166,13 +182,13 @@ __device__ __forceinline__ double warp_rhs(WarpCell<N, R, LUT>& c, double x) {
   __syncwarp();
   for (int r = c.lane; r < R; r += 32) {
     double f = c.sm->kf[r];
-    for (int i = 0; i < c_mech.nl[r]; ++i) {
-      const int sp = c_mech.left[r][i];
+    for (int i = 0; i < c.M->nl[r]; ++i) {
+      const int sp = c.M->left[r][i];
       if (sp >= 0) f = f * c.sm->z[sp];
     }
     double b = c.sm->kr[r];
-    for (int i = 0; i < c_mech.nr[r]; ++i) {
-      const int sp = c_mech.right[r][i];
+    for (int i = 0; i < c.M->nr[r]; ++i) {
+      const int sp = c.M->right[r][i];
       if (sp >= 0) b = b * c.sm->z[sp];
     }
     c.sm->q[r] = f - b;
@@ -180,10 +196,10 @@ __device__ __forceinline__ double warp_rhs(WarpCell<N, R, LUT>& c, double x) {
   __syncwarp();
   double acc = 0.0;
   if (c.lane < N) {
-    const int n = c_mech.sp_n[c.lane];
+    const int n = c.M->sp_n[c.lane];
     for (int u = 0; u < n; ++u) {
-      const double q = c.sm->q[c_mech.sp_r[c.lane][u]];
-      acc = c_mech.sp_sgn[c.lane][u] > 0 ? acc + q : acc - q;
+      const double q = c.sm->q[c.M->sp_r[c.lane][u]];
+      acc = c.M->sp_sgn[c.lane][u] > 0 ? acc + q : acc - q;
     }
   }
   return acc;
@@ -192,11 +208,11 @@ __device__ __forceinline__ double warp_rhs(WarpCell<N, R, LUT>& c, double x) {
 // d(net rate of reaction r)/dz_sp for factor position p on one side, at z.
 template <int N, int R, typename LUT>
 __device__ __forceinline__ double rate_partial(const WarpCell<N, R, LUT>& c, int r, int side, int p) {
-  const int cnt = side ? c_mech.nr[r] : c_mech.nl[r];
+  const int cnt = side ? c.M->nr[r] : c.M->nl[r];
   double d = side ? c.sm->kr[r] : c.sm->kf[r];
   for (int qq = 0; qq < cnt; ++qq) {
     if (qq == p) continue;
-    const int sq = side ? c_mech.right[r][qq] : c_mech.left[r][qq];
+    const int sq = side ? c.M->right[r][qq] : c.M->left[r][qq];
     if (sq >= 0) d = d * c.sm->z[sq];
   }
   return side ? -d : d;
@@ -213,14 +229,14 @@ __device__ void warp_analytic_matrix(WarpCell<N, R, LUT>& c, double factor) {
     double row[N];
 #pragma unroll
     for (int j = 0; j < N; ++j) row[j] = 0.0;
-    const int n = c_mech.sp_n[i];
+    const int n = c.M->sp_n[i];
     for (int u = 0; u < n; ++u) {
-      const int r = c_mech.sp_r[i][u];
-      const double sgn = c_mech.sp_sgn[i][u] > 0 ? factor : -factor;
+      const int r = c.M->sp_r[i][u];
+      const double sgn = c.M->sp_sgn[i][u] > 0 ? factor : -factor;
       for (int side = 0; side < 2; ++side) {
-        const int cnt = side ? c_mech.nr[r] : c_mech.nl[r];
+        const int cnt = side ? c.M->nr[r] : c.M->nl[r];
         for (int p = 0; p < cnt; ++p) {
-          const int sp = side ? c_mech.right[r][p] : c_mech.left[r][p];
+          const int sp = side ? c.M->right[r][p] : c.M->left[r][p];
           if (sp < 0) continue;
           const double d = sgn * rate_partial(c, r, side, p);
 #pragma unroll
@@ -242,9 +258,9 @@ __device__ double warp_jac_vec(WarpCell<N, R, LUT>& c) {
   for (int r = c.lane; r < R; r += 32) {
     double dq = 0.0;
     for (int side = 0; side < 2; ++side) {
-      const int cnt = side ? c_mech.nr[r] : c_mech.nl[r];
+      const int cnt = side ? c.M->nr[r] : c.M->nl[r];
       for (int p = 0; p < cnt; ++p) {
-        const int sp = side ? c_mech.right[r][p] : c_mech.left[r][p];
+        const int sp = side ? c.M->right[r][p] : c.M->left[r][p];
         if (sp < 0) continue;
         dq = dq + rate_partial(c, r, side, p) * c.sm->w[sp];
       }
@@ -254,10 +270,10 @@ __device__ double warp_jac_vec(WarpCell<N, R, LUT>& c) {
   __syncwarp();
   double acc = 0.0;
   if (c.lane < N) {
-    const int n = c_mech.sp_n[c.lane];
+    const int n = c.M->sp_n[c.lane];
     for (int u = 0; u < n; ++u) {
-      const double q = c.sm->q[c_mech.sp_r[c.lane][u]];
-      acc = c_mech.sp_sgn[c.lane][u] > 0 ? acc + q : acc - q;
+      const double q = c.sm->q[c.M->sp_r[c.lane][u]];
+      acc = c.M->sp_sgn[c.lane][u] > 0 ? acc + q : acc - q;
     }
   }
   return acc;
@@ -274,7 +290,8 @@ __device__ int warp_dgefa(WarpCell<N, R, LUT>& c) {
 #pragma unroll 1
   for (int k = 0; k < N - 1; ++k) {
     const double v = (i >= k && i < N) ? (double)fabs(a[i][k]) : -1.0;
-    const int l = warp_argmax(v, i, nullptr);
+    int l = warp_argmax(v, i, nullptr);
+    l = l < k ? k : (l > N - 1 ? N - 1 : l);
     piv |= (unsigned long long)l << (4 * k);
     if (a[l][k] == (LUT)0) {
       info = k + 1;
@@ -343,7 +360,7 @@ __device__ __forceinline__ void warp_ddpsc(WarpCell<N, R, LUT>& c, int ksgn) {
 
 template <int N, int R, typename LUT>
 __device__ __forceinline__ void warp_ddscl(WarpCell<N, R, LUT>& c, double rh) {
-  const double hmax = c_mech.hmax;
+  const double hmax = c.M->hmax;
   if (c.h < 1.0) {
     const double ah = fabs(c.h);
     rh = NRG_FMIN(NRG_FMIN(ah * rh, ah * c.rmax), hmax) / ah;
@@ -377,7 +394,7 @@ __device__ void warp_ddntl(WarpCell<N, R, LUT>& c) {
   const double sum = wnrm2<N>(c.s1) / sqrt((double)N);
   if (sum > c.eps / fabs(c.h)) c.h = copysign(c.eps / sum, c.h);
   c.yh[1] = c.h * c.s2;
-  c.fac = c_mech.sqrt_uround;
+  c.fac = c.M->sqrt_uround;
 }
 
 template <int N, int R, int JAC, typename LUT>
@@ -387,7 +404,7 @@ __device__ void warp_ddpst(WarpCell<N, R, LUT>& c) {
   const double el1h = EL(1, c.nq) * c.h;
   if (JAC == kJacFD) {
     const double FACMAX = 0.5, BU = 0.5;
-    const double br = c_mech.br, bl = c_mech.bl, bp = c_mech.bp, facmin = c_mech.facmin;
+    const double br = c.M->br, bl = c.M->bl, bp = c.M->bp, facmin = c.M->facmin;
 #pragma unroll 1
     for (int j = 0; j < N; ++j) {
       const double yj = __shfl_sync(kFullMask, c.y, j);
@@ -413,7 +430,8 @@ __device__ void warp_ddpst(WarpCell<N, R, LUT>& c) {
       if (c.lane < N) c.sm->a[c.lane][j] = (LUT)((f1 - c.s2) * factor);
       const double di = c.lane < N ? fabs(c.s2 - f1) : -1.0;
       double diff;
-      const int imax = warp_argmax(di, c.lane, &diff);
+      int imax = warp_argmax(di, c.lane, &diff);
+      imax = imax > N - 1 ? N - 1 : imax;
       const double s2m = fabs(__shfl_sync(kFullMask, c.s2, imax));
       const double s1m = fabs(__shfl_sync(kFullMask, f1, imax));
       if (NRG_FMIN(s2m, s1m) > 0.0) {
@@ -468,7 +486,7 @@ __device__ int warp_ddstp(WarpCell<N, R, LUT>& c) {
   const double BIAS1 = 1.3, BIAS2 = 1.2, BIAS3 = 1.4, RCTEST = 0.3, RMFAIL = 2.0, RMNORM = 10.0,
                TRSHLD = 1.0;
   const int MXFAIL = 3, MXITER = 3, MXTRY = 50, NDJSTP = 10;
-  const double uround = c_mech.uround;
+  const double uround = c.M->uround;
   const double eps = c.eps;
   const double sqn = sqrt((double)N);
   int ntry = 0, nfail = 0, iter = 0;
@@ -632,7 +650,7 @@ __device__ bool warp_cell_begin(WarpCell<N, R, LUT>& c, const StepArgs& a, long 
   }
   const double rho = a.rho[cid];
   const double yk = c.lane < N ? a.Y[c.lane * a.ld + cid] : 0.0;
-  const double ci = c.lane < N ? yk * rho / c_mech.W[c.lane] : 0.0;
+  const double ci = c.lane < N ? yk * rho / c.M->W[c.lane] : 0.0;
   double yc[N];
   wgather<N>(ci, yc);
   warp_rate_constants(c, Tc, yc);
@@ -647,9 +665,9 @@ __device__ bool warp_cell_begin(WarpCell<N, R, LUT>& c, const StepArgs& a, long 
   c.fac = 0.0;
   c.tout = a.dt;
   c.t = 0.0;
-  const double h = (c.tout - c.t) * (1.0 - 4.0 * c_mech.uround);
-  c.h = copysign(NRG_FMIN(fabs(h), c_mech.hmax), h);
-  c.eps = c_mech.eps;
+  const double h = (c.tout - c.t) * (1.0 - 4.0 * c.M->uround);
+  c.h = copysign(NRG_FMIN(fabs(h), c.M->hmax), h);
+  c.eps = c.M->eps;
   c.jtask = 0;
   c.nstep = 0;
   c.nstepl = 0;
@@ -670,10 +688,10 @@ __device__ bool warp_cell_begin(WarpCell<N, R, LUT>& c, const StepArgs& a, long 
 
 template <int N, int R, int JAC, typename LUT>
 __device__ int warp_cell_advance(WarpCell<N, R, LUT>& c, int mxstep) {
-  c.ywt = NRG_FMAX(c_mech.ewt, fabs(c.y));
+  c.ywt = NRG_FMAX(c.M->ewt, fabs(c.y));
   const double sum = NRG_FMAX(1.0, wnrm2<N>(c.y / c.ywt) / sqrt((double)N));
-  if (c.eps < sum * c_mech.uround) {
-    c.eps = sum * c_mech.uround * (1.0 + 10.0 * c_mech.uround);
+  if (c.eps < sum * c.M->uround) {
+    c.eps = sum * c.M->uround * (1.0 + 10.0 * c.M->uround);
     c.y = c.yh[0];
     return kCellOk;
   }
@@ -702,7 +720,7 @@ __device__ void warp_cell_finish(const WarpCell<N, R, LUT>& c, const StepArgs& a
   const double dt = a.dt;
   const double rho = a.rho[cid];
   const double dc = c.y - c.conc_in;
-  const double yp = c.lane < N ? dc * c_mech.W[c.lane] / dt : 0.0;
+  const double yp = c.lane < N ? dc * c.M->W[c.lane] / dt : 0.0;
   if (c.lane < N) {
     a.Y_prod[c.lane * a.ld + cid] = yp;
     a.Y_prod2[c.lane * a.ld + cid] = dc;
@@ -714,7 +732,7 @@ __device__ void warp_cell_finish(const WarpCell<N, R, LUT>& c, const StepArgs& a
 #pragma unroll
   for (int k = 0; k < N; ++k) {
     finite = finite && isfinite(dcv[k]);
-    E = E - c_mech.h_ref[k] * dcv[k] / dt;
+    E = E - c.M->h_ref[k] * dcv[k] / dt;
   }
   if (a.T_after) {
     const double y0 = c.lane < N ? a.Y[c.lane * a.ld + cid] : 0.0;
