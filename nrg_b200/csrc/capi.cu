@@ -147,11 +147,10 @@ std::string build_dev_mech(const nrg::Mechanism& m, DevMech* d) {
     for (int uu = 0; uu < u; ++uu) {
       const int k = d->upd_k[r][uu];
       if (d->sp_n[k] >= nrg::kMaxSpecUpd) return "species appears in too many reactions";
-      d->sp_r[k][d->sp_n[k]] = r;
-      d->sp_sgn[k][d->sp_n[k]] = d->upd_prod[r][uu] ? 1 : -1;
+      d->sp_list[d->sp_n[k]][k] = (r << 1) | (d->upd_prod[r][uu] ? 1 : 0);
       d->sp_n[k] += 1;
     }
-    for (int k = 0; k < N; ++k) d->eff[r][k] = m.eff[(size_t)r * N + k];
+    for (int k = 0; k < N; ++k) d->eff_t[k][r] = m.eff[(size_t)r * N + k];
   }
   for (int k = 0; k < N; ++k) {
     for (int s = 0; s < 2; ++s)

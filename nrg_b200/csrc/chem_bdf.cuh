@@ -53,6 +53,8 @@ struct SmemStore {
   static constexpr int kW = kZD + N;
   static constexpr int kDoubles = kW + N;
   static constexpr int kBytesPerThread = kDoubles * 8 + N * N * (int)sizeof(LUT);
+  using lut_t = LUT;
+  static constexpr int kBS = BS;
   double* d;
   LUT* f;
   __device__ __forceinline__ void bind(char* smem, int tid) {
@@ -67,6 +69,21 @@ struct SmemStore {
   __device__ __forceinline__ double& w(int k) { return d[(kW + k) * BS]; }
   __device__ __forceinline__ LUT& a(int j, int i) { return f[(j * N + i) * BS]; }  // A(i+1, j+1)
 };
+
+template <int N, int R, typename LUT, int BS>
+struct CellState;
+
+// Out-of-line hot routines of the thread-per-cell integrator.  They touch only
+// the cell's shared-memory arrays (passed as the two base pointers), so the
+// register-resident vectors are never forced to local memory by the call.
+template <int N, int R, typename LUT, int BS>
+__device__ __noinline__ void nl_rhs(double* d, LUT* f);
+template <int N, int R, typename LUT, int BS>
+__device__ __noinline__ void nl_analytic_matrix(double* d, LUT* f, double factor);
+template <int N, int R, typename LUT, int BS>
+__device__ __noinline__ unsigned long long nl_dgefa(double* d, LUT* f, int* info);
+template <int N, int R, typename LUT, int BS>
+__device__ __noinline__ void nl_rate_constants(double* d, LUT* f, double T);
 
 template <int N, int R, typename LUT, int BS>
 struct CellState : SmemStore<N, R, LUT, BS> {
@@ -131,6 +148,10 @@ __device__ __forceinline__ double d_cp(double T, int k) {
   cp = cp * t + a[0];
   return cp;
 }
+
+// One out-of-line copy of pow for the step-size control (called from many
+// sites; inlining each copy bloats the kernel past the instruction cache).
+static __device__ __noinline__ double npow(double x, double y) { return pow(x, y); }
 
 // x ** dnu for the integer stoichiometric change of a reaction
 __device__ __forceinline__ double int_pow(double x, double dnu) {
@@ -241,7 +262,7 @@ template <int N, int R, class CS>
 __device__ __forceinline__ void rhs_at(CS& c, const double (&v)[N], double (&out)[N]) {
 #pragma unroll
   for (int k = 0; k < N; ++k) c.z(k) = v[k];
-  rhs<N, R>(c);
+  nl_rhs<N, R, typename CS::lut_t, CS::kBS>(c.d, c.f);
 #pragma unroll
   for (int k = 0; k < N; ++k) out[k] = c.zd(k);
 }
@@ -378,7 +399,7 @@ __device__ __forceinline__ double dnrm2(const double (&dx)[N]) {
 
 // dgefa.f90:60-117 on the shared-memory matrix (column-major a(j, i) = A(i, j))
 template <int N, class CS>
-__device__ int dgefa(CS& c) {
+__device__ __forceinline__ int dgefa(CS& c, unsigned long long* piv_out) {
   using LUT = typename std::remove_reference<decltype(c.a(0, 0))>::type;
   int info = 0;
   unsigned long long piv = 0;
@@ -410,7 +431,7 @@ __device__ int dgefa(CS& c) {
     }
   }
   piv |= (unsigned long long)(N - 1) << (4 * (N - 1));
-  c.piv = piv;
+  *piv_out = piv;
   if (c.a(N - 1, N - 1) == (LUT)0) info = N;
   return info;
 }
@@ -440,6 +461,40 @@ __device__ __forceinline__ void dgesl(CS& c, double (&b)[N]) {
       for (int i = 0; i < k; ++i) b[i] = b[i] + t * (double)c.a(k, i);
     }
   }
+}
+
+template <int N, int R, typename LUT, int BS>
+__device__ __noinline__ void nl_rhs(double* d, LUT* f) {
+  SmemStore<N, R, LUT, BS> s;
+  s.d = d;
+  s.f = f;
+  rhs<N, R>(s);
+}
+
+template <int N, int R, typename LUT, int BS>
+__device__ __noinline__ void nl_analytic_matrix(double* d, LUT* f, double factor) {
+  SmemStore<N, R, LUT, BS> s;
+  s.d = d;
+  s.f = f;
+  analytic_iteration_matrix<N, R>(s, factor);
+}
+
+template <int N, int R, typename LUT, int BS>
+__device__ __noinline__ unsigned long long nl_dgefa(double* d, LUT* f, int* info) {
+  SmemStore<N, R, LUT, BS> s;
+  s.d = d;
+  s.f = f;
+  unsigned long long piv = 0;
+  *info = dgefa<N>(s, &piv);
+  return piv;
+}
+
+template <int N, int R, typename LUT, int BS>
+__device__ __noinline__ void nl_rate_constants(double* d, LUT* f, double T) {
+  SmemStore<N, R, LUT, BS> s;
+  s.d = d;
+  s.f = f;
+  rate_constants<N, R>(s, T);
 }
 
 // --------------------------------------------------------- SLATEC pieces
@@ -533,7 +588,7 @@ __device__ void ddpst(CS& c) {
       dy = (c.nq == 1) ? copysign(dy, sel(c.s2, j)) : copysign(dy, c.yh(2, j));
       dy = (yj + dy) - yj;
       c.z(j) = yj + dy;
-      rhs<N, R>(c);
+      nl_rhs<N, R, typename CS::lut_t, CS::kBS>(c.d, c.f);
       c.z(j) = yj;
       const double factor = -(el1h / dy);
       double diff = -1.0, s2m = 0.0, s1m = 0.0;
@@ -558,9 +613,10 @@ __device__ void ddpst(CS& c) {
   } else {
 #pragma unroll
     for (int k = 0; k < N; ++k) c.z(k) = c.y[k];
-    analytic_iteration_matrix<N, R>(c, -el1h);
+    nl_analytic_matrix<N, R, typename CS::lut_t, CS::kBS>(c.d, c.f, -el1h);
   }
-  const int info = dgefa<N>(c);
+  int info = 0;
+  c.piv = nl_dgefa<N, R, typename CS::lut_t, CS::kBS>(c.d, c.f, &info);
   if (info != 0) c.ier = 1;
 }
 
@@ -664,7 +720,7 @@ L160:
   ddpsc<N>(-1, c);
   c.nwait = c.nq + 2;
   if (c.jtask != 0 && c.jtask != 2) c.rmax = RMFAIL;
-  rh = (iter == 0) ? 0.3 : 0.9 * pow(eps / ctest, 0.2);
+  rh = (iter == 0) ? 0.3 : 0.9 * npow(eps / ctest, 0.2);
   if (rh * c.h == 0.0) goto L400;
   ddscl<N>(c, rh);
   goto L100;
@@ -679,12 +735,12 @@ L170:
     nfail = nfail + 1;
     if (nfail < MXFAIL || c.nq == 1) {
       if (c.jtask != 0 && c.jtask != 2) c.rmax = RMFAIL;
-      const double rh2 = 1.0 / (BIAS2 * pow(etest / eps, 1.0 / (double)(c.nq + 1)));
+      const double rh2 = 1.0 / (BIAS2 * npow(etest / eps, 1.0 / (double)(c.nq + 1)));
       if (c.nq > 1) {
 #pragma unroll
         for (int i = 0; i < N; ++i) c.s2[i] = c.yh(c.nq, i) / NRG_FMAX(fabs(c.y[i]), c.ywt[i]);
         const double erdn = dnrm2<N>(c.s2) / (TQ(1, c.nq) * sqn);
-        const double rh1 = 1.0 / NRG_FMAX(1.0, BIAS1 * pow(erdn / eps, 1.0 / (double)c.nq));
+        const double rh1 = 1.0 / NRG_FMAX(1.0, BIAS1 * npow(erdn / eps, 1.0 / (double)c.nq));
         if (rh2 < rh1) {
           c.nq = c.nq - 1;
           c.rc = c.rc * EL(1, c.nq) / EL(1, c.nq + 1);
@@ -719,7 +775,7 @@ L170:
 #pragma unroll
   for (int i = 0; i < N; ++i) c.y[i] = c.yh(0, i);
   if (c.jtask == 0 || c.jtask == 2) {
-    rh = 1.0 / NRG_FMAX(uround, BIAS2 * pow(etest / eps, 1.0 / (double)(c.nq + 1)));
+    rh = 1.0 / NRG_FMAX(uround, BIAS2 * npow(etest / eps, 1.0 / (double)(c.nq + 1)));
     if (rh > TRSHLD) ddscl<N>(c, rh);
   } else if (c.nwait > 1) {
     c.nwait = c.nwait - 1;
@@ -735,9 +791,9 @@ L170:
 #pragma unroll
       for (int i = 0; i < N; ++i) c.s2[i] = c.yh(c.nq, i) / NRG_FMAX(fabs(c.y[i]), c.ywt[i]);
       const double erdn = dnrm2<N>(c.s2) / (TQ(1, c.nq) * sqn);
-      rh1 = 1.0 / NRG_FMAX(uround, BIAS1 * pow(erdn / eps, 1.0 / (double)c.nq));
+      rh1 = 1.0 / NRG_FMAX(uround, BIAS1 * npow(erdn / eps, 1.0 / (double)c.nq));
     }
-    rh2 = 1.0 / NRG_FMAX(uround, BIAS2 * pow(etest / eps, 1.0 / (double)(c.nq + 1)));
+    rh2 = 1.0 / NRG_FMAX(uround, BIAS2 * npow(etest / eps, 1.0 / (double)(c.nq + 1)));
     if (c.nq == kMaxOrd) {
       rh3 = 0.0;
     } else {
@@ -745,7 +801,7 @@ L170:
       for (int i = 0; i < N; ++i)
         c.s2[i] = (c.s1[i] - c.yh(kMaxOrd, i)) / NRG_FMAX(fabs(c.y[i]), c.ywt[i]);
       const double erup = dnrm2<N>(c.s2) / (TQ(3, c.nq) * sqn);
-      rh3 = 1.0 / NRG_FMAX(uround, BIAS3 * pow(erup / eps, 1.0 / (double)(c.nq + 2)));
+      rh3 = 1.0 / NRG_FMAX(uround, BIAS3 * npow(erup / eps, 1.0 / (double)(c.nq + 2)));
     }
     if (rh1 > rh2 && rh1 >= rh3) {
       rh = rh1;
@@ -803,10 +859,10 @@ __device__ bool cell_begin(CS& c, const StepArgs& a, long cid) {
   for (int r = 0; r < R; ++r) {
     double s = 0.0;
 #pragma unroll
-    for (int k = 0; k < N; ++k) s = s + yk[k] * rho / c_mech.W[k] * c_mech.eff[r][k];
+    for (int k = 0; k < N; ++k) s = s + yk[k] * rho / c_mech.W[k] * c_mech.eff_t[k][r];
     c.kr(r) = s;  // third-body sum, consumed by rate_constants
   }
-  rate_constants<N, R>(c, Tc);
+  nl_rate_constants<N, R, typename CS::lut_t, CS::kBS>(c.d, c.f, Tc);
 #pragma unroll
   for (int k = 0; k < N; ++k) {
     const double ci = yk[k] * rho / c_mech.W[k];

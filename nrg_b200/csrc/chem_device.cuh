@@ -32,7 +32,7 @@ struct DevMech {
   double A_low[kMaxReactions], beta_low[kMaxReactions], E_low[kMaxReactions];
   double troe[kMaxReactions][4];
   double dnu[kMaxReactions];
-  double eff[kMaxReactions][kMaxSpecies];
+  double eff_t[kMaxSpecies][kMaxReactions];  // third-body efficiency, species-major
   double a[kMaxSpecies][2][7];  // NASA-7 times R
   double W[kMaxSpecies];
   double invW[kMaxSpecies];
@@ -41,11 +41,11 @@ struct DevMech {
   double el[13 * 12], tq[3 * 12];
   double eps, ewt, hmax, uround;
   double sqrt_uround, br, bl, bp, facmin;
-  // per-species update lists in reaction order: reaction index and sign of
-  // the net rate (+1 product occurrence, -1 reactant occurrence)
+  // per-species update lists in reaction order, entry-major so that lanes
+  // owning consecutive species read consecutive words: (r << 1) | 1 for a
+  // product occurrence of species k in reaction r, (r << 1) for a reactant one
   int sp_n[kMaxSpecies];
-  int sp_r[kMaxSpecies][kMaxSpecUpd];
-  int sp_sgn[kMaxSpecies][kMaxSpecUpd];
+  int sp_list[kMaxSpecUpd][kMaxSpecies];
   // element composition for conservation checks (H, O, N) in atoms/molecule
   double elem[3][kMaxSpecies];
 };

@@ -33,11 +33,17 @@ struct WarpSmem {
   LUT a[N][N];      // iteration matrix, row-major: a[i][j] = A(i+1, j+1)
 };
 
+// What the out-of-line warp routines need: passed by value, so calling them
+// never forces the register-resident cell state to local memory.
 template <int N, int R, typename LUT>
-struct WarpCell {
+struct WarpCtx {
   const DevMech* M;  // block-shared copy of the mechanism tables
   WarpSmem<N, R, LUT>* sm;
   int lane;
+};
+
+template <int N, int R, typename LUT>
+struct WarpCell : WarpCtx<N, R, LUT> {
   double yh[kMaxOrd + 1];  // Nordsieck row `lane`
   double y, ywt, s1, s2, fac, conc_in;
   double h, t, tout, rc, rmax, trend, eps;  // warp-uniform
@@ -96,8 +102,10 @@ __device__ __forceinline__ int warp_argmax(double v, int idx, double* vmax) {
 // Rate constants of the reactions owned by this lane (calculate_rate_constants,
 // chemical_kinetics_solver.f90:360-493); third-body concentration folded in.
 template <int N, int R, typename LUT>
-__device__ void warp_rate_constants(WarpCell<N, R, LUT>& c, double Tin, const double (&yc)[N]) {
+__device__ __noinline__ void warp_rate_constants(const WarpCtx<N, R, LUT> c, double Tin, double ci) {
   const double RG = 8.31446261815324, PATM = 101325.0;
+  double yc[N];
+  wgather<N>(ci, yc);
   const double T = NRG_FMIN(Tin, 10000.0);
   if (c.lane < N) {
     const double logt = log(NRG_FMIN(T, 6000.0));
@@ -121,7 +129,7 @@ __device__ void warp_rate_constants(WarpCell<N, R, LUT>& c, double Tin, const do
   for (int r = c.lane; r < R; r += 32) {
     double mc = 0.0;
 #pragma unroll
-    for (int k = 0; k < N; ++k) mc = mc + yc[k] * c.M->eff[r][k];
+    for (int k = 0; k < N; ++k) mc = mc + yc[k] * c.M->eff_t[k][r];
     double d_s = 0.0, d_h = 0.0;
     bool m_left = false, m_right = false;
     for (int i = 0; i < c.M->nr[r]; ++i) {
@@ -176,7 +184,7 @@ __device__ void warp_rate_constants(WarpCell<N, R, LUT>& c, double Tin, const do
 // chemical_kinetics_solver.f90:495-540), summed per species in reaction
 // order from the net rates.
 template <int N, int R, typename LUT>
-__device__ __forceinline__ double warp_rhs(WarpCell<N, R, LUT>& c, double x) {
+__device__ __noinline__ double warp_rhs(const WarpCtx<N, R, LUT> c, double x) {
   __syncwarp();
   if (c.lane < N) c.sm->z[c.lane] = x;
   __syncwarp();
@@ -198,8 +206,9 @@ __device__ __forceinline__ double warp_rhs(WarpCell<N, R, LUT>& c, double x) {
   if (c.lane < N) {
     const int n = c.M->sp_n[c.lane];
     for (int u = 0; u < n; ++u) {
-      const double q = c.sm->q[c.M->sp_r[c.lane][u]];
-      acc = c.M->sp_sgn[c.lane][u] > 0 ? acc + q : acc - q;
+      const int e = c.M->sp_list[u][c.lane];
+      const double q = c.sm->q[e >> 1];
+      acc = (e & 1) ? acc + q : acc - q;
     }
   }
   return acc;
@@ -207,7 +216,7 @@ __device__ __forceinline__ double warp_rhs(WarpCell<N, R, LUT>& c, double x) {
 
 // d(net rate of reaction r)/dz_sp for factor position p on one side, at z.
 template <int N, int R, typename LUT>
-__device__ __forceinline__ double rate_partial(const WarpCell<N, R, LUT>& c, int r, int side, int p) {
+__device__ __forceinline__ double rate_partial(const WarpCtx<N, R, LUT>& c, int r, int side, int p) {
   const int cnt = side ? c.M->nr[r] : c.M->nl[r];
   double d = side ? c.sm->kr[r] : c.sm->kf[r];
   for (int qq = 0; qq < cnt; ++qq) {
@@ -220,9 +229,9 @@ __device__ __forceinline__ double rate_partial(const WarpCell<N, R, LUT>& c, int
 
 // Row `lane` of I + factor * J (J = dZdot/dZ, analytic) into the shared matrix.
 template <int N, int R, typename LUT>
-__device__ void warp_analytic_matrix(WarpCell<N, R, LUT>& c, double factor) {
+__device__ __noinline__ void warp_analytic_matrix(const WarpCtx<N, R, LUT> c, double y, double factor) {
   __syncwarp();
-  if (c.lane < N) c.sm->z[c.lane] = c.y;
+  if (c.lane < N) c.sm->z[c.lane] = y;
   __syncwarp();
   if (c.lane < N) {
     const int i = c.lane;
@@ -231,8 +240,9 @@ __device__ void warp_analytic_matrix(WarpCell<N, R, LUT>& c, double factor) {
     for (int j = 0; j < N; ++j) row[j] = 0.0;
     const int n = c.M->sp_n[i];
     for (int u = 0; u < n; ++u) {
-      const int r = c.M->sp_r[i][u];
-      const double sgn = c.M->sp_sgn[i][u] > 0 ? factor : -factor;
+      const int e = c.M->sp_list[u][i];
+      const int r = e >> 1;
+      const double sgn = (e & 1) ? factor : -factor;
       for (int side = 0; side < 2; ++side) {
         const int cnt = side ? c.M->nr[r] : c.M->nl[r];
         for (int p = 0; p < cnt; ++p) {
@@ -253,7 +263,7 @@ __device__ void warp_analytic_matrix(WarpCell<N, R, LUT>& c, double factor) {
 
 // (J v)_lane with v in sm->w and the state in sm->z (mixed-mode residual).
 template <int N, int R, typename LUT>
-__device__ double warp_jac_vec(WarpCell<N, R, LUT>& c) {
+__device__ __noinline__ double warp_jac_vec(const WarpCtx<N, R, LUT> c) {
   __syncwarp();
   for (int r = c.lane; r < R; r += 32) {
     double dq = 0.0;
@@ -272,8 +282,9 @@ __device__ double warp_jac_vec(WarpCell<N, R, LUT>& c) {
   if (c.lane < N) {
     const int n = c.M->sp_n[c.lane];
     for (int u = 0; u < n; ++u) {
-      const double q = c.sm->q[c.M->sp_r[c.lane][u]];
-      acc = c.M->sp_sgn[c.lane][u] > 0 ? acc + q : acc - q;
+      const int e = c.M->sp_list[u][c.lane];
+      const double q = c.sm->q[e >> 1];
+      acc = (e & 1) ? acc + q : acc - q;
     }
   }
   return acc;
@@ -281,7 +292,7 @@ __device__ double warp_jac_vec(WarpCell<N, R, LUT>& c) {
 
 // dgefa.f90:60-117 on the shared row-major matrix, rows spread over lanes.
 template <int N, int R, typename LUT>
-__device__ int warp_dgefa(WarpCell<N, R, LUT>& c) {
+__device__ __noinline__ unsigned long long warp_dgefa(const WarpCtx<N, R, LUT> c, int* info_out) {
   int info = 0;
   unsigned long long piv = 0;
   const int i = c.lane;
@@ -317,9 +328,9 @@ __device__ int warp_dgefa(WarpCell<N, R, LUT>& c) {
     __syncwarp();
   }
   piv |= (unsigned long long)(N - 1) << (4 * (N - 1));
-  c.piv = piv;
   if (a[N - 1][N - 1] == (LUT)0) info = N;
-  return info;
+  *info_out = info;
+  return piv;
 }
 
 // dgesl.f90:71-131 (JOB = 0) on a lane-distributed right-hand side.
@@ -388,7 +399,7 @@ __device__ void warp_ddntl(WarpCell<N, R, LUT>& c) {
   c.trend = 1.0;
   c.nq = 1;
   c.nwait = 3;
-  c.s2 = warp_rhs(c, c.y);
+  c.s2 = warp_rhs<N, R, LUT>(c, c.y);
   c.nfe += 1;
   c.s1 = c.s2 / NRG_FMAX(1.0, c.ywt);
   const double sum = wnrm2<N>(c.s1) / sqrt((double)N);
@@ -425,7 +436,7 @@ __device__ void warp_ddpst(WarpCell<N, R, LUT>& c) {
       }
       dy = copysign(dy, sg);
       dy = (yj + dy) - yj;
-      const double f1 = warp_rhs(c, c.lane == j ? yj + dy : c.y);
+      const double f1 = warp_rhs<N, R, LUT>(c, c.lane == j ? yj + dy : c.y);
       const double factor = -(el1h / dy);
       if (c.lane < N) c.sm->a[c.lane][j] = (LUT)((f1 - c.s2) * factor);
       const double di = c.lane < N ? fabs(c.s2 - f1) : -1.0;
@@ -447,9 +458,10 @@ __device__ void warp_ddpst(WarpCell<N, R, LUT>& c) {
     if (c.lane < N) c.sm->a[c.lane][c.lane] += (LUT)1;
     __syncwarp();
   } else {
-    warp_analytic_matrix(c, -el1h);
+    warp_analytic_matrix<N, R, LUT>(c, c.y, -el1h);
   }
-  const int info = warp_dgefa(c);
+  int info = 0;
+  c.piv = warp_dgefa<N, R, LUT>(c, &info);
   if (info != 0) c.ier = 1;
 }
 
@@ -464,7 +476,7 @@ __device__ double warp_ddcor(WarpCell<N, R, LUT>& c) {
       c.sm->z[c.lane] = c.y;
       c.sm->w[c.lane] = x;
     }
-    const double jx = warp_jac_vec(c);
+    const double jx = warp_jac_vec<N, R, LUT>(c);
     const double r = b - (x - el1h * jx);
     x = x + warp_dgesl(c, r);
     c.nsolve += 1;
@@ -506,7 +518,7 @@ L100:
 L110:
   iter = 0;
   c.y = c.yh[0];
-  c.s2 = warp_rhs(c, c.y);
+  c.s2 = warp_rhs<N, R, LUT>(c, c.y);
   c.nfe += 1;
   if (evaljc || c.ier) {
     warp_ddpst<N, R, JAC>(c);
@@ -525,7 +537,7 @@ L130:
   iter = iter + 1;
   if (iter < MXITER) {
     c.y = c.yh[0] + EL(1, c.nq) * c.s1;
-    c.s2 = warp_rhs(c, c.y);
+    c.s2 = warp_rhs<N, R, LUT>(c, c.y);
     c.nfe += 1;
     goto L130;
   }
@@ -538,7 +550,7 @@ L160:
   warp_ddpsc(c, -1);
   c.nwait = c.nq + 2;
   if (c.jtask != 0 && c.jtask != 2) c.rmax = RMFAIL;
-  rh = (iter == 0) ? 0.3 : 0.9 * pow(eps / ctest, 0.2);
+  rh = (iter == 0) ? 0.3 : 0.9 * npow(eps / ctest, 0.2);
   if (rh * c.h == 0.0) goto L400;
   warp_ddscl(c, rh);
   goto L100;
@@ -551,10 +563,10 @@ L170:
     nfail = nfail + 1;
     if (nfail < MXFAIL || c.nq == 1) {
       if (c.jtask != 0 && c.jtask != 2) c.rmax = RMFAIL;
-      const double rh2 = 1.0 / (BIAS2 * pow(etest / eps, 1.0 / (double)(c.nq + 1)));
+      const double rh2 = 1.0 / (BIAS2 * npow(etest / eps, 1.0 / (double)(c.nq + 1)));
       if (c.nq > 1) {
         const double erdn = wnorm(c, yh_get(c.yh, c.nq)) / (TQ(1, c.nq) * sqn);
-        const double rh1 = 1.0 / NRG_FMAX(1.0, BIAS1 * pow(erdn / eps, 1.0 / (double)c.nq));
+        const double rh1 = 1.0 / NRG_FMAX(1.0, BIAS1 * npow(erdn / eps, 1.0 / (double)c.nq));
         if (rh2 < rh1) {
           c.nq = c.nq - 1;
           c.rc = c.rc * EL(1, c.nq) / EL(1, c.nq + 1);
@@ -585,7 +597,7 @@ L170:
     if (j <= c.nq) c.yh[j] = c.yh[j] + EL(j + 1, c.nq) * c.s1;
   c.y = c.yh[0];
   if (c.jtask == 0 || c.jtask == 2) {
-    rh = 1.0 / NRG_FMAX(uround, BIAS2 * pow(etest / eps, 1.0 / (double)(c.nq + 1)));
+    rh = 1.0 / NRG_FMAX(uround, BIAS2 * npow(etest / eps, 1.0 / (double)(c.nq + 1)));
     if (rh > TRSHLD) warp_ddscl(c, rh);
   } else if (c.nwait > 1) {
     c.nwait = c.nwait - 1;
@@ -596,14 +608,14 @@ L170:
       rh1 = 0.0;
     } else {
       const double erdn = wnorm(c, yh_get(c.yh, c.nq)) / (TQ(1, c.nq) * sqn);
-      rh1 = 1.0 / NRG_FMAX(uround, BIAS1 * pow(erdn / eps, 1.0 / (double)c.nq));
+      rh1 = 1.0 / NRG_FMAX(uround, BIAS1 * npow(erdn / eps, 1.0 / (double)c.nq));
     }
-    rh2 = 1.0 / NRG_FMAX(uround, BIAS2 * pow(etest / eps, 1.0 / (double)(c.nq + 1)));
+    rh2 = 1.0 / NRG_FMAX(uround, BIAS2 * npow(etest / eps, 1.0 / (double)(c.nq + 1)));
     if (c.nq == kMaxOrd) {
       rh3 = 0.0;
     } else {
       const double erup = wnorm(c, c.s1 - c.yh[kMaxOrd]) / (TQ(3, c.nq) * sqn);
-      rh3 = 1.0 / NRG_FMAX(uround, BIAS3 * pow(erup / eps, 1.0 / (double)(c.nq + 2)));
+      rh3 = 1.0 / NRG_FMAX(uround, BIAS3 * npow(erup / eps, 1.0 / (double)(c.nq + 2)));
     }
     if (rh1 > rh2 && rh1 >= rh3) {
       rh = rh1;
@@ -651,9 +663,7 @@ __device__ bool warp_cell_begin(WarpCell<N, R, LUT>& c, const StepArgs& a, long 
   const double rho = a.rho[cid];
   const double yk = c.lane < N ? a.Y[c.lane * a.ld + cid] : 0.0;
   const double ci = c.lane < N ? yk * rho / c.M->W[c.lane] : 0.0;
-  double yc[N];
-  wgather<N>(ci, yc);
-  warp_rate_constants(c, Tc, yc);
+  warp_rate_constants<N, R, LUT>(c, Tc, ci);
   c.conc_in = ci;
   c.y = ci;
 #pragma unroll
