@@ -161,6 +161,48 @@ NRG_API int nrg_mech_tables(const char* mechanism_path, const char* thermo_path,
  * nrg_chem_create when h is NULL). */
 NRG_API const char* nrg_chem_last_error(nrg_chem* h);
 
+/* ---- Gated surrogate (no counterpart in the reference: NRG has no learned
+ * chemistry).  A BF16 MLP predicts the per-cell increment (dY_1..dY_9, dT)
+ * from (T, log p, Y_1..Y_9, log10 dt); cells outside the training hull, or
+ * whose prediction fails the element-conservation or temperature check, are
+ * integrated by the FP64 kernel.  x_bf16 arrays hold n x 16 bf16 standardised
+ * features, y arrays n x 10 fp32 standardised targets (device memory). */
+NRG_API int nrg_surrogate_param_count(void);
+NRG_API int nrg_surrogate_norm_count(void);
+NRG_API int nrg_surrogate_init(nrg_chem* h, unsigned long long seed);
+NRG_API int nrg_surrogate_get_params(nrg_chem* h, float* params);
+NRG_API int nrg_surrogate_set_params(nrg_chem* h, const float* params);
+NRG_API int nrg_surrogate_get_norm(nrg_chem* h, float* norm);
+NRG_API int nrg_surrogate_set_norm(nrg_chem* h, const float* norm);
+/* Training arrays from integrated states (Y_prod, T_after from
+ * nrg_chem_integrate with the same dt / dt_cells); also fits the feature and
+ * target scaling and the training hull (widened by hull_margin of each range). */
+NRG_API int nrg_surrogate_prepare(nrg_chem* h, long n, long ld, double dt, const double* dt_cells,
+                                  const double* T, const double* rho, const double* Y, const double* Y_prod,
+                                  const double* T_after, float hull_margin, void* x_bf16, float* y);
+NRG_API int nrg_surrogate_features(nrg_chem* h, long n, long ld, double dt, const double* dt_cells,
+                                   const double* T, const double* rho, const double* Y, float* xraw,
+                                   void* x_bf16);
+NRG_API int nrg_surrogate_forward(nrg_chem* h, long n, const void* x_bf16, float* out);
+/* Mean-squared-error gradient over n rows into host memory (no update). */
+NRG_API int nrg_surrogate_grad(nrg_chem* h, long n, const void* x_bf16, const float* y, float* grads_host,
+                               double* loss_host);
+NRG_API int nrg_surrogate_train(nrg_chem* h, long n, const void* x_bf16, const float* y, int epochs, int batch,
+                                float lr, unsigned long long seed, float* loss_per_epoch);
+/* Gate: element residual bound (element mass fraction), bound on the gap
+ * between the network's dT and the energy closure of its dY (K), |dT| bound (K). */
+NRG_API int nrg_surrogate_set_gate(nrg_chem* h, double elem_tol, double dT_tol, double dT_max);
+NRG_API int nrg_surrogate_enable(nrg_chem* h, int enable);
+NRG_API int nrg_surrogate_save(nrg_chem* h, const char* path);
+NRG_API int nrg_surrogate_load(nrg_chem* h, const char* path);
+
+/* FP64 integration with an optional per-cell step dt_cells (device, n
+ * entries); never uses the surrogate.  Same layout as nrg_chem_step_device. */
+NRG_API int nrg_chem_integrate(nrg_chem* h, long n, long ld, double dt, const double* dt_cells,
+                               const double* T, const double* rho, const double* Y, const signed char* bc,
+                               double* Y_prod, double* Y_prod2, double* E_f_prod, double* T_after,
+                               unsigned char* status, void* stream, nrg_chem_stats* stats);
+
 /* Measured dependent-FMA FP64 throughput of the current device, TFLOP/s. */
 NRG_API int nrg_fp64_peak_tflops(double* tflops);
 

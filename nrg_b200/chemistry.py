@@ -79,6 +79,24 @@ SIGNATURES = {
     "nrg_chem_species_name": (_I, [_VP, _I, ctypes.c_char_p, _I]),
     "nrg_mech_tables": (_I, [_CP, _CP, _CP, _D, _I, ctypes.POINTER(_I), ctypes.POINTER(_I)] + [_VP] * 7),
     "nrg_chem_last_error": (ctypes.c_char_p, [_VP]),
+    "nrg_surrogate_param_count": (_I, []),
+    "nrg_surrogate_norm_count": (_I, []),
+    "nrg_surrogate_init": (_I, [_VP, ctypes.c_ulonglong]),
+    "nrg_surrogate_get_params": (_I, [_VP, _VP]),
+    "nrg_surrogate_set_params": (_I, [_VP, _VP]),
+    "nrg_surrogate_get_norm": (_I, [_VP, _VP]),
+    "nrg_surrogate_set_norm": (_I, [_VP, _VP]),
+    "nrg_surrogate_prepare": (_I, [_VP, _L, _L, _D, _VP, _VP, _VP, _VP, _VP, _VP, ctypes.c_float, _VP, _VP]),
+    "nrg_surrogate_features": (_I, [_VP, _L, _L, _D, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "nrg_surrogate_forward": (_I, [_VP, _L, _VP, _VP]),
+    "nrg_surrogate_grad": (_I, [_VP, _L, _VP, _VP, _VP, ctypes.POINTER(_D)]),
+    "nrg_surrogate_train": (_I, [_VP, _L, _VP, _VP, _I, _I, ctypes.c_float, ctypes.c_ulonglong, _VP]),
+    "nrg_surrogate_set_gate": (_I, [_VP, _D, _D, _D]),
+    "nrg_surrogate_enable": (_I, [_VP, _I]),
+    "nrg_surrogate_save": (_I, [_VP, _CP]),
+    "nrg_surrogate_load": (_I, [_VP, _CP]),
+    "nrg_chem_integrate": (_I, [_VP, _L, _L, _D, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP,
+                                ctypes.POINTER(Stats)]),
     "nrg_fp64_peak_tflops": (_I, [ctypes.POINTER(_D)]),
 }
 
@@ -289,6 +307,18 @@ class ChemicalKineticsSolver:
         _check(lib().nrg_chem_step_device(
             self._h, float(time_step), n, ld, _ptr(T), _ptr(rho), _ptr(Y), _ptr(bc), _ptr(Y_prod),
             _ptr(Y_prod2), _ptr(E_f_prod), _ptr(T_after), _ptr(status),
+            ctypes.c_void_p(stream) if stream else None, ctypes.byref(st)), self._h)
+        return st.as_dict()
+
+    def integrate(self, dt, T, rho, Y, Y_prod, Y_prod2, E_f_prod, dt_cells=None, bc=None, T_after=None,
+                  status=None) -> dict:
+        """FP64 integration (never the surrogate) with an optional per-cell dt."""
+        import torch
+        st = Stats()
+        stream = torch.cuda.current_stream(T.device).cuda_stream
+        _check(lib().nrg_chem_integrate(
+            self._h, T.numel(), Y.shape[1], float(dt), _ptr(dt_cells), _ptr(T), _ptr(rho), _ptr(Y), _ptr(bc),
+            _ptr(Y_prod), _ptr(Y_prod2), _ptr(E_f_prod), _ptr(T_after), _ptr(status),
             ctypes.c_void_p(stream) if stream else None, ctypes.byref(st)), self._h)
         return st.as_dict()
 

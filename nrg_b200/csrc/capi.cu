@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdio>
 #include <cfloat>
 #include <cmath>
 #include <cstring>
@@ -425,6 +426,10 @@ extern "C" int nrg_chem_step_device(nrg_chem* h, double time_step, long n, long 
   a.status = status;
   a.mxstep = 10000;
   a.mech = h->d_mech;
+  a.dt_cells = nullptr;
+  a.cell_list = nullptr;
+  a.n_list = 0;
+  a.n_list_dev = nullptr;
   if (n == 0) {
     if (stats) std::memset(stats, 0, sizeof(*stats));
     return NRG_OK;
@@ -490,6 +495,10 @@ extern "C" int nrg_chem_step(nrg_chem* h, double time_step, const nrg_field_desc
   a.status = h->d_status;
   a.mxstep = 10000;
   a.mech = h->d_mech;
+  a.dt_cells = nullptr;
+  a.cell_list = nullptr;
+  a.n_list = 0;
+  a.n_list_dev = nullptr;
   if (!(time_step > 0.0)) return fail(h, NRG_ERR_ARG, "time_step must be > 0");
   rc = run_step(h, a, s, stats);
   if (rc) return rc;
@@ -525,6 +534,10 @@ extern "C" int nrg_chem_autotune(nrg_chem* h, double time_step, long n, long ld,
   a.Y_prod = Y_prod; a.Y_prod2 = Y_prod2; a.E_f_prod = E_f_prod; a.T_after = nullptr; a.status = nullptr;
   a.mxstep = 10000;
   a.mech = h->d_mech;
+  a.dt_cells = nullptr;
+  a.cell_list = nullptr;
+  a.n_list = 0;
+  a.n_list_dev = nullptr;
   std::vector<LaunchCfg> cands;
   for (int block : {128, 256})
     for (int per_sm : {0, 1, 2, 4})
@@ -662,4 +675,198 @@ extern "C" int nrg_fp64_peak_tflops(double* tflops) {
   const double flops = 2.0 * 8 * 16 * (double)iters * blocks * threads;
   *tflops = flops / (ms * 1e-3) / 1e12;
   return NRG_OK;
+}
+
+// ------------------------------------------------------------- surrogate
+namespace {
+int order_after_legacy(nrg_chem* h) {
+  CK(h, cudaEventRecord(h->ev_in, (cudaStream_t)0));
+  CK(h, cudaStreamWaitEvent(h->stream, h->ev_in, 0));
+  return NRG_OK;
+}
+int sfail(nrg_chem* h, const std::string& e) { return e.empty() ? NRG_OK : fail(h, NRG_ERR_CUDA, e); }
+constexpr int kNormFloats = 4 * nrg::kMlpIn + nrg::kMlpOut + 1;
+void norm_to_floats(const nrg::MlpNorm& m, float* f) {
+  int k = 0;
+  for (int j = 0; j < nrg::kMlpIn; ++j) f[k++] = m.x_mu[j];
+  for (int j = 0; j < nrg::kMlpIn; ++j) f[k++] = m.x_sd[j];
+  for (int j = 0; j < nrg::kMlpIn; ++j) f[k++] = m.x_min[j];
+  for (int j = 0; j < nrg::kMlpIn; ++j) f[k++] = m.x_max[j];
+  for (int j = 0; j < nrg::kMlpOut; ++j) f[k++] = m.y_sd[j];
+  f[k++] = m.hull_margin;
+}
+nrg::MlpNorm floats_to_norm(const float* f) {
+  nrg::MlpNorm m{};
+  int k = 0;
+  for (int j = 0; j < nrg::kMlpIn; ++j) m.x_mu[j] = f[k++];
+  for (int j = 0; j < nrg::kMlpIn; ++j) m.x_sd[j] = f[k++];
+  for (int j = 0; j < nrg::kMlpIn; ++j) m.x_min[j] = f[k++];
+  for (int j = 0; j < nrg::kMlpIn; ++j) m.x_max[j] = f[k++];
+  for (int j = 0; j < nrg::kMlpOut; ++j) m.y_sd[j] = f[k++];
+  m.hull_margin = f[k++];
+  return m;
+}
+}  // namespace
+
+extern "C" int nrg_surrogate_param_count(void) { return nrg::surrogate_param_count(); }
+extern "C" int nrg_surrogate_norm_count(void) { return kNormFloats; }
+
+extern "C" int nrg_surrogate_init(nrg_chem* h, unsigned long long seed) {
+  if (!h) return NRG_ERR_ARG;
+  CK(h, cudaSetDevice(h->device));
+  return sfail(h, nrg::surrogate_init(h->sur, seed, h->stream));
+}
+
+extern "C" int nrg_surrogate_get_params(nrg_chem* h, float* params) {
+  if (!h || !params) return NRG_ERR_ARG;
+  return sfail(h, nrg::surrogate_get_params(h->sur, params, h->stream));
+}
+
+extern "C" int nrg_surrogate_set_params(nrg_chem* h, const float* params) {
+  if (!h || !params) return NRG_ERR_ARG;
+  return sfail(h, nrg::surrogate_set_params(h->sur, params, h->stream));
+}
+
+extern "C" int nrg_surrogate_get_norm(nrg_chem* h, float* norm) {
+  if (!h || !norm) return NRG_ERR_ARG;
+  norm_to_floats(nrg::surrogate_get_norm(h->sur), norm);
+  return NRG_OK;
+}
+
+extern "C" int nrg_surrogate_set_norm(nrg_chem* h, const float* norm) {
+  if (!h || !norm) return NRG_ERR_ARG;
+  return sfail(h, nrg::surrogate_set_norm(h->sur, floats_to_norm(norm)));
+}
+
+extern "C" int nrg_surrogate_prepare(nrg_chem* h, long n, long ld, double dt, const double* dt_cells,
+                                     const double* T, const double* rho, const double* Y, const double* Y_prod,
+                                     const double* T_after, float hull_margin, void* x_bf16, float* y) {
+  if (!h || n <= 0 || ld < n || !T || !rho || !Y || !Y_prod || !T_after || !x_bf16 || !y)
+    return fail(h, NRG_ERR_ARG, "bad arguments to nrg_surrogate_prepare");
+  CK(h, cudaSetDevice(h->device));
+  int rc = order_after_legacy(h);
+  if (rc) return rc;
+  return sfail(h, nrg::surrogate_prepare(h->sur, n, ld, dt, dt_cells, T, rho, Y, Y_prod, T_after, hull_margin,
+                                         (__nv_bfloat16*)x_bf16, y, h->stream));
+}
+
+extern "C" int nrg_surrogate_features(nrg_chem* h, long n, long ld, double dt, const double* dt_cells,
+                                      const double* T, const double* rho, const double* Y, float* xraw,
+                                      void* x_bf16) {
+  if (!h || n < 0 || ld < n || (n > 0 && (!T || !rho || !Y))) return fail(h, NRG_ERR_ARG, "bad features args");
+  CK(h, cudaSetDevice(h->device));
+  int rc = order_after_legacy(h);
+  if (rc) return rc;
+  std::string e = nrg::surrogate_features(h->sur, n, ld, dt, dt_cells, T, rho, Y, xraw, (__nv_bfloat16*)x_bf16,
+                                          h->stream);
+  if (!e.empty()) return sfail(h, e);
+  CK(h, cudaStreamSynchronize(h->stream));
+  return NRG_OK;
+}
+
+extern "C" int nrg_surrogate_forward(nrg_chem* h, long n, const void* x_bf16, float* out) {
+  if (!h || n <= 0 || !x_bf16 || !out) return fail(h, NRG_ERR_ARG, "bad forward args");
+  CK(h, cudaSetDevice(h->device));
+  int rc = order_after_legacy(h);
+  if (rc) return rc;
+  return sfail(h, nrg::surrogate_forward(h->sur, n, (const __nv_bfloat16*)x_bf16, out, h->stream));
+}
+
+extern "C" int nrg_surrogate_grad(nrg_chem* h, long n, const void* x_bf16, const float* y, float* grads_host,
+                                  double* loss_host) {
+  if (!h || n <= 0 || !x_bf16 || !y) return fail(h, NRG_ERR_ARG, "bad grad args");
+  CK(h, cudaSetDevice(h->device));
+  int rc = order_after_legacy(h);
+  if (rc) return rc;
+  return sfail(h, nrg::surrogate_grad(h->sur, n, (const __nv_bfloat16*)x_bf16, y, grads_host, loss_host, h->stream));
+}
+
+extern "C" int nrg_surrogate_train(nrg_chem* h, long n, const void* x_bf16, const float* y, int epochs, int batch,
+                                   float lr, unsigned long long seed, float* loss_per_epoch) {
+  if (!h || n <= 0 || !x_bf16 || !y || epochs <= 0 || !(lr > 0.f)) return fail(h, NRG_ERR_ARG, "bad train args");
+  CK(h, cudaSetDevice(h->device));
+  int rc = order_after_legacy(h);
+  if (rc) return rc;
+  return sfail(h, nrg::surrogate_train(h->sur, n, (const __nv_bfloat16*)x_bf16, y, epochs, batch, lr, seed,
+                                       loss_per_epoch, h->stream));
+}
+
+extern "C" int nrg_surrogate_set_gate(nrg_chem* h, double elem_tol, double dT_tol, double dT_max) {
+  if (!h || !(elem_tol >= 0) || !(dT_tol >= 0) || !(dT_max >= 0)) return NRG_ERR_ARG;
+  nrg::surrogate_set_gate(h->sur, elem_tol, dT_tol, dT_max);
+  return NRG_OK;
+}
+
+extern "C" int nrg_surrogate_enable(nrg_chem* h, int enable) {
+  if (!h) return NRG_ERR_ARG;
+  nrg::surrogate_set_ready(h->sur, enable != 0);
+  return NRG_OK;
+}
+
+extern "C" int nrg_surrogate_save(nrg_chem* h, const char* path) {
+  if (!h || !path) return NRG_ERR_ARG;
+  const int P = nrg::surrogate_param_count();
+  std::vector<float> p((size_t)P), nm(kNormFloats);
+  int rc = nrg_surrogate_get_params(h, p.data());
+  if (rc) return rc;
+  norm_to_floats(nrg::surrogate_get_norm(h->sur), nm.data());
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return fail(h, NRG_ERR_IO, std::string("cannot write ") + path);
+  const char magic[8] = {'N', 'R', 'G', 'S', 'U', 'R', '1', '\0'};
+  bool ok = std::fwrite(magic, 1, 8, f) == 8 && std::fwrite(&P, 4, 1, f) == 1 &&
+            std::fwrite(p.data(), 4, (size_t)P, f) == (size_t)P &&
+            std::fwrite(nm.data(), 4, (size_t)kNormFloats, f) == (size_t)kNormFloats;
+  ok = (std::fclose(f) == 0) && ok;
+  return ok ? NRG_OK : fail(h, NRG_ERR_IO, std::string("short write to ") + path);
+}
+
+extern "C" int nrg_surrogate_load(nrg_chem* h, const char* path) {
+  if (!h || !path) return NRG_ERR_ARG;
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return fail(h, NRG_ERR_IO, std::string("cannot read ") + path);
+  char magic[8];
+  int P = 0;
+  const int want = nrg::surrogate_param_count();
+  std::vector<float> p((size_t)want), nm(kNormFloats);
+  bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "NRGSUR1", 8) == 0 &&
+            std::fread(&P, 4, 1, f) == 1 && P == want && std::fread(p.data(), 4, (size_t)P, f) == (size_t)P &&
+            std::fread(nm.data(), 4, (size_t)kNormFloats, f) == (size_t)kNormFloats;
+  std::fclose(f);
+  if (!ok) return fail(h, NRG_ERR_IO, std::string("not a surrogate model file: ") + path);
+  int rc = nrg_surrogate_set_params(h, p.data());
+  if (rc) return rc;
+  rc = nrg_surrogate_set_norm(h, nm.data());
+  if (rc) return rc;
+  nrg::surrogate_set_ready(h->sur, true);
+  return NRG_OK;
+}
+
+extern "C" int nrg_chem_integrate(nrg_chem* h, long n, long ld, double dt, const double* dt_cells,
+                                  const double* T, const double* rho, const double* Y, const signed char* bc,
+                                  double* Y_prod, double* Y_prod2, double* E_f_prod, double* T_after,
+                                  unsigned char* status, void* stream, nrg_chem_stats* stats) {
+  if (!h) return NRG_ERR_ARG;
+  const int saved = h->mode;
+  if (h->mode == NRG_MODE_SURROGATE) h->mode = NRG_MODE_FAST;
+  if (n < 0 || ld < n || (!(dt > 0.0) && !dt_cells)) { h->mode = saved; return fail(h, NRG_ERR_ARG, "bad integrate args"); }
+  if (n > 0 && (!T || !rho || !Y || !Y_prod || !Y_prod2 || !E_f_prod)) {
+    h->mode = saved;
+    return fail(h, NRG_ERR_ARG, "null field pointer");
+  }
+  CK(h, cudaSetDevice(h->device));
+  StepArgs a{};
+  a.n = n; a.ld = ld; a.dt = dt > 0.0 ? dt : 1.0; a.T = T; a.rho = rho; a.Y = Y; a.bc = (const int8_t*)bc;
+  a.Y_prod = Y_prod; a.Y_prod2 = Y_prod2; a.E_f_prod = E_f_prod; a.T_after = T_after; a.status = status;
+  a.mxstep = 10000; a.mech = h->d_mech; a.dt_cells = dt_cells; a.cell_list = nullptr; a.n_list = 0;
+  a.n_list_dev = nullptr;
+  int rc = NRG_OK;
+  if (n == 0) {
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+  } else {
+    CK(h, cudaEventRecord(h->ev_in, (cudaStream_t)stream));
+    CK(h, cudaStreamWaitEvent(h->stream, h->ev_in, 0));
+    rc = run_step(h, a, h->stream, stats);
+  }
+  h->mode = saved;
+  return rc;
 }

@@ -869,7 +869,7 @@ __device__ bool cell_begin(CS& c, const StepArgs& a, long cid) {
     c.yh(0, k) = ci;
     c.y[k] = ci;
   }
-  c.tout = a.dt;
+  c.tout = a.dt_cells ? a.dt_cells[cid] : a.dt;
   c.t = 0.0;
   const double h = (c.tout - c.t) * (1.0 - 4.0 * c_mech.uround);
   c.h = copysign(NRG_FMIN(fabs(h), c_mech.hmax), h);
@@ -985,7 +985,7 @@ __device__ double temperature_after(double T0, const double (&Y0)[N], const doub
 // Outputs of a finished cell (chemical_kinetics_solver.f90:318-340).
 template <int N, class CS>
 __device__ void cell_finish(const CS& c, const StepArgs& a, long cid, int st) {
-  const double dt = a.dt;
+  const double dt = c.tout;
   const double rho = a.rho[cid];
   double E = 0.0;
   bool finite = true;

@@ -42,11 +42,13 @@ __device__ __forceinline__ void block_flush_counters(unsigned long long* counter
 template <int N, int R, int JAC, typename LUT, int BS>
 __global__ void __launch_bounds__(BS, 1) k_chem_plain(StepArgs a, unsigned long long* counters) {
   extern __shared__ __align__(16) char smem[];
-  const long cid = (long)blockIdx.x * BS + threadIdx.x;
+  const long li = (long)blockIdx.x * BS + threadIdx.x;
+  const long nl = a.cell_list ? (long)(a.n_list_dev ? *a.n_list_dev : a.n_list) : a.n;
+  const long cid = (a.cell_list && li < nl) ? (long)a.cell_list[li] : li;
   unsigned long long v[kCntSlots] = {0, 0, 0, 0, 0, 0};
   CellState<N, R, LUT, BS> c;
   c.bind(smem, threadIdx.x);
-  if (cid < a.n) {
+  if (li < nl) {
     if (cell_begin<N, R>(c, a, cid)) {
       int st;
       while ((st = cell_advance<N, R, JAC, LUT>(c, a.mxstep)) == 0) {
@@ -70,7 +72,8 @@ __global__ void __launch_bounds__(BS, 1) k_chem_queue(StepArgs a, int* queue, in
   unsigned long long v[kCntSlots] = {0, 0, 0, 0, 0, 0};
   CellState<N, R, LUT, BS> c;
   c.bind(smem, threadIdx.x);
-  long cur = 0, left = 0;  // current cell and cells still reserved by this lane
+  long cur = 0, left = 0, cid = 0;  // logical index, cells still reserved, cell id
+  const long nl = a.cell_list ? (long)(a.n_list_dev ? *a.n_list_dev : a.n_list) : a.n;
   bool have = false;
   for (;;) {
     if (!have) {
@@ -86,13 +89,14 @@ __global__ void __launch_bounds__(BS, 1) k_chem_queue(StepArgs a, int* queue, in
         ++cur;
       }
       --left;
-      if (cur >= a.n) break;
-      have = cell_begin<N, R>(c, a, cur);
+      if (cur >= nl) break;
+      cid = a.cell_list ? (long)a.cell_list[cur] : cur;
+      have = cell_begin<N, R>(c, a, cid);
       if (!have) continue;
     }
     const int st = cell_advance<N, R, JAC, LUT>(c, a.mxstep);
     if (st) {
-      cell_finish<N>(c, a, cur, st);
+      cell_finish<N>(c, a, cid, st);
       v[kCntCells] += 1;
       v[kCntSteps] += c.nstep;
       v[kCntRhs] += c.nfe;
@@ -120,7 +124,8 @@ static cudaError_t launch_bs(const StepArgs& a, const LaunchCfg& cfg, int* queue
     e = cudaFuncSetAttribute(k_chem_plain<N, R, JAC, LUT, BS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem);
     if (e != cudaSuccess) return e;
-    const long grid = (a.n + BS - 1) / BS;
+    const long nl = a.cell_list ? (long)a.n_list : a.n;
+    const long grid = (nl + BS - 1) / BS;
     if (grid > 0) k_chem_plain<N, R, JAC, LUT, BS><<<(unsigned)grid, BS, smem, s>>>(a, counters);
   }
   return cudaGetLastError();
@@ -147,6 +152,7 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) k_chem_warp(St
   c.M = &sM;
   c.lane = threadIdx.x & 31;
   c.sm = &sm[threadIdx.x >> 5];
+  const long nl = a.cell_list ? (long)(a.n_list_dev ? *a.n_list_dev : a.n_list) : a.n;
   long cur = 0, left = 0;
   for (;;) {
     if (left == 0) {
@@ -158,12 +164,13 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) k_chem_warp(St
       ++cur;
     }
     --left;
-    if (cur >= a.n) break;
-    if (!warp_cell_begin(c, a, cur)) continue;
+    if (cur >= nl) break;
+    const long cid = a.cell_list ? (long)a.cell_list[cur] : cur;
+    if (!warp_cell_begin(c, a, cid)) continue;
     int st;
     while ((st = warp_cell_advance<N, R, JAC>(c, a.mxstep)) == 0) {
     }
-    warp_cell_finish(c, a, cur, st);
+    warp_cell_finish(c, a, cid, st);
     if (c.lane == 0) {
       v[kCntCells] += 1;
       v[kCntSteps] += c.nstep;

@@ -25,7 +25,11 @@ struct StepArgs {
   double* T_after;    // may be null
   uint8_t* status;    // may be null
   int mxstep;
-  const DevMech* mech;  // device copy of the mechanism tables (global memory)
+  const DevMech* mech;     // device copy of the mechanism tables (global memory)
+  const double* dt_cells;  // per-cell step (training pairs); null: dt for every cell
+  const int* cell_list;    // integrate only these cells (gated fallback); null: 0..n-1
+  int n_list;              // number of entries in cell_list (grid bound when n_list_dev is set)
+  const int* n_list_dev;   // device-side entry count of cell_list (may be null)
 };
 
 enum KernelKind { kKernelThreadGrid = 0, kKernelThreadQueue = 1, kKernelWarpQueue = 2 };

@@ -673,7 +673,7 @@ __device__ bool warp_cell_begin(WarpCell<N, R, LUT>& c, const StepArgs& a, long 
   c.s1 = 0.0;
   c.s2 = 0.0;
   c.fac = 0.0;
-  c.tout = a.dt;
+  c.tout = a.dt_cells ? a.dt_cells[cid] : a.dt;
   c.t = 0.0;
   const double h = (c.tout - c.t) * (1.0 - 4.0 * c.M->uround);
   c.h = copysign(NRG_FMIN(fabs(h), c.M->hmax), h);
@@ -727,7 +727,7 @@ __device__ int warp_cell_advance(WarpCell<N, R, LUT>& c, int mxstep) {
 
 template <int N, int R, typename LUT>
 __device__ void warp_cell_finish(const WarpCell<N, R, LUT>& c, const StepArgs& a, long cid, int st) {
-  const double dt = a.dt;
+  const double dt = c.tout;
   const double rho = a.rho[cid];
   const double dc = c.y - c.conc_in;
   const double yp = c.lane < N ? dc * c.M->W[c.lane] / dt : 0.0;

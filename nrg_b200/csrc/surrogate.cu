@@ -1,19 +1,884 @@
-// Gated MLP surrogate (placeholder until the tensor-core kernels land).
+// Gated MLP surrogate of the per-cell chemistry increment.
+//
+// Training and the unfused inference path use one BF16 tensor-core GEMM
+// (mma.sync m16n8k16, FP32 accumulate) with a fused bias/GELU epilogue; the
+// gate decides per cell whether the prediction is used or the cell goes to
+// the FP64 integrator:
+//   * skip rule of the reference (T < 305 K or bc /= 0): zero sources;
+//   * training hull: every raw feature inside the training min/max widened by
+//     hull_margin of its range;
+//   * element conservation: |sum_k a_ek (W_e / W_k) dY_k| <= elem_tol for the
+//     elements H, O, N (element mass fraction units);
+//   * temperature: the network's dT agrees within dT_tol with the FP64 energy
+//     closure of its own dY, and |dT| <= dT_max.
+// Rejected cells are compacted in cell order (so neighbouring cells stay
+// neighbours for the integrator) and integrated by the FP64 kernel.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <random>
+#include <vector>
+
+#include "chem_bdf.cuh"
 #include "surrogate.hpp"
 
 namespace nrg {
 
-struct Surrogate {
-  bool ready = false;
+// ------------------------------------------------------------------ GEMM
+struct GemmArgs {
+  int M, N, K;
+  const __nv_bfloat16* A;
+  long sam, sak;
+  const __nv_bfloat16* B;
+  long sbk, sbn;
+  float* C;  // fp32 result (may be null)
+  long ldc;
+  const float* bias;   // per column (may be null)
+  __nv_bfloat16* H;    // bf16 activation output (may be null)
+  long ldh;
+  int gelu;            // H = bf16(gelu(C)) when set, else bf16(C)
 };
 
-Surrogate* surrogate_create(const DevMech&) { return new Surrogate(); }
-void surrogate_destroy(Surrogate* s) { delete s; }
-bool surrogate_ready(const Surrogate* s) { return s && s->ready; }
+__device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 lo, __nv_bfloat16 hi) {
+  return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+}
 
-cudaError_t surrogate_step(Surrogate*, const StepArgs&, const LaunchCfg&, int*, unsigned long long*,
-                           cudaStream_t, const FallbackFn&) {
-  return cudaErrorNotSupported;
+__device__ __forceinline__ void mma_bf16_16816(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                               uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// C[M,N] = sum_k A[m,k] B[k,n]; 128 threads, 64x64 block tile, 32x32 per warp.
+__global__ void __launch_bounds__(128) k_gemm_bf16(GemmArgs g) {
+  constexpr int BM = 64, BN = 64, BK = 32;
+  __shared__ __nv_bfloat16 As[BM][BK + 8];
+  __shared__ __nv_bfloat16 Bs[BK][BN + 8];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 1, wn = warp & 1;
+  const int g8 = lane >> 2, tq = lane & 3;
+  const long m0 = (long)blockIdx.x * BM, n0 = (long)blockIdx.y * BN;
+  float acc[2][4][4];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.f;
+  const __nv_bfloat16 zero = __float2bfloat16(0.f);
+  for (int k0 = 0; k0 < g.K; k0 += BK) {
+    for (int e = tid; e < BM * BK; e += 128) {
+      const int r = e / BK, kk = e % BK;
+      const long m = m0 + r, k = k0 + kk;
+      As[r][kk] = (m < g.M && k < g.K) ? g.A[m * g.sam + k * g.sak] : zero;
+    }
+    for (int e = tid; e < BK * BN; e += 128) {
+      const int kk = e / BN, cc = e % BN;
+      const long k = k0 + kk, n = n0 + cc;
+      Bs[kk][cc] = (k < g.K && n < g.N) ? g.B[k * g.sbk + n * g.sbn] : zero;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int ks = 0; ks < BK; ks += 16) {
+      uint32_t a[2][4], b[4][2];
+#pragma unroll
+      for (int mi = 0; mi < 2; ++mi) {
+        const int r = wm * 32 + mi * 16 + g8;
+        a[mi][0] = pack_bf16(As[r][ks + 2 * tq], As[r][ks + 2 * tq + 1]);
+        a[mi][1] = pack_bf16(As[r + 8][ks + 2 * tq], As[r + 8][ks + 2 * tq + 1]);
+        a[mi][2] = pack_bf16(As[r][ks + 2 * tq + 8], As[r][ks + 2 * tq + 9]);
+        a[mi][3] = pack_bf16(As[r + 8][ks + 2 * tq + 8], As[r + 8][ks + 2 * tq + 9]);
+      }
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni) {
+        const int cc = wn * 32 + ni * 8 + g8;
+        b[ni][0] = pack_bf16(Bs[ks + 2 * tq][cc], Bs[ks + 2 * tq + 1][cc]);
+        b[ni][1] = pack_bf16(Bs[ks + 2 * tq + 8][cc], Bs[ks + 2 * tq + 9][cc]);
+      }
+#pragma unroll
+      for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+          mma_bf16_16816(acc[mi][ni], a[mi][0], a[mi][1], a[mi][2], a[mi][3], b[ni][0], b[ni][1]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const long m = m0 + wm * 32 + mi * 16 + g8 + (q >= 2 ? 8 : 0);
+        const long n = n0 + wn * 32 + ni * 8 + 2 * tq + (q & 1);
+        if (m >= g.M || n >= g.N) continue;
+        float v = acc[mi][ni][q];
+        if (g.bias) v += g.bias[n];
+        if (g.C) g.C[m * g.ldc + n] = v;
+        if (g.H) g.H[m * g.ldh + n] = __float2bfloat16(g.gelu ? gelu_f(v) : v);
+      }
+}
+
+static cudaError_t gemm(const GemmArgs& g, cudaStream_t st) {
+  dim3 grid((unsigned)((g.M + 63) / 64), (unsigned)((g.N + 63) / 64));
+  if (grid.x == 0 || grid.y == 0) return cudaSuccess;
+  k_gemm_bf16<<<grid, 128, 0, st>>>(g);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------- small kernels
+__global__ void k_loss_grad(long B, const float* O, const float* Y, float* dOf, __nv_bfloat16* dOb,
+                            double* loss) {
+  double part = 0.0;
+  const float scale = 2.0f / (float)(B * kMlpOut);
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < B * kMlpOutPad; i += (long)gridDim.x * blockDim.x) {
+    const long b = i / kMlpOutPad;
+    const int j = (int)(i % kMlpOutPad);
+    float d = 0.f;
+    if (j < kMlpOut) {
+      const float e = O[b * kMlpOutPad + j] - Y[b * kMlpOut + j];
+      part += (double)e * e;
+      d = scale * e;
+    }
+    dOf[i] = d;
+    dOb[i] = __float2bfloat16(d);
+  }
+  for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
+  if ((threadIdx.x & 31) == 0 && loss) atomicAdd(loss, part / (double)(B * kMlpOut));
+}
+
+__global__ void k_gelu_back(long n, const float* dH, const float* Z, float* dZf, __nv_bfloat16* dZb) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const float d = dH[i] * gelu_grad_f(Z[i]);
+    dZf[i] = d;
+    dZb[i] = __float2bfloat16(d);
+  }
+}
+
+// db[c] = sum over rows of M[r][c] (one block per column)
+__global__ void k_colsum(long rows, int ncols, const float* M, float* db) {
+  const int c = blockIdx.x;
+  float s = 0.f;
+  for (long r = threadIdx.x; r < rows; r += blockDim.x) s += M[r * ncols + c];
+  __shared__ float red[32];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.f;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) db[c] = s;
+  }
+}
+
+__global__ void k_adam(long n, float* w, const float* g, float* m, float* v, __nv_bfloat16* wb, float lr,
+                       float b1, float b2, float eps, float bc1, float bc2) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    const float wi = w[i] - lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+    w[i] = wi;
+    if (wb) wb[i] = __float2bfloat16(wi);
+  }
+}
+
+__global__ void k_to_bf16(long n, const float* x, __nv_bfloat16* y) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    y[i] = __float2bfloat16(x[i]);
+}
+
+__global__ void k_gather_rows(long nb, const int* idx, const __nv_bfloat16* X, const float* Y,
+                              __nv_bfloat16* Xb, float* Yb) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nb; i += (long)gridDim.x * blockDim.x) {
+    const long r = idx[i];
+#pragma unroll
+    for (int j = 0; j < kMlpInPad; ++j) Xb[i * kMlpInPad + j] = X[r * kMlpInPad + j];
+#pragma unroll
+    for (int j = 0; j < kMlpOut; ++j) Yb[i * kMlpOut + j] = Y[r * kMlpOut + j];
+  }
+}
+
+// Raw features of a cell: T, log(p/1 atm), Y_1..Y_9, log10(dt).
+template <int N>
+__device__ __forceinline__ void cell_features(double T, double rho, const double (&y)[N], double dt, float* f) {
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < N; ++k) s += y[k] / c_mech.W[k];
+  const double p = rho * 8.31446261815324 * T * s;
+  f[0] = (float)T;
+  f[1] = (float)log(p / 101325.0);
+#pragma unroll
+  for (int k = 0; k < N; ++k) f[2 + k] = (float)y[k];
+  f[11] = (float)log10(dt);
+}
+
+__global__ void k_features(long n, long ld, double dt, const double* dt_cells, const double* T, const double* rho,
+                           const double* Y, const MlpNorm* nm, float* xraw, __nv_bfloat16* x) {
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
+    double y[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) y[k] = Y[k * ld + c];
+    float f[kMlpIn];
+    cell_features<9>(T[c], rho[c], y, dt_cells ? dt_cells[c] : dt, f);
+    if (xraw)
+#pragma unroll
+      for (int j = 0; j < kMlpIn; ++j) xraw[c * kMlpIn + j] = f[j];
+    if (x) {
+#pragma unroll
+      for (int j = 0; j < kMlpInPad; ++j)
+        x[c * kMlpInPad + j] = __float2bfloat16(j < kMlpIn ? (f[j] - nm->x_mu[j]) / nm->x_sd[j] : 0.f);
+    }
+  }
+}
+
+// Gate and outputs.  flag[c] = 1 sends the cell to the FP64 fallback.
+struct GateCfg {
+  double elem_tol, dT_tol, dT_max;
+};
+
+__global__ void k_gate(StepArgs a, const float* O, const MlpNorm* nm, GateCfg gc, unsigned char* flag,
+                       unsigned long long* counters) {
+  unsigned long long n_sur = 0;
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < a.n; c += (long)gridDim.x * blockDim.x) {
+    const double T0 = a.T[c];
+    if (!((T0 >= 305.0) && (a.bc == nullptr || a.bc[c] == 0))) {
+#pragma unroll
+      for (int k = 0; k < 9; ++k) a.Y_prod[k * a.ld + c] = 0.0;
+      a.E_f_prod[c] = 0.0;
+      if (a.T_after) a.T_after[c] = T0;
+      if (a.status) a.status[c] = kCellSkipped;
+      flag[c] = 0;
+      continue;
+    }
+    const double rho = a.rho[c];
+    const double dt = a.dt_cells ? a.dt_cells[c] : a.dt;
+    double y0[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) y0[k] = a.Y[k * a.ld + c];
+    float f[kMlpIn];
+    cell_features<9>(T0, rho, y0, dt, f);
+    bool ok = true;
+#pragma unroll
+    for (int j = 0; j < kMlpIn; ++j) {
+      const float span = nm->x_max[j] - nm->x_min[j];
+      const float lo = nm->x_min[j] - nm->hull_margin * span, hi = nm->x_max[j] + nm->hull_margin * span;
+      ok = ok && (f[j] >= lo) && (f[j] <= hi);
+    }
+    double dY[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      dY[k] = (double)O[c * kMlpOutPad + k] * (double)nm->y_sd[k];
+      ok = ok && isfinite(dY[k]);
+    }
+    const double dT_net = (double)O[c * kMlpOutPad + 9] * (double)nm->y_sd[9];
+    ok = ok && isfinite(dT_net) && fabs(dT_net) <= gc.dT_max;
+    // element conservation (H, O, N) of the predicted increment
+    const double We[3] = {1.00794e-3, 15.9994e-3, 14.0067e-3};
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+      double r = 0.0;
+#pragma unroll
+      for (int k = 0; k < 9; ++k) r += c_mech.elem[e][k] * We[e] / c_mech.W[k] * dY[k];
+      ok = ok && fabs(r) <= gc.elem_tol;
+    }
+    double E = 0.0;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) E = E - c_mech.h_ref[k] * (dY[k] * rho / c_mech.W[k]) / dt;
+    if (ok) {
+      const double T1 = temperature_after<9>(T0, y0, dY, E * dt / rho);
+      ok = fabs((T1 - T0) - dT_net) <= gc.dT_tol;
+      if (ok) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+          a.Y_prod[k * a.ld + c] = dY[k] * rho / dt;
+          a.Y_prod2[k * a.ld + c] = dY[k] * rho / c_mech.W[k];
+        }
+        a.E_f_prod[c] = E;
+        if (a.T_after) a.T_after[c] = T1;
+        if (a.status) a.status[c] = kCellSurrogate;
+        ++n_sur;
+      }
+    }
+    flag[c] = ok ? 0 : 1;
+  }
+  if (counters) {
+    for (int o = 16; o > 0; o >>= 1) n_sur += __shfl_down_sync(0xffffffffu, n_sur, o);
+    if ((threadIdx.x & 31) == 0 && n_sur) atomicAdd(&counters[6], n_sur);
+  }
+}
+
+// Order-preserving compaction of flagged cells: per-block counts, a single
+// block scan of the counts, then an in-block ballot scan for the scatter.
+constexpr int kCompactBlock = 1024;
+
+__global__ void k_flag_count(long n, const unsigned char* flag, int* block_count) {
+  const long i = (long)blockIdx.x * kCompactBlock + threadIdx.x;
+  const int f = (i < n) ? (int)flag[i] : 0;
+  const int cnt = __syncthreads_count(f);
+  if (threadIdx.x == 0) block_count[blockIdx.x] = cnt;
+}
+
+__global__ void k_scan_counts(int nb, const int* block_count, int* block_off, int* total,
+                              unsigned long long* counters) {
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < nb; base += blockDim.x) {
+    const int i = base + threadIdx.x;
+    const int v = i < nb ? block_count[i] : 0;
+    // inclusive warp scan, then across warps
+    int x = v;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    __shared__ int wsum[32];
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    if (w == 0) {
+      int s = lane < (int)(blockDim.x >> 5) ? wsum[lane] : 0;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, s, o);
+        if (lane >= o) s += y;
+      }
+      wsum[lane] = s;
+    }
+    __syncthreads();
+    const int incl = x + (w > 0 ? wsum[w - 1] : 0);
+    if (i < nb) block_off[i] = carry + incl - v;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry += incl;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    *total = carry;
+    if (counters) counters[7] += (unsigned long long)carry;
+  }
+}
+
+__global__ void k_compact(long n, const unsigned char* flag, const int* block_off, int* list) {
+  const long i = (long)blockIdx.x * kCompactBlock + threadIdx.x;
+  const int f = (i < n) ? (int)flag[i] : 0;
+  const unsigned bal = __ballot_sync(0xffffffffu, f);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __shared__ int wcount[kCompactBlock / 32];
+  if (lane == 0) wcount[w] = __popc(bal);
+  __syncthreads();
+  int before = 0;
+  for (int q = 0; q < w; ++q) before += wcount[q];
+  if (f) list[block_off[blockIdx.x] + before + __popc(bal & ((1u << lane) - 1u))] = (int)i;
+}
+
+// Raw training targets: dY_k = Y_prod_k dt / rho and dT = T_after - T.
+__global__ void k_targets(long n, long ld, double dt, const double* dt_cells, const double* T, const double* rho,
+                          const double* Y_prod, const double* T_after, float* y) {
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
+    const double d = dt_cells ? dt_cells[c] : dt;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) y[c * kMlpOut + k] = (float)(Y_prod[k * ld + c] * d / rho[c]);
+    y[c * kMlpOut + 9] = (float)(T_after[c] - T[c]);
+  }
+}
+
+// Per-column mean, standard deviation, min and max (one block per column).
+__global__ void k_colstats(long rows, int ncols, const float* M, double* out) {
+  const int c = blockIdx.x;
+  double s = 0.0, q = 0.0, lo = 1e300, hi = -1e300;
+  for (long r = threadIdx.x; r < rows; r += blockDim.x) {
+    const double v = M[r * ncols + c];
+    s += v;
+    q += v * v;
+    lo = v < lo ? v : lo;
+    hi = v > hi ? v : hi;
+  }
+  __shared__ double sh[4][32];
+  for (int o = 16; o > 0; o >>= 1) {
+    s += __shfl_down_sync(0xffffffffu, s, o);
+    q += __shfl_down_sync(0xffffffffu, q, o);
+    lo = fmin(lo, __shfl_down_sync(0xffffffffu, lo, o));
+    hi = fmax(hi, __shfl_down_sync(0xffffffffu, hi, o));
+  }
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) { sh[0][w] = s; sh[1][w] = q; sh[2][w] = lo; sh[3][w] = hi; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double S = 0, Q = 0, L = 1e300, H = -1e300;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
+      S += sh[0][i]; Q += sh[1][i]; L = fmin(L, sh[2][i]); H = fmax(H, sh[3][i]);
+    }
+    const double mu = S / (double)rows;
+    out[c * 4 + 0] = mu;
+    out[c * 4 + 1] = sqrt(fmax(Q / (double)rows - mu * mu, 0.0));
+    out[c * 4 + 2] = L;
+    out[c * 4 + 3] = H;
+  }
+}
+
+__global__ void k_standardize(long n, const float* xraw, const float* yraw, const MlpNorm* nm,
+                              __nv_bfloat16* x, float* y) {
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int j = 0; j < kMlpInPad; ++j)
+      x[c * kMlpInPad + j] = __float2bfloat16(j < kMlpIn ? (xraw[c * kMlpIn + j] - nm->x_mu[j]) / nm->x_sd[j] : 0.f);
+#pragma unroll
+    for (int j = 0; j < kMlpOut; ++j) y[c * kMlpOut + j] = yraw[c * kMlpOut + j] / nm->y_sd[j];
+  }
+}
+
+// -------------------------------------------------------------- state
+struct Surrogate {
+  bool ready = false;
+  bool uploaded = false;
+  GateCfg gate{1e-6, 0.5, 50.0};
+  MlpNorm norm{};
+  MlpNorm* d_norm = nullptr;
+  // parameters: fp32 master, Adam moments, bf16 working copies, gradients
+  float* w = nullptr;
+  float* m = nullptr;
+  float* v = nullptr;
+  float* gr = nullptr;
+  __nv_bfloat16* wb = nullptr;
+  long n_params = 0;
+  long offW[kMlpLayers], offb[kMlpLayers];
+  long step = 0;
+  // activation buffers (grow-only)
+  long cap = 0;
+  __nv_bfloat16 *X = nullptr, *H[kMlpLayers] = {}, *dHb = nullptr;
+  float *Z[kMlpLayers] = {}, *O = nullptr, *dOf = nullptr, *dHf = nullptr, *dZf = nullptr;
+  __nv_bfloat16* dOb = nullptr;
+  float* Yb = nullptr;
+  int* idx = nullptr;
+  double* d_loss = nullptr;
+  // inference buffers (features, two activation buffers, outputs)
+  long icap = 0;
+  __nv_bfloat16 *iX = nullptr, *iH[2] = {nullptr, nullptr};
+  float* iO = nullptr;
+  // gate / compaction buffers
+  long gcap = 0;
+  unsigned char* flag = nullptr;
+  int *block_count = nullptr, *block_off = nullptr, *list = nullptr, *n_list = nullptr;
+};
+
+static long param_layout(Surrogate* s) {
+  long off = 0;
+  for (int l = 0; l < kMlpLayers; ++l) {
+    s->offW[l] = off;
+    off += (long)mlp_out(l) * mlp_in(l);
+    s->offb[l] = off;
+    off += mlp_out(l);
+  }
+  return off;
+}
+
+int surrogate_param_count() {
+  int off = 0;
+  for (int l = 0; l < kMlpLayers; ++l) off += mlp_out(l) * mlp_in(l) + mlp_out(l);
+  return off;
+}
+
+Surrogate* surrogate_create(const DevMech& dm) {
+  Surrogate* s = new Surrogate();
+  s->n_params = param_layout(s);
+  cudaMemcpyToSymbol(c_mech, &dm, sizeof(DevMech));
+  const size_t P = (size_t)s->n_params;
+  if (cudaMalloc(&s->w, P * 4) != cudaSuccess || cudaMalloc(&s->m, P * 4) != cudaSuccess ||
+      cudaMalloc(&s->v, P * 4) != cudaSuccess || cudaMalloc(&s->gr, P * 4) != cudaSuccess ||
+      cudaMalloc(&s->wb, P * 2) != cudaSuccess || cudaMalloc(&s->d_norm, sizeof(MlpNorm)) != cudaSuccess ||
+      cudaMalloc(&s->d_loss, sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    s->uploaded = false;
+    return s;
+  }
+  cudaMemset(s->w, 0, P * 4);
+  cudaMemset(s->m, 0, P * 4);
+  cudaMemset(s->v, 0, P * 4);
+  cudaMemset(s->wb, 0, P * 2);
+  s->uploaded = true;
+  return s;
+}
+
+static void free_act(Surrogate* s) {
+  cudaFree(s->X);
+  for (int l = 0; l < kMlpLayers; ++l) {
+    cudaFree(s->H[l]);
+    cudaFree(s->Z[l]);
+    s->H[l] = nullptr;
+    s->Z[l] = nullptr;
+  }
+  cudaFree(s->dHb); cudaFree(s->O); cudaFree(s->dOf); cudaFree(s->dHf); cudaFree(s->dZf); cudaFree(s->dOb);
+  cudaFree(s->Yb); cudaFree(s->idx);
+  s->X = s->dHb = s->dOb = nullptr;
+  s->O = s->dOf = s->dHf = s->dZf = s->Yb = nullptr;
+  s->idx = nullptr;
+  s->cap = 0;
+}
+
+void surrogate_destroy(Surrogate* s) {
+  if (!s) return;
+  free_act(s);
+  cudaFree(s->w); cudaFree(s->m); cudaFree(s->v); cudaFree(s->gr); cudaFree(s->wb); cudaFree(s->d_norm);
+  cudaFree(s->iX); cudaFree(s->iH[0]); cudaFree(s->iH[1]); cudaFree(s->iO);
+  cudaFree(s->d_loss); cudaFree(s->flag); cudaFree(s->block_count); cudaFree(s->block_off); cudaFree(s->list);
+  cudaFree(s->n_list);
+  delete s;
+}
+
+bool surrogate_ready(const Surrogate* s) { return s && s->ready && s->uploaded; }
+void surrogate_set_ready(Surrogate* s, bool r) { s->ready = r; }
+void surrogate_set_gate(Surrogate* s, double elem_tol, double dT_tol, double dT_max) {
+  s->gate = GateCfg{elem_tol, dT_tol, dT_max};
+}
+
+static std::string ck(cudaError_t e, const char* what) {
+  return e == cudaSuccess ? std::string() : std::string(what) + ": " + cudaGetErrorString(e);
+}
+
+static std::string ensure_act(Surrogate* s, long n) {
+  if (n <= s->cap) return "";
+  free_act(s);
+  const long np = (n + 63) / 64 * 64;
+  std::string e;
+  e = ck(cudaMalloc(&s->X, np * kMlpInPad * 2), "alloc X");
+  if (!e.empty()) return e;
+  for (int l = 0; l < kMlpLayers; ++l) {
+    if ((e = ck(cudaMalloc(&s->H[l], np * mlp_out(l) * 2), "alloc H")).size()) return e;
+    if ((e = ck(cudaMalloc(&s->Z[l], np * mlp_out(l) * 4), "alloc Z")).size()) return e;
+  }
+  if ((e = ck(cudaMalloc(&s->O, np * kMlpOutPad * 4), "alloc O")).size()) return e;
+  if ((e = ck(cudaMalloc(&s->dOf, np * kMlpOutPad * 4), "alloc dO")).size()) return e;
+  if ((e = ck(cudaMalloc(&s->dOb, np * kMlpOutPad * 2), "alloc dO")).size()) return e;
+  if ((e = ck(cudaMalloc(&s->dHf, np * kMlpHid * 4), "alloc dH")).size()) return e;
+  if ((e = ck(cudaMalloc(&s->dHb, np * kMlpHid * 2), "alloc dH")).size()) return e;
+  if ((e = ck(cudaMalloc(&s->dZf, np * kMlpHid * 4), "alloc dZ")).size()) return e;
+  if ((e = ck(cudaMalloc(&s->Yb, np * kMlpOut * 4), "alloc Y")).size()) return e;
+  if ((e = ck(cudaMalloc(&s->idx, np * 4), "alloc idx")).size()) return e;
+  s->cap = np;
+  return "";
+}
+
+static std::string ensure_infer(Surrogate* s, long n) {
+  if (n <= s->icap) return "";
+  cudaFree(s->iX); cudaFree(s->iH[0]); cudaFree(s->iH[1]); cudaFree(s->iO);
+  s->iX = s->iH[0] = s->iH[1] = nullptr;
+  s->iO = nullptr;
+  s->icap = 0;
+  const long np = (n + 63) / 64 * 64;
+  std::string e;
+  if ((e = ck(cudaMalloc(&s->iX, np * kMlpInPad * 2), "alloc X")).size()) return e;
+  if ((e = ck(cudaMalloc(&s->iH[0], np * kMlpHid * 2), "alloc H")).size()) return e;
+  if ((e = ck(cudaMalloc(&s->iH[1], np * kMlpHid * 2), "alloc H")).size()) return e;
+  if ((e = ck(cudaMalloc(&s->iO, np * kMlpOutPad * 4), "alloc O")).size()) return e;
+  s->icap = np;
+  return "";
+}
+
+static std::string ensure_gate(Surrogate* s, long n) {
+  if (n <= s->gcap) return "";
+  cudaFree(s->flag); cudaFree(s->block_count); cudaFree(s->block_off); cudaFree(s->list); cudaFree(s->n_list);
+  const long nb = (n + kCompactBlock - 1) / kCompactBlock;
+  std::string e;
+  if ((e = ck(cudaMalloc(&s->flag, n), "alloc flag")).size()) return e;
+  if ((e = ck(cudaMalloc(&s->block_count, nb * 4), "alloc counts")).size()) return e;
+  if ((e = ck(cudaMalloc(&s->block_off, nb * 4), "alloc offsets")).size()) return e;
+  if ((e = ck(cudaMalloc(&s->list, n * 4), "alloc list")).size()) return e;
+  if ((e = ck(cudaMalloc(&s->n_list, 4), "alloc count")).size()) return e;
+  s->gcap = n;
+  return "";
+}
+
+std::string surrogate_init(Surrogate* s, unsigned long long seed, cudaStream_t st) {
+  std::vector<float> h((size_t)s->n_params, 0.f);
+  std::mt19937_64 rng(seed);
+  for (int l = 0; l < kMlpLayers; ++l) {
+    const int fan_in = l == 0 ? kMlpIn : kMlpHid;
+    const float bound = std::sqrt(6.0f / (float)fan_in) * (l == kMlpLayers - 1 ? 0.25f : 1.0f);
+    std::uniform_real_distribution<float> U(-bound, bound);
+    for (int o = 0; o < mlp_out(l); ++o)
+      for (int i = 0; i < mlp_in(l); ++i) {
+        const bool live = (l == 0 ? i < kMlpIn : true) && (l == kMlpLayers - 1 ? o < kMlpOut : true);
+        h[s->offW[l] + (long)o * mlp_in(l) + i] = live ? U(rng) : 0.f;
+      }
+  }
+  s->step = 0;
+  std::string e = surrogate_set_params(s, h.data(), st);
+  if (!e.empty()) return e;
+  cudaMemsetAsync(s->m, 0, s->n_params * 4, st);
+  cudaMemsetAsync(s->v, 0, s->n_params * 4, st);
+  return ck(cudaStreamSynchronize(st), "init");
+}
+
+std::string surrogate_set_norm(Surrogate* s, const MlpNorm& norm) {
+  s->norm = norm;
+  return ck(cudaMemcpy(s->d_norm, &norm, sizeof(MlpNorm), cudaMemcpyHostToDevice), "norm upload");
+}
+
+MlpNorm surrogate_get_norm(const Surrogate* s) { return s->norm; }
+
+std::string surrogate_get_params(Surrogate* s, float* host, cudaStream_t st) {
+  std::string e = ck(cudaMemcpyAsync(host, s->w, s->n_params * 4, cudaMemcpyDeviceToHost, st), "params D2H");
+  if (!e.empty()) return e;
+  return ck(cudaStreamSynchronize(st), "params D2H");
+}
+
+std::string surrogate_set_params(Surrogate* s, const float* host, cudaStream_t st) {
+  std::string e = ck(cudaMemcpyAsync(s->w, host, s->n_params * 4, cudaMemcpyHostToDevice, st), "params H2D");
+  if (!e.empty()) return e;
+  k_to_bf16<<<64, 256, 0, st>>>(s->n_params, s->w, s->wb);
+  return ck(cudaStreamSynchronize(st), "params H2D");
+}
+
+std::string surrogate_features(Surrogate* s, long n, long ld, double dt, const double* dt_cells, const double* T,
+                               const double* rho, const double* Y, float* xraw, __nv_bfloat16* x,
+                               cudaStream_t st) {
+  if (n <= 0) return "";
+  k_features<<<std::min<long>((n + 255) / 256, 148 * 16), 256, 0, st>>>(n, ld, dt, dt_cells, T, rho, Y, s->d_norm,
+                                                                      xraw, x);
+  return ck(cudaGetLastError(), "features");
+}
+
+// Forward over n rows of bf16 features; keeps H/Z for backward.
+static cudaError_t forward(Surrogate* s, long n, const __nv_bfloat16* x, float* out, cudaStream_t st) {
+  const __nv_bfloat16* in = x;
+  for (int l = 0; l < kMlpLayers; ++l) {
+    GemmArgs g{};
+    g.M = (int)n;
+    g.N = mlp_out(l);
+    g.K = mlp_in(l);
+    g.A = in;
+    g.sam = mlp_in(l);
+    g.sak = 1;
+    g.B = s->wb + s->offW[l];
+    g.sbk = 1;
+    g.sbn = mlp_in(l);
+    g.bias = s->w + s->offb[l];
+    const bool last = l == kMlpLayers - 1;
+    g.C = last ? out : s->Z[l];
+    g.ldc = mlp_out(l);
+    g.H = last ? nullptr : s->H[l];
+    g.ldh = mlp_out(l);
+    g.gelu = 1;
+    cudaError_t e = gemm(g, st);
+    if (e != cudaSuccess) return e;
+    in = s->H[l];
+  }
+  return cudaSuccess;
+}
+
+std::string surrogate_forward(Surrogate* s, long n, const __nv_bfloat16* x, float* out, cudaStream_t st) {
+  std::string e = ensure_act(s, n);
+  if (!e.empty()) return e;
+  e = ck(forward(s, n, x, out, st), "forward");
+  if (!e.empty()) return e;
+  return ck(cudaStreamSynchronize(st), "forward");
+}
+
+// Inference forward: bf16 activations ping-pong, no pre-activations kept.
+static cudaError_t forward_infer(Surrogate* s, long n, const __nv_bfloat16* x, float* out, cudaStream_t st) {
+  const __nv_bfloat16* in = x;
+  for (int l = 0; l < kMlpLayers; ++l) {
+    GemmArgs g{};
+    g.M = (int)n;
+    g.N = mlp_out(l);
+    g.K = mlp_in(l);
+    g.A = in;
+    g.sam = mlp_in(l);
+    g.sak = 1;
+    g.B = s->wb + s->offW[l];
+    g.sbk = 1;
+    g.sbn = mlp_in(l);
+    g.bias = s->w + s->offb[l];
+    const bool last = l == kMlpLayers - 1;
+    g.C = last ? out : nullptr;
+    g.ldc = mlp_out(l);
+    g.H = last ? nullptr : s->iH[l & 1];
+    g.ldh = mlp_out(l);
+    g.gelu = 1;
+    cudaError_t e = gemm(g, st);
+    if (e != cudaSuccess) return e;
+    in = s->iH[l & 1];
+  }
+  return cudaSuccess;
+}
+
+// Gradients of the MSE over B rows (x in s->X-like layout, y normalised).
+static cudaError_t backward(Surrogate* s, long B, const __nv_bfloat16* x, const float* y, cudaStream_t st) {
+  cudaError_t e = forward(s, B, x, s->O, st);
+  if (e != cudaSuccess) return e;
+  k_loss_grad<<<std::min<long>((B * kMlpOutPad + 255) / 256, 1024), 256, 0, st>>>(B, s->O, y, s->dOf, s->dOb,
+                                                                                   s->d_loss);
+  const __nv_bfloat16* dZb = s->dOb;
+  const float* dZf = s->dOf;
+  for (int l = kMlpLayers - 1; l >= 0; --l) {
+    const __nv_bfloat16* Hin = l == 0 ? x : s->H[l - 1];
+    // dW[out][in] = sum_b dZ[b][out] Hin[b][in]
+    GemmArgs g{};
+    g.M = mlp_out(l);
+    g.N = mlp_in(l);
+    g.K = (int)B;
+    g.A = dZb;
+    g.sam = 1;
+    g.sak = mlp_out(l);
+    g.B = Hin;
+    g.sbk = mlp_in(l);
+    g.sbn = 1;
+    g.C = s->gr + s->offW[l];
+    g.ldc = mlp_in(l);
+    if ((e = gemm(g, st)) != cudaSuccess) return e;
+    k_colsum<<<mlp_out(l), 256, 0, st>>>(B, mlp_out(l), dZf, s->gr + s->offb[l]);
+    if (l == 0) break;
+    // dH[b][in] = sum_out dZ[b][out] W[out][in]
+    GemmArgs h{};
+    h.M = (int)B;
+    h.N = mlp_in(l);
+    h.K = mlp_out(l);
+    h.A = dZb;
+    h.sam = mlp_out(l);
+    h.sak = 1;
+    h.B = s->wb + s->offW[l];
+    h.sbk = mlp_in(l);
+    h.sbn = 1;
+    h.C = s->dHf;
+    h.ldc = mlp_in(l);
+    if ((e = gemm(h, st)) != cudaSuccess) return e;
+    const long cnt = B * kMlpHid;
+    k_gelu_back<<<std::min<long>((cnt + 255) / 256, 4096), 256, 0, st>>>(cnt, s->dHf, s->Z[l - 1], s->dZf,
+                                                                         s->dHb);
+    dZb = s->dHb;
+    dZf = s->dZf;
+  }
+  return cudaGetLastError();
+}
+
+std::string surrogate_grad(Surrogate* s, long n, const __nv_bfloat16* x, const float* y, float* grads_host,
+                           double* loss, cudaStream_t st) {
+  std::string e = ensure_act(s, n);
+  if (!e.empty()) return e;
+  cudaMemsetAsync(s->d_loss, 0, sizeof(double), st);
+  if ((e = ck(backward(s, n, x, y, st), "backward")).size()) return e;
+  if (grads_host) cudaMemcpyAsync(grads_host, s->gr, s->n_params * 4, cudaMemcpyDeviceToHost, st);
+  if (loss) cudaMemcpyAsync(loss, s->d_loss, sizeof(double), cudaMemcpyDeviceToHost, st);
+  return ck(cudaStreamSynchronize(st), "grad");
+}
+
+std::string surrogate_train(Surrogate* s, long n, const __nv_bfloat16* x, const float* y, int epochs, int batch,
+                            float lr, unsigned long long seed, float* loss_per_epoch, cudaStream_t st) {
+  if (n < batch || batch < 64 || (batch % 64)) return "need n >= batch, batch a multiple of 64";
+  std::string e = ensure_act(s, batch);
+  if (!e.empty()) return e;
+  std::vector<int> perm((size_t)n);
+  for (long i = 0; i < n; ++i) perm[i] = (int)i;
+  std::mt19937_64 rng(seed);
+  int* d_perm = nullptr;
+  if ((e = ck(cudaMalloc(&d_perm, n * 4), "alloc perm")).size()) return e;
+  __nv_bfloat16* Xb = nullptr;
+  if ((e = ck(cudaMalloc(&Xb, (long)batch * kMlpInPad * 2), "alloc batch")).size()) {
+    cudaFree(d_perm);
+    return e;
+  }
+  const long steps = n / batch;
+  for (int ep = 0; ep < epochs; ++ep) {
+    std::shuffle(perm.begin(), perm.end(), rng);
+    cudaMemcpyAsync(d_perm, perm.data(), n * 4, cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(s->d_loss, 0, sizeof(double), st);
+    for (long it = 0; it < steps; ++it) {
+      k_gather_rows<<<(batch + 255) / 256, 256, 0, st>>>(batch, d_perm + it * batch, x, y, Xb, s->Yb);
+      cudaError_t ce = backward(s, batch, Xb, s->Yb, st);
+      if (ce != cudaSuccess) {
+        cudaFree(d_perm);
+        cudaFree(Xb);
+        return ck(ce, "train step");
+      }
+      s->step += 1;
+      const float b1 = 0.9f, b2 = 0.999f;
+      const float bc1 = 1.f - std::pow(b1, (float)s->step), bc2 = 1.f - std::pow(b2, (float)s->step);
+      k_adam<<<64, 256, 0, st>>>(s->n_params, s->w, s->gr, s->m, s->v, s->wb, lr, b1, b2, 1e-8f, bc1, bc2);
+    }
+    double L = 0.0;
+    cudaMemcpyAsync(&L, s->d_loss, sizeof(double), cudaMemcpyDeviceToHost, st);
+    if ((e = ck(cudaStreamSynchronize(st), "train epoch")).size()) {
+      cudaFree(d_perm);
+      cudaFree(Xb);
+      return e;
+    }
+    if (loss_per_epoch) loss_per_epoch[ep] = (float)(L / (double)steps);
+  }
+  cudaFree(d_perm);
+  cudaFree(Xb);
+  return "";
+}
+
+std::string surrogate_prepare(Surrogate* s, long n, long ld, double dt, const double* dt_cells, const double* T,
+                              const double* rho, const double* Y, const double* Y_prod, const double* T_after,
+                              float hull_margin, __nv_bfloat16* x, float* y, cudaStream_t st) {
+  if (n <= 0) return "no training states";
+  float *xraw = nullptr, *yraw = nullptr;
+  double* stats = nullptr;
+  std::string e;
+  if ((e = ck(cudaMalloc(&xraw, n * kMlpIn * 4), "alloc raw features")).size()) return e;
+  if ((e = ck(cudaMalloc(&yraw, n * kMlpOut * 4), "alloc raw targets")).size()) { cudaFree(xraw); return e; }
+  if ((e = ck(cudaMalloc(&stats, (kMlpIn + kMlpOut) * 4 * 8), "alloc stats")).size()) {
+    cudaFree(xraw); cudaFree(yraw); return e;
+  }
+  const int grid = (int)std::min<long>((n + 255) / 256, 148 * 16);
+  k_features<<<grid, 256, 0, st>>>(n, ld, dt, dt_cells, T, rho, Y, s->d_norm, xraw, nullptr);
+  k_targets<<<grid, 256, 0, st>>>(n, ld, dt, dt_cells, T, rho, Y_prod, T_after, yraw);
+  k_colstats<<<kMlpIn, 1024, 0, st>>>(n, kMlpIn, xraw, stats);
+  k_colstats<<<kMlpOut, 1024, 0, st>>>(n, kMlpOut, yraw, stats + kMlpIn * 4);
+  std::vector<double> hs((kMlpIn + kMlpOut) * 4);
+  cudaMemcpyAsync(hs.data(), stats, hs.size() * 8, cudaMemcpyDeviceToHost, st);
+  if ((e = ck(cudaStreamSynchronize(st), "training statistics")).empty()) {
+    MlpNorm nm{};
+    for (int j = 0; j < kMlpIn; ++j) {
+      nm.x_mu[j] = (float)hs[j * 4 + 0];
+      nm.x_sd[j] = (float)std::max(hs[j * 4 + 1], 1e-12);
+      nm.x_min[j] = (float)hs[j * 4 + 2];
+      nm.x_max[j] = (float)hs[j * 4 + 3];
+    }
+    for (int j = 0; j < kMlpOut; ++j) nm.y_sd[j] = (float)std::max(hs[(kMlpIn + j) * 4 + 1], 1e-30);
+    nm.hull_margin = hull_margin;
+    e = surrogate_set_norm(s, nm);
+    if (e.empty()) {
+      k_standardize<<<grid, 256, 0, st>>>(n, xraw, yraw, s->d_norm, x, y);
+      e = ck(cudaStreamSynchronize(st), "standardize");
+    }
+  }
+  cudaFree(xraw);
+  cudaFree(yraw);
+  cudaFree(stats);
+  return e;
+}
+
+cudaError_t surrogate_step(Surrogate* s, const StepArgs& a, const LaunchCfg& cfg, int* queue,
+                           unsigned long long* counters, cudaStream_t st, const FallbackFn& fallback) {
+  (void)cfg;
+  (void)queue;
+  if (!ensure_infer(s, a.n).empty() || !ensure_gate(s, a.n).empty()) return cudaErrorMemoryAllocation;
+  const long n = a.n;
+  k_features<<<std::min<long>((n + 255) / 256, 148 * 16), 256, 0, st>>>(n, a.ld, a.dt, a.dt_cells, a.T, a.rho, a.Y,
+                                                                      s->d_norm, nullptr, s->iX);
+  cudaError_t e = forward_infer(s, n, s->iX, s->iO, st);
+  if (e != cudaSuccess) return e;
+  k_gate<<<std::min<long>((n + 255) / 256, 148 * 16), 256, 0, st>>>(a, s->iO, s->d_norm, s->gate, s->flag,
+                                                                  counters);
+  const int nb = (int)((n + kCompactBlock - 1) / kCompactBlock);
+  k_flag_count<<<nb, kCompactBlock, 0, st>>>(n, s->flag, s->block_count);
+  k_scan_counts<<<1, 1024, 0, st>>>(nb, s->block_count, s->block_off, s->n_list, counters);
+  k_compact<<<nb, kCompactBlock, 0, st>>>(n, s->flag, s->block_off, s->list);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  StepArgs fa = a;
+  fa.cell_list = s->list;
+  fa.n_list_dev = s->n_list;
+  fa.n_list = (int)n;  // upper bound for the grid; the kernel reads the device count
+  return fallback(fa, st);
 }
 
 }  // namespace nrg

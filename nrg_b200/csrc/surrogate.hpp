@@ -2,11 +2,13 @@
 #pragma once
 
 #include <functional>
+#include <string>
 
 #include <cuda_runtime.h>
 
 #include "chem_device.cuh"
 #include "chem_kernels.hpp"
+#include "mlp.cuh"
 
 namespace nrg {
 
@@ -18,9 +20,38 @@ Surrogate* surrogate_create(const DevMech& dm);
 void surrogate_destroy(Surrogate* s);
 bool surrogate_ready(const Surrogate* s);
 
-// Enqueues gate + inference + compaction + FP64 fallback for the cells that
-// fail the gate.  counters[6] / [7] receive surrogate / fallback cell counts.
+// Enqueues features -> MLP -> gate/outputs -> compaction -> FP64 fallback
+// on the cells the gate rejects.  counters[6] / [7] receive surrogate /
+// fallback cell counts.
 cudaError_t surrogate_step(Surrogate* s, const StepArgs& a, const LaunchCfg& cfg, int* queue,
                            unsigned long long* counters, cudaStream_t st, const FallbackFn& fallback);
+
+// ---- training / inspection (device pointers unless stated)
+std::string surrogate_init(Surrogate* s, unsigned long long seed, cudaStream_t st);
+std::string surrogate_set_norm(Surrogate* s, const MlpNorm& norm);
+MlpNorm surrogate_get_norm(const Surrogate* s);
+// flattened fp32 parameters, per layer W[out][in_pad] then b[out]
+int surrogate_param_count();
+std::string surrogate_get_params(Surrogate* s, float* host, cudaStream_t st);
+std::string surrogate_set_params(Surrogate* s, const float* host, cudaStream_t st);
+// raw features (n x 12 fp32) and standardised padded bf16 features (n x 16)
+std::string surrogate_features(Surrogate* s, long n, long ld, double dt, const double* dt_cells,
+                               const double* T, const double* rho, const double* Y, float* xraw,
+                               __nv_bfloat16* x, cudaStream_t st);
+// network outputs (n x 16 fp32, normalised units) for bf16 features
+std::string surrogate_forward(Surrogate* s, long n, const __nv_bfloat16* x, float* out, cudaStream_t st);
+// gradient of the mean squared error over one batch (no update)
+std::string surrogate_grad(Surrogate* s, long n, const __nv_bfloat16* x, const float* y, float* grads_host,
+                           double* loss, cudaStream_t st);
+// Adam training over n samples; loss_per_epoch (host) may be null
+std::string surrogate_train(Surrogate* s, long n, const __nv_bfloat16* x, const float* y, int epochs, int batch,
+                            float lr, unsigned long long seed, float* loss_per_epoch, cudaStream_t st);
+// raw features and targets of integrated training states, fitted
+// standardisation and training hull, standardised bf16 x (n x 16) and y (n x 10)
+std::string surrogate_prepare(Surrogate* s, long n, long ld, double dt, const double* dt_cells, const double* T,
+                              const double* rho, const double* Y, const double* Y_prod, const double* T_after,
+                              float hull_margin, __nv_bfloat16* x, float* y, cudaStream_t st);
+void surrogate_set_ready(Surrogate* s, bool ready);
+void surrogate_set_gate(Surrogate* s, double elem_tol, double dT_tol, double dT_max);
 
 }  // namespace nrg

@@ -1,0 +1,165 @@
+"""Training and use of the gated chemistry surrogate (BF16 MLP + FP64 fallback).
+
+The learned part has no counterpart in the reference.  Training pairs are
+produced on the GPU by the FP64 integrator from the 1,048,576-cell mixed
+distribution (T ~ U[800, 2600] K, p ~ U[0.5, 5] atm) with dt ~ log-U[1e-7,
+1e-5] s; the network is trained by the library's own BF16 tensor-core
+forward/backward kernels with Adam.  All arithmetic runs in libnrg_chem.so;
+torch only provides device buffers.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import time
+
+import numpy as np
+
+from . import fields
+from .chemistry import ChemicalKineticsSolver, _check, _ptr, lib
+
+MODEL_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "models")
+DEFAULT_MODEL = os.path.join(MODEL_DIR, "keromnes_surrogate.bin")
+
+
+def param_count() -> int:
+    return lib().nrg_surrogate_param_count()
+
+
+def layer_shapes():
+    """(out, in_padded) of the five layers."""
+    return [(128, 16), (128, 128), (128, 128), (128, 128), (16, 128)]
+
+
+def unflatten(p: np.ndarray):
+    out, off = [], 0
+    for o, i in layer_shapes():
+        W = p[off:off + o * i].reshape(o, i)
+        off += o * i
+        b = p[off:off + o]
+        off += o
+        out.append((W, b))
+    return out
+
+
+class Surrogate:
+    """Owns the MLP state of a ChemicalKineticsSolver handle."""
+
+    def __init__(self, solver: ChemicalKineticsSolver):
+        self.solver = solver
+        self.h = solver.handle
+
+    def init(self, seed: int = 0) -> None:
+        _check(lib().nrg_surrogate_init(self.h, ctypes.c_ulonglong(seed)), self.h)
+
+    def params(self) -> np.ndarray:
+        p = np.zeros(param_count(), np.float32)
+        _check(lib().nrg_surrogate_get_params(self.h, p.ctypes.data), self.h)
+        return p
+
+    def set_params(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, np.float32)
+        _check(lib().nrg_surrogate_set_params(self.h, p.ctypes.data), self.h)
+
+    def norm(self) -> np.ndarray:
+        v = np.zeros(lib().nrg_surrogate_norm_count(), np.float32)
+        _check(lib().nrg_surrogate_get_norm(self.h, v.ctypes.data), self.h)
+        return v
+
+    def set_norm(self, v: np.ndarray) -> None:
+        v = np.ascontiguousarray(v, np.float32)
+        _check(lib().nrg_surrogate_set_norm(self.h, v.ctypes.data), self.h)
+
+    def set_gate(self, elem_tol=1e-6, dT_tol=0.5, dT_max=50.0) -> None:
+        _check(lib().nrg_surrogate_set_gate(self.h, elem_tol, dT_tol, dT_max), self.h)
+
+    def enable(self, on: bool = True) -> None:
+        _check(lib().nrg_surrogate_enable(self.h, int(on)), self.h)
+
+    def save(self, path: str) -> None:
+        os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+        _check(lib().nrg_surrogate_save(self.h, path.encode()), self.h)
+
+    def load(self, path: str) -> None:
+        _check(lib().nrg_surrogate_load(self.h, path.encode()), self.h)
+
+    # ---- device-level pieces (torch tensors as buffers)
+    def forward(self, x_bf16):
+        import torch
+        out = torch.empty((x_bf16.shape[0], 16), dtype=torch.float32, device=x_bf16.device)
+        torch.cuda.synchronize()
+        _check(lib().nrg_surrogate_forward(self.h, x_bf16.shape[0], _ptr(x_bf16), _ptr(out)), self.h)
+        return out
+
+    def grad(self, x_bf16, y):
+        import torch
+        g = np.zeros(param_count(), np.float32)
+        loss = ctypes.c_double()
+        torch.cuda.synchronize()
+        _check(lib().nrg_surrogate_grad(self.h, x_bf16.shape[0], _ptr(x_bf16), _ptr(y), g.ctypes.data,
+                                        ctypes.byref(loss)), self.h)
+        return g, loss.value
+
+    def train(self, x_bf16, y, epochs=10, batch=4096, lr=1e-3, seed=0):
+        import torch
+        losses = np.zeros(epochs, np.float32)
+        torch.cuda.synchronize()
+        _check(lib().nrg_surrogate_train(self.h, x_bf16.shape[0], _ptr(x_bf16), _ptr(y), epochs, batch,
+                                         ctypes.c_float(lr), ctypes.c_ulonglong(seed), losses.ctypes.data), self.h)
+        return losses
+
+    def features(self, f: fields.Field, xraw=True):
+        import torch
+        dev = torch.device("cuda")
+        T, rho, Y = (torch.tensor(a, device=dev) for a in (f.T, f.rho, f.Y))
+        dtc = None if f.dt_cells is None else torch.tensor(f.dt_cells, device=dev)
+        xr = torch.empty((f.n, 12), dtype=torch.float32, device=dev) if xraw else None
+        x = torch.empty((f.n, 16), dtype=torch.bfloat16, device=dev)
+        torch.cuda.synchronize()
+        _check(lib().nrg_surrogate_features(self.h, f.n, f.n, float(f.dt if f.dt == f.dt else 1e-6), _ptr(dtc),
+                                            _ptr(T), _ptr(rho), _ptr(Y), _ptr(xr), _ptr(x)), self.h)
+        return x, xr
+
+
+def training_pairs(solver: ChemicalKineticsSolver, W: np.ndarray, n: int, seed: int = 3,
+                   hull_margin: float = 0.02):
+    """Integrates n config-3 states with their own dt (FP64 integrator) and
+    returns standardised (x_bf16, y) device tensors plus timing."""
+    import torch
+    f = fields.config3_pairs(W, n, seed=seed)
+    # neighbouring lanes take similar paths when states are sorted by (dt, T)
+    order = np.lexsort((f.T, np.round(np.log10(f.dt_cells) * 8)))
+    f = fields.Field(f.name, f.T[order], f.rho[order], f.p[order], np.ascontiguousarray(f.Y[:, order]), f.dt,
+                     f.shape, f.dt_cells[order])
+    dev = torch.device("cuda")
+    T, rho, Y = (torch.tensor(a, device=dev) for a in (f.T, f.rho, f.Y))
+    dtc = torch.tensor(f.dt_cells, device=dev)
+    Yp, Yp2 = torch.zeros_like(Y), torch.zeros_like(Y)
+    Ef, Ta = torch.zeros_like(T), torch.zeros_like(T)
+    st = torch.zeros(n, dtype=torch.uint8, device=dev)
+    t0 = time.perf_counter()
+    stats = solver.integrate(1.0, T, rho, Y, Yp, Yp2, Ef, dt_cells=dtc, T_after=Ta, status=st)
+    t_int = time.perf_counter() - t0
+    x = torch.empty((n, 16), dtype=torch.bfloat16, device=dev)
+    y = torch.empty((n, 10), dtype=torch.float32, device=dev)
+    torch.cuda.synchronize()
+    _check(lib().nrg_surrogate_prepare(solver.handle, n, n, 1.0, _ptr(dtc), _ptr(T), _ptr(rho), _ptr(Y), _ptr(Yp),
+                                       _ptr(Ta), ctypes.c_float(hull_margin), _ptr(x), _ptr(y)), solver.handle)
+    return x, y, {"integrate_s": t_int, "integrator_stats": stats, "n": n}
+
+
+def train_default(solver: ChemicalKineticsSolver, W: np.ndarray, n_train: int = 4_000_000, epochs: int = 20,
+                  batch: int = 4096, lr: float = 1e-3, seed: int = 0, gate=(1e-6, 0.5, 50.0)) -> dict:
+    """Full recipe: pairs -> Adam training -> gate settings -> enabled."""
+    sur = Surrogate(solver)
+    t0 = time.perf_counter()
+    x, y, info = training_pairs(solver, W, n_train)
+    sur.init(seed)
+    t1 = time.perf_counter()
+    losses = sur.train(x, y, epochs=epochs, batch=batch, lr=lr, seed=seed + 1)
+    t2 = time.perf_counter()
+    sur.set_gate(*gate)
+    sur.enable(True)
+    info.update({"pairs_s": t1 - t0, "train_s": t2 - t1, "losses": losses.tolist(), "epochs": epochs,
+                 "batch": batch, "lr": lr})
+    return info
