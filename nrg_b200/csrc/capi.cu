@@ -241,8 +241,12 @@ cudaError_t enqueue_step(nrg_chem* h, const StepArgs& a, cudaStream_t s) {
 
 // Runs the step on stream s, through a CUDA graph when enabled.
 int run_step(nrg_chem* h, const StepArgs& a, cudaStream_t s, nrg_chem_stats* stats) {
-  if (h->mode == NRG_MODE_SURROGATE && !nrg::surrogate_ready(h->sur))
-    return fail(h, NRG_ERR_STATE, "surrogate mode selected but no trained model is loaded");
+  if (h->mode == NRG_MODE_SURROGATE) {
+    if (!nrg::surrogate_ready(h->sur))
+      return fail(h, NRG_ERR_STATE, "surrogate mode selected but no trained model is loaded");
+    const std::string e = nrg::surrogate_reserve(h->sur, a.n);
+    if (!e.empty()) return fail(h, NRG_ERR_CUDA, e);
+  }
   CK(h, cudaEventRecord(h->ev0, s));
   if (h->use_graph) {
     cudaGraph_t g = nullptr;

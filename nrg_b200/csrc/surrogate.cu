@@ -857,11 +857,18 @@ std::string surrogate_prepare(Surrogate* s, long n, long ld, double dt, const do
   return e;
 }
 
+std::string surrogate_reserve(Surrogate* s, long n) {
+  std::string e = ensure_infer(s, n);
+  if (!e.empty()) return e;
+  return ensure_gate(s, n);
+}
+
 cudaError_t surrogate_step(Surrogate* s, const StepArgs& a, const LaunchCfg& cfg, int* queue,
                            unsigned long long* counters, cudaStream_t st, const FallbackFn& fallback) {
   (void)cfg;
   (void)queue;
-  if (!ensure_infer(s, a.n).empty() || !ensure_gate(s, a.n).empty()) return cudaErrorMemoryAllocation;
+  // buffers are reserved by surrogate_reserve before any graph capture
+  if (a.n > s->icap || a.n > s->gcap) return cudaErrorMemoryAllocation;
   const long n = a.n;
   k_features<<<std::min<long>((n + 255) / 256, 148 * 16), 256, 0, st>>>(n, a.ld, a.dt, a.dt_cells, a.T, a.rho, a.Y,
                                                                       s->d_norm, nullptr, s->iX);

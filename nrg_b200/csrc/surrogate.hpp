@@ -20,6 +20,10 @@ Surrogate* surrogate_create(const DevMech& dm);
 void surrogate_destroy(Surrogate* s);
 bool surrogate_ready(const Surrogate* s);
 
+// Allocates the inference and compaction buffers for n cells (call outside
+// stream capture).
+std::string surrogate_reserve(Surrogate* s, long n);
+
 // Enqueues features -> MLP -> gate/outputs -> compaction -> FP64 fallback
 // on the cells the gate rejects.  counters[6] / [7] receive surrogate /
 // fallback cell counts.
