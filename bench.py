@@ -135,7 +135,7 @@ def flop_model(tables: dict, mode: str) -> dict:
 
 def algorithmic_flops(st: dict, fm: dict) -> float:
     st = {k: float(v) for k, v in st.items()}
-    return (st["cells_active"] * fm["setup"] + st["rhs_evals"] * fm["rhs"] + st["jacobians"] * fm["jac"]
+    return ((st["cells_active"] - st.get("cells_surrogate", 0.0)) * fm["setup"] + st["rhs_evals"] * fm["rhs"] + st["jacobians"] * fm["jac"]
             + st["solves"] * fm["solve"] + st["steps"] * fm["step"])
 
 
@@ -212,6 +212,9 @@ def run_reference(args):
 
 
 # ------------------------------------------------------------------ our arm
+MLP_FLOPS_PER_CELL = 2 * (12 * 128 + 3 * 128 * 128 + 128 * 10)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -227,55 +230,97 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     from nrg_b200 import fields as F, keromnes_paths
     from nrg_b200.chemistry import ChemicalKineticsSolver, DataManager, fp64_peak_tflops, mechanism_tables
+    from nrg_b200.surrogate import DEFAULT_MODEL, Surrogate, train_default
     decks = keromnes_paths()
     tables = mechanism_tables(*decks)
     W = tables["molar_mass"]
     field = F.config4(W, n_side=args.n_side)
     n = field.n
-    mode = args.mode
-    solver = ChemicalKineticsSolver(None, *decks, mode="fast")
-    if mode == "auto":
-        mode = "fast"
-    solver.set_mode(mode)
     dev = torch.device("cuda", local)
+    solver = ChemicalKineticsSolver(None, *decks, mode="fast")
     T, rho, Y = (torch.tensor(a, device=dev) for a in (field.T, field.rho, field.Y))
-    Yp, Yp2 = torch.zeros_like(Y), torch.zeros_like(Y)
-    Ef = torch.zeros_like(T)
-    # launch shape: autotuned on a strided sample of the field
-    samp = F.slice_field(field, 131072, stride=32, offset=3)
+
+    # launch shape of the FP64 integrator: autotuned on a contiguous block of
+    # rows (neighbouring cells take similar integration paths)
+    nsamp = min(n, 262144)
+    samp = F.slice_field(field, nsamp, stride=1, offset=(n - nsamp) // 2)
     sT, sr, sY = (torch.tensor(a, device=dev) for a in (samp.T, samp.rho, samp.Y))
     solver.autotune(samp.dt, sT, sr, sY, torch.zeros_like(sY), torch.zeros_like(sY), torch.zeros_like(sT))
     launch = solver.get_launch()
     del sT, sr, sY
+
+    mode = args.mode
+    train_info = None
+    if mode in ("auto", "surrogate"):
+        sur = Surrogate(solver)
+        if os.path.exists(DEFAULT_MODEL):
+            sur.load(DEFAULT_MODEL)
+            sur.set_gate()
+            train_info = {"model": os.path.relpath(DEFAULT_MODEL, ROOT), "trained": "loaded"}
+        else:
+            info = train_default(solver, W)
+            sur.save(DEFAULT_MODEL)
+            train_info = {"trained": "in this run", "pairs": info["n"], "epochs": info["epochs"],
+                          "pairs_s": info["pairs_s"], "train_s": info["train_s"], "final_loss": info["losses"][-1]}
+        mode = "surrogate"
     peak_fp64 = fp64_peak_tflops()
 
-    def step():
-        return solver.step_device(field.dt, T, rho, Y, Yp, Yp2, Ef)
+    def make_out():
+        return (torch.zeros_like(Y), torch.zeros_like(Y), torch.zeros_like(T), torch.zeros_like(T),
+                torch.zeros(n, dtype=torch.uint8, device=dev))
 
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    stats = []
-    with ClockSampler(local) as clk:
+    def time_arm(arm_mode):
+        Yp, Yp2, Ef, Ta, st = make_out()
+        solver.set_mode(arm_mode)
+        for _ in range(args.warmup):
+            solver.step_device(field.dt, T, rho, Y, Yp, Yp2, Ef, T_after=Ta, status=st)
         torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(args.steps):
-            stats.append(step())
-        e1.record()
-        torch.cuda.synchronize()
-    el_ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([el_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        el_ms = float(t.item())
-        dist.barrier()
-    value = args.steps * n * world / (el_ms * 1e-3)
+        if world > 1:
+            dist.barrier()
+        stats = []
+        with ClockSampler(local) as clk:
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(args.steps):
+                stats.append(solver.step_device(field.dt, T, rho, Y, Yp, Yp2, Ef, T_after=Ta, status=st))
+            e1.record()
+            torch.cuda.synchronize()
+        el = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([el], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            el = float(t.item())
+        # one untimed step with per-phase events for the roofline
+        solver.set_timing(True)
+        ph = solver.step_device(field.dt, T, rho, Y, Yp, Yp2, Ef, T_after=Ta, status=st)
+        solver.set_timing(False)
+        return el, stats, ph, clk.summary(), (Yp, Yp2, Ef, Ta, st)
 
-    # end-to-end: the drop-in host path (Fortran-layout host arrays with a
-    # ghost layer, copies in both directions inside the timed region)
+    el_plain, st_plain, ph_plain, clk_plain, out_plain = time_arm("fast")
+    if mode == "surrogate":
+        el, stats, ph, clocks, out = time_arm("surrogate")
+    else:
+        solver.set_mode(mode)
+        el, stats, ph, clocks, out = (el_plain, st_plain, ph_plain, clk_plain, out_plain) if mode == "fast" \
+            else time_arm(mode)
+    value = args.steps * n * world / (el * 1e-3)
+    plain_value = args.steps * n * world / (el_plain * 1e-3)
+
+    # accuracy of the measured path against the plain FP64 integrator
+    acc = None
+    if mode != "fast":
+        Yp_p, _, _, Ta_p, st_p = (x.cpu().numpy() for x in out_plain)
+        Yp_s, _, _, Ta_s, st_s = (x.cpu().numpy() for x in out)
+        act = st_p != 0
+        dT = np.abs(Ta_s - Ta_p)[act]
+        dYk = (np.abs(Yp_s - Yp_p) * field.dt / field.rho[None, :])[:, act]
+        acc = {"vs": "plain FP64 GPU integrator (same inputs)", "active_cells": int(act.sum()),
+               "max_abs_dT_K": float(dT.max()), "p99_abs_dT_K": float(np.percentile(dT, 99)),
+               "max_abs_dY": float(dYk.max()), "max_abs_dY_per_species": [float(v) for v in dYk.max(1)],
+               "accepted_cells": int((st_s == 5).sum()), "fallback_cells": int(ph["cells_fallback"]),
+               "fallback_fraction_of_active": float(ph["cells_fallback"]) / max(1, int(act.sum()))}
+
     e2e = None
     if not args.no_e2e:
         nx, ny = field.shape
@@ -287,8 +332,13 @@ def main():
         m.interior(m.fields["density"])[...] = field.rho.reshape(ny, nx).T[:, :, None]
         for k in range(9):
             m.interior(m.fields["specie_mass_fraction"][k])[...] = field.Y[k].reshape(ny, nx).T[:, :, None]
-        host = ChemicalKineticsSolver(m, *decks, mode=mode)
-        host.set_launch(**{k: v for k, v in launch.items()})
+        host = ChemicalKineticsSolver(m, *decks, mode="fast")
+        host.set_launch(**launch)
+        if mode == "surrogate":
+            hs = Surrogate(host)
+            hs.load(DEFAULT_MODEL)
+            hs.set_gate()
+        host.set_mode(mode)
         host.solve_chemical_kinetics(field.dt)
         if world > 1:
             dist.barrier()
@@ -307,17 +357,29 @@ def main():
 
     if rank == 0:
         st = stats[-1]
-        fm = flop_model(tables, mode)
-        flops = algorithmic_flops(st, fm)
-        kern_ms = float(np.median([s["device_ms"] for s in stats]))
-        achieved = flops / (kern_ms * 1e-3) / 1e12
         peaks = load_peaks()
+        fm = flop_model(tables, "fast")
+        phases = {"mlp_ms": ph["phase_ms"][0], "gate_ms": ph["phase_ms"][1], "integrator_ms": ph["phase_ms"][2]}
+        integ_flops = algorithmic_flops(ph, fm)
+        integ_tf = integ_flops / max(phases["integrator_ms"], 1e-9) * 1e-9
+        if mode == "surrogate" and phases["mlp_ms"] > phases["integrator_ms"]:
+            mlp_tf = MLP_FLOPS_PER_CELL * n / max(phases["mlp_ms"], 1e-9) * 1e-9
+            roof = {"bound": "tensor", "achieved": mlp_tf, "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
+                    "frac": mlp_tf / peaks["bf16_tflops"], "traffic": None, "kernel": "MLP layers (BF16)",
+                    "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)"}
+        else:
+            roof = {"bound": "fp64", "achieved": integ_tf, "peak": peak_fp64, "unit": "TFLOP/s",
+                    "frac": integ_tf / peak_fp64, "traffic": None,
+                    "kernel": "FP64 BDF integrator (" + launch["kernel"] + ")",
+                    "peak_source": "measured live: dependent-FMA FP64 probe (MEASURED_PEAKS.json has no FP64 figure)",
+                    "flops_per_launch": integ_flops, "flop_model": fm}
         cpu = cpu_baseline(field, W, decks, args.cpu_seconds)
-        clocks = clk.summary()
+        launches = 11 if mode == "surrogate" else 1
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": el_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "warmup": args.warmup, "ms_per_step": el / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64+bf16" if mode == "surrogate" else "f64",
+            "data": "synthetic",
             "config": {"workload": f"flame field {args.n_side}x{args.n_side} ({n:,} cells), dt=1e-6 s, p=1 atm, "
                                    f"KEROMNES H2/air (9 species, 24 reactions)",
                        "path": {"fast": "plain FP64 integrator, analytic Jacobian",
@@ -325,17 +387,16 @@ def main():
                                 "mixed": "FP32 LU + FP64 residual/refinement",
                                 "surrogate": "BF16 MLP surrogate + gated FP64 fallback"}[mode],
                        "launch": launch, "l2": "inputs (370 MB) larger than L2; no flush",
-                       "active_cells": st["cells_active"], "cells_fallback": st["cells_fallback"],
-                       "cells_surrogate": st["cells_surrogate"],
-                       "steps_per_active_cell": st["steps"] / max(1, st["cells_active"])},
-            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak_fp64, "unit": "TFLOP/s",
-                         "frac": achieved / peak_fp64, "traffic": None,
-                         "kernel": "k_chem_warp (warp-per-cell BDF integrator)" if launch["kernel"] == "warp_queue" else "k_chem_queue/k_chem_plain (thread-per-cell BDF integrator)",
-                         "peak_source": "measured live: dependent-FMA FP64 probe (MEASURED_PEAKS.json has no FP64 figure)",
-                         "flops_per_step": flops, "flop_model": fm},
+                       "active_cells": int(ph["cells_active"])},
+            "plain_fp64": {"value": plain_value, "ms_per_step": el_plain / args.steps,
+                           "ratio_surrogate_over_plain": value / plain_value},
+            "accuracy": acc,
+            "surrogate_model": train_info,
+            "phases_ms": phases,
+            "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": e2e,
-            "gpu_launches": args.steps * 1,
+            "gpu_launches": args.steps * launches,
             "clocks": clocks,
             "peaks_file": {k: peaks.get(k) for k in ("hbm_gbs", "bf16_tflops", "bf16_tflops_sustained")},
         }

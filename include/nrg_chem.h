@@ -86,6 +86,9 @@ typedef struct {
   long long cells_fallback;  /* active cells sent to the FP64 integrator by the gate */
   long long steps, rhs_evals, jacobians, solves;
   double device_ms;          /* device time of the step (CUDA events) */
+  /* per-phase device time when phase timing is on (nrg_chem_set_timing):
+   * [0] features + MLP, [1] gate + compaction, [2] FP64 integrator, [3] unused */
+  double phase_ms[4];
 } nrg_chem_stats;
 
 /* Replaces chemical_kinetics_solver_c(manager) (chemical_kinetics_solver.f90:
@@ -137,6 +140,10 @@ NRG_API int nrg_chem_autotune(nrg_chem* h, double time_step, long n, long ld, co
 
 /* Capture the step in a CUDA graph (1) or launch directly (0). */
 NRG_API int nrg_chem_set_graph(nrg_chem* h, int enable);
+
+/* Per-phase CUDA-event timing of the step (stats.phase_ms); launches the step
+ * without a graph while enabled. */
+NRG_API int nrg_chem_set_timing(nrg_chem* h, int enable);
 
 /* Mechanism size and parsed tables (for checks against the reference decks).
  * Arrays may be NULL; sizes follow n_species (N) and n_reactions (R):

@@ -55,10 +55,13 @@ class Stats(ctypes.Structure):
         ("steps", ctypes.c_longlong), ("rhs_evals", ctypes.c_longlong),
         ("jacobians", ctypes.c_longlong), ("solves", ctypes.c_longlong),
         ("device_ms", ctypes.c_double),
+        ("phase_ms", ctypes.c_double * 4),
     ]
 
     def as_dict(self) -> dict:
-        return {k: getattr(self, k) for k, _ in self._fields_}
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["phase_ms"] = list(self.phase_ms)
+        return d
 
 
 # every symbol include/nrg_chem.h declares, with its ctypes signature
@@ -74,6 +77,7 @@ SIGNATURES = {
     "nrg_chem_get_launch": (_I, [_VP] + [ctypes.POINTER(_I)] * 4),
     "nrg_chem_autotune": (_I, [_VP, _D, _L, _L, _VP, _VP, _VP, _VP, _VP, _VP, _VP, ctypes.POINTER(_D)]),
     "nrg_chem_set_graph": (_I, [_VP, _I]),
+    "nrg_chem_set_timing": (_I, [_VP, _I]),
     "nrg_chem_info": (_I, [_VP, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "nrg_chem_tables": (_I, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "nrg_chem_species_name": (_I, [_VP, _I, ctypes.c_char_p, _I]),
@@ -252,6 +256,9 @@ class ChemicalKineticsSolver:
 
     def set_graph(self, enable: bool) -> None:
         _check(lib().nrg_chem_set_graph(self._h, int(enable)), self._h)
+
+    def set_timing(self, enable: bool) -> None:
+        _check(lib().nrg_chem_set_timing(self._h, int(enable)), self._h)
 
     @property
     def handle(self):

@@ -31,6 +31,8 @@ struct nrg_chem {
   int mode = NRG_MODE_FAST;
   LaunchCfg cfg;
   bool use_graph = true;
+  bool timing = false;
+  cudaEvent_t ph[4] = {nullptr, nullptr, nullptr, nullptr};
   int* d_queue = nullptr;
   DevMech* d_mech = nullptr;  // global copy of the tables for kernels that stage them in shared memory
   unsigned long long* d_counters = nullptr;
@@ -231,12 +233,21 @@ cudaError_t enqueue_integrator(nrg_chem* h, const StepArgs& a, const LaunchCfg& 
 cudaError_t enqueue_step(nrg_chem* h, const StepArgs& a, cudaStream_t s) {
   cudaError_t e = cudaMemsetAsync(h->d_counters, 0, sizeof(unsigned long long) * 8, s);
   if (e != cudaSuccess) return e;
-  if (h->mode == NRG_MODE_SURROGATE) return nrg::surrogate_step(h->sur, a, h->cfg, h->d_queue, h->d_counters, s,
-                                                                 [h](const StepArgs& fa, cudaStream_t fs) {
-                                                                   LaunchCfg c = h->cfg;
-                                                                   return enqueue_integrator(h, fa, c, fs);
-                                                                 });
-  return enqueue_integrator(h, a, h->cfg, s);
+  cudaEvent_t* ph = h->timing ? h->ph : nullptr;
+  if (h->mode == NRG_MODE_SURROGATE)
+    return nrg::surrogate_step(h->sur, a, h->cfg, h->d_queue, h->d_counters, s,
+                               [h, ph](const StepArgs& fa, cudaStream_t fs) {
+                                 if (ph) cudaEventRecord(ph[2], fs);
+                                 LaunchCfg c = h->cfg;
+                                 cudaError_t e = enqueue_integrator(h, fa, c, fs);
+                                 if (ph) cudaEventRecord(ph[3], fs);
+                                 return e;
+                               },
+                               ph);
+  if (ph) cudaEventRecord(ph[2], s);
+  cudaError_t e2 = enqueue_integrator(h, a, h->cfg, s);
+  if (ph) cudaEventRecord(ph[3], s);
+  return e2;
 }
 
 // Runs the step on stream s, through a CUDA graph when enabled.
@@ -248,7 +259,10 @@ int run_step(nrg_chem* h, const StepArgs& a, cudaStream_t s, nrg_chem_stats* sta
     if (!e.empty()) return fail(h, NRG_ERR_CUDA, e);
   }
   CK(h, cudaEventRecord(h->ev0, s));
-  if (h->use_graph) {
+  if (h->timing) {
+    for (int i = 0; i < 4; ++i) CK(h, cudaEventRecord(h->ph[i], s));
+  }
+  if (h->use_graph && !h->timing) {
     cudaGraph_t g = nullptr;
     CK(h, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = enqueue_step(h, a, s);
@@ -294,6 +308,17 @@ int run_step(nrg_chem* h, const StepArgs& a, cudaStream_t s, nrg_chem_stats* sta
     stats->cells_fallback = (long long)h->h_counters[7];
     if (h->mode == NRG_MODE_SURROGATE) stats->cells_active += stats->cells_surrogate;
     stats->device_ms = ms;
+    if (h->timing) {
+      float p = 0.f;
+      if (h->mode == NRG_MODE_SURROGATE) {
+        cudaEventElapsedTime(&p, h->ev0, h->ph[1]);  // features + MLP (ph[1] = gate start)
+        stats->phase_ms[0] = p;
+        cudaEventElapsedTime(&p, h->ph[1], h->ph[2]);
+        stats->phase_ms[1] = p;
+      }
+      cudaEventElapsedTime(&p, h->ph[2], h->ph[3]);
+      stats->phase_ms[2] = p;
+    }
   }
   return NRG_OK;
 }
@@ -330,7 +355,9 @@ extern "C" int nrg_chem_create(const char* mechanism_path, const char* thermo_pa
       (ce = cudaMalloc(&h->d_counters, sizeof(unsigned long long) * 8)) != cudaSuccess ||
       (ce = cudaMallocHost(&h->h_counters, sizeof(unsigned long long) * 8)) != cudaSuccess ||
       (ce = cudaEventCreate(&h->ev0)) != cudaSuccess || (ce = cudaEventCreate(&h->ev1)) != cudaSuccess ||
-      (ce = cudaEventCreateWithFlags(&h->ev_in, cudaEventDisableTiming)) != cudaSuccess) {
+      (ce = cudaEventCreateWithFlags(&h->ev_in, cudaEventDisableTiming)) != cudaSuccess ||
+      (ce = cudaEventCreate(&h->ph[0])) != cudaSuccess || (ce = cudaEventCreate(&h->ph[1])) != cudaSuccess ||
+      (ce = cudaEventCreate(&h->ph[2])) != cudaSuccess || (ce = cudaEventCreate(&h->ph[3])) != cudaSuccess) {
     std::string msg = std::string("CUDA initialisation failed: ") + cudaGetErrorString(ce);
     nrg_chem_destroy(h);
     return fail(nullptr, NRG_ERR_CUDA, msg);
@@ -363,6 +390,8 @@ extern "C" int nrg_chem_destroy(nrg_chem* h) {
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->ev_in) cudaEventDestroy(h->ev_in);
+  for (int i = 0; i < 4; ++i)
+    if (h->ph[i]) cudaEventDestroy(h->ph[i]);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return NRG_OK;
@@ -401,6 +430,12 @@ extern "C" int nrg_chem_get_launch(nrg_chem* h, int* kernel, int* block, int* gr
 extern "C" int nrg_chem_set_graph(nrg_chem* h, int enable) {
   if (!h) return NRG_ERR_ARG;
   h->use_graph = enable != 0;
+  return NRG_OK;
+}
+
+extern "C" int nrg_chem_set_timing(nrg_chem* h, int enable) {
+  if (!h) return NRG_ERR_ARG;
+  h->timing = enable != 0;
   return NRG_OK;
 }
 

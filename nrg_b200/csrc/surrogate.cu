@@ -864,7 +864,8 @@ std::string surrogate_reserve(Surrogate* s, long n) {
 }
 
 cudaError_t surrogate_step(Surrogate* s, const StepArgs& a, const LaunchCfg& cfg, int* queue,
-                           unsigned long long* counters, cudaStream_t st, const FallbackFn& fallback) {
+                           unsigned long long* counters, cudaStream_t st, const FallbackFn& fallback,
+                           cudaEvent_t* ph) {
   (void)cfg;
   (void)queue;
   // buffers are reserved by surrogate_reserve before any graph capture
@@ -874,6 +875,7 @@ cudaError_t surrogate_step(Surrogate* s, const StepArgs& a, const LaunchCfg& cfg
                                                                       s->d_norm, nullptr, s->iX);
   cudaError_t e = forward_infer(s, n, s->iX, s->iO, st);
   if (e != cudaSuccess) return e;
+  if (ph) cudaEventRecord(ph[1], st);
   k_gate<<<std::min<long>((n + 255) / 256, 148 * 16), 256, 0, st>>>(a, s->iO, s->d_norm, s->gate, s->flag,
                                                                   counters);
   const int nb = (int)((n + kCompactBlock - 1) / kCompactBlock);

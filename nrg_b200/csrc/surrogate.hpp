@@ -27,8 +27,11 @@ std::string surrogate_reserve(Surrogate* s, long n);
 // Enqueues features -> MLP -> gate/outputs -> compaction -> FP64 fallback
 // on the cells the gate rejects.  counters[6] / [7] receive surrogate /
 // fallback cell counts.
+// ph (may be null): events recorded at phase boundaries (ph[1] gate start;
+// the fallback callback records ph[2] / ph[3] around the integrator).
 cudaError_t surrogate_step(Surrogate* s, const StepArgs& a, const LaunchCfg& cfg, int* queue,
-                           unsigned long long* counters, cudaStream_t st, const FallbackFn& fallback);
+                           unsigned long long* counters, cudaStream_t st, const FallbackFn& fallback,
+                           cudaEvent_t* ph);
 
 // ---- training / inspection (device pointers unless stated)
 std::string surrogate_init(Surrogate* s, unsigned long long seed, cudaStream_t st);
