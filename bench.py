@@ -134,7 +134,7 @@ def flop_model(tables: dict, mode: str) -> dict:
 
 
 def algorithmic_flops(st: dict, fm: dict) -> float:
-    st = {k: float(v) for k, v in st.items()}
+    st = {k: float(v) for k, v in st.items() if not isinstance(v, (list, tuple))}
     return ((st["cells_active"] - st.get("cells_surrogate", 0.0)) * fm["setup"] + st["rhs_evals"] * fm["rhs"] + st["jacobians"] * fm["jac"]
             + st["solves"] * fm["solve"] + st["steps"] * fm["step"])
 

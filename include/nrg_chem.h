@@ -183,10 +183,12 @@ NRG_API int nrg_surrogate_get_norm(nrg_chem* h, float* norm);
 NRG_API int nrg_surrogate_set_norm(nrg_chem* h, const float* norm);
 /* Training arrays from integrated states (Y_prod, T_after from
  * nrg_chem_integrate with the same dt / dt_cells); also fits the feature and
- * target scaling and the training hull (widened by hull_margin of each range). */
+ * target scaling and the training hull (widened by hull_margin of each range);
+ * targets are divided by (dt / 1e-6)^dt_pow before standardisation. */
 NRG_API int nrg_surrogate_prepare(nrg_chem* h, long n, long ld, double dt, const double* dt_cells,
                                   const double* T, const double* rho, const double* Y, const double* Y_prod,
-                                  const double* T_after, float hull_margin, void* x_bf16, float* y);
+                                  const double* T_after, float hull_margin, float dt_pow, void* x_bf16,
+                                  float* y);
 NRG_API int nrg_surrogate_features(nrg_chem* h, long n, long ld, double dt, const double* dt_cells,
                                    const double* T, const double* rho, const double* Y, float* xraw,
                                    void* x_bf16);

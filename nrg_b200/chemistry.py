@@ -90,7 +90,8 @@ SIGNATURES = {
     "nrg_surrogate_set_params": (_I, [_VP, _VP]),
     "nrg_surrogate_get_norm": (_I, [_VP, _VP]),
     "nrg_surrogate_set_norm": (_I, [_VP, _VP]),
-    "nrg_surrogate_prepare": (_I, [_VP, _L, _L, _D, _VP, _VP, _VP, _VP, _VP, _VP, ctypes.c_float, _VP, _VP]),
+    "nrg_surrogate_prepare": (_I, [_VP, _L, _L, _D, _VP, _VP, _VP, _VP, _VP, _VP, ctypes.c_float, ctypes.c_float,
+                                   _VP, _VP]),
     "nrg_surrogate_features": (_I, [_VP, _L, _L, _D, _VP, _VP, _VP, _VP, _VP, _VP]),
     "nrg_surrogate_forward": (_I, [_VP, _L, _VP, _VP]),
     "nrg_surrogate_grad": (_I, [_VP, _L, _VP, _VP, _VP, ctypes.POINTER(_D)]),

@@ -724,7 +724,7 @@ int order_after_legacy(nrg_chem* h) {
   return NRG_OK;
 }
 int sfail(nrg_chem* h, const std::string& e) { return e.empty() ? NRG_OK : fail(h, NRG_ERR_CUDA, e); }
-constexpr int kNormFloats = 4 * nrg::kMlpIn + nrg::kMlpOut + 1;
+constexpr int kNormFloats = 4 * nrg::kMlpIn + nrg::kMlpOut + 2;
 void norm_to_floats(const nrg::MlpNorm& m, float* f) {
   int k = 0;
   for (int j = 0; j < nrg::kMlpIn; ++j) f[k++] = m.x_mu[j];
@@ -733,6 +733,7 @@ void norm_to_floats(const nrg::MlpNorm& m, float* f) {
   for (int j = 0; j < nrg::kMlpIn; ++j) f[k++] = m.x_max[j];
   for (int j = 0; j < nrg::kMlpOut; ++j) f[k++] = m.y_sd[j];
   f[k++] = m.hull_margin;
+  f[k++] = m.dt_pow;
 }
 nrg::MlpNorm floats_to_norm(const float* f) {
   nrg::MlpNorm m{};
@@ -743,6 +744,7 @@ nrg::MlpNorm floats_to_norm(const float* f) {
   for (int j = 0; j < nrg::kMlpIn; ++j) m.x_max[j] = f[k++];
   for (int j = 0; j < nrg::kMlpOut; ++j) m.y_sd[j] = f[k++];
   m.hull_margin = f[k++];
+  m.dt_pow = f[k++];
   return m;
 }
 }  // namespace
@@ -779,14 +781,15 @@ extern "C" int nrg_surrogate_set_norm(nrg_chem* h, const float* norm) {
 
 extern "C" int nrg_surrogate_prepare(nrg_chem* h, long n, long ld, double dt, const double* dt_cells,
                                      const double* T, const double* rho, const double* Y, const double* Y_prod,
-                                     const double* T_after, float hull_margin, void* x_bf16, float* y) {
+                                     const double* T_after, float hull_margin, float dt_pow, void* x_bf16,
+                                     float* y) {
   if (!h || n <= 0 || ld < n || !T || !rho || !Y || !Y_prod || !T_after || !x_bf16 || !y)
     return fail(h, NRG_ERR_ARG, "bad arguments to nrg_surrogate_prepare");
   CK(h, cudaSetDevice(h->device));
   int rc = order_after_legacy(h);
   if (rc) return rc;
   return sfail(h, nrg::surrogate_prepare(h->sur, n, ld, dt, dt_cells, T, rho, Y, Y_prod, T_after, hull_margin,
-                                         (__nv_bfloat16*)x_bf16, y, h->stream));
+                                         dt_pow, (__nv_bfloat16*)x_bf16, y, h->stream));
 }
 
 extern "C" int nrg_surrogate_features(nrg_chem* h, long n, long ld, double dt, const double* dt_cells,
@@ -851,7 +854,7 @@ extern "C" int nrg_surrogate_save(nrg_chem* h, const char* path) {
   norm_to_floats(nrg::surrogate_get_norm(h->sur), nm.data());
   FILE* f = std::fopen(path, "wb");
   if (!f) return fail(h, NRG_ERR_IO, std::string("cannot write ") + path);
-  const char magic[8] = {'N', 'R', 'G', 'S', 'U', 'R', '1', '\0'};
+  const char magic[8] = {'N', 'R', 'G', 'S', 'U', 'R', '2', '\0'};
   bool ok = std::fwrite(magic, 1, 8, f) == 8 && std::fwrite(&P, 4, 1, f) == 1 &&
             std::fwrite(p.data(), 4, (size_t)P, f) == (size_t)P &&
             std::fwrite(nm.data(), 4, (size_t)kNormFloats, f) == (size_t)kNormFloats;
@@ -867,7 +870,7 @@ extern "C" int nrg_surrogate_load(nrg_chem* h, const char* path) {
   int P = 0;
   const int want = nrg::surrogate_param_count();
   std::vector<float> p((size_t)want), nm(kNormFloats);
-  bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "NRGSUR1", 8) == 0 &&
+  bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "NRGSUR2", 8) == 0 &&
             std::fread(&P, 4, 1, f) == 1 && P == want && std::fread(p.data(), 4, (size_t)P, f) == (size_t)P &&
             std::fread(nm.data(), 4, (size_t)kNormFloats, f) == (size_t)kNormFloats;
   std::fclose(f);

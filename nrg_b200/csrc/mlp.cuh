@@ -4,8 +4,8 @@
 //   input  (12): T, log(p / 1 atm), Y_1..Y_9, log10(dt), each standardised by
 //                the training-set mean and standard deviation; padded to 16
 //   hidden     : 4 layers x 128, GELU (tanh form)
-//   output (10): dY_1..dY_9 and dT, each divided by its training-set standard
-//                deviation; padded to 16
+//   output (10): dY_1..dY_9 and dT, divided by (dt / 1e-6)^dt_pow and then by
+//                the training-set standard deviation; padded to 16
 // Weights and activations are BF16, accumulation FP32.
 #pragma once
 
@@ -25,7 +25,13 @@ struct MlpNorm {
   float x_min[kMlpIn], x_max[kMlpIn];  // raw-feature range of the training states
   float y_sd[kMlpOut];
   float hull_margin;                   // fraction of the range added on both sides
+  float dt_pow;                        // targets are divided by (dt / 1e-6)^dt_pow
 };
+
+// Target scale of a sample with step dt: (dt / 1e-6)^dt_pow, from log10(dt).
+__host__ __device__ __forceinline__ float target_scale(float log10_dt, float dt_pow) {
+  return dt_pow == 0.f ? 1.f : exp10f(dt_pow * (log10_dt + 6.0f));
+}
 
 __device__ __forceinline__ float tanh_fast(float x) {
   float y;

@@ -272,13 +272,14 @@ __global__ void k_gate(StepArgs a, const float* O, const MlpNorm* nm, GateCfg gc
       const float lo = nm->x_min[j] - nm->hull_margin * span, hi = nm->x_max[j] + nm->hull_margin * span;
       ok = ok && (f[j] >= lo) && (f[j] <= hi);
     }
+    const double sc = (double)target_scale(f[11], nm->dt_pow);
     double dY[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
-      dY[k] = (double)O[c * kMlpOutPad + k] * (double)nm->y_sd[k];
+      dY[k] = (double)O[c * kMlpOutPad + k] * (double)nm->y_sd[k] * sc;
       ok = ok && isfinite(dY[k]);
     }
-    const double dT_net = (double)O[c * kMlpOutPad + 9] * (double)nm->y_sd[9];
+    const double dT_net = (double)O[c * kMlpOutPad + 9] * (double)nm->y_sd[9] * sc;
     ok = ok && isfinite(dT_net) && fabs(dT_net) <= gc.dT_max;
     // element conservation (H, O, N) of the predicted increment
     const double We[3] = {1.00794e-3, 15.9994e-3, 14.0067e-3};
@@ -380,12 +381,13 @@ __global__ void k_compact(long n, const unsigned char* flag, const int* block_of
 
 // Raw training targets: dY_k = Y_prod_k dt / rho and dT = T_after - T.
 __global__ void k_targets(long n, long ld, double dt, const double* dt_cells, const double* T, const double* rho,
-                          const double* Y_prod, const double* T_after, float* y) {
+                          const double* Y_prod, const double* T_after, float dt_pow, float* y) {
   for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
     const double d = dt_cells ? dt_cells[c] : dt;
+    const double sc = (double)target_scale((float)log10(d), dt_pow);
 #pragma unroll
-    for (int k = 0; k < 9; ++k) y[c * kMlpOut + k] = (float)(Y_prod[k * ld + c] * d / rho[c]);
-    y[c * kMlpOut + 9] = (float)(T_after[c] - T[c]);
+    for (int k = 0; k < 9; ++k) y[c * kMlpOut + k] = (float)(Y_prod[k * ld + c] * d / rho[c] / sc);
+    y[c * kMlpOut + 9] = (float)((T_after[c] - T[c]) / sc);
   }
 }
 
@@ -785,6 +787,8 @@ std::string surrogate_train(Surrogate* s, long n, const __nv_bfloat16* x, const 
     return e;
   }
   const long steps = n / batch;
+  const double total = (double)steps * epochs;
+  long t_local = 0;
   for (int ep = 0; ep < epochs; ++ep) {
     std::shuffle(perm.begin(), perm.end(), rng);
     cudaMemcpyAsync(d_perm, perm.data(), n * 4, cudaMemcpyHostToDevice, st);
@@ -798,9 +802,12 @@ std::string surrogate_train(Surrogate* s, long n, const __nv_bfloat16* x, const 
         return ck(ce, "train step");
       }
       s->step += 1;
+      // cosine decay from lr to lr/20 over the run
+      const double frac = (double)(t_local++) / total;
+      const float lr_t = (float)(lr * (0.05 + 0.95 * 0.5 * (1.0 + std::cos(3.141592653589793 * frac))));
       const float b1 = 0.9f, b2 = 0.999f;
       const float bc1 = 1.f - std::pow(b1, (float)s->step), bc2 = 1.f - std::pow(b2, (float)s->step);
-      k_adam<<<64, 256, 0, st>>>(s->n_params, s->w, s->gr, s->m, s->v, s->wb, lr, b1, b2, 1e-8f, bc1, bc2);
+      k_adam<<<64, 256, 0, st>>>(s->n_params, s->w, s->gr, s->m, s->v, s->wb, lr_t, b1, b2, 1e-8f, bc1, bc2);
     }
     double L = 0.0;
     cudaMemcpyAsync(&L, s->d_loss, sizeof(double), cudaMemcpyDeviceToHost, st);
@@ -818,7 +825,7 @@ std::string surrogate_train(Surrogate* s, long n, const __nv_bfloat16* x, const 
 
 std::string surrogate_prepare(Surrogate* s, long n, long ld, double dt, const double* dt_cells, const double* T,
                               const double* rho, const double* Y, const double* Y_prod, const double* T_after,
-                              float hull_margin, __nv_bfloat16* x, float* y, cudaStream_t st) {
+                              float hull_margin, float dt_pow, __nv_bfloat16* x, float* y, cudaStream_t st) {
   if (n <= 0) return "no training states";
   float *xraw = nullptr, *yraw = nullptr;
   double* stats = nullptr;
@@ -830,7 +837,7 @@ std::string surrogate_prepare(Surrogate* s, long n, long ld, double dt, const do
   }
   const int grid = (int)std::min<long>((n + 255) / 256, 148 * 16);
   k_features<<<grid, 256, 0, st>>>(n, ld, dt, dt_cells, T, rho, Y, s->d_norm, xraw, nullptr);
-  k_targets<<<grid, 256, 0, st>>>(n, ld, dt, dt_cells, T, rho, Y_prod, T_after, yraw);
+  k_targets<<<grid, 256, 0, st>>>(n, ld, dt, dt_cells, T, rho, Y_prod, T_after, dt_pow, yraw);
   k_colstats<<<kMlpIn, 1024, 0, st>>>(n, kMlpIn, xraw, stats);
   k_colstats<<<kMlpOut, 1024, 0, st>>>(n, kMlpOut, yraw, stats + kMlpIn * 4);
   std::vector<double> hs((kMlpIn + kMlpOut) * 4);
@@ -845,6 +852,7 @@ std::string surrogate_prepare(Surrogate* s, long n, long ld, double dt, const do
     }
     for (int j = 0; j < kMlpOut; ++j) nm.y_sd[j] = (float)std::max(hs[(kMlpIn + j) * 4 + 1], 1e-30);
     nm.hull_margin = hull_margin;
+    nm.dt_pow = dt_pow;
     e = surrogate_set_norm(s, nm);
     if (e.empty()) {
       k_standardize<<<grid, 256, 0, st>>>(n, xraw, yraw, s->d_norm, x, y);

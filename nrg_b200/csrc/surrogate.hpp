@@ -57,7 +57,7 @@ std::string surrogate_train(Surrogate* s, long n, const __nv_bfloat16* x, const 
 // standardisation and training hull, standardised bf16 x (n x 16) and y (n x 10)
 std::string surrogate_prepare(Surrogate* s, long n, long ld, double dt, const double* dt_cells, const double* T,
                               const double* rho, const double* Y, const double* Y_prod, const double* T_after,
-                              float hull_margin, __nv_bfloat16* x, float* y, cudaStream_t st);
+                              float hull_margin, float dt_pow, __nv_bfloat16* x, float* y, cudaStream_t st);
 void surrogate_set_ready(Surrogate* s, bool ready);
 void surrogate_set_gate(Surrogate* s, double elem_tol, double dT_tol, double dT_max);
 

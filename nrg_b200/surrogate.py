@@ -122,7 +122,7 @@ class Surrogate:
 
 
 def training_pairs(solver: ChemicalKineticsSolver, W: np.ndarray, n: int, seed: int = 3,
-                   hull_margin: float = 0.02):
+                   hull_margin: float = 0.02, dt_pow: float = 0.5):
     """Integrates n config-3 states with their own dt (FP64 integrator) and
     returns standardised (x_bf16, y) device tensors plus timing."""
     import torch
@@ -144,16 +144,18 @@ def training_pairs(solver: ChemicalKineticsSolver, W: np.ndarray, n: int, seed: 
     y = torch.empty((n, 10), dtype=torch.float32, device=dev)
     torch.cuda.synchronize()
     _check(lib().nrg_surrogate_prepare(solver.handle, n, n, 1.0, _ptr(dtc), _ptr(T), _ptr(rho), _ptr(Y), _ptr(Yp),
-                                       _ptr(Ta), ctypes.c_float(hull_margin), _ptr(x), _ptr(y)), solver.handle)
+                                       _ptr(Ta), ctypes.c_float(hull_margin), ctypes.c_float(dt_pow), _ptr(x),
+                                       _ptr(y)), solver.handle)
     return x, y, {"integrate_s": t_int, "integrator_stats": stats, "n": n}
 
 
 def train_default(solver: ChemicalKineticsSolver, W: np.ndarray, n_train: int = 4_000_000, epochs: int = 20,
-                  batch: int = 4096, lr: float = 1e-3, seed: int = 0, gate=(1e-6, 0.5, 50.0)) -> dict:
+                  batch: int = 4096, lr: float = 1e-3, seed: int = 0, gate=(1e-6, 0.5, 50.0),
+                  dt_pow: float = 0.5) -> dict:
     """Full recipe: pairs -> Adam training -> gate settings -> enabled."""
     sur = Surrogate(solver)
     t0 = time.perf_counter()
-    x, y, info = training_pairs(solver, W, n_train)
+    x, y, info = training_pairs(solver, W, n_train, dt_pow=dt_pow)
     sur.init(seed)
     t1 = time.perf_counter()
     losses = sur.train(x, y, epochs=epochs, batch=batch, lr=lr, seed=seed + 1)
@@ -161,5 +163,5 @@ def train_default(solver: ChemicalKineticsSolver, W: np.ndarray, n_train: int = 
     sur.set_gate(*gate)
     sur.enable(True)
     info.update({"pairs_s": t1 - t0, "train_s": t2 - t1, "losses": losses.tolist(), "epochs": epochs,
-                 "batch": batch, "lr": lr})
+                 "batch": batch, "lr": lr, "dt_pow": dt_pow})
     return info
