@@ -118,6 +118,23 @@ NRG_API int nrg_chem_step_device(nrg_chem* h, double time_step, long n, long ld,
                          double* Y_prod2, double* E_f_prod, double* T_after, unsigned char* status,
                          void* stream, nrg_chem_stats* stats);
 
+/* No counterpart in the reference.  The same FP64 step as
+ * nrg_chem_step_device for callers that must not allocate device memory while
+ * stepping (for example a host code whose device memory is owned by its own
+ * pool, or that steps from a context where cudaMalloc is not allowed): this
+ * call allocates nothing.  Its scratch (cell flags, scan, the list of active
+ * cells, queue head, counters) is one fixed device array inside the library,
+ * about 5.3 MB, which every GPU that loads the library keeps until exit; n is
+ * limited to 1,048,576 cells per call and larger n is rejected with
+ * NRG_ERR_ARG.  The first call on each device looks up the array's address
+ * (set-up), so make that first call before any stream capture.  All calls on
+ * a device share the array: calls that overlap on the GPU (several streams or
+ * host threads at once) race on it.  Surrogate mode is not available here. */
+NRG_API int nrg_chem_step_device_noalloc(nrg_chem* h, double time_step, long n, long ld, const double* T,
+                                         const double* rho, const double* Y, const signed char* bc,
+                                         double* Y_prod, double* Y_prod2, double* E_f_prod, double* T_after,
+                                         unsigned char* status, void* stream, nrg_chem_stats* stats);
+
 /* Mode (enum nrg_mode).  The reference's ODE_solver selector
  * (chemical_kinetics_solver.f90:91,309-316) has no GPU counterpart for
  * 'table_approximated'. */

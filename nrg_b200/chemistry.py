@@ -72,6 +72,8 @@ SIGNATURES = {
     "nrg_chem_step": (_I, [_VP, _D, ctypes.POINTER(FieldDesc), ctypes.POINTER(Stats)]),
     "nrg_chem_step_device": (_I, [_VP, _D, _L, _L, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP,
                                   ctypes.POINTER(Stats)]),
+    "nrg_chem_step_device_noalloc": (_I, [_VP, _D, _L, _L, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP,
+                                          ctypes.POINTER(Stats)]),
     "nrg_chem_set_mode": (_I, [_VP, _I]),
     "nrg_chem_set_launch": (_I, [_VP, _I, _I, _I, _I]),
     "nrg_chem_get_launch": (_I, [_VP] + [ctypes.POINTER(_I)] * 4),
@@ -327,6 +329,23 @@ class ChemicalKineticsSolver:
         _check(lib().nrg_chem_integrate(
             self._h, T.numel(), Y.shape[1], float(dt), _ptr(dt_cells), _ptr(T), _ptr(rho), _ptr(Y), _ptr(bc),
             _ptr(Y_prod), _ptr(Y_prod2), _ptr(E_f_prod), _ptr(T_after), _ptr(status),
+            ctypes.c_void_p(stream) if stream else None, ctypes.byref(st)), self._h)
+        return st.as_dict()
+
+    def step_device_noalloc(self, time_step, T, rho, Y, Y_prod, Y_prod2, E_f_prod, bc=None, T_after=None,
+                            status=None, stream=None) -> dict:
+        """step_device for callers that cannot allocate device memory during a
+        step: the library uses a fixed scratch array of its own (at most
+        1,048,576 cells per call) and allocates nothing."""
+        n = T.numel()
+        ld = Y.shape[1]
+        if stream is None and hasattr(T, "device"):
+            import torch
+            stream = torch.cuda.current_stream(T.device).cuda_stream
+        st = Stats()
+        _check(lib().nrg_chem_step_device_noalloc(
+            self._h, float(time_step), n, ld, _ptr(T), _ptr(rho), _ptr(Y), _ptr(bc), _ptr(Y_prod),
+            _ptr(Y_prod2), _ptr(E_f_prod), _ptr(T_after), _ptr(status),
             ctypes.c_void_p(stream) if stream else None, ctypes.byref(st)), self._h)
         return st.as_dict()
 

@@ -7,6 +7,7 @@
 #include <cfloat>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -911,4 +912,214 @@ extern "C" int nrg_chem_integrate(nrg_chem* h, long n, long ld, double dt, const
   }
   h->mode = saved;
   return rc;
+}
+
+// ------------------------------------------------- no-allocation step
+// nrg_chem_step_device_noalloc: the compacted FP64 integration (skip rule ->
+// order-preserving list of active cells -> integrator over the list) with all
+// of its scratch -- cell flags, per-block counts and offsets, the cell list,
+// the work-queue head and the statistics counters -- in one file-scope device
+// array instead of memory allocated by the library.  It serves callers that
+// must not allocate device memory during a step.
+namespace {
+
+constexpr long kNaMaxCells = 1L << 20;  // 1,048,576 cells per call
+constexpr int kNaBlock = 1024;
+constexpr int kNaMaxBlocks = (int)(kNaMaxCells / kNaBlock);
+constexpr size_t kNaOffQueue = 0;                    // int
+constexpr size_t kNaOffNList = 4;                    // int
+constexpr size_t kNaOffCounters = 64;                // 8 x unsigned long long
+constexpr size_t kNaOffBlockCount = 256;             // kNaMaxBlocks x int
+constexpr size_t kNaOffBlockOff = 256 + 4 * kNaMaxBlocks;
+constexpr size_t kNaOffList = 256 + 8 * kNaMaxBlocks;  // kNaMaxCells x int (256-aligned)
+constexpr size_t kNaOffFlag = kNaOffList + 4 * (size_t)kNaMaxCells;
+constexpr size_t kNaBytes = kNaOffFlag + (size_t)kNaMaxCells;  // about 5.3 MB
+static_assert(kNaOffList % 256 == 0, "cell list must stay 256-byte aligned");
+
+}  // namespace
+
+// Every GPU that loads the library holds this array until the process exits.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
+
+namespace {
+
+std::mutex g_na_mutex;
+unsigned char* g_na_addr[64] = {};  // device address of g_noalloc_scratch per device
+
+// Set-up, once per device, with that device current: the array's name is only
+// a host-side stand-in, so the kernels get the address the runtime reports.
+unsigned char* noalloc_scratch(int dev, std::string* err) {
+  std::lock_guard<std::mutex> lock(g_na_mutex);
+  if (dev < 0 || dev >= 64) {
+    *err = "device ordinal out of range for the no-allocation scratch table";
+    return nullptr;
+  }
+  if (!g_na_addr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      *err = std::string("cudaGetSymbolAddress(no-allocation scratch): ") + cudaGetErrorString(e);
+      return nullptr;
+    }
+    g_na_addr[dev] = static_cast<unsigned char*>(p);
+  }
+  return g_na_addr[dev];
+}
+
+__global__ void k_na_flag(StepArgs a, int n_species, unsigned char* flag) {
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < a.n; c += (long)gridDim.x * blockDim.x) {
+    const double Tc = a.T[c];
+    const bool active = (Tc >= 305.0) && (a.bc == nullptr || a.bc[c] == 0);
+    flag[c] = active ? 1 : 0;
+    if (!active) {  // skip rule of the reference: zero sources, Y_prod2 untouched
+      for (int k = 0; k < n_species; ++k) a.Y_prod[k * a.ld + c] = 0.0;
+      a.E_f_prod[c] = 0.0;
+      if (a.status) a.status[c] = nrg::kCellSkipped;
+    }
+  }
+}
+
+__global__ void k_na_count(long n, const unsigned char* flag, int* block_count) {
+  const long i = (long)blockIdx.x * kNaBlock + threadIdx.x;
+  const int cnt = __syncthreads_count(i < n ? (int)flag[i] : 0);
+  if (threadIdx.x == 0) block_count[blockIdx.x] = cnt;
+}
+
+__global__ void k_na_scan(int nb, const int* block_count, int* block_off, int* total) {
+  __shared__ int wsum[32];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int base = 0; base < nb; base += blockDim.x) {
+    const int i = base + threadIdx.x;
+    const int v = i < nb ? block_count[i] : 0;
+    int x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    if (w == 0) {
+      int s = lane < (int)(blockDim.x >> 5) ? wsum[lane] : 0;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, s, o);
+        if (lane >= o) s += y;
+      }
+      wsum[lane] = s;
+    }
+    __syncthreads();
+    const int incl = x + (w > 0 ? wsum[w - 1] : 0);
+    if (i < nb) block_off[i] = carry + incl - v;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry += incl;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *total = carry;
+}
+
+__global__ void k_na_compact(long n, const unsigned char* flag, const int* block_off, int* list) {
+  __shared__ int wcount[kNaBlock / 32];
+  const long i = (long)blockIdx.x * kNaBlock + threadIdx.x;
+  const int f = i < n ? (int)flag[i] : 0;
+  const unsigned bal = __ballot_sync(0xffffffffu, f);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) wcount[w] = __popc(bal);
+  __syncthreads();
+  int before = 0;
+  for (int q = 0; q < w; ++q) before += wcount[q];
+  if (f) list[block_off[blockIdx.x] + before + __popc(bal & ((1u << lane) - 1u))] = (int)i;
+}
+
+}  // namespace
+
+extern "C" int nrg_chem_step_device_noalloc(nrg_chem* h, double time_step, long n, long ld, const double* T,
+                                            const double* rho, const double* Y, const signed char* bc,
+                                            double* Y_prod, double* Y_prod2, double* E_f_prod, double* T_after,
+                                            unsigned char* status, void* stream, nrg_chem_stats* stats) {
+  if (!h) return NRG_ERR_ARG;
+  if (n < 0 || ld < n) return fail(h, NRG_ERR_ARG, "need 0 <= n <= ld");
+  if (n > kNaMaxCells)
+    return fail(h, NRG_ERR_ARG,
+                "nrg_chem_step_device_noalloc takes at most 1048576 cells per call (its scratch is a fixed "
+                "device array); split the field or use nrg_chem_step_device");
+  if (!(time_step > 0.0) || !std::isfinite(time_step)) return fail(h, NRG_ERR_ARG, "time_step must be > 0");
+  if (n > 0 && (!T || !rho || !Y || !Y_prod || !Y_prod2 || !E_f_prod))
+    return fail(h, NRG_ERR_ARG, "null field pointer");
+  if (h->mode == NRG_MODE_SURROGATE)
+    return fail(h, NRG_ERR_STATE, "the surrogate needs buffers sized to the field; use nrg_chem_step_device");
+  if (n == 0) {
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    return NRG_OK;
+  }
+  CK(h, cudaSetDevice(h->device));
+  std::string err;
+  unsigned char* base = noalloc_scratch(h->device, &err);
+  if (!base) return fail(h, NRG_ERR_CUDA, err);
+  int* queue = reinterpret_cast<int*>(base + kNaOffQueue);
+  int* n_list = reinterpret_cast<int*>(base + kNaOffNList);
+  unsigned long long* counters = reinterpret_cast<unsigned long long*>(base + kNaOffCounters);
+  int* block_count = reinterpret_cast<int*>(base + kNaOffBlockCount);
+  int* block_off = reinterpret_cast<int*>(base + kNaOffBlockOff);
+  int* list = reinterpret_cast<int*>(base + kNaOffList);
+  unsigned char* flag = base + kNaOffFlag;
+
+  cudaStream_t s = h->stream;
+  CK(h, cudaEventRecord(h->ev_in, (cudaStream_t)stream));
+  CK(h, cudaStreamWaitEvent(s, h->ev_in, 0));
+  StepArgs a{};
+  a.n = n;
+  a.ld = ld;
+  a.dt = time_step;
+  a.T = T;
+  a.rho = rho;
+  a.Y = Y;
+  a.bc = (const int8_t*)bc;
+  a.Y_prod = Y_prod;
+  a.Y_prod2 = Y_prod2;
+  a.E_f_prod = E_f_prod;
+  a.T_after = T_after;
+  a.status = status;
+  a.mxstep = 10000;
+  a.mech = h->d_mech;
+  a.dt_cells = nullptr;
+  a.cell_list = nullptr;
+  a.n_list = 0;
+  a.n_list_dev = nullptr;
+  const int nb = (int)((n + kNaBlock - 1) / kNaBlock);
+  CK(h, cudaEventRecord(h->ev0, s));
+  // queue head, list length and counters start at zero on every call
+  CK(h, cudaMemsetAsync(base, 0, kNaOffBlockCount, s));
+  k_na_flag<<<(unsigned)std::min<long>((n + 255) / 256, 148L * 16), 256, 0, s>>>(a, h->mech.n(), flag);
+  k_na_count<<<nb, kNaBlock, 0, s>>>(n, flag, block_count);
+  k_na_scan<<<1, 1024, 0, s>>>(nb, block_count, block_off, n_list);
+  k_na_compact<<<nb, kNaBlock, 0, s>>>(n, flag, block_off, list);
+  CK(h, cudaGetLastError());
+  StepArgs fa = a;
+  fa.cell_list = list;
+  fa.n_list = (int)n;  // grid bound; the kernels read the device-side count
+  fa.n_list_dev = n_list;
+  LaunchCfg cfg = h->cfg;
+  if (cfg.kernel == nrg::kKernelThreadQueue && cfg.grid <= 0) cfg.grid = h->num_sms;
+  const cudaError_t le = nrg::launch_chem(h->mech.n(), h->mech.r(), jac_of(h->mode), h->mode == NRG_MODE_MIXED,
+                                          fa, cfg, queue, counters, s);
+  if (le != cudaSuccess) return cuda_fail(h, le, "no-allocation integrator launch");
+  CK(h, cudaEventRecord(h->ev1, s));
+  CK(h, cudaMemcpyAsync(h->h_counters, counters, sizeof(unsigned long long) * 8, cudaMemcpyDeviceToHost, s));
+  CK(h, cudaStreamSynchronize(s));
+  if (stats) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    std::memset(stats, 0, sizeof(*stats));
+    stats->cells = n;
+    stats->cells_active = (long long)h->h_counters[0];
+    stats->steps = (long long)h->h_counters[1];
+    stats->rhs_evals = (long long)h->h_counters[2];
+    stats->jacobians = (long long)h->h_counters[3];
+    stats->solves = (long long)h->h_counters[4];
+    stats->cells_bad = (long long)h->h_counters[5];
+    stats->device_ms = ms;
+  }
+  return NRG_OK;
 }
