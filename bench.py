@@ -213,6 +213,20 @@ def run_reference(args):
 
 # ------------------------------------------------------------------ our arm
 MLP_FLOPS_PER_CELL = 2 * (12 * 128 + 3 * 128 * 128 + 128 * 10)
+PROFILE = os.path.join(ROOT, "profiles", "fp64_integrator_flame.md")
+
+
+def integrator_traffic():
+    """DRAM bytes (read + write) per integrator launch on the full field, from
+    the committed ncu summary (line 'traffic_bytes_per_launch: N')."""
+    try:
+        with open(PROFILE) as fh:
+            for line in fh:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
 
 
 def main():
@@ -230,7 +244,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     from nrg_b200 import fields as F, keromnes_paths
     from nrg_b200.chemistry import ChemicalKineticsSolver, DataManager, fp64_peak_tflops, mechanism_tables
-    from nrg_b200.surrogate import DEFAULT_MODEL, Surrogate, train_default
+    from nrg_b200.surrogate import DEFAULT_MODEL, RECIPE, Surrogate, train_default
     decks = keromnes_paths()
     tables = mechanism_tables(*decks)
     W = tables["molar_mass"]
@@ -255,13 +269,15 @@ def main():
         sur = Surrogate(solver)
         if os.path.exists(DEFAULT_MODEL):
             sur.load(DEFAULT_MODEL)
-            sur.set_gate()
-            train_info = {"model": os.path.relpath(DEFAULT_MODEL, ROOT), "trained": "loaded"}
+            sur.set_gate(*RECIPE["gate"])
+            train_info = {"model": os.path.relpath(DEFAULT_MODEL, ROOT), "trained": "loaded",
+                          "gate": list(RECIPE["gate"])}
         else:
             info = train_default(solver, W)
             sur.save(DEFAULT_MODEL)
-            train_info = {"trained": "in this run", "pairs": info["n"], "epochs": info["epochs"],
-                          "pairs_s": info["pairs_s"], "train_s": info["train_s"], "final_loss": info["losses"][-1]}
+            train_info = {"trained": "in this run", "pairs": info["n"], "epochs": info["recipe"]["epochs"],
+                          "pairs_s": info["pairs_s"], "train_s": info["train_s"], "final_loss": info["losses"][-1],
+                          "gate": list(RECIPE["gate"])}
         mode = "surrogate"
     peak_fp64 = fp64_peak_tflops()
 
@@ -337,7 +353,7 @@ def main():
         if mode == "surrogate":
             hs = Surrogate(host)
             hs.load(DEFAULT_MODEL)
-            hs.set_gate()
+            hs.set_gate(*RECIPE["gate"])
         host.set_mode(mode)
         host.solve_chemical_kinetics(field.dt)
         if world > 1:
@@ -359,22 +375,27 @@ def main():
         st = stats[-1]
         peaks = load_peaks()
         fm = flop_model(tables, "fast")
-        phases = {"mlp_ms": ph["phase_ms"][0], "gate_ms": ph["phase_ms"][1], "integrator_ms": ph["phase_ms"][2]}
+        phases = {"inference_ms": ph["phase_ms"][0], "compaction_ms": ph["phase_ms"][1],
+                  "integrator_ms": ph["phase_ms"][2]}
         integ_flops = algorithmic_flops(ph, fm)
         integ_tf = integ_flops / max(phases["integrator_ms"], 1e-9) * 1e-9
-        if mode == "surrogate" and phases["mlp_ms"] > phases["integrator_ms"]:
-            mlp_tf = MLP_FLOPS_PER_CELL * n / max(phases["mlp_ms"], 1e-9) * 1e-9
-            roof = {"bound": "tensor", "achieved": mlp_tf, "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
-                    "frac": mlp_tf / peaks["bf16_tflops"], "traffic": None, "kernel": "MLP layers (BF16)",
-                    "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)"}
-        else:
-            roof = {"bound": "fp64", "achieved": integ_tf, "peak": peak_fp64, "unit": "TFLOP/s",
-                    "frac": integ_tf / peak_fp64, "traffic": None,
-                    "kernel": "FP64 BDF integrator (" + launch["kernel"] + ")",
-                    "peak_source": "measured live: dependent-FMA FP64 probe (MEASURED_PEAKS.json has no FP64 figure)",
-                    "flops_per_launch": integ_flops, "flop_model": fm}
+        roof = {"bound": "fp64", "achieved": integ_tf, "peak": peak_fp64, "unit": "TFLOP/s",
+                "frac": integ_tf / peak_fp64, "traffic": integrator_traffic(),
+                "kernel": "FP64 BDF integrator (" + launch["kernel"] + "), the dominant kernel",
+                "peak_source": "measured live: dependent-FMA FP64 probe (MEASURED_PEAKS.json has no FP64 figure)",
+                "flops_per_launch": integ_flops, "flop_model": fm}
+        roof_mlp = None
+        if mode == "surrogate":
+            # fused kernel: MLP of every active cell + the FP64 gate; tensor
+            # share is a lower bound because the gate is inside the same time
+            mlp_flops = MLP_FLOPS_PER_CELL * float(ph["cells_active"])
+            mlp_tf = mlp_flops / max(phases["inference_ms"], 1e-9) * 1e-9
+            roof_mlp = {"bound": "tensor", "achieved": mlp_tf, "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
+                        "frac": mlp_tf / peaks["bf16_tflops"], "kernel": "k_mlp_gate_tc (features + 5 tcgen05 "
+                        "layers + FP64 gate)", "flops_per_launch": mlp_flops,
+                        "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst), of measured"}
         cpu = cpu_baseline(field, W, decks, args.cpu_seconds)
-        launches = 11 if mode == "surrogate" else 1
+        launches = 5 if mode == "surrogate" else 1  # fused MLP+gate, 3 compaction kernels, integrator
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": el / args.steps, "higher_is_better": True,
@@ -394,6 +415,7 @@ def main():
             "surrogate_model": train_info,
             "phases_ms": phases,
             "roofline": roof,
+            "roofline_mlp": roof_mlp,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": args.steps * launches,

@@ -87,7 +87,9 @@ typedef struct {
   long long steps, rhs_evals, jacobians, solves;
   double device_ms;          /* device time of the step (CUDA events) */
   /* per-phase device time when phase timing is on (nrg_chem_set_timing):
-   * [0] features + MLP, [1] gate + compaction, [2] FP64 integrator, [3] unused */
+   * [0] surrogate inference (fused path: features + MLP + gate in one kernel;
+   * unfused: features + MLP), [1] compaction (unfused: gate + compaction),
+   * [2] FP64 integrator, [3] unused */
   double phase_ms[4];
 } nrg_chem_stats;
 
@@ -198,13 +200,20 @@ NRG_API int nrg_surrogate_get_params(nrg_chem* h, float* params);
 NRG_API int nrg_surrogate_set_params(nrg_chem* h, const float* params);
 NRG_API int nrg_surrogate_get_norm(nrg_chem* h, float* norm);
 NRG_API int nrg_surrogate_set_norm(nrg_chem* h, const float* norm);
+/* Choices made when training arrays are prepared. */
+typedef struct nrg_surrogate_opts {
+  float hull_margin;    /* fraction of each raw feature's range added on both sides of the hull */
+  float dt_pow;         /* targets are divided by (dt / 1e-6)^dt_pow */
+  unsigned log_mask;    /* bit k: Y_k enters the network as log10(Y_k + log_eps) (k < 9) */
+  float log_eps;        /* > 0 */
+  int common_dY_scale;  /* 1: one scale for all dY_k (absolute-error loss); 0: per species */
+} nrg_surrogate_opts;
 /* Training arrays from integrated states (Y_prod, T_after from
  * nrg_chem_integrate with the same dt / dt_cells); also fits the feature and
- * target scaling and the training hull (widened by hull_margin of each range);
- * targets are divided by (dt / 1e-6)^dt_pow before standardisation. */
+ * target scaling and the training hull (on the raw features). */
 NRG_API int nrg_surrogate_prepare(nrg_chem* h, long n, long ld, double dt, const double* dt_cells,
                                   const double* T, const double* rho, const double* Y, const double* Y_prod,
-                                  const double* T_after, float hull_margin, float dt_pow, void* x_bf16,
+                                  const double* T_after, const nrg_surrogate_opts* opts, void* x_bf16,
                                   float* y);
 NRG_API int nrg_surrogate_features(nrg_chem* h, long n, long ld, double dt, const double* dt_cells,
                                    const double* T, const double* rho, const double* Y, float* xraw,
@@ -215,9 +224,21 @@ NRG_API int nrg_surrogate_grad(nrg_chem* h, long n, const void* x_bf16, const fl
                                double* loss_host);
 NRG_API int nrg_surrogate_train(nrg_chem* h, long n, const void* x_bf16, const float* y, int epochs, int batch,
                                 float lr, unsigned long long seed, float* loss_per_epoch);
-/* Gate: element residual bound (element mass fraction), bound on the gap
- * between the network's dT and the energy closure of its dY (K), |dT| bound (K). */
-NRG_API int nrg_surrogate_set_gate(nrg_chem* h, double elem_tol, double dT_tol, double dT_max);
+/* Gate: element residual (element mass fraction, H/O/N) of the dY that is
+ * written, after its orthogonal projection onto the element-conserving
+ * increments; residual of the network's own dY before that projection; bound
+ * on the gap between the network's dT and the FP64 energy closure of the
+ * written dY (K); |dT| bound (K). */
+NRG_API int nrg_surrogate_set_gate(nrg_chem* h, double elem_tol, double raw_elem_tol, double dT_tol,
+                                   double dT_max);
+/* Inference path of the surrogate step: 1 (default) one fused kernel
+ * (features, the five layers on tcgen05 tensor cores with TMEM accumulators,
+ * gate); 0 the unfused chain (features, one GEMM per layer, gate kernel). */
+NRG_API int nrg_surrogate_set_inference(nrg_chem* h, int fused);
+/* Network outputs (n x 16 fp32, normalised units) of the fused kernel for
+ * every cell, no gate (device arrays, same layout as nrg_chem_step_device). */
+NRG_API int nrg_surrogate_infer(nrg_chem* h, long n, long ld, double dt, const double* dt_cells, const double* T,
+                                const double* rho, const double* Y, float* out);
 NRG_API int nrg_surrogate_enable(nrg_chem* h, int enable);
 NRG_API int nrg_surrogate_save(nrg_chem* h, const char* path);
 NRG_API int nrg_surrogate_load(nrg_chem* h, const char* path);

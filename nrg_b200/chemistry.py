@@ -92,13 +92,14 @@ SIGNATURES = {
     "nrg_surrogate_set_params": (_I, [_VP, _VP]),
     "nrg_surrogate_get_norm": (_I, [_VP, _VP]),
     "nrg_surrogate_set_norm": (_I, [_VP, _VP]),
-    "nrg_surrogate_prepare": (_I, [_VP, _L, _L, _D, _VP, _VP, _VP, _VP, _VP, _VP, ctypes.c_float, ctypes.c_float,
-                                   _VP, _VP]),
+    "nrg_surrogate_prepare": (_I, [_VP, _L, _L, _D, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "nrg_surrogate_features": (_I, [_VP, _L, _L, _D, _VP, _VP, _VP, _VP, _VP, _VP]),
     "nrg_surrogate_forward": (_I, [_VP, _L, _VP, _VP]),
     "nrg_surrogate_grad": (_I, [_VP, _L, _VP, _VP, _VP, ctypes.POINTER(_D)]),
     "nrg_surrogate_train": (_I, [_VP, _L, _VP, _VP, _I, _I, ctypes.c_float, ctypes.c_ulonglong, _VP]),
-    "nrg_surrogate_set_gate": (_I, [_VP, _D, _D, _D]),
+    "nrg_surrogate_set_gate": (_I, [_VP, _D, _D, _D, _D]),
+    "nrg_surrogate_set_inference": (_I, [_VP, _I]),
+    "nrg_surrogate_infer": (_I, [_VP, _L, _L, _D, _VP, _VP, _VP, _VP, _VP]),
     "nrg_surrogate_enable": (_I, [_VP, _I]),
     "nrg_surrogate_save": (_I, [_VP, _CP]),
     "nrg_surrogate_load": (_I, [_VP, _CP]),

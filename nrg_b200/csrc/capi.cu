@@ -321,6 +321,10 @@ int run_step(nrg_chem* h, const StepArgs& a, cudaStream_t s, nrg_chem_stats* sta
       stats->phase_ms[2] = p;
     }
   }
+  if (h->mode == NRG_MODE_SURROGATE) {
+    const std::string e = nrg::surrogate_check(h->sur, s);
+    if (!e.empty()) return fail(h, NRG_ERR_CUDA, e);
+  }
   return NRG_OK;
 }
 
@@ -725,7 +729,7 @@ int order_after_legacy(nrg_chem* h) {
   return NRG_OK;
 }
 int sfail(nrg_chem* h, const std::string& e) { return e.empty() ? NRG_OK : fail(h, NRG_ERR_CUDA, e); }
-constexpr int kNormFloats = 4 * nrg::kMlpIn + nrg::kMlpOut + 2;
+constexpr int kNormFloats = 4 * nrg::kMlpIn + nrg::kMlpOut + 4;
 void norm_to_floats(const nrg::MlpNorm& m, float* f) {
   int k = 0;
   for (int j = 0; j < nrg::kMlpIn; ++j) f[k++] = m.x_mu[j];
@@ -735,6 +739,8 @@ void norm_to_floats(const nrg::MlpNorm& m, float* f) {
   for (int j = 0; j < nrg::kMlpOut; ++j) f[k++] = m.y_sd[j];
   f[k++] = m.hull_margin;
   f[k++] = m.dt_pow;
+  f[k++] = m.log_mask;
+  f[k++] = m.log_eps;
 }
 nrg::MlpNorm floats_to_norm(const float* f) {
   nrg::MlpNorm m{};
@@ -746,6 +752,8 @@ nrg::MlpNorm floats_to_norm(const float* f) {
   for (int j = 0; j < nrg::kMlpOut; ++j) m.y_sd[j] = f[k++];
   m.hull_margin = f[k++];
   m.dt_pow = f[k++];
+  m.log_mask = f[k++];
+  m.log_eps = f[k++];
   return m;
 }
 }  // namespace
@@ -782,15 +790,18 @@ extern "C" int nrg_surrogate_set_norm(nrg_chem* h, const float* norm) {
 
 extern "C" int nrg_surrogate_prepare(nrg_chem* h, long n, long ld, double dt, const double* dt_cells,
                                      const double* T, const double* rho, const double* Y, const double* Y_prod,
-                                     const double* T_after, float hull_margin, float dt_pow, void* x_bf16,
+                                     const double* T_after, const nrg_surrogate_opts* opts, void* x_bf16,
                                      float* y) {
-  if (!h || n <= 0 || ld < n || !T || !rho || !Y || !Y_prod || !T_after || !x_bf16 || !y)
+  if (!h || n <= 0 || ld < n || !T || !rho || !Y || !Y_prod || !T_after || !opts || !x_bf16 || !y)
     return fail(h, NRG_ERR_ARG, "bad arguments to nrg_surrogate_prepare");
+  if (!(opts->hull_margin >= 0.f) || !(opts->log_eps > 0.f) || (opts->log_mask >> 9))
+    return fail(h, NRG_ERR_ARG, "bad nrg_surrogate_opts (hull_margin >= 0, log_eps > 0, log_mask < 512)");
   CK(h, cudaSetDevice(h->device));
   int rc = order_after_legacy(h);
   if (rc) return rc;
-  return sfail(h, nrg::surrogate_prepare(h->sur, n, ld, dt, dt_cells, T, rho, Y, Y_prod, T_after, hull_margin,
-                                         dt_pow, (__nv_bfloat16*)x_bf16, y, h->stream));
+  const nrg::PrepareOpts o{opts->hull_margin, opts->dt_pow, opts->log_mask, opts->log_eps, opts->common_dY_scale};
+  return sfail(h, nrg::surrogate_prepare(h->sur, n, ld, dt, dt_cells, T, rho, Y, Y_prod, T_after, o,
+                                         (__nv_bfloat16*)x_bf16, y, h->stream));
 }
 
 extern "C" int nrg_surrogate_features(nrg_chem* h, long n, long ld, double dt, const double* dt_cells,
@@ -834,10 +845,30 @@ extern "C" int nrg_surrogate_train(nrg_chem* h, long n, const void* x_bf16, cons
                                        loss_per_epoch, h->stream));
 }
 
-extern "C" int nrg_surrogate_set_gate(nrg_chem* h, double elem_tol, double dT_tol, double dT_max) {
-  if (!h || !(elem_tol >= 0) || !(dT_tol >= 0) || !(dT_max >= 0)) return NRG_ERR_ARG;
-  nrg::surrogate_set_gate(h->sur, elem_tol, dT_tol, dT_max);
+extern "C" int nrg_surrogate_set_gate(nrg_chem* h, double elem_tol, double raw_elem_tol, double dT_tol,
+                                      double dT_max) {
+  if (!h || !(elem_tol >= 0) || !(raw_elem_tol >= 0) || !(dT_tol >= 0) || !(dT_max >= 0)) return NRG_ERR_ARG;
+  nrg::surrogate_set_gate(h->sur, elem_tol, raw_elem_tol, dT_tol, dT_max);
   return NRG_OK;
+}
+
+extern "C" int nrg_surrogate_set_inference(nrg_chem* h, int fused) {
+  if (!h) return NRG_ERR_ARG;
+  nrg::surrogate_set_fused(h->sur, fused != 0);
+  return NRG_OK;
+}
+
+extern "C" int nrg_surrogate_infer(nrg_chem* h, long n, long ld, double dt, const double* dt_cells, const double* T,
+                                   const double* rho, const double* Y, float* out) {
+  if (!h || n < 0 || ld < n || (n > 0 && (!T || !rho || !Y || !out)) || (!(dt > 0.0) && !dt_cells))
+    return fail(h, NRG_ERR_ARG, "bad arguments to nrg_surrogate_infer");
+  CK(h, cudaSetDevice(h->device));
+  int rc = order_after_legacy(h);
+  if (rc) return rc;
+  StepArgs a{};
+  a.n = n; a.ld = ld; a.dt = dt > 0.0 ? dt : 1.0; a.dt_cells = dt_cells; a.T = T; a.rho = rho; a.Y = Y;
+  a.mech = h->d_mech;
+  return sfail(h, nrg::surrogate_infer(h->sur, a, out, h->stream));
 }
 
 extern "C" int nrg_surrogate_enable(nrg_chem* h, int enable) {
@@ -855,7 +886,7 @@ extern "C" int nrg_surrogate_save(nrg_chem* h, const char* path) {
   norm_to_floats(nrg::surrogate_get_norm(h->sur), nm.data());
   FILE* f = std::fopen(path, "wb");
   if (!f) return fail(h, NRG_ERR_IO, std::string("cannot write ") + path);
-  const char magic[8] = {'N', 'R', 'G', 'S', 'U', 'R', '2', '\0'};
+  const char magic[8] = {'N', 'R', 'G', 'S', 'U', 'R', '3', '\0'};
   bool ok = std::fwrite(magic, 1, 8, f) == 8 && std::fwrite(&P, 4, 1, f) == 1 &&
             std::fwrite(p.data(), 4, (size_t)P, f) == (size_t)P &&
             std::fwrite(nm.data(), 4, (size_t)kNormFloats, f) == (size_t)kNormFloats;
@@ -871,7 +902,7 @@ extern "C" int nrg_surrogate_load(nrg_chem* h, const char* path) {
   int P = 0;
   const int want = nrg::surrogate_param_count();
   std::vector<float> p((size_t)want), nm(kNormFloats);
-  bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "NRGSUR2", 8) == 0 &&
+  bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "NRGSUR3", 8) == 0 &&
             std::fread(&P, 4, 1, f) == 1 && P == want && std::fread(p.data(), 4, (size_t)P, f) == (size_t)P &&
             std::fread(nm.data(), 4, (size_t)kNormFloats, f) == (size_t)kNormFloats;
   std::fclose(f);

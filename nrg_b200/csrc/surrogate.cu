@@ -7,8 +7,11 @@
 //   * skip rule of the reference (T < 305 K or bc /= 0): zero sources;
 //   * training hull: every raw feature inside the training min/max widened by
 //     hull_margin of its range;
-//   * element conservation: |sum_k a_ek (W_e / W_k) dY_k| <= elem_tol for the
-//     elements H, O, N (element mass fraction units);
+//   * element conservation: the network's dY has an element residual
+//     |sum_k a_ek (W_e / W_k) dY_k| <= raw_elem_tol for H, O, N (element mass
+//     fraction units); it is then projected orthogonally onto the conserving
+//     increments in FP64 and the residual of what is written must be
+//     <= elem_tol;
 //   * temperature: the network's dT agrees within dT_tol with the FP64 energy
 //     closure of its own dY, and |dT| <= dT_max.
 // Rejected cells are compacted in cell order (so neighbouring cells stay
@@ -23,6 +26,7 @@
 
 #include "chem_bdf.cuh"
 #include "surrogate.hpp"
+#include "tc_sm100.cuh"
 
 namespace nrg {
 
@@ -234,27 +238,144 @@ __global__ void k_features(long n, long ld, double dt, const double* dt_cells, c
     if (x) {
 #pragma unroll
       for (int j = 0; j < kMlpInPad; ++j)
-        x[c * kMlpInPad + j] = __float2bfloat16(j < kMlpIn ? (f[j] - nm->x_mu[j]) / nm->x_sd[j] : 0.f);
+        x[c * kMlpInPad + j] = __float2bfloat16(j < kMlpIn ? net_input(*nm, j, f[j]) : 0.f);
     }
   }
 }
 
 // Gate and outputs.  flag[c] = 1 sends the cell to the FP64 fallback.
 struct GateCfg {
-  double elem_tol, dT_tol, dT_max;
+  double elem_tol;      // element residual of the dY that is written (after projection)
+  double raw_elem_tol;  // element residual of the network's own dY
+  double dT_tol, dT_max;
 };
+
+// Element residual max_e |sum_k a_ek (W_e / W_k) dY_k| (element mass fraction)
+// for H, O, N.
+__device__ __forceinline__ double element_residual(const double (&dY)[9]) {
+  const double We[3] = {1.00794e-3, 15.9994e-3, 14.0067e-3};
+  double m = 0.0;
+#pragma unroll
+  for (int e = 0; e < 3; ++e) {
+    double r = 0.0;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) r += c_mech.elem[e][k] * We[e] / c_mech.W[k] * dY[k];
+    m = fmax(m, fabs(r));
+  }
+  return m;
+}
+
+// Orthogonal projector onto the element-conserving increments
+// {dY : sum_k a_ek dY_k / W_k = 0 for H, O, N}: P = I - sum_q q q^T over an
+// orthonormal basis q of the rows a_e / W (Gram-Schmidt; elements absent from
+// the mechanism drop out).
+__device__ void element_projector(double (*P)[9]) {
+  double q[3][9];
+  int nq = 0;
+  for (int e = 0; e < 3; ++e) {
+    double v[9], n0 = 0.0;
+    for (int k = 0; k < 9; ++k) {
+      v[k] = c_mech.elem[e][k] / c_mech.W[k];
+      n0 += v[k] * v[k];
+    }
+    for (int i = 0; i < nq; ++i) {
+      double d = 0.0;
+      for (int k = 0; k < 9; ++k) d += q[i][k] * v[k];
+      for (int k = 0; k < 9; ++k) v[k] -= d * q[i][k];
+    }
+    double nn = 0.0;
+    for (int k = 0; k < 9; ++k) nn += v[k] * v[k];
+    if (!(n0 > 0.0) || nn <= 1e-24 * n0) continue;
+    const double r = 1.0 / sqrt(nn);
+    for (int k = 0; k < 9; ++k) q[nq][k] = v[k] * r;
+    ++nq;
+  }
+  for (int i = 0; i < 9; ++i)
+    for (int j = 0; j < 9; ++j) {
+      double x = i == j ? 1.0 : 0.0;
+      for (int b = 0; b < nq; ++b) x -= q[b][i] * q[b][j];
+      P[i][j] = x;
+    }
+}
+
+// Skip rule of the reference (T < 305 K or a boundary marker): zero sources,
+// T unchanged.  Returns true for a skipped cell.
+__device__ __forceinline__ bool write_if_skipped(const StepArgs& a, long c, double T0) {
+  if ((T0 >= 305.0) && (a.bc == nullptr || a.bc[c] == 0)) return false;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) a.Y_prod[k * a.ld + c] = 0.0;
+  a.E_f_prod[c] = 0.0;
+  if (a.T_after) a.T_after[c] = T0;
+  if (a.status) a.status[c] = kCellSkipped;
+  return true;
+}
+
+// Gate of one active cell on its network outputs o (normalised units): hull
+// of the raw features f, element residuals, FP64 projection, energy closure.
+// Writes the sources of an accepted cell and returns whether it was accepted.
+__device__ __noinline__ bool gate_active_cell(const StepArgs& a, long c, double T0, double rho, double dt,
+                                                 const double (&y0)[9], const float (&f)[kMlpIn],
+                                                 const float* o, const MlpNorm* nm, const GateCfg& gc,
+                                                 const double (*P)[9]) {
+  bool ok = true;
+#pragma unroll
+  for (int j = 0; j < kMlpIn; ++j) {
+    const float span = nm->x_max[j] - nm->x_min[j];
+    const float lo = nm->x_min[j] - nm->hull_margin * span, hi = nm->x_max[j] + nm->hull_margin * span;
+    ok = ok && (f[j] >= lo) && (f[j] <= hi);
+  }
+  const double sc = (double)target_scale(f[11], nm->dt_pow);
+  double dYn[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    dYn[k] = (double)o[k] * (double)nm->y_sd[k] * sc;
+    ok = ok && isfinite(dYn[k]);
+  }
+  const double dT_net = (double)o[9] * (double)nm->y_sd[9] * sc;
+  ok = ok && isfinite(dT_net) && fabs(dT_net) <= gc.dT_max;
+  ok = ok && element_residual(dYn) <= gc.raw_elem_tol;
+  if (!ok) return false;
+  // the written increment conserves H, O and N: projection in FP64
+  double dY[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    double x = 0.0;
+#pragma unroll
+    for (int j = 0; j < 9; ++j) x += P[i][j] * dYn[j];
+    dY[i] = x;
+  }
+  if (!(element_residual(dY) <= gc.elem_tol)) return false;
+  double E = 0.0;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) E = E - c_mech.h_ref[k] * (dY[k] * rho / c_mech.W[k]) / dt;
+  const double T1 = temperature_after<9>(T0, y0, dY, E * dt / rho);
+  if (!(fabs((T1 - T0) - dT_net) <= gc.dT_tol)) return false;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    a.Y_prod[k * a.ld + c] = dY[k] * rho / dt;
+    a.Y_prod2[k * a.ld + c] = dY[k] * rho / c_mech.W[k];
+  }
+  a.E_f_prod[c] = E;
+  if (a.T_after) a.T_after[c] = T1;
+  if (a.status) a.status[c] = kCellSurrogate;
+  return true;
+}
+
+__device__ __forceinline__ void count_surrogate(unsigned long long n_sur, unsigned long long* counters) {
+  if (!counters) return;
+  for (int o = 16; o > 0; o >>= 1) n_sur += __shfl_down_sync(0xffffffffu, n_sur, o);
+  if ((threadIdx.x & 31) == 0 && n_sur) atomicAdd(&counters[6], n_sur);
+}
 
 __global__ void k_gate(StepArgs a, const float* O, const MlpNorm* nm, GateCfg gc, unsigned char* flag,
                        unsigned long long* counters) {
+  __shared__ double P[9][9];
+  if (threadIdx.x == 0) element_projector(P);
+  __syncthreads();
   unsigned long long n_sur = 0;
   for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < a.n; c += (long)gridDim.x * blockDim.x) {
     const double T0 = a.T[c];
-    if (!((T0 >= 305.0) && (a.bc == nullptr || a.bc[c] == 0))) {
-#pragma unroll
-      for (int k = 0; k < 9; ++k) a.Y_prod[k * a.ld + c] = 0.0;
-      a.E_f_prod[c] = 0.0;
-      if (a.T_after) a.T_after[c] = T0;
-      if (a.status) a.status[c] = kCellSkipped;
+    if (write_if_skipped(a, c, T0)) {
       flag[c] = 0;
       continue;
     }
@@ -265,54 +386,235 @@ __global__ void k_gate(StepArgs a, const float* O, const MlpNorm* nm, GateCfg gc
     for (int k = 0; k < 9; ++k) y0[k] = a.Y[k * a.ld + c];
     float f[kMlpIn];
     cell_features<9>(T0, rho, y0, dt, f);
-    bool ok = true;
-#pragma unroll
-    for (int j = 0; j < kMlpIn; ++j) {
-      const float span = nm->x_max[j] - nm->x_min[j];
-      const float lo = nm->x_min[j] - nm->hull_margin * span, hi = nm->x_max[j] + nm->hull_margin * span;
-      ok = ok && (f[j] >= lo) && (f[j] <= hi);
+    const bool acc = gate_active_cell(a, c, T0, rho, dt, y0, f, O + c * kMlpOutPad, nm, gc, P);
+    n_sur += acc;
+    flag[c] = acc ? 0 : 1;
+  }
+  count_surrogate(n_sur, counters);
+}
+
+// ------------------------------------------------- fused tcgen05 inference
+// One kernel per step for features -> 5 MLP layers -> gate.  Persistent CTAs
+// of two warpgroups; each warpgroup streams its own 128-cell tiles (thread t
+// of the group owns cell t of the tile, which is TMEM lane t).  Per tile:
+// features are standardised into a bf16 K-major operand in shared memory,
+// one thread issues the layer's tcgen05.mma (M = 128, A = activations,
+// B = weights, both in shared memory; FP32 accumulator in this group's 128
+// TMEM columns) and commits to the group's mbarrier; the epilogue reads the
+// thread's accumulator row with tcgen05.ld, adds the bias, applies GELU and
+// writes the next layer's bf16 operand.  The weights (104 KB) stay in shared
+// memory for the kernel's lifetime.  While one group runs its epilogue the
+// other group's MMAs run.  Every wait is bounded: on a timeout the group
+// stops issuing MMAs, sends its remaining cells to the FP64 fallback and
+// records the event in *err.
+constexpr int kTcGroups = 2;
+constexpr uint32_t kTcW0 = 0;                             // layer 0: 128 x 16
+constexpr uint32_t kTcW1 = 4096;                          // layers 1-3: 128 x 128
+constexpr uint32_t kTcW4 = kTcW1 + 3 * 32768;             // layer 4: 16 x 128
+constexpr uint32_t kTcAct = kTcW4 + 4096;                 // per group 128 x 128 bf16
+constexpr uint32_t kTcBias = kTcAct + kTcGroups * 32768;  // fp32, 4 x 128 + 16
+constexpr uint32_t kTcMisc = kTcBias + (4 * kMlpHid + kMlpOutPad) * 4;
+constexpr uint32_t kTcSmem = kTcMisc + 1024;
+constexpr uint64_t kTcWaitNs = 1000000000ull;  // 1 s per MMA wait
+
+struct TcArgs {
+  StepArgs a;
+  const MlpNorm* nm;
+  GateCfg gc;
+  const __nv_bfloat16* wb;  // bf16 parameters (per layer W[out][in_pad], then b)
+  const float* w;           // fp32 parameters (biases read from here)
+  long offW[kMlpLayers], offb[kMlpLayers];
+  unsigned char* flag;          // gate: 1 = FP64 fallback
+  unsigned long long* counters;
+  float* out;                   // optional: network outputs, n x 16 (normalised units)
+  int gate;                     // 0: outputs only, every cell
+  unsigned int* err;            // bit 0: an MMA wait timed out
+};
+
+__device__ __forceinline__ uint4 pack8(const float* v) {
+  uint4 r;
+  r.x = pack_bf16(__float2bfloat16(v[0]), __float2bfloat16(v[1]));
+  r.y = pack_bf16(__float2bfloat16(v[2]), __float2bfloat16(v[3]));
+  r.z = pack_bf16(__float2bfloat16(v[4]), __float2bfloat16(v[5]));
+  r.w = pack_bf16(__float2bfloat16(v[6]), __float2bfloat16(v[7]));
+  return r;
+}
+
+__global__ void __launch_bounds__(128 * kTcGroups, 1) k_mlp_gate_tc(TcArgs p) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  const StepArgs& a = p.a;
+  const int tid = threadIdx.x, g = tid >> 7, t = tid & 127, wq = t >> 5;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + kTcMisc);         // [kTcGroups]
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kTcMisc + 16);
+  uint32_t* vote = reinterpret_cast<uint32_t*>(sm + kTcMisc + 32);    // [group][parity][warp]
+  double(*P)[9] = reinterpret_cast<double(*)[9]>(sm + kTcMisc + 128);
+  float* bias = reinterpret_cast<float*>(sm + kTcBias);
+
+  // weights into the K-major canonical layout, biases, barriers, TMEM
+  for (int i = tid; i < kMlpHid * 2; i += blockDim.x) {
+    const int n = i >> 1, kc = i & 1;
+    *reinterpret_cast<uint4*>(sm + kTcW0 + tc::kmajor_off(n, kc, 16)) =
+        *reinterpret_cast<const uint4*>(p.wb + p.offW[0] + n * 16 + kc * 8);
+  }
+  for (int l = 1; l <= 3; ++l)
+    for (int i = tid; i < kMlpHid * 16; i += blockDim.x) {
+      const int n = i >> 4, kc = i & 15;
+      *reinterpret_cast<uint4*>(sm + kTcW1 + (l - 1) * 32768 + tc::kmajor_off(n, kc, 128)) =
+          *reinterpret_cast<const uint4*>(p.wb + p.offW[l] + n * 128 + kc * 8);
     }
-    const double sc = (double)target_scale(f[11], nm->dt_pow);
-    double dY[9];
+  for (int i = tid; i < kMlpOutPad * 16; i += blockDim.x) {
+    const int n = i >> 4, kc = i & 15;
+    *reinterpret_cast<uint4*>(sm + kTcW4 + tc::kmajor_off(n, kc, 128)) =
+        *reinterpret_cast<const uint4*>(p.wb + p.offW[4] + n * 128 + kc * 8);
+  }
+  for (int i = tid; i < 4 * kMlpHid + kMlpOutPad; i += blockDim.x)
+    bias[i] = i < 4 * kMlpHid ? p.w[p.offb[i / kMlpHid] + i % kMlpHid] : p.w[p.offb[4] + (i - 4 * kMlpHid)];
+  if (tid == 0) {
+    for (int i = 0; i < kTcGroups; ++i) tc::mbar_init(tc::smem_u32(&mbar[i]), 1);
+    tc::mbar_init_fence();
+    element_projector(P);
+  }
+  if (tid < 32) tc::tmem_alloc(tc::smem_u32(tslot), 128 * kTcGroups);
+  tc::fence_async_smem();
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tbase = *tslot;
+
+  const uint32_t bar_id = 1 + g;
+  unsigned char* actp = sm + kTcAct + g * 32768;
+  const uint32_t act = tc::smem_u32(actp);
+  const uint32_t wsm = tc::smem_u32(sm);
+  const uint32_t mb = tc::smem_u32(&mbar[g]);
+  const uint32_t d_tmem = tbase + (uint32_t)g * 128u;
+  const uint32_t my_tmem = d_tmem + ((uint32_t)(wq * 32) << 16);
+  constexpr uint32_t kIdHid = tc::idesc_bf16_f32(128, 128), kIdOut = tc::idesc_bf16_f32(128, 16);
+  uint32_t phase = 0;
+  bool aborted = false;
+  unsigned long long n_sur = 0;
+  const long ntiles = (a.n + 127) / 128;
+  int par = 0;
+  for (long tile = (long)blockIdx.x * kTcGroups + g; tile < ntiles; tile += (long)gridDim.x * kTcGroups, par ^= 1) {
+    const long c = tile * 128 + t;
+    bool need = false;
+    double T0 = 0.0, rho = 0.0, dt = 1.0, y0[9];
+    float f[kMlpIn];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) {
-      dY[k] = (double)O[c * kMlpOutPad + k] * (double)nm->y_sd[k] * sc;
-      ok = ok && isfinite(dY[k]);
-    }
-    const double dT_net = (double)O[c * kMlpOutPad + 9] * (double)nm->y_sd[9] * sc;
-    ok = ok && isfinite(dT_net) && fabs(dT_net) <= gc.dT_max;
-    // element conservation (H, O, N) of the predicted increment
-    const double We[3] = {1.00794e-3, 15.9994e-3, 14.0067e-3};
+    for (int k = 0; k < 9; ++k) y0[k] = 0.0;
 #pragma unroll
-    for (int e = 0; e < 3; ++e) {
-      double r = 0.0;
+    for (int j = 0; j < kMlpIn; ++j) f[j] = 0.f;
+    if (c < a.n) {
+      T0 = a.T[c];
+      need = p.gate ? !write_if_skipped(a, c, T0) : true;
+      if (p.gate && !need) p.flag[c] = 0;
+      if (need) {
+        rho = a.rho[c];
+        dt = a.dt_cells ? a.dt_cells[c] : a.dt;
 #pragma unroll
-      for (int k = 0; k < 9; ++k) r += c_mech.elem[e][k] * We[e] / c_mech.W[k] * dY[k];
-      ok = ok && fabs(r) <= gc.elem_tol;
-    }
-    double E = 0.0;
-#pragma unroll
-    for (int k = 0; k < 9; ++k) E = E - c_mech.h_ref[k] * (dY[k] * rho / c_mech.W[k]) / dt;
-    if (ok) {
-      const double T1 = temperature_after<9>(T0, y0, dY, E * dt / rho);
-      ok = fabs((T1 - T0) - dT_net) <= gc.dT_tol;
-      if (ok) {
-#pragma unroll
-        for (int k = 0; k < 9; ++k) {
-          a.Y_prod[k * a.ld + c] = dY[k] * rho / dt;
-          a.Y_prod2[k * a.ld + c] = dY[k] * rho / c_mech.W[k];
-        }
-        a.E_f_prod[c] = E;
-        if (a.T_after) a.T_after[c] = T1;
-        if (a.status) a.status[c] = kCellSurrogate;
-        ++n_sur;
+        for (int k = 0; k < 9; ++k) y0[k] = a.Y[k * a.ld + c];
+        cell_features<9>(T0, rho, y0, dt, f);
       }
     }
-    flag[c] = ok ? 0 : 1;
+    if (aborted) {
+      if (need && p.gate) p.flag[c] = 1;
+      continue;
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, need);
+    if ((t & 31) == 0) vote[(g * 2 + par) * 4 + wq] = bal;
+    tc::bar_sync(bar_id, 128);
+    const uint32_t* vv = vote + (g * 2 + par) * 4;
+    if ((vv[0] | vv[1] | vv[2] | vv[3]) == 0u) continue;
+
+    // layer 0 operand: 16 standardised bf16 features of this thread's cell
+    {
+      float xs[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) xs[j] = (need && j < kMlpIn) ? net_input(*p.nm, j, f[j]) : 0.f;
+      *reinterpret_cast<uint4*>(actp + tc::kmajor_off(t, 0, 16)) = pack8(xs);
+      *reinterpret_cast<uint4*>(actp + tc::kmajor_off(t, 1, 16)) = pack8(xs + 8);
+    }
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    tc::bar_sync(bar_id, 128);
+    if (t == 0) {
+      tc::fence_after_sync();
+      tc::mma_bf16(d_tmem, tc::smem_desc(act, 128, 256), tc::smem_desc(wsm + kTcW0, 128, 256), kIdHid, 0);
+      tc::commit(mb);
+    }
+    bool ok = true;
+    for (int l = 0; l < 4 && ok; ++l) {
+      // epilogue of layer l: bias + GELU -> bf16 operand of layer l + 1
+      ok = __all_sync(0xffffffffu, tc::mbar_wait(mb, phase, kTcWaitNs));  // tcgen05.ld is warp-wide
+      phase ^= 1u;
+      tc::fence_after_sync();
+      if (ok) {
+        const float* bl = bias + l * kMlpHid;
+#pragma unroll 1
+        for (int q = 0; q < 4; ++q) {
+          uint32_t r[32];
+          tc::tmem_ld32(my_tmem + q * 32, r);
+          tc::tmem_ld_wait();
+          float h[32];
+#pragma unroll
+          for (int j = 0; j < 32; ++j) h[j] = gelu_f(__uint_as_float(r[j]) + bl[q * 32 + j]);
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+            *reinterpret_cast<uint4*>(actp + tc::kmajor_off(t, q * 4 + i, 128)) = pack8(h + 8 * i);
+        }
+      }
+      tc::fence_async_smem();
+      tc::fence_before_sync();
+      ok = tc::bar_and(bar_id, 128, ok);
+      if (ok && t == 0) {
+        tc::fence_after_sync();
+        const bool last = l == 3;
+        const uint32_t wl = last ? wsm + kTcW4 : wsm + kTcW1 + (uint32_t)l * 32768u;
+#pragma unroll
+        for (int s = 0; s < 8; ++s)
+          tc::mma_bf16(d_tmem, tc::smem_desc(act + s * 256, 128, 2048), tc::smem_desc(wl + s * 256, 128, 2048),
+                       last ? kIdOut : kIdHid, s > 0);
+        tc::commit(mb);
+      }
+    }
+    float o[kMlpOutPad];
+    if (ok) {
+      ok = __all_sync(0xffffffffu, tc::mbar_wait(mb, phase, kTcWaitNs));
+      phase ^= 1u;
+      tc::fence_after_sync();
+      if (ok) {
+        uint32_t r[16];
+        tc::tmem_ld16(my_tmem, r);
+        tc::tmem_ld_wait();
+#pragma unroll
+        for (int j = 0; j < kMlpOutPad; ++j) o[j] = __uint_as_float(r[j]) + bias[4 * kMlpHid + j];
+      }
+      tc::fence_before_sync();
+      ok = tc::bar_and(bar_id, 128, ok);
+    }
+    if (!ok) {
+      aborted = true;
+      if (t == 0) atomicOr(p.err, 1u);
+      if (need && p.gate) p.flag[c] = 1;
+      continue;
+    }
+    if (need) {
+      if (p.out) {
+#pragma unroll
+        for (int j = 0; j < kMlpOutPad; ++j) p.out[c * kMlpOutPad + j] = j < kMlpOut ? o[j] : 0.f;
+      }
+      if (p.gate) {
+        const bool acc = gate_active_cell(a, c, T0, rho, dt, y0, f, o, p.nm, p.gc, P);
+        n_sur += acc;
+        p.flag[c] = acc ? 0 : 1;
+      }
+    }
   }
-  if (counters) {
-    for (int o = 16; o > 0; o >>= 1) n_sur += __shfl_down_sync(0xffffffffu, n_sur, o);
-    if ((threadIdx.x & 31) == 0 && n_sur) atomicAdd(&counters[6], n_sur);
+  count_surrogate(n_sur, p.counters);
+  tc::fence_before_sync();
+  __syncthreads();
+  if (tid < 32) {
+    tc::fence_after_sync();
+    tc::tmem_dealloc(tbase, 128 * kTcGroups);
   }
 }
 
@@ -425,12 +727,18 @@ __global__ void k_colstats(long rows, int ncols, const float* M, double* out) {
   }
 }
 
+// Network inputs before standardisation (log transform of the chosen species).
+__global__ void k_transform(long n, const float* xraw, float log_mask, float log_eps, float* xt) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n * kMlpIn; i += (long)gridDim.x * blockDim.x)
+    xt[i] = net_feature(log_mask, log_eps, (int)(i % kMlpIn), xraw[i]);
+}
+
 __global__ void k_standardize(long n, const float* xraw, const float* yraw, const MlpNorm* nm,
                               __nv_bfloat16* x, float* y) {
   for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
 #pragma unroll
     for (int j = 0; j < kMlpInPad; ++j)
-      x[c * kMlpInPad + j] = __float2bfloat16(j < kMlpIn ? (xraw[c * kMlpIn + j] - nm->x_mu[j]) / nm->x_sd[j] : 0.f);
+      x[c * kMlpInPad + j] = __float2bfloat16(j < kMlpIn ? net_input(*nm, j, xraw[c * kMlpIn + j]) : 0.f);
 #pragma unroll
     for (int j = 0; j < kMlpOut; ++j) y[c * kMlpOut + j] = yraw[c * kMlpOut + j] / nm->y_sd[j];
   }
@@ -440,7 +748,7 @@ __global__ void k_standardize(long n, const float* xraw, const float* yraw, cons
 struct Surrogate {
   bool ready = false;
   bool uploaded = false;
-  GateCfg gate{1e-6, 0.5, 50.0};
+  GateCfg gate{1e-6, 1e-5, 0.1, 50.0};
   MlpNorm norm{};
   MlpNorm* d_norm = nullptr;
   // parameters: fp32 master, Adam moments, bf16 working copies, gradients
@@ -464,6 +772,11 @@ struct Surrogate {
   long icap = 0;
   __nv_bfloat16 *iX = nullptr, *iH[2] = {nullptr, nullptr};
   float* iO = nullptr;
+  // fused tcgen05 inference (default) or the unfused GEMM chain + gate
+  bool fused = true;
+  int num_sms = 0;
+  unsigned int* d_err = nullptr;  // bit 0: an MMA wait of the fused kernel timed out
+  unsigned int* h_err = nullptr;  // pinned
   // gate / compaction buffers
   long gcap = 0;
   unsigned char* flag = nullptr;
@@ -495,11 +808,17 @@ Surrogate* surrogate_create(const DevMech& dm) {
   if (cudaMalloc(&s->w, P * 4) != cudaSuccess || cudaMalloc(&s->m, P * 4) != cudaSuccess ||
       cudaMalloc(&s->v, P * 4) != cudaSuccess || cudaMalloc(&s->gr, P * 4) != cudaSuccess ||
       cudaMalloc(&s->wb, P * 2) != cudaSuccess || cudaMalloc(&s->d_norm, sizeof(MlpNorm)) != cudaSuccess ||
-      cudaMalloc(&s->d_loss, sizeof(double)) != cudaSuccess) {
+      cudaMalloc(&s->d_loss, sizeof(double)) != cudaSuccess || cudaMalloc(&s->d_err, 4) != cudaSuccess ||
+      cudaMallocHost(&s->h_err, 4) != cudaSuccess) {
     cudaGetLastError();
     s->uploaded = false;
     return s;
   }
+  cudaMemset(s->d_err, 0, 4);
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaFuncSetAttribute(k_mlp_gate_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
   cudaMemset(s->w, 0, P * 4);
   cudaMemset(s->m, 0, P * 4);
   cudaMemset(s->v, 0, P * 4);
@@ -531,13 +850,15 @@ void surrogate_destroy(Surrogate* s) {
   cudaFree(s->iX); cudaFree(s->iH[0]); cudaFree(s->iH[1]); cudaFree(s->iO);
   cudaFree(s->d_loss); cudaFree(s->flag); cudaFree(s->block_count); cudaFree(s->block_off); cudaFree(s->list);
   cudaFree(s->n_list);
+  cudaFree(s->d_err);
+  cudaFreeHost(s->h_err);
   delete s;
 }
 
 bool surrogate_ready(const Surrogate* s) { return s && s->ready && s->uploaded; }
 void surrogate_set_ready(Surrogate* s, bool r) { s->ready = r; }
-void surrogate_set_gate(Surrogate* s, double elem_tol, double dT_tol, double dT_max) {
-  s->gate = GateCfg{elem_tol, dT_tol, dT_max};
+void surrogate_set_gate(Surrogate* s, double elem_tol, double raw_elem_tol, double dT_tol, double dT_max) {
+  s->gate = GateCfg{elem_tol, raw_elem_tol, dT_tol, dT_max};
 }
 
 static std::string ck(cudaError_t e, const char* what) {
@@ -825,51 +1146,118 @@ std::string surrogate_train(Surrogate* s, long n, const __nv_bfloat16* x, const 
 
 std::string surrogate_prepare(Surrogate* s, long n, long ld, double dt, const double* dt_cells, const double* T,
                               const double* rho, const double* Y, const double* Y_prod, const double* T_after,
-                              float hull_margin, float dt_pow, __nv_bfloat16* x, float* y, cudaStream_t st) {
+                              const PrepareOpts& o, __nv_bfloat16* x, float* y, cudaStream_t st) {
   if (n <= 0) return "no training states";
-  float *xraw = nullptr, *yraw = nullptr;
+  float *xraw = nullptr, *xt = nullptr, *yraw = nullptr;
   double* stats = nullptr;
   std::string e;
+  auto release = [&]() {
+    cudaFree(xraw);
+    cudaFree(xt);
+    cudaFree(yraw);
+    cudaFree(stats);
+  };
   if ((e = ck(cudaMalloc(&xraw, n * kMlpIn * 4), "alloc raw features")).size()) return e;
-  if ((e = ck(cudaMalloc(&yraw, n * kMlpOut * 4), "alloc raw targets")).size()) { cudaFree(xraw); return e; }
-  if ((e = ck(cudaMalloc(&stats, (kMlpIn + kMlpOut) * 4 * 8), "alloc stats")).size()) {
-    cudaFree(xraw); cudaFree(yraw); return e;
-  }
+  if ((e = ck(cudaMalloc(&xt, n * kMlpIn * 4), "alloc network inputs")).size()) { release(); return e; }
+  if ((e = ck(cudaMalloc(&yraw, n * kMlpOut * 4), "alloc raw targets")).size()) { release(); return e; }
+  if ((e = ck(cudaMalloc(&stats, (2 * kMlpIn + kMlpOut) * 4 * 8), "alloc stats")).size()) { release(); return e; }
+  const float log_mask = (float)(o.log_mask & 0x1ffu);
   const int grid = (int)std::min<long>((n + 255) / 256, 148 * 16);
   k_features<<<grid, 256, 0, st>>>(n, ld, dt, dt_cells, T, rho, Y, s->d_norm, xraw, nullptr);
-  k_targets<<<grid, 256, 0, st>>>(n, ld, dt, dt_cells, T, rho, Y_prod, T_after, dt_pow, yraw);
+  k_transform<<<grid, 256, 0, st>>>(n, xraw, log_mask, o.log_eps, xt);
+  k_targets<<<grid, 256, 0, st>>>(n, ld, dt, dt_cells, T, rho, Y_prod, T_after, o.dt_pow, yraw);
   k_colstats<<<kMlpIn, 1024, 0, st>>>(n, kMlpIn, xraw, stats);
-  k_colstats<<<kMlpOut, 1024, 0, st>>>(n, kMlpOut, yraw, stats + kMlpIn * 4);
-  std::vector<double> hs((kMlpIn + kMlpOut) * 4);
+  k_colstats<<<kMlpIn, 1024, 0, st>>>(n, kMlpIn, xt, stats + kMlpIn * 4);
+  k_colstats<<<kMlpOut, 1024, 0, st>>>(n, kMlpOut, yraw, stats + 2 * kMlpIn * 4);
+  std::vector<double> hs((2 * kMlpIn + kMlpOut) * 4);
   cudaMemcpyAsync(hs.data(), stats, hs.size() * 8, cudaMemcpyDeviceToHost, st);
   if ((e = ck(cudaStreamSynchronize(st), "training statistics")).empty()) {
     MlpNorm nm{};
     for (int j = 0; j < kMlpIn; ++j) {
-      nm.x_mu[j] = (float)hs[j * 4 + 0];
-      nm.x_sd[j] = (float)std::max(hs[j * 4 + 1], 1e-12);
-      nm.x_min[j] = (float)hs[j * 4 + 2];
+      nm.x_min[j] = (float)hs[j * 4 + 2];                       // hull: raw features
       nm.x_max[j] = (float)hs[j * 4 + 3];
+      nm.x_mu[j] = (float)hs[(kMlpIn + j) * 4 + 0];             // scaling: network inputs
+      nm.x_sd[j] = (float)std::max(hs[(kMlpIn + j) * 4 + 1], 1e-12);
     }
-    for (int j = 0; j < kMlpOut; ++j) nm.y_sd[j] = (float)std::max(hs[(kMlpIn + j) * 4 + 1], 1e-30);
-    nm.hull_margin = hull_margin;
-    nm.dt_pow = dt_pow;
+    const double* ys = hs.data() + 2 * kMlpIn * 4;
+    double sd_max = 0.0;
+    for (int j = 0; j < kMlpOut - 1; ++j) sd_max = std::max(sd_max, ys[j * 4 + 1]);
+    for (int j = 0; j < kMlpOut; ++j) {
+      // one scale for all dY_k makes the loss an absolute-error loss, the
+      // measure of the tolerance |dY_k| <= const
+      const double sdj = (o.common_dY_scale && j < kMlpOut - 1) ? sd_max : ys[j * 4 + 1];
+      nm.y_sd[j] = (float)std::max(sdj, 1e-30);
+    }
+    nm.hull_margin = o.hull_margin;
+    nm.dt_pow = o.dt_pow;
+    nm.log_mask = log_mask;
+    nm.log_eps = o.log_eps;
     e = surrogate_set_norm(s, nm);
     if (e.empty()) {
       k_standardize<<<grid, 256, 0, st>>>(n, xraw, yraw, s->d_norm, x, y);
       e = ck(cudaStreamSynchronize(st), "standardize");
     }
   }
-  cudaFree(xraw);
-  cudaFree(yraw);
-  cudaFree(stats);
+  release();
   return e;
 }
 
 std::string surrogate_reserve(Surrogate* s, long n) {
-  std::string e = ensure_infer(s, n);
-  if (!e.empty()) return e;
+  if (!s->fused) {
+    std::string e = ensure_infer(s, n);
+    if (!e.empty()) return e;
+  }
   return ensure_gate(s, n);
 }
+
+static TcArgs tc_args(Surrogate* s, const StepArgs& a, unsigned long long* counters, float* out, int gate) {
+  TcArgs p{};
+  p.a = a;
+  p.nm = s->d_norm;
+  p.gc = s->gate;
+  p.wb = s->wb;
+  p.w = s->w;
+  for (int l = 0; l < kMlpLayers; ++l) {
+    p.offW[l] = s->offW[l];
+    p.offb[l] = s->offb[l];
+  }
+  p.flag = s->flag;
+  p.counters = counters;
+  p.out = out;
+  p.gate = gate;
+  p.err = s->d_err;
+  return p;
+}
+
+static cudaError_t launch_tc(Surrogate* s, const TcArgs& p, cudaStream_t st) {
+  const long ntiles = (p.a.n + 127) / 128;
+  const int grid = (int)std::max<long>(1, std::min<long>(s->num_sms > 0 ? s->num_sms : 148,
+                                                         (ntiles + kTcGroups - 1) / kTcGroups));
+  k_mlp_gate_tc<<<grid, 128 * kTcGroups, kTcSmem, st>>>(p);
+  return cudaGetLastError();
+}
+
+std::string surrogate_infer(Surrogate* s, const StepArgs& a, float* out, cudaStream_t st) {
+  if (a.n <= 0) return "";
+  std::string e = ck(launch_tc(s, tc_args(s, a, nullptr, out, 0), st), "fused inference");
+  if (!e.empty()) return e;
+  if ((e = ck(cudaStreamSynchronize(st), "fused inference")).size()) return e;
+  return surrogate_check(s, st);
+}
+
+std::string surrogate_check(Surrogate* s, cudaStream_t st) {
+  cudaMemcpyAsync(s->h_err, s->d_err, 4, cudaMemcpyDeviceToHost, st);
+  std::string e = ck(cudaStreamSynchronize(st), "surrogate error word");
+  if (!e.empty()) return e;
+  if (*s->h_err) {
+    cudaMemsetAsync(s->d_err, 0, 4, st);
+    cudaStreamSynchronize(st);
+    return "a tensor-core wait of the fused MLP kernel timed out; the affected cells were integrated in FP64";
+  }
+  return "";
+}
+
+void surrogate_set_fused(Surrogate* s, bool fused) { s->fused = fused; }
 
 cudaError_t surrogate_step(Surrogate* s, const StepArgs& a, const LaunchCfg& cfg, int* queue,
                            unsigned long long* counters, cudaStream_t st, const FallbackFn& fallback,
@@ -877,15 +1265,20 @@ cudaError_t surrogate_step(Surrogate* s, const StepArgs& a, const LaunchCfg& cfg
   (void)cfg;
   (void)queue;
   // buffers are reserved by surrogate_reserve before any graph capture
-  if (a.n > s->icap || a.n > s->gcap) return cudaErrorMemoryAllocation;
+  if (a.n > s->gcap || (!s->fused && a.n > s->icap)) return cudaErrorMemoryAllocation;
   const long n = a.n;
-  k_features<<<std::min<long>((n + 255) / 256, 148 * 16), 256, 0, st>>>(n, a.ld, a.dt, a.dt_cells, a.T, a.rho, a.Y,
-                                                                      s->d_norm, nullptr, s->iX);
-  cudaError_t e = forward_infer(s, n, s->iX, s->iO, st);
-  if (e != cudaSuccess) return e;
-  if (ph) cudaEventRecord(ph[1], st);
-  k_gate<<<std::min<long>((n + 255) / 256, 148 * 16), 256, 0, st>>>(a, s->iO, s->d_norm, s->gate, s->flag,
-                                                                  counters);
+  cudaError_t e;
+  if (s->fused) {
+    if ((e = launch_tc(s, tc_args(s, a, counters, nullptr, 1), st)) != cudaSuccess) return e;
+    if (ph) cudaEventRecord(ph[1], st);
+  } else {
+    k_features<<<std::min<long>((n + 255) / 256, 148 * 16), 256, 0, st>>>(n, a.ld, a.dt, a.dt_cells, a.T, a.rho,
+                                                                        a.Y, s->d_norm, nullptr, s->iX);
+    if ((e = forward_infer(s, n, s->iX, s->iO, st)) != cudaSuccess) return e;
+    if (ph) cudaEventRecord(ph[1], st);
+    k_gate<<<std::min<long>((n + 255) / 256, 148 * 16), 256, 0, st>>>(a, s->iO, s->d_norm, s->gate, s->flag,
+                                                                    counters);
+  }
   const int nb = (int)((n + kCompactBlock - 1) / kCompactBlock);
   k_flag_count<<<nb, kCompactBlock, 0, st>>>(n, s->flag, s->block_count);
   k_scan_counts<<<1, 1024, 0, st>>>(nb, s->block_count, s->block_off, s->n_list, counters);

@@ -27,8 +27,9 @@ std::string surrogate_reserve(Surrogate* s, long n);
 // Enqueues features -> MLP -> gate/outputs -> compaction -> FP64 fallback
 // on the cells the gate rejects.  counters[6] / [7] receive surrogate /
 // fallback cell counts.
-// ph (may be null): events recorded at phase boundaries (ph[1] gate start;
-// the fallback callback records ph[2] / ph[3] around the integrator).
+// ph (may be null): events recorded at phase boundaries: ph[1] after the
+// fused MLP + gate kernel (unfused path: after the last GEMM, before the gate
+// kernel); the fallback callback records ph[2] / ph[3] around the integrator.
 cudaError_t surrogate_step(Surrogate* s, const StepArgs& a, const LaunchCfg& cfg, int* queue,
                            unsigned long long* counters, cudaStream_t st, const FallbackFn& fallback,
                            cudaEvent_t* ph);
@@ -53,12 +54,28 @@ std::string surrogate_grad(Surrogate* s, long n, const __nv_bfloat16* x, const f
 // Adam training over n samples; loss_per_epoch (host) may be null
 std::string surrogate_train(Surrogate* s, long n, const __nv_bfloat16* x, const float* y, int epochs, int batch,
                             float lr, unsigned long long seed, float* loss_per_epoch, cudaStream_t st);
+// Choices made when the training arrays are prepared.
+struct PrepareOpts {
+  float hull_margin;    // fraction of each raw feature's range added on both sides of the hull
+  float dt_pow;         // targets are divided by (dt / 1e-6)^dt_pow
+  unsigned log_mask;    // bit k: Y_k enters the network as log10(Y_k + log_eps)
+  float log_eps;
+  int common_dY_scale;  // 1: one scale for all dY_k; 0: each its own standard deviation
+};
 // raw features and targets of integrated training states, fitted
 // standardisation and training hull, standardised bf16 x (n x 16) and y (n x 10)
 std::string surrogate_prepare(Surrogate* s, long n, long ld, double dt, const double* dt_cells, const double* T,
                               const double* rho, const double* Y, const double* Y_prod, const double* T_after,
-                              float hull_margin, float dt_pow, __nv_bfloat16* x, float* y, cudaStream_t st);
+                              const PrepareOpts& opts, __nv_bfloat16* x, float* y, cudaStream_t st);
 void surrogate_set_ready(Surrogate* s, bool ready);
-void surrogate_set_gate(Surrogate* s, double elem_tol, double dT_tol, double dT_max);
+// Inference path of surrogate_step: fused tcgen05 kernel (default) or the
+// unfused GEMM chain followed by the gate kernel.
+void surrogate_set_fused(Surrogate* s, bool fused);
+// Fused features + MLP over the n cells of a (no gate): out is n x 16 fp32
+// network outputs in normalised units; synchronises.
+std::string surrogate_infer(Surrogate* s, const StepArgs& a, float* out, cudaStream_t st);
+// Reads and clears the fused kernel's error word (after the step's work).
+std::string surrogate_check(Surrogate* s, cudaStream_t st);
+void surrogate_set_gate(Surrogate* s, double elem_tol, double raw_elem_tol, double dT_tol, double dT_max);
 
 }  // namespace nrg

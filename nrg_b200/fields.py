@@ -59,15 +59,28 @@ def _finish(name, T, p, Y, W, dt, shape, dt_cells=None) -> Field:
                  np.ascontiguousarray(Y), dt, shape, dt_cells)
 
 
+def radical_mask() -> int:
+    """Bit k set for each radical species k (mechanism order)."""
+    return sum(1 << SPECIES.index(s) for s in RADICALS)
+
+
 def random_state(n: int, rng: np.random.Generator, W: np.ndarray, T_lo: float, T_hi: float,
-                 p_lo: float = 1.0, p_hi: float = 1.0):
+                 p_lo: float = 1.0, p_hi: float = 1.0, coupled: float = 0.0):
+    """Each radical mass fraction is log-uniform on [1e-8, 1e-3].  The five
+    radicals are drawn independently, except in a fraction `coupled` of the
+    cells where they share one draw (same marginals, radical pools of one
+    size, as at a flame front)."""
     Yr, Yp, idx = _stoich(W)
     T = rng.uniform(T_lo, T_hi, n)
     c = rng.uniform(0.0, 1.0, n)
     p = P_ATM * (rng.uniform(p_lo, p_hi, n) if p_hi > p_lo else np.full(n, p_lo))
     Y = (1.0 - c)[None, :] * Yr[:, None] + c[None, :] * Yp[:, None]
-    for s in RADICALS:
-        Y[idx[s]] = 10.0 ** rng.uniform(-8.0, -3.0, n)
+    u = rng.uniform(0.0, 1.0, (len(RADICALS), n))
+    if coupled > 0.0:
+        same = rng.uniform(0.0, 1.0, n) < coupled
+        u[:, same] = u[0, same][None, :]
+    for i, s in enumerate(RADICALS):
+        Y[idx[s]] = 10.0 ** (-8.0 + 5.0 * u[i])
     return T, p, Y
 
 
@@ -98,10 +111,11 @@ def config2(W: np.ndarray, n_side: int = 1024, seed: int = 2) -> Field:
     return _finish("config2", T, p, Y, W, 1e-5, (n_side, n_side))
 
 
-def config3_pairs(W: np.ndarray, n: int, seed: int = 3) -> Field:
-    """Training states: the config-2 distribution with dt ~ log-U[1e-7, 1e-5]."""
+def config3_pairs(W: np.ndarray, n: int, seed: int = 3, coupled: float = 0.0) -> Field:
+    """Training states: the config-2 distribution with dt ~ log-U[1e-7, 1e-5]
+    (radicals shared in a fraction `coupled` of the states)."""
     rng = np.random.Generator(np.random.PCG64(seed))
-    T, p, Y = random_state(n, rng, W, 800.0, 2600.0, 0.5, 5.0)
+    T, p, Y = random_state(n, rng, W, 800.0, 2600.0, 0.5, 5.0, coupled)
     dts = 10.0 ** rng.uniform(-7.0, -5.0, n)
     return _finish("config3", T, p, Y, W, float("nan"), (n,), dts)
 

@@ -70,8 +70,24 @@ class Surrogate:
         v = np.ascontiguousarray(v, np.float32)
         _check(lib().nrg_surrogate_set_norm(self.h, v.ctypes.data), self.h)
 
-    def set_gate(self, elem_tol=1e-6, dT_tol=0.5, dT_max=50.0) -> None:
-        _check(lib().nrg_surrogate_set_gate(self.h, elem_tol, dT_tol, dT_max), self.h)
+    def set_gate(self, elem_tol=1e-6, raw_elem_tol=1e-5, dT_tol=0.1, dT_max=50.0) -> None:
+        _check(lib().nrg_surrogate_set_gate(self.h, elem_tol, raw_elem_tol, dT_tol, dT_max), self.h)
+
+    def set_inference(self, fused: bool = True) -> None:
+        """Fused tcgen05 kernel (default) or the unfused GEMM chain + gate."""
+        _check(lib().nrg_surrogate_set_inference(self.h, int(fused)), self.h)
+
+    def infer(self, f: fields.Field):
+        """Network outputs (n x 16, normalised units) of the fused kernel."""
+        import torch
+        dev = torch.device("cuda")
+        T, rho, Y = (torch.tensor(a, device=dev) for a in (f.T, f.rho, f.Y))
+        dtc = None if f.dt_cells is None else torch.tensor(f.dt_cells, device=dev)
+        out = torch.empty((f.n, 16), dtype=torch.float32, device=dev)
+        torch.cuda.synchronize()
+        _check(lib().nrg_surrogate_infer(self.h, f.n, f.n, float(f.dt if f.dt == f.dt else 1e-6), _ptr(dtc),
+                                         _ptr(T), _ptr(rho), _ptr(Y), _ptr(out)), self.h)
+        return out
 
     def enable(self, on: bool = True) -> None:
         _check(lib().nrg_surrogate_enable(self.h, int(on)), self.h)
@@ -121,12 +137,26 @@ class Surrogate:
         return x, xr
 
 
+class PrepareOpts(ctypes.Structure):
+    """nrg_surrogate_opts."""
+    _fields_ = [("hull_margin", ctypes.c_float), ("dt_pow", ctypes.c_float), ("log_mask", ctypes.c_uint),
+                ("log_eps", ctypes.c_float), ("common_dY_scale", ctypes.c_int)]
+
+
+# Training recipe (the defaults of training_pairs / train_default).
+RECIPE = dict(n_train=4_000_000, epochs=30, batch=4096, lr=1e-3, coupled=0.5, hull_margin=0.02, dt_pow=1.0,
+              log_mask=fields.radical_mask(), log_eps=1e-8, common_dY_scale=1,
+              gate=(1e-6, 1e-5, 0.1, 50.0))
+
+
 def training_pairs(solver: ChemicalKineticsSolver, W: np.ndarray, n: int, seed: int = 3,
-                   hull_margin: float = 0.02, dt_pow: float = 0.5):
+                   hull_margin: float = RECIPE["hull_margin"], dt_pow: float = RECIPE["dt_pow"],
+                   coupled: float = RECIPE["coupled"], log_mask: int = RECIPE["log_mask"],
+                   log_eps: float = RECIPE["log_eps"], common_dY_scale: int = RECIPE["common_dY_scale"]):
     """Integrates n config-3 states with their own dt (FP64 integrator) and
     returns standardised (x_bf16, y) device tensors plus timing."""
     import torch
-    f = fields.config3_pairs(W, n, seed=seed)
+    f = fields.config3_pairs(W, n, seed=seed, coupled=coupled)
     # neighbouring lanes take similar paths when states are sorted by (dt, T)
     order = np.lexsort((f.T, np.round(np.log10(f.dt_cells) * 8)))
     f = fields.Field(f.name, f.T[order], f.rho[order], f.p[order], np.ascontiguousarray(f.Y[:, order]), f.dt,
@@ -142,26 +172,29 @@ def training_pairs(solver: ChemicalKineticsSolver, W: np.ndarray, n: int, seed: 
     t_int = time.perf_counter() - t0
     x = torch.empty((n, 16), dtype=torch.bfloat16, device=dev)
     y = torch.empty((n, 10), dtype=torch.float32, device=dev)
+    opts = PrepareOpts(hull_margin, dt_pow, log_mask, log_eps, common_dY_scale)
     torch.cuda.synchronize()
     _check(lib().nrg_surrogate_prepare(solver.handle, n, n, 1.0, _ptr(dtc), _ptr(T), _ptr(rho), _ptr(Y), _ptr(Yp),
-                                       _ptr(Ta), ctypes.c_float(hull_margin), ctypes.c_float(dt_pow), _ptr(x),
-                                       _ptr(y)), solver.handle)
+                                       _ptr(Ta), ctypes.byref(opts), _ptr(x), _ptr(y)), solver.handle)
     return x, y, {"integrate_s": t_int, "integrator_stats": stats, "n": n}
 
 
-def train_default(solver: ChemicalKineticsSolver, W: np.ndarray, n_train: int = 4_000_000, epochs: int = 20,
-                  batch: int = 4096, lr: float = 1e-3, seed: int = 0, gate=(1e-6, 0.5, 50.0),
-                  dt_pow: float = 0.5) -> dict:
-    """Full recipe: pairs -> Adam training -> gate settings -> enabled."""
+def train_default(solver: ChemicalKineticsSolver, W: np.ndarray, seed: int = 0, **overrides) -> dict:
+    """Full recipe (RECIPE, with overrides): pairs -> Adam training -> gate
+    settings -> enabled."""
+    r = dict(RECIPE, **overrides)
     sur = Surrogate(solver)
     t0 = time.perf_counter()
-    x, y, info = training_pairs(solver, W, n_train, dt_pow=dt_pow)
+    x, y, info = training_pairs(solver, W, r["n_train"], hull_margin=r["hull_margin"], dt_pow=r["dt_pow"],
+                                coupled=r["coupled"], log_mask=r["log_mask"], log_eps=r["log_eps"],
+                                common_dY_scale=r["common_dY_scale"])
     sur.init(seed)
     t1 = time.perf_counter()
-    losses = sur.train(x, y, epochs=epochs, batch=batch, lr=lr, seed=seed + 1)
+    losses = sur.train(x, y, epochs=r["epochs"], batch=r["batch"], lr=r["lr"], seed=seed + 1)
     t2 = time.perf_counter()
-    sur.set_gate(*gate)
+    del x, y
+    sur.set_gate(*r["gate"])
     sur.enable(True)
-    info.update({"pairs_s": t1 - t0, "train_s": t2 - t1, "losses": losses.tolist(), "epochs": epochs,
-                 "batch": batch, "lr": lr, "dt_pow": dt_pow})
+    info.update({"pairs_s": t1 - t0, "train_s": t2 - t1, "losses": losses.tolist(),
+                 "recipe": {k: v for k, v in r.items()}})
     return info

@@ -80,3 +80,94 @@ def test_save_load_round_trip(sur, tmp_path):
     sur.load(path)
     np.testing.assert_array_equal(sur.params(), p)
     np.testing.assert_array_equal(sur.norm(), nrm)
+
+
+@pytest.fixture(scope="module")
+def fitted(solver, sur, W):
+    """Scaling fitted on 65,536 training pairs and a briefly trained network."""
+    from nrg_b200.surrogate import training_pairs
+    x, y, _ = training_pairs(solver, W, 65536, seed=9)
+    sur.init(seed=1)
+    sur.train(x, y, epochs=2, batch=1024, lr=1e-3, seed=2)
+    return sur
+
+
+def test_fused_inference_matches_unfused_and_cpu(fitted, W):
+    f = fields.slice_field(fields.config0(W), 2000)  # 15 full 128-cell tiles and a ragged one
+    out_tc = fitted.infer(f).cpu().numpy()
+    xb, _ = fitted.features(f, xraw=False)
+    out_gemm = fitted.forward(xb).cpu().numpy()
+    ref, _ = mlp_ref.forward(fitted.params(), xb.float().cpu().numpy().astype(np.float64))
+    scale = np.max(np.abs(ref[:, :10]))
+    assert np.max(np.abs(out_tc[:, :10] - ref[:, :10])) <= 2e-2 * scale
+    assert np.max(np.abs(out_tc[:, :10] - out_gemm[:, :10])) <= 2e-2 * scale
+    assert np.all(out_tc[:, 10:] == 0.0)
+
+
+def test_fused_step_matches_unfused_step(solver, fitted, W):
+    f = fields.slice_field(fields.config0(W), 3000)
+    f.T[:40] = 300.0
+    f.T[1000:2000] = 700.0  # below the training hull (T >= 800 K less 2 %): FP64 fallback
+    bc = np.zeros(f.n, np.int8)
+    bc[40:80] = 1
+    fitted.set_gate(1e-6, 1e9, 1e9, 1e9)  # open gate: the hull alone decides
+    fitted.enable(True)
+    res = {}
+    try:
+        for fused in (True, False):
+            fitted.set_inference(fused)
+            res[fused] = run_device(solver, f, "surrogate", bc=bc, y_prod2_init=np.full((9, f.n), 3.25))[0]
+    finally:
+        fitted.set_inference(True)
+        solver.set_mode("fast")
+    a, b = res[True], res[False]
+    assert np.all(a["status"][:80] == 0) and np.all(b["status"][:80] == 0)
+    assert np.all(a["Y_prod"][:, :80] == 0.0) and np.all(a["Y_prod2"][:, :80] == 3.25)
+    same = a["status"] == b["status"]
+    assert same.mean() >= 0.99, same.mean()
+    sur_both = same & (a["status"] == 5)
+    fb_both = same & (a["status"] == 1)
+    assert sur_both.sum() > 1500 and 990 <= fb_both.sum() <= 1000, (sur_both.sum(), fb_both.sum())
+    # the FP64 fallback gives the same bits whichever path chose the cell
+    np.testing.assert_array_equal(a["Y_prod"][:, fb_both], b["Y_prod"][:, fb_both])
+    np.testing.assert_array_equal(a["T_after"][fb_both], b["T_after"][fb_both])
+    d = np.abs(a["Y_prod"] - b["Y_prod"])[:, sur_both] * f.dt / f.rho[None, sur_both]
+    m = np.abs(b["Y_prod"])[:, sur_both].max() * f.dt / f.rho[sur_both].min()
+    assert d.max() <= 2e-2 * m, (d.max(), m)
+
+
+def test_trained_network_gain_on_flame_rows(decks, W):
+    """What the trained network gains over the plain FP64 integrator on 128
+    rows (262,144 cells) of the 2048 x 2048 flame field: the same step in less
+    device time, accepted cells within |dT| <= 1 K and |dY_k| <= 1e-4 of the
+    FP64 result, fallback cells bit-identical to it."""
+    from nrg_b200.chemistry import ChemicalKineticsSolver
+    from nrg_b200.surrogate import DEFAULT_MODEL, RECIPE, Surrogate
+    full = fields.config4(W)
+    f = fields.slice_field(full, 128 * 2048, offset=960 * 2048)
+    s = ChemicalKineticsSolver(None, *decks, mode="fast")
+    try:
+        s.set_launch(kernel="thread", block=64)
+        sur = Surrogate(s)
+        sur.load(DEFAULT_MODEL)
+        sur.set_gate(*RECIPE["gate"])
+        plain, st_p = run_device(s, f, "fast")
+        plain, st_p = run_device(s, f, "fast")
+        sg, st_s = run_device(s, f, "surrogate")
+        sg, st_s = run_device(s, f, "surrogate")
+    finally:
+        s.close()
+    act = plain["status"] != 0
+    acc = sg["status"] == 5
+    fb = act & ~acc
+    assert np.array_equal(sg["status"] == 0, ~act)
+    assert acc.sum() >= 0.5 * act.sum(), (acc.sum(), act.sum())
+    dT = np.abs(sg["T_after"] - plain["T_after"])[acc]
+    dYk = (np.abs(sg["Y_prod"] - plain["Y_prod"]) * f.dt / f.rho[None, :])[:, acc]
+    assert dT.max() <= 1.0 and dYk.max() <= 1e-4, (dT.max(), dYk.max())
+    np.testing.assert_array_equal(sg["Y_prod"][:, fb], plain["Y_prod"][:, fb])
+    np.testing.assert_array_equal(sg["T_after"][fb], plain["T_after"][fb])
+    gain = st_p["device_ms"] / st_s["device_ms"]
+    print(f"surrogate answers {acc.sum()} of {act.sum()} active cells; device time "
+          f"{st_p['device_ms']:.1f} ms -> {st_s['device_ms']:.1f} ms ({gain:.2f}x)")
+    assert gain > 1.2, gain
