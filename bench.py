@@ -154,19 +154,26 @@ def cpu_baseline(field, W, decks, seconds: float) -> dict:
     from nrg_b200 import fields as F
     m = op.Mechanism(*decks, 1.0, "cal.mol")
     cores = os.cpu_count() or 1
-    n0 = 2048
-    probe = F.slice_field(field, n0, stride=max(1, field.n // n0), offset=1)
+    probe = sample_cells(field, 4096, seed=1)
     t0 = time.perf_counter()
     m.chem_step(probe.dt, probe.T, probe.rho, probe.Y, threads=cores)
-    rate = n0 / max(time.perf_counter() - t0, 1e-6)
-    n = int(min(field.n, max(n0, rate * seconds)))
-    samp = F.slice_field(field, n, stride=max(1, field.n // n), offset=7)
+    rate = probe.n / max(time.perf_counter() - t0, 1e-6)
+    n = int(min(field.n, max(probe.n, rate * seconds)))
+    samp = sample_cells(field, n, seed=7)
     t0 = time.perf_counter()
     m.chem_step(samp.dt, samp.T, samp.rho, samp.Y, threads=cores)
     dt = time.perf_counter() - t0
     return {"value": n / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{n} cells, every {max(1, field.n // n)}th cell of the {field.name} field "
+            "sample": f"{n} cells drawn uniformly (seeded) from the {field.name} field "
                       f"({dt:.1f} s, OpenMP dynamic schedule)"}
+
+
+def sample_cells(field, n: int, seed: int):
+    """n cells drawn uniformly without replacement (seeded), in cell order."""
+    from nrg_b200 import fields as F
+    idx = np.sort(np.random.default_rng(seed).choice(field.n, size=min(n, field.n), replace=False))
+    return F.Field(field.name, field.T[idx].copy(), field.rho[idx].copy(), field.p[idx].copy(),
+                   np.ascontiguousarray(field.Y[:, idx]), field.dt, (len(idx),))
 
 
 # ------------------------------------------------------------ reference arm
@@ -183,13 +190,12 @@ def run_reference(args):
     m = op.Mechanism(*decks, 1.0, "cal.mol")
     cores = os.cpu_count() or 1
     # sample sized so that a step takes ~ cpu-seconds
-    n0 = 2048
-    probe = F.slice_field(field, n0, stride=max(1, field.n // n0), offset=1)
+    probe = sample_cells(field, 4096, seed=1)
     t0 = time.perf_counter()
     m.chem_step(probe.dt, probe.T, probe.rho, probe.Y, threads=cores)
-    rate = n0 / max(time.perf_counter() - t0, 1e-6)
-    n = int(min(field.n, max(n0, rate * args.cpu_seconds)))
-    samp = F.slice_field(field, n, stride=max(1, field.n // n), offset=7)
+    rate = probe.n / max(time.perf_counter() - t0, 1e-6)
+    n = int(min(field.n, max(probe.n, rate * args.cpu_seconds)))
+    samp = sample_cells(field, n, seed=7)
     for _ in range(args.warmup):
         m.chem_step(samp.dt, samp.T, samp.rho, samp.Y, threads=cores)
     t0 = time.perf_counter()
@@ -197,7 +203,7 @@ def run_reference(args):
         m.chem_step(samp.dt, samp.T, samp.rho, samp.Y, threads=cores)
     el = time.perf_counter() - t0
     value = args.steps * n / el
-    sample = (f"{n} cells per step, every {max(1, field.n // n)}th cell of the {args.n_side}x{args.n_side} flame field; "
+    sample = (f"{n} cells per step drawn uniformly (seeded) from the {args.n_side}x{args.n_side} flame field; "
               f"C restatement of the reference Fortran + SLATEC DDRIV3 path (no Fortran compiler on the box)")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
@@ -216,14 +222,15 @@ MLP_FLOPS_PER_CELL = 2 * (12 * 128 + 3 * 128 * 128 + 128 * 10)
 PROFILE = os.path.join(ROOT, "profiles", "fp64_integrator_flame.md")
 
 
-def integrator_traffic():
-    """DRAM bytes (read + write) per integrator launch on the full field, from
-    the committed ncu summary (line 'traffic_bytes_per_launch: N')."""
+def integrator_traffic(cells_integrated: float):
+    """DRAM bytes (read + write) of one integrator launch: the per-cell figure
+    of the committed ncu capture (line 'traffic_bytes_per_integrated_cell: N')
+    times the cells this launch integrated."""
     try:
         with open(PROFILE) as fh:
             for line in fh:
-                if line.startswith("traffic_bytes_per_launch:"):
-                    return float(line.split(":", 1)[1].split()[0])
+                if line.startswith("traffic_bytes_per_integrated_cell:"):
+                    return float(line.split(":", 1)[1].split()[0]) * cells_integrated
     except OSError:
         pass
     return None
@@ -380,7 +387,8 @@ def main():
         integ_flops = algorithmic_flops(ph, fm)
         integ_tf = integ_flops / max(phases["integrator_ms"], 1e-9) * 1e-9
         roof = {"bound": "fp64", "achieved": integ_tf, "peak": peak_fp64, "unit": "TFLOP/s",
-                "frac": integ_tf / peak_fp64, "traffic": integrator_traffic(),
+                "frac": integ_tf / peak_fp64,
+                "traffic": integrator_traffic(float(ph["cells_active"]) - float(ph.get("cells_surrogate", 0))),
                 "kernel": "FP64 BDF integrator (" + launch["kernel"] + "), the dominant kernel",
                 "peak_source": "measured live: dependent-FMA FP64 probe (MEASURED_PEAKS.json has no FP64 figure)",
                 "flops_per_launch": integ_flops, "flop_model": fm}

@@ -55,6 +55,7 @@ struct SmemStore {
   static constexpr int kBytesPerThread = kDoubles * 8 + N * N * (int)sizeof(LUT);
   using lut_t = LUT;
   static constexpr int kBS = BS;
+  static constexpr int kR = R;
   double* d;
   LUT* f;
   __device__ __forceinline__ void bind(char* smem, int tid) {
@@ -110,13 +111,25 @@ __device__ __forceinline__ void put(double (&v)[N], int j, double x) {
     if (i == j) v[i] = x;
 }
 
+// Correctly rounded double division kept out of line: the integrator divides
+// at dozens of sites inside unrolled species loops, and one shared copy keeps
+// the kernel small enough for the instruction cache.
+static __device__ __noinline__ double ddiv(double a, double b) { return a / b; }
+
 #define NRG_FMAX(a, b) ((a) >= (b) ? (a) : (b))
 #define NRG_FMIN(a, b) ((a) <= (b) ? (a) : (b))
 
 // -------------------------------------------------------------- thermo
 __device__ __forceinline__ int nasa_set(double t) { return t >= 1000.0 ? 1 : 0; }
 
-__device__ __forceinline__ double d_enthalpy(double T, int k) {
+// Single out-of-line copies of the thermo polynomials and of the libm calls
+// used once per cell (rate constants, energy closure): the kernel image stays
+// small enough for the instruction cache.
+static __device__ __noinline__ double nexp(double x) { return exp(x); }
+static __device__ __noinline__ double nlog(double x) { return log(x); }
+static __device__ __noinline__ double nlog10(double x) { return log10(x); }
+
+static __device__ __noinline__ double d_enthalpy(double T, int k) {
   double t = NRG_FMIN(T, 6000.0);
   const double* a = c_mech.a[k][nasa_set(t)];
   double h = a[4] / 5.0;
@@ -128,7 +141,7 @@ __device__ __forceinline__ double d_enthalpy(double T, int k) {
   return h * t;
 }
 
-__device__ __forceinline__ double d_entropy(double T, int k, double logt) {
+static __device__ __noinline__ double d_entropy(double T, int k, double logt) {
   double t = NRG_FMIN(T, 6000.0);
   const double* a = c_mech.a[k][nasa_set(t)];
   double s = a[4] / 4.0;
@@ -138,7 +151,7 @@ __device__ __forceinline__ double d_entropy(double T, int k, double logt) {
   return s * t + a[6] + a[0] * logt;
 }
 
-__device__ __forceinline__ double d_cp(double T, int k) {
+static __device__ __noinline__ double d_cp(double T, int k) {
   double t = NRG_FMIN(T, 6000.0);
   const double* a = c_mech.a[k][nasa_set(t)];
   double cp = a[4];
@@ -157,10 +170,10 @@ static __device__ __noinline__ double npow(double x, double y) { return pow(x, y
 __device__ __forceinline__ double int_pow(double x, double dnu) {
   if (dnu == 0.0) return 1.0;
   if (dnu == 1.0) return x;
-  if (dnu == -1.0) return 1.0 / x;
+  if (dnu == -1.0) return ddiv(1.0, x);
   if (dnu == 2.0) return x * x;
-  if (dnu == -2.0) return 1.0 / (x * x);
-  return pow(x, dnu);
+  if (dnu == -2.0) return ddiv(1.0, x * x);
+  return npow(x, dnu);
 }
 
 // calculate_rate_constants (chemical_kinetics_solver.f90:360-493).  The
@@ -171,13 +184,13 @@ template <int N, int R, class CS>
 __device__ void rate_constants(CS& c, double Tin) {
   const double RG = 8.31446261815324, PATM = 101325.0;
   const double T = NRG_FMIN(Tin, 10000.0);
-  const double logt = log(NRG_FMIN(T, 6000.0));
-#pragma unroll
+  const double logt = nlog(NRG_FMIN(T, 6000.0));
+#pragma unroll 1
   for (int k = 0; k < N; ++k) {
     c.z(k) = d_entropy(T, k, logt);
     c.zd(k) = d_enthalpy(T, k);
   }
-  const double conc_ref = PATM / RG / T;
+  const double conc_ref = ddiv(ddiv(PATM, RG), T);
 #pragma unroll 1
   for (int r = 0; r < R; ++r) {
     const double mc = c.kr(r);
@@ -196,34 +209,34 @@ __device__ void rate_constants(CS& c, double Tin) {
       d_h = d_h - c.zd(sp);
     }
     const int type = c_mech.type[r];
-    const double kinf = c_mech.A[r] * pow(T, c_mech.beta[r]) * exp(-(c_mech.E[r] / RG / T));
+    const double kinf = c_mech.A[r] * npow(T, c_mech.beta[r]) * nexp(-ddiv(ddiv(c_mech.E[r], RG), T));
     double k = kinf;
     if (type == 2 || type == 3 || type == 7) {
-      const double k0 = c_mech.A_low[r] * pow(T, c_mech.beta_low[r]) * exp(-(c_mech.E_low[r] / RG / T));
-      const double rp = k0 * mc / kinf;
-      k = kinf * (rp / (1.0 + rp));
+      const double k0 = c_mech.A_low[r] * npow(T, c_mech.beta_low[r]) * nexp(-ddiv(ddiv(c_mech.E_low[r], RG), T));
+      const double rp = ddiv(k0 * mc, kinf);
+      k = kinf * ddiv(rp, 1.0 + rp);
       if (type == 3) {
         const double al = c_mech.troe[r][0];
-        const double Fc = (1.0 - al) * exp(-(T / c_mech.troe[r][1])) + al * exp(-(T / c_mech.troe[r][2])) +
-                          exp(-(c_mech.troe[r][3] / T));
-        const double lf = log10(Fc);
+        const double Fc = (1.0 - al) * nexp(-ddiv(T, c_mech.troe[r][1])) + al * nexp(-ddiv(T, c_mech.troe[r][2])) +
+                          nexp(-ddiv(c_mech.troe[r][3], T));
+        const double lf = nlog10(Fc);
         const double cc = -0.4 - 0.67 * lf;
         const double nn = 0.75 - 1.27 * lf;
         double blend;
         if (rp != 0.0) {
-          const double lr = log10(rp);
-          const double x = (lr + cc) / (nn - 0.14 * (lr + cc));
-          blend = pow(Fc, 1.0 / (1.0 + x * x));
+          const double lr = nlog10(rp);
+          const double x = ddiv(lr + cc, nn - 0.14 * (lr + cc));
+          blend = npow(Fc, ddiv(1.0, 1.0 + x * x));
         } else {
-          blend = pow(Fc, -1.0 / 0.14);
+          blend = npow(Fc, ddiv(-1.0, 0.14));
         }
         k = k * blend;
       }
     }
     double kr = 0.0;
     if (type < 5) {
-      const double Kp = exp(d_s / RG - d_h / RG / T);
-      kr = k / (Kp * int_pow(conc_ref, c_mech.dnu[r]));
+      const double Kp = nexp(ddiv(d_s, RG) - ddiv(ddiv(d_h, RG), T));
+      kr = ddiv(k, Kp * int_pow(conc_ref, c_mech.dnu[r]));
     }
     c.kf(r) = m_left ? k * mc : k;
     c.kr(r) = m_right ? kr * mc : kr;
@@ -236,7 +249,7 @@ template <int N, int R, class CS>
 __device__ __forceinline__ void rhs(CS& c) {
 #pragma unroll
   for (int k = 0; k < N; ++k) c.zd(k) = 0.0;
-#pragma unroll 4
+#pragma unroll 1
   for (int r = 0; r < R; ++r) {
     double f = c.kf(r);
     for (int i = 0; i < c_mech.nl[r]; ++i) {
@@ -341,13 +354,13 @@ __device__ void jac_vec(CS& c) {
 // state machine over an unrolled loop (phases 1-4 of the reference's
 // ASSIGN/GO TO form: zero, small-scaled, mid-range, large-scaled).
 template <int N>
-__device__ __forceinline__ double dnrm2(const double (&dx)[N]) {
+__device__ __noinline__ double dnrm2_nl(const double* dx) {
   const double cutlo = 8.232e-11, cuthi = 1.304e19;
   const double hitest = cuthi / (double)N;
   enum { S30, S50, S70, S85, S110 };
   int st = S30;
   double sum = 0.0, xmax = 0.0;
-#pragma unroll
+#pragma unroll 1
   for (int i = 0; i < N; ++i) {
     const double x = dx[i], ax = fabs(x);
     if (st == S30) {
@@ -361,7 +374,7 @@ __device__ __forceinline__ double dnrm2(const double (&dx)[N]) {
       } else {
         st = S70;
         xmax = ax;
-        const double q = x / xmax;
+        const double q = ddiv(x, xmax);
         sum = sum + q * q;
         continue;
       }
@@ -374,10 +387,10 @@ __device__ __forceinline__ double dnrm2(const double (&dx)[N]) {
     }
     if (st == S70 || st == S110) {
       if (ax <= xmax) {
-        const double q = x / xmax;
+        const double q = ddiv(x, xmax);
         sum = sum + q * q;
       } else {
-        const double q = xmax / x;
+        const double q = ddiv(xmax, x);
         sum = 1.0 + sum * (q * q);
         xmax = ax;
       }
@@ -385,9 +398,9 @@ __device__ __forceinline__ double dnrm2(const double (&dx)[N]) {
     }
     // S85: mid-range, unscaled
     if (ax >= hitest) {
-      sum = (sum / x) / x;
+      sum = ddiv(ddiv(sum, x), x);
       xmax = ax;
-      const double q = x / xmax;
+      const double q = ddiv(x, xmax);
       sum = sum + q * q;
       st = S110;
     } else {
@@ -395,6 +408,14 @@ __device__ __forceinline__ double dnrm2(const double (&dx)[N]) {
     }
   }
   return st == S85 ? sqrt(sum) : xmax * sqrt(sum);
+}
+
+template <int N>
+__device__ __forceinline__ double dnrm2(const double (&dx)[N]) {
+  double t[N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) t[i] = dx[i];
+  return dnrm2_nl<N>(t);
 }
 
 // dgefa.f90:60-117 on the shared-memory matrix (column-major a(j, i) = A(i, j))
@@ -454,7 +475,7 @@ __device__ __forceinline__ void dgesl(CS& c, double (&b)[N]) {
   }
 #pragma unroll
   for (int k = N - 1; k >= 0; --k) {
-    b[k] = b[k] / (double)c.a(k, k);
+    b[k] = ddiv(b[k], (double)c.a(k, k));
     const double t = -b[k];
     if (t != 0.0) {
 #pragma unroll
@@ -498,9 +519,13 @@ __device__ __noinline__ void nl_rate_constants(double* d, LUT* f, double T) {
 }
 
 // --------------------------------------------------------- SLATEC pieces
-template <int N, class CS>
-__device__ __forceinline__ void ddpsc(int ksgn, CS& c) {
-  const int nq = c.nq;
+// ddpsc.f90:22-40 on the Nordsieck array (shared memory only, so one
+// out-of-line copy serves every call site).
+template <int N, int R, typename LUT, int BS>
+__device__ __noinline__ void nl_ddpsc(double* d, LUT* f, int ksgn, int nq) {
+  SmemStore<N, R, LUT, BS> c;
+  c.d = d;
+  c.f = f;
   for (int j1 = 1; j1 <= nq; ++j1)
     for (int j2 = j1; j2 <= nq; ++j2) {
       const int j = nq - j2 + j1;  // 1-based column
@@ -515,20 +540,36 @@ __device__ __forceinline__ void ddpsc(int ksgn, CS& c) {
 }
 
 template <int N, class CS>
-__device__ __forceinline__ void ddscl(CS& c, double rh) {
+__device__ __forceinline__ void ddpsc(int ksgn, CS& c) {
+  nl_ddpsc<N, CS::kR, typename CS::lut_t, CS::kBS>(c.d, c.f, ksgn, c.nq);
+}
+
+// ddscl.f90:20-37: limits rh, rescales columns 1..nq of the Nordsieck array;
+// returns the rh applied.
+template <int N, int R, typename LUT, int BS>
+__device__ __noinline__ double nl_ddscl(double* d, LUT* f, int nq, double h, double rmax, double rh) {
+  SmemStore<N, R, LUT, BS> c;
+  c.d = d;
+  c.f = f;
   const double hmax = c_mech.hmax;
-  if (c.h < 1.0) {
-    const double ah = fabs(c.h);
-    rh = NRG_FMIN(NRG_FMIN(ah * rh, ah * c.rmax), hmax) / ah;
+  if (h < 1.0) {
+    const double ah = fabs(h);
+    rh = ddiv(NRG_FMIN(NRG_FMIN(ah * rh, ah * rmax), hmax), ah);
   } else {
-    rh = NRG_FMIN(NRG_FMIN(rh, c.rmax), hmax / fabs(c.h));
+    rh = NRG_FMIN(NRG_FMIN(rh, rmax), ddiv(hmax, fabs(h)));
   }
   double r1 = 1.0;
-  for (int j = 1; j <= c.nq; ++j) {
+  for (int j = 1; j <= nq; ++j) {
     r1 = r1 * rh;
 #pragma unroll
     for (int i = 0; i < N; ++i) c.yh(j, i) = c.yh(j, i) * r1;
   }
+  return rh;
+}
+
+template <int N, class CS>
+__device__ __forceinline__ void ddscl(CS& c, double rh) {
+  rh = nl_ddscl<N, CS::kR, typename CS::lut_t, CS::kBS>(c.d, c.f, c.nq, c.h, c.rmax, rh);
   c.h = c.h * rh;
   c.rc = c.rc * rh;
 }
@@ -548,9 +589,9 @@ __device__ void ddntl(CS& c) {
   rhs_at<N, R>(c, c.y, c.s2);
   c.nfe += 1;
 #pragma unroll
-  for (int i = 0; i < N; ++i) c.s1[i] = c.s2[i] / NRG_FMAX(1.0, c.ywt[i]);
-  const double sum = dnrm2<N>(c.s1) / sqrt((double)N);
-  if (sum > c.eps / fabs(c.h)) c.h = copysign(c.eps / sum, c.h);
+  for (int i = 0; i < N; ++i) c.s1[i] = ddiv(c.s2[i], NRG_FMAX(1.0, c.ywt[i]));
+  const double sum = ddiv(dnrm2<N>(c.s1), sqrt((double)N));
+  if (sum > ddiv(c.eps, fabs(c.h))) c.h = copysign(ddiv(c.eps, sum), c.h);
 #pragma unroll
   for (int i = 0; i < N; ++i) c.yh(1, i) = c.h * c.s2[i];
 #pragma unroll
@@ -590,7 +631,7 @@ __device__ void ddpst(CS& c) {
       c.z(j) = yj + dy;
       nl_rhs<N, R, typename CS::lut_t, CS::kBS>(c.d, c.f);
       c.z(j) = yj;
-      const double factor = -(el1h / dy);
+      const double factor = -ddiv(el1h, dy);
       double diff = -1.0, s2m = 0.0, s1m = 0.0;
 #pragma unroll
       for (int i = 0; i < N; ++i) {
@@ -652,9 +693,9 @@ __device__ double ddcor(CS& c) {
 #pragma unroll
   for (int i = 0; i < N; ++i) {
     c.s1[i] = c.s1[i] + x[i];
-    c.s2[i] = x[i] / NRG_FMAX(fabs(c.y[i]), c.ywt[i]);
+    c.s2[i] = ddiv(x[i], NRG_FMAX(fabs(c.y[i]), c.ywt[i]));
   }
-  return dnrm2<N>(c.s2) / sqrt((double)N);
+  return ddiv(dnrm2<N>(c.s2), sqrt((double)N));
 }
 
 // One DDSTP call (ddstp.f90:72-459); returns JSTATE (1 ok, 2 h vanished,
@@ -670,11 +711,8 @@ __device__ int ddstp(CS& c) {
   int ntry = 0, nfail = 0, iter = 0;
   bool evaljc;
   double told = c.t, ctest = 0.0, d = 0.0, d1 = 0.0, etest, rh;
-  if (c.jtask <= 0) {
-    ddntl<N, R>(c);
-    if (c.h == 0.0) goto L400;
-    if (c.ier) goto L420;
-  }
+  bool restart = false;  // ddntl after MXFAIL failures (then RMAX = RMNORM)
+  if (c.jtask <= 0) goto L_NTL;
 L100:
   ntry = ntry + 1;
   if (ntry > MXTRY) goto L410;
@@ -698,7 +736,7 @@ L110:
   for (int i = 0; i < N; ++i) c.s1[i] = 0.0;
 L130:
   d = ddcor<N, R, LUT>(c);
-  if (iter > 0) c.trend = NRG_FMAX(0.9 * c.trend, d / d1);
+  if (iter > 0) c.trend = NRG_FMAX(0.9 * c.trend, ddiv(d, d1));
   d1 = d;
   ctest = NRG_FMIN(2.0 * c.trend, 1.0) * d;
   if (ctest <= eps) goto L170;
@@ -720,30 +758,30 @@ L160:
   ddpsc<N>(-1, c);
   c.nwait = c.nq + 2;
   if (c.jtask != 0 && c.jtask != 2) c.rmax = RMFAIL;
-  rh = (iter == 0) ? 0.3 : 0.9 * npow(eps / ctest, 0.2);
+  rh = (iter == 0) ? 0.3 : 0.9 * npow(ddiv(eps, ctest), 0.2);
   if (rh * c.h == 0.0) goto L400;
   ddscl<N>(c, rh);
   goto L100;
 L170:
   c.convrg = 1;
 #pragma unroll
-  for (int i = 0; i < N; ++i) c.s2[i] = c.s1[i] / NRG_FMAX(fabs(c.y[i]), c.ywt[i]);
-  etest = dnrm2<N>(c.s2) / (TQ(2, c.nq) * sqn);
+  for (int i = 0; i < N; ++i) c.s2[i] = ddiv(c.s1[i], NRG_FMAX(fabs(c.y[i]), c.ywt[i]));
+  etest = ddiv(dnrm2<N>(c.s2), TQ(2, c.nq) * sqn);
   if (etest > eps) {
     c.t = told;
     ddpsc<N>(-1, c);
     nfail = nfail + 1;
     if (nfail < MXFAIL || c.nq == 1) {
       if (c.jtask != 0 && c.jtask != 2) c.rmax = RMFAIL;
-      const double rh2 = 1.0 / (BIAS2 * npow(etest / eps, 1.0 / (double)(c.nq + 1)));
+      const double rh2 = ddiv(1.0, BIAS2 * npow(ddiv(etest, eps), ddiv(1.0, (double)(c.nq + 1))));
       if (c.nq > 1) {
 #pragma unroll
-        for (int i = 0; i < N; ++i) c.s2[i] = c.yh(c.nq, i) / NRG_FMAX(fabs(c.y[i]), c.ywt[i]);
-        const double erdn = dnrm2<N>(c.s2) / (TQ(1, c.nq) * sqn);
-        const double rh1 = 1.0 / NRG_FMAX(1.0, BIAS1 * npow(erdn / eps, 1.0 / (double)c.nq));
+        for (int i = 0; i < N; ++i) c.s2[i] = ddiv(c.yh(c.nq, i), NRG_FMAX(fabs(c.y[i]), c.ywt[i]));
+        const double erdn = ddiv(dnrm2<N>(c.s2), TQ(1, c.nq) * sqn);
+        const double rh1 = ddiv(1.0, NRG_FMAX(1.0, BIAS1 * npow(ddiv(erdn, eps), ddiv(1.0, (double)c.nq))));
         if (rh2 < rh1) {
           c.nq = c.nq - 1;
-          c.rc = c.rc * EL(1, c.nq) / EL(1, c.nq + 1);
+          c.rc = ddiv(c.rc * EL(1, c.nq), EL(1, c.nq + 1));
           rh = rh1;
         } else {
           rh = rh2;
@@ -760,11 +798,8 @@ L170:
     c.jtask = 2;
 #pragma unroll
     for (int i = 0; i < N; ++i) c.y[i] = c.yh(0, i);
-    ddntl<N, R>(c);
-    c.rmax = RMNORM;
-    if (c.h == 0.0) goto L400;
-    if (c.ier) goto L420;
-    goto L100;
+    restart = true;
+    goto L_NTL;
   }
   c.nstep += 1;
   for (int j = 0; j <= c.nq; ++j) {
@@ -775,7 +810,7 @@ L170:
 #pragma unroll
   for (int i = 0; i < N; ++i) c.y[i] = c.yh(0, i);
   if (c.jtask == 0 || c.jtask == 2) {
-    rh = 1.0 / NRG_FMAX(uround, BIAS2 * npow(etest / eps, 1.0 / (double)(c.nq + 1)));
+    rh = ddiv(1.0, NRG_FMAX(uround, BIAS2 * npow(ddiv(etest, eps), ddiv(1.0, (double)(c.nq + 1)))));
     if (rh > TRSHLD) ddscl<N>(c, rh);
   } else if (c.nwait > 1) {
     c.nwait = c.nwait - 1;
@@ -789,25 +824,25 @@ L170:
       rh1 = 0.0;
     } else {
 #pragma unroll
-      for (int i = 0; i < N; ++i) c.s2[i] = c.yh(c.nq, i) / NRG_FMAX(fabs(c.y[i]), c.ywt[i]);
-      const double erdn = dnrm2<N>(c.s2) / (TQ(1, c.nq) * sqn);
-      rh1 = 1.0 / NRG_FMAX(uround, BIAS1 * npow(erdn / eps, 1.0 / (double)c.nq));
+      for (int i = 0; i < N; ++i) c.s2[i] = ddiv(c.yh(c.nq, i), NRG_FMAX(fabs(c.y[i]), c.ywt[i]));
+      const double erdn = ddiv(dnrm2<N>(c.s2), TQ(1, c.nq) * sqn);
+      rh1 = ddiv(1.0, NRG_FMAX(uround, BIAS1 * npow(ddiv(erdn, eps), ddiv(1.0, (double)c.nq))));
     }
-    rh2 = 1.0 / NRG_FMAX(uround, BIAS2 * npow(etest / eps, 1.0 / (double)(c.nq + 1)));
+    rh2 = ddiv(1.0, NRG_FMAX(uround, BIAS2 * npow(ddiv(etest, eps), ddiv(1.0, (double)(c.nq + 1)))));
     if (c.nq == kMaxOrd) {
       rh3 = 0.0;
     } else {
 #pragma unroll
       for (int i = 0; i < N; ++i)
-        c.s2[i] = (c.s1[i] - c.yh(kMaxOrd, i)) / NRG_FMAX(fabs(c.y[i]), c.ywt[i]);
-      const double erup = dnrm2<N>(c.s2) / (TQ(3, c.nq) * sqn);
-      rh3 = 1.0 / NRG_FMAX(uround, BIAS3 * npow(erup / eps, 1.0 / (double)(c.nq + 2)));
+        c.s2[i] = ddiv(c.s1[i] - c.yh(kMaxOrd, i), NRG_FMAX(fabs(c.y[i]), c.ywt[i]));
+      const double erup = ddiv(dnrm2<N>(c.s2), TQ(3, c.nq) * sqn);
+      rh3 = ddiv(1.0, NRG_FMAX(uround, BIAS3 * npow(ddiv(erup, eps), ddiv(1.0, (double)(c.nq + 2)))));
     }
     if (rh1 > rh2 && rh1 >= rh3) {
       rh = rh1;
       if (rh <= TRSHLD) goto L380;
       c.nq = c.nq - 1;
-      c.rc = c.rc * EL(1, c.nq) / EL(1, c.nq + 1);
+      c.rc = ddiv(c.rc * EL(1, c.nq), EL(1, c.nq + 1));
     } else if (rh2 >= rh1 && rh2 >= rh3) {
       rh = rh2;
       if (rh <= TRSHLD) goto L380;
@@ -816,9 +851,9 @@ L170:
       if (rh <= TRSHLD) goto L380;
       const double e = EL(c.nq + 1, c.nq);
 #pragma unroll
-      for (int i = 0; i < N; ++i) c.yh(c.nq + 1, i) = c.s1[i] * e / (double)(c.nq + 1);
+      for (int i = 0; i < N; ++i) c.yh(c.nq + 1, i) = ddiv(c.s1[i] * e, (double)(c.nq + 1));
       c.nq = c.nq + 1;
-      c.rc = c.rc * EL(1, c.nq) / EL(1, c.nq - 1);
+      c.rc = ddiv(c.rc * EL(1, c.nq), EL(1, c.nq - 1));
     }
     ddscl<N>(c, rh);
     c.rmax = RMNORM;
@@ -826,6 +861,13 @@ L170:
     c.nwait = c.nq + 2;
   }
   return 1;
+L_NTL:
+  // the one inlined copy of DDNTL (first step and restart after failures)
+  ddntl<N, R>(c);
+  if (restart) c.rmax = RMNORM;
+  if (c.h == 0.0) goto L400;
+  if (c.ier) goto L420;
+  goto L100;
 L400:
 #pragma unroll
   for (int i = 0; i < N; ++i) c.y[i] = c.yh(0, i);
@@ -901,8 +943,8 @@ __device__ int cell_advance(CS& c, int mxstep) {
 #pragma unroll
   for (int i = 0; i < N; ++i) c.ywt[i] = NRG_FMAX(c_mech.ewt, fabs(c.y[i]));
 #pragma unroll
-  for (int i = 0; i < N; ++i) c.s2[i] = c.y[i] / c.ywt[i];
-  const double sum = NRG_FMAX(1.0, dnrm2<N>(c.s2) / sqrt((double)N));
+  for (int i = 0; i < N; ++i) c.s2[i] = ddiv(c.y[i], c.ywt[i]);
+  const double sum = NRG_FMAX(1.0, ddiv(dnrm2<N>(c.s2), sqrt((double)N)));
   if (c.eps < sum * c_mech.uround) {
     c.eps = sum * c_mech.uround * (1.0 + 10.0 * c_mech.uround);
 #pragma unroll
@@ -924,7 +966,7 @@ __device__ int cell_advance(CS& c, int mxstep) {
   if (c.t < c.tout) return 0;
 #pragma unroll
   for (int i = 0; i < N; ++i) c.y[i] = c.yh(c.nq, i);
-  const double r = (c.tout - c.t) / c.h;
+  const double r = ddiv(c.tout - c.t, c.h);
   for (int jj = 1; jj <= c.nq; ++jj) {
     const int j = c.nq - jj;
 #pragma unroll
@@ -938,34 +980,34 @@ __device__ int cell_advance(CS& c, int mxstep) {
 // table_approximated_real_gas.f90:404-440 -> calculate_temperature,
 // thermophysical_properties_class.f90:409-452).
 template <int N>
-__device__ double temperature_after(double T0, const double (&Y0)[N], const double (&dY)[N], double dE) {
+__device__ __noinline__ double temperature_after_nl(double T0, const double* Y0, const double* dY, double dE) {
   const double RG = 8.31446261815324;
   double X[N], avg = 0.0;
-#pragma unroll
-  for (int k = 0; k < N; ++k) avg = avg + Y0[k] / c_mech.W[k];
-  const double W0 = 1.0 / avg;
+#pragma unroll 1
+  for (int k = 0; k < N; ++k) avg = avg + ddiv(Y0[k], c_mech.W[k]);
+  const double W0 = ddiv(1.0, avg);
   double e0 = 0.0, h0 = 0.0;
-#pragma unroll
+#pragma unroll 1
   for (int k = 0; k < N; ++k) {
-    X[k] = Y0[k] / c_mech.W[k] * W0;
+    X[k] = ddiv(Y0[k], c_mech.W[k]) * W0;
     e0 = e0 + (d_enthalpy(T0, k) - RG * T0) * X[k];
   }
-#pragma unroll
+#pragma unroll 1
   for (int k = 0; k < N; ++k) h0 = h0 + c_mech.h_ref[k] * X[k];
-  const double e1 = (e0 - h0) / W0 + dE;
+  const double e1 = ddiv(e0 - h0, W0) + dE;
   avg = 0.0;
   double Y1[N];
-#pragma unroll
+#pragma unroll 1
   for (int k = 0; k < N; ++k) {
     Y1[k] = Y0[k] + dY[k];
-    avg = avg + Y1[k] / c_mech.W[k];
+    avg = avg + ddiv(Y1[k], c_mech.W[k]);
   }
-  const double W1 = 1.0 / avg;
+  const double W1 = ddiv(1.0, avg);
   double hc = 0.0, cp = 0.0;
   double temp = NRG_FMIN(T0, 6000.0);
-#pragma unroll
+#pragma unroll 1
   for (int k = 0; k < N; ++k) {
-    X[k] = Y1[k] / c_mech.W[k] * W1;
+    X[k] = ddiv(Y1[k], c_mech.W[k]) * W1;
     hc = hc + c_mech.h_ref[k] * X[k];
     cp = cp + d_cp(temp, k) * X[k];
   }
@@ -973,13 +1015,25 @@ __device__ double temperature_after(double T0, const double (&Y0)[N], const doub
   const double tol = (double)1e-08f;  // single-precision literal in the reference
   for (int it = 0; it < 1000; ++it) {
     double e = 0.0;
-#pragma unroll
+#pragma unroll 1
     for (int k = 0; k < N; ++k) e = e + (d_enthalpy(temp, k) - RG * temp) * X[k];
-    const double res = (ei - (e - hc)) / cp;
+    const double res = ddiv(ei - (e - hc), cp);
     temp = temp + res;
     if (fabs(res) < tol) break;
   }
   return temp;
+}
+
+template <int N>
+__device__ __forceinline__ double temperature_after(double T0, const double (&Y0)[N], const double (&dY)[N],
+                                                    double dE) {
+  double a[N], b[N];
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    a[k] = Y0[k];
+    b[k] = dY[k];
+  }
+  return temperature_after_nl<N>(T0, a, b, dE);
 }
 
 // Outputs of a finished cell (chemical_kinetics_solver.f90:318-340).
