@@ -143,11 +143,11 @@ NRG_API int nrg_chem_step_device_noalloc(nrg_chem* h, double time_step, long n, 
 NRG_API int nrg_chem_set_mode(nrg_chem* h, int mode);
 
 /* Launch shape.  kernel: 0 = one thread per cell over a grid covering the
- * cells, 1 = one thread per cell pulling cells from a device work queue,
- * 2 = one warp per cell pulling cells from the work queue (default).  block:
- * 64 for kernels 0/1 (each cell keeps ~1.7 KB in shared memory), 128 or 256
- * for kernel 2.  grid: persistent grid size (0 = fill the GPU).  chunk: cells
- * reserved per queue fetch (1..64). */
+ * cells (default), 1 = one thread per cell pulling cells from a device work
+ * queue, 2 = one warp per cell pulling cells from the work queue.  block: 32
+ * (default) or 64 for kernels 0/1 (each cell keeps ~1.6 KB in shared memory),
+ * 128 or 256 for kernel 2.  grid: persistent grid size (0 = fill the GPU).
+ * chunk: cells reserved per queue fetch (1..64). */
 NRG_API int nrg_chem_set_launch(nrg_chem* h, int kernel, int block, int grid, int chunk);
 NRG_API int nrg_chem_get_launch(nrg_chem* h, int* kernel, int* block, int* grid, int* chunk);
 

@@ -373,8 +373,8 @@ extern "C" int nrg_chem_create(const char* mechanism_path, const char* thermo_pa
     nrg_chem_destroy(h);
     return fail(nullptr, NRG_ERR_CUDA, msg);
   }
-  h->cfg.kernel = nrg::kKernelWarpQueue;
-  h->cfg.block = 256;
+  h->cfg.kernel = nrg::kKernelThreadGrid;  // the fastest shape measured on the flame field
+  h->cfg.block = 32;
   h->cfg.grid = 0;
   h->cfg.chunk = 1;
   h->sur = nrg::surrogate_create(h->dm);
@@ -412,10 +412,10 @@ extern "C" int nrg_chem_set_mode(nrg_chem* h, int mode) {
 extern "C" int nrg_chem_set_launch(nrg_chem* h, int kernel, int block, int grid, int chunk) {
   if (!h) return NRG_ERR_ARG;
   const bool ok_kernel = kernel >= 0 && kernel <= 2;
-  const bool ok_block = kernel == 2 ? (block == 128 || block == 256) : block == 64;
+  const bool ok_block = kernel == 2 ? (block == 128 || block == 256) : (block == 32 || block == 64);
   if (!ok_kernel || !ok_block || chunk < 1 || chunk > 64 || grid < 0)
     return fail(h, NRG_ERR_ARG,
-                "launch shape out of range (kernel 0/1: block 64; kernel 2: block 128 or 256; chunk 1..64)");
+                "launch shape out of range (kernel 0/1: block 32 or 64; kernel 2: block 128 or 256; chunk 1..64)");
   h->cfg.kernel = kernel;
   h->cfg.block = block;
   h->cfg.grid = grid;
@@ -582,17 +582,18 @@ extern "C" int nrg_chem_autotune(nrg_chem* h, double time_step, long n, long ld,
   a.cell_list = nullptr;
   a.n_list = 0;
   a.n_list_dev = nullptr;
+  // candidate shapes: warp per cell (occupancy-derived persistent grid),
+  // thread per cell from the work queue (1 or 2 blocks of 64 per SM, chunk 1
+  // or 2) and thread per cell over the plain grid (32- or 64-thread blocks)
   std::vector<LaunchCfg> cands;
-  for (int block : {128, 256})
-    for (int per_sm : {0, 1, 2, 4})
-      for (int chunk : {1, 4}) {
-        LaunchCfg c;
-        c.kernel = nrg::kKernelWarpQueue;
-        c.block = block;
-        c.grid = per_sm * h->num_sms;  // 0: occupancy-derived
-        c.chunk = chunk;
-        cands.push_back(c);
-      }
+  for (int block : {128, 256}) {
+    LaunchCfg c;
+    c.kernel = nrg::kKernelWarpQueue;
+    c.block = block;
+    c.grid = 0;
+    c.chunk = 1;
+    cands.push_back(c);
+  }
   for (int per_sm : {1, 2})
     for (int chunk : {1, 2}) {
       LaunchCfg c;
@@ -602,10 +603,10 @@ extern "C" int nrg_chem_autotune(nrg_chem* h, double time_step, long n, long ld,
       c.chunk = chunk;
       cands.push_back(c);
     }
-  {
+  for (int block : {32, 64}) {
     LaunchCfg c;
     c.kernel = nrg::kKernelThreadGrid;
-    c.block = 64;
+    c.block = block;
     cands.push_back(c);
   }
   cudaStream_t s = h->stream;

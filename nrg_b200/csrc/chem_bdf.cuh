@@ -51,7 +51,8 @@ struct SmemStore {
   static constexpr int kZ = kKR + R;
   static constexpr int kZD = kZ + N;
   static constexpr int kW = kZD + N;
-  static constexpr int kDoubles = kW + N;
+  // w (Jacobian-vector input) is used only by the FP32-LU refinement
+  static constexpr int kDoubles = kW + (sizeof(LUT) == 4 ? N : 0);
   static constexpr int kBytesPerThread = kDoubles * 8 + N * N * (int)sizeof(LUT);
   using lut_t = LUT;
   static constexpr int kBS = BS;

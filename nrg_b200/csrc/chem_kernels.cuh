@@ -199,7 +199,10 @@ static cudaError_t launch_warp(const StepArgs& a, const LaunchCfg& cfg, int* que
 }
 
 // Launches one (JAC, LUT) variant: cfg.kernel selects thread-per-cell (grid
-// or work queue, 64-thread blocks) or warp-per-cell (128- or 256-thread blocks).
+// or work queue, 32- or 64-thread blocks) or warp-per-cell (128- or 256-thread
+// blocks).  With 32-thread blocks every warp is its own block, so an SM slot
+// is handed to a new block as soon as the warp's cells are done instead of
+// waiting for the slowest warp of a larger block.
 template <int N, int R, int JAC, typename LUT>
 static cudaError_t launch_variant(const StepArgs& a, const LaunchCfg& cfg, int* queue,
                                   unsigned long long* counters, cudaStream_t s) {
@@ -210,8 +213,11 @@ static cudaError_t launch_variant(const StepArgs& a, const LaunchCfg& cfg, int* 
       default: return cudaErrorInvalidValue;
     }
   }
-  if (cfg.block != 64) return cudaErrorInvalidValue;
-  return launch_bs<N, R, JAC, LUT, 64>(a, cfg, queue, counters, s);
+  switch (cfg.block) {
+    case 32: return launch_bs<N, R, JAC, LUT, 32>(a, cfg, queue, counters, s);
+    case 64: return launch_bs<N, R, JAC, LUT, 64>(a, cfg, queue, counters, s);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 }  // namespace nrg

@@ -35,8 +35,8 @@ struct StepArgs {
 enum KernelKind { kKernelThreadGrid = 0, kKernelThreadQueue = 1, kKernelWarpQueue = 2 };
 
 struct LaunchCfg {
-  int kernel = kKernelWarpQueue;  // KernelKind
-  int block = 256;                // threads per block
+  int kernel = kKernelThreadGrid;  // KernelKind
+  int block = 32;                  // threads per block
   int grid = 0;                   // persistent grid (0: fill the GPU)
   int chunk = 1;                  // cells reserved per queue fetch (per lane or per warp)
 };

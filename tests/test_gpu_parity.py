@@ -72,13 +72,25 @@ def test_launch_shapes_and_graph_agree(solver, W):
     solver.set_launch(kernel="warp_queue", block=256, grid=0, chunk=1)
 
 
-@pytest.mark.parametrize("kernel", ["thread", "thread_queue"])
-def test_thread_per_cell_kernels_parity(solver, oracle_mech, W, kernel):
+@pytest.mark.parametrize("kernel,block", [("thread", 64), ("thread", 32), ("thread_queue", 64),
+                                          ("thread_queue", 32)])
+def test_thread_per_cell_kernels_parity(solver, oracle_mech, W, kernel, block):
     f = fields.slice_field(fields.config0(W), 1024)
     o = oracle_run(oracle_mech, f)
     for mode in ("reference", "fast"):
-        g, _ = run_device(solver, f, mode, launch=dict(kernel=kernel, block=64, grid=0, chunk=1))
+        g, _ = run_device(solver, f, mode, launch=dict(kernel=kernel, block=block, grid=0, chunk=1))
         check_parity(g, o, f, np.ones(f.n, bool))
+    solver.set_launch(kernel="warp_queue", block=256, grid=0, chunk=1)
+
+
+def test_thread_block_sizes_give_identical_results(solver, W):
+    """Per-cell arithmetic does not depend on the block shape."""
+    f = fields.slice_field(fields.config1(W, n_side=128), 4000, stride=3)
+    outs = [run_device(solver, f, "fast", launch=dict(kernel=k, block=b, grid=0, chunk=1))[0]
+            for k, b in (("thread", 64), ("thread", 32), ("thread_queue", 32))]
+    for g in outs[1:]:
+        for key in ("Y_prod", "Y_prod2", "E_f_prod", "T_after", "status"):
+            np.testing.assert_array_equal(g[key], outs[0][key])
     solver.set_launch(kernel="warp_queue", block=256, grid=0, chunk=1)
 
 
@@ -139,3 +151,25 @@ def test_host_layout_drop_in(decks, oracle_mech, W):
     # ghost layer untouched
     assert np.all(m.fields["specie_production_chemistry2"][0][0, :, :] == -1.0)
     s.close()
+
+
+def test_mixed_precision_config2_error_per_species(solver, oracle_mech, W):
+    """Config 2 (T ~ U[800, 2600] K, p ~ U[0.5, 5] atm, dt = 1e-5 s): the FP32
+    LU with FP64 residual and one refinement sweep against the FP64 oracle,
+    reported per species.  The Newton matrix only steers the chord
+    iteration, so the converged step keeps the FP64 path's accuracy."""
+    f = fields.slice_field(fields.config2(W, n_side=128), 4096, stride=3)
+    o = oracle_run(oracle_mech, f)
+    rows = []
+    for mode in ("fast", "mixed"):
+        g, st = run_device(solver, f, mode)
+        assert st["cells_bad"] == 0
+        e = np.abs(dY(g, f) - dY(o, f)).max(axis=1)
+        et = np.max(np.abs(g["T_after"] - o["T_after"]) / f.T)
+        rows.append((mode, e, et))
+        assert e.max() <= TOL_Y, (mode, e)
+        assert et <= TOL_T, (mode, et)
+    names = fields.SPECIES
+    for mode, e, et in rows:
+        print(f"{mode:6s} max|dY_k - oracle|: " + " ".join(f"{n}={v:.1e}" for n, v in zip(names, e))
+              + f"  max|dT|/T={et:.1e}")
