@@ -25,7 +25,8 @@ static thread_local std::string g_create_error;
 
 struct nrg_chem {
   nrg::Mechanism mech;
-  DevMech dm;
+  DevMech dm;   // tables over all species
+  DevMech dmr;  // reaction lists over the reacting species (fast / mixed thread kernels)
   int device = 0;
   int num_sms = 148;
   cudaStream_t stream = nullptr;
@@ -167,6 +168,9 @@ std::string build_dev_mech(const nrg::Mechanism& m, DevMech* d) {
     formula_elements(m.species[k], e);
     for (int q = 0; q < 3; ++q) d->elem[q][k] = e[q];
   }
+  d->NI = N;
+  for (int k = 0; k < N; ++k) d->full_of[k] = k;
+  d->n_inert = 0;
   gear_coefficients(d->el, d->tq);
   d->eps = 1.0e-9;
   d->ewt = 1.0e-4;
@@ -178,6 +182,38 @@ std::string build_dev_mech(const nrg::Mechanism& m, DevMech* d) {
   d->bp = std::pow(DBL_EPSILON, -0.15);
   d->facmin = std::pow(DBL_EPSILON, 0.78);
   return "";
+}
+
+// Tables for the integrators that skip inert species: the reaction lists
+// renumbered over the species that react (mechanism order kept).
+void reduce_dev_mech(const DevMech& full, DevMech* d) {
+  *d = full;
+  bool reacts[nrg::kMaxSpecies] = {};
+  for (int r = 0; r < full.R; ++r) {
+    for (int i = 0; i < full.nl[r]; ++i)
+      if (full.left[r][i] >= 0) reacts[full.left[r][i]] = true;
+    for (int i = 0; i < full.nr[r]; ++i)
+      if (full.right[r][i] >= 0) reacts[full.right[r][i]] = true;
+  }
+  int int_of[nrg::kMaxSpecies];
+  d->NI = 0;
+  d->n_inert = 0;
+  for (int k = 0; k < full.N; ++k) {
+    if (reacts[k]) {
+      int_of[k] = d->NI;
+      d->full_of[d->NI++] = k;
+    } else {
+      int_of[k] = -1;
+      d->inert_of[d->n_inert++] = k;
+    }
+  }
+  for (int r = 0; r < full.R; ++r) {
+    for (int i = 0; i < 3; ++i) {
+      if (d->left[r][i] >= 0) d->left[r][i] = int_of[d->left[r][i]];
+      if (d->right[r][i] >= 0) d->right[r][i] = int_of[d->right[r][i]];
+    }
+    for (int u = 0; u < d->nupd[r]; ++u) d->upd_k[r][u] = int_of[d->upd_k[r][u]];
+  }
 }
 
 void free_staging(nrg_chem* h) {
@@ -227,7 +263,7 @@ cudaError_t enqueue_integrator(nrg_chem* h, const StepArgs& a, const LaunchCfg& 
   }
   LaunchCfg c = cfg;
   if (c.kernel == nrg::kKernelThreadQueue && c.grid <= 0) c.grid = h->num_sms;
-  return nrg::launch_chem(h->mech.n(), h->mech.r(), jac_of(h->mode), h->mode == NRG_MODE_MIXED, a, c,
+  return nrg::launch_chem(h->mech.n(), h->dmr.NI, h->mech.r(), jac_of(h->mode), h->mode == NRG_MODE_MIXED, a, c,
                           h->d_queue, h->d_counters, s);
 }
 
@@ -367,7 +403,8 @@ extern "C" int nrg_chem_create(const char* mechanism_path, const char* thermo_pa
     nrg_chem_destroy(h);
     return fail(nullptr, NRG_ERR_CUDA, msg);
   }
-  nrg::upload_mechanism(h->dm, h->stream);
+  reduce_dev_mech(h->dm, &h->dmr);
+  nrg::upload_mechanism(h->dm, h->dmr, h->stream);
   if ((ce = cudaStreamSynchronize(h->stream)) != cudaSuccess) {
     std::string msg = std::string("mechanism upload failed: ") + cudaGetErrorString(ce);
     nrg_chem_destroy(h);
@@ -1134,7 +1171,7 @@ extern "C" int nrg_chem_step_device_noalloc(nrg_chem* h, double time_step, long 
   fa.n_list_dev = n_list;
   LaunchCfg cfg = h->cfg;
   if (cfg.kernel == nrg::kKernelThreadQueue && cfg.grid <= 0) cfg.grid = h->num_sms;
-  const cudaError_t le = nrg::launch_chem(h->mech.n(), h->mech.r(), jac_of(h->mode), h->mode == NRG_MODE_MIXED,
+  const cudaError_t le = nrg::launch_chem(h->mech.n(), h->dmr.NI, h->mech.r(), jac_of(h->mode), h->mode == NRG_MODE_MIXED,
                                           fa, cfg, queue, counters, s);
   if (le != cudaSuccess) return cuda_fail(h, le, "no-allocation integrator launch");
   CK(h, cudaEventRecord(h->ev1, s));

@@ -72,7 +72,7 @@ struct SmemStore {
   __device__ __forceinline__ LUT& a(int j, int i) { return f[(j * N + i) * BS]; }  // A(i+1, j+1)
 };
 
-template <int N, int R, typename LUT, int BS>
+template <int N, int R, typename LUT, int BS, int NF = N>
 struct CellState;
 
 // Out-of-line hot routines of the thread-per-cell integrator.  They touch only
@@ -87,9 +87,13 @@ __device__ __noinline__ unsigned long long nl_dgefa(double* d, LUT* f, int* info
 template <int N, int R, typename LUT, int BS>
 __device__ __noinline__ void nl_rate_constants(double* d, LUT* f, double T);
 
-template <int N, int R, typename LUT, int BS>
+// N integrated species (vectors, Nordsieck rows, LU), NF mechanism species
+// (inputs, outputs, norms' sqrt(NF)); NF - N inert species are not integrated.
+template <int N, int R, typename LUT, int BS, int NF>
 struct CellState : SmemStore<N, R, LUT, BS> {
+  static constexpr int kNF = NF;
   double y[N], ywt[N], s1[N], s2[N], fac[N];
+  double yinr[NF > N ? NF - N : 1];  // y / YWT of the inert species (constant over the step)
   unsigned long long piv;  // ipvt, 4 bits per row
   double h, t, tout, rc, rmax, trend, eps;
   int nq, nwait, jtask, nstep, nfe, nje, nsolve, jstepl, nstepl, convrg, ier;
@@ -188,8 +192,8 @@ __device__ void rate_constants(CS& c, double Tin) {
   const double logt = nlog(NRG_FMIN(T, 6000.0));
 #pragma unroll 1
   for (int k = 0; k < N; ++k) {
-    c.z(k) = d_entropy(T, k, logt);
-    c.zd(k) = d_enthalpy(T, k);
+    c.z(k) = d_entropy(T, c_mech.full_of[k], logt);
+    c.zd(k) = d_enthalpy(T, c_mech.full_of[k]);
   }
   const double conc_ref = ddiv(ddiv(PATM, RG), T);
 #pragma unroll 1
@@ -591,7 +595,7 @@ __device__ void ddntl(CS& c) {
   c.nfe += 1;
 #pragma unroll
   for (int i = 0; i < N; ++i) c.s1[i] = ddiv(c.s2[i], NRG_FMAX(1.0, c.ywt[i]));
-  const double sum = ddiv(dnrm2<N>(c.s1), sqrt((double)N));
+  const double sum = ddiv(dnrm2<N>(c.s1), sqrt((double)CS::kNF));
   if (sum > ddiv(c.eps, fabs(c.h))) c.h = copysign(ddiv(c.eps, sum), c.h);
 #pragma unroll
   for (int i = 0; i < N; ++i) c.yh(1, i) = c.h * c.s2[i];
@@ -696,7 +700,7 @@ __device__ double ddcor(CS& c) {
     c.s1[i] = c.s1[i] + x[i];
     c.s2[i] = ddiv(x[i], NRG_FMAX(fabs(c.y[i]), c.ywt[i]));
   }
-  return ddiv(dnrm2<N>(c.s2), sqrt((double)N));
+  return ddiv(dnrm2<N>(c.s2), sqrt((double)CS::kNF));
 }
 
 // One DDSTP call (ddstp.f90:72-459); returns JSTATE (1 ok, 2 h vanished,
@@ -708,7 +712,7 @@ __device__ int ddstp(CS& c) {
   const int MXFAIL = 3, MXITER = 3, MXTRY = 50, NDJSTP = 10;
   const double uround = c_mech.uround;
   const double eps = c.eps;
-  const double sqn = sqrt((double)N);
+  const double sqn = sqrt((double)CS::kNF);
   int ntry = 0, nfail = 0, iter = 0;
   bool evaljc;
   double told = c.t, ctest = 0.0, d = 0.0, d1 = 0.0, etest, rh;
@@ -885,32 +889,50 @@ L420:
 // Returns false when the cell is passed through (outputs already written).
 template <int N, int R, class CS>
 __device__ bool cell_begin(CS& c, const StepArgs& a, long cid) {
+  constexpr int NF = CS::kNF;
   const double Tc = a.T[cid];
   const bool active = (Tc >= 305.0) && (a.bc == nullptr || a.bc[cid] == 0);
   if (!active) {
 #pragma unroll
-    for (int k = 0; k < N; ++k) a.Y_prod[k * a.ld + cid] = 0.0;
+    for (int k = 0; k < NF; ++k) a.Y_prod[k * a.ld + cid] = 0.0;
     a.E_f_prod[cid] = 0.0;
     if (a.status) a.status[cid] = kCellSkipped;
     return false;
   }
   const double rho = a.rho[cid];
-  double yk[N];
+  double yk[NF];
 #pragma unroll
-  for (int k = 0; k < N; ++k) yk[k] = a.Y[k * a.ld + cid];
+  for (int k = 0; k < NF; ++k) yk[k] = a.Y[k * a.ld + cid];
 #pragma unroll 1
   for (int r = 0; r < R; ++r) {
     double s = 0.0;
 #pragma unroll
-    for (int k = 0; k < N; ++k) s = s + yk[k] * rho / c_mech.W[k] * c_mech.eff_t[k][r];
+    for (int k = 0; k < NF; ++k) s = s + yk[k] * rho / c_mech.W[k] * c_mech.eff_t[k][r];
     c.kr(r) = s;  // third-body sum, consumed by rate_constants
   }
   nl_rate_constants<N, R, typename CS::lut_t, CS::kBS>(c.d, c.f, Tc);
+  if (NF == N) {
 #pragma unroll
-  for (int k = 0; k < N; ++k) {
-    const double ci = yk[k] * rho / c_mech.W[k];
-    c.yh(0, k) = ci;
-    c.y[k] = ci;
+    for (int k = 0; k < N; ++k) {
+      const double ci = yk[k] * rho / c_mech.W[k];
+      c.yh(0, k) = ci;
+      c.y[k] = ci;
+    }
+  } else {
+    double ci[NF];
+#pragma unroll
+    for (int k = 0; k < NF; ++k) ci[k] = yk[k] * rho / c_mech.W[k];
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      const double v = ci[c_mech.full_of[i]];
+      c.yh(0, i) = v;
+      c.y[i] = v;
+    }
+#pragma unroll
+    for (int j = 0; j < (NF > N ? NF - N : 1); ++j) {
+      const double v = ci[c_mech.inert_of[j]];
+      c.yinr[j] = ddiv(v, NRG_FMAX(c_mech.ewt, fabs(v)));
+    }
   }
   c.tout = a.dt_cells ? a.dt_cells[cid] : a.dt;
   c.t = 0.0;
@@ -945,7 +967,20 @@ __device__ int cell_advance(CS& c, int mxstep) {
   for (int i = 0; i < N; ++i) c.ywt[i] = NRG_FMAX(c_mech.ewt, fabs(c.y[i]));
 #pragma unroll
   for (int i = 0; i < N; ++i) c.s2[i] = ddiv(c.y[i], c.ywt[i]);
-  const double sum = NRG_FMAX(1.0, ddiv(dnrm2<N>(c.s2), sqrt((double)N)));
+  double sum;
+  if (CS::kNF == N) {
+    sum = NRG_FMAX(1.0, ddiv(dnrm2<N>(c.s2), sqrt((double)N)));
+  } else {
+    // the accuracy test runs over every species in mechanism order, the
+    // inert ones included (their y / YWT is fixed)
+    constexpr int NF = CS::kNF;
+    double t[NF];
+#pragma unroll
+    for (int i = 0; i < N; ++i) t[c_mech.full_of[i]] = c.s2[i];
+#pragma unroll
+    for (int j = 0; j < (NF > N ? NF - N : 1); ++j) t[c_mech.inert_of[j]] = c.yinr[j];
+    sum = NRG_FMAX(1.0, ddiv(dnrm2_nl<NF>(t), sqrt((double)NF)));
+  }
   if (c.eps < sum * c_mech.uround) {
     c.eps = sum * c_mech.uround * (1.0 + 10.0 * c_mech.uround);
 #pragma unroll
@@ -1037,19 +1072,33 @@ __device__ __forceinline__ double temperature_after(double T0, const double (&Y0
   return temperature_after_nl<N>(T0, a, b, dE);
 }
 
-// Outputs of a finished cell (chemical_kinetics_solver.f90:318-340).
+// Outputs of a finished cell (chemical_kinetics_solver.f90:318-340); inert
+// species keep their concentration, so their sources are exactly zero.
 template <int N, class CS>
 __device__ void cell_finish(const CS& c, const StepArgs& a, long cid, int st) {
+  constexpr int NF = CS::kNF;
   const double dt = c.tout;
   const double rho = a.rho[cid];
   double E = 0.0;
   bool finite = true;
-  double Y0[N], dYm[N];
+  double Y0[NF], dYm[NF], dcs[NF];
 #pragma unroll
-  for (int k = 0; k < N; ++k) {
-    Y0[k] = a.Y[k * a.ld + cid];
-    const double ci = Y0[k] * rho / c_mech.W[k];
-    const double dc = c.y[k] - ci;
+  for (int k = 0; k < NF; ++k) Y0[k] = a.Y[k * a.ld + cid];
+  if (NF == N) {
+#pragma unroll
+    for (int k = 0; k < NF; ++k) dcs[k] = c.y[k] - Y0[k] * rho / c_mech.W[k];
+  } else {
+#pragma unroll
+    for (int k = 0; k < NF; ++k) dcs[k] = 0.0;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      const int k = c_mech.full_of[i];
+      dcs[k] = c.y[i] - Y0[k] * rho / c_mech.W[k];
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < NF; ++k) {
+    const double dc = dcs[k];
     finite = finite && isfinite(dc);
     const double yp = dc * c_mech.W[k] / dt;
     a.Y_prod[k * a.ld + cid] = yp;
@@ -1058,7 +1107,7 @@ __device__ void cell_finish(const CS& c, const StepArgs& a, long cid, int st) {
     dYm[k] = yp * dt / rho;
   }
   a.E_f_prod[cid] = E;
-  if (a.T_after) a.T_after[cid] = temperature_after<N>(a.T[cid], Y0, dYm, E * dt / rho);
+  if (a.T_after) a.T_after[cid] = temperature_after<NF>(a.T[cid], Y0, dYm, E * dt / rho);
   if (a.status) a.status[cid] = finite ? (uint8_t)st : (uint8_t)kCellNonfinite;
 }
 

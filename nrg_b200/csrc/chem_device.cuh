@@ -48,6 +48,16 @@ struct DevMech {
   int sp_list[kMaxSpecUpd][kMaxSpecies];
   // element composition for conservation checks (H, O, N) in atoms/molecule
   double elem[3][kMaxSpecies];
+  // Integrated species.  Species that appear in no reaction (third bodies
+  // only, N2 in the H2/air mechanisms) have a zero right-hand side; the
+  // thread-per-cell integrators of the analytic-Jacobian and mixed modes
+  // integrate only the NI others.  In the copy of the tables those kernels
+  // use, left/right/upd_k hold integrated indices; every per-species array
+  // above stays indexed by mechanism species.
+  int NI;
+  int full_of[kMaxSpecies];   // integrated index -> mechanism species
+  int n_inert;
+  int inert_of[kMaxSpecies];  // the inert species (mechanism index)
 };
 
 // Per-cell status byte written by the integrator.

@@ -11,8 +11,8 @@ void upload_mechanism_ref(const DevMech& m, cudaStream_t s);
 void upload_mechanism_fast(const DevMech& m, cudaStream_t s);
 void upload_mechanism_mixed(const DevMech& m, cudaStream_t s);
 cudaError_t launch_chem_ref(const StepArgs&, const LaunchCfg&, int*, unsigned long long*, cudaStream_t);
-cudaError_t launch_chem_fast(const StepArgs&, const LaunchCfg&, int*, unsigned long long*, cudaStream_t);
-cudaError_t launch_chem_mixed(const StepArgs&, const LaunchCfg&, int*, unsigned long long*, cudaStream_t);
+cudaError_t launch_chem_fast(const StepArgs&, const LaunchCfg&, int*, unsigned long long*, cudaStream_t, int);
+cudaError_t launch_chem_mixed(const StepArgs&, const LaunchCfg&, int*, unsigned long long*, cudaStream_t, int);
 
 __global__ void k_fp64_peak(double* out, int iters) {
   double a0 = threadIdx.x * 1e-9, a1 = a0 + 1.0, a2 = a0 + 2.0, a3 = a0 + 3.0;
@@ -30,20 +30,22 @@ __global__ void k_fp64_peak(double* out, int iters) {
 }
 
 // ------------------------------------------------------------ launchers
-void upload_mechanism(const DevMech& m, cudaStream_t s) {
-  // every translation unit holding kernels keeps its own copy of the tables
-  cudaMemcpyToSymbolAsync(c_mech, &m, sizeof(DevMech), 0, cudaMemcpyHostToDevice, s);
-  upload_mechanism_ref(m, s);
-  upload_mechanism_fast(m, s);
-  upload_mechanism_mixed(m, s);
+void upload_mechanism(const DevMech& full, const DevMech& reduced, cudaStream_t s) {
+  // every translation unit holding kernels keeps its own copy of the tables;
+  // the analytic-Jacobian and mixed variants integrate the reacting species only
+  cudaMemcpyToSymbolAsync(c_mech, &full, sizeof(DevMech), 0, cudaMemcpyHostToDevice, s);
+  upload_mechanism_ref(full, s);
+  upload_mechanism_fast(reduced, s);
+  upload_mechanism_mixed(reduced, s);
 }
 
-cudaError_t launch_chem(int n_species, int n_reactions, int jac, bool mixed, const StepArgs& a,
+cudaError_t launch_chem(int n_species, int n_int, int n_reactions, int jac, bool mixed, const StepArgs& a,
                         const LaunchCfg& cfg, int* queue, unsigned long long* counters,
                         cudaStream_t s) {
   if (n_species != 9 || n_reactions != 24) return cudaErrorNotSupported;
-  if (mixed) return launch_chem_mixed(a, cfg, queue, counters, s);
-  return jac == kJacFD ? launch_chem_ref(a, cfg, queue, counters, s) : launch_chem_fast(a, cfg, queue, counters, s);
+  if (mixed) return launch_chem_mixed(a, cfg, queue, counters, s, n_int);
+  return jac == kJacFD ? launch_chem_ref(a, cfg, queue, counters, s)
+                       : launch_chem_fast(a, cfg, queue, counters, s, n_int);
 }
 
 int smem_bytes_per_cell(int n_species, int n_reactions, bool mixed) {

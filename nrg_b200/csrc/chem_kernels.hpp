@@ -41,11 +41,13 @@ struct LaunchCfg {
   int chunk = 1;                  // cells reserved per queue fetch (per lane or per warp)
 };
 
-void upload_mechanism(const DevMech& m, cudaStream_t s);
+// full: tables over all species; reduced: the same with reaction lists
+// numbered over the reacting species (thread-per-cell fast / mixed variants)
+void upload_mechanism(const DevMech& full, const DevMech& reduced, cudaStream_t s);
 
 // jac: 0 finite-difference (reference DDPST), 1 analytic.  mixed: float LU.
 // queue must point at a zeroed device int for the work-queue kernels.
-cudaError_t launch_chem(int n_species, int n_reactions, int jac, bool mixed, const StepArgs& a,
+cudaError_t launch_chem(int n_species, int n_int, int n_reactions, int jac, bool mixed, const StepArgs& a,
                         const LaunchCfg& cfg, int* queue, unsigned long long* counters,
                         cudaStream_t s);
 
