@@ -45,6 +45,9 @@ def parse():
     p.add_argument("--n-side", type=int, default=2048)
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--kernel", choices=["thread", "thread_queue", "warp_queue"], default=None,
+                   help="fix the integrator launch instead of autotuning it (with --block)")
+    p.add_argument("--block", type=int, default=32)
     return p.parse_args()
 
 
@@ -263,12 +266,15 @@ def main():
 
     # launch shape of the FP64 integrator: autotuned on a contiguous block of
     # rows (neighbouring cells take similar integration paths)
-    nsamp = min(n, 262144)
-    samp = F.slice_field(field, nsamp, stride=1, offset=(n - nsamp) // 2)
-    sT, sr, sY = (torch.tensor(a, device=dev) for a in (samp.T, samp.rho, samp.Y))
-    solver.autotune(samp.dt, sT, sr, sY, torch.zeros_like(sY), torch.zeros_like(sY), torch.zeros_like(sT))
+    if args.kernel:
+        solver.set_launch(kernel=args.kernel, block=args.block)
+    else:
+        nsamp = min(n, 262144)
+        samp = F.slice_field(field, nsamp, stride=1, offset=(n - nsamp) // 2)
+        sT, sr, sY = (torch.tensor(a, device=dev) for a in (samp.T, samp.rho, samp.Y))
+        solver.autotune(samp.dt, sT, sr, sY, torch.zeros_like(sY), torch.zeros_like(sY), torch.zeros_like(sT))
+        del sT, sr, sY
     launch = solver.get_launch()
-    del sT, sr, sY
 
     mode = args.mode
     train_info = None

@@ -254,23 +254,32 @@ template <int N, int R, class CS>
 __device__ __forceinline__ void rhs(CS& c) {
 #pragma unroll
   for (int k = 0; k < N; ++k) c.zd(k) = 0.0;
+// Fixed-trip inner loops (3 reactant and 3 product slots, unused and M
+// slots hold -1 and multiply by 1.0, which leaves every product unchanged; 6
+// update slots under a predicate): no data-dependent branches per reaction.
 #pragma unroll 1
   for (int r = 0; r < R; ++r) {
     double f = c.kf(r);
-    for (int i = 0; i < c_mech.nl[r]; ++i) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
       const int sp = c_mech.left[r][i];
-      if (sp >= 0) f = f * c.z(sp);
+      f = f * (sp >= 0 ? c.z(sp) : 1.0);
     }
     double b = c.kr(r);
-    for (int i = 0; i < c_mech.nr[r]; ++i) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
       const int sp = c_mech.right[r][i];
-      if (sp >= 0) b = b * c.z(sp);
+      b = b * (sp >= 0 ? c.z(sp) : 1.0);
     }
     const double q = f - b;
-    for (int u = 0; u < c_mech.nupd[r]; ++u) {
-      const int k = c_mech.upd_k[r][u];
-      if (c_mech.upd_prod[r][u]) c.zd(k) += q;
-      else c.zd(k) -= q;
+    const int nu = c_mech.nupd[r];
+#pragma unroll
+    for (int u = 0; u < 6; ++u) {
+      if (u < nu) {
+        const int k = c_mech.upd_k[r][u];
+        const double v = c.zd(k);
+        c.zd(k) = c_mech.upd_prod[r][u] ? v + q : v - q;
+      }
     }
   }
 }
@@ -289,31 +298,37 @@ __device__ __forceinline__ void rhs_at(CS& c, const double (&v)[N], double (&out
 // at z, written straight into the LU storage.
 template <int N, int R, class CS>
 __device__ void analytic_iteration_matrix(CS& c, double factor) {
+  using LUT_T = typename CS::lut_t;
 #pragma unroll
   for (int j = 0; j < N; ++j)
 #pragma unroll
     for (int i = 0; i < N; ++i) c.a(j, i) = 0;
 #pragma unroll 1
   for (int r = 0; r < R; ++r) {
-    const int nl = c_mech.nl[r], nr = c_mech.nr[r], nu = c_mech.nupd[r];
+    const int nu = c_mech.nupd[r];
+#pragma unroll
     for (int side = 0; side < 2; ++side) {
-      const int cnt = side ? nr : nl;
       const double k = side ? c.kr(r) : c.kf(r);
       const double sgn = side ? -factor : factor;  // d(f - b)
-      for (int p = 0; p < cnt; ++p) {
+#pragma unroll
+      for (int p = 0; p < 3; ++p) {
         const int sp = side ? c_mech.right[r][p] : c_mech.left[r][p];
         if (sp < 0) continue;
         double d = k;
-        for (int q = 0; q < cnt; ++q) {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
           if (q == p) continue;
           const int sq = side ? c_mech.right[r][q] : c_mech.left[r][q];
-          if (sq >= 0) d = d * c.z(sq);
+          d = d * (sq >= 0 ? c.z(sq) : 1.0);
         }
         d = d * sgn;
-        for (int u = 0; u < nu; ++u) {
-          const int k2 = c_mech.upd_k[r][u];
-          if (c_mech.upd_prod[r][u]) c.a(sp, k2) += d;
-          else c.a(sp, k2) -= d;
+#pragma unroll
+        for (int u = 0; u < 6; ++u) {
+          if (u < nu) {
+            const int k2 = c_mech.upd_k[r][u];
+            const LUT_T v = c.a(sp, k2);
+            c.a(sp, k2) = c_mech.upd_prod[r][u] ? v + d : v - d;
+          }
         }
       }
     }
