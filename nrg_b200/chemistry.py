@@ -98,6 +98,7 @@ SIGNATURES = {
     "nrg_surrogate_grad": (_I, [_VP, _L, _VP, _VP, _VP, ctypes.POINTER(_D)]),
     "nrg_surrogate_train": (_I, [_VP, _L, _VP, _VP, _I, _I, ctypes.c_float, ctypes.c_ulonglong, _VP]),
     "nrg_surrogate_set_gate": (_I, [_VP, _D, _D, _D, _D]),
+    "nrg_chem_set_specialised": (_I, [_VP, _I]),
     "nrg_surrogate_set_inference": (_I, [_VP, _I]),
     "nrg_surrogate_infer": (_I, [_VP, _L, _L, _D, _VP, _VP, _VP, _VP, _VP]),
     "nrg_surrogate_enable": (_I, [_VP, _I]),
@@ -260,6 +261,11 @@ class ChemicalKineticsSolver:
 
     def set_graph(self, enable: bool) -> None:
         _check(lib().nrg_chem_set_graph(self._h, int(enable)), self._h)
+
+    def set_specialised(self, enable: bool) -> None:
+        """Generated mechanism-specialised RHS / iteration matrix (default when
+        the mechanism matches) or the table-driven loops."""
+        _check(lib().nrg_chem_set_specialised(self._h, int(enable)), self._h)
 
     def set_timing(self, enable: bool) -> None:
         _check(lib().nrg_chem_set_timing(self._h, int(enable)), self._h)

@@ -27,6 +27,7 @@ struct nrg_chem {
   nrg::Mechanism mech;
   DevMech dm;   // tables over all species
   DevMech dmr;  // reaction lists over the reacting species (fast / mixed thread kernels)
+  bool spec = false;  // use the generated mechanism-specialised RHS / iteration matrix
   int device = 0;
   int num_sms = 148;
   cudaStream_t stream = nullptr;
@@ -263,7 +264,7 @@ cudaError_t enqueue_integrator(nrg_chem* h, const StepArgs& a, const LaunchCfg& 
   }
   LaunchCfg c = cfg;
   if (c.kernel == nrg::kKernelThreadQueue && c.grid <= 0) c.grid = h->num_sms;
-  return nrg::launch_chem(h->mech.n(), h->dmr.NI, h->mech.r(), jac_of(h->mode), h->mode == NRG_MODE_MIXED, a, c,
+  return nrg::launch_chem(h->mech.n(), h->dmr.NI, h->spec, h->mech.r(), jac_of(h->mode), h->mode == NRG_MODE_MIXED, a, c,
                           h->d_queue, h->d_counters, s);
 }
 
@@ -404,6 +405,7 @@ extern "C" int nrg_chem_create(const char* mechanism_path, const char* thermo_pa
     return fail(nullptr, NRG_ERR_CUDA, msg);
   }
   reduce_dev_mech(h->dm, &h->dmr);
+  h->spec = nrg::matches_specialised(h->dmr);
   nrg::upload_mechanism(h->dm, h->dmr, h->stream);
   if ((ce = cudaStreamSynchronize(h->stream)) != cudaSuccess) {
     std::string msg = std::string("mechanism upload failed: ") + cudaGetErrorString(ce);
@@ -443,6 +445,14 @@ extern "C" int nrg_chem_set_mode(nrg_chem* h, int mode) {
   if (!h) return NRG_ERR_ARG;
   if (mode < NRG_MODE_REFERENCE || mode > NRG_MODE_SURROGATE) return fail(h, NRG_ERR_ARG, "unknown mode");
   h->mode = mode;
+  return NRG_OK;
+}
+
+extern "C" int nrg_chem_set_specialised(nrg_chem* h, int enable) {
+  if (!h) return NRG_ERR_ARG;
+  if (enable && !nrg::matches_specialised(h->dmr))
+    return fail(h, NRG_ERR_UNSUPPORTED, "the mechanism does not match the generated specialised code");
+  h->spec = enable != 0;
   return NRG_OK;
 }
 
@@ -1175,7 +1185,7 @@ extern "C" int nrg_chem_step_device_noalloc(nrg_chem* h, double time_step, long 
   fa.n_list_dev = n_list;
   LaunchCfg cfg = h->cfg;
   if (cfg.kernel == nrg::kKernelThreadQueue && cfg.grid <= 0) cfg.grid = h->num_sms;
-  const cudaError_t le = nrg::launch_chem(h->mech.n(), h->dmr.NI, h->mech.r(), jac_of(h->mode), h->mode == NRG_MODE_MIXED,
+  const cudaError_t le = nrg::launch_chem(h->mech.n(), h->dmr.NI, h->spec, h->mech.r(), jac_of(h->mode), h->mode == NRG_MODE_MIXED,
                                           fa, cfg, queue, counters, s);
   if (le != cudaSuccess) return cuda_fail(h, le, "no-allocation integrator launch");
   CK(h, cudaEventRecord(h->ev1, s));

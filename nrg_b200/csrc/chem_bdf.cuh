@@ -28,6 +28,7 @@
 
 #include "chem_device.cuh"
 #include "chem_kernels.hpp"
+#include "gen_keromnes.cuh"
 
 namespace nrg {
 
@@ -72,15 +73,15 @@ struct SmemStore {
   __device__ __forceinline__ LUT& a(int j, int i) { return f[(j * N + i) * BS]; }  // A(i+1, j+1)
 };
 
-template <int N, int R, typename LUT, int BS, int NF = N>
+template <int N, int R, typename LUT, int BS, int NF = N, bool SPEC = false>
 struct CellState;
 
 // Out-of-line hot routines of the thread-per-cell integrator.  They touch only
 // the cell's shared-memory arrays (passed as the two base pointers), so the
 // register-resident vectors are never forced to local memory by the call.
-template <int N, int R, typename LUT, int BS>
+template <int N, int R, typename LUT, int BS, bool SPEC>
 __device__ __noinline__ void nl_rhs(double* d, LUT* f);
-template <int N, int R, typename LUT, int BS>
+template <int N, int R, typename LUT, int BS, bool SPEC>
 __device__ __noinline__ void nl_analytic_matrix(double* d, LUT* f, double factor);
 template <int N, int R, typename LUT, int BS>
 __device__ __noinline__ unsigned long long nl_dgefa(double* d, LUT* f, int* info);
@@ -89,9 +90,12 @@ __device__ __noinline__ void nl_rate_constants(double* d, LUT* f, double T);
 
 // N integrated species (vectors, Nordsieck rows, LU), NF mechanism species
 // (inputs, outputs, norms' sqrt(NF)); NF - N inert species are not integrated.
-template <int N, int R, typename LUT, int BS, int NF>
+// SPEC: right-hand side and iteration matrix from the generated
+// mechanism-specialised code (gen_keromnes.cuh) instead of the tables.
+template <int N, int R, typename LUT, int BS, int NF, bool SPEC>
 struct CellState : SmemStore<N, R, LUT, BS> {
   static constexpr int kNF = NF;
+  static constexpr bool kSpec = SPEC;
   double y[N], ywt[N], s1[N], s2[N], fac[N];
   double yinr[NF > N ? NF - N : 1];  // y / YWT of the inert species (constant over the step)
   unsigned long long piv;  // ipvt, 4 bits per row
@@ -257,28 +261,31 @@ __device__ __forceinline__ void rhs(CS& c) {
 // Fixed-trip inner loops (3 reactant and 3 product slots, unused and M
 // slots hold -1 and multiply by 1.0, which leaves every product unchanged; 6
 // update slots under a predicate): no data-dependent branches per reaction.
+// Explicitly rounded operations (never fused into FMAs) make the result
+// independent of how the compiler schedules this loop, so the generated
+// straight-line version (gen_keromnes.cuh) gives the same bits.
 #pragma unroll 1
   for (int r = 0; r < R; ++r) {
     double f = c.kf(r);
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
       const int sp = c_mech.left[r][i];
-      f = f * (sp >= 0 ? c.z(sp) : 1.0);
+      f = __dmul_rn(f, sp >= 0 ? c.z(sp) : 1.0);
     }
     double b = c.kr(r);
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
       const int sp = c_mech.right[r][i];
-      b = b * (sp >= 0 ? c.z(sp) : 1.0);
+      b = __dmul_rn(b, sp >= 0 ? c.z(sp) : 1.0);
     }
-    const double q = f - b;
+    const double q = __dsub_rn(f, b);
     const int nu = c_mech.nupd[r];
 #pragma unroll
     for (int u = 0; u < 6; ++u) {
       if (u < nu) {
         const int k = c_mech.upd_k[r][u];
         const double v = c.zd(k);
-        c.zd(k) = c_mech.upd_prod[r][u] ? v + q : v - q;
+        c.zd(k) = c_mech.upd_prod[r][u] ? __dadd_rn(v, q) : __dsub_rn(v, q);
       }
     }
   }
@@ -289,7 +296,7 @@ template <int N, int R, class CS>
 __device__ __forceinline__ void rhs_at(CS& c, const double (&v)[N], double (&out)[N]) {
 #pragma unroll
   for (int k = 0; k < N; ++k) c.z(k) = v[k];
-  nl_rhs<N, R, typename CS::lut_t, CS::kBS>(c.d, c.f);
+  nl_rhs<N, R, typename CS::lut_t, CS::kBS, CS::kSpec>(c.d, c.f);
 #pragma unroll
   for (int k = 0; k < N; ++k) out[k] = c.zd(k);
 }
@@ -319,15 +326,15 @@ __device__ void analytic_iteration_matrix(CS& c, double factor) {
         for (int q = 0; q < 3; ++q) {
           if (q == p) continue;
           const int sq = side ? c_mech.right[r][q] : c_mech.left[r][q];
-          d = d * (sq >= 0 ? c.z(sq) : 1.0);
+          d = __dmul_rn(d, sq >= 0 ? c.z(sq) : 1.0);
         }
-        d = d * sgn;
+        d = __dmul_rn(d, sgn);
 #pragma unroll
         for (int u = 0; u < 6; ++u) {
           if (u < nu) {
             const int k2 = c_mech.upd_k[r][u];
-            const LUT_T v = c.a(sp, k2);
-            c.a(sp, k2) = c_mech.upd_prod[r][u] ? v + d : v - d;
+            const double v = (double)c.a(sp, k2);
+            c.a(sp, k2) = (LUT_T)(c_mech.upd_prod[r][u] ? __dadd_rn(v, d) : __dsub_rn(v, d));
           }
         }
       }
@@ -504,20 +511,30 @@ __device__ __forceinline__ void dgesl(CS& c, double (&b)[N]) {
   }
 }
 
-template <int N, int R, typename LUT, int BS>
+template <int N, int R, typename LUT, int BS, bool SPEC>
 __device__ __noinline__ void nl_rhs(double* d, LUT* f) {
   SmemStore<N, R, LUT, BS> s;
   s.d = d;
   s.f = f;
-  rhs<N, R>(s);
+  if constexpr (SPEC) {
+    static_assert(N == gen::kSpecN && R == gen::kSpecR, "specialised code is for another mechanism size");
+    gen::spec_rhs(s);
+  } else {
+    rhs<N, R>(s);
+  }
 }
 
-template <int N, int R, typename LUT, int BS>
+template <int N, int R, typename LUT, int BS, bool SPEC>
 __device__ __noinline__ void nl_analytic_matrix(double* d, LUT* f, double factor) {
   SmemStore<N, R, LUT, BS> s;
   s.d = d;
   s.f = f;
-  analytic_iteration_matrix<N, R>(s, factor);
+  if constexpr (SPEC) {
+    static_assert(N == gen::kSpecN && R == gen::kSpecR, "specialised code is for another mechanism size");
+    gen::spec_matrix<SmemStore<N, R, LUT, BS>, LUT>(s, factor);
+  } else {
+    analytic_iteration_matrix<N, R>(s, factor);
+  }
 }
 
 template <int N, int R, typename LUT, int BS>
@@ -649,7 +666,7 @@ __device__ void ddpst(CS& c) {
       dy = (c.nq == 1) ? copysign(dy, sel(c.s2, j)) : copysign(dy, c.yh(2, j));
       dy = (yj + dy) - yj;
       c.z(j) = yj + dy;
-      nl_rhs<N, R, typename CS::lut_t, CS::kBS>(c.d, c.f);
+      nl_rhs<N, R, typename CS::lut_t, CS::kBS, CS::kSpec>(c.d, c.f);
       c.z(j) = yj;
       const double factor = -ddiv(el1h, dy);
       double diff = -1.0, s2m = 0.0, s1m = 0.0;
@@ -674,7 +691,7 @@ __device__ void ddpst(CS& c) {
   } else {
 #pragma unroll
     for (int k = 0; k < N; ++k) c.z(k) = c.y[k];
-    nl_analytic_matrix<N, R, typename CS::lut_t, CS::kBS>(c.d, c.f, -el1h);
+    nl_analytic_matrix<N, R, typename CS::lut_t, CS::kBS, CS::kSpec>(c.d, c.f, -el1h);
   }
   int info = 0;
   c.piv = nl_dgefa<N, R, typename CS::lut_t, CS::kBS>(c.d, c.f, &info);

@@ -8,10 +8,13 @@ void upload_mechanism_fast(const DevMech& m, cudaStream_t s) {
 }
 
 cudaError_t launch_chem_fast(const StepArgs& a, const LaunchCfg& cfg, int* queue,
-                              unsigned long long* counters, cudaStream_t s, int n_int) {
-  // the mechanism's inert species (third bodies only) are not integrated
-  if (n_int == 8) return launch_variant<9, 8, 24, kJacAnalytic, double>(a, cfg, queue, counters, s);
-  if (n_int == 9) return launch_variant<9, 9, 24, kJacAnalytic, double>(a, cfg, queue, counters, s);
+                              unsigned long long* counters, cudaStream_t s, int n_int, bool spec) {
+  // the mechanism's inert species (third bodies only) are not integrated;
+  // spec: the parsed mechanism matches the generated specialised code
+  if (n_int == gen::kSpecN && spec)
+    return launch_variant<9, gen::kSpecN, 24, kJacAnalytic, double, true>(a, cfg, queue, counters, s);
+  if (n_int == 8) return launch_variant<9, 8, 24, kJacAnalytic, double, false>(a, cfg, queue, counters, s);
+  if (n_int == 9) return launch_variant<9, 9, 24, kJacAnalytic, double, false>(a, cfg, queue, counters, s);
   return cudaErrorNotSupported;
 }
 

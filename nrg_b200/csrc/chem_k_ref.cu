@@ -9,7 +9,7 @@ void upload_mechanism_ref(const DevMech& m, cudaStream_t s) {
 
 cudaError_t launch_chem_ref(const StepArgs& a, const LaunchCfg& cfg, int* queue,
                               unsigned long long* counters, cudaStream_t s) {
-  return launch_variant<9, 9, 24, kJacFD, double>(a, cfg, queue, counters, s);
+  return launch_variant<9, 9, 24, kJacFD, double, false>(a, cfg, queue, counters, s);
 }
 
 }  // namespace nrg

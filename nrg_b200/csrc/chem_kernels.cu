@@ -11,8 +11,8 @@ void upload_mechanism_ref(const DevMech& m, cudaStream_t s);
 void upload_mechanism_fast(const DevMech& m, cudaStream_t s);
 void upload_mechanism_mixed(const DevMech& m, cudaStream_t s);
 cudaError_t launch_chem_ref(const StepArgs&, const LaunchCfg&, int*, unsigned long long*, cudaStream_t);
-cudaError_t launch_chem_fast(const StepArgs&, const LaunchCfg&, int*, unsigned long long*, cudaStream_t, int);
-cudaError_t launch_chem_mixed(const StepArgs&, const LaunchCfg&, int*, unsigned long long*, cudaStream_t, int);
+cudaError_t launch_chem_fast(const StepArgs&, const LaunchCfg&, int*, unsigned long long*, cudaStream_t, int, bool);
+cudaError_t launch_chem_mixed(const StepArgs&, const LaunchCfg&, int*, unsigned long long*, cudaStream_t, int, bool);
 
 __global__ void k_fp64_peak(double* out, int iters) {
   double a0 = threadIdx.x * 1e-9, a1 = a0 + 1.0, a2 = a0 + 2.0, a3 = a0 + 3.0;
@@ -39,13 +39,26 @@ void upload_mechanism(const DevMech& full, const DevMech& reduced, cudaStream_t 
   upload_mechanism_mixed(reduced, s);
 }
 
-cudaError_t launch_chem(int n_species, int n_int, int n_reactions, int jac, bool mixed, const StepArgs& a,
-                        const LaunchCfg& cfg, int* queue, unsigned long long* counters,
+cudaError_t launch_chem(int n_species, int n_int, bool spec, int n_reactions, int jac, bool mixed,
+                        const StepArgs& a, const LaunchCfg& cfg, int* queue, unsigned long long* counters,
                         cudaStream_t s) {
   if (n_species != 9 || n_reactions != 24) return cudaErrorNotSupported;
-  if (mixed) return launch_chem_mixed(a, cfg, queue, counters, s, n_int);
+  if (mixed) return launch_chem_mixed(a, cfg, queue, counters, s, n_int, spec);
   return jac == kJacFD ? launch_chem_ref(a, cfg, queue, counters, s)
-                       : launch_chem_fast(a, cfg, queue, counters, s, n_int);
+                       : launch_chem_fast(a, cfg, queue, counters, s, n_int, spec);
+}
+
+bool matches_specialised(const DevMech& reduced) {
+  if (reduced.NI != gen::kSpecN || reduced.R != gen::kSpecR) return false;
+  for (int r = 0; r < reduced.R; ++r) {
+    if (reduced.nupd[r] != gen::kSpecNupd[r]) return false;
+    for (int i = 0; i < 3; ++i)
+      if (reduced.left[r][i] != gen::kSpecLeft[r][i] || reduced.right[r][i] != gen::kSpecRight[r][i]) return false;
+    for (int u = 0; u < reduced.nupd[r]; ++u)
+      if (reduced.upd_k[r][u] != gen::kSpecUpdK[r][u] || reduced.upd_prod[r][u] != gen::kSpecUpdProd[r][u])
+        return false;
+  }
+  return true;
 }
 
 int smem_bytes_per_cell(int n_species, int n_reactions, bool mixed) {

@@ -39,14 +39,14 @@ __device__ __forceinline__ void block_flush_counters(unsigned long long* counter
   if (threadIdx.x < kCntSlots && s_cnt[threadIdx.x]) atomicAdd(&counters[threadIdx.x], s_cnt[threadIdx.x]);
 }
 
-template <int N, int R, int JAC, typename LUT, int BS, int NF>
+template <int N, int R, int JAC, typename LUT, int BS, int NF, bool SPEC>
 __global__ void __launch_bounds__(BS, 1) k_chem_plain(StepArgs a, unsigned long long* counters) {
   extern __shared__ __align__(16) char smem[];
   const long li = (long)blockIdx.x * BS + threadIdx.x;
   const long nl = a.cell_list ? (long)(a.n_list_dev ? *a.n_list_dev : a.n_list) : a.n;
   const long cid = (a.cell_list && li < nl) ? (long)a.cell_list[li] : li;
   unsigned long long v[kCntSlots] = {0, 0, 0, 0, 0, 0};
-  CellState<N, R, LUT, BS, NF> c;
+  CellState<N, R, LUT, BS, NF, SPEC> c;
   c.bind(smem, threadIdx.x);
   if (li < nl) {
     if (cell_begin<N, R>(c, a, cid)) {
@@ -65,12 +65,12 @@ __global__ void __launch_bounds__(BS, 1) k_chem_plain(StepArgs a, unsigned long 
   if (counters) block_flush_counters(counters, v);
 }
 
-template <int N, int R, int JAC, typename LUT, int BS, int NF>
+template <int N, int R, int JAC, typename LUT, int BS, int NF, bool SPEC>
 __global__ void __launch_bounds__(BS, 1) k_chem_queue(StepArgs a, int* queue, int chunk,
                                                        unsigned long long* counters) {
   extern __shared__ __align__(16) char smem[];
   unsigned long long v[kCntSlots] = {0, 0, 0, 0, 0, 0};
-  CellState<N, R, LUT, BS, NF> c;
+  CellState<N, R, LUT, BS, NF, SPEC> c;
   c.bind(smem, threadIdx.x);
   long cur = 0, left = 0, cid = 0;  // logical index, cells still reserved, cell id
   const long nl = a.cell_list ? (long)(a.n_list_dev ? *a.n_list_dev : a.n_list) : a.n;
@@ -109,24 +109,24 @@ __global__ void __launch_bounds__(BS, 1) k_chem_queue(StepArgs a, int* queue, in
   if (counters) block_flush_counters(counters, v);
 }
 
-template <int N, int R, int JAC, typename LUT, int BS, int NF>
+template <int N, int R, int JAC, typename LUT, int BS, int NF, bool SPEC>
 static cudaError_t launch_bs(const StepArgs& a, const LaunchCfg& cfg, int* queue,
                              unsigned long long* counters, cudaStream_t s) {
   const size_t smem = (size_t)BS * SmemStore<N, R, LUT, BS>::kBytesPerThread;
   cudaError_t e;
   if (cfg.kernel == kKernelThreadQueue) {
-    e = cudaFuncSetAttribute(k_chem_queue<N, R, JAC, LUT, BS, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(k_chem_queue<N, R, JAC, LUT, BS, NF, SPEC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem);
     if (e != cudaSuccess) return e;
     const int grid = cfg.grid > 0 ? cfg.grid : 148;
-    k_chem_queue<N, R, JAC, LUT, BS, NF><<<grid, BS, smem, s>>>(a, queue, cfg.chunk, counters);
+    k_chem_queue<N, R, JAC, LUT, BS, NF, SPEC><<<grid, BS, smem, s>>>(a, queue, cfg.chunk, counters);
   } else {
-    e = cudaFuncSetAttribute(k_chem_plain<N, R, JAC, LUT, BS, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(k_chem_plain<N, R, JAC, LUT, BS, NF, SPEC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem);
     if (e != cudaSuccess) return e;
     const long nl = a.cell_list ? (long)a.n_list : a.n;
     const long grid = (nl + BS - 1) / BS;
-    if (grid > 0) k_chem_plain<N, R, JAC, LUT, BS, NF><<<(unsigned)grid, BS, smem, s>>>(a, counters);
+    if (grid > 0) k_chem_plain<N, R, JAC, LUT, BS, NF, SPEC><<<(unsigned)grid, BS, smem, s>>>(a, counters);
   }
   return cudaGetLastError();
 }
@@ -205,8 +205,9 @@ static cudaError_t launch_warp(const StepArgs& a, const LaunchCfg& cfg, int* que
 // waiting for the slowest warp of a larger block.  NF mechanism species, NI of
 // them integrated by the thread-per-cell kernels (the translation unit's
 // tables are numbered over those NI); the warp kernel integrates all NF from
-// the full tables it copies to shared memory.
-template <int NF, int NI, int R, int JAC, typename LUT>
+// the full tables it copies to shared memory.  SPEC: the thread kernels use
+// the generated mechanism-specialised RHS and iteration matrix.
+template <int NF, int NI, int R, int JAC, typename LUT, bool SPEC>
 static cudaError_t launch_variant(const StepArgs& a, const LaunchCfg& cfg, int* queue,
                                   unsigned long long* counters, cudaStream_t s) {
   if (cfg.kernel == kKernelWarpQueue) {
@@ -217,8 +218,8 @@ static cudaError_t launch_variant(const StepArgs& a, const LaunchCfg& cfg, int* 
     }
   }
   switch (cfg.block) {
-    case 32: return launch_bs<NI, R, JAC, LUT, 32, NF>(a, cfg, queue, counters, s);
-    case 64: return launch_bs<NI, R, JAC, LUT, 64, NF>(a, cfg, queue, counters, s);
+    case 32: return launch_bs<NI, R, JAC, LUT, 32, NF, SPEC>(a, cfg, queue, counters, s);
+    case 64: return launch_bs<NI, R, JAC, LUT, 64, NF, SPEC>(a, cfg, queue, counters, s);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -47,7 +47,10 @@ void upload_mechanism(const DevMech& full, const DevMech& reduced, cudaStream_t 
 
 // jac: 0 finite-difference (reference DDPST), 1 analytic.  mixed: float LU.
 // queue must point at a zeroed device int for the work-queue kernels.
-cudaError_t launch_chem(int n_species, int n_int, int n_reactions, int jac, bool mixed, const StepArgs& a,
+// True when the reduced reaction lists equal those the generated
+// mechanism-specialised code was written for.
+bool matches_specialised(const DevMech& reduced);
+cudaError_t launch_chem(int n_species, int n_int, bool spec, int n_reactions, int jac, bool mixed, const StepArgs& a,
                         const LaunchCfg& cfg, int* queue, unsigned long long* counters,
                         cudaStream_t s);
 
