@@ -244,14 +244,12 @@ def main():
     if args.impl == "reference":
         return run_reference(args)
     import torch
-    import torch.distributed as dist
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch.distributed as tdist
+    from nrg_b200 import dist
+    rank, world, local = dist.world()
     torch.cuda.set_device(local)
     if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist.init("nccl", timeout_s=600)
     from nrg_b200 import fields as F, keromnes_paths
     from nrg_b200.chemistry import ChemicalKineticsSolver, DataManager, fp64_peak_tflops, mechanism_tables
     from nrg_b200.surrogate import DEFAULT_MODEL, RECIPE, Surrogate, train_default
@@ -304,8 +302,7 @@ def main():
         for _ in range(args.warmup):
             solver.step_device(field.dt, T, rho, Y, Yp, Yp2, Ef, T_after=Ta, status=st)
         torch.cuda.synchronize()
-        if world > 1:
-            dist.barrier()
+        dist.barrier()
         stats = []
         with ClockSampler(local) as clk:
             torch.cuda.synchronize()
@@ -315,11 +312,7 @@ def main():
                 stats.append(solver.step_device(field.dt, T, rho, Y, Yp, Yp2, Ef, T_after=Ta, status=st))
             e1.record()
             torch.cuda.synchronize()
-        el = e0.elapsed_time(e1)
-        if world > 1:
-            t = torch.tensor([el], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            el = float(t.item())
+        el = dist.max_over_ranks(e0.elapsed_time(e1), dev)  # the job's time: its slowest rank
         # one untimed step with per-phase events for the roofline
         solver.set_timing(True)
         ph = solver.step_device(field.dt, T, rho, Y, Yp, Yp2, Ef, T_after=Ta, status=st)
@@ -369,16 +362,11 @@ def main():
             hs.set_gate(*RECIPE["gate"])
         host.set_mode(mode)
         host.solve_chemical_kinetics(field.dt)
-        if world > 1:
-            dist.barrier()
+        dist.barrier()
         t0 = time.perf_counter()
         for _ in range(args.steps):
             host.solve_chemical_kinetics(field.dt)
-        el2 = time.perf_counter() - t0
-        if world > 1:
-            t = torch.tensor([el2], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            el2 = float(t.item())
+        el2 = dist.max_over_ranks(time.perf_counter() - t0, dev)
         e2e = {"value": args.steps * n * world / el2, "unit": UNIT,
                "h2d_bytes_per_step": n * H2D_BYTES_PER_CELL, "d2h_bytes_per_step": n * D2H_BYTES_PER_CELL,
                "path": "nrg_chem_step (host Fortran-layout arrays, gather/H2D/step/D2H/scatter)"}
@@ -440,7 +428,7 @@ def main():
     solver.close()
     if world > 1:
         dist.barrier()
-        dist.destroy_process_group()
+        tdist.destroy_process_group()
     return 0
 
 
