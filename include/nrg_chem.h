@@ -137,6 +137,24 @@ NRG_API int nrg_chem_step_device_noalloc(nrg_chem* h, double time_step, long n, 
                                          double* Y_prod, double* Y_prod2, double* E_f_prod, double* T_after,
                                          unsigned char* status, void* stream, nrg_chem_stats* stats);
 
+/* The chemistry sources applied to the flow state and the state equation,
+ * on device arrays (same layout as nrg_chem_step_device), for cells with
+ * bc == 0 (bc may be NULL).  Replaces the reactive terms of the source
+ * integration (cpm_solver.f90:513-560: E_f += E_f_prod * dt / rho,
+ * Y += Y_prod * dt / rho) followed by apply_state_equation
+ * (table_approximated_real_gas.f90:368-470), so the chemistry step's outputs
+ * update Y, E_f, T and p without leaving the GPU.  Y_prod and E_f_prod may be
+ * NULL (state equation only; time_step is then ignored).  v: dims (0..3)
+ * velocity components, v[d * ld + c].  T is read as the Newton start of the
+ * temperature solve and overwritten.  cp_mass, h_s, h_full, v_s,
+ * mix_mol_mass and status may be NULL; status: 0 skipped, 1 ok, 2 negative
+ * gamma, p or rho (the reference stops the run there). */
+NRG_API int nrg_chem_apply_state_device(nrg_chem* h, double time_step, long n, long ld, int dims,
+                                        const double* rho, const double* Y_prod, const double* E_f_prod,
+                                        const signed char* bc, double* Y, double* E_f, const double* v, double* T,
+                                        double* p, double* gamma, double* cp_mass, double* h_s, double* h_full,
+                                        double* v_s, double* mix_mol_mass, unsigned char* status, void* stream);
+
 /* Mode (enum nrg_mode).  The reference's ODE_solver selector
  * (chemical_kinetics_solver.f90:91,309-316) has no GPU counterpart for
  * 'table_approximated'. */

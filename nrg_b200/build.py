@@ -23,7 +23,7 @@ SOURCES = {
     "chem_k_ref.cu": ["--fmad=false"],
     "chem_k_fast.cu": [],
     "chem_k_mixed.cu": [],
-    "chem_kernels.cu": [],
+    "chem_kernels.cu": ["--fmad=false"],  # state equation in the reference's operation order
     "capi.cu": [],
     "surrogate.cu": [],
     "mechanism.cpp": [],

@@ -99,6 +99,7 @@ SIGNATURES = {
     "nrg_surrogate_train": (_I, [_VP, _L, _VP, _VP, _I, _I, ctypes.c_float, ctypes.c_ulonglong, _VP]),
     "nrg_surrogate_set_gate": (_I, [_VP, _D, _D, _D, _D]),
     "nrg_chem_set_specialised": (_I, [_VP, _I]),
+    "nrg_chem_apply_state_device": (_I, [_VP, _D, _L, _L, _I] + [_VP] * 17),
     "nrg_surrogate_set_inference": (_I, [_VP, _I]),
     "nrg_surrogate_infer": (_I, [_VP, _L, _L, _D, _VP, _VP, _VP, _VP, _VP]),
     "nrg_surrogate_enable": (_I, [_VP, _I]),
@@ -261,6 +262,20 @@ class ChemicalKineticsSolver:
 
     def set_graph(self, enable: bool) -> None:
         _check(lib().nrg_chem_set_graph(self._h, int(enable)), self._h)
+
+    def apply_state_device(self, rho, Y, E_f, T, p, gamma, v=None, time_step=0.0, Y_prod=None, E_f_prod=None,
+                           bc=None, cp_mass=None, h_s=None, h_full=None, v_s=None, mix_mol_mass=None,
+                           status=None) -> None:
+        """Chemistry sources into (Y, E_f) and the state equation, on torch
+        CUDA tensors (Y species-major (N, n); v (dims, n) or None)."""
+        import torch
+        n = T.numel()
+        dims = 0 if v is None else int(v.shape[0])
+        _check(lib().nrg_chem_apply_state_device(
+            self._h, float(time_step), n, Y.shape[1], dims, _ptr(rho), _ptr(Y_prod), _ptr(E_f_prod), _ptr(bc),
+            _ptr(Y), _ptr(E_f), _ptr(v), _ptr(T), _ptr(p), _ptr(gamma), _ptr(cp_mass), _ptr(h_s), _ptr(h_full),
+            _ptr(v_s), _ptr(mix_mol_mass), _ptr(status),
+            ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)), self._h)
 
     def set_specialised(self, enable: bool) -> None:
         """Generated mechanism-specialised RHS / iteration matrix (default when

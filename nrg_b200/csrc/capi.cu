@@ -679,6 +679,30 @@ extern "C" int nrg_chem_autotune(nrg_chem* h, double time_step, long n, long ld,
   return NRG_OK;
 }
 
+extern "C" int nrg_chem_apply_state_device(nrg_chem* h, double time_step, long n, long ld, int dims,
+                                           const double* rho, const double* Y_prod, const double* E_f_prod,
+                                           const signed char* bc, double* Y, double* E_f, const double* v,
+                                           double* T, double* p, double* gamma, double* cp_mass, double* h_s,
+                                           double* h_full, double* v_s, double* mix_mol_mass,
+                                           unsigned char* status, void* stream) {
+  if (!h) return NRG_ERR_ARG;
+  if (n < 0 || ld < n || dims < 0 || dims > 3 || (dims > 0 && !v) ||
+      (n > 0 && (!rho || !Y || !E_f || !T || !p || !gamma)) || ((Y_prod || E_f_prod) && !(time_step > 0.0)))
+    return fail(h, NRG_ERR_ARG, "bad arguments to nrg_chem_apply_state_device");
+  CK(h, cudaSetDevice(h->device));
+  CK(h, cudaEventRecord(h->ev_in, (cudaStream_t)stream));
+  CK(h, cudaStreamWaitEvent(h->stream, h->ev_in, 0));
+  nrg::ApplyStateArgs a{};
+  a.n = n; a.ld = ld; a.dims = dims; a.dt = time_step; a.rho = rho; a.Y_prod = Y_prod; a.E_f_prod = E_f_prod;
+  a.bc = (const int8_t*)bc; a.Y = Y; a.E_f = E_f; a.v = v; a.T = T; a.p = p; a.gamma = gamma;
+  a.cp_mass = cp_mass; a.h_s = h_s; a.h_full = h_full; a.v_s = v_s; a.mix_mol_mass = mix_mol_mass;
+  a.status = status;
+  const cudaError_t e = nrg::launch_apply_state(h->mech.n(), a, h->stream);
+  if (e != cudaSuccess) return cuda_fail(h, e, "state equation launch");
+  CK(h, cudaStreamSynchronize(h->stream));
+  return NRG_OK;
+}
+
 extern "C" int nrg_chem_info(nrg_chem* h, int* n_species, int* n_reactions) {
   if (!h) return NRG_ERR_ARG;
   if (n_species) *n_species = h->mech.n();

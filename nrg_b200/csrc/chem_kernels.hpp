@@ -32,6 +32,30 @@ struct StepArgs {
   const int* n_list_dev;   // device-side entry count of cell_list (may be null)
 };
 
+// Chemistry sources applied to the state, then the state equation.
+struct ApplyStateArgs {
+  long n, ld;
+  int dims;                 // velocity components in v
+  double dt;
+  const double* rho;
+  const double* Y_prod;     // may be null (state equation only)
+  const double* E_f_prod;   // may be null
+  const int8_t* bc;         // may be null
+  double* Y;                // in/out, species-major
+  double* E_f;              // in/out (total energy per mass)
+  const double* v;          // dims x ld (may be null when dims == 0)
+  double* T;                // in: Newton start; out
+  double* p;
+  double* gamma;
+  double* cp_mass;          // optional outputs from here on
+  double* h_s;
+  double* h_full;
+  double* v_s;
+  double* mix_mol_mass;
+  uint8_t* status;          // 0 skipped (bc), 1 ok, 2 negative gamma, p or rho
+};
+cudaError_t launch_apply_state(int n_species, const ApplyStateArgs& a, cudaStream_t s);
+
 enum KernelKind { kKernelThreadGrid = 0, kKernelThreadQueue = 1, kKernelWarpQueue = 2 };
 
 struct LaunchCfg {

@@ -93,6 +93,19 @@ double orc_dnrm2(int n, const double *dx, int incx);
 /* Gear (MINT=2) coefficient tables, EL(13,12) and TQ(3,12) column-major */
 void orc_ddcst(int maxord, double *el, double *tq);
 
+/* The chemistry sources applied to the state (the reactive terms of
+ * cpm_solver.f90:513-560: E_f += E_f_prod*dt/rho, Y += Y_prod*dt/rho) and the
+ * state equation (apply_state_equation, table_approximated_real_gas.f90:
+ * 368-470) for cells with bc == 0 (bc may be NULL).  Y_prod / E_f_prod may be
+ * NULL (state equation only).  v holds dims velocity components (v[d*n+c]).
+ * T is read as the Newton start and overwritten.  Per-cell status: 0 skipped
+ * (bc), 1 ok, 2 negative gamma, p or rho (the reference stops there). */
+int orc_apply_state(const orc_mech *m, long n, int dims, double dt, const double *rho,
+                    const double *Y_prod, const double *E_f_prod, const signed char *bc,
+                    double *Y, double *E_f, const double *v, double *T, double *p,
+                    double *gamma, double *cp_mass, double *h_s, double *h_full, double *v_s,
+                    double *mix_mol_mass, unsigned char *status, int n_threads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -68,6 +68,11 @@ def lib():
         L.orc_chem_step_mx.restype = ctypes.c_int
         L.orc_temperature_after.argtypes = [ctypes.POINTER(OrcMech), ctypes.c_long, ctypes.c_double,
                                             dp, dp, dp, dp, dp, dp, ctypes.c_int]
+        L.orc_apply_state.argtypes = [ctypes.POINTER(OrcMech), ctypes.c_long, ctypes.c_int, ctypes.c_double,
+                                      dp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, dp, dp,
+                                      ctypes.c_void_p, dp, dp, dp, dp, dp, dp, dp, dp, ctypes.c_void_p,
+                                      ctypes.c_int]
+        L.orc_apply_state.restype = ctypes.c_int
         L.orc_rate_constants.argtypes = [ctypes.POINTER(OrcMech), ctypes.c_double, dp, dp, dp]
         L.orc_rate_constants.restype = None
         L.orc_rhs.argtypes = [ctypes.POINTER(OrcMech), dp, dp, dp, dp, dp]
@@ -154,6 +159,33 @@ class Mechanism:
         args = [np.ascontiguousarray(a, dtype=np.float64) for a in (T, rho, Y, Y_prod, E_f_prod)]
         lib().orc_temperature_after(ctypes.byref(self.m), n, float(dt), *[_dp(a) for a in args],
                                     _dp(out), int(threads))
+        return out
+
+    def apply_state(self, rho, Y, E_f, T, v=None, dt=0.0, Y_prod=None, E_f_prod=None, bc=None, threads=0):
+        """Chemistry sources applied to (Y, E_f), then the state equation
+        (orc_apply_state).  Y is (N, n) SoA, v (dims, n) or None.  Returns the
+        updated Y, E_f, T and p, gamma, cp, h_s, h_full, v_s, mix_mol_mass,
+        status."""
+        n = rho.shape[0]
+        N = self.m.n_species
+        Y = np.array(Y, dtype=np.float64).reshape(N, n)
+        E_f = np.array(E_f, dtype=np.float64)
+        T = np.array(T, dtype=np.float64)
+        rho = np.ascontiguousarray(rho, dtype=np.float64)
+        dims = 0 if v is None else int(np.asarray(v).shape[0])
+        vv = np.zeros((1, n)) if v is None else np.ascontiguousarray(v, dtype=np.float64)
+        out = {k: np.zeros(n) for k in ("p", "gamma", "cp", "h_s", "h_full", "v_s", "mix_mol_mass")}
+        st = np.zeros(n, np.uint8)
+        yp = None if Y_prod is None else np.ascontiguousarray(Y_prod, dtype=np.float64)
+        ep = None if E_f_prod is None else np.ascontiguousarray(E_f_prod, dtype=np.float64)
+        bcv = None if bc is None else np.ascontiguousarray(bc, dtype=np.int8)
+        vp = lambda a: None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+        lib().orc_apply_state(ctypes.byref(self.m), n, dims, float(dt), _dp(rho), vp(yp), vp(ep), vp(bcv),
+                              _dp(Y), _dp(E_f), vv.ctypes.data_as(ctypes.c_void_p), _dp(T), _dp(out["p"]),
+                              _dp(out["gamma"]), _dp(out["cp"]), _dp(out["h_s"]), _dp(out["h_full"]),
+                              _dp(out["v_s"]), _dp(out["mix_mol_mass"]), st.ctypes.data_as(ctypes.c_void_p),
+                              int(threads))
+        out.update(Y=Y, E_f=E_f, T=T, status=st)
         return out
 
     def rate_constants(self, T, mix_conc):

@@ -913,3 +913,58 @@ int orc_temperature_after(const orc_mech *m, long n, double dt,
     }
     return 0;
 }
+
+/* ------------------------------------------------ sources + state equation */
+/* The reactive terms of the source integration in cpm_solver.f90:513-560
+ * (E_f_int = E_f + E_f_prod * dt / rho, Y_int = Y + Y_prod * dt / rho; the
+ * renormalisation there is commented out) followed by apply_state_equation,
+ * table_approximated_real_gas.f90:368-470, for cells with bc == 0. */
+int orc_apply_state(const orc_mech *m, long n, int dims, double dt, const double *rho,
+                    const double *Y_prod, const double *E_f_prod, const signed char *bc,
+                    double *Y, double *E_f, const double *v, double *T, double *p,
+                    double *gamma, double *cp_mass, double *h_s, double *h_full, double *v_s,
+                    double *mix_mol_mass, unsigned char *status, int n_threads) {
+    const int N = m->n_species;
+#ifdef _OPENMP
+    int nt = n_threads > 0 ? n_threads : omp_get_max_threads();
+#pragma omp parallel for schedule(static) num_threads(nt)
+#else
+    (void)n_threads;
+#endif
+    for (long c = 0; c < n; c++) {
+        if (bc && bc[c] != 0) {
+            if (status) status[c] = 0;
+            continue;
+        }
+        if (E_f_prod) E_f[c] = E_f[c] + E_f_prod[c] * dt / rho[c];
+        if (Y_prod)
+            for (int k = 0; k < N; k++)
+                Y[(long)k * n + c] = Y[(long)k * n + c] + Y_prod[(long)k * n + c] * dt / rho[c];
+        double e_i = E_f[c];
+        for (int d = 0; d < dims; d++) e_i = e_i - 0.5 * (v[(long)d * n + c] * v[(long)d * n + c]);
+        double avg = 0.0;
+        for (int k = 0; k < N; k++)
+            if (m->molar_mass[k] != 0.0) avg = avg + Y[(long)k * n + c] / m->molar_mass[k];
+        avg = 1.0 / avg;
+        mix_mol_mass[c] = avg;
+        double X[ORC_NMAX];
+        for (int k = 0; k < N; k++)
+            X[k] = m->molar_mass[k] != 0.0 ? Y[(long)k * n + c] / m->molar_mass[k] * avg : 0.0;
+        e_i = e_i * avg;
+        const double h_s_tref = mixture_enthalpy(m, T_REF, X);
+        const double t = calculate_temperature(m, T[c], e_i, X);
+        T[c] = t;
+        p[c] = t * rho[c] * R_GASE_J / avg;
+        const double cp = mixture_cp(m, t, X);
+        const double cv = cp - R_GASE_J;
+        gamma[c] = cp / cv;
+        const double h = mixture_enthalpy(m, t, X);
+        h_s[c] = (h - h_s_tref) / avg;
+        h_full[c] = h / avg;
+        cp_mass[c] = cp / avg;
+        const int bad = (gamma[c] < 0.0) || (p[c] < 0.0) || (rho[c] < 0.0);
+        if (status) status[c] = bad ? 2 : 1;
+        v_s[c] = sqrt(gamma[c] * p[c] / rho[c]);
+    }
+    return 0;
+}

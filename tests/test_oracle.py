@@ -180,3 +180,56 @@ def test_energy_closure_round_trip(oracle_mech, W):
     zero = np.zeros((9, n))
     T1 = oracle_mech.temperature_after(f.dt, f.T[:n], f.rho[:n], f.Y[:, :n], zero, np.zeros(n))
     np.testing.assert_allclose(T1, f.T[:n], rtol=1e-9)
+
+
+def _energy_per_mass(m, T, Y, W, v):
+    """Total energy per mass of (T, Y, v): sensible internal energy above
+    T_ref plus kinetic (the inverse of the state equation's energy)."""
+    R = 8.31446261815324
+    X = Y / W[:, None]
+    Wm = 1.0 / X.sum(0)
+    X = X * Wm
+    e = np.zeros(T.shape[0])
+    h0 = np.zeros(T.shape[0])
+    for c in range(T.shape[0]):
+        for k in range(W.shape[0]):
+            e[c] += (m.enthalpy(T[c], k) - R * T[c]) * X[k, c]
+            h0[c] += m.enthalpy(298.15, k) * X[k, c]
+    return (e - h0) / Wm + 0.5 * (v * v).sum(0)
+
+
+def test_state_equation_recovers_temperature(oracle_mech, W):
+    """apply_state_equation inverts the energy of a known state: T back to
+    the Newton tolerance, p = rho R T / W_mix, gamma and v_s consistent."""
+    from nrg_b200 import fields
+    f = fields.slice_field(fields.config0(W), 256)
+    rng = np.random.default_rng(5)
+    v = rng.uniform(-300.0, 300.0, (2, f.n))
+    E = _energy_per_mass(oracle_mech, f.T, f.Y, W, v)
+    out = oracle_mech.apply_state(f.rho, f.Y, E, f.T * 0.9, v=v)
+    assert np.all(out["status"] == 1)
+    assert np.max(np.abs(out["T"] - f.T)) < 1e-6
+    Wm = 1.0 / (f.Y / W[:, None]).sum(0)
+    np.testing.assert_allclose(out["p"], f.rho * 8.31446261815324 * out["T"] / Wm, rtol=1e-14)
+    np.testing.assert_allclose(out["mix_mol_mass"], Wm, rtol=1e-14)
+    assert np.all((out["gamma"] > 1.0) & (out["gamma"] < 1.67))
+    np.testing.assert_allclose(out["v_s"], np.sqrt(out["gamma"] * out["p"] / f.rho), rtol=1e-14)
+
+
+def test_state_equation_applies_the_chemistry_sources(oracle_mech, W):
+    """Y += Y_prod dt / rho and E_f += E_f_prod dt / rho before the state
+    equation; bc cells untouched."""
+    from nrg_b200 import fields
+    f = fields.slice_field(fields.config0(W), 64)
+    o = oracle_mech.chem_step(f.dt, f.T, f.rho, f.Y)
+    E = _energy_per_mass(oracle_mech, f.T, f.Y, W, np.zeros((0, f.n)))
+    bc = np.zeros(f.n, np.int8)
+    bc[:4] = 1
+    out = oracle_mech.apply_state(f.rho, f.Y, E, f.T, dt=f.dt, Y_prod=o["Y_prod"], E_f_prod=o["E_f_prod"], bc=bc)
+    act = bc == 0
+    np.testing.assert_array_equal(out["Y"][:, ~act], f.Y[:, ~act])
+    np.testing.assert_allclose(out["Y"][:, act], (f.Y + o["Y_prod"] * f.dt / f.rho)[:, act], rtol=0, atol=1e-15)
+    # the closure of the chemistry step gives the same temperature
+    T1 = oracle_mech.temperature_after(f.dt, f.T, f.rho, f.Y, o["Y_prod"], o["E_f_prod"])
+    assert np.max(np.abs(out["T"][act] - T1[act])) < 1e-6
+    assert np.all(out["status"][~act] == 0)
