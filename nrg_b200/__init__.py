@@ -9,7 +9,18 @@ import os
 MECH_DIR = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "tests", "golden", "mechanism")
 
 
+MECHANISMS = ("KEROMNES", "ZHANG", "TEREZA", "KONNOV")
+
+
+def mechanism_paths(name: str = "KEROMNES"):
+    """Input decks of one of the reference's H2/air mechanisms (mechanism,
+    thermo, molar masses), as in its task_setup directory."""
+    if name not in MECHANISMS:
+        raise ValueError(f"unknown mechanism {name!r}; have {MECHANISMS}")
+    return (os.path.join(MECH_DIR, f"{name}.txt"), os.path.join(MECH_DIR, f"{name}_THERMO.txt"),
+            os.path.join(MECH_DIR, "molar_masses.dat"))
+
+
 def keromnes_paths():
     """The reference's H2/air input decks (mechanism, thermo, molar masses)."""
-    return (os.path.join(MECH_DIR, "KEROMNES.txt"), os.path.join(MECH_DIR, "KEROMNES_THERMO.txt"),
-            os.path.join(MECH_DIR, "molar_masses.dat"))
+    return mechanism_paths("KEROMNES")

@@ -289,8 +289,39 @@ cudaError_t enqueue_step(nrg_chem* h, const StepArgs& a, cudaStream_t s) {
 }
 
 // Runs the step on stream s, through a CUDA graph when enabled.
+// The kernels read the mechanism from per-translation-unit __constant__
+// tables, one set per device.  Before a handle launches work, its tables are
+// put in place if another handle (possibly another mechanism) put its own
+// there last; the switch waits for the device to be idle, so calls of
+// handles with different tables are serialised rather than overlapped.
+std::mutex g_tables_mu;
+const nrg_chem* g_tables_owner[64] = {};
+
+cudaError_t use_tables(nrg_chem* h) {
+  std::lock_guard<std::mutex> lock(g_tables_mu);
+  const int d = h->device;
+  if (d < 0 || d >= 64) return cudaErrorInvalidDevice;
+  if (g_tables_owner[d] == h) return cudaSuccess;
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return e;
+  nrg::upload_mechanism(h->dm, h->dmr, h->stream);
+  nrg::surrogate_upload_tables(h->dm, h->stream);
+  e = cudaStreamSynchronize(h->stream);
+  if (e == cudaSuccess) g_tables_owner[d] = h;
+  return e;
+}
+
+void release_tables(const nrg_chem* h) {
+  std::lock_guard<std::mutex> lock(g_tables_mu);
+  for (auto& o : g_tables_owner)
+    if (o == h) o = nullptr;
+}
+
 int run_step(nrg_chem* h, const StepArgs& a, cudaStream_t s, nrg_chem_stats* stats) {
+  CK(h, use_tables(h));
   if (h->mode == NRG_MODE_SURROGATE) {
+    if (!(h->mech.n() == 9 && h->mech.r() == 24))
+      return fail(h, NRG_ERR_UNSUPPORTED, "the surrogate is built for the 9-species, 24-reaction mechanism");
     if (!nrg::surrogate_ready(h->sur))
       return fail(h, NRG_ERR_STATE, "surrogate mode selected but no trained model is loaded");
     const std::string e = nrg::surrogate_reserve(h->sur, a.n);
@@ -381,7 +412,7 @@ extern "C" int nrg_chem_create(const char* mechanism_path, const char* thermo_pa
   if (!e.empty()) { delete h; return fail(nullptr, NRG_ERR_IO, e); }
   e = build_dev_mech(h->mech, &h->dm);
   if (!e.empty()) { delete h; return fail(nullptr, NRG_ERR_UNSUPPORTED, e); }
-  if (!(h->mech.n() == 9 && h->mech.r() == 24)) {
+  if (!nrg::supported_mechanism(h->mech.n(), h->mech.r())) {
     std::string msg = "no compiled kernel for " + std::to_string(h->mech.n()) + " species / " +
                       std::to_string(h->mech.r()) + " reactions";
     delete h;
@@ -406,8 +437,8 @@ extern "C" int nrg_chem_create(const char* mechanism_path, const char* thermo_pa
   }
   reduce_dev_mech(h->dm, &h->dmr);
   h->spec = nrg::matches_specialised(h->dmr);
-  nrg::upload_mechanism(h->dm, h->dmr, h->stream);
-  if ((ce = cudaStreamSynchronize(h->stream)) != cudaSuccess) {
+  h->sur = nrg::surrogate_create(h->dm);
+  if ((ce = use_tables(h)) != cudaSuccess) {
     std::string msg = std::string("mechanism upload failed: ") + cudaGetErrorString(ce);
     nrg_chem_destroy(h);
     return fail(nullptr, NRG_ERR_CUDA, msg);
@@ -416,12 +447,12 @@ extern "C" int nrg_chem_create(const char* mechanism_path, const char* thermo_pa
   h->cfg.block = 32;
   h->cfg.grid = 0;
   h->cfg.chunk = 1;
-  h->sur = nrg::surrogate_create(h->dm);
   *out = h;
   return NRG_OK;
 }
 
 extern "C" int nrg_chem_destroy(nrg_chem* h) {
+  if (h) release_tables(h);
   if (!h) return NRG_ERR_ARG;
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
@@ -502,6 +533,7 @@ extern "C" int nrg_chem_step_device(nrg_chem* h, double time_step, long n, long 
     return fail(h, NRG_ERR_ARG, "null field pointer");
   if (n > 0x7fffffffL / 2) return fail(h, NRG_ERR_ARG, "too many cells for one call");
   CK(h, cudaSetDevice(h->device));
+  CK(h, use_tables(h));
   StepArgs a;
   a.n = n;
   a.ld = ld;
@@ -620,6 +652,7 @@ extern "C" int nrg_chem_autotune(nrg_chem* h, double time_step, long n, long ld,
   if (n <= 0 || ld < n || !T || !rho || !Y || !Y_prod || !Y_prod2 || !E_f_prod)
     return fail(h, NRG_ERR_ARG, "autotune needs device inputs with n > 0");
   CK(h, cudaSetDevice(h->device));
+  CK(h, use_tables(h));
   StepArgs a;
   a.n = n; a.ld = ld; a.dt = time_step; a.T = T; a.rho = rho; a.Y = Y; a.bc = (const int8_t*)bc;
   a.Y_prod = Y_prod; a.Y_prod2 = Y_prod2; a.E_f_prod = E_f_prod; a.T_after = nullptr; a.status = nullptr;
@@ -666,6 +699,11 @@ extern "C" int nrg_chem_autotune(nrg_chem* h, double time_step, long n, long ld,
       CK(h, cudaMemsetAsync(h->d_counters, 0, sizeof(unsigned long long) * 8, s));
       CK(h, cudaEventRecord(h->ev0, s));
       cudaError_t e = enqueue_integrator(h, a, c, s);
+      if (e == cudaErrorNotSupported) {  // shape not compiled for this mechanism
+        cudaGetLastError();
+        CK(h, cudaStreamSynchronize(s));
+        break;
+      }
       if (e != cudaSuccess) return cuda_fail(h, e, "autotune launch");
       CK(h, cudaEventRecord(h->ev1, s));
       CK(h, cudaStreamSynchronize(s));
@@ -690,6 +728,7 @@ extern "C" int nrg_chem_apply_state_device(nrg_chem* h, double time_step, long n
       (n > 0 && (!rho || !Y || !E_f || !T || !p || !gamma)) || ((Y_prod || E_f_prod) && !(time_step > 0.0)))
     return fail(h, NRG_ERR_ARG, "bad arguments to nrg_chem_apply_state_device");
   CK(h, cudaSetDevice(h->device));
+  CK(h, use_tables(h));
   CK(h, cudaEventRecord(h->ev_in, (cudaStream_t)stream));
   CK(h, cudaStreamWaitEvent(h->stream, h->ev_in, 0));
   nrg::ApplyStateArgs a{};
@@ -840,6 +879,7 @@ extern "C" int nrg_surrogate_norm_count(void) { return kNormFloats; }
 extern "C" int nrg_surrogate_init(nrg_chem* h, unsigned long long seed) {
   if (!h) return NRG_ERR_ARG;
   CK(h, cudaSetDevice(h->device));
+  CK(h, use_tables(h));
   return sfail(h, nrg::surrogate_init(h->sur, seed, h->stream));
 }
 
@@ -873,6 +913,7 @@ extern "C" int nrg_surrogate_prepare(nrg_chem* h, long n, long ld, double dt, co
   if (!(opts->hull_margin >= 0.f) || !(opts->log_eps > 0.f) || (opts->log_mask >> 9))
     return fail(h, NRG_ERR_ARG, "bad nrg_surrogate_opts (hull_margin >= 0, log_eps > 0, log_mask < 512)");
   CK(h, cudaSetDevice(h->device));
+  CK(h, use_tables(h));
   int rc = order_after_legacy(h);
   if (rc) return rc;
   const nrg::PrepareOpts o{opts->hull_margin, opts->dt_pow, opts->log_mask, opts->log_eps, opts->common_dY_scale};
@@ -885,6 +926,7 @@ extern "C" int nrg_surrogate_features(nrg_chem* h, long n, long ld, double dt, c
                                       void* x_bf16) {
   if (!h || n < 0 || ld < n || (n > 0 && (!T || !rho || !Y))) return fail(h, NRG_ERR_ARG, "bad features args");
   CK(h, cudaSetDevice(h->device));
+  CK(h, use_tables(h));
   int rc = order_after_legacy(h);
   if (rc) return rc;
   std::string e = nrg::surrogate_features(h->sur, n, ld, dt, dt_cells, T, rho, Y, xraw, (__nv_bfloat16*)x_bf16,
@@ -897,6 +939,7 @@ extern "C" int nrg_surrogate_features(nrg_chem* h, long n, long ld, double dt, c
 extern "C" int nrg_surrogate_forward(nrg_chem* h, long n, const void* x_bf16, float* out) {
   if (!h || n <= 0 || !x_bf16 || !out) return fail(h, NRG_ERR_ARG, "bad forward args");
   CK(h, cudaSetDevice(h->device));
+  CK(h, use_tables(h));
   int rc = order_after_legacy(h);
   if (rc) return rc;
   return sfail(h, nrg::surrogate_forward(h->sur, n, (const __nv_bfloat16*)x_bf16, out, h->stream));
@@ -906,6 +949,7 @@ extern "C" int nrg_surrogate_grad(nrg_chem* h, long n, const void* x_bf16, const
                                   double* loss_host) {
   if (!h || n <= 0 || !x_bf16 || !y) return fail(h, NRG_ERR_ARG, "bad grad args");
   CK(h, cudaSetDevice(h->device));
+  CK(h, use_tables(h));
   int rc = order_after_legacy(h);
   if (rc) return rc;
   return sfail(h, nrg::surrogate_grad(h->sur, n, (const __nv_bfloat16*)x_bf16, y, grads_host, loss_host, h->stream));
@@ -915,6 +959,7 @@ extern "C" int nrg_surrogate_train(nrg_chem* h, long n, const void* x_bf16, cons
                                    float lr, unsigned long long seed, float* loss_per_epoch) {
   if (!h || n <= 0 || !x_bf16 || !y || epochs <= 0 || !(lr > 0.f)) return fail(h, NRG_ERR_ARG, "bad train args");
   CK(h, cudaSetDevice(h->device));
+  CK(h, use_tables(h));
   int rc = order_after_legacy(h);
   if (rc) return rc;
   return sfail(h, nrg::surrogate_train(h->sur, n, (const __nv_bfloat16*)x_bf16, y, epochs, batch, lr, seed,
@@ -939,6 +984,7 @@ extern "C" int nrg_surrogate_infer(nrg_chem* h, long n, long ld, double dt, cons
   if (!h || n < 0 || ld < n || (n > 0 && (!T || !rho || !Y || !out)) || (!(dt > 0.0) && !dt_cells))
     return fail(h, NRG_ERR_ARG, "bad arguments to nrg_surrogate_infer");
   CK(h, cudaSetDevice(h->device));
+  CK(h, use_tables(h));
   int rc = order_after_legacy(h);
   if (rc) return rc;
   StepArgs a{};
@@ -1004,6 +1050,7 @@ extern "C" int nrg_chem_integrate(nrg_chem* h, long n, long ld, double dt, const
     return fail(h, NRG_ERR_ARG, "null field pointer");
   }
   CK(h, cudaSetDevice(h->device));
+  CK(h, use_tables(h));
   StepArgs a{};
   a.n = n; a.ld = ld; a.dt = dt > 0.0 ? dt : 1.0; a.T = T; a.rho = rho; a.Y = Y; a.bc = (const int8_t*)bc;
   a.Y_prod = Y_prod; a.Y_prod2 = Y_prod2; a.E_f_prod = E_f_prod; a.T_after = T_after; a.status = status;
@@ -1161,6 +1208,7 @@ extern "C" int nrg_chem_step_device_noalloc(nrg_chem* h, double time_step, long 
     return NRG_OK;
   }
   CK(h, cudaSetDevice(h->device));
+  CK(h, use_tables(h));
   std::string err;
   unsigned char* base = noalloc_scratch(h->device, &err);
   if (!base) return fail(h, NRG_ERR_CUDA, err);

@@ -12,9 +12,12 @@ namespace nrg {
 void upload_mechanism_ref(const DevMech& m, cudaStream_t s);
 void upload_mechanism_fast(const DevMech& m, cudaStream_t s);
 void upload_mechanism_mixed(const DevMech& m, cudaStream_t s);
-cudaError_t launch_chem_ref(const StepArgs&, const LaunchCfg&, int*, unsigned long long*, cudaStream_t);
-cudaError_t launch_chem_fast(const StepArgs&, const LaunchCfg&, int*, unsigned long long*, cudaStream_t, int, bool);
-cudaError_t launch_chem_mixed(const StepArgs&, const LaunchCfg&, int*, unsigned long long*, cudaStream_t, int, bool);
+bool supported_mechanism(int n_species, int n_reactions);
+cudaError_t launch_chem_ref(const StepArgs&, const LaunchCfg&, int*, unsigned long long*, cudaStream_t, int, int);
+cudaError_t launch_chem_fast(const StepArgs&, const LaunchCfg&, int*, unsigned long long*, cudaStream_t, int, bool,
+                             int, int);
+cudaError_t launch_chem_mixed(const StepArgs&, const LaunchCfg&, int*, unsigned long long*, cudaStream_t, int, bool,
+                              int, int);
 
 __global__ void k_fp64_peak(double* out, int iters) {
   double a0 = threadIdx.x * 1e-9, a1 = a0 + 1.0, a2 = a0 + 2.0, a3 = a0 + 3.0;
@@ -129,10 +132,14 @@ __global__ void k_apply_state(ApplyStateArgs a) {
 }
 
 cudaError_t launch_apply_state(int n_species, const ApplyStateArgs& a, cudaStream_t s) {
-  if (n_species != 9) return cudaErrorNotSupported;
   if (a.n <= 0) return cudaSuccess;
   const long grid = std::min<long>((a.n + 127) / 128, 148L * 16);
-  k_apply_state<9><<<(unsigned)grid, 128, 0, s>>>(a);
+  switch (n_species) {
+    case 9: k_apply_state<9><<<(unsigned)grid, 128, 0, s>>>(a); break;
+    case 10: k_apply_state<10><<<(unsigned)grid, 128, 0, s>>>(a); break;
+    case 13: k_apply_state<13><<<(unsigned)grid, 128, 0, s>>>(a); break;
+    default: return cudaErrorNotSupported;
+  }
   return cudaGetLastError();
 }
 
@@ -149,10 +156,15 @@ void upload_mechanism(const DevMech& full, const DevMech& reduced, cudaStream_t 
 cudaError_t launch_chem(int n_species, int n_int, bool spec, int n_reactions, int jac, bool mixed,
                         const StepArgs& a, const LaunchCfg& cfg, int* queue, unsigned long long* counters,
                         cudaStream_t s) {
-  if (n_species != 9 || n_reactions != 24) return cudaErrorNotSupported;
-  if (mixed) return launch_chem_mixed(a, cfg, queue, counters, s, n_int, spec);
-  return jac == kJacFD ? launch_chem_ref(a, cfg, queue, counters, s)
-                       : launch_chem_fast(a, cfg, queue, counters, s, n_int, spec);
+  if (!supported_mechanism(n_species, n_reactions)) return cudaErrorNotSupported;
+  if (mixed) return launch_chem_mixed(a, cfg, queue, counters, s, n_int, spec, n_species, n_reactions);
+  return jac == kJacFD ? launch_chem_ref(a, cfg, queue, counters, s, n_species, n_reactions)
+                       : launch_chem_fast(a, cfg, queue, counters, s, n_int, spec, n_species, n_reactions);
+}
+
+bool supported_mechanism(int n_species, int n_reactions) {
+  return (n_species == 9 && n_reactions == 24) || (n_species == 9 && n_reactions == 28) ||
+         (n_species == 10 && n_reactions == 24) || (n_species == 13 && n_reactions == 71);
 }
 
 bool matches_specialised(const DevMech& reduced) {

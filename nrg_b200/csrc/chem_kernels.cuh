@@ -132,13 +132,17 @@ static cudaError_t launch_bs(const StepArgs& a, const LaunchCfg& cfg, int* queue
 }
 
 
+__host__ __device__ constexpr size_t warp_tables_bytes() { return (sizeof(DevMech) + 15) / 16 * 16; }
+
 // Warp-per-cell persistent kernel: every warp pulls `chunk` cells at a time
 // from the work queue and integrates them one after the other.
 template <int N, int R, int JAC, typename LUT, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) k_chem_warp(StepArgs a, int* queue, int chunk,
                                                          unsigned long long* counters) {
-  __shared__ WarpSmem<N, R, LUT> sm[WARPS];
-  __shared__ __align__(16) DevMech sM;
+  // dynamic shared memory: the mechanism tables, then one scratch per warp
+  extern __shared__ __align__(16) char wsmem[];
+  DevMech& sM = *reinterpret_cast<DevMech*>(wsmem);
+  WarpSmem<N, R, LUT>* sm = reinterpret_cast<WarpSmem<N, R, LUT>*>(wsmem + warp_tables_bytes());
   {
     // lanes read per-reaction and per-species entries at different addresses,
     // which __constant__ memory would serialize: work from a shared copy
@@ -186,15 +190,19 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) k_chem_warp(St
 template <int N, int R, int JAC, typename LUT, int WARPS>
 static cudaError_t launch_warp(const StepArgs& a, const LaunchCfg& cfg, int* queue,
                                unsigned long long* counters, cudaStream_t s) {
+  const size_t smem = warp_tables_bytes() + WARPS * sizeof(WarpSmem<N, R, LUT>);
+  cudaError_t e = cudaFuncSetAttribute(k_chem_warp<N, R, JAC, LUT, WARPS>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
   int grid = cfg.grid;
   if (grid <= 0) {
     int dev = 0, sms = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_chem_warp<N, R, JAC, LUT, WARPS>, WARPS * 32, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_chem_warp<N, R, JAC, LUT, WARPS>, WARPS * 32, smem);
     grid = sms * (per_sm > 0 ? per_sm : 1);
   }
-  k_chem_warp<N, R, JAC, LUT, WARPS><<<grid, WARPS * 32, 0, s>>>(a, queue, cfg.chunk, counters);
+  k_chem_warp<N, R, JAC, LUT, WARPS><<<grid, WARPS * 32, smem, s>>>(a, queue, cfg.chunk, counters);
   return cudaGetLastError();
 }
 
@@ -220,6 +228,19 @@ static cudaError_t launch_variant(const StepArgs& a, const LaunchCfg& cfg, int* 
   switch (cfg.block) {
     case 32: return launch_bs<NI, R, JAC, LUT, 32, NF, SPEC>(a, cfg, queue, counters, s);
     case 64: return launch_bs<NI, R, JAC, LUT, 64, NF, SPEC>(a, cfg, queue, counters, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+// The thread-per-cell grid kernel only (the shape used for the mechanisms
+// other than the default one, which get no queue / warp variants).
+template <int NF, int NI, int R, int JAC, typename LUT>
+static cudaError_t launch_grid(const StepArgs& a, const LaunchCfg& cfg, int* queue, unsigned long long* counters,
+                               cudaStream_t s) {
+  if (cfg.kernel != kKernelThreadGrid) return cudaErrorNotSupported;
+  switch (cfg.block) {
+    case 32: return launch_bs<NI, R, JAC, LUT, 32, NF, false>(a, cfg, queue, counters, s);
+    case 64: return launch_bs<NI, R, JAC, LUT, 64, NF, false>(a, cfg, queue, counters, s);
     default: return cudaErrorInvalidValue;
   }
 }

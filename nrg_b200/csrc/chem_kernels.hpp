@@ -71,6 +71,10 @@ void upload_mechanism(const DevMech& full, const DevMech& reduced, cudaStream_t 
 
 // jac: 0 finite-difference (reference DDPST), 1 analytic.  mixed: float LU.
 // queue must point at a zeroed device int for the work-queue kernels.
+// Mechanism sizes (species, reactions) with compiled kernels: KEROMNES
+// (9, 24; every launch shape), ZHANG (9, 28), TEREZA (10, 24), KONNOV
+// (13, 71) (thread-per-cell grid, reference and analytic-Jacobian modes).
+bool supported_mechanism(int n_species, int n_reactions);
 // True when the reduced reaction lists equal those the generated
 // mechanism-specialised code was written for.
 bool matches_specialised(const DevMech& reduced);

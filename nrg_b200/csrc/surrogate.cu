@@ -800,10 +800,14 @@ int surrogate_param_count() {
   return off;
 }
 
+void surrogate_upload_tables(const DevMech& dm, cudaStream_t st) {
+  cudaMemcpyToSymbolAsync(c_mech, &dm, sizeof(DevMech), 0, cudaMemcpyHostToDevice, st);
+}
+
 Surrogate* surrogate_create(const DevMech& dm) {
   Surrogate* s = new Surrogate();
   s->n_params = param_layout(s);
-  cudaMemcpyToSymbol(c_mech, &dm, sizeof(DevMech));
+  (void)dm;  // the gate's tables are put in place with the handle's (surrogate_upload_tables)
   const size_t P = (size_t)s->n_params;
   if (cudaMalloc(&s->w, P * 4) != cudaSuccess || cudaMalloc(&s->m, P * 4) != cudaSuccess ||
       cudaMalloc(&s->v, P * 4) != cudaSuccess || cudaMalloc(&s->gr, P * 4) != cudaSuccess ||

@@ -17,6 +17,8 @@ struct Surrogate;
 using FallbackFn = std::function<cudaError_t(const StepArgs&, cudaStream_t)>;
 
 Surrogate* surrogate_create(const DevMech& dm);
+// The gate's copy of the mechanism tables (per translation unit).
+void surrogate_upload_tables(const DevMech& dm, cudaStream_t st);
 void surrogate_destroy(Surrogate* s);
 bool surrogate_ready(const Surrogate* s);
 

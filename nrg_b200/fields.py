@@ -153,3 +153,16 @@ def slice_field(f: Field, n: int, stride: int = 1, offset: int = 0) -> Field:
     return Field(f.name + f"[{n}]", f.T[sel].copy(), f.rho[sel].copy(), f.p[sel].copy(),
                  np.ascontiguousarray(f.Y[:, sel]), f.dt, (n,),
                  None if f.dt_cells is None else f.dt_cells[sel].copy())
+
+
+def state_for_species(f: Field, names, W: np.ndarray) -> Field:
+    """The same cells for a mechanism with other species: H2, O2, N2, H2O
+    and the five radicals keep their mass fractions, species the field does
+    not carry (excited or other states) start at zero; rho is recomputed from
+    p, T and the new mixture molar mass."""
+    idx = {s: i for i, s in enumerate(SPECIES)}
+    Y = np.zeros((len(names), f.n))
+    for k, nm in enumerate(names):
+        if nm in idx:
+            Y[k] = f.Y[idx[nm]]
+    return _finish(f.name, f.T.copy(), f.p.copy(), Y, W, f.dt, f.shape, f.dt_cells)

@@ -430,8 +430,13 @@ static int read_reactions(recfile *f, orc_mech *m) {
                 m->reaction_type[r] = 3;
                 if (r_type == 2) m->reaction_type[r] = 7;
                 rf_backspace(f);
-                ld_read_string_reals(f, s2, sizeof s2, v, 4, &error);
-                for (int q = 0; q < 4; q++) m->troe[r][q] = v[q];
+                /* a list-directed read assigns the items read before an
+                 * error; the others keep their value (zero from the
+                 * allocation, chemical_properties_class.f90:156).  ZHANG.txt:27
+                 * gives three TROE parameters: the read runs into the next
+                 * record, fails there and consumes it. */
+                const int got = ld_read_string_reals(f, s2, sizeof s2, v, 4, &error);
+                for (int q = 0; q < got && q < 4; q++) m->troe[r][q] = v[q];
             } else {
                 rf_backspace(f);
             }

@@ -191,3 +191,48 @@ def test_specialised_code_gives_the_table_driven_bits(decks, W, mode):
         s.close()
     for key in ("Y_prod", "Y_prod2", "E_f_prod", "T_after", "status"):
         np.testing.assert_array_equal(outs[0][key], outs[1][key])
+
+
+@pytest.mark.parametrize("name", ["ZHANG", "TEREZA", "KONNOV"])
+def test_other_reference_mechanisms_parity(name):
+    """The reference's other H2/air mechanisms (9/28, 10/24 and 13/71
+    species/reactions, compiled for the thread-per-cell grid kernel) against
+    the oracle in both FP64 modes."""
+    from nrg_b200 import mechanism_paths
+    from nrg_b200.chemistry import ChemicalKineticsSolver
+    from oracle import oracle_py as op
+    paths = mechanism_paths(name)
+    om = op.Mechanism(*paths, 1.0, "cal.mol")
+    W = om.tables()["molar_mass"]
+    names = om.species()[:om.n_species]
+    base = fields.slice_field(fields.config0(fields_W()), 1024)
+    f = fields.state_for_species(base, names, W)
+    o = oracle_run(om, f)
+    s = ChemicalKineticsSolver(None, *paths, mode="reference")
+    try:
+        s.autotune(f.dt, *[x for x in _dev(f)], *_dev_out(f))
+        for mode in ("reference", "fast"):
+            g, st = run_device(s, f, mode)
+            assert st["cells_bad"] == 0, (mode, st)
+            check_parity(g, o, f, np.ones(f.n, bool))
+    finally:
+        s.close()
+
+
+def fields_W():
+    from nrg_b200 import keromnes_paths
+    from nrg_b200.chemistry import mechanism_tables
+    return mechanism_tables(*keromnes_paths())["molar_mass"]
+
+
+def _dev(f):
+    import torch
+    d = torch.device("cuda")
+    return torch.tensor(f.T, device=d), torch.tensor(f.rho, device=d), torch.tensor(f.Y, device=d)
+
+
+def _dev_out(f):
+    import torch
+    d = torch.device("cuda")
+    Y = torch.zeros((f.Y.shape[0], f.n), dtype=torch.float64, device=d)
+    return Y, torch.zeros_like(Y), torch.zeros(f.n, dtype=torch.float64, device=d)

@@ -1,6 +1,7 @@
 """The product's deck reader (libnrg_chem, host only) against the oracle's
 restatement of the reference readers: tables must agree bit for bit."""
 import numpy as np
+import pytest
 
 from nrg_b200 import chemistry
 
@@ -38,3 +39,24 @@ def test_bad_units_rejected(decks):
     import pytest
     with pytest.raises(KeyError):
         chemistry.mechanism_tables(*decks, 1.0, "erg.mol")
+
+
+@pytest.mark.parametrize("name", ["KEROMNES", "ZHANG", "TEREZA", "KONNOV"])
+def test_other_reference_mechanisms_parse_alike(name):
+    """The reference's other H2/air decks: the product reader and the
+    oracle's restatement give the same tables bit for bit."""
+    from nrg_b200 import mechanism_paths
+    from oracle import oracle_py as op
+    paths = mechanism_paths(name)
+    p = chemistry.mechanism_tables(*paths, 1.0, "cal.mol")
+    o = op.Mechanism(*paths, 1.0, "cal.mol").tables()
+    assert p["n_species"] == len(o["species"]) - 1
+    np.testing.assert_array_equal(p["reaction_type"], o["reaction_type"])
+    np.testing.assert_array_equal(p["coeffs"], o["coeffs"])
+    arr = np.stack([o["A"], o["beta"], o["E_act"], o["A_low"], o["beta_low"], o["E_act_low"],
+                    o["troe"][:, 0], o["troe"][:, 1], o["troe"][:, 2]], axis=1)
+    np.testing.assert_array_equal(p["arrhenius"], arr)
+    np.testing.assert_array_equal(p["troe3"], o["troe"][:, 3])
+    np.testing.assert_array_equal(p["eff"], o["eff"])
+    np.testing.assert_array_equal(p["a_coeffs"], o["a_coeffs"])
+    np.testing.assert_array_equal(p["molar_mass"], o["molar_mass"])
