@@ -48,6 +48,10 @@ def parse():
     p.add_argument("--kernel", choices=["thread", "thread_queue", "warp_queue"], default=None,
                    help="fix the integrator launch instead of autotuning it (with --block)")
     p.add_argument("--block", type=int, default=32)
+    p.add_argument("--mechanism", default="KEROMNES", choices=["KEROMNES", "ZHANG", "TEREZA", "KONNOV"],
+                   help="reference H2/air mechanism; the others run the plain FP64 path on the same flame field")
+    p.add_argument("--state-eq", action="store_true",
+                   help="also time the sources + state-equation update of the field (nrg_chem_apply_state_device)")
     return p.parse_args()
 
 
@@ -140,6 +144,35 @@ def algorithmic_flops(st: dict, fm: dict) -> float:
     st = {k: float(v) for k, v in st.items() if not isinstance(v, (list, tuple))}
     return ((st["cells_active"] - st.get("cells_surrogate", 0.0)) * fm["setup"] + st["rhs_evals"] * fm["rhs"] + st["jacobians"] * fm["jac"]
             + st["solves"] * fm["solve"] + st["steps"] * fm["step"])
+
+
+def energy_per_mass(field, tables) -> np.ndarray:
+    """Sensible internal energy per mass above T_ref of each cell (the energy
+    the state equation inverts), from the NASA-7 tables: measurement set-up
+    for --state-eq."""
+    R = 8.31446261815324
+    a = tables["a_coeffs"]  # (N, 2, 7), times R
+    W = tables["molar_mass"]
+    X = field.Y / W[:, None]
+    Wm = 1.0 / X.sum(0)
+    X = X * Wm
+
+    def h(T):
+        t = np.minimum(T, 6000.0)
+        s = (t >= 1000.0).astype(int)
+        out = np.zeros((W.shape[0], T.shape[0]))
+        for k in range(W.shape[0]):
+            c = a[k][s]  # (n, 7)
+            v = c[:, 4] / 5.0
+            for i in (3, 2, 1):
+                v = v * t + c[:, i] / (i + 1.0)
+            v = v * t + c[:, 0]
+            out[k] = (v + c[:, 5] / t) * t
+        return out
+
+    e = ((h(field.T) - R * field.T[None, :]) * X).sum(0)
+    h0 = (h(np.full_like(field.T, 298.15)) * X).sum(0)
+    return (e - h0) / Wm
 
 
 def load_peaks() -> dict:
@@ -250,16 +283,20 @@ def main():
     torch.cuda.set_device(local)
     if world > 1:
         dist.init("nccl", timeout_s=600)
-    from nrg_b200 import fields as F, keromnes_paths
+    from nrg_b200 import fields as F, keromnes_paths, mechanism_paths
     from nrg_b200.chemistry import ChemicalKineticsSolver, DataManager, fp64_peak_tflops, mechanism_tables
     from nrg_b200.surrogate import DEFAULT_MODEL, RECIPE, Surrogate, train_default
-    decks = keromnes_paths()
+    decks = mechanism_paths(args.mechanism)
     tables = mechanism_tables(*decks)
     W = tables["molar_mass"]
-    field = F.config4(W, n_side=args.n_side)
-    n = field.n
     dev = torch.device("cuda", local)
     solver = ChemicalKineticsSolver(None, *decks, mode="fast")
+    field = F.config4(mechanism_tables(*keromnes_paths())["molar_mass"], n_side=args.n_side)
+    if args.mechanism != "KEROMNES":
+        # the same flame, in the mechanism's species (others start at zero)
+        field = F.state_for_species(field, solver.species_names[:tables["n_species"]], W)
+        args.no_e2e = True
+    n = field.n
     T, rho, Y = (torch.tensor(a, device=dev) for a in (field.T, field.rho, field.Y))
 
     # launch shape of the FP64 integrator: autotuned on a contiguous block of
@@ -275,6 +312,8 @@ def main():
     launch = solver.get_launch()
 
     mode = args.mode
+    if args.mechanism != "KEROMNES" and mode == "auto":
+        mode = "fast"
     train_info = None
     if mode in ("auto", "surrogate"):
         sur = Surrogate(solver)
@@ -343,6 +382,40 @@ def main():
                "accepted_cells": int((st_s == 5).sum()), "fallback_cells": int(ph["cells_fallback"]),
                "fallback_fraction_of_active": float(ph["cells_fallback"]) / max(1, int(act.sum()))}
 
+    state_eq = None
+    if args.state_eq:
+        # sources of the last plain step into (Y, E_f), then the state
+        # equation, over the whole field; inputs restored before each call
+        Yp_p, _, Ef_p, _, _ = out_plain
+        E0 = torch.tensor(energy_per_mass(field, tables), device=dev)
+        Yw, Ew, Tw = torch.empty_like(Y), torch.empty_like(E0), torch.empty_like(T)
+        outs = [torch.empty_like(T) for _ in range(7)]
+        stq = torch.empty(n, dtype=torch.uint8, device=dev)
+        times = []
+        for rep in range(args.warmup + args.steps):
+            Yw.copy_(Y)
+            Ew.copy_(E0)
+            Tw.copy_(T)
+            torch.cuda.synchronize()
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a0.record()
+            solver.apply_state_device(rho, Yw, Ew, Tw, outs[0], outs[1], time_step=field.dt, Y_prod=Yp_p,
+                                      E_f_prod=Ef_p, cp_mass=outs[2], h_s=outs[3], h_full=outs[4], v_s=outs[5],
+                                      mix_mol_mass=outs[6], status=stq)
+            a1.record()
+            torch.cuda.synchronize()
+            if rep >= args.warmup:
+                times.append(a0.elapsed_time(a1))
+        ms = statistics.median(times)
+        nsp = int(tables["n_species"])
+        bpc = 8 * (2 * nsp + 5) + 8 * (nsp + 9) + 1  # read rho,Y,E_f,T,Y_prod,E_f_prod; write Y,E_f,T,7 props,status
+        dT = np.abs(Tw.cpu().numpy() - out_plain[3].cpu().numpy())
+        state_eq = {"ms": ms, "cells_per_s": n / (ms * 1e-3), "bytes_per_cell": bpc,
+                    "algorithmic_GB_s": bpc * n / (ms * 1e-3) * 1e-9,
+                    "max_abs_T_minus_step_closure_K": float(dT[out_plain[4].cpu().numpy() != 0].max()),
+                    "what": "nrg_chem_apply_state_device: sources of the plain step into Y, E_f, then the state "
+                            "equation (T Newton, p, gamma, cp, h_s, h_full, sound speed)"}
+
     e2e = None
     if not args.no_e2e:
         nx, ny = field.shape
@@ -404,7 +477,8 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f64+bf16" if mode == "surrogate" else "f64",
             "data": "synthetic",
             "config": {"workload": f"flame field {args.n_side}x{args.n_side} ({n:,} cells), dt=1e-6 s, p=1 atm, "
-                                   f"KEROMNES H2/air (9 species, 24 reactions)",
+                                   f"{args.mechanism} H2/air ({tables['n_species']} species, "
+                                   f"{tables['n_reactions']} reactions)",
                        "path": {"fast": "plain FP64 integrator, analytic Jacobian",
                                 "reference": "plain FP64 integrator, reference FD Jacobian",
                                 "mixed": "FP32 LU + FP64 residual/refinement",
@@ -418,6 +492,7 @@ def main():
             "phases_ms": phases,
             "roofline": roof,
             "roofline_mlp": roof_mlp,
+            "state_equation": state_eq,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": args.steps * launches,
