@@ -176,11 +176,12 @@ NRG_API int nrg_chem_autotune(nrg_chem* h, double time_step, long n, long ld, co
                       double* Y_prod2, double* E_f_prod, double* ms_best);
 
 /* Right-hand side and analytic iteration matrix of the thread-per-cell
- * FP64 and mixed kernels: 1 = straight-line code generated for the KEROMNES
- * reaction structure (nrg_b200/gen_mech.py; registers instead of table walks
- * through shared memory), used by default when the parsed mechanism has
- * exactly that structure; 0 = the table-driven loops.  Both give the same
- * bits.  No counterpart in the reference. */
+ * analytic-Jacobian kernels: 1 = straight-line code generated for the reaction
+ * structure of one of the four reference mechanisms (KEROMNES, ZHANG, TEREZA,
+ * KONNOV; nrg_b200/gen_mech.py; registers instead of table walks through
+ * shared memory), used by default when the parsed mechanism has exactly that
+ * structure; 0 = the table-driven loops.  Both give the same bits.  No
+ * counterpart in the reference. */
 NRG_API int nrg_chem_set_specialised(nrg_chem* h, int enable);
 
 /* Capture the step in a CUDA graph (1) or launch directly (0). */

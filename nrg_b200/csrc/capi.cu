@@ -27,7 +27,7 @@ struct nrg_chem {
   nrg::Mechanism mech;
   DevMech dm;   // tables over all species
   DevMech dmr;  // reaction lists over the reacting species (fast / mixed thread kernels)
-  bool spec = false;  // use the generated mechanism-specialised RHS / iteration matrix
+  int spec = 0;  // generated mechanism-specialised RHS / iteration matrix in use (0: tables)
   int device = 0;
   int num_sms = 148;
   cudaStream_t stream = nullptr;
@@ -436,7 +436,7 @@ extern "C" int nrg_chem_create(const char* mechanism_path, const char* thermo_pa
     return fail(nullptr, NRG_ERR_CUDA, msg);
   }
   reduce_dev_mech(h->dm, &h->dmr);
-  h->spec = nrg::matches_specialised(h->dmr);
+  h->spec = nrg::match_specialised(h->dmr);
   h->sur = nrg::surrogate_create(h->dm);
   if ((ce = use_tables(h)) != cudaSuccess) {
     std::string msg = std::string("mechanism upload failed: ") + cudaGetErrorString(ce);
@@ -481,9 +481,10 @@ extern "C" int nrg_chem_set_mode(nrg_chem* h, int mode) {
 
 extern "C" int nrg_chem_set_specialised(nrg_chem* h, int enable) {
   if (!h) return NRG_ERR_ARG;
-  if (enable && !nrg::matches_specialised(h->dmr))
-    return fail(h, NRG_ERR_UNSUPPORTED, "the mechanism does not match the generated specialised code");
-  h->spec = enable != 0;
+  const int id = nrg::match_specialised(h->dmr);
+  if (enable && id == 0)
+    return fail(h, NRG_ERR_UNSUPPORTED, "the mechanism matches none of the generated specialised codes");
+  h->spec = enable ? id : 0;
   return NRG_OK;
 }
 

@@ -28,7 +28,7 @@
 
 #include "chem_device.cuh"
 #include "chem_kernels.hpp"
-#include "gen_keromnes.cuh"
+#include "gen_mechanisms.cuh"
 
 namespace nrg {
 
@@ -73,15 +73,15 @@ struct SmemStore {
   __device__ __forceinline__ LUT& a(int j, int i) { return f[(j * N + i) * BS]; }  // A(i+1, j+1)
 };
 
-template <int N, int R, typename LUT, int BS, int NF = N, bool SPEC = false>
+template <int N, int R, typename LUT, int BS, int NF = N, int SPEC = 0>
 struct CellState;
 
 // Out-of-line hot routines of the thread-per-cell integrator.  They touch only
 // the cell's shared-memory arrays (passed as the two base pointers), so the
 // register-resident vectors are never forced to local memory by the call.
-template <int N, int R, typename LUT, int BS, bool SPEC>
+template <int N, int R, typename LUT, int BS, int SPEC>
 __device__ __noinline__ void nl_rhs(double* d, LUT* f);
-template <int N, int R, typename LUT, int BS, bool SPEC>
+template <int N, int R, typename LUT, int BS, int SPEC>
 __device__ __noinline__ void nl_analytic_matrix(double* d, LUT* f, double factor);
 template <int N, int R, typename LUT, int BS>
 __device__ __noinline__ unsigned long long nl_dgefa(double* d, LUT* f, int* info);
@@ -90,12 +90,12 @@ __device__ __noinline__ void nl_rate_constants(double* d, LUT* f, double T);
 
 // N integrated species (vectors, Nordsieck rows, LU), NF mechanism species
 // (inputs, outputs, norms' sqrt(NF)); NF - N inert species are not integrated.
-// SPEC: right-hand side and iteration matrix from the generated
-// mechanism-specialised code (gen_keromnes.cuh) instead of the tables.
-template <int N, int R, typename LUT, int BS, int NF, bool SPEC>
+// SPEC: 0 for the table-driven right-hand side and iteration matrix, else
+// the number of the generated mechanism-specialised code (gen_mechanisms.cuh).
+template <int N, int R, typename LUT, int BS, int NF, int SPEC>
 struct CellState : SmemStore<N, R, LUT, BS> {
   static constexpr int kNF = NF;
-  static constexpr bool kSpec = SPEC;
+  static constexpr int kSpec = SPEC;
   double y[N], ywt[N], s1[N], s2[N], fac[N];
   unsigned long long piv;  // ipvt, 4 bits per row
   double h, t, tout, rc, rmax, trend, eps;
@@ -510,27 +510,27 @@ __device__ __forceinline__ void dgesl(CS& c, double (&b)[N]) {
   }
 }
 
-template <int N, int R, typename LUT, int BS, bool SPEC>
+template <int N, int R, typename LUT, int BS, int SPEC>
 __device__ __noinline__ void nl_rhs(double* d, LUT* f) {
   SmemStore<N, R, LUT, BS> s;
   s.d = d;
   s.f = f;
-  if constexpr (SPEC) {
-    static_assert(N == gen::kSpecN && R == gen::kSpecR, "specialised code is for another mechanism size");
-    gen::spec_rhs(s);
+  if constexpr (SPEC != 0) {
+    static_assert(N == SpecOf<SPEC>::kN && R == SpecOf<SPEC>::kR, "specialised code is for another mechanism size");
+    SpecOf<SPEC>::rhs(s);
   } else {
     rhs<N, R>(s);
   }
 }
 
-template <int N, int R, typename LUT, int BS, bool SPEC>
+template <int N, int R, typename LUT, int BS, int SPEC>
 __device__ __noinline__ void nl_analytic_matrix(double* d, LUT* f, double factor) {
   SmemStore<N, R, LUT, BS> s;
   s.d = d;
   s.f = f;
-  if constexpr (SPEC) {
-    static_assert(N == gen::kSpecN && R == gen::kSpecR, "specialised code is for another mechanism size");
-    gen::spec_matrix<SmemStore<N, R, LUT, BS>, LUT>(s, factor);
+  if constexpr (SPEC != 0) {
+    static_assert(N == SpecOf<SPEC>::kN && R == SpecOf<SPEC>::kR, "specialised code is for another mechanism size");
+    SpecOf<SPEC>::template matrix<SmemStore<N, R, LUT, BS>, LUT>(s, factor);
   } else {
     analytic_iteration_matrix<N, R>(s, factor);
   }

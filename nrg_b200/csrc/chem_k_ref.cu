@@ -12,7 +12,7 @@ cudaError_t launch_chem_ref(const StepArgs& a, const LaunchCfg& cfg, int* queue,
   // H2/air mechanisms of the reference's task set-ups: KEROMNES (all shapes),
   // ZHANG, TEREZA, KONNOV (thread-per-cell grid)
   if (n_species == 9 && n_reactions == 24)
-    return launch_variant<9, 9, 24, kJacFD, double, false>(a, cfg, queue, counters, s);
+    return launch_variant<9, 9, 24, kJacFD, double, 0>(a, cfg, queue, counters, s);
   if (n_species == 9 && n_reactions == 28) return launch_grid<9, 9, 28, kJacFD, double>(a, cfg, queue, counters, s);
   if (n_species == 10 && n_reactions == 24)
     return launch_grid<10, 10, 24, kJacFD, double>(a, cfg, queue, counters, s);

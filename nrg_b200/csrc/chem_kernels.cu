@@ -14,9 +14,9 @@ void upload_mechanism_fast(const DevMech& m, cudaStream_t s);
 void upload_mechanism_mixed(const DevMech& m, cudaStream_t s);
 bool supported_mechanism(int n_species, int n_reactions);
 cudaError_t launch_chem_ref(const StepArgs&, const LaunchCfg&, int*, unsigned long long*, cudaStream_t, int, int);
-cudaError_t launch_chem_fast(const StepArgs&, const LaunchCfg&, int*, unsigned long long*, cudaStream_t, int, bool,
+cudaError_t launch_chem_fast(const StepArgs&, const LaunchCfg&, int*, unsigned long long*, cudaStream_t, int, int,
                              int, int);
-cudaError_t launch_chem_mixed(const StepArgs&, const LaunchCfg&, int*, unsigned long long*, cudaStream_t, int, bool,
+cudaError_t launch_chem_mixed(const StepArgs&, const LaunchCfg&, int*, unsigned long long*, cudaStream_t, int, int,
                               int, int);
 
 __global__ void k_fp64_peak(double* out, int iters) {
@@ -153,7 +153,7 @@ void upload_mechanism(const DevMech& full, const DevMech& reduced, cudaStream_t 
   upload_mechanism_mixed(reduced, s);
 }
 
-cudaError_t launch_chem(int n_species, int n_int, bool spec, int n_reactions, int jac, bool mixed,
+cudaError_t launch_chem(int n_species, int n_int, int spec, int n_reactions, int jac, bool mixed,
                         const StepArgs& a, const LaunchCfg& cfg, int* queue, unsigned long long* counters,
                         cudaStream_t s) {
   if (!supported_mechanism(n_species, n_reactions)) return cudaErrorNotSupported;
@@ -167,18 +167,7 @@ bool supported_mechanism(int n_species, int n_reactions) {
          (n_species == 10 && n_reactions == 24) || (n_species == 13 && n_reactions == 71);
 }
 
-bool matches_specialised(const DevMech& reduced) {
-  if (reduced.NI != gen::kSpecN || reduced.R != gen::kSpecR) return false;
-  for (int r = 0; r < reduced.R; ++r) {
-    if (reduced.nupd[r] != gen::kSpecNupd[r]) return false;
-    for (int i = 0; i < 3; ++i)
-      if (reduced.left[r][i] != gen::kSpecLeft[r][i] || reduced.right[r][i] != gen::kSpecRight[r][i]) return false;
-    for (int u = 0; u < reduced.nupd[r]; ++u)
-      if (reduced.upd_k[r][u] != gen::kSpecUpdK[r][u] || reduced.upd_prod[r][u] != gen::kSpecUpdProd[r][u])
-        return false;
-  }
-  return true;
-}
+int match_specialised(const DevMech& reduced) { return match_specialised_tables(reduced); }
 
 int smem_bytes_per_cell(int n_species, int n_reactions, bool mixed) {
   if (n_species == 9 && n_reactions == 24)

@@ -39,7 +39,7 @@ __device__ __forceinline__ void block_flush_counters(unsigned long long* counter
   if (threadIdx.x < kCntSlots && s_cnt[threadIdx.x]) atomicAdd(&counters[threadIdx.x], s_cnt[threadIdx.x]);
 }
 
-template <int N, int R, int JAC, typename LUT, int BS, int NF, bool SPEC>
+template <int N, int R, int JAC, typename LUT, int BS, int NF, int SPEC>
 __global__ void __launch_bounds__(BS, 1) k_chem_plain(StepArgs a, unsigned long long* counters) {
   extern __shared__ __align__(16) char smem[];
   const long li = (long)blockIdx.x * BS + threadIdx.x;
@@ -65,7 +65,7 @@ __global__ void __launch_bounds__(BS, 1) k_chem_plain(StepArgs a, unsigned long 
   if (counters) block_flush_counters(counters, v);
 }
 
-template <int N, int R, int JAC, typename LUT, int BS, int NF, bool SPEC>
+template <int N, int R, int JAC, typename LUT, int BS, int NF, int SPEC>
 __global__ void __launch_bounds__(BS, 1) k_chem_queue(StepArgs a, int* queue, int chunk,
                                                        unsigned long long* counters) {
   extern __shared__ __align__(16) char smem[];
@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(BS, 1) k_chem_queue(StepArgs a, int* queue, in
   if (counters) block_flush_counters(counters, v);
 }
 
-template <int N, int R, int JAC, typename LUT, int BS, int NF, bool SPEC>
+template <int N, int R, int JAC, typename LUT, int BS, int NF, int SPEC>
 static cudaError_t launch_bs(const StepArgs& a, const LaunchCfg& cfg, int* queue,
                              unsigned long long* counters, cudaStream_t s) {
   const size_t smem = (size_t)BS * SmemStore<N, R, LUT, BS>::kBytesPerThread;
@@ -213,9 +213,9 @@ static cudaError_t launch_warp(const StepArgs& a, const LaunchCfg& cfg, int* que
 // waiting for the slowest warp of a larger block.  NF mechanism species, NI of
 // them integrated by the thread-per-cell kernels (the translation unit's
 // tables are numbered over those NI); the warp kernel integrates all NF from
-// the full tables it copies to shared memory.  SPEC: the thread kernels use
-// the generated mechanism-specialised RHS and iteration matrix.
-template <int NF, int NI, int R, int JAC, typename LUT, bool SPEC>
+// the full tables it copies to shared memory.  SPEC != 0: the thread kernels
+// use that generated mechanism-specialised RHS and iteration matrix.
+template <int NF, int NI, int R, int JAC, typename LUT, int SPEC>
 static cudaError_t launch_variant(const StepArgs& a, const LaunchCfg& cfg, int* queue,
                                   unsigned long long* counters, cudaStream_t s) {
   if (cfg.kernel == kKernelWarpQueue) {
@@ -234,13 +234,13 @@ static cudaError_t launch_variant(const StepArgs& a, const LaunchCfg& cfg, int* 
 
 // The thread-per-cell grid kernel only (the shape used for the mechanisms
 // other than the default one, which get no queue / warp variants).
-template <int NF, int NI, int R, int JAC, typename LUT>
+template <int NF, int NI, int R, int JAC, typename LUT, int SPEC = 0>
 static cudaError_t launch_grid(const StepArgs& a, const LaunchCfg& cfg, int* queue, unsigned long long* counters,
                                cudaStream_t s) {
   if (cfg.kernel != kKernelThreadGrid) return cudaErrorNotSupported;
   switch (cfg.block) {
-    case 32: return launch_bs<NI, R, JAC, LUT, 32, NF, false>(a, cfg, queue, counters, s);
-    case 64: return launch_bs<NI, R, JAC, LUT, 64, NF, false>(a, cfg, queue, counters, s);
+    case 32: return launch_bs<NI, R, JAC, LUT, 32, NF, SPEC>(a, cfg, queue, counters, s);
+    case 64: return launch_bs<NI, R, JAC, LUT, 64, NF, SPEC>(a, cfg, queue, counters, s);
     default: return cudaErrorInvalidValue;
   }
 }

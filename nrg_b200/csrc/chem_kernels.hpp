@@ -75,10 +75,10 @@ void upload_mechanism(const DevMech& full, const DevMech& reduced, cudaStream_t 
 // (9, 24; every launch shape), ZHANG (9, 28), TEREZA (10, 24), KONNOV
 // (13, 71) (thread-per-cell grid, reference and analytic-Jacobian modes).
 bool supported_mechanism(int n_species, int n_reactions);
-// True when the reduced reaction lists equal those the generated
-// mechanism-specialised code was written for.
-bool matches_specialised(const DevMech& reduced);
-cudaError_t launch_chem(int n_species, int n_int, bool spec, int n_reactions, int jac, bool mixed, const StepArgs& a,
+// The number (1..) of the generated mechanism-specialised code whose reaction
+// lists equal the reduced ones, 0 when none does.
+int match_specialised(const DevMech& reduced);
+cudaError_t launch_chem(int n_species, int n_int, int spec, int n_reactions, int jac, bool mixed, const StepArgs& a,
                         const LaunchCfg& cfg, int* queue, unsigned long long* counters,
                         cudaStream_t s);
 
