@@ -111,11 +111,12 @@ def config2(W: np.ndarray, n_side: int = 1024, seed: int = 2) -> Field:
     return _finish("config2", T, p, Y, W, 1e-5, (n_side, n_side))
 
 
-def config3_pairs(W: np.ndarray, n: int, seed: int = 3, coupled: float = 0.0) -> Field:
+def config3_pairs(W: np.ndarray, n: int, seed: int = 3, coupled: float = 0.0, T_lo: float = 800.0) -> Field:
     """Training states: the config-2 distribution with dt ~ log-U[1e-7, 1e-5]
-    (radicals shared in a fraction `coupled` of the states)."""
+    (radicals shared in a fraction `coupled` of the states; T_lo < 800 K
+    widens the temperature range down to a flame's preheat zone)."""
     rng = np.random.Generator(np.random.PCG64(seed))
-    T, p, Y = random_state(n, rng, W, 800.0, 2600.0, 0.5, 5.0, coupled)
+    T, p, Y = random_state(n, rng, W, T_lo, 2600.0, 0.5, 5.0, coupled)
     dts = 10.0 ** rng.uniform(-7.0, -5.0, n)
     return _finish("config3", T, p, Y, W, float("nan"), (n,), dts)
 

@@ -148,18 +148,19 @@ class PrepareOpts(ctypes.Structure):
 # a validation flame field (config4 geometry, seed 5) as the widest setting
 # whose accepted cells stay within 0.8 K and 8e-5 of the FP64 result.
 RECIPE = dict(n_train=4_000_000, epochs=60, batch=4096, lr=2e-3, coupled=0.5, hull_margin=0.02, dt_pow=1.0,
-              log_mask=0, log_eps=1e-7, common_dY_scale=0,
+              log_mask=0, log_eps=1e-7, common_dY_scale=0, T_lo=800.0,
               gate=(1e-6, 2e-6, 0.15, 5.0))
 
 
 def training_pairs(solver: ChemicalKineticsSolver, W: np.ndarray, n: int, seed: int = 3,
                    hull_margin: float = RECIPE["hull_margin"], dt_pow: float = RECIPE["dt_pow"],
                    coupled: float = RECIPE["coupled"], log_mask: int = RECIPE["log_mask"],
-                   log_eps: float = RECIPE["log_eps"], common_dY_scale: int = RECIPE["common_dY_scale"]):
+                   log_eps: float = RECIPE["log_eps"], common_dY_scale: int = RECIPE["common_dY_scale"],
+                   T_lo: float = RECIPE["T_lo"]):
     """Integrates n config-3 states with their own dt (FP64 integrator) and
     returns standardised (x_bf16, y) device tensors plus timing."""
     import torch
-    f = fields.config3_pairs(W, n, seed=seed, coupled=coupled)
+    f = fields.config3_pairs(W, n, seed=seed, coupled=coupled, T_lo=T_lo)
     # neighbouring lanes take similar paths when states are sorted by (dt, T)
     order = np.lexsort((f.T, np.round(np.log10(f.dt_cells) * 8)))
     f = fields.Field(f.name, f.T[order], f.rho[order], f.p[order], np.ascontiguousarray(f.Y[:, order]), f.dt,
@@ -190,7 +191,7 @@ def train_default(solver: ChemicalKineticsSolver, W: np.ndarray, seed: int = 0, 
     t0 = time.perf_counter()
     x, y, info = training_pairs(solver, W, r["n_train"], hull_margin=r["hull_margin"], dt_pow=r["dt_pow"],
                                 coupled=r["coupled"], log_mask=r["log_mask"], log_eps=r["log_eps"],
-                                common_dY_scale=r["common_dY_scale"])
+                                common_dY_scale=r["common_dY_scale"], T_lo=r["T_lo"])
     sur.init(seed)
     t1 = time.perf_counter()
     losses = sur.train(x, y, epochs=r["epochs"], batch=r["batch"], lr=r["lr"], seed=seed + 1)
