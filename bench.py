@@ -50,6 +50,9 @@ def parse():
     p.add_argument("--block", type=int, default=32)
     p.add_argument("--mechanism", default="KEROMNES", choices=["KEROMNES", "ZHANG", "TEREZA", "KONNOV"],
                    help="reference H2/air mechanism; the others run the plain FP64 path on the same flame field")
+    p.add_argument("--predictor", action="store_true",
+                   help="also time the low-Mach species predictor on a 2048 x 2048 flame block "
+                        "(nrg_species_predictor_device)")
     p.add_argument("--state-eq", action="store_true",
                    help="also time the sources + state-equation update of the field (nrg_chem_apply_state_device)")
     return p.parse_args()
@@ -272,6 +275,55 @@ def integrator_traffic(cells_integrated: float):
     return None
 
 
+# Algorithmic HBM bytes per interior cell of the species predictor (N species):
+# read rho, Y_k, the two normal face velocities, the diffusion and chemistry
+# sources, bc; write rho_old, Y_old, rho_int, Y_int; the commit reads rho_int,
+# Y_int and writes rho, Y.
+def predictor_bytes_per_cell(N: int, dims: int = 2) -> int:
+    return 8 * (N + 1) + 8 * dims + 8 * 2 * N + 1 + 8 * 2 * (N + 1) + 8 * 2 * (N + 1)
+
+
+def time_predictor(solver, tables, args, dev, peaks) -> dict:
+    """nrg_species_predictor_device on a 2048 x 2048 flame block (ghost layer
+    included), 9 species, dt = 1e-7 s, seeded face velocities of both signs;
+    inputs restored before each call (outside the timed region)."""
+    import torch
+    from nrg_b200 import fields as F
+    N = int(tables["n_species"])
+    W = np.asarray(tables["molar_mass"])
+    b = F.predictor_block(W, 2, (args.n_side, args.n_side), seed=31, bc_fraction=0.0)
+    if N != b.Y.shape[0]:
+        return None
+    t = lambda a: torch.tensor(np.ascontiguousarray(a), device=dev)
+    rho0, Y0 = t(b.rho), t(b.Y)
+    rho, Y = rho0.clone(), Y0.clone()
+    rho_old, Y_old, rho_int, Y_int = (torch.empty_like(x) for x in (rho0, Y0, rho0, Y0))
+    v_f = [t(v) for v in b.v_f]
+    diff, chem = t(b.Y_prod_diff), t(b.Y_prod_chem)
+    times = []
+    for rep in range(args.warmup + args.steps):
+        rho.copy_(rho0)
+        Y.copy_(Y0)
+        torch.cuda.synchronize()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record()
+        solver.species_predictor_device(b.dt, 2, b.n_cells, b.dx, v_f, rho, Y, rho_old, Y_old, rho_int, Y_int,
+                                        Y_prod_diff=diff, Y_prod_chem=chem)
+        a1.record()
+        torch.cuda.synchronize()
+        if rep >= args.warmup:
+            times.append(a0.elapsed_time(a1))
+    ms = statistics.median(times)
+    cells = args.n_side * args.n_side
+    bpc = predictor_bytes_per_cell(N)
+    gbs = bpc * cells / (ms * 1e-3) * 1e-9
+    return {"ms": ms, "cells_per_s": cells / (ms * 1e-3), "bytes_per_cell": bpc, "algorithmic_GB_s": gbs,
+            "frac_of_measured_hbm": gbs / peaks["hbm_gbs"], "launches": 2,
+            "what": "nrg_species_predictor_device (k_predictor + k_predictor_commit): CHARM convective update "
+                    "of rho*Y_k with the EOS correction, diffusion + chemistry sources, clip, renormalise; "
+                    f"{args.n_side} x {args.n_side} cells, 2-D, inputs larger than L2"}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -416,6 +468,10 @@ def main():
                     "what": "nrg_chem_apply_state_device: sources of the plain step into Y, E_f, then the state "
                             "equation (T Newton, p, gamma, cp, h_s, h_full, sound speed)"}
 
+    predictor = None
+    if args.predictor:
+        predictor = time_predictor(solver, tables, args, dev, load_peaks())
+
     e2e = None
     if not args.no_e2e:
         nx, ny = field.shape
@@ -493,6 +549,7 @@ def main():
             "roofline": roof,
             "roofline_mlp": roof_mlp,
             "state_equation": state_eq,
+            "species_predictor": predictor,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": args.steps * launches,

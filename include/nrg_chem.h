@@ -155,6 +155,45 @@ NRG_API int nrg_chem_apply_state_device(nrg_chem* h, double time_step, long n, l
                                         double* p, double* gamma, double* cp_mass, double* h_s, double* h_full,
                                         double* v_s, double* mix_mol_mass, unsigned char* status, void* stream);
 
+/* Block of the low-Mach solver's cell fields on the device, for
+ * nrg_species_predictor_device.  Cell arrays include the ghost layer: extents
+ * e[d] = n[d] + 2 for the dims active directions and 1 for the others, cell
+ * (i, j, k) (0-based, interior 1..n[d] in active directions) at
+ * i + e0 * (j + e1 * k), species s at [s * ld + cell] -- the reference's
+ * cells(0:n+1, 0:n+1, 1:1) arrays (get_local_utter_cells_bounds,
+ * computational_domain_class.f90:497-504) stacked by species. */
+typedef struct {
+  int dims;      /* 1..3 */
+  int n[3];      /* interior cells per active direction */
+  long long ld;  /* species stride of the cell arrays, >= e0 * e1 * e2 */
+  int coord;     /* 0 cartesian, 1 cylindrical (x = r), 2 spherical (x = r) */
+  double dx;     /* cell_size(1): the reference divides every direction's fluxes by it */
+} nrg_grid_desc;
+
+/* Replaces calculate_interm_Y_predictor (fds_low_mach_solver.f90:785-954) on
+ * device arrays: the explicit convective update of rho*Y_k with CHARM-limited
+ * face values and the equation-of-state correction of the most abundant
+ * species (eos_corrected_species_face_vector, :5011-5070), plus dt times the
+ * diffusion, chemistry and particle sources, clipped at zero and
+ * renormalised; for interior cells with bc == 0: rho_old, Y_old = the old
+ * rho, Y; rho_int, Y_int = the new ones (left unchanged where all rho*Y_k
+ * clip to zero, as the reference does); then rho, Y = rho_int, Y_int.  The
+ * mechanism of h supplies the species count and molar masses.  v_f: dims
+ * pointers, v_f[d] the reference's face field of velocity component d,
+ * v_f%pr(d)%cells(1:dims, 0:n+2, ...) in Fortran order (element (c, i, j, k)
+ * at c + dims * (i + f0 * (j + f1 * k)), f[d] = e[d] + 1 for active
+ * directions; face i is the low face of cell i).  x_center: e0 cell-centre x
+ * coordinates (mesh%mesh(1, i, j, k)), needed for coord 1 and 2, else NULL.
+ * bc, Y_prod_diff (diffusion_flag off), Y_prod_chem (reactive_flag off) may
+ * be NULL; n_particle_phases <= 4 source arrays.  Same stream rules as
+ * nrg_chem_step_device. */
+NRG_API int nrg_species_predictor_device(nrg_chem* h, double time_step, const nrg_grid_desc* grid,
+                                         const double* const* v_f, const double* x_center, const signed char* bc,
+                                         const double* Y_prod_diff, const double* Y_prod_chem,
+                                         int n_particle_phases, const double* const* Y_prod_particles, double* rho,
+                                         double* Y, double* rho_old, double* Y_old, double* rho_int, double* Y_int,
+                                         void* stream);
+
 /* Mode (enum nrg_mode).  The reference's ODE_solver selector
  * (chemical_kinetics_solver.f90:91,309-316) has no GPU counterpart for
  * 'table_approximated'. */

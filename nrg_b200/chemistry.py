@@ -47,6 +47,12 @@ class FieldDesc(ctypes.Structure):
     ]
 
 
+class GridDesc(ctypes.Structure):
+    """nrg_grid_desc: a block of the low-Mach solver's cell fields."""
+    _fields_ = [("dims", ctypes.c_int), ("n", ctypes.c_int * 3), ("ld", ctypes.c_longlong),
+                ("coord", ctypes.c_int), ("dx", ctypes.c_double)]
+
+
 class Stats(ctypes.Structure):
     _fields_ = [
         ("cells", ctypes.c_longlong), ("cells_active", ctypes.c_longlong),
@@ -108,6 +114,8 @@ SIGNATURES = {
     "nrg_chem_integrate": (_I, [_VP, _L, _L, _D, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP,
                                 ctypes.POINTER(Stats)]),
     "nrg_fp64_peak_tflops": (_I, [ctypes.POINTER(_D)]),
+    "nrg_species_predictor_device": (_I, [_VP, _D, ctypes.POINTER(GridDesc), _VP, _VP, _VP, _VP, _VP, _I, _VP]
+                                     + [_VP] * 7),
 }
 
 _lib = None
@@ -275,6 +283,24 @@ class ChemicalKineticsSolver:
             self._h, float(time_step), n, Y.shape[1], dims, _ptr(rho), _ptr(Y_prod), _ptr(E_f_prod), _ptr(bc),
             _ptr(Y), _ptr(E_f), _ptr(v), _ptr(T), _ptr(p), _ptr(gamma), _ptr(cp_mass), _ptr(h_s), _ptr(h_full),
             _ptr(v_s), _ptr(mix_mol_mass), _ptr(status),
+            ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)), self._h)
+
+    def species_predictor_device(self, time_step, dims, n_cells, dx, v_f, rho, Y, rho_old, Y_old, rho_int, Y_int,
+                                 coord=0, x_center=None, bc=None, Y_prod_diff=None, Y_prod_chem=None,
+                                 Y_prod_particles=()) -> None:
+        """calculate_interm_Y_predictor on torch CUDA tensors: cell fields
+        flat over the block with its ghost layer (Y-like fields (N, ld)), v_f a
+        list of `dims` face fields in the reference's layout
+        (nrg_species_predictor_device)."""
+        import torch
+        g = GridDesc(int(dims), (ctypes.c_int * 3)(*(list(n_cells) + [1] * (3 - len(n_cells)))), rho.numel(),
+                     int(coord), float(dx))
+        vf = (ctypes.c_void_p * 3)(*([_ptr(v) for v in v_f] + [None] * (3 - len(v_f))))
+        parts = (ctypes.c_void_p * max(1, len(Y_prod_particles)))(*[_ptr(a) for a in Y_prod_particles])
+        _check(lib().nrg_species_predictor_device(
+            self._h, float(time_step), ctypes.byref(g), ctypes.cast(vf, ctypes.c_void_p), _ptr(x_center), _ptr(bc),
+            _ptr(Y_prod_diff), _ptr(Y_prod_chem), len(Y_prod_particles), ctypes.cast(parts, ctypes.c_void_p),
+            _ptr(rho), _ptr(Y), _ptr(rho_old), _ptr(Y_old), _ptr(rho_int), _ptr(Y_int),
             ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)), self._h)
 
     def set_specialised(self, enable: bool) -> None:

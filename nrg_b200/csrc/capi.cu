@@ -16,6 +16,7 @@
 #include "chem_kernels.hpp"
 #include "mechanism.hpp"
 #include "surrogate.hpp"
+#include "transport.hpp"
 
 using nrg::DevMech;
 using nrg::LaunchCfg;
@@ -739,6 +740,50 @@ extern "C" int nrg_chem_apply_state_device(nrg_chem* h, double time_step, long n
   a.status = status;
   const cudaError_t e = nrg::launch_apply_state(h->mech.n(), a, h->stream);
   if (e != cudaSuccess) return cuda_fail(h, e, "state equation launch");
+  CK(h, cudaStreamSynchronize(h->stream));
+  return NRG_OK;
+}
+
+extern "C" int nrg_species_predictor_device(nrg_chem* h, double time_step, const nrg_grid_desc* grid,
+                                            const double* const* v_f, const double* x_center, const signed char* bc,
+                                            const double* Y_prod_diff, const double* Y_prod_chem,
+                                            int n_particle_phases, const double* const* Y_prod_particles,
+                                            double* rho, double* Y, double* rho_old, double* Y_old, double* rho_int,
+                                            double* Y_int, void* stream) {
+  if (!h) return NRG_ERR_ARG;
+  nrg::PredictorArgs a;
+  const int N = h->mech.n();
+  bool ok = grid && N <= nrg::kPredictorMaxSpecies && v_f && rho && Y && rho_old && Y_old && rho_int && Y_int &&
+            n_particle_phases >= 0 && n_particle_phases <= nrg::kPredictorMaxParticlePhases &&
+            (n_particle_phases == 0 || Y_prod_particles) && std::isfinite(time_step) &&
+            nrg::predictor_grid(a, grid->dims, grid->n) && grid->coord >= 0 && grid->coord <= 2 &&
+            (grid->coord == 0 || x_center) && grid->dx > 0.0;
+  if (ok) {
+    for (int d = 0; d < grid->dims; ++d) ok = ok && v_f[d];
+    for (int p = 0; p < n_particle_phases; ++p) ok = ok && Y_prod_particles[p];
+    ok = ok && grid->ld >= a.e[0] * a.e[1] * a.e[2];
+  }
+  if (!ok) return fail(h, NRG_ERR_ARG, "bad arguments to nrg_species_predictor_device");
+  a.coord = grid->coord;
+  a.ld = (long)grid->ld;
+  a.dx = grid->dx;
+  a.inv_dx = 1.0 / grid->dx;
+  a.dt = time_step;
+  for (int s = 0; s < N; ++s) a.W[s] = h->dm.W[s];
+  a.rho = rho; a.Y = Y;
+  for (int d = 0; d < grid->dims; ++d) a.v_f[d] = v_f[d];
+  a.x_center = x_center; a.bc = (const int8_t*)bc;
+  a.Y_prod_diff = Y_prod_diff; a.Y_prod_chem = Y_prod_chem;
+  a.n_part = n_particle_phases;
+  for (int p = 0; p < n_particle_phases; ++p) a.Y_prod_part[p] = Y_prod_particles[p];
+  a.rho_old = rho_old; a.Y_old = Y_old; a.rho_int = rho_int; a.Y_int = Y_int;
+  a.rho_out = rho; a.Y_out = Y;
+  CK(h, cudaSetDevice(h->device));
+  CK(h, cudaEventRecord(h->ev_in, (cudaStream_t)stream));
+  CK(h, cudaStreamWaitEvent(h->stream, h->ev_in, 0));
+  const cudaError_t e = nrg::launch_species_predictor(N, a, h->stream);
+  if (e == cudaErrorNotSupported) return fail(h, NRG_ERR_UNSUPPORTED, "no species predictor for this species count");
+  if (e != cudaSuccess) return cuda_fail(h, e, "species predictor launch");
   CK(h, cudaStreamSynchronize(h->stream));
   return NRG_OK;
 }

@@ -167,3 +167,65 @@ def state_for_species(f: Field, names, W: np.ndarray) -> Field:
         if nm in idx:
             Y[k] = f.Y[idx[nm]]
     return _finish(f.name, f.T.copy(), f.p.copy(), Y, W, f.dt, f.shape, f.dt_cells)
+
+
+@dataclass
+class PredictorBlock:
+    """Cell and face fields of one block of the low-Mach solver, flat with the
+    ghost layer (layout of nrg_grid_desc / nrg_species_predictor_device)."""
+    dims: int
+    n_cells: tuple
+    dx: float
+    dt: float
+    coord: int
+    rho: np.ndarray          # (ld,)
+    Y: np.ndarray            # (N, ld)
+    v_f: list                # dims face fields, each (dims * f0 * f1 * f2,)
+    x_center: np.ndarray     # (e0,)
+    bc: np.ndarray           # (ld,) int8
+    Y_prod_diff: np.ndarray  # (N, ld)
+    Y_prod_chem: np.ndarray  # (N, ld)
+
+    @property
+    def ld(self) -> int:
+        return self.rho.shape[0]
+
+
+def predictor_block(W: np.ndarray, dims: int, n_cells, seed: int = 0, coord: int = 0, dx: float = 10e-6,
+                    dt: float = 1e-7, bc_fraction: float = 0.02, zero_face_fraction: float = 0.05) -> PredictorBlock:
+    """A flame front along x (as the config-4 field: tanh profile from 300 K
+    to 2400 K, radicals Gaussian at the front) on a block with its ghost
+    layer, plus seeded face velocities of both signs (some exactly zero),
+    diffusion and chemistry sources of the size the step produces, and a few
+    cells with bc /= 0."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    n = list(n_cells) + [1] * (3 - len(n_cells))
+    e = [n[d] + 2 if d < dims else 1 for d in range(3)]
+    f = [e[d] + 1 if d < dims else 1 for d in range(3)]
+    ld = e[0] * e[1] * e[2]
+    i = np.arange(ld) % e[0]
+    j = (np.arange(ld) // e[0]) % e[1]
+    k = np.arange(ld) // (e[0] * e[1])
+    x = (i - 0.5) * dx
+    xf = 0.5 * n[0] * dx + 0.15 * n[0] * dx * np.sin(2.0 * np.pi * (j + 0.5 * k) / max(e[1], 4))
+    s = (x - xf) / (0.1 * n[0] * dx)
+    c = 0.5 * (1.0 + np.tanh(s))
+    T = 300.0 + 2100.0 * c
+    Yr, Yp, idx = _stoich(W)
+    Y = (1.0 - c)[None, :] * Yr[:, None] + c[None, :] * Yp[:, None]
+    g = np.exp(-0.5 * s ** 2)
+    for sp in RADICALS:
+        Y[idx[sp]] = 1e-3 * g * rng.uniform(0.5, 1.5, ld)
+    fl = _finish("predictor", T, np.full(ld, P_ATM), Y, W, dt, (ld,))
+    v_f = []
+    for d in range(dims):
+        v = rng.uniform(-6.0, 10.0, dims * f[0] * f[1] * f[2])
+        v[rng.uniform(0.0, 1.0, v.shape[0]) < zero_face_fraction] = 0.0
+        v_f.append(v)
+    x_center = (np.arange(e[0]) - 0.5) * dx + (20.0 * dx if coord else 0.0)
+    bc = (rng.uniform(0.0, 1.0, ld) < bc_fraction).astype(np.int8)
+    N = W.shape[0]
+    Y_prod_diff = rng.normal(0.0, 50.0, (N, ld))
+    Y_prod_chem = rng.normal(0.0, 200.0, (N, ld)) * g[None, :]
+    return PredictorBlock(dims, tuple(n[:dims]), dx, dt, coord, fl.rho, np.ascontiguousarray(fl.Y), v_f, x_center,
+                          bc, Y_prod_diff, Y_prod_chem)

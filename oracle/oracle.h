@@ -106,6 +106,13 @@ int orc_apply_state(const orc_mech *m, long n, int dims, double dt, const double
                     double *gamma, double *cp_mass, double *h_s, double *h_full, double *v_s,
                     double *mix_mol_mass, unsigned char *status, int n_threads);
 
+/* Species predictor of the low-Mach solver (orc_transport.c; layout there). */
+int orc_species_predictor(int N, const double *W, int dims, const int n_cells[3], long ld, int coord, double dx,
+                          double dt, const double *const v_f[3], const double *x_center, const signed char *bc,
+                          const double *Y_prod_diff, const double *Y_prod_chem, int n_part,
+                          const double *const *Y_prod_part, double *rho, double *Y, double *rho_old,
+                          double *Y_old, double *rho_int, double *Y_int);
+
 #ifdef __cplusplus
 }
 #endif

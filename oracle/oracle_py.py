@@ -73,6 +73,11 @@ def lib():
                                       ctypes.c_void_p, dp, dp, dp, dp, dp, dp, dp, dp, ctypes.c_void_p,
                                       ctypes.c_int]
         L.orc_apply_state.restype = ctypes.c_int
+        L.orc_species_predictor.argtypes = [ctypes.c_int, dp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                            ctypes.c_long, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                            ctypes.c_void_p * 3] + [ctypes.c_void_p] * 4 + [
+                                            ctypes.c_int, ctypes.c_void_p] + [dp] * 6
+        L.orc_species_predictor.restype = ctypes.c_int
         L.orc_rate_constants.argtypes = [ctypes.POINTER(OrcMech), ctypes.c_double, dp, dp, dp]
         L.orc_rate_constants.restype = None
         L.orc_rhs.argtypes = [ctypes.POINTER(OrcMech), dp, dp, dp, dp, dp]
@@ -222,3 +227,38 @@ def ddcst(maxord=5):
     tq = np.zeros(3 * 12)
     lib().orc_ddcst(maxord, _dp(el), _dp(tq))
     return el.reshape(12, 13).T, tq.reshape(12, 3).T
+
+
+def species_predictor(W, dims, n_cells, coord, dx, dt, v_f, rho, Y, rho_int, Y_int, x_center=None, bc=None,
+                      Y_prod_diff=None, Y_prod_chem=None, Y_prod_part=(), rho_old=None, Y_old=None):
+    """The low-Mach species predictor (orc_species_predictor) on copies of
+    the cell fields.  Cell fields are flat (ld,) or (N, ld) arrays in the
+    layout of orc_transport.c; v_f is a list of `dims` face fields.  Returns
+    dict(rho, Y, rho_old, Y_old, rho_int, Y_int)."""
+    W = np.ascontiguousarray(W, dtype=np.float64)
+    N = W.shape[0]
+    ld = rho.shape[0]
+    c = lambda a: np.array(a, dtype=np.float64, copy=True)
+    out = dict(rho=c(rho), Y=c(Y).reshape(N, ld), rho_int=c(rho_int), Y_int=c(Y_int).reshape(N, ld),
+               rho_old=np.zeros(ld) if rho_old is None else c(rho_old),
+               Y_old=np.zeros((N, ld)) if Y_old is None else c(Y_old).reshape(N, ld))
+    keep = []
+
+    def vp(a, dtype=np.float64):
+        if a is None:
+            return None
+        a = np.ascontiguousarray(a, dtype=dtype)
+        keep.append(a)
+        return a.ctypes.data_as(ctypes.c_void_p)
+
+    vf = (ctypes.c_void_p * 3)(*([vp(v) for v in v_f] + [None] * (3 - len(v_f))))
+    parts = (ctypes.c_void_p * max(1, len(Y_prod_part)))(*[vp(a) for a in Y_prod_part])
+    nc = (ctypes.c_int * 3)(*(list(n_cells) + [1] * (3 - len(n_cells))))
+    rc = lib().orc_species_predictor(N, _dp(W), int(dims), nc, ld, int(coord), float(dx), float(dt), vf,
+                                     vp(x_center), vp(bc, np.int8), vp(Y_prod_diff), vp(Y_prod_chem),
+                                     len(Y_prod_part), ctypes.cast(parts, ctypes.c_void_p),
+                                     _dp(out["rho"]), _dp(out["Y"]), _dp(out["rho_old"]), _dp(out["Y_old"]),
+                                     _dp(out["rho_int"]), _dp(out["Y_int"]))
+    if rc != 0:
+        raise ValueError(f"orc_species_predictor: bad arguments ({rc})")
+    return out
