@@ -50,11 +50,12 @@ def parse():
     p.add_argument("--block", type=int, default=32)
     p.add_argument("--mechanism", default="KEROMNES", choices=["KEROMNES", "ZHANG", "TEREZA", "KONNOV"],
                    help="reference H2/air mechanism; the others run the plain FP64 path on the same flame field")
-    p.add_argument("--predictor", action="store_true",
-                   help="also time the low-Mach species predictor on a 2048 x 2048 flame block "
+    p.add_argument("--no-predictor", dest="predictor", action="store_false",
+                   help="skip timing the low-Mach species predictor on an n-side x n-side flame block "
                         "(nrg_species_predictor_device)")
-    p.add_argument("--state-eq", action="store_true",
-                   help="also time the sources + state-equation update of the field (nrg_chem_apply_state_device)")
+    p.add_argument("--no-state-eq", dest="state_eq", action="store_false",
+                   help="skip timing the sources + state-equation update of the field "
+                        "(nrg_chem_apply_state_device)")
     return p.parse_args()
 
 

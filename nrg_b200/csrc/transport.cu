@@ -31,25 +31,21 @@ namespace {
 
 constexpr int kTX = 32;
 
+// charm_face_value without branches: both candidates are formed from safe
+// operands and the reference's choice selects one, so the selected value has
+// the reference's bits and the N + 1 face values of a face can overlap.
 __device__ __forceinline__ double charm(double a0, double a1, double a2, double a3, double v) {
-  double phi_up, B_r, r;
+  const bool pos = v > 0.0;
   const double phi_loc = a2 - a1;
-  if (v > 0.0)
-    phi_up = a1 - a0;
-  else
-    phi_up = a3 - a2;
-  if (phi_loc != 0.0)
-    r = phi_up / phi_loc;
-  else
-    r = 0.0;
-  if (r > 1.0e-10) {
-    const double s = 1.0 / r;
-    B_r = s * (3.0 * s + 1.0) / (s + 1.0) / (s + 1.0);
-  } else {
-    B_r = 0.0;
-  }
-  if (v > 0.0) return a1 + B_r * 0.5 * phi_up;
-  return a2 - B_r * 0.5 * phi_up;
+  const double up_pos = a1 - a0, up_neg = a3 - a2;
+  const double phi_up = pos ? up_pos : up_neg;
+  const bool has_loc = phi_loc != 0.0;
+  const double r = has_loc ? phi_up / (has_loc ? phi_loc : 1.0) : 0.0;
+  const bool lim = r > 1.0e-10;
+  const double s = 1.0 / (lim ? r : 1.0);
+  const double B_r = lim ? s * (3.0 * s + 1.0) / (s + 1.0) / (s + 1.0) : 0.0;
+  const double h = B_r * 0.5 * phi_up;
+  return pos ? a1 + h : a2 - h;
 }
 
 // Per staged cell: rho*Y_k, sum_k rho*Y_k / W_k (species order, from 0.0) and
@@ -80,10 +76,12 @@ __device__ __forceinline__ void charm_face_flux(const double* W, RY at, ROW row_
 #pragma unroll
   for (int s = 0; s < N; ++s) phi[s] = charm(at(0, s), at(1, s), at(2, s), at(3, s), v);
   const double row_face = charm(row_at(0), row_at(1), row_at(2), row_at(3), v);
+  double q[N];
+#pragma unroll
+  for (int s = 0; s < N; ++s) q[s] = phi[s] / W[s];
   double sum_not_gamma = 0.0;
 #pragma unroll
-  for (int s = 0; s < N; ++s)
-    if (s != gam) sum_not_gamma = sum_not_gamma + phi[s] / W[s];
+  for (int s = 0; s < N; ++s) sum_not_gamma = s != gam ? sum_not_gamma + q[s] : sum_not_gamma;
   double pg = 0.0;
 #pragma unroll
   for (int s = 0; s < N; ++s)
@@ -94,8 +92,8 @@ __device__ __forceinline__ void charm_face_flux(const double* W, RY at, ROW row_
 
 }  // namespace
 
-template <int N>
-__global__ void __launch_bounds__(256) k_predictor(PredictorArgs a) {
+template <int N, bool Z3>
+__global__ void __launch_bounds__(256, Z3 ? 1 : (N == 9 ? 3 : 2)) k_predictor(PredictorArgs a) {
   extern __shared__ double sm[];
   const int TY = blockDim.y;
   const bool two_d = a.dims >= 2;
@@ -129,46 +127,35 @@ __global__ void __launch_bounds__(256) k_predictor(PredictorArgs a) {
   }
   __syncthreads();
 
-  // x faces: face fi is the low face of cell i0 + fi, between staged columns fi + 1 and fi + 2
+  // faces, x then y in one job list: x face (fi, fj) is the low face of
+  // cell (i0 + fi, j0 + fj), its four stencil cells are staged columns
+  // fi .. fi + 3 of row fj + 2; y faces likewise along the rows
   const long f0 = a.f[0], f1 = a.f[1];
-  for (int q = tid; q < (kTX + 1) * TY; q += nthr) {
-    const int fi = q % (kTX + 1), fj = q / (kTX + 1);
+  const int nxf = (kTX + 1) * TY, nyf = two_d ? kTX * (TY + 1) : 0;
+  for (int q = tid; q < nxf + nyf; q += nthr) {
+    const bool xf = q < nxf;
+    const int r = xf ? q : q - nxf;
+    const int fi = xf ? r % (kTX + 1) : r % kTX, fj = xf ? r / (kTX + 1) : r / kTX;
     const long i = i0 + fi, j = j0 + fj;
-    if (i > a.hi[0] + 1 || j > a.hi[1]) continue;
-    const double v = a.v_f[0][a.dims * (i + f0 * (j + f1 * k))];
-    const int rowq = (two_d ? fj + 2 : 0) * RX;
+    if (xf ? (i > a.hi[0] + 1 || j > a.hi[1]) : (i > a.hi[0] || j > a.hi[1] + 1)) continue;
+    const int d = xf ? 0 : 1;
+    const double v = a.v_f[d][d + a.dims * (i + f0 * (j + f1 * k))];
+    const bool edge = xf ? (i == a.lo[0] || i == a.hi[0] + 1) : (j == a.lo[1] || j == a.hi[1] + 1);
+    const int st = xf ? 1 : RX;
+    const int b = xf ? (two_d ? fj + 2 : 0) * RX + fi : fj * RX + fi + 2;
+    double* out = xf ? s_fx + fj * (kTX + 1) + fi : s_fy + fj * kTX + fi;
+    const int ostride = xf ? TY * (kTX + 1) : (TY + 1) * kTX;
     double F[N];
-    if (i == a.lo[0] || i == a.hi[0] + 1) {
-      const int up = rowq + (v > 0.0 ? fi + 1 : fi + 2);
+    if (edge) {
+      const int up = b + (v > 0.0 ? 1 : 2) * st;
 #pragma unroll
       for (int s = 0; s < N; ++s) F[s] = s_rY[s * nst + up] * v;
     } else {
-      const int b = rowq + fi;
-      charm_face_flux<N>(a.W, [&](int n, int s) { return s_rY[s * nst + b + n]; }, [&](int n) { return s_row[b + n]; },
-                         s_gam[b + (v > 0.0 ? 1 : 2)], v, F);
+      charm_face_flux<N>(a.W, [&](int n, int s) { return s_rY[s * nst + b + n * st]; },
+                         [&](int n) { return s_row[b + n * st]; }, s_gam[b + (v > 0.0 ? 1 : 2) * st], v, F);
     }
 #pragma unroll
-    for (int s = 0; s < N; ++s) s_fx[(s * TY + fj) * (kTX + 1) + fi] = F[s];
-  }
-  if (two_d) {
-    for (int q = tid; q < kTX * (TY + 1); q += nthr) {
-      const int fi = q % kTX, fj = q / kTX;
-      const long i = i0 + fi, j = j0 + fj;
-      if (i > a.hi[0] || j > a.hi[1] + 1) continue;
-      const double v = a.v_f[1][1 + a.dims * (i + f0 * (j + f1 * k))];
-      double F[N];
-      if (j == a.lo[1] || j == a.hi[1] + 1) {
-        const int up = (v > 0.0 ? fj + 1 : fj + 2) * RX + fi + 2;
-#pragma unroll
-        for (int s = 0; s < N; ++s) F[s] = s_rY[s * nst + up] * v;
-      } else {
-        const int b = fj * RX + fi + 2;
-        charm_face_flux<N>(a.W, [&](int n, int s) { return s_rY[s * nst + b + n * RX]; },
-                           [&](int n) { return s_row[b + n * RX]; }, s_gam[b + (v > 0.0 ? 1 : 2) * RX], v, F);
-      }
-#pragma unroll
-      for (int s = 0; s < N; ++s) s_fy[(s * (TY + 1) + fj) * kTX + fi] = F[s];
-    }
+    for (int s = 0; s < N; ++s) out[s * ostride] = F[s];
   }
   __syncthreads();
 
@@ -205,7 +192,7 @@ __global__ void __launch_bounds__(256) k_predictor(PredictorArgs a) {
       rhs[s] = rhs[s] - (fr * 1.0 - fl * 1.0) * a.inv_dx;
     }
   }
-  if (a.dims == 3) {
+  if (Z3) {
     // z faces from global memory: low face kf = k (cells k-1 | k), high face kf = k + 1
     const long pz = e0 * e1;
     double Fz[2][N];
@@ -299,12 +286,14 @@ static cudaError_t launch_n(const PredictorArgs& a, cudaStream_t s) {
   const int RX = 32 + 4, RY = two_d ? TY + 4 : 1, nst = RX * RY;
   const size_t doubles = (size_t)N * nst + nst + (size_t)N * TY * 33 + (two_d ? (size_t)N * (TY + 1) * 32 : 0);
   const size_t smem = doubles * sizeof(double) + (size_t)nst * sizeof(int);
-  cudaError_t e = cudaFuncSetAttribute(k_predictor<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  auto kern = a.dims == 3 ? k_predictor<N, true> : k_predictor<N, false>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   if (e != cudaSuccess) return e;
   const long nx = a.hi[0] - a.lo[0] + 1, ny = a.hi[1] - a.lo[1] + 1, nz = a.hi[2] - a.lo[2] + 1;
   const dim3 grid((unsigned)((nx + 31) / 32), (unsigned)((ny + TY - 1) / TY), (unsigned)nz);
   if (grid.y > 65535u || grid.z > 65535u) return cudaErrorInvalidValue;
-  k_predictor<N><<<grid, dim3(32, TY), smem, s>>>(a);
+  kern<<<grid, dim3(32, TY), smem, s>>>(a);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   int dev = 0, sms = 148;
