@@ -53,6 +53,9 @@ def parse():
     p.add_argument("--no-predictor", dest="predictor", action="store_false",
                    help="skip timing the low-Mach species predictor on an n-side x n-side flame block "
                         "(nrg_species_predictor_device)")
+    p.add_argument("--no-diffusivity", dest="diffusivity", action="store_false",
+                   help="skip timing the mixture-averaged diffusion coefficients of the field "
+                        "(nrg_mixture_diffusivity_device)")
     p.add_argument("--no-state-eq", dest="state_eq", action="store_false",
                    help="skip timing the sources + state-equation update of the field "
                         "(nrg_chem_apply_state_device)")
@@ -325,6 +328,37 @@ def time_predictor(solver, tables, args, dev, peaks) -> dict:
                     f"{args.n_side} x {args.n_side} cells, 2-D, inputs larger than L2"}
 
 
+def time_diffusivity(solver, tables, args, dev, field, T, Y) -> dict:
+    """nrg_mixture_diffusivity_device over the flame field (the mechanism's
+    transport deck; mixture molar mass from Y)."""
+    import torch
+    from nrg_b200 import transport_path
+    solver.load_transport(transport_path(args.mechanism))
+    W = np.asarray(tables["molar_mass"])
+    N = int(tables["n_species"])
+    mm = torch.tensor(1.0 / np.sum(field.Y / W[:, None], axis=0), device=dev)
+    p = torch.tensor(field.p, device=dev)
+    D = torch.empty_like(Y)
+    times = []
+    for rep in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record()
+        solver.mixture_diffusivity_device(T, p, Y, mm, D)
+        a1.record()
+        torch.cuda.synchronize()
+        if rep >= args.warmup:
+            times.append(a0.elapsed_time(a1))
+    ms = statistics.median(times)
+    n = field.n
+    bpc = 8 * (N + 3) + 8 * N  # read T, p, mix_mol_mass, Y; write D
+    return {"ms": ms, "cells_per_s": n / (ms * 1e-3), "bytes_per_cell": bpc,
+            "algorithmic_GB_s": bpc * n / (ms * 1e-3) * 1e-9, "pairs_per_cell": N * (N - 1) // 2,
+            "what": "nrg_mixture_diffusivity_device: Chapman-Enskog binary coefficients (Neufeld collision "
+                    "integral: one pow and three exp per species pair) and the mixture-averaged coefficient "
+                    "of every species, every cell of the field"}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -473,6 +507,10 @@ def main():
     if args.predictor:
         predictor = time_predictor(solver, tables, args, dev, load_peaks())
 
+    diffusivity = None
+    if args.diffusivity:
+        diffusivity = time_diffusivity(solver, tables, args, dev, field, T, Y)
+
     e2e = None
     if not args.no_e2e:
         nx, ny = field.shape
@@ -551,6 +589,7 @@ def main():
             "roofline_mlp": roof_mlp,
             "state_equation": state_eq,
             "species_predictor": predictor,
+            "mixture_diffusivity": diffusivity,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": args.steps * launches,

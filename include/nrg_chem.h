@@ -194,6 +194,34 @@ NRG_API int nrg_species_predictor_device(nrg_chem* h, double time_step, const nr
                                          double* Y, double* rho_old, double* Y_old, double* rho_int, double* Y_int,
                                          void* stream);
 
+/* Reads the transport deck (thermophysical_properties%set_properties
+ * transport part, thermophysical_properties_class.f90:163-171, 1343-1414):
+ * Lennard-Jones well depth and collision diameter of every mechanism species
+ * (e.g. KEROMNES_TRANSDATA.txt) and the binary diffusivity constants.
+ * NRG_ERR_IO when a species is missing (the reference stops the program). */
+NRG_API int nrg_chem_load_transport(nrg_chem* h, const char* transport_path);
+
+/* Host-only parse (no CUDA call) of the three decks plus the transport deck:
+ * n_species well depths [K], collision diameters [nm] and the n_species x
+ * n_species binary diffusivity constants (row-major, symmetric), as
+ * nrg_chem_load_transport builds them.  Any output pointer may be NULL.  No
+ * counterpart in the reference. */
+NRG_API int nrg_mech_transport_tables(const char* mechanism_path, const char* thermo_path,
+                                      const char* molar_masses_path, const char* transport_path,
+                                      double* well_depth, double* collision_diameter, double* binary_diffusivity);
+
+/* Replaces calculate_diffusivity_coeff (fickean_diffusion_solver.f90:358-395)
+ * on device arrays: the mixture-averaged diffusion coefficient of every
+ * species (mixture_averaged_diffusion_coefficients,
+ * thermophysical_properties_class.f90:768-814, with the Chapman-Enskog binary
+ * coefficients of :737-762 and the Neufeld collision integral of :560-577) in
+ * each of n cells; D = 0 where bc /= 0 (bc may be NULL).  Y and D
+ * species-major at [k * ld + c]; mix_mol_mass as written by
+ * nrg_chem_apply_state_device.  Needs nrg_chem_load_transport. */
+NRG_API int nrg_mixture_diffusivity_device(nrg_chem* h, long n, long ld, const double* T, const double* p,
+                                           const double* Y, const double* mix_mol_mass, const signed char* bc,
+                                           double* D, void* stream);
+
 /* Mode (enum nrg_mode).  The reference's ODE_solver selector
  * (chemical_kinetics_solver.f90:91,309-316) has no GPU counterpart for
  * 'table_approximated'. */

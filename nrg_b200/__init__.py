@@ -24,3 +24,11 @@ def mechanism_paths(name: str = "KEROMNES"):
 def keromnes_paths():
     """The reference's H2/air input decks (mechanism, thermo, molar masses)."""
     return mechanism_paths("KEROMNES")
+
+
+def transport_path(name: str = "KEROMNES"):
+    """The mechanism's transport deck (Lennard-Jones parameters), as in the
+    reference's task_setup/thermophysical_data directory."""
+    if name not in MECHANISMS:
+        raise ValueError(f"unknown mechanism {name!r}; have {MECHANISMS}")
+    return os.path.join(MECH_DIR, f"{name}_TRANSDATA.txt")

@@ -27,6 +27,7 @@ SOURCES = {
     "capi.cu": [],
     "surrogate.cu": [],
     "transport.cu": ["--fmad=false"],  # species predictor in the reference's operation order
+    "diffusion.cu": ["--fmad=false"],
     "mechanism.cpp": [],
 }
 

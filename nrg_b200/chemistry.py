@@ -114,6 +114,9 @@ SIGNATURES = {
     "nrg_chem_integrate": (_I, [_VP, _L, _L, _D, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP,
                                 ctypes.POINTER(Stats)]),
     "nrg_fp64_peak_tflops": (_I, [ctypes.POINTER(_D)]),
+    "nrg_chem_load_transport": (_I, [_VP, _CP]),
+    "nrg_mech_transport_tables": (_I, [_CP] * 4 + [_VP] * 3),
+    "nrg_mixture_diffusivity_device": (_I, [_VP, _L, _L] + [_VP] * 7),
     "nrg_species_predictor_device": (_I, [_VP, _D, ctypes.POINTER(GridDesc), _VP, _VP, _VP, _VP, _VP, _I, _VP]
                                      + [_VP] * 7),
 }
@@ -167,6 +170,18 @@ def mechanism_tables(mechanism, thermo, molar_masses, default_enhanced_efficienc
                                                     "eff", "a_coeffs", "molar_mass")]))
     t["n_species"], t["n_reactions"] = N, R
     return t
+
+
+def transport_tables(mechanism, thermo, molar_masses, transport) -> dict:
+    """Transport deck of the mechanism's species as the library reads it
+    (host only, no GPU): well depths, collision diameters [nm], binary
+    diffusivity constants."""
+    N = mechanism_tables(mechanism, thermo, molar_masses)["n_species"]
+    eps, sg, bdc = np.zeros(N), np.zeros(N), np.zeros((N, N))
+    _check(lib().nrg_mech_transport_tables(str(mechanism).encode(), str(thermo).encode(),
+                                           str(molar_masses).encode(), str(transport).encode(),
+                                           _ptr(eps), _ptr(sg), _ptr(bdc)))
+    return {"well_depth": eps, "collision_diameter": sg, "binary_diffusivity_constant": bdc}
 
 
 @dataclass
@@ -301,6 +316,17 @@ class ChemicalKineticsSolver:
             self._h, float(time_step), ctypes.byref(g), ctypes.cast(vf, ctypes.c_void_p), _ptr(x_center), _ptr(bc),
             _ptr(Y_prod_diff), _ptr(Y_prod_chem), len(Y_prod_particles), ctypes.cast(parts, ctypes.c_void_p),
             _ptr(rho), _ptr(Y), _ptr(rho_old), _ptr(Y_old), _ptr(rho_int), _ptr(Y_int),
+            ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)), self._h)
+
+    def load_transport(self, transport_path: str) -> None:
+        """Transport deck of the mechanism's species (nrg_chem_load_transport)."""
+        _check(lib().nrg_chem_load_transport(self._h, transport_path.encode()), self._h)
+
+    def mixture_diffusivity_device(self, T, p, Y, mix_mol_mass, D, bc=None) -> None:
+        """calculate_diffusivity_coeff on torch CUDA tensors (Y, D: (N, n))."""
+        import torch
+        _check(lib().nrg_mixture_diffusivity_device(
+            self._h, T.numel(), Y.shape[1], _ptr(T), _ptr(p), _ptr(Y), _ptr(mix_mol_mass), _ptr(bc), _ptr(D),
             ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)), self._h)
 
     def set_specialised(self, enable: bool) -> None:

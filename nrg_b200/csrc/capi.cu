@@ -17,6 +17,7 @@
 #include "mechanism.hpp"
 #include "surrogate.hpp"
 #include "transport.hpp"
+#include "diffusion.hpp"
 
 using nrg::DevMech;
 using nrg::LaunchCfg;
@@ -29,6 +30,8 @@ struct nrg_chem {
   DevMech dm;   // tables over all species
   DevMech dmr;  // reaction lists over the reacting species (fast / mixed thread kernels)
   int spec = 0;  // generated mechanism-specialised RHS / iteration matrix in use (0: tables)
+  bool has_transport = false;
+  nrg::DiffusivityArgs diff;  // pair tables of the loaded transport deck
   int device = 0;
   int num_sms = 148;
   cudaStream_t stream = nullptr;
@@ -784,6 +787,71 @@ extern "C" int nrg_species_predictor_device(nrg_chem* h, double time_step, const
   const cudaError_t e = nrg::launch_species_predictor(N, a, h->stream);
   if (e == cudaErrorNotSupported) return fail(h, NRG_ERR_UNSUPPORTED, "no species predictor for this species count");
   if (e != cudaSuccess) return cuda_fail(h, e, "species predictor launch");
+  CK(h, cudaStreamSynchronize(h->stream));
+  return NRG_OK;
+}
+
+extern "C" int nrg_chem_load_transport(nrg_chem* h, const char* transport_path) {
+  if (!h || !transport_path) return NRG_ERR_ARG;
+  const int N = h->mech.n();
+  if (N > nrg::kDiffMaxSpecies) return fail(h, NRG_ERR_UNSUPPORTED, "too many species for the diffusivity kernel");
+  const std::string e = nrg::load_transport(transport_path, &h->mech);
+  if (!e.empty()) return fail(h, NRG_ERR_IO, e);
+  nrg::DiffusivityArgs& d = h->diff;
+  d = nrg::DiffusivityArgs();
+  d.N = N;
+  for (int k = 0; k < N; ++k) d.W[k] = h->mech.molar_mass[k];
+  int q = 0;
+  for (int i = 0; i < N - 1; ++i)
+    for (int j = i + 1; j < N; ++j, ++q) {
+      const double eps_i = h->mech.well_depth[i], eps_j = h->mech.well_depth[j];
+      d.bdc[q] = h->mech.binary_diffusivity[(size_t)i * N + j];
+      d.pair_ok[q] = d.bdc[q] > 0.0 && eps_i > 0.0 && eps_j > 0.0;
+      if (!d.pair_ok[q]) continue;
+      const double sq = std::sqrt(eps_i * eps_j);  // the reference's per-call value, bit for bit
+      int u = 0;
+      while (u < d.n_uniq && d.uniq_sq[u] != sq) ++u;
+      if (u == d.n_uniq) d.uniq_sq[d.n_uniq++] = sq;
+      d.pair_u[q] = (unsigned char)u;
+    }
+  h->has_transport = true;
+  return NRG_OK;
+}
+
+extern "C" int nrg_mech_transport_tables(const char* mechanism_path, const char* thermo_path,
+                                         const char* molar_masses_path, const char* transport_path,
+                                         double* well_depth, double* collision_diameter,
+                                         double* binary_diffusivity) {
+  if (!mechanism_path || !thermo_path || !molar_masses_path || !transport_path)
+    return fail(nullptr, NRG_ERR_ARG, "null path");
+  nrg::Mechanism m;
+  std::string e = nrg::load_mechanism(mechanism_path, thermo_path, molar_masses_path, 1.0, nrg::EactUnits::cal_mol, &m);
+  if (e.empty()) e = nrg::load_transport(transport_path, &m);
+  if (!e.empty()) return fail(nullptr, NRG_ERR_IO, e);
+  const int N = m.n();
+  for (int k = 0; k < N; ++k) {
+    if (well_depth) well_depth[k] = m.well_depth[k];
+    if (collision_diameter) collision_diameter[k] = m.collision_diameter[k];
+  }
+  if (binary_diffusivity)
+    for (size_t i = 0; i < (size_t)N * N; ++i) binary_diffusivity[i] = m.binary_diffusivity[i];
+  return NRG_OK;
+}
+
+extern "C" int nrg_mixture_diffusivity_device(nrg_chem* h, long n, long ld, const double* T, const double* p,
+                                              const double* Y, const double* mix_mol_mass, const signed char* bc,
+                                              double* D, void* stream) {
+  if (!h) return NRG_ERR_ARG;
+  if (!h->has_transport) return fail(h, NRG_ERR_STATE, "no transport deck loaded (nrg_chem_load_transport)");
+  if (n < 0 || ld < n || (n > 0 && (!T || !p || !Y || !mix_mol_mass || !D)))
+    return fail(h, NRG_ERR_ARG, "bad arguments to nrg_mixture_diffusivity_device");
+  nrg::DiffusivityArgs a = h->diff;
+  a.n = n; a.ld = ld; a.T = T; a.p = p; a.Y = Y; a.m_mix = mix_mol_mass; a.bc = (const int8_t*)bc; a.D = D;
+  CK(h, cudaSetDevice(h->device));
+  CK(h, cudaEventRecord(h->ev_in, (cudaStream_t)stream));
+  CK(h, cudaStreamWaitEvent(h->stream, h->ev_in, 0));
+  const cudaError_t e = nrg::launch_mixture_diffusivity(a, h->stream);
+  if (e != cudaSuccess) return cuda_fail(h, e, "diffusivity launch");
   CK(h, cudaStreamSynchronize(h->stream));
   return NRG_OK;
 }

@@ -398,7 +398,58 @@ bool molar_mass(Deck& d, const std::string& name, double* w) {
   return false;
 }
 
+// get_transport_properties (thermophysical_properties_class.f90:1379-1414):
+// one header record, then READ(u,*) name, geometry, eps/k_B, sigma until the
+// name matches; sigma is converted from Angstrom to nm.
+bool transport_record(Deck& d, const std::string& name, double* eps, double* sigma) {
+  d.rewind();
+  std::string hdr;
+  if (!d.item(&hdr)) return false;
+  std::vector<std::string> v;
+  while (true) {
+    if (!d.items(&v, 4) || v.size() < 4) return false;
+    char* end = nullptr;
+    std::strtol(v[1].c_str(), &end, 10);
+    if (v[1].empty() || *end != 0) return false;
+    double e, sg;
+    if (!fortran_real(v[2], &e) || !fortran_real(v[3], &sg)) return false;
+    if (same(v[0], name)) {
+      *eps = e;
+      *sigma = sg * 0.1;
+      return true;
+    }
+  }
+}
+
 }  // namespace
+
+std::string load_transport(const std::string& transport_path, Mechanism* m) {
+  Deck tr;
+  if (!tr.open(transport_path)) return "cannot open transport file " + transport_path;
+  const int n = m->n();
+  m->well_depth.assign(n, 0.0);
+  m->collision_diameter.assign(n, 0.0);
+  for (int k = 0; k < n; ++k) {
+    const std::string name = m->species[k].substr(0, 10);  // character(len=10) dummy
+    if (!transport_record(tr, name, &m->well_depth[k], &m->collision_diameter[k]))
+      return "transport data missing or unreadable for " + name;
+  }
+  // initialize_binary_diffusivity_constants (:1343-1377)
+  m->binary_diffusivity.assign((size_t)n * n, 0.0);
+  const std::vector<double>&W = m->molar_mass, &sg = m->collision_diameter;
+  for (int i = 0; i < n - 1; ++i) {
+    if (W[i] <= 0.0 || sg[i] <= 0.0) continue;
+    for (int j = i + 1; j < n; ++j) {
+      if (W[j] <= 0.0 || sg[j] <= 0.0) continue;
+      double red = 0.5 * (sg[i] + sg[j]);
+      red = red * red;
+      const double inv_mu = (W[i] + W[j]) / (W[i] * W[j]);
+      m->binary_diffusivity[(size_t)i * n + j] = 0.00001 * 0.595 * std::sqrt(inv_mu) / red;
+      m->binary_diffusivity[(size_t)j * n + i] = m->binary_diffusivity[(size_t)i * n + j];
+    }
+  }
+  return "";
+}
 
 std::string load_mechanism(const std::string& mech_path, const std::string& thermo_path,
                            const std::string& molar_path, double eff_default, EactUnits units,

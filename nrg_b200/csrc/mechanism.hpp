@@ -34,6 +34,9 @@ struct Mechanism {
   std::vector<double> eff;           // [r * n + k]
   std::vector<double> a_coeffs;      // [(k * 2 + set) * 7 + i], multiplied by R
   std::vector<double> molar_mass;    // kg/mol
+  // transport deck (load_transport): eps/k_B [K], sigma [nm], binary
+  // diffusivity constants [i * n + j] (symmetric, 0 on the diagonal)
+  std::vector<double> well_depth, collision_diameter, binary_diffusivity;
   int n() const { return (int)species.size(); }
   int r() const { return (int)reactions.size(); }
 };
@@ -43,6 +46,10 @@ struct Mechanism {
 std::string load_mechanism(const std::string& mech_path, const std::string& thermo_path,
                            const std::string& molar_path, double eff_default, EactUnits units,
                            Mechanism* out);
+
+// Transport deck for the species of m (thermophysical_properties_class.f90:
+// 1343-1414); empty string on success.
+std::string load_transport(const std::string& transport_path, Mechanism* m);
 
 // NASA-7 helpers with the reference's evaluation order
 // (thermophysical_properties_class.f90:225-300).

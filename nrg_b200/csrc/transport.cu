@@ -111,17 +111,37 @@ __global__ void __launch_bounds__(256, Z3 ? 1 : (N == 9 ? 3 : 2)) k_predictor(Pr
   const long k = a.lo[2] + blockIdx.z;
   const long e0 = a.e[0], e1 = a.e[1];
 
-  // stage the tile and its halo (cells outside the array stay unused)
+  // stage the tile and its halo (cells outside the array stay unused): first
+  // the raw rho and Y_k (loads only, so a thread's cells are all in flight at
+  // once), then, by the same thread, rho*Y_k, sum rho*Y_k / W_k and the most
+  // abundant species in place
+#pragma unroll 2
   for (int q = tid; q < nst; q += nthr) {
     const int rx = q % RX, ry = q / RX;
     const long i = i0 - 2 + rx, j = two_d ? j0 - 2 + ry : j0;
     if (i < 0 || i >= e0 || j < 0 || j >= e1) continue;
     const long c = i + e0 * (j + e1 * k);
-    double rY[N], row;
-    int gam;
-    cell_terms<N>(a, c, rY, row, gam);
+    s_row[q] = a.rho[c];
 #pragma unroll
-    for (int s = 0; s < N; ++s) s_rY[s * nst + q] = rY[s];
+    for (int s = 0; s < N; ++s) s_rY[s * nst + q] = a.Y[(long)s * a.ld + c];
+  }
+  for (int q = tid; q < nst; q += nthr) {
+    const int rx = q % RX, ry = q / RX;
+    const long i = i0 - 2 + rx, j = two_d ? j0 - 2 + ry : j0;
+    if (i < 0 || i >= e0 || j < 0 || j >= e1) continue;
+    const double rho = s_row[q];
+    double row = 0.0, mx = -DBL_MAX;
+    int gam = 0;
+#pragma unroll
+    for (int s = 0; s < N; ++s) {
+      const double rY = rho * s_rY[s * nst + q];
+      s_rY[s * nst + q] = rY;
+      row = row + rY / a.W[s];
+      if (rY > mx) {
+        mx = rY;
+        gam = s;
+      }
+    }
     s_row[q] = row;
     s_gam[q] = gam;
   }

@@ -44,6 +44,16 @@ typedef struct {
     double molar_mass[ORC_NMAX];
 } orc_mech;
 
+/* Transport data of the mechanism's species (thermophysical_properties_class
+ * .f90:137-210, 1343-1414): Lennard-Jones well depth eps/k_B [K], collision
+ * diameter [nm], binary diffusivity constants (symmetric, 0 on the diagonal). */
+typedef struct {
+    int n_species;
+    double well_depth[ORC_NMAX];
+    double collision_diameter[ORC_NMAX];
+    double bdc[ORC_NMAX][ORC_NMAX];
+} orc_transport;
+
 /* per-cell DDRIV3 counters */
 typedef struct {
     int nstate; /* DDRIV3 NSTATE on return (2 = ok, 3 = MXSTEP, 12 = fatal) */
@@ -105,6 +115,19 @@ int orc_apply_state(const orc_mech *m, long n, int dims, double dt, const double
                     double *Y, double *E_f, const double *v, double *T, double *p,
                     double *gamma, double *cp_mass, double *h_s, double *h_full, double *v_s,
                     double *mix_mol_mass, unsigned char *status, int n_threads);
+
+/* Reads the transport deck for the mechanism's species.  Returns 0 on success. */
+int orc_load_transport(const orc_mech *m, const char *transport_path, orc_transport *out);
+
+/* Neufeld collision integral (calculate_omega, :560-577), binary diffusion
+ * coefficient (:737-762) and the mixture-averaged coefficients of every cell
+ * (mixture_averaged_diffusion_coefficients :768-814 as called by
+ * calculate_diffusivity_coeff, fickean_diffusion_solver.f90:358-395: zero in
+ * cells with bc /= 0).  Y and D: species-major, stride n. */
+double orc_omega(double T_red, int l, int s);
+double orc_binary_diffusion(const orc_mech *m, const orc_transport *t, double T, double p, int i, int j);
+void orc_mixture_diffusivity(const orc_mech *m, const orc_transport *t, long n, const double *T, const double *p,
+                             const double *Y, const double *m_mix, const signed char *bc, double *D, int n_threads);
 
 /* Species predictor of the low-Mach solver (orc_transport.c; layout there). */
 int orc_species_predictor(int N, const double *W, int dims, const int n_cells[3], long ld, int coord, double dx,

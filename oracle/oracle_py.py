@@ -40,6 +40,15 @@ class OrcMech(ctypes.Structure):
     ]
 
 
+class OrcTransport(ctypes.Structure):
+    _fields_ = [
+        ("n_species", ctypes.c_int),
+        ("well_depth", ctypes.c_double * NMAX),
+        ("collision_diameter", ctypes.c_double * NMAX),
+        ("bdc", (ctypes.c_double * NMAX) * NMAX),
+    ]
+
+
 class OrcCounters(ctypes.Structure):
     _fields_ = [("nstate", ctypes.c_int), ("nstep", ctypes.c_int),
                 ("nfe", ctypes.c_int), ("nje", ctypes.c_int)]
@@ -78,6 +87,16 @@ def lib():
                                             ctypes.c_void_p * 3] + [ctypes.c_void_p] * 4 + [
                                             ctypes.c_int, ctypes.c_void_p] + [dp] * 6
         L.orc_species_predictor.restype = ctypes.c_int
+        L.orc_load_transport.argtypes = [ctypes.POINTER(OrcMech), ctypes.c_char_p, ctypes.POINTER(OrcTransport)]
+        L.orc_load_transport.restype = ctypes.c_int
+        L.orc_omega.argtypes = [ctypes.c_double, ctypes.c_int, ctypes.c_int]
+        L.orc_omega.restype = ctypes.c_double
+        L.orc_binary_diffusion.argtypes = [ctypes.POINTER(OrcMech), ctypes.POINTER(OrcTransport), ctypes.c_double,
+                                           ctypes.c_double, ctypes.c_int, ctypes.c_int]
+        L.orc_binary_diffusion.restype = ctypes.c_double
+        L.orc_mixture_diffusivity.argtypes = [ctypes.POINTER(OrcMech), ctypes.POINTER(OrcTransport), ctypes.c_long,
+                                              dp, dp, dp, dp, ctypes.c_void_p, dp, ctypes.c_int]
+        L.orc_mixture_diffusivity.restype = None
         L.orc_rate_constants.argtypes = [ctypes.POINTER(OrcMech), ctypes.c_double, dp, dp, dp]
         L.orc_rate_constants.restype = None
         L.orc_rhs.argtypes = [ctypes.POINTER(OrcMech), dp, dp, dp, dp, dp]
@@ -192,6 +211,36 @@ class Mechanism:
                               int(threads))
         out.update(Y=Y, E_f=E_f, T=T, status=st)
         return out
+
+    def load_transport(self, transport_path) -> None:
+        """Transport deck for this mechanism's species (orc_load_transport)."""
+        self.tr = OrcTransport()
+        rc = lib().orc_load_transport(ctypes.byref(self.m), transport_path.encode(), ctypes.byref(self.tr))
+        if rc != 0:
+            raise RuntimeError(f"oracle transport load failed: {rc}")
+
+    def transport_tables(self) -> dict:
+        N = self.m.n_species
+        return {"well_depth": np.array(self.tr.well_depth[:N]),
+                "collision_diameter": np.array(self.tr.collision_diameter[:N]),
+                "binary_diffusivity_constant": np.array([[self.tr.bdc[i][j] for j in range(N)] for i in range(N)])}
+
+    def binary_diffusion(self, T, p, i, j) -> float:
+        return lib().orc_binary_diffusion(ctypes.byref(self.m), ctypes.byref(self.tr), float(T), float(p), i, j)
+
+    def mixture_diffusivity(self, T, p, Y, m_mix, bc=None) -> np.ndarray:
+        """calculate_diffusivity_coeff over n cells: (N, n) mixture-averaged
+        diffusion coefficients (zero where bc /= 0)."""
+        n = T.shape[0]
+        N = self.m.n_species
+        T, p, m_mix = (np.ascontiguousarray(a, dtype=np.float64) for a in (T, p, m_mix))
+        Y = np.ascontiguousarray(Y, dtype=np.float64).reshape(N, n)
+        D = np.zeros((N, n))
+        bcv = None if bc is None else np.ascontiguousarray(bc, dtype=np.int8)
+        lib().orc_mixture_diffusivity(ctypes.byref(self.m), ctypes.byref(self.tr), n, _dp(T), _dp(p), _dp(Y),
+                                      _dp(m_mix), None if bcv is None else bcv.ctypes.data_as(ctypes.c_void_p),
+                                      _dp(D), 0)
+        return D
 
     def rate_constants(self, T, mix_conc):
         R = self.m.n_reactions

@@ -17,6 +17,7 @@
 #include "oracle.h"
 
 #include <ctype.h>
+#include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -620,5 +621,68 @@ int orc_load_mechanism(const char *mech_path, const char *thermo_path,
     }
     rf_close(&tf);
     rf_close(&wf);
+    return 0;
+}
+
+
+/* get_transport_properties (thermophysical_properties_class.f90:1379-1414):
+ * the first record is a header; then READ(u,*) name, geometry, eps/k_B,
+ * sigma [Angstrom] until the name matches (an unreadable record or the end of
+ * the file stops the reference's program).  sigma is returned in nm. */
+static int get_transport(recfile *f, const char *name, double *eps, double *sigma) {
+    f->pos = 0;
+    *eps = 0.0;
+    *sigma = 0.0;
+    char hdr[256];
+    if (!ld_read_string(f, hdr, sizeof hdr)) return -1;
+    for (;;) {
+        ldscan sc = {f, NULL, f->pos};
+        char tok[4][256];
+        for (int i = 0; i < 4; i++)
+            if (ld_next(&sc, tok[i], sizeof tok[i]) != 1) return -1;
+        char *end;
+        strtol(tok[1], &end, 10);
+        if (*end != 0 || end == tok[1]) return -1;
+        double e, sg;
+        if (fortran_real(tok[2], &e) || fortran_real(tok[3], &sg)) return -1;
+        if (fstr_eq(tok[0], name)) {
+            *eps = e;
+            *sigma = sg * 0.1;
+            break;
+        }
+    }
+    f->pos = 0;
+    return 0;
+}
+
+int orc_load_transport(const orc_mech *m, const char *transport_path, orc_transport *out) {
+    memset(out, 0, sizeof *out);
+    recfile tf;
+    if (rf_open(&tf, transport_path)) return 1;
+    const int N = m->n_species;
+    out->n_species = N;
+    for (int k = 0; k < N; k++) {
+        char name[11];
+        strncpy(name, m->species_names[k], 10); /* character(len=10) dummy */
+        name[10] = 0;
+        if (get_transport(&tf, name, &out->well_depth[k], &out->collision_diameter[k])) {
+            rf_close(&tf);
+            return 2;
+        }
+    }
+    rf_close(&tf);
+    /* initialize_binary_diffusivity_constants (:1343-1377) */
+    const double *W = m->molar_mass, *sg = out->collision_diameter;
+    for (int i = 0; i < N - 1; i++) {
+        if (W[i] <= 0.0 || sg[i] <= 0.0) continue;
+        for (int j = i + 1; j < N; j++) {
+            if (W[j] <= 0.0 || sg[j] <= 0.0) continue;
+            double red = 0.5 * (sg[i] + sg[j]);
+            red = red * red;
+            const double inv_mu = (W[i] + W[j]) / (W[i] * W[j]);
+            out->bdc[i][j] = 0.00001 * 0.595 * sqrt(inv_mu) / red;
+            out->bdc[j][i] = out->bdc[i][j];
+        }
+    }
     return 0;
 }

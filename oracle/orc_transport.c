@@ -13,9 +13,11 @@
  * component d (the reference's v_f%pr(d)%cells(dims, 0:n+2, ...)): extents
  * f[d] = e[d] + 1 (active) or 1, element (c, i, j, k) at
  * c + dims*(i + f0*(j + f1*k)); face i is the low face of cell i.
+ * The second half restates the mixture-averaged diffusion coefficients.
  * Parity with the reference is unpinned: it ships no known-answer test for
- * this routine. */
+ * these routines. */
 #include <float.h>
+#include <math.h>
 #include <stddef.h>
 
 #include "oracle.h"
@@ -187,4 +189,75 @@ int orc_species_predictor(int N, const double *W, int dims, const int n_cells[3]
                 }
             }
     return 0;
+}
+
+/* ------------------------------------------------------------------------
+ * Mixture-averaged diffusion coefficients (thermophysical_properties_class
+ * .f90:560-577, 737-814) with the Neufeld, Janzen and Aziz (1972) collision
+ * integral fits the reference sets in set_properties (:173-207).
+ * ---------------------------------------------------------------------- */
+static const double OMEGA_C[3][8] = {
+    /* (1,1) */ {1.06036, 0.15610, 0.19300, 0.47635, 1.03587, 1.52996, 1.76474, 3.89411},
+    /* (1,2) */ {1.00220, 0.15530, 0.16105, 0.72751, 0.86125, 2.06848, 1.95162, 4.84492},
+    /* (2,2) */ {1.16145, 0.14874, 0.52487, 0.77320, 2.16178, 2.43787, 0.0, 0.0}};
+
+double orc_omega(double T_red, int l, int s) {
+    const double *c = OMEGA_C[l == 2 ? 2 : (s == 2 ? 1 : 0)];
+    if (T_red < 70.0)
+        return c[0] / pow(T_red, c[1]) + c[2] / exp(c[3] * T_red) + c[4] / exp(c[5] * T_red) +
+               c[6] / exp(c[7] * T_red);
+    return c[0] / pow(T_red, c[1]);
+}
+
+double orc_binary_diffusion(const orc_mech *m, const orc_transport *t, double T, double p, int i, int j) {
+    (void)m;
+    if (T <= 0.0 || p <= 0.0) return 0.0;
+    if (i == j) return 0.0;
+    const int i1 = i < j ? i : j, i2 = i < j ? j : i;
+    if (t->bdc[i1][i2] <= 0.0) return 0.0;
+    if (t->well_depth[i1] <= 0.0 || t->well_depth[i2] <= 0.0) return 0.0;
+    const double T_red = T / sqrt(t->well_depth[i1] * t->well_depth[i2]);
+    const double omega = orc_omega(T_red, 1, 1);
+    if (omega <= 0.0) return 0.0;
+    return t->bdc[i1][i2] * pow(T, 1.5) / (p * omega);
+}
+
+static void mixture_cell(const orc_mech *m, const orc_transport *t, double T, double p, const double *Y,
+                         double m_mix, double *D) {
+    const int N = m->n_species;
+    const double *W = m->molar_mass;
+    for (int i = 0; i < N; i++) D[i] = 0.0;
+    if (N <= 0 || T <= 0.0 || p <= 0.0 || m_mix <= 0.0) return;
+    double Db[ORC_NMAX][ORC_NMAX];
+    for (int i = 0; i < N - 1; i++)
+        for (int j = i + 1; j < N; j++) Db[i][j] = orc_binary_diffusion(m, t, T, p, i, j);
+    for (int i = 0; i < N; i++) {
+        if (W[i] <= 0.0) continue;
+        double acc = 0.0;
+        for (int j = 0; j < N; j++) {
+            if (j == i) continue;
+            if (W[j] <= 0.0) continue;
+            const double Dij = j > i ? Db[i][j] : Db[j][i];
+            if (Dij <= 0.0) continue;
+            acc = acc + (1.0 - Y[i]) * W[i] * Y[j] / (Dij * W[j]);
+            acc = acc + Y[i] * Y[j] / Dij;
+        }
+        if (acc > 1.0e-10) D[i] = (1.0 - Y[i]) * W[i] / (acc * m_mix);
+    }
+}
+
+void orc_mixture_diffusivity(const orc_mech *m, const orc_transport *t, long n, const double *T, const double *p,
+                             const double *Y, const double *m_mix, const signed char *bc, double *D, int n_threads) {
+    const int N = m->n_species;
+    (void)n_threads;
+#pragma omp parallel for schedule(static)
+    for (long c = 0; c < n; c++) {
+        double y[ORC_NMAX], d[ORC_NMAX];
+        for (int k = 0; k < N; k++) d[k] = 0.0;
+        if (!bc || bc[c] == 0) {
+            for (int k = 0; k < N; k++) y[k] = Y[(long)k * n + c];
+            mixture_cell(m, t, T[c], p[c], y, m_mix[c], d);
+        }
+        for (int k = 0; k < N; k++) D[(long)k * n + c] = d[k];
+    }
 }
