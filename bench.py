@@ -48,8 +48,9 @@ def parse():
     p.add_argument("--kernel", choices=["thread", "thread_queue", "warp_queue"], default=None,
                    help="fix the integrator launch instead of autotuning it (with --block)")
     p.add_argument("--block", type=int, default=32)
-    p.add_argument("--mechanism", default="KEROMNES", choices=["KEROMNES", "ZHANG", "TEREZA", "KONNOV"],
-                   help="reference H2/air mechanism; the others run the plain FP64 path on the same flame field")
+    p.add_argument("--mechanism", default="KEROMNES", choices=["KEROMNES", "ZHANG", "TEREZA", "KONNOV", "ACETYLENE"],
+                   help="reference mechanism; the others run the plain FP64 path on the same flame field "
+                        "(ACETYLENE: the same geometry with a C2H2/O2/Ar mixture)")
     p.add_argument("--no-predictor", dest="predictor", action="store_false",
                    help="skip timing the low-Mach species predictor on an n-side x n-side flame block "
                         "(nrg_species_predictor_device)")
@@ -190,12 +191,11 @@ def load_peaks() -> dict:
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "fallback": True}
 
 
-def cpu_baseline(field, W, decks, seconds: float) -> dict:
+def cpu_baseline(field, W, decks, seconds: float, units: str = "cal.mol") -> dict:
     """CPU restatement of the reference path (oracle, all host cores) on a
     strided sample of the same field, sized to about `seconds` of work."""
     from oracle import oracle_py as op
-    from nrg_b200 import fields as F
-    m = op.Mechanism(*decks, 1.0, "cal.mol")
+    m = op.Mechanism(*decks, 1.0, units)
     cores = os.cpu_count() or 1
     probe = sample_cells(field, 4096, seed=1)
     t0 = time.perf_counter()
@@ -370,16 +370,22 @@ def main():
     torch.cuda.set_device(local)
     if world > 1:
         dist.init("nccl", timeout_s=600)
-    from nrg_b200 import fields as F, keromnes_paths, mechanism_paths
+    from nrg_b200 import eact_units, fields as F, keromnes_paths, mechanism_paths
     from nrg_b200.chemistry import ChemicalKineticsSolver, DataManager, fp64_peak_tflops, mechanism_tables
     from nrg_b200.surrogate import DEFAULT_MODEL, RECIPE, Surrogate, train_default
     decks = mechanism_paths(args.mechanism)
-    tables = mechanism_tables(*decks)
+    units = eact_units(args.mechanism)
+    tables = mechanism_tables(*decks, 1.0, units)
     W = tables["molar_mass"]
     dev = torch.device("cuda", local)
-    solver = ChemicalKineticsSolver(None, *decks, mode="fast")
+    solver = ChemicalKineticsSolver(None, *decks, E_act_units=units, mode="fast")
     field = F.config4(mechanism_tables(*keromnes_paths())["molar_mass"], n_side=args.n_side)
-    if args.mechanism != "KEROMNES":
+    if args.mechanism == "ACETYLENE":
+        # the same flame geometry with the C2H2/O2/Ar mixture
+        field = F.acetylene_flame(solver.species_names[:tables["n_species"]], W, n_side=args.n_side)
+        args.no_e2e = True
+        args.predictor = args.diffusivity = False
+    elif args.mechanism != "KEROMNES":
         # the same flame, in the mechanism's species (others start at zero)
         field = F.state_for_species(field, solver.species_names[:tables["n_species"]], W)
         args.no_e2e = True
@@ -564,7 +570,7 @@ def main():
                         "frac": mlp_tf / peaks["bf16_tflops"], "kernel": "k_mlp_gate_tc (features + 5 tcgen05 "
                         "layers + FP64 gate)", "flops_per_launch": mlp_flops,
                         "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst), of measured"}
-        cpu = cpu_baseline(field, W, decks, args.cpu_seconds)
+        cpu = cpu_baseline(field, W, decks, args.cpu_seconds, units)
         launches = 5 if mode == "surrogate" else 1  # fused MLP+gate, 3 compaction kernels, integrator
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -572,7 +578,7 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f64+bf16" if mode == "surrogate" else "f64",
             "data": "synthetic",
             "config": {"workload": f"flame field {args.n_side}x{args.n_side} ({n:,} cells), dt=1e-6 s, p=1 atm, "
-                                   f"{args.mechanism} H2/air ({tables['n_species']} species, "
+                                   f"{args.mechanism} {'C2H2/O2/Ar' if args.mechanism == 'ACETYLENE' else 'H2/air'} ({tables['n_species']} species, "
                                    f"{tables['n_reactions']} reactions)",
                        "path": {"fast": "plain FP64 integrator, analytic Jacobian",
                                 "reference": "plain FP64 integrator, reference FD Jacobian",

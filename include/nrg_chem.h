@@ -18,7 +18,7 @@
 extern "C" {
 #endif
 
-#define NRG_MAX_SPECIES 16
+#define NRG_MAX_SPECIES 24
 
 #if defined(__GNUC__)
 #define NRG_API __attribute__((visibility("default")))

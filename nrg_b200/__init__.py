@@ -9,16 +9,32 @@ import os
 MECH_DIR = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "tests", "golden", "mechanism")
 
 
+# the reference's H2/air mechanisms (task_setup/chemical_mechanisms)
 MECHANISMS = ("KEROMNES", "ZHANG", "TEREZA", "KONNOV")
+# plus its C2H2/O2 deck, the only one with carbon species, whose thermo and
+# transport data are the FFCM-1 files of task_setup/thermophysical_data
+ALL_MECHANISMS = MECHANISMS + ("ACETYLENE",)
+_DECKS = {"ACETYLENE": ("ACETYLENE_Varatharajan.txt", "FFCM-1_thermo.txt", "FFCM-1_transport.txt")}
+
+
+def _check_name(name: str) -> None:
+    if name not in ALL_MECHANISMS:
+        raise ValueError(f"unknown mechanism {name!r}; have {ALL_MECHANISMS}")
 
 
 def mechanism_paths(name: str = "KEROMNES"):
-    """Input decks of one of the reference's H2/air mechanisms (mechanism,
-    thermo, molar masses), as in its task_setup directory."""
-    if name not in MECHANISMS:
-        raise ValueError(f"unknown mechanism {name!r}; have {MECHANISMS}")
-    return (os.path.join(MECH_DIR, f"{name}.txt"), os.path.join(MECH_DIR, f"{name}_THERMO.txt"),
-            os.path.join(MECH_DIR, "molar_masses.dat"))
+    """Input decks of one of the reference's mechanisms (mechanism, thermo,
+    molar masses), as in its task_setup directory."""
+    _check_name(name)
+    mech, thermo = (_DECKS[name][:2] if name in _DECKS else (f"{name}.txt", f"{name}_THERMO.txt"))
+    return (os.path.join(MECH_DIR, mech), os.path.join(MECH_DIR, thermo), os.path.join(MECH_DIR, "molar_masses.dat"))
+
+
+def eact_units(name: str = "KEROMNES") -> str:
+    """Activation-energy units of the deck (its header comment; the H2/air
+    setups use cal.mol, 1D_laminar_velocity.f90:327-336)."""
+    _check_name(name)
+    return "J.mol" if name == "ACETYLENE" else "cal.mol"
 
 
 def keromnes_paths():
@@ -29,6 +45,5 @@ def keromnes_paths():
 def transport_path(name: str = "KEROMNES"):
     """The mechanism's transport deck (Lennard-Jones parameters), as in the
     reference's task_setup/thermophysical_data directory."""
-    if name not in MECHANISMS:
-        raise ValueError(f"unknown mechanism {name!r}; have {MECHANISMS}")
-    return os.path.join(MECH_DIR, f"{name}_TRANSDATA.txt")
+    _check_name(name)
+    return os.path.join(MECH_DIR, _DECKS[name][2] if name in _DECKS else f"{name}_TRANSDATA.txt")

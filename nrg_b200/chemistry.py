@@ -23,7 +23,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libnrg_chem.so")
-NRG_MAX_SPECIES = 16
+NRG_MAX_SPECIES = 24
 
 MODES = {"reference": 0, "fast": 1, "mixed": 2, "surrogate": 3}
 EACT_UNITS = {"J.mol": 0, "kJ.mol": 1, "cal.mol": 2, "kcal.mol": 3}

@@ -11,7 +11,7 @@
 
 namespace nrg {
 
-constexpr int kMaxSpecies = 16;
+constexpr int kMaxSpecies = 24;
 constexpr int kMaxReactions = 96;
 constexpr int kMaxOrd = 5;  // MXORD for Gear (MINT = 2)
 constexpr int kMaxSpecUpd = 64;  // reactions touching one species

@@ -28,6 +28,9 @@ cudaError_t launch_chem_fast(const StepArgs& a, const LaunchCfg& cfg, int* queue
   if (n_species == 13 && n_reactions == 71 && n_int == 13)
     return spec == kSpecKonnov ? launch_grid<13, 13, 71, kA, double, kSpecKonnov>(a, cfg, queue, counters, s)
                                : launch_grid<13, 13, 71, kA, double>(a, cfg, queue, counters, s);
+  if (n_species == 17 && n_reactions == 25 && n_int == 15)
+    return spec == kSpecAcetylene ? launch_grid<17, 15, 25, kA, double, kSpecAcetylene>(a, cfg, queue, counters, s)
+                                  : launch_grid<17, 15, 25, kA, double>(a, cfg, queue, counters, s);
   return cudaErrorNotSupported;
 }
 

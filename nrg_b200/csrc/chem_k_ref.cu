@@ -18,6 +18,8 @@ cudaError_t launch_chem_ref(const StepArgs& a, const LaunchCfg& cfg, int* queue,
     return launch_grid<10, 10, 24, kJacFD, double>(a, cfg, queue, counters, s);
   if (n_species == 13 && n_reactions == 71)
     return launch_grid<13, 13, 71, kJacFD, double>(a, cfg, queue, counters, s);
+  if (n_species == 17 && n_reactions == 25)
+    return launch_grid<17, 17, 25, kJacFD, double>(a, cfg, queue, counters, s);
   return cudaErrorNotSupported;
 }
 

@@ -138,6 +138,7 @@ cudaError_t launch_apply_state(int n_species, const ApplyStateArgs& a, cudaStrea
     case 9: k_apply_state<9><<<(unsigned)grid, 128, 0, s>>>(a); break;
     case 10: k_apply_state<10><<<(unsigned)grid, 128, 0, s>>>(a); break;
     case 13: k_apply_state<13><<<(unsigned)grid, 128, 0, s>>>(a); break;
+    case 17: k_apply_state<17><<<(unsigned)grid, 128, 0, s>>>(a); break;
     default: return cudaErrorNotSupported;
   }
   return cudaGetLastError();
@@ -164,7 +165,8 @@ cudaError_t launch_chem(int n_species, int n_int, int spec, int n_reactions, int
 
 bool supported_mechanism(int n_species, int n_reactions) {
   return (n_species == 9 && n_reactions == 24) || (n_species == 9 && n_reactions == 28) ||
-         (n_species == 10 && n_reactions == 24) || (n_species == 13 && n_reactions == 71);
+         (n_species == 10 && n_reactions == 24) || (n_species == 13 && n_reactions == 71) ||
+         (n_species == 17 && n_reactions == 25);
 }
 
 int match_specialised(const DevMech& reduced) { return match_specialised_tables(reduced); }

@@ -126,6 +126,17 @@ def config4(W: np.ndarray, n_side: int = 2048, seed: int = 4) -> Field:
     (delta = 0.5 mm) from 300 K to 2400 K along x, front position perturbed in
     y by 8 seeded sinusoids of amplitude 0.2 mm, radicals Gaussian at the front
     with peak mass fraction 1e-3, p = 1 atm, dt = 1e-6 s."""
+    T, c, g = _flame_geometry(n_side, seed)
+    Yr, Yp, idx = _stoich(W)
+    Y = (1.0 - c)[None, :] * Yr[:, None] + c[None, :] * Yp[:, None]
+    for sp in RADICALS:
+        Y[idx[sp]] = 1e-3 * g
+    n = n_side * n_side
+    return _finish("config4", T, np.full(n, P_ATM), Y, W, 1e-6, (n_side, n_side))
+
+
+def _flame_geometry(n_side: int, seed: int):
+    """Flat (T, progress c, front Gaussian g) of the config-4 geometry."""
     rng = np.random.Generator(np.random.PCG64(seed))
     dx = 10e-6
     delta = 0.5e-3
@@ -139,14 +150,47 @@ def config4(W: np.ndarray, n_side: int = 2048, seed: int = 4) -> Field:
     s = (x[None, :] - xf[:, None]) / delta
     c = 0.5 * (1.0 + np.tanh(s))
     T = 300.0 + 2100.0 * c
-    Yr, Yp, idx = _stoich(W)
-    cf = c.reshape(-1)
-    Y = (1.0 - cf)[None, :] * Yr[:, None] + cf[None, :] * Yp[:, None]
-    g = np.exp(-0.5 * (s.reshape(-1)) ** 2)
-    for sp in RADICALS:
-        Y[idx[sp]] = 1e-3 * g
+    return T.reshape(-1), c.reshape(-1), np.exp(-0.5 * (s.reshape(-1)) ** 2)
+
+
+ACETYLENE_RADICALS = ["H", "O", "OH", "HO2", "HCO", "CH3", "HCCO"]
+
+
+def _acetylene_mix(names, W):
+    """Stoichiometric C2H2/O2 in 70 % argon (mole) and its complete products."""
+    idx = {s: i for i, s in enumerate(names)}
+    Xr, Xp = np.zeros(len(names)), np.zeros(len(names))
+    Xr[idx["C2H2"]], Xr[idx["O2"]], Xr[idx["AR"]] = 2.0, 5.0, 16.33
+    Xp[idx["CO2"]], Xp[idx["H2O"]], Xp[idx["AR"]] = 4.0, 2.0, 16.33
+    return Xr * W / np.sum(Xr * W), Xp * W / np.sum(Xp * W), idx
+
+
+def acetylene_state(names, W: np.ndarray, n: int, seed: int = 0, T_lo: float = 1000.0, T_hi: float = 2600.0,
+                    dt: float = 1e-6) -> Field:
+    """Random cells of the C2H2/O2/Ar mechanism: T ~ U[T_lo, T_hi], p = 1
+    atm, progress c ~ U[0, 1] between the stoichiometric mixture and its
+    products, radicals log-uniform on [1e-8, 1e-4]."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    Yr, Yp, idx = _acetylene_mix(names, W)
+    T = rng.uniform(T_lo, T_hi, n)
+    c = rng.uniform(0.0, 1.0, n)
+    Y = (1.0 - c)[None, :] * Yr[:, None] + c[None, :] * Yp[:, None]
+    for sp in ACETYLENE_RADICALS:
+        Y[idx[sp]] = 10.0 ** rng.uniform(-8.0, -4.0, n)
+    return _finish("acetylene", T, np.full(n, P_ATM), Y, W, dt, (n,))
+
+
+def acetylene_flame(names, W: np.ndarray, n_side: int = 2048, seed: int = 4) -> Field:
+    """The config-4 flame geometry with the C2H2/O2/Ar mixture: same
+    temperature field, reactants to products along the front, radicals
+    Gaussian at the front with peak mass fraction 1e-4."""
+    T, c, g = _flame_geometry(n_side, seed)
+    Yr, Yp, idx = _acetylene_mix(names, W)
+    Y = (1.0 - c)[None, :] * Yr[:, None] + c[None, :] * Yp[:, None]
+    for sp in ACETYLENE_RADICALS:
+        Y[idx[sp]] = 1e-4 * g
     n = n_side * n_side
-    return _finish("config4", T.reshape(-1), np.full(n, P_ATM), Y, W, 1e-6, (n_side, n_side))
+    return _finish("acetylene_flame", T, np.full(n, P_ATM), Y, W, 1e-6, (n_side, n_side))
 
 
 def slice_field(f: Field, n: int, stride: int = 1, offset: int = 0) -> Field:

@@ -242,6 +242,36 @@ def test_other_reference_mechanisms_parity(name):
         s.close()
 
 
+def test_acetylene_mechanism_parity():
+    """The reference's C2H2/O2 deck (17 species, 25 irreversible reactions,
+    FFCM-1 thermo data, E_act in J/mol) on random C2H2/O2/Ar cells against
+    the oracle in both FP64 modes, and its generated code against its table
+    walk."""
+    from nrg_b200 import eact_units, mechanism_paths
+    from nrg_b200.chemistry import ChemicalKineticsSolver, mechanism_tables
+    from oracle import oracle_py as op
+    paths = mechanism_paths("ACETYLENE")
+    units = eact_units("ACETYLENE")
+    om = op.Mechanism(*paths, 1.0, units)
+    W = mechanism_tables(*paths, 1.0, units)["molar_mass"]
+    f = fields.acetylene_state(om.species()[:om.n_species], W, 1024, seed=3)
+    o = oracle_run(om, f)
+    s = ChemicalKineticsSolver(None, *paths, E_act_units=units, mode="reference")
+    try:
+        outs = {}
+        for mode in ("reference", "fast"):
+            g, st = run_device(s, f, mode, launch=dict(kernel="thread", block=32, grid=0, chunk=1))
+            assert st["cells_bad"] == 0, (mode, st)
+            check_parity(g, o, f, np.ones(f.n, bool))
+            outs[mode] = g
+        s.set_specialised(False)
+        g, _ = run_device(s, f, "fast", launch=dict(kernel="thread", block=32, grid=0, chunk=1))
+        for key in ("Y_prod", "Y_prod2", "E_f_prod", "T_after", "status"):
+            np.testing.assert_array_equal(g[key], outs["fast"][key])
+    finally:
+        s.close()
+
+
 def fields_W():
     from nrg_b200 import keromnes_paths
     from nrg_b200.chemistry import mechanism_tables

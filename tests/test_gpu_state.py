@@ -73,3 +73,28 @@ def test_chemistry_step_then_state_update_on_device(solver, oracle_mech, W):
     assert np.max(np.abs(g["p"] - o["p"])[act] / o["p"][act]) <= 1e-6
     # the state equation's T equals the chemistry step's own closure
     assert np.max(np.abs(g["T"][act] - g_step["T_after"][act])) < 1e-6
+
+
+def test_acetylene_state_equation_matches_oracle():
+    """The 17-species C2H2/O2 deck with the FFCM-1 thermo data."""
+    from nrg_b200 import eact_units, mechanism_paths
+    from nrg_b200.chemistry import ChemicalKineticsSolver, mechanism_tables
+    from oracle import oracle_py as op
+    paths = mechanism_paths("ACETYLENE")
+    units = eact_units("ACETYLENE")
+    om = op.Mechanism(*paths, 1.0, units)
+    W17 = mechanism_tables(*paths, 1.0, units)["molar_mass"]
+    f = fields.acetylene_state(om.species()[:om.n_species], W17, 2000, seed=4)
+    rng = np.random.default_rng(9)
+    v = rng.uniform(-300.0, 300.0, (2, f.n))
+    E = _energy_per_mass(om, f.T, f.Y, W17, v)
+    T0 = f.T * rng.uniform(0.9, 1.1, f.n)
+    s = ChemicalKineticsSolver(None, *paths, E_act_units=units, mode="fast")
+    try:
+        g = _device_state(s, f, E, v, T0)
+    finally:
+        s.close()
+    o = om.apply_state(f.rho, f.Y, E, T0, v=v)
+    np.testing.assert_array_equal(g["status"], o["status"])
+    for k in KEYS:
+        np.testing.assert_allclose(g[k], o[k], rtol=1e-13, atol=0, err_msg=k)

@@ -7,7 +7,7 @@ import os
 import numpy as np
 import pytest
 
-from nrg_b200 import MECHANISMS, mechanism_paths, transport_path
+from nrg_b200 import MECHANISMS, eact_units, mechanism_paths, transport_path
 from oracle import oracle_py as op
 
 P_ATM = 101325.0
@@ -20,11 +20,11 @@ def om():
     return m
 
 
-@pytest.mark.parametrize("name", MECHANISMS)
+@pytest.mark.parametrize("name", MECHANISMS + ("ACETYLENE",))
 def test_transport_tables_product_equals_oracle(name):
     from nrg_b200.chemistry import transport_tables
     t = transport_tables(*mechanism_paths(name), transport_path(name))
-    m = op.Mechanism(*mechanism_paths(name), 1.0, "cal.mol")
+    m = op.Mechanism(*mechanism_paths(name), 1.0, eact_units(name))
     m.load_transport(transport_path(name))
     o = m.transport_tables()
     for k in t:
