@@ -748,7 +748,7 @@ __global__ void k_standardize(long n, const float* xraw, const float* yraw, cons
 struct Surrogate {
   bool ready = false;
   bool uploaded = false;
-  GateCfg gate{1e-6, 2e-6, 0.15, 5.0};
+  GateCfg gate{1e-6, 5e-6, 0.2, 5.0};
   MlpNorm norm{};
   MlpNorm* d_norm = nullptr;
   // parameters: fp32 master, Adam moments, bf16 working copies, gradients

@@ -70,7 +70,7 @@ class Surrogate:
         v = np.ascontiguousarray(v, np.float32)
         _check(lib().nrg_surrogate_set_norm(self.h, v.ctypes.data), self.h)
 
-    def set_gate(self, elem_tol=1e-6, raw_elem_tol=2e-6, dT_tol=0.15, dT_max=5.0) -> None:
+    def set_gate(self, elem_tol=1e-6, raw_elem_tol=5e-6, dT_tol=0.2, dT_max=5.0) -> None:
         _check(lib().nrg_surrogate_set_gate(self.h, elem_tol, raw_elem_tol, dT_tol, dT_max), self.h)
 
     def set_inference(self, fused: bool = True) -> None:
@@ -147,9 +147,9 @@ class PrepareOpts(ctypes.Structure):
 # The gate thresholds (elem_tol, raw_elem_tol, dT_tol, dT_max) were chosen on
 # a validation flame field (config4 geometry, seed 5) as the widest setting
 # whose accepted cells stay within 0.8 K and 8e-5 of the FP64 result.
-RECIPE = dict(n_train=4_000_000, epochs=60, batch=4096, lr=2e-3, coupled=0.5, hull_margin=0.02, dt_pow=1.0,
+RECIPE = dict(n_train=4_000_000, epochs=150, batch=4096, lr=2e-3, coupled=0.5, hull_margin=0.02, dt_pow=1.0,
               log_mask=0, log_eps=1e-7, common_dY_scale=0, T_lo=800.0,
-              gate=(1e-6, 2e-6, 0.15, 5.0))
+              gate=(1e-6, 5e-6, 0.2, 5.0))
 
 
 def training_pairs(solver: ChemicalKineticsSolver, W: np.ndarray, n: int, seed: int = 3,
