@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -35,6 +36,8 @@ struct nrg_chem {
   int device = 0;
   int num_sms = 148;
   cudaStream_t stream = nullptr;
+  cudaStream_t copy_stream = nullptr;       // host-path transfers, overlapped with the host gather / scatter
+  cudaEvent_t ev_chunk[8] = {};             // host path: D2H of chunk p done
   int mode = NRG_MODE_FAST;
   LaunchCfg cfg;
   bool use_graph = true;
@@ -231,6 +234,24 @@ void free_staging(nrg_chem* h) {
   h->d_bc = h->h_bc = nullptr;
   h->d_status = h->h_status = nullptr;
   h->cap = 0;
+}
+
+// Runs f(r) for every r in [r0, r1) on the host's hardware threads (contiguous
+// blocks of rows per thread).
+template <class F>
+void parallel_rows(long r0, long r1, F f) {
+  const long n = r1 - r0;
+  if (n <= 0) return;
+  long T = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  T = std::min(T, n);
+  auto body = [&](long t) {
+    for (long r = r0 + n * t / T; r < r0 + n * (t + 1) / T; ++r) f(r);
+  };
+  std::vector<std::thread> th;
+  th.reserve((size_t)T - 1);
+  for (long t = 1; t < T; ++t) th.emplace_back(body, t);
+  body(0);
+  for (std::thread& x : th) x.join();
 }
 
 int ensure_staging(nrg_chem* h, size_t n) {
@@ -472,6 +493,9 @@ extern "C" int nrg_chem_destroy(nrg_chem* h) {
   for (int i = 0; i < 4; ++i)
     if (h->ph[i]) cudaEventDestroy(h->ph[i]);
   if (h->stream) cudaStreamDestroy(h->stream);
+  if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
+  for (cudaEvent_t& e : h->ev_chunk)
+    if (e) cudaEventDestroy(e);
   delete h;
   return NRG_OK;
 }
@@ -587,27 +611,47 @@ extern "C" int nrg_chem_step(nrg_chem* h, double time_step, const nrg_field_desc
     if (stats) std::memset(stats, 0, sizeof(*stats));
     return NRG_OK;
   }
+  if (!(time_step > 0.0)) return fail(h, NRG_ERR_ARG, "time_step must be > 0");
   int rc = ensure_staging(h, (size_t)n);
   if (rc) return rc;
-  // gather the interior (i fastest, as the reference's collapse(3) loop)
-  auto lin = [&](int i, int j, int k) {
-    return ((long)(k - f->lb[2]) * ext[1] + (j - f->lb[1])) * ext[0] + (i - f->lb[0]);
+  if (!h->copy_stream) {
+    CK(h, cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+    for (cudaEvent_t& e : h->ev_chunk) CK(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  // The interior is handled as rows along i (contiguous in the reference's
+  // column-major arrays); rows are split into chunks so that the host gather
+  // of chunk p + 1 overlaps the H2D copy of chunk p, and the host scatter of
+  // chunk p overlaps the D2H copy of chunk p + 1.  Each chunk's gather and
+  // scatter run on all host threads.
+  const long rowlen = cnt[0], nrow = cnt[1] * cnt[2];
+  auto row_base = [&](long r) {
+    const int j = f->lo[1] + (int)(r % cnt[1]), k = f->lo[2] + (int)(r / cnt[1]);
+    return ((long)(k - f->lb[2]) * ext[1] + (j - f->lb[1])) * ext[0] + (f->lo[0] - f->lb[0]);
   };
-  long c = 0;
-  for (int k = f->lo[2]; k <= f->hi[2]; ++k)
-    for (int j = f->lo[1]; j <= f->hi[1]; ++j)
-      for (int i = f->lo[0]; i <= f->hi[0]; ++i, ++c) {
-        long L = lin(i, j, k);
-        h->h_T[c] = f->T[L];
-        h->h_rho[c] = f->rho[L];
-        h->h_bc[c] = f->bc_markers ? f->bc_markers[L] : 0;
-        for (int s = 0; s < N; ++s) h->h_Y[(size_t)s * n + c] = f->Y[s][L];
-      }
-  cudaStream_t s = h->stream;
-  CK(h, cudaMemcpyAsync(h->d_T, h->h_T, n * 8, cudaMemcpyHostToDevice, s));
-  CK(h, cudaMemcpyAsync(h->d_rho, h->h_rho, n * 8, cudaMemcpyHostToDevice, s));
-  CK(h, cudaMemcpyAsync(h->d_Y, h->h_Y, (size_t)N * n * 8, cudaMemcpyHostToDevice, s));
-  CK(h, cudaMemcpyAsync(h->d_bc, h->h_bc, n, cudaMemcpyHostToDevice, s));
+  const int P = (int)std::min<long>(8, nrow);
+  const size_t rb = (size_t)rowlen * 8;
+  cudaStream_t s = h->stream, cs = h->copy_stream;
+  for (int p = 0; p < P; ++p) {
+    const long r0 = nrow * p / P, r1 = nrow * (p + 1) / P, c0 = r0 * rowlen, nc = (r1 - r0) * rowlen;
+    parallel_rows(r0, r1, [&](long r) {
+      const long L = row_base(r), c = r * rowlen;
+      std::memcpy(h->h_T + c, f->T + L, rb);
+      std::memcpy(h->h_rho + c, f->rho + L, rb);
+      if (f->bc_markers)
+        std::memcpy(h->h_bc + c, f->bc_markers + L, (size_t)rowlen);
+      else
+        std::memset(h->h_bc + c, 0, (size_t)rowlen);
+      for (int sp = 0; sp < N; ++sp) std::memcpy(h->h_Y + (size_t)sp * n + c, f->Y[sp] + L, rb);
+    });
+    CK(h, cudaMemcpyAsync(h->d_T + c0, h->h_T + c0, nc * 8, cudaMemcpyHostToDevice, cs));
+    CK(h, cudaMemcpyAsync(h->d_rho + c0, h->h_rho + c0, nc * 8, cudaMemcpyHostToDevice, cs));
+    CK(h, cudaMemcpyAsync(h->d_bc + c0, h->h_bc + c0, nc, cudaMemcpyHostToDevice, cs));
+    for (int sp = 0; sp < N; ++sp)
+      CK(h, cudaMemcpyAsync(h->d_Y + (size_t)sp * n + c0, h->h_Y + (size_t)sp * n + c0, nc * 8,
+                            cudaMemcpyHostToDevice, cs));
+  }
+  CK(h, cudaEventRecord(h->ev_in, cs));
+  CK(h, cudaStreamWaitEvent(s, h->ev_in, 0));
   StepArgs a;
   a.n = n;
   a.ld = n;
@@ -627,26 +671,34 @@ extern "C" int nrg_chem_step(nrg_chem* h, double time_step, const nrg_field_desc
   a.cell_list = nullptr;
   a.n_list = 0;
   a.n_list_dev = nullptr;
-  if (!(time_step > 0.0)) return fail(h, NRG_ERR_ARG, "time_step must be > 0");
-  rc = run_step(h, a, s, stats);
+  rc = run_step(h, a, s, stats);  // returns with the step finished
   if (rc) return rc;
-  CK(h, cudaMemcpyAsync(h->h_Yp, h->d_Yp, (size_t)N * n * 8, cudaMemcpyDeviceToHost, s));
-  CK(h, cudaMemcpyAsync(h->h_Yp2, h->d_Yp2, (size_t)N * n * 8, cudaMemcpyDeviceToHost, s));
-  CK(h, cudaMemcpyAsync(h->h_Ef, h->d_Ef, n * 8, cudaMemcpyDeviceToHost, s));
-  CK(h, cudaMemcpyAsync(h->h_status, h->d_status, n, cudaMemcpyDeviceToHost, s));
-  CK(h, cudaStreamSynchronize(s));
-  c = 0;
-  for (int k = f->lo[2]; k <= f->hi[2]; ++k)
-    for (int j = f->lo[1]; j <= f->hi[1]; ++j)
-      for (int i = f->lo[0]; i <= f->hi[0]; ++i, ++c) {
-        long L = lin(i, j, k);
-        f->E_f_prod[L] = h->h_Ef[c];
-        const bool touched = h->h_status[c] != NRG_CELL_SKIPPED;
-        for (int sp = 0; sp < N; ++sp) {
-          f->Y_prod[sp][L] = h->h_Yp[(size_t)sp * n + c];
-          if (touched) f->Y_prod2[sp][L] = h->h_Yp2[(size_t)sp * n + c];  // reference leaves it
-        }
+  for (int p = 0; p < P; ++p) {
+    const long c0 = nrow * p / P * rowlen, nc = (nrow * (p + 1) / P - nrow * p / P) * rowlen;
+    for (int sp = 0; sp < N; ++sp) {
+      CK(h, cudaMemcpyAsync(h->h_Yp + (size_t)sp * n + c0, h->d_Yp + (size_t)sp * n + c0, nc * 8,
+                            cudaMemcpyDeviceToHost, cs));
+      CK(h, cudaMemcpyAsync(h->h_Yp2 + (size_t)sp * n + c0, h->d_Yp2 + (size_t)sp * n + c0, nc * 8,
+                            cudaMemcpyDeviceToHost, cs));
+    }
+    CK(h, cudaMemcpyAsync(h->h_Ef + c0, h->d_Ef + c0, nc * 8, cudaMemcpyDeviceToHost, cs));
+    CK(h, cudaMemcpyAsync(h->h_status + c0, h->d_status + c0, nc, cudaMemcpyDeviceToHost, cs));
+    CK(h, cudaEventRecord(h->ev_chunk[p], cs));
+  }
+  for (int p = 0; p < P; ++p) {
+    CK(h, cudaEventSynchronize(h->ev_chunk[p]));
+    parallel_rows(nrow * p / P, nrow * (p + 1) / P, [&](long r) {
+      const long L = row_base(r), c = r * rowlen;
+      std::memcpy(f->E_f_prod + L, h->h_Ef + c, rb);
+      for (int sp = 0; sp < N; ++sp) {
+        std::memcpy(f->Y_prod[sp] + L, h->h_Yp + (size_t)sp * n + c, rb);
+        double* y2 = f->Y_prod2[sp] + L;
+        const double* src = h->h_Yp2 + (size_t)sp * n + c;
+        for (long i = 0; i < rowlen; ++i)
+          if (h->h_status[c + i] != NRG_CELL_SKIPPED) y2[i] = src[i];  // the reference leaves it in skipped cells
       }
+    });
+  }
   return NRG_OK;
 }
 
