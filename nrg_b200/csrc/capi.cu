@@ -36,8 +36,10 @@ struct nrg_chem {
   int device = 0;
   int num_sms = 148;
   cudaStream_t stream = nullptr;
-  cudaStream_t copy_stream = nullptr;       // host-path transfers, overlapped with the host gather / scatter
-  cudaEvent_t ev_chunk[8] = {};             // host path: D2H of chunk p done
+  // host path: H2D and D2H copy streams and per-chunk events (copied in,
+  // stepped, copied out), so that transfers and host work overlap the steps
+  cudaStream_t copy_in = nullptr, copy_out = nullptr;
+  cudaEvent_t ev_h2d[8] = {}, ev_step[8] = {}, ev_chunk[8] = {};
   int mode = NRG_MODE_FAST;
   LaunchCfg cfg;
   bool use_graph = true;
@@ -293,10 +295,9 @@ cudaError_t enqueue_integrator(nrg_chem* h, const StepArgs& a, const LaunchCfg& 
                           h->d_queue, h->d_counters, s);
 }
 
-cudaError_t enqueue_step(nrg_chem* h, const StepArgs& a, cudaStream_t s) {
-  cudaError_t e = cudaMemsetAsync(h->d_counters, 0, sizeof(unsigned long long) * 8, s);
-  if (e != cudaSuccess) return e;
-  cudaEvent_t* ph = h->timing ? h->ph : nullptr;
+// The step's kernels on stream s, adding to the device counters; ph: the
+// phase events (or nullptr).
+cudaError_t enqueue_step_body(nrg_chem* h, const StepArgs& a, cudaStream_t s, cudaEvent_t* ph) {
   if (h->mode == NRG_MODE_SURROGATE)
     return nrg::surrogate_step(h->sur, a, h->cfg, h->d_queue, h->d_counters, s,
                                [h, ph](const StepArgs& fa, cudaStream_t fs) {
@@ -311,6 +312,12 @@ cudaError_t enqueue_step(nrg_chem* h, const StepArgs& a, cudaStream_t s) {
   cudaError_t e2 = enqueue_integrator(h, a, h->cfg, s);
   if (ph) cudaEventRecord(ph[3], s);
   return e2;
+}
+
+cudaError_t enqueue_step(nrg_chem* h, const StepArgs& a, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(h->d_counters, 0, sizeof(unsigned long long) * 8, s);
+  if (e != cudaSuccess) return e;
+  return enqueue_step_body(h, a, s, h->timing ? h->ph : nullptr);
 }
 
 // Runs the step on stream s, through a CUDA graph when enabled.
@@ -342,16 +349,63 @@ void release_tables(const nrg_chem* h) {
     if (o == h) o = nullptr;
 }
 
-int run_step(nrg_chem* h, const StepArgs& a, cudaStream_t s, nrg_chem_stats* stats) {
+// Tables in place, surrogate ready and its scratch sized for up to n cells.
+int step_prepare(nrg_chem* h, long n) {
   CK(h, use_tables(h));
   if (h->mode == NRG_MODE_SURROGATE) {
     if (!(h->mech.n() == 9 && h->mech.r() == 24))
       return fail(h, NRG_ERR_UNSUPPORTED, "the surrogate is built for the 9-species, 24-reaction mechanism");
     if (!nrg::surrogate_ready(h->sur))
       return fail(h, NRG_ERR_STATE, "surrogate mode selected but no trained model is loaded");
-    const std::string e = nrg::surrogate_reserve(h->sur, a.n);
+    const std::string e = nrg::surrogate_reserve(h->sur, n);
     if (!e.empty()) return fail(h, NRG_ERR_CUDA, e);
   }
+  return NRG_OK;
+}
+
+// After the step's work was queued on s between h->ev0 and h->ev1: waits for
+// it, fills stats (may be NULL) and checks the surrogate's error word.
+int step_finish(nrg_chem* h, cudaStream_t s, long n, nrg_chem_stats* stats) {
+  CK(h, cudaMemcpyAsync(h->h_counters, h->d_counters, sizeof(unsigned long long) * 8,
+                        cudaMemcpyDeviceToHost, s));
+  CK(h, cudaStreamSynchronize(s));
+  if (stats) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    std::memset(stats, 0, sizeof(*stats));
+    stats->cells = n;
+    stats->cells_active = (long long)h->h_counters[0];
+    stats->steps = (long long)h->h_counters[1];
+    stats->rhs_evals = (long long)h->h_counters[2];
+    stats->jacobians = (long long)h->h_counters[3];
+    stats->solves = (long long)h->h_counters[4];
+    stats->cells_bad = (long long)h->h_counters[5];
+    stats->cells_surrogate = (long long)h->h_counters[6];
+    stats->cells_fallback = (long long)h->h_counters[7];
+    if (h->mode == NRG_MODE_SURROGATE) stats->cells_active += stats->cells_surrogate;
+    stats->device_ms = ms;
+    if (h->timing) {
+      float p = 0.f;
+      if (h->mode == NRG_MODE_SURROGATE) {
+        cudaEventElapsedTime(&p, h->ev0, h->ph[1]);  // features + MLP (ph[1] = gate start)
+        stats->phase_ms[0] = p;
+        cudaEventElapsedTime(&p, h->ph[1], h->ph[2]);
+        stats->phase_ms[1] = p;
+      }
+      cudaEventElapsedTime(&p, h->ph[2], h->ph[3]);
+      stats->phase_ms[2] = p;
+    }
+  }
+  if (h->mode == NRG_MODE_SURROGATE) {
+    const std::string e = nrg::surrogate_check(h->sur, s);
+    if (!e.empty()) return fail(h, NRG_ERR_CUDA, e);
+  }
+  return NRG_OK;
+}
+
+int run_step(nrg_chem* h, const StepArgs& a, cudaStream_t s, nrg_chem_stats* stats) {
+  int rc = step_prepare(h, a.n);
+  if (rc) return rc;
   CK(h, cudaEventRecord(h->ev0, s));
   if (h->timing) {
     for (int i = 0; i < 4; ++i) CK(h, cudaEventRecord(h->ph[i], s));
@@ -384,41 +438,7 @@ int run_step(nrg_chem* h, const StepArgs& a, cudaStream_t s, nrg_chem_stats* sta
     if (e != cudaSuccess) return cuda_fail(h, e, "enqueue_step");
   }
   CK(h, cudaEventRecord(h->ev1, s));
-  CK(h, cudaMemcpyAsync(h->h_counters, h->d_counters, sizeof(unsigned long long) * 8,
-                        cudaMemcpyDeviceToHost, s));
-  CK(h, cudaStreamSynchronize(s));
-  if (stats) {
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
-    std::memset(stats, 0, sizeof(*stats));
-    stats->cells = a.n;
-    stats->cells_active = (long long)h->h_counters[0];
-    stats->steps = (long long)h->h_counters[1];
-    stats->rhs_evals = (long long)h->h_counters[2];
-    stats->jacobians = (long long)h->h_counters[3];
-    stats->solves = (long long)h->h_counters[4];
-    stats->cells_bad = (long long)h->h_counters[5];
-    stats->cells_surrogate = (long long)h->h_counters[6];
-    stats->cells_fallback = (long long)h->h_counters[7];
-    if (h->mode == NRG_MODE_SURROGATE) stats->cells_active += stats->cells_surrogate;
-    stats->device_ms = ms;
-    if (h->timing) {
-      float p = 0.f;
-      if (h->mode == NRG_MODE_SURROGATE) {
-        cudaEventElapsedTime(&p, h->ev0, h->ph[1]);  // features + MLP (ph[1] = gate start)
-        stats->phase_ms[0] = p;
-        cudaEventElapsedTime(&p, h->ph[1], h->ph[2]);
-        stats->phase_ms[1] = p;
-      }
-      cudaEventElapsedTime(&p, h->ph[2], h->ph[3]);
-      stats->phase_ms[2] = p;
-    }
-  }
-  if (h->mode == NRG_MODE_SURROGATE) {
-    const std::string e = nrg::surrogate_check(h->sur, s);
-    if (!e.empty()) return fail(h, NRG_ERR_CUDA, e);
-  }
-  return NRG_OK;
+  return step_finish(h, s, a.n, stats);
 }
 
 }  // namespace
@@ -493,9 +513,11 @@ extern "C" int nrg_chem_destroy(nrg_chem* h) {
   for (int i = 0; i < 4; ++i)
     if (h->ph[i]) cudaEventDestroy(h->ph[i]);
   if (h->stream) cudaStreamDestroy(h->stream);
-  if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
-  for (cudaEvent_t& e : h->ev_chunk)
-    if (e) cudaEventDestroy(e);
+  if (h->copy_in) cudaStreamDestroy(h->copy_in);
+  if (h->copy_out) cudaStreamDestroy(h->copy_out);
+  for (cudaEvent_t* arr : {h->ev_h2d, h->ev_step, h->ev_chunk})
+    for (int i = 0; i < 8; ++i)
+      if (arr[i]) cudaEventDestroy(arr[i]);
   delete h;
   return NRG_OK;
 }
@@ -614,15 +636,21 @@ extern "C" int nrg_chem_step(nrg_chem* h, double time_step, const nrg_field_desc
   if (!(time_step > 0.0)) return fail(h, NRG_ERR_ARG, "time_step must be > 0");
   int rc = ensure_staging(h, (size_t)n);
   if (rc) return rc;
-  if (!h->copy_stream) {
-    CK(h, cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
-    for (cudaEvent_t& e : h->ev_chunk) CK(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  if (!h->copy_in) {
+    CK(h, cudaStreamCreateWithFlags(&h->copy_in, cudaStreamNonBlocking));
+    CK(h, cudaStreamCreateWithFlags(&h->copy_out, cudaStreamNonBlocking));
+    for (cudaEvent_t* arr : {h->ev_h2d, h->ev_step, h->ev_chunk})
+      for (int i = 0; i < 8; ++i) CK(h, cudaEventCreateWithFlags(&arr[i], cudaEventDisableTiming));
   }
+  rc = step_prepare(h, n);
+  if (rc) return rc;
   // The interior is handled as rows along i (contiguous in the reference's
-  // column-major arrays); rows are split into chunks so that the host gather
-  // of chunk p + 1 overlaps the H2D copy of chunk p, and the host scatter of
-  // chunk p overlaps the D2H copy of chunk p + 1.  Each chunk's gather and
-  // scatter run on all host threads.
+  // column-major arrays), split into up to eight chunks of rows.  Per chunk:
+  // gather on all host threads into pinned staging, H2D on copy_in, the step
+  // on the compute stream, D2H on copy_out, scatter on all host threads.  The
+  // host gathers chunk p + 1 while chunk p is copied and stepped, copy_in runs
+  // ahead of the steps, and chunk p is copied out and scattered while later
+  // chunks are stepped.
   const long rowlen = cnt[0], nrow = cnt[1] * cnt[2];
   auto row_base = [&](long r) {
     const int j = f->lo[1] + (int)(r % cnt[1]), k = f->lo[2] + (int)(r / cnt[1]);
@@ -630,10 +658,18 @@ extern "C" int nrg_chem_step(nrg_chem* h, double time_step, const nrg_field_desc
   };
   const int P = (int)std::min<long>(8, nrow);
   const size_t rb = (size_t)rowlen * 8;
-  cudaStream_t s = h->stream, cs = h->copy_stream;
+  cudaStream_t s = h->stream, ci = h->copy_in, co = h->copy_out;
+  auto chunk_cells = [&](int p, long* c0, long* nc) {
+    const long r0 = nrow * p / P, r1 = nrow * (p + 1) / P;
+    *c0 = r0 * rowlen;
+    *nc = (r1 - r0) * rowlen;
+  };
+  CK(h, cudaMemsetAsync(h->d_counters, 0, sizeof(unsigned long long) * 8, s));
+  CK(h, cudaEventRecord(h->ev0, s));
   for (int p = 0; p < P; ++p) {
-    const long r0 = nrow * p / P, r1 = nrow * (p + 1) / P, c0 = r0 * rowlen, nc = (r1 - r0) * rowlen;
-    parallel_rows(r0, r1, [&](long r) {
+    long c0, nc;
+    chunk_cells(p, &c0, &nc);
+    parallel_rows(nrow * p / P, nrow * (p + 1) / P, [&](long r) {
       const long L = row_base(r), c = r * rowlen;
       std::memcpy(h->h_T + c, f->T + L, rb);
       std::memcpy(h->h_rho + c, f->rho + L, rb);
@@ -643,48 +679,48 @@ extern "C" int nrg_chem_step(nrg_chem* h, double time_step, const nrg_field_desc
         std::memset(h->h_bc + c, 0, (size_t)rowlen);
       for (int sp = 0; sp < N; ++sp) std::memcpy(h->h_Y + (size_t)sp * n + c, f->Y[sp] + L, rb);
     });
-    CK(h, cudaMemcpyAsync(h->d_T + c0, h->h_T + c0, nc * 8, cudaMemcpyHostToDevice, cs));
-    CK(h, cudaMemcpyAsync(h->d_rho + c0, h->h_rho + c0, nc * 8, cudaMemcpyHostToDevice, cs));
-    CK(h, cudaMemcpyAsync(h->d_bc + c0, h->h_bc + c0, nc, cudaMemcpyHostToDevice, cs));
+    CK(h, cudaMemcpyAsync(h->d_T + c0, h->h_T + c0, nc * 8, cudaMemcpyHostToDevice, ci));
+    CK(h, cudaMemcpyAsync(h->d_rho + c0, h->h_rho + c0, nc * 8, cudaMemcpyHostToDevice, ci));
+    CK(h, cudaMemcpyAsync(h->d_bc + c0, h->h_bc + c0, nc, cudaMemcpyHostToDevice, ci));
     for (int sp = 0; sp < N; ++sp)
       CK(h, cudaMemcpyAsync(h->d_Y + (size_t)sp * n + c0, h->h_Y + (size_t)sp * n + c0, nc * 8,
-                            cudaMemcpyHostToDevice, cs));
-  }
-  CK(h, cudaEventRecord(h->ev_in, cs));
-  CK(h, cudaStreamWaitEvent(s, h->ev_in, 0));
-  StepArgs a;
-  a.n = n;
-  a.ld = n;
-  a.dt = time_step;
-  a.T = h->d_T;
-  a.rho = h->d_rho;
-  a.Y = h->d_Y;
-  a.bc = h->d_bc;
-  a.Y_prod = h->d_Yp;
-  a.Y_prod2 = h->d_Yp2;
-  a.E_f_prod = h->d_Ef;
-  a.T_after = nullptr;
-  a.status = h->d_status;
-  a.mxstep = 10000;
-  a.mech = h->d_mech;
-  a.dt_cells = nullptr;
-  a.cell_list = nullptr;
-  a.n_list = 0;
-  a.n_list_dev = nullptr;
-  rc = run_step(h, a, s, stats);  // returns with the step finished
-  if (rc) return rc;
-  for (int p = 0; p < P; ++p) {
-    const long c0 = nrow * p / P * rowlen, nc = (nrow * (p + 1) / P - nrow * p / P) * rowlen;
+                            cudaMemcpyHostToDevice, ci));
+    CK(h, cudaEventRecord(h->ev_h2d[p], ci));
+    CK(h, cudaStreamWaitEvent(s, h->ev_h2d[p], 0));
+    StepArgs a;
+    a.n = nc;
+    a.ld = n;
+    a.dt = time_step;
+    a.T = h->d_T + c0;
+    a.rho = h->d_rho + c0;
+    a.Y = h->d_Y + c0;
+    a.bc = h->d_bc + c0;
+    a.Y_prod = h->d_Yp + c0;
+    a.Y_prod2 = h->d_Yp2 + c0;
+    a.E_f_prod = h->d_Ef + c0;
+    a.T_after = nullptr;
+    a.status = h->d_status + c0;
+    a.mxstep = 10000;
+    a.mech = h->d_mech;
+    a.dt_cells = nullptr;
+    a.cell_list = nullptr;
+    a.n_list = 0;
+    a.n_list_dev = nullptr;
+    const cudaError_t e = enqueue_step_body(h, a, s, nullptr);
+    if (e != cudaSuccess) return cuda_fail(h, e, "enqueue_step");
+    CK(h, cudaEventRecord(h->ev_step[p], s));
+    CK(h, cudaStreamWaitEvent(co, h->ev_step[p], 0));
     for (int sp = 0; sp < N; ++sp) {
       CK(h, cudaMemcpyAsync(h->h_Yp + (size_t)sp * n + c0, h->d_Yp + (size_t)sp * n + c0, nc * 8,
-                            cudaMemcpyDeviceToHost, cs));
+                            cudaMemcpyDeviceToHost, co));
       CK(h, cudaMemcpyAsync(h->h_Yp2 + (size_t)sp * n + c0, h->d_Yp2 + (size_t)sp * n + c0, nc * 8,
-                            cudaMemcpyDeviceToHost, cs));
+                            cudaMemcpyDeviceToHost, co));
     }
-    CK(h, cudaMemcpyAsync(h->h_Ef + c0, h->d_Ef + c0, nc * 8, cudaMemcpyDeviceToHost, cs));
-    CK(h, cudaMemcpyAsync(h->h_status + c0, h->d_status + c0, nc, cudaMemcpyDeviceToHost, cs));
-    CK(h, cudaEventRecord(h->ev_chunk[p], cs));
+    CK(h, cudaMemcpyAsync(h->h_Ef + c0, h->d_Ef + c0, nc * 8, cudaMemcpyDeviceToHost, co));
+    CK(h, cudaMemcpyAsync(h->h_status + c0, h->d_status + c0, nc, cudaMemcpyDeviceToHost, co));
+    CK(h, cudaEventRecord(h->ev_chunk[p], co));
   }
+  CK(h, cudaEventRecord(h->ev1, s));
   for (int p = 0; p < P; ++p) {
     CK(h, cudaEventSynchronize(h->ev_chunk[p]));
     parallel_rows(nrow * p / P, nrow * (p + 1) / P, [&](long r) {
@@ -699,7 +735,7 @@ extern "C" int nrg_chem_step(nrg_chem* h, double time_step, const nrg_field_desc
       }
     });
   }
-  return NRG_OK;
+  return step_finish(h, s, n, stats);
 }
 
 extern "C" int nrg_chem_autotune(nrg_chem* h, double time_step, long n, long ld, const double* T,
