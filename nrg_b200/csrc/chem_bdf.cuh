@@ -51,9 +51,7 @@ struct SmemStore {
   static constexpr int kKR = kKF + R;
   static constexpr int kZ = kKR + R;
   static constexpr int kZD = kZ + N;
-  static constexpr int kW = kZD + N;
-  // w (Jacobian-vector input) is used only by the FP32-LU refinement
-  static constexpr int kDoubles = kW + (sizeof(LUT) == 4 ? N : 0);
+  static constexpr int kDoubles = kZD + N;
   static constexpr int kBytesPerThread = kDoubles * 8 + N * N * (int)sizeof(LUT);
   using lut_t = LUT;
   static constexpr int kBS = BS;
@@ -69,7 +67,6 @@ struct SmemStore {
   __device__ __forceinline__ double& kr(int r) { return d[(kKR + r) * BS]; }
   __device__ __forceinline__ double& z(int k) { return d[(kZ + k) * BS]; }
   __device__ __forceinline__ double& zd(int k) { return d[(kZD + k) * BS]; }
-  __device__ __forceinline__ double& w(int k) { return d[(kW + k) * BS]; }
   __device__ __forceinline__ LUT& a(int j, int i) { return f[(j * N + i) * BS]; }  // A(i+1, j+1)
 };
 
@@ -341,39 +338,6 @@ __device__ void analytic_iteration_matrix(CS& c, double factor) {
   }
 #pragma unroll
   for (int i = 0; i < N; ++i) c.a(i, i) += 1;
-}
-
-// out = J v at z (analytic; used for the FP64 residual of the mixed solve).
-// v is read from c.w, out accumulated into c.zd.
-template <int N, int R, class CS>
-__device__ void jac_vec(CS& c) {
-#pragma unroll
-  for (int k = 0; k < N; ++k) c.zd(k) = 0.0;
-#pragma unroll 1
-  for (int r = 0; r < R; ++r) {
-    const int nl = c_mech.nl[r], nr = c_mech.nr[r], nu = c_mech.nupd[r];
-    double dq = 0.0;
-    for (int side = 0; side < 2; ++side) {
-      const int cnt = side ? nr : nl;
-      const double k = side ? -c.kr(r) : c.kf(r);
-      for (int p = 0; p < cnt; ++p) {
-        const int sp = side ? c_mech.right[r][p] : c_mech.left[r][p];
-        if (sp < 0) continue;
-        double d = k;
-        for (int q = 0; q < cnt; ++q) {
-          if (q == p) continue;
-          const int sq = side ? c_mech.right[r][q] : c_mech.left[r][q];
-          if (sq >= 0) d = d * c.z(sq);
-        }
-        dq = dq + d * c.w(sp);
-      }
-    }
-    for (int u = 0; u < nu; ++u) {
-      const int k2 = c_mech.upd_k[r][u];
-      if (c_mech.upd_prod[r][u]) c.zd(k2) += dq;
-      else c.zd(k2) -= dq;
-    }
-  }
 }
 
 // dnrm2.f90:75-162, Lawson-Hanson scaled two-norm, restated as a per-element
@@ -697,9 +661,11 @@ __device__ void ddpst(CS& c) {
   if (info != 0) c.ier = 1;
 }
 
-// Corrector solve (DDCOR MITER=2, IMPL=0, ddcor.f90:61-107).  With float LU
-// factors the solve is followed by one step of iterative refinement whose
-// residual b - (I - h l0 J) x is formed in FP64 with an analytic J v.
+// Corrector solve (DDCOR MITER=2, IMPL=0, ddcor.f90:61-107).  The right-hand
+// side (the corrector residual) is always formed in FP64 from FP64 state; with
+// float LU factors (mixed mode) the chord iteration that calls this solve
+// until the FP64 convergence test passes is itself the iterative refinement of
+// the FP32 solution, so no further sweep is made per solve.
 template <int N, int R, typename LUT, class CS>
 __device__ double ddcor(CS& c) {
   double b[N];
@@ -709,22 +675,6 @@ __device__ double ddcor(CS& c) {
 #pragma unroll
   for (int i = 0; i < N; ++i) x[i] = b[i];
   dgesl<N>(c, x);
-  if (sizeof(LUT) == 4) {
-    const double el1h = EL(1, c.nq) * c.h;
-#pragma unroll
-    for (int k = 0; k < N; ++k) {
-      c.z(k) = c.y[k];
-      c.w(k) = x[k];
-    }
-    jac_vec<N, R>(c);
-    double r[N];
-#pragma unroll
-    for (int i = 0; i < N; ++i) r[i] = b[i] - (x[i] - el1h * c.zd(i));
-    dgesl<N>(c, r);
-#pragma unroll
-    for (int i = 0; i < N; ++i) x[i] = x[i] + r[i];
-    c.nsolve += 1;
-  }
   c.nsolve += 1;
 #pragma unroll
   for (int i = 0; i < N; ++i) {
