@@ -3,7 +3,7 @@
 
 Workload (default): the 2048 x 2048 premixed-flame field (4,194,304 cells,
 dt = 1e-6 s, p = 1 atm) of the H2/air KEROMNES mechanism, synthetic and seeded
-(nrg_b200/fields.py: config4).  A step is one chemistry step over the whole
+(nrg_b200/fields.py: flame_field).  A step is one chemistry step over the whole
 field.  Inputs (370 MB of FP64 state) are larger than the 126 MB L2, so no
 flush is needed between steps.
 
@@ -207,7 +207,7 @@ def cpu_baseline(field, W, decks, seconds: float, units: str = "cal.mol") -> dic
     m.chem_step(samp.dt, samp.T, samp.rho, samp.Y, threads=cores)
     dt = time.perf_counter() - t0
     return {"value": n / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{n} cells drawn uniformly (seeded) from the {field.name} field "
+            "sample": f"{n} cells drawn uniformly (seeded) from the {field.name.replace('_', ' ')} "
                       f"({dt:.1f} s, OpenMP dynamic schedule)"}
 
 
@@ -228,7 +228,7 @@ def run_reference(args):
     from nrg_b200.chemistry import mechanism_tables
     decks = keromnes_paths()
     W = mechanism_tables(*decks)["molar_mass"]
-    field = F.config4(W, n_side=args.n_side)
+    field = F.flame_field(W, n_side=args.n_side)
     from oracle import oracle_py as op
     m = op.Mechanism(*decks, 1.0, "cal.mol")
     cores = os.cpu_count() or 1
@@ -379,7 +379,7 @@ def main():
     W = tables["molar_mass"]
     dev = torch.device("cuda", local)
     solver = ChemicalKineticsSolver(None, *decks, E_act_units=units, mode="fast")
-    field = F.config4(mechanism_tables(*keromnes_paths())["molar_mass"], n_side=args.n_side)
+    field = F.flame_field(mechanism_tables(*keromnes_paths())["molar_mass"], n_side=args.n_side)
     if args.mechanism == "ACETYLENE":
         # the same flame geometry with the C2H2/O2/Ar mixture
         field = F.acetylene_flame(solver.species_names[:tables["n_species"]], W, n_side=args.n_side)

@@ -84,15 +84,15 @@ def random_state(n: int, rng: np.random.Generator, W: np.ndarray, T_lo: float, T
     return T, p, Y
 
 
-def config0(W: np.ndarray, n_side: int = 64) -> Field:
+def random_field(W: np.ndarray, n_side: int = 64) -> Field:
     """4,096 cells, T ~ U[1000, 2400] K, p = 1 atm, dt = 1e-6 s."""
     rng = np.random.Generator(np.random.PCG64(0))
     n = n_side * n_side
     T, p, Y = random_state(n, rng, W, 1000.0, 2400.0)
-    return _finish("config0", T, p, Y, W, 1e-6, (n_side, n_side))
+    return _finish("random_field", T, p, Y, W, 1e-6, (n_side, n_side))
 
 
-def config1(W: np.ndarray, n_side: int = 512) -> Field:
+def ignition_field(W: np.ndarray, n_side: int = 512) -> Field:
     """262,144 cells, dt = 1e-5 s; 20 % of cells within +-50 K of the
     temperature whose ignition delay is 1e-5 s (uneven substep counts)."""
     rng = np.random.Generator(np.random.PCG64(1))
@@ -100,28 +100,28 @@ def config1(W: np.ndarray, n_side: int = 512) -> Field:
     T, p, Y = random_state(n, rng, W, 1000.0, 2400.0)
     hot = rng.uniform(0.0, 1.0, n) < 0.2
     T[hot] = T_IGNITION_1E5 + rng.uniform(-50.0, 50.0, int(hot.sum()))
-    return _finish("config1", T, p, Y, W, 1e-5, (n_side, n_side))
+    return _finish("ignition_field", T, p, Y, W, 1e-5, (n_side, n_side))
 
 
-def config2(W: np.ndarray, n_side: int = 1024, seed: int = 2) -> Field:
+def wide_range_field(W: np.ndarray, n_side: int = 1024, seed: int = 2) -> Field:
     """1,048,576 cells, T ~ U[800, 2600] K, p ~ U[0.5, 5] atm, dt = 1e-5 s."""
     rng = np.random.Generator(np.random.PCG64(seed))
     n = n_side * n_side
     T, p, Y = random_state(n, rng, W, 800.0, 2600.0, 0.5, 5.0)
-    return _finish("config2", T, p, Y, W, 1e-5, (n_side, n_side))
+    return _finish("wide_range_field", T, p, Y, W, 1e-5, (n_side, n_side))
 
 
-def config3_pairs(W: np.ndarray, n: int, seed: int = 3, coupled: float = 0.0, T_lo: float = 800.0) -> Field:
-    """Training states: the config-2 distribution with dt ~ log-U[1e-7, 1e-5]
+def training_states(W: np.ndarray, n: int, seed: int = 3, coupled: float = 0.0, T_lo: float = 800.0) -> Field:
+    """Training states: the wide-range distribution with dt ~ log-U[1e-7, 1e-5]
     (radicals shared in a fraction `coupled` of the states; T_lo < 800 K
     widens the temperature range down to a flame's preheat zone)."""
     rng = np.random.Generator(np.random.PCG64(seed))
     T, p, Y = random_state(n, rng, W, T_lo, 2600.0, 0.5, 5.0, coupled)
     dts = 10.0 ** rng.uniform(-7.0, -5.0, n)
-    return _finish("config3", T, p, Y, W, float("nan"), (n,), dts)
+    return _finish("training_states", T, p, Y, W, float("nan"), (n,), dts)
 
 
-def config4(W: np.ndarray, n_side: int = 2048, seed: int = 4) -> Field:
+def flame_field(W: np.ndarray, n_side: int = 2048, seed: int = 4) -> Field:
     """Premixed-flame-like field: 2048 x 2048 cells of 10 um, tanh front
     (delta = 0.5 mm) from 300 K to 2400 K along x, front position perturbed in
     y by 8 seeded sinusoids of amplitude 0.2 mm, radicals Gaussian at the front
@@ -132,11 +132,11 @@ def config4(W: np.ndarray, n_side: int = 2048, seed: int = 4) -> Field:
     for sp in RADICALS:
         Y[idx[sp]] = 1e-3 * g
     n = n_side * n_side
-    return _finish("config4", T, np.full(n, P_ATM), Y, W, 1e-6, (n_side, n_side))
+    return _finish("flame_field", T, np.full(n, P_ATM), Y, W, 1e-6, (n_side, n_side))
 
 
 def _flame_geometry(n_side: int, seed: int):
-    """Flat (T, progress c, front Gaussian g) of the config-4 geometry."""
+    """Flat (T, progress c, front Gaussian g) of the flame geometry."""
     rng = np.random.Generator(np.random.PCG64(seed))
     dx = 10e-6
     delta = 0.5e-3
@@ -181,7 +181,7 @@ def acetylene_state(names, W: np.ndarray, n: int, seed: int = 0, T_lo: float = 1
 
 
 def acetylene_flame(names, W: np.ndarray, n_side: int = 2048, seed: int = 4) -> Field:
-    """The config-4 flame geometry with the C2H2/O2/Ar mixture: same
+    """The flame flame geometry with the C2H2/O2/Ar mixture: same
     temperature field, reactants to products along the front, radicals
     Gaussian at the front with peak mass fraction 1e-4."""
     T, c, g = _flame_geometry(n_side, seed)
@@ -237,7 +237,7 @@ class PredictorBlock:
 
 def predictor_block(W: np.ndarray, dims: int, n_cells, seed: int = 0, coord: int = 0, dx: float = 10e-6,
                     dt: float = 1e-7, bc_fraction: float = 0.02, zero_face_fraction: float = 0.05) -> PredictorBlock:
-    """A flame front along x (as the config-4 field: tanh profile from 300 K
+    """A flame front along x (as the flame field: tanh profile from 300 K
     to 2400 K, radicals Gaussian at the front) on a block with its ghost
     layer, plus seeded face velocities of both signs (some exactly zero),
     diffusion and chemistry sources of the size the step produces, and a few

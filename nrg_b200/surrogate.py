@@ -145,7 +145,7 @@ class PrepareOpts(ctypes.Structure):
 
 # Training recipe (the defaults of training_pairs / train_default).
 # The gate thresholds (elem_tol, raw_elem_tol, dT_tol, dT_max) were chosen on
-# a validation flame field (config4 geometry, seed 5) as the widest setting
+# a validation flame field (flame_field geometry, seed 5) as the widest setting
 # whose accepted cells stay within 0.8 K and 8e-5 of the FP64 result.
 RECIPE = dict(n_train=4_000_000, epochs=150, batch=4096, lr=2e-3, coupled=0.5, hull_margin=0.02, dt_pow=1.0,
               log_mask=0, log_eps=1e-7, common_dY_scale=0, T_lo=800.0,
@@ -157,10 +157,10 @@ def training_pairs(solver: ChemicalKineticsSolver, W: np.ndarray, n: int, seed: 
                    coupled: float = RECIPE["coupled"], log_mask: int = RECIPE["log_mask"],
                    log_eps: float = RECIPE["log_eps"], common_dY_scale: int = RECIPE["common_dY_scale"],
                    T_lo: float = RECIPE["T_lo"]):
-    """Integrates n config-3 states with their own dt (FP64 integrator) and
+    """Integrates n training states with their own dt (FP64 integrator) and
     returns standardised (x_bf16, y) device tensors plus timing."""
     import torch
-    f = fields.config3_pairs(W, n, seed=seed, coupled=coupled, T_lo=T_lo)
+    f = fields.training_states(W, n, seed=seed, coupled=coupled, T_lo=T_lo)
     # neighbouring lanes take similar paths when states are sorted by (dt, T)
     order = np.lexsort((f.T, np.round(np.log10(f.dt_cells) * 8)))
     f = fields.Field(f.name, f.T[order], f.rho[order], f.p[order], np.ascontiguousarray(f.Y[:, order]), f.dt,

@@ -1,7 +1,7 @@
 """One rank of the two-process CPU test of the multi-process plumbing
 (launched by tests/test_dist.py through torch.distributed.run, gloo).
 
-Each rank steps its own block of rows of the 64 x 64 config-0 field with the
+Each rank steps its own block of rows of the 64 x 64 4,096-cell random field with the
 oracle and writes its block; rank 0 also records the max-over-ranks value."""
 import os
 import sys
@@ -19,7 +19,7 @@ def main(out_dir: str) -> int:
     rank, world, _ = dist.world()
     dist.init("gloo", timeout_s=120)
     m = op.Mechanism(*keromnes_paths(), 1.0, "cal.mol")
-    f = fields.config0(m.tables()["molar_mass"])
+    f = fields.random_field(m.tables()["molar_mass"])
     side = f.shape[0]
     r0, r1 = dist.row_block(side, rank, world)
     sel = np.arange(r0 * side, r1 * side)

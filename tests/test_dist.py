@@ -42,7 +42,7 @@ def test_two_gloo_ranks_step_disjoint_rows(tmp_path, oracle_mech, W):
     r = subprocess.run(cmd, cwd=ROOT, env=env, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     got = np.concatenate([np.load(tmp_path / f"rank{k}.npy") for k in range(2)], axis=1)
-    f = fields.config0(W)
+    f = fields.random_field(W)
     ref = oracle_mech.chem_step(f.dt, f.T, f.rho, f.Y, threads=1)["Y_prod"]
     np.testing.assert_array_equal(got, ref)
     assert float((tmp_path / "max.txt").read_text()) == 2.0

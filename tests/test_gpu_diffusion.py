@@ -1,5 +1,5 @@
 """nrg_mixture_diffusivity_device (calculate_diffusivity_coeff,
-fickean_diffusion_solver.f90:358-395) against the oracle on the config-2
+fickean_diffusion_solver.f90:358-395) against the oracle on the wide-range
 state distribution (T ~ U[800, 2600] K, p ~ U[0.5, 5] atm) for the four
 reference mechanisms.  Tolerance: 1e-12 relative per coefficient (the device
 and host pow / exp may differ in the last bit; the rest of the arithmetic is
@@ -25,7 +25,7 @@ def test_diffusivity_matches_oracle(name):
     try:
         s.load_transport(transport_path(name))
         W9 = mechanism_tables(*mechanism_paths("KEROMNES"))["molar_mass"]
-        base = fields.slice_field(fields.config2(W9, n_side=128), 8192, stride=2)
+        base = fields.slice_field(fields.wide_range_field(W9, n_side=128), 8192, stride=2)
         f = fields.state_for_species(base, s.species_names, W)
         mm = 1.0 / np.sum(f.Y / W[:, None], axis=0)
         bc = (np.arange(f.n) % 97 == 5).astype(np.int8)

@@ -38,8 +38,8 @@ def check_parity(g, o, f, active):
 
 
 @pytest.mark.parametrize("mode", ["reference", "fast"])
-def test_config0_parity(solver, oracle_mech, W, mode):
-    f = fields.config0(W)
+def test_random_field_parity(solver, oracle_mech, W, mode):
+    f = fields.random_field(W)
     o = oracle_run(oracle_mech, f)
     g, st = run_device(solver, f, mode)
     assert np.all(g["status"] == 1)
@@ -51,8 +51,8 @@ def test_config0_parity(solver, oracle_mech, W, mode):
         assert abs(st["rhs_evals"] - o["nfe"].sum()) <= 0.01 * o["nfe"].sum()
 
 
-def test_config1_sample_parity(solver, oracle_mech, W):
-    f = fields.slice_field(fields.config1(W, n_side=128), 2048, stride=7)
+def test_ignition_field_sample_parity(solver, oracle_mech, W):
+    f = fields.slice_field(fields.ignition_field(W, n_side=128), 2048, stride=7)
     o = oracle_run(oracle_mech, f)
     for mode in ("reference", "fast"):
         g, _ = run_device(solver, f, mode)
@@ -60,7 +60,7 @@ def test_config1_sample_parity(solver, oracle_mech, W):
 
 
 def test_launch_shapes_and_graph_agree(solver, W):
-    f = fields.config0(W)
+    f = fields.random_field(W)
     base, _ = run_device(solver, f, "fast", launch=dict(kernel="warp_queue", block=256))
     for launch in (dict(kernel="warp_queue", block=128, grid=0, chunk=1),
                    dict(kernel="warp_queue", block=256, grid=296, chunk=4),
@@ -75,7 +75,7 @@ def test_launch_shapes_and_graph_agree(solver, W):
 @pytest.mark.parametrize("kernel,block", [("thread", 64), ("thread", 32), ("thread_queue", 64),
                                           ("thread_queue", 32)])
 def test_thread_per_cell_kernels_parity(solver, oracle_mech, W, kernel, block):
-    f = fields.slice_field(fields.config0(W), 1024)
+    f = fields.slice_field(fields.random_field(W), 1024)
     o = oracle_run(oracle_mech, f)
     for mode in ("reference", "fast"):
         g, _ = run_device(solver, f, mode, launch=dict(kernel=kernel, block=block, grid=0, chunk=1))
@@ -85,7 +85,7 @@ def test_thread_per_cell_kernels_parity(solver, oracle_mech, W, kernel, block):
 
 def test_thread_block_sizes_give_identical_results(solver, W):
     """Per-cell arithmetic does not depend on the block shape."""
-    f = fields.slice_field(fields.config1(W, n_side=128), 4000, stride=3)
+    f = fields.slice_field(fields.ignition_field(W, n_side=128), 4000, stride=3)
     outs = [run_device(solver, f, "fast", launch=dict(kernel=k, block=b, grid=0, chunk=1))[0]
             for k, b in (("thread", 64), ("thread", 32), ("thread_queue", 32))]
     for g in outs[1:]:
@@ -95,7 +95,7 @@ def test_thread_block_sizes_give_identical_results(solver, W):
 
 
 def test_skip_rule_bc_and_untouched_y_prod2(solver, oracle_mech, W):
-    f = fields.slice_field(fields.config0(W), 1024)
+    f = fields.slice_field(fields.random_field(W), 1024)
     f.T[:32] = 300.0
     bc = np.zeros(f.n, np.int8)
     bc[32:64] = 1
@@ -112,7 +112,7 @@ def test_skip_rule_bc_and_untouched_y_prod2(solver, oracle_mech, W):
 
 def test_empty_and_nonfinite_inputs(solver, W):
     import torch
-    f = fields.slice_field(fields.config0(W), 256)
+    f = fields.slice_field(fields.random_field(W), 256)
     z = torch.zeros((9, 0), dtype=torch.float64, device="cuda")
     e = torch.zeros(0, dtype=torch.float64, device="cuda")
     st = solver.step_device(1e-6, e, e, z, z, z, e)
@@ -126,7 +126,7 @@ def test_empty_and_nonfinite_inputs(solver, W):
 def test_host_layout_drop_in(decks, oracle_mech, W):
     """solve_chemical_kinetics on Fortran-layout host arrays with ghost cells."""
     from nrg_b200.chemistry import DataManager, chemical_kinetics_solver_c
-    f = fields.config0(W)
+    f = fields.random_field(W)
     nx, ny = f.shape
     m = DataManager.block(nx, ny)
     T = m.create_scalar_field("temperature")
@@ -153,12 +153,12 @@ def test_host_layout_drop_in(decks, oracle_mech, W):
     s.close()
 
 
-def test_mixed_precision_config2_error_per_species(solver, oracle_mech, W):
+def test_mixed_precision_wide_range_error_per_species(solver, oracle_mech, W):
     """Config 2 (T ~ U[800, 2600] K, p ~ U[0.5, 5] atm, dt = 1e-5 s): the FP32
     LU with FP64 residual and one refinement sweep against the FP64 oracle,
     reported per species.  The Newton matrix only steers the chord
     iteration, so the converged step keeps the FP64 path's accuracy."""
-    f = fields.slice_field(fields.config2(W, n_side=128), 4096, stride=3)
+    f = fields.slice_field(fields.wide_range_field(W, n_side=128), 4096, stride=3)
     o = oracle_run(oracle_mech, f)
     rows = []
     for mode in ("fast", "mixed"):
@@ -180,7 +180,7 @@ def test_specialised_code_gives_the_table_driven_bits(decks, W, mode):
     """The generated straight-line RHS / iteration matrix and the table walk
     perform the same operations in the same order."""
     from nrg_b200.chemistry import ChemicalKineticsSolver
-    f = fields.slice_field(fields.config1(W, n_side=128), 4000, stride=3)
+    f = fields.slice_field(fields.ignition_field(W, n_side=128), 4000, stride=3)
     s = ChemicalKineticsSolver(None, *decks, mode=mode)
     try:
         outs = []
@@ -202,7 +202,7 @@ def test_other_mechanisms_specialised_code_gives_the_table_driven_bits(name):
     paths = mechanism_paths(name)
     s = ChemicalKineticsSolver(None, *paths, mode="fast")
     try:
-        base = fields.slice_field(fields.config1(fields_W(), n_side=128), 2000, stride=5)
+        base = fields.slice_field(fields.ignition_field(fields_W(), n_side=128), 2000, stride=5)
         f = fields.state_for_species(base, s.species_names, mechanism_tables(*paths)["molar_mass"])
         outs = []
         for spec in (True, False):
@@ -228,7 +228,7 @@ def test_other_reference_mechanisms_parity(name):
     om = op.Mechanism(*paths, 1.0, "cal.mol")
     W = om.tables()["molar_mass"]
     names = om.species()[:om.n_species]
-    base = fields.slice_field(fields.config0(fields_W()), 1024)
+    base = fields.slice_field(fields.random_field(fields_W()), 1024)
     f = fields.state_for_species(base, names, W)
     o = oracle_run(om, f)
     s = ChemicalKineticsSolver(None, *paths, mode="reference")

@@ -40,7 +40,7 @@ def _device_state(solver, f, E, v, T0, bc=None, Y_prod=None, E_f_prod=None):
 
 
 def test_state_equation_matches_oracle(solver, oracle_mech, W):
-    f = fields.slice_field(fields.config2(W, n_side=64), 3000)
+    f = fields.slice_field(fields.wide_range_field(W, n_side=64), 3000)
     rng = np.random.default_rng(8)
     v = rng.uniform(-500.0, 500.0, (3, f.n))
     E = _energy_per_mass(oracle_mech, f.T, f.Y, W, v)
@@ -56,7 +56,7 @@ def test_state_equation_matches_oracle(solver, oracle_mech, W):
 def test_chemistry_step_then_state_update_on_device(solver, oracle_mech, W):
     """Step, then sources + state equation, all on the device, against the
     oracle chain; bc cells untouched."""
-    f = fields.slice_field(fields.config0(W), 2048)
+    f = fields.slice_field(fields.random_field(W), 2048)
     bc = np.zeros(f.n, np.int8)
     bc[100:140] = 1
     g_step, _ = run_device(solver, f, "fast", bc=bc)

@@ -93,7 +93,7 @@ def fitted(solver, sur, W):
 
 
 def test_fused_inference_matches_unfused_and_cpu(fitted, W):
-    f = fields.slice_field(fields.config0(W), 2000)  # 15 full 128-cell tiles and a ragged one
+    f = fields.slice_field(fields.random_field(W), 2000)  # 15 full 128-cell tiles and a ragged one
     out_tc = fitted.infer(f).cpu().numpy()
     xb, _ = fitted.features(f, xraw=False)
     out_gemm = fitted.forward(xb).cpu().numpy()
@@ -105,7 +105,7 @@ def test_fused_inference_matches_unfused_and_cpu(fitted, W):
 
 
 def test_fused_step_matches_unfused_step(solver, fitted, W):
-    f = fields.slice_field(fields.config0(W), 3000)
+    f = fields.slice_field(fields.random_field(W), 3000)
     f.T[:40] = 300.0
     f.T[1000:2000] = 700.0  # below the training hull (T >= 800 K less 2 %): FP64 fallback
     bc = np.zeros(f.n, np.int8)
@@ -143,7 +143,7 @@ def test_trained_network_gain_on_flame_rows(decks, W):
     FP64 result, fallback cells bit-identical to it."""
     from nrg_b200.chemistry import ChemicalKineticsSolver
     from nrg_b200.surrogate import DEFAULT_MODEL, RECIPE, Surrogate
-    full = fields.config4(W)
+    full = fields.flame_field(W)
     f = fields.slice_field(full, 128 * 2048, offset=960 * 2048)
     s = ChemicalKineticsSolver(None, *decks, mode="fast")
     try:

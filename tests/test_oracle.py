@@ -116,7 +116,7 @@ def _numpy_rhs(t, z, kf, kr, mc):
 
 def test_rates_and_rhs_independent_restatement(oracle_mech, W):
     t = oracle_mech.tables()
-    f = fields.config0(W)
+    f = fields.random_field(W)
     for c in range(0, f.n, 397):
         C0 = f.Y[:, c] * f.rho[c] / W
         mc = np.array([np.sum(C0 * t["eff"][r]) for r in range(24)])
@@ -132,7 +132,7 @@ def test_rates_and_rhs_independent_restatement(oracle_mech, W):
 def test_oracle_against_scipy_bdf(oracle_mech, W):
     from scipy.integrate import solve_ivp
     t = oracle_mech.tables()
-    f = fields.config0(W)
+    f = fields.random_field(W)
     sel = np.arange(0, f.n, 256)
     out = oracle_mech.chem_step(f.dt, f.T[sel], f.rho[sel], f.Y[:, sel])
     for j, c in enumerate(sel):
@@ -147,7 +147,7 @@ def test_oracle_against_scipy_bdf(oracle_mech, W):
 
 
 def test_oracle_conservation_and_skip_rule(oracle_mech, W):
-    f = fields.config0(W)
+    f = fields.random_field(W)
     n = 512
     T = f.T[:n].copy()
     T[:8] = 300.0  # below the 305 K threshold
@@ -169,13 +169,13 @@ def test_oracle_conservation_and_skip_rule(oracle_mech, W):
 
 
 def test_oracle_mxstep_flag(oracle_mech, W):
-    f = fields.config0(W)
+    f = fields.random_field(W)
     out = oracle_mech.chem_step(f.dt, f.T[:64], f.rho[:64], f.Y[:, :64], mxstep=5)
     assert np.all(out["nstate"] == 3) and np.all(out["nstep"] == 5)
 
 
 def test_energy_closure_round_trip(oracle_mech, W):
-    f = fields.config0(W)
+    f = fields.random_field(W)
     n = 64
     zero = np.zeros((9, n))
     T1 = oracle_mech.temperature_after(f.dt, f.T[:n], f.rho[:n], f.Y[:, :n], zero, np.zeros(n))
@@ -202,7 +202,7 @@ def test_state_equation_recovers_temperature(oracle_mech, W):
     """apply_state_equation inverts the energy of a known state: T back to
     the Newton tolerance, p = rho R T / W_mix, gamma and v_s consistent."""
     from nrg_b200 import fields
-    f = fields.slice_field(fields.config0(W), 256)
+    f = fields.slice_field(fields.random_field(W), 256)
     rng = np.random.default_rng(5)
     v = rng.uniform(-300.0, 300.0, (2, f.n))
     E = _energy_per_mass(oracle_mech, f.T, f.Y, W, v)
@@ -220,7 +220,7 @@ def test_state_equation_applies_the_chemistry_sources(oracle_mech, W):
     """Y += Y_prod dt / rho and E_f += E_f_prod dt / rho before the state
     equation; bc cells untouched."""
     from nrg_b200 import fields
-    f = fields.slice_field(fields.config0(W), 64)
+    f = fields.slice_field(fields.random_field(W), 64)
     o = oracle_mech.chem_step(f.dt, f.T, f.rho, f.Y)
     E = _energy_per_mass(oracle_mech, f.T, f.Y, W, np.zeros((0, f.n)))
     bc = np.zeros(f.n, np.int8)
