@@ -289,3 +289,52 @@ def _dev_out(f):
     d = torch.device("cuda")
     Y = torch.zeros((f.Y.shape[0], f.n), dtype=torch.float64, device=d)
     return Y, torch.zeros_like(Y), torch.zeros(f.n, dtype=torch.float64, device=d)
+
+
+@pytest.mark.parametrize("shape", [(37, 5, 3), (3, 1, 1), (11, 13, 1)])
+def test_host_layout_shapes_match_the_device_step(decks, W, shape):
+    """The host path (row chunks gathered, copied, stepped and scattered in
+    overlap) on 3-D, single-row and few-row blocks with bc cells gives the
+    device path's bits, leaves ghost cells alone and keeps Y_prod2 in
+    skipped cells."""
+    from nrg_b200.chemistry import ChemicalKineticsSolver, DataManager, chemical_kinetics_solver_c
+    nx, ny, nz = shape
+    n = nx * ny * nz
+    f = fields.slice_field(fields.ignition_field(W, n_side=64), n, stride=3)
+    bc_flat = (np.arange(n) % 7 == 3).astype(np.int8)
+    m = DataManager.block(nx, ny, nz)
+    T = m.create_scalar_field("temperature")
+    m.create_scalar_field("pressure")
+    rho = m.create_scalar_field("density")
+    Y = m.create_vector_field("specie_mass_fraction", 9)
+    bc = np.full(m.shape, 5, np.int8, order="F")
+    m.fields["bc_markers"] = bc
+    cube = lambda a: a.reshape(nz, ny, nx).transpose(2, 1, 0)  # cell order: i fastest, then j, then k
+    m.interior(T)[...] = cube(f.T)
+    m.interior(rho)[...] = cube(f.rho)
+    m.interior(bc)[...] = cube(bc_flat)
+    for k in range(9):
+        m.interior(Y[k])[...] = cube(f.Y[k])
+    s = chemical_kinetics_solver_c(m, *decks, mode="fast")
+    for k in range(9):
+        m.fields["specie_production_chemistry2"][k][...] = -1.0
+    s.set_launch(kernel="thread", block=32, grid=0, chunk=1)
+    st = s.solve_chemical_kinetics(f.dt)
+    s.close()
+    assert st["cells"] == n
+    d = ChemicalKineticsSolver(None, *decks, mode="fast")
+    try:
+        g, _ = run_device(d, f, "fast", bc=bc_flat, launch=dict(kernel="thread", block=32, grid=0, chunk=1),
+                          y_prod2_init=np.full((9, n), -1.0))
+    finally:
+        d.close()
+    flat = lambda a: m.interior(a).transpose(2, 1, 0).reshape(-1)
+    yp = np.stack([flat(a) for a in m.fields["specie_production_chemistry"]])
+    yp2 = np.stack([flat(a) for a in m.fields["specie_production_chemistry2"]])
+    np.testing.assert_array_equal(yp, g["Y_prod"])
+    np.testing.assert_array_equal(yp2, g["Y_prod2"])
+    np.testing.assert_array_equal(flat(m.fields["energy_production_chemistry"]), g["E_f_prod"])
+    assert np.all(yp2[:, bc_flat != 0] == -1.0)
+    ghost = np.ones(m.shape, bool)
+    ghost[tuple(slice(lo - l, hi - l + 1) for lo, hi, l in zip(m.lo, m.hi, m.lb))] = False
+    assert np.all(m.fields["specie_production_chemistry2"][0][ghost] == -1.0)
