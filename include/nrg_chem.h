@@ -277,6 +277,13 @@ NRG_API int nrg_mech_tables(const char* mechanism_path, const char* thermo_path,
                             int* coeffs, double* arrhenius, double* troe3, double* eff,
                             double* a_coeffs, double* molar_mass);
 
+/* Failure-handling self test (no counterpart in the reference): one warp
+ * waits, with the bounded mbarrier wait that every wait of the tensor-core
+ * kernel uses, on a barrier that nothing arrives at; the wait gives up after
+ * limit_ns (at most 2 s), *timed_out is set to 1 and waited_ms (may be NULL)
+ * to the time waited, and the context stays usable. */
+NRG_API int nrg_selftest_bounded_wait(long long limit_ns, int* timed_out, double* waited_ms);
+
 /* Message of the last failing call on this handle (or of the last failing
  * nrg_chem_create when h is NULL). */
 NRG_API const char* nrg_chem_last_error(nrg_chem* h);

@@ -114,6 +114,7 @@ SIGNATURES = {
     "nrg_chem_integrate": (_I, [_VP, _L, _L, _D, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP,
                                 ctypes.POINTER(Stats)]),
     "nrg_fp64_peak_tflops": (_I, [ctypes.POINTER(_D)]),
+    "nrg_selftest_bounded_wait": (_I, [ctypes.c_longlong, ctypes.POINTER(_I), ctypes.POINTER(_D)]),
     "nrg_chem_load_transport": (_I, [_VP, _CP]),
     "nrg_mech_transport_tables": (_I, [_CP] * 4 + [_VP] * 3),
     "nrg_mixture_diffusivity_device": (_I, [_VP, _L, _L] + [_VP] * 7),

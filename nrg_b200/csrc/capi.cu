@@ -1011,6 +1011,12 @@ extern "C" const char* nrg_chem_last_error(nrg_chem* h) {
   return h ? h->err.c_str() : g_create_error.c_str();
 }
 
+extern "C" int nrg_selftest_bounded_wait(long long limit_ns, int* timed_out, double* waited_ms) {
+  if (limit_ns <= 0 || limit_ns > 2000000000LL || !timed_out) return NRG_ERR_ARG;
+  const std::string e = nrg::bounded_wait_probe((unsigned long long)limit_ns, timed_out, waited_ms);
+  return e.empty() ? NRG_OK : fail(nullptr, NRG_ERR_CUDA, e);
+}
+
 extern "C" int nrg_fp64_peak_tflops(double* tflops) {
   if (!tflops) return NRG_ERR_ARG;
   int dev = 0, sms = 0;

@@ -1295,4 +1295,43 @@ cudaError_t surrogate_step(Surrogate* s, const StepArgs& a, const LaunchCfg& cfg
   return fallback(fa, st);
 }
 
+// Bounded-wait probe: one warp waits on an mbarrier that nothing arrives at,
+// with the same bounded wait the tensor-core kernel uses, and reports that the
+// wait gave up (and after how long) instead of hanging.
+__global__ void k_bounded_wait_probe(unsigned long long limit_ns, int* timed_out, unsigned long long* waited_ns) {
+  __shared__ __align__(8) unsigned long long bar;
+  const uint32_t mb = tc::smem_u32(&bar);
+  if (threadIdx.x == 0) tc::mbar_init(mb, 1);
+  __syncwarp();
+  const uint64_t t0 = tc::globaltimer_ns();
+  const bool ok = tc::mbar_wait(mb, 0, limit_ns);  // phase 0 never completes
+  const uint64_t t1 = tc::globaltimer_ns();
+  if (threadIdx.x == 0) {
+    *timed_out = ok ? 0 : 1;
+    *waited_ns = t1 - t0;
+  }
+}
+
+std::string bounded_wait_probe(unsigned long long limit_ns, int* timed_out, double* waited_ms) {
+  int* d_flag = nullptr;
+  unsigned long long* d_ns = nullptr;
+  std::string err;
+  if (cudaMalloc(&d_flag, sizeof(int)) != cudaSuccess || cudaMalloc(&d_ns, sizeof(unsigned long long)) != cudaSuccess)
+    err = "cudaMalloc";
+  if (err.empty()) {
+    k_bounded_wait_probe<<<1, 32>>>(limit_ns, d_flag, d_ns);
+    int f = 0;
+    unsigned long long ns = 0;
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(&f, d_flag, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(&ns, d_ns, sizeof(ns), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) err = cudaGetErrorString(e);
+    if (timed_out) *timed_out = f;
+    if (waited_ms) *waited_ms = (double)ns * 1e-6;
+  }
+  cudaFree(d_flag);
+  cudaFree(d_ns);
+  return err;
+}
+
 }  // namespace nrg

@@ -25,6 +25,9 @@ bool surrogate_ready(const Surrogate* s);
 // Allocates the inference and compaction buffers for n cells (call outside
 // stream capture).
 std::string surrogate_reserve(Surrogate* s, long n);
+// One warp waits on an mbarrier nothing arrives at, with the bounded wait of
+// the tensor-core kernel (limit_ns); reports whether the wait gave up.
+std::string bounded_wait_probe(unsigned long long limit_ns, int* timed_out, double* waited_ms);
 
 // Enqueues features -> MLP -> gate/outputs -> compaction -> FP64 fallback
 // on the cells the gate rejects.  counters[6] / [7] receive surrogate /
