@@ -48,6 +48,8 @@ def parse():
     p.add_argument("--kernel", choices=["thread", "thread_queue", "warp_queue"], default=None,
                    help="fix the integrator launch instead of autotuning it (with --block)")
     p.add_argument("--block", type=int, default=32)
+    p.add_argument("--cell-order", choices=["temperature", "cell"], default="temperature",
+                   help="order in which the FP64 integrator takes the cells (same results)")
     p.add_argument("--mechanism", default="KEROMNES", choices=["KEROMNES", "ZHANG", "TEREZA", "KONNOV", "ACETYLENE"],
                    help="reference mechanism; the others run the plain FP64 path on the same flame field "
                         "(ACETYLENE: the same geometry with a C2H2/O2/Ar mixture)")
@@ -392,6 +394,7 @@ def main():
     n = field.n
     T, rho, Y = (torch.tensor(a, device=dev) for a in (field.T, field.rho, field.Y))
 
+    solver.set_cell_order(args.cell_order == "temperature")
     # launch shape of the FP64 integrator: autotuned on a contiguous block of
     # rows (neighbouring cells take similar integration paths)
     if args.kernel:
@@ -530,6 +533,7 @@ def main():
             m.interior(m.fields["specie_mass_fraction"][k])[...] = field.Y[k].reshape(ny, nx).T[:, :, None]
         host = ChemicalKineticsSolver(m, *decks, mode="fast")
         host.set_launch(**launch)
+        host.set_cell_order(args.cell_order == "temperature")
         if mode == "surrogate":
             hs = Surrogate(host)
             hs.load(DEFAULT_MODEL)
@@ -550,7 +554,7 @@ def main():
         st = stats[-1]
         peaks = load_peaks()
         fm = flop_model(tables, "fast")
-        phases = {"inference_ms": ph["phase_ms"][0], "compaction_ms": ph["phase_ms"][1],
+        phases = {"inference_ms": ph["phase_ms"][0], "fallback_order_ms": ph["phase_ms"][1],
                   "integrator_ms": ph["phase_ms"][2]}
         integ_flops = algorithmic_flops(ph, fm)
         integ_tf = integ_flops / max(phases["integrator_ms"], 1e-9) * 1e-9
@@ -571,7 +575,13 @@ def main():
                         "layers + FP64 gate)", "flops_per_launch": mlp_flops,
                         "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst), of measured"}
         cpu = cpu_baseline(field, W, decks, args.cpu_seconds, units)
-        launches = 5 if mode == "surrogate" else 1  # fused MLP+gate, 3 compaction kernels, integrator
+        # per step: fused MLP + gate (surrogate), the cell order (3 radix passes of
+        # count / scan / scatter, or 3 compaction kernels for the fallback in cell
+        # order), the integrator
+        if args.cell_order == "temperature":
+            launches = 11 if mode == "surrogate" else 10
+        else:
+            launches = 5 if mode == "surrogate" else 1
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": el / args.steps, "higher_is_better": True,
@@ -584,7 +594,7 @@ def main():
                                 "reference": "plain FP64 integrator, reference FD Jacobian",
                                 "mixed": "FP32 LU + FP64 residual/refinement",
                                 "surrogate": "BF16 MLP surrogate + gated FP64 fallback"}[mode],
-                       "launch": launch, "l2": "inputs (370 MB) larger than L2; no flush",
+                       "launch": launch, "cell_order": args.cell_order, "l2": "inputs (370 MB) larger than L2; no flush",
                        "active_cells": int(ph["cells_active"])},
             "plain_fp64": {"value": plain_value, "ms_per_step": el_plain / args.steps,
                            "ratio_surrogate_over_plain": value / plain_value},

@@ -254,6 +254,14 @@ NRG_API int nrg_chem_set_specialised(nrg_chem* h, int enable);
 /* Capture the step in a CUDA graph (1) or launch directly (0). */
 NRG_API int nrg_chem_set_graph(nrg_chem* h, int enable);
 
+/* Order in which the FP64 integrator takes the cells of a step (the plain
+ * step and the surrogate's fallback cells): 1 (default) = sorted by
+ * temperature (stable radix sort on a 1/1024 K key, cells the step skips
+ * first), so that the lanes of a warp take similar BDF paths; 0 = cell order.  Cells are independent, so both give the same results.  No
+ * counterpart in the reference (its OpenMP loop takes cells one by one,
+ * chemical_kinetics_solver.f90:222). */
+NRG_API int nrg_chem_set_cell_order(nrg_chem* h, int enable);
+
 /* Per-phase CUDA-event timing of the step (stats.phase_ms); launches the step
  * without a graph while enabled. */
 NRG_API int nrg_chem_set_timing(nrg_chem* h, int enable);

@@ -26,6 +26,7 @@ SOURCES = {
     "chem_kernels.cu": ["--fmad=false"],  # state equation in the reference's operation order
     "capi.cu": [],
     "surrogate.cu": [],
+    "order.cu": [],
     "transport.cu": ["--fmad=false"],  # species predictor in the reference's operation order
     "diffusion.cu": ["--fmad=false"],
     "mechanism.cpp": [],

@@ -85,6 +85,7 @@ SIGNATURES = {
     "nrg_chem_get_launch": (_I, [_VP] + [ctypes.POINTER(_I)] * 4),
     "nrg_chem_autotune": (_I, [_VP, _D, _L, _L, _VP, _VP, _VP, _VP, _VP, _VP, _VP, ctypes.POINTER(_D)]),
     "nrg_chem_set_graph": (_I, [_VP, _I]),
+    "nrg_chem_set_cell_order": (_I, [_VP, _I]),
     "nrg_chem_set_timing": (_I, [_VP, _I]),
     "nrg_chem_info": (_I, [_VP, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "nrg_chem_tables": (_I, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
@@ -286,6 +287,11 @@ class ChemicalKineticsSolver:
 
     def set_graph(self, enable: bool) -> None:
         _check(lib().nrg_chem_set_graph(self._h, int(enable)), self._h)
+
+    def set_cell_order(self, by_temperature: bool) -> None:
+        """Integrator takes the cells grouped by temperature (default) or in
+        cell order; the results are the same."""
+        _check(lib().nrg_chem_set_cell_order(self._h, int(by_temperature)), self._h)
 
     def apply_state_device(self, rho, Y, E_f, T, p, gamma, v=None, time_step=0.0, Y_prod=None, E_f_prod=None,
                            bc=None, cp_mass=None, h_s=None, h_full=None, v_s=None, mix_mol_mass=None,

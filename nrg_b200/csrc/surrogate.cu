@@ -26,6 +26,7 @@
 
 #include "chem_bdf.cuh"
 #include "surrogate.hpp"
+#include "order.hpp"
 #include "tc_sm100.cuh"
 
 namespace nrg {
@@ -781,6 +782,9 @@ struct Surrogate {
   long gcap = 0;
   unsigned char* flag = nullptr;
   int *block_count = nullptr, *block_off = nullptr, *list = nullptr, *n_list = nullptr;
+  // fallback cells in temperature order (order.hpp) or in cell order
+  bool order_cells = true;
+  OrderScratch order;
 };
 
 static long param_layout(Surrogate* s) {
@@ -854,6 +858,7 @@ void surrogate_destroy(Surrogate* s) {
   cudaFree(s->iX); cudaFree(s->iH[0]); cudaFree(s->iH[1]); cudaFree(s->iO);
   cudaFree(s->d_loss); cudaFree(s->flag); cudaFree(s->block_count); cudaFree(s->block_off); cudaFree(s->list);
   cudaFree(s->n_list);
+  order_free(&s->order);
   cudaFree(s->d_err);
   cudaFreeHost(s->h_err);
   delete s;
@@ -861,6 +866,7 @@ void surrogate_destroy(Surrogate* s) {
 
 bool surrogate_ready(const Surrogate* s) { return s && s->ready && s->uploaded; }
 void surrogate_set_ready(Surrogate* s, bool r) { s->ready = r; }
+void surrogate_set_cell_order(Surrogate* s, bool by_temperature) { s->order_cells = by_temperature; }
 void surrogate_set_gate(Surrogate* s, double elem_tol, double raw_elem_tol, double dT_tol, double dT_max) {
   s->gate = GateCfg{elem_tol, raw_elem_tol, dT_tol, dT_max};
 }
@@ -918,6 +924,7 @@ static std::string ensure_gate(Surrogate* s, long n) {
   if ((e = ck(cudaMalloc(&s->block_off, nb * 4), "alloc offsets")).size()) return e;
   if ((e = ck(cudaMalloc(&s->list, n * 4), "alloc list")).size()) return e;
   if ((e = ck(cudaMalloc(&s->n_list, 4), "alloc count")).size()) return e;
+  if ((e = order_reserve(&s->order, n)).size()) return e;
   s->gcap = n;
   return "";
 }
@@ -1283,11 +1290,19 @@ cudaError_t surrogate_step(Surrogate* s, const StepArgs& a, const LaunchCfg& cfg
     k_gate<<<std::min<long>((n + 255) / 256, 148 * 16), 256, 0, st>>>(a, s->iO, s->d_norm, s->gate, s->flag,
                                                                     counters);
   }
-  const int nb = (int)((n + kCompactBlock - 1) / kCompactBlock);
-  k_flag_count<<<nb, kCompactBlock, 0, st>>>(n, s->flag, s->block_count);
-  k_scan_counts<<<1, 1024, 0, st>>>(nb, s->block_count, s->block_off, s->n_list, counters);
-  k_compact<<<nb, kCompactBlock, 0, st>>>(n, s->flag, s->block_off, s->list);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (s->order_cells) {
+    // rejected cells grouped by temperature: the fallback's warps then hold
+    // cells with similar BDF paths
+    if ((e = order_cells_by_temperature(n, a.T, a.bc, s->flag, &s->order, s->list, s->n_list,
+                                        counters ? counters + 7 : nullptr, st)) != cudaSuccess)
+      return e;
+  } else {
+    const int nb = (int)((n + kCompactBlock - 1) / kCompactBlock);
+    k_flag_count<<<nb, kCompactBlock, 0, st>>>(n, s->flag, s->block_count);
+    k_scan_counts<<<1, 1024, 0, st>>>(nb, s->block_count, s->block_off, s->n_list, counters);
+    k_compact<<<nb, kCompactBlock, 0, st>>>(n, s->flag, s->block_off, s->list);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
   StepArgs fa = a;
   fa.cell_list = s->list;
   fa.n_list_dev = s->n_list;

@@ -73,6 +73,8 @@ std::string surrogate_prepare(Surrogate* s, long n, long ld, double dt, const do
                               const double* rho, const double* Y, const double* Y_prod, const double* T_after,
                               const PrepareOpts& opts, __nv_bfloat16* x, float* y, cudaStream_t st);
 void surrogate_set_ready(Surrogate* s, bool ready);
+// Fallback cells grouped by temperature (default) or in cell order.
+void surrogate_set_cell_order(Surrogate* s, bool by_temperature);
 // Inference path of surrogate_step: fused tcgen05 kernel (default) or the
 // unfused GEMM chain followed by the gate kernel.
 void surrogate_set_fused(Surrogate* s, bool fused);

@@ -94,6 +94,36 @@ def test_thread_block_sizes_give_identical_results(solver, W):
     solver.set_launch(kernel="warp_queue", block=256, grid=0, chunk=1)
 
 
+@pytest.mark.parametrize("mode", ["reference", "fast", "mixed"])
+def test_temperature_order_changes_no_result(solver, W, mode):
+    """The integrator takes a step's cells grouped by temperature (default) or
+    in cell order: same bits, same statuses and same event counts, with
+    skipped, boundary-marked and hot cells mixed into a flame sample, for
+    every launch shape."""
+    f = fields.slice_field(fields.flame_field(W, n_side=256), 5000, stride=13)
+    f.T[:40] = 300.0
+    f.T[40:48] = 3500.0
+    bc = np.zeros(f.n, np.int8)
+    bc[60:90] = 1
+    init2 = np.full((9, f.n), 3.25)
+    keys = ("cells_active", "steps", "rhs_evals", "jacobians", "solves", "cells_bad")
+    try:
+        for launch in (dict(kernel="thread", block=32, grid=0, chunk=1),
+                       dict(kernel="thread_queue", block=64, grid=0, chunk=2),
+                       dict(kernel="warp_queue", block=128, grid=0, chunk=1)):
+            solver.set_cell_order(False)
+            a, sa = run_device(solver, f, mode, bc=bc, launch=launch, y_prod2_init=init2)
+            solver.set_cell_order(True)
+            b, sb = run_device(solver, f, mode, bc=bc, launch=launch, y_prod2_init=init2)
+            for k in ("Y_prod", "Y_prod2", "E_f_prod", "T_after", "status"):
+                np.testing.assert_array_equal(b[k], a[k], err_msg=f"{k} {launch}")
+            assert all(sb[k] == sa[k] for k in keys), (sa, sb)
+            assert sb["cells_active"] == int(np.sum((f.T >= 305.0) & (bc == 0))) and sb["cells_bad"] == 0
+    finally:
+        solver.set_cell_order(True)
+        solver.set_launch(kernel="warp_queue", block=256, grid=0, chunk=1)
+
+
 def test_skip_rule_bc_and_untouched_y_prod2(solver, oracle_mech, W):
     f = fields.slice_field(fields.random_field(W), 1024)
     f.T[:32] = 300.0

@@ -171,3 +171,28 @@ def test_trained_network_gain_on_flame_rows(decks, W):
     print(f"surrogate answers {acc.sum()} of {act.sum()} active cells; device time "
           f"{st_p['device_ms']:.1f} ms -> {st_s['device_ms']:.1f} ms ({gain:.2f}x)")
     assert gain > 1.2, gain
+
+
+def test_fallback_order_changes_no_result(decks, W):
+    """The surrogate's rejected cells go to the FP64 fallback grouped by
+    temperature (default) or in cell order: the same bits and counts."""
+    from nrg_b200.chemistry import ChemicalKineticsSolver
+    from nrg_b200.surrogate import DEFAULT_MODEL, RECIPE, Surrogate
+    f = fields.slice_field(fields.flame_field(W), 16 * 2048, offset=1000 * 2048)
+    s = ChemicalKineticsSolver(None, *decks, mode="fast")
+    try:
+        s.set_launch(kernel="thread", block=32)
+        sur = Surrogate(s)
+        sur.load(DEFAULT_MODEL)
+        sur.set_gate(*RECIPE["gate"])
+        s.set_cell_order(False)
+        a, sa = run_device(s, f, "surrogate")
+        s.set_cell_order(True)
+        b, sb = run_device(s, f, "surrogate")
+    finally:
+        s.close()
+    for k in ("Y_prod", "Y_prod2", "E_f_prod", "T_after", "status"):
+        np.testing.assert_array_equal(b[k], a[k], err_msg=k)
+    for k in ("cells_active", "cells_surrogate", "cells_fallback", "steps", "solves"):
+        assert sb[k] == sa[k], (k, sa, sb)
+    assert 0 < sb["cells_fallback"] < sb["cells_active"]
