@@ -1,7 +1,7 @@
 // Temperature order of the integrator's cells: a stable least-significant-
 // digit radix sort of (key, cell) pairs over three 8-bit digits.  Per pass:
-// digit counts per 4096-cell tile, one exclusive scan over (digit, tile),
-// then a stable scatter (tile order, then warp order, then lane order).
+// digit counts per 8192-cell tile, exclusive scans over the tiles of each
+// digit and over the digits, then a stable scatter (tile order, then warp order, then lane order).
 // Small HBM-bound kernels next to the integrator's step.
 #include <climits>
 
@@ -14,7 +14,6 @@ constexpr int kThreads = 1024;
 constexpr int kWarps = kThreads / 32;
 constexpr int kRounds = kOrderTile / kThreads;
 constexpr int kDigits = 1 << kOrderDigitBits;
-constexpr int kScanPer = 4;  // scan entries per thread and iteration
 static_assert(kOrderTile % kThreads == 0, "a tile is a whole number of block-wide rounds");
 static_assert(kDigits <= kThreads, "one thread per digit in the column scans");
 static_assert(kOrderKeyBits % kOrderDigitBits == 0, "whole digits");
@@ -73,72 +72,81 @@ __global__ void __launch_bounds__(kThreads) k_rs_count(PassIn p, int* counts, in
     }
   }
   __syncthreads();
-  if (threadIdx.x < kDigits) counts[threadIdx.x * tiles + blockIdx.x] = sh[threadIdx.x];
+  if (threadIdx.x < kDigits) counts[(long)threadIdx.x * tiles + blockIdx.x] = sh[threadIdx.x];
 }
 
-// Exclusive scan of counts[0, m) in place (one block); the total goes to
-// *total and *total2 (may be null) and is added to *counter (may be null).
-__global__ void __launch_bounds__(kThreads) k_rs_scan(int* counts, long m, int* total, int* total2,
-                                                      unsigned long long* counter) {
-  __shared__ int wsum[kWarps];
-  __shared__ int carry;
-  if (threadIdx.x == 0) carry = 0;
-  __syncthreads();
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (long base = 0; base < m; base += (long)kThreads * kScanPer) {
-    const long i0 = base + (long)threadIdx.x * kScanPer;
-    int v[kScanPer];
-    int s = 0;
-#pragma unroll
-    for (int j = 0; j < kScanPer; ++j) {
-      v[j] = i0 + j < m ? counts[i0 + j] : 0;
-      s += v[j];
-    }
-    int x = s;
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += y;
-    }
-    if (lane == 31) wsum[w] = x;
-    __syncthreads();
-    if (w == 0) {
-      int z = wsum[lane];
-      for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, z, o);
-        if (lane >= o) z += y;
-      }
-      wsum[lane] = z;
-    }
-    __syncthreads();
-    const int incl = x + (w > 0 ? wsum[w - 1] : 0);
-    int run = carry + incl - s;
-#pragma unroll
-    for (int j = 0; j < kScanPer; ++j) {
-      if (i0 + j < m) counts[i0 + j] = run;
-      run += v[j];
-    }
-    __syncthreads();
-    if (threadIdx.x == kThreads - 1) carry += incl;
-    __syncthreads();
+// Block-wide exclusive scan of one int per thread (blockDim.x a multiple of
+// 32, at most 1024; wsum holds blockDim.x / 32 ints); returns the thread's
+// exclusive prefix and sets *sum to the block total.
+__device__ __forceinline__ int block_exclusive_scan(int v, int* wsum, int* sum) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (int)(blockDim.x >> 5);
+  int x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
   }
+  if (lane == 31) wsum[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    int z = lane < nw ? wsum[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, z, o);
+      if (lane >= o) z += y;
+    }
+    if (lane < nw) wsum[lane] = z;
+  }
+  __syncthreads();
+  const int incl = x + (w > 0 ? wsum[w - 1] : 0);
+  *sum = wsum[nw - 1];
+  __syncthreads();  // wsum is reused by the next call
+  return incl - v;
+}
+
+// Per digit (one block each): exclusive scan of its tile counts in place
+// (coalesced over the tiles) and the digit's total to digit_base[digit].
+__global__ void __launch_bounds__(kThreads) k_rs_scan_tiles(int* counts, int tiles, int* digit_base) {
+  __shared__ int wsum[kWarps];
+  int* row = counts + (long)blockIdx.x * tiles;
+  int carry = 0;
+  for (int base = 0; base < tiles; base += kThreads) {
+    const int i = base + threadIdx.x;
+    const int v = i < tiles ? row[i] : 0;
+    int sum = 0;
+    const int ex = block_exclusive_scan(v, wsum, &sum);
+    if (i < tiles) row[i] = carry + ex;
+    carry += sum;
+  }
+  if (threadIdx.x == 0) digit_base[blockIdx.x] = carry;
+}
+
+// Exclusive scan of the digit totals in place (one block of kDigits threads);
+// the grand total goes to *total and *total2 (may be null) and is added to
+// *counter (may be null).
+__global__ void __launch_bounds__(kDigits) k_rs_scan_digits(int* digit_base, int* total, int* total2,
+                                                            unsigned long long* counter) {
+  __shared__ int wsum[kDigits / 32];
+  const int v = digit_base[threadIdx.x];
+  int sum = 0;
+  const int ex = block_exclusive_scan(v, wsum, &sum);
+  digit_base[threadIdx.x] = ex;
   if (threadIdx.x == 0) {
-    *total = carry;
-    if (total2) *total2 = carry;
-    if (counter) *counter += (unsigned long long)carry;
+    *total = sum;
+    if (total2) *total2 = sum;
+    if (counter) *counter += (unsigned long long)sum;
   }
 }
 
 // Stable scatter of one tile: an item's slot is its tile's offset for its
 // digit, plus the items of that digit in earlier rounds, earlier warps of
 // this round and earlier lanes of its warp.
-__global__ void __launch_bounds__(kThreads) k_rs_scatter(PassIn p, const int* offsets, int tiles,
-                                                         uint32_t* keys_out, int* vals_out) {
+__global__ void __launch_bounds__(kThreads) k_rs_scatter(PassIn p, const int* offsets, const int* digit_base,
+                                                         int tiles, uint32_t* keys_out, int* vals_out) {
   __shared__ int s_off[kDigits];
   __shared__ int s_w[kWarps][kDigits];
   const int t = threadIdx.x;
   const unsigned lane = t & 31u;
   const int w = t >> 5;
-  if (t < kDigits) s_off[t] = offsets[t * tiles + blockIdx.x];
+  if (t < kDigits) s_off[t] = digit_base[t] + offsets[(long)t * tiles + blockIdx.x];
   const long nitems = pass_items(p);
   const long base = (long)blockIdx.x * kOrderTile;
   for (int r = 0; r < kRounds; ++r) {
@@ -186,6 +194,7 @@ std::string order_reserve(OrderScratch* o, long n) {
   if (cudaMalloc(&o->keys[0], b) != cudaSuccess || cudaMalloc(&o->keys[1], b) != cudaSuccess ||
       cudaMalloc(&o->vals[0], b) != cudaSuccess || cudaMalloc(&o->vals[1], b) != cudaSuccess ||
       cudaMalloc(&o->counts, sizeof(int) * (size_t)kDigits * tiles) != cudaSuccess ||
+      cudaMalloc(&o->digit_base, sizeof(int) * kDigits) != cudaSuccess ||
       cudaMalloc(&o->total, sizeof(int)) != cudaSuccess) {
     cudaGetLastError();
     order_free(o);
@@ -203,8 +212,10 @@ void order_free(OrderScratch* o) {
     o->vals[i] = nullptr;
   }
   cudaFree(o->counts);
+  cudaFree(o->digit_base);
   cudaFree(o->total);
   o->counts = nullptr;
+  o->digit_base = nullptr;
   o->total = nullptr;
   o->cap = 0;
 }
@@ -215,7 +226,6 @@ cudaError_t order_cells_by_temperature(long n, const double* T, const int8_t* bc
   if (n < 0 || !o || n > o->cap || !list || !count || (n > 0 && !T)) return cudaErrorInvalidValue;
   if (n == 0) return cudaMemsetAsync(count, 0, sizeof(int), s);
   const int tiles = (int)((n + kOrderTile - 1) / kOrderTile);
-  const long m = (long)kDigits * tiles;
   for (int pass = 0; pass < kOrderPasses; ++pass) {
     PassIn p{};
     p.n = n;
@@ -231,10 +241,11 @@ cudaError_t order_cells_by_temperature(long n, const double* T, const int8_t* bc
     }
     const bool last = pass == kOrderPasses - 1;
     k_rs_count<<<tiles, kThreads, 0, s>>>(p, o->counts, tiles);
-    k_rs_scan<<<1, kThreads, 0, s>>>(o->counts, m, o->total, last ? count : nullptr,
-                                     pass == 0 ? counter : nullptr);
-    k_rs_scatter<<<tiles, kThreads, 0, s>>>(p, o->counts, tiles, last ? nullptr : o->keys[pass & 1],
-                                            last ? list : o->vals[pass & 1]);
+    k_rs_scan_tiles<<<kDigits, kThreads, 0, s>>>(o->counts, tiles, o->digit_base);
+    k_rs_scan_digits<<<1, kDigits, 0, s>>>(o->digit_base, o->total, last ? count : nullptr,
+                                           pass == 0 ? counter : nullptr);
+    k_rs_scatter<<<tiles, kThreads, 0, s>>>(p, o->counts, o->digit_base, tiles,
+                                            last ? nullptr : o->keys[pass & 1], last ? list : o->vals[pass & 1]);
   }
   return cudaGetLastError();
 }

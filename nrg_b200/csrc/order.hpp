@@ -21,14 +21,15 @@ namespace nrg {
 constexpr int kOrderKeyBits = 24;
 constexpr int kOrderDigitBits = 8;
 constexpr int kOrderPasses = kOrderKeyBits / kOrderDigitBits;
-constexpr int kOrderTile = 4096;  // cells per block of the radix passes
+constexpr int kOrderTile = 8192;  // cells per block of the radix passes
 
 // Device scratch of the sort for up to cap cells (grow-only).
 struct OrderScratch {
   long cap = 0;
   uint32_t* keys[2] = {nullptr, nullptr};
   int* vals[2] = {nullptr, nullptr};
-  int* counts = nullptr;  // 256 digits x tiles, then their exclusive scan
+  int* counts = nullptr;      // 256 digits x tiles, then their exclusive scans per digit
+  int* digit_base = nullptr;  // 256 digit totals, then their exclusive scan
   int* total = nullptr;   // cells taken (device)
 };
 
