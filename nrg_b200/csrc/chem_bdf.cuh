@@ -80,7 +80,7 @@ template <int N, int R, typename LUT, int BS, int SPEC>
 __device__ __noinline__ void nl_rhs(double* d, LUT* f);
 template <int N, int R, typename LUT, int BS, int SPEC>
 __device__ __noinline__ void nl_analytic_matrix(double* d, LUT* f, double factor);
-template <int N, int R, typename LUT, int BS>
+template <int N, int R, typename LUT, int BS, bool RECIP>
 __device__ __noinline__ unsigned long long nl_dgefa(double* d, LUT* f, int* info);
 template <int N, int R, typename LUT, int BS>
 __device__ __noinline__ void nl_rate_constants(double* d, LUT* f, double T);
@@ -408,8 +408,12 @@ __device__ __forceinline__ double dnrm2(const double (&dx)[N]) {
   return dnrm2_nl<N>(t);
 }
 
-// dgefa.f90:60-117 on the shared-memory matrix (column-major a(j, i) = A(i, j))
-template <int N, class CS>
+// dgefa.f90:60-117 on the shared-memory matrix (column-major a(j, i) = A(i, j)).
+// RECIP: each pivot is replaced by its reciprocal (the -1/pivot the
+// elimination forms anyway, negated), so that dgesl<RECIP> multiplies where
+// the reference divides; used by the analytic-Jacobian and mixed modes, whose
+// results agree with the reference's to its tolerance, not bit for bit.
+template <int N, bool RECIP, class CS>
 __device__ __forceinline__ int dgefa(CS& c, unsigned long long* piv_out) {
   using LUT = typename std::remove_reference<decltype(c.a(0, 0))>::type;
   int info = 0;
@@ -430,6 +434,7 @@ __device__ __forceinline__ int dgefa(CS& c, unsigned long long* piv_out) {
       c.a(k, k) = t;
     }
     const LUT t = (LUT)-1 / c.a(k, k);
+    if (RECIP) c.a(k, k) = -t;
     for (int i = k + 1; i < N; ++i) c.a(k, i) = t * c.a(k, i);
     for (int j = k + 1; j < N; ++j) {
       const LUT tj = c.a(j, l);
@@ -444,11 +449,13 @@ __device__ __forceinline__ int dgefa(CS& c, unsigned long long* piv_out) {
   piv |= (unsigned long long)(N - 1) << (4 * (N - 1));
   *piv_out = piv;
   if (c.a(N - 1, N - 1) == (LUT)0) info = N;
+  else if (RECIP) c.a(N - 1, N - 1) = (LUT)1 / c.a(N - 1, N - 1);
   return info;
 }
 
-// dgesl.f90:71-131, JOB = 0, on the register vector b
-template <int N, class CS>
+// dgesl.f90:71-131, JOB = 0, on the register vector b (RECIP: the factors
+// hold the pivots' reciprocals, see dgefa)
+template <int N, bool RECIP, class CS>
 __device__ __forceinline__ void dgesl(CS& c, double (&b)[N]) {
 #pragma unroll
   for (int k = 0; k < N - 1; ++k) {
@@ -465,7 +472,7 @@ __device__ __forceinline__ void dgesl(CS& c, double (&b)[N]) {
   }
 #pragma unroll
   for (int k = N - 1; k >= 0; --k) {
-    b[k] = ddiv(b[k], (double)c.a(k, k));
+    b[k] = RECIP ? b[k] * (double)c.a(k, k) : ddiv(b[k], (double)c.a(k, k));
     const double t = -b[k];
     if (t != 0.0) {
 #pragma unroll
@@ -500,13 +507,13 @@ __device__ __noinline__ void nl_analytic_matrix(double* d, LUT* f, double factor
   }
 }
 
-template <int N, int R, typename LUT, int BS>
+template <int N, int R, typename LUT, int BS, bool RECIP>
 __device__ __noinline__ unsigned long long nl_dgefa(double* d, LUT* f, int* info) {
   SmemStore<N, R, LUT, BS> s;
   s.d = d;
   s.f = f;
   unsigned long long piv = 0;
-  *info = dgefa<N>(s, &piv);
+  *info = dgefa<N, RECIP>(s, &piv);
   return piv;
 }
 
@@ -657,7 +664,7 @@ __device__ void ddpst(CS& c) {
     nl_analytic_matrix<N, R, typename CS::lut_t, CS::kBS, CS::kSpec>(c.d, c.f, -el1h);
   }
   int info = 0;
-  c.piv = nl_dgefa<N, R, typename CS::lut_t, CS::kBS>(c.d, c.f, &info);
+  c.piv = nl_dgefa<N, R, typename CS::lut_t, CS::kBS, JAC != kJacFD>(c.d, c.f, &info);
   if (info != 0) c.ier = 1;
 }
 
@@ -666,7 +673,7 @@ __device__ void ddpst(CS& c) {
 // float LU factors (mixed mode) the chord iteration that calls this solve
 // until the FP64 convergence test passes is itself the iterative refinement of
 // the FP32 solution, so no further sweep is made per solve.
-template <int N, int R, typename LUT, class CS>
+template <int N, int R, int JAC, typename LUT, class CS>
 __device__ double ddcor(CS& c) {
   double b[N];
 #pragma unroll
@@ -674,7 +681,7 @@ __device__ double ddcor(CS& c) {
   double x[N];
 #pragma unroll
   for (int i = 0; i < N; ++i) x[i] = b[i];
-  dgesl<N>(c, x);
+  dgesl<N, JAC != kJacFD>(c, x);
   c.nsolve += 1;
 #pragma unroll
   for (int i = 0; i < N; ++i) {
@@ -721,7 +728,7 @@ L110:
 #pragma unroll
   for (int i = 0; i < N; ++i) c.s1[i] = 0.0;
 L130:
-  d = ddcor<N, R, LUT>(c);
+  d = ddcor<N, R, JAC, LUT>(c);
   if (iter > 0) c.trend = NRG_FMAX(0.9 * c.trend, ddiv(d, d1));
   d1 = d;
   ctest = NRG_FMIN(2.0 * c.trend, 1.0) * d;
