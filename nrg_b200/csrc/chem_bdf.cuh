@@ -408,6 +408,27 @@ __device__ __forceinline__ double dnrm2(const double (&dx)[N]) {
   return dnrm2_nl<N>(t);
 }
 
+// sqrt by Newton's iteration at compile time (constant scale factors).
+__host__ __device__ constexpr double ct_sqrt(double x, double g = 1.0, int it = 0) {
+  return it == 64 ? g : ct_sqrt(x, 0.5 * (g + x / g), it + 1);
+}
+
+// Weighted norms of the step and error tests.  Reference mode: dnrm2, for the
+// reference's bits.  Analytic-Jacobian and mixed modes: sqrt of the sum of
+// squares in registers (no divisions, no call), which differs from dnrm2 by
+// rounding only; dnrm2 takes over if the sum leaves the safe range.
+template <int N, int JAC>
+__device__ __forceinline__ double step_norm(const double (&dx)[N]) {
+  if constexpr (JAC == kJacFD) {
+    return dnrm2<N>(dx);
+  } else {
+    double s = 0.0;
+#pragma unroll
+    for (int i = 0; i < N; ++i) s = fma(dx[i], dx[i], s);
+    return s < 1e300 ? sqrt(s) : dnrm2<N>(dx);
+  }
+}
+
 // dgefa.f90:60-117 on the shared-memory matrix (column-major a(j, i) = A(i, j)).
 // RECIP: each pivot is replaced by its reciprocal (the -1/pivot the
 // elimination forms anyway, negated), so that dgesl<RECIP> multiplies where
@@ -688,7 +709,11 @@ __device__ double ddcor(CS& c) {
     c.s1[i] = c.s1[i] + x[i];
     c.s2[i] = ddiv(x[i], NRG_FMAX(fabs(c.y[i]), c.ywt[i]));
   }
-  return ddiv(dnrm2<N>(c.s2), sqrt((double)CS::kNF));
+  if constexpr (JAC == kJacFD) return ddiv(dnrm2<N>(c.s2), sqrt((double)CS::kNF));
+  else {
+    constexpr double kInvSqrtNF = 1.0 / ct_sqrt((double)CS::kNF);
+    return step_norm<N, JAC>(c.s2) * kInvSqrtNF;
+  }
 }
 
 // One DDSTP call (ddstp.f90:72-459); returns JSTATE (1 ok, 2 h vanished,
@@ -759,7 +784,7 @@ L170:
   c.convrg = 1;
 #pragma unroll
   for (int i = 0; i < N; ++i) c.s2[i] = ddiv(c.s1[i], NRG_FMAX(fabs(c.y[i]), c.ywt[i]));
-  etest = ddiv(dnrm2<N>(c.s2), TQ(2, c.nq) * sqn);
+  etest = ddiv(step_norm<N, JAC>(c.s2), TQ(2, c.nq) * sqn);
   if (etest > eps) {
     c.t = told;
     ddpsc<N>(-1, c);
@@ -770,7 +795,7 @@ L170:
       if (c.nq > 1) {
 #pragma unroll
         for (int i = 0; i < N; ++i) c.s2[i] = ddiv(c.yh(c.nq, i), NRG_FMAX(fabs(c.y[i]), c.ywt[i]));
-        const double erdn = ddiv(dnrm2<N>(c.s2), TQ(1, c.nq) * sqn);
+        const double erdn = ddiv(step_norm<N, JAC>(c.s2), TQ(1, c.nq) * sqn);
         const double rh1 = ddiv(1.0, NRG_FMAX(1.0, BIAS1 * npow(ddiv(erdn, eps), ddiv(1.0, (double)c.nq))));
         if (rh2 < rh1) {
           c.nq = c.nq - 1;
@@ -818,7 +843,7 @@ L170:
     } else {
 #pragma unroll
       for (int i = 0; i < N; ++i) c.s2[i] = ddiv(c.yh(c.nq, i), NRG_FMAX(fabs(c.y[i]), c.ywt[i]));
-      const double erdn = ddiv(dnrm2<N>(c.s2), TQ(1, c.nq) * sqn);
+      const double erdn = ddiv(step_norm<N, JAC>(c.s2), TQ(1, c.nq) * sqn);
       rh1 = ddiv(1.0, NRG_FMAX(uround, BIAS1 * npow(ddiv(erdn, eps), ddiv(1.0, (double)c.nq))));
     }
     rh2 = ddiv(1.0, NRG_FMAX(uround, BIAS2 * npow(ddiv(etest, eps), ddiv(1.0, (double)(c.nq + 1)))));
@@ -828,7 +853,7 @@ L170:
 #pragma unroll
       for (int i = 0; i < N; ++i)
         c.s2[i] = ddiv(c.s1[i] - c.yh(kMaxOrd, i), NRG_FMAX(fabs(c.y[i]), c.ywt[i]));
-      const double erup = ddiv(dnrm2<N>(c.s2), TQ(3, c.nq) * sqn);
+      const double erup = ddiv(step_norm<N, JAC>(c.s2), TQ(3, c.nq) * sqn);
       rh3 = ddiv(1.0, NRG_FMAX(uround, BIAS3 * npow(ddiv(erup, eps), ddiv(1.0, (double)(c.nq + 2)))));
     }
     if (rh1 > rh2 && rh1 >= rh3) {
