@@ -408,6 +408,26 @@ __device__ __forceinline__ double dnrm2(const double (&dx)[N]) {
   return dnrm2_nl<N>(t);
 }
 
+// Division by a weight of the step and error norms.  Reference mode: the
+// reference's division.  Analytic-Jacobian and mixed modes: multiplication by
+// a reciprocal from the hardware approximation (rcp.approx.ftz.f64) refined by
+// one Newton step r (1 + (1 - w r)), which squares its relative error (to
+// about 2^-44): these norms only steer step sizes, orders and the error test.
+// Weights are at least the error-weight floor, so w is a positive normal
+// number unless it is not finite (then the division is used).
+template <int JAC>
+__device__ __forceinline__ double wdiv(double x, double w) {
+  if constexpr (JAC == kJacFD) {
+    return ddiv(x, w);
+  } else {
+    if (!(w < 1e300)) return ddiv(x, w);
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(w));
+    const double e = fma(-w, r, 1.0);
+    return x * fma(r, e, r);
+  }
+}
+
 // sqrt by Newton's iteration at compile time (constant scale factors).
 __host__ __device__ constexpr double ct_sqrt(double x, double g = 1.0, int it = 0) {
   return it == 64 ? g : ct_sqrt(x, 0.5 * (g + x / g), it + 1);
@@ -707,7 +727,7 @@ __device__ double ddcor(CS& c) {
 #pragma unroll
   for (int i = 0; i < N; ++i) {
     c.s1[i] = c.s1[i] + x[i];
-    c.s2[i] = ddiv(x[i], NRG_FMAX(fabs(c.y[i]), c.ywt[i]));
+    c.s2[i] = wdiv<JAC>(x[i], NRG_FMAX(fabs(c.y[i]), c.ywt[i]));
   }
   if constexpr (JAC == kJacFD) return ddiv(dnrm2<N>(c.s2), sqrt((double)CS::kNF));
   else {
@@ -783,7 +803,7 @@ L160:
 L170:
   c.convrg = 1;
 #pragma unroll
-  for (int i = 0; i < N; ++i) c.s2[i] = ddiv(c.s1[i], NRG_FMAX(fabs(c.y[i]), c.ywt[i]));
+  for (int i = 0; i < N; ++i) c.s2[i] = wdiv<JAC>(c.s1[i], NRG_FMAX(fabs(c.y[i]), c.ywt[i]));
   etest = ddiv(step_norm<N, JAC>(c.s2), TQ(2, c.nq) * sqn);
   if (etest > eps) {
     c.t = told;
@@ -794,7 +814,7 @@ L170:
       const double rh2 = ddiv(1.0, BIAS2 * npow(ddiv(etest, eps), ddiv(1.0, (double)(c.nq + 1))));
       if (c.nq > 1) {
 #pragma unroll
-        for (int i = 0; i < N; ++i) c.s2[i] = ddiv(c.yh(c.nq, i), NRG_FMAX(fabs(c.y[i]), c.ywt[i]));
+        for (int i = 0; i < N; ++i) c.s2[i] = wdiv<JAC>(c.yh(c.nq, i), NRG_FMAX(fabs(c.y[i]), c.ywt[i]));
         const double erdn = ddiv(step_norm<N, JAC>(c.s2), TQ(1, c.nq) * sqn);
         const double rh1 = ddiv(1.0, NRG_FMAX(1.0, BIAS1 * npow(ddiv(erdn, eps), ddiv(1.0, (double)c.nq))));
         if (rh2 < rh1) {
@@ -842,7 +862,7 @@ L170:
       rh1 = 0.0;
     } else {
 #pragma unroll
-      for (int i = 0; i < N; ++i) c.s2[i] = ddiv(c.yh(c.nq, i), NRG_FMAX(fabs(c.y[i]), c.ywt[i]));
+      for (int i = 0; i < N; ++i) c.s2[i] = wdiv<JAC>(c.yh(c.nq, i), NRG_FMAX(fabs(c.y[i]), c.ywt[i]));
       const double erdn = ddiv(step_norm<N, JAC>(c.s2), TQ(1, c.nq) * sqn);
       rh1 = ddiv(1.0, NRG_FMAX(uround, BIAS1 * npow(ddiv(erdn, eps), ddiv(1.0, (double)c.nq))));
     }
@@ -852,7 +872,7 @@ L170:
     } else {
 #pragma unroll
       for (int i = 0; i < N; ++i)
-        c.s2[i] = ddiv(c.s1[i] - c.yh(kMaxOrd, i), NRG_FMAX(fabs(c.y[i]), c.ywt[i]));
+        c.s2[i] = wdiv<JAC>(c.s1[i] - c.yh(kMaxOrd, i), NRG_FMAX(fabs(c.y[i]), c.ywt[i]));
       const double erup = ddiv(step_norm<N, JAC>(c.s2), TQ(3, c.nq) * sqn);
       rh3 = ddiv(1.0, NRG_FMAX(uround, BIAS3 * npow(ddiv(erup, eps), ddiv(1.0, (double)(c.nq + 2)))));
     }
