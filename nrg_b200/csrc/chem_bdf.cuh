@@ -42,8 +42,9 @@ enum JacMode { kJacFD = 0, kJacAnalytic = 1 };
 // Per-cell arrays live in shared memory in an [element][thread] layout: for
 // element e, the BS threads of a block touch BS consecutive words, so every
 // warp access is bank-conflict free.  Vectors that are only ever indexed by
-// unrolled loops (y, YWT, SAVE1, SAVE2, FAC) stay in registers; the pivot
-// vector is packed into one 64-bit register (4 bits per row).
+// unrolled loops (y, YWT, SAVE1, SAVE2, FAC) stay in registers; the row
+// permutation of the LU factors is packed into one or two 64-bit registers
+// (RowPerm).
 template <int N, int R, typename LUT, int BS>
 struct SmemStore {
   static constexpr int kYH = 0;
@@ -73,6 +74,37 @@ struct SmemStore {
 template <int N, int R, typename LUT, int BS, int NF = N, int SPEC = 0>
 struct CellState;
 
+// Row permutation of the LU factors, packed in registers: row indices 0..N-1
+// in 4-bit fields up to 16 rows, else in 5-bit fields (12 per 64-bit word).
+template <int N>
+struct RowPerm {
+  static constexpr int kBits = N <= 16 ? 4 : 5;
+  static constexpr int kPer = 64 / kBits;
+  static constexpr int kWords = (N + kPer - 1) / kPer;
+  static constexpr unsigned long long kMask = (1ull << kBits) - 1ull;
+  unsigned long long w[kWords];
+  __device__ __forceinline__ void identity() {
+#pragma unroll
+    for (int q = 0; q < kWords; ++q) w[q] = 0;
+#pragma unroll
+    for (int k = 0; k < N; ++k) w[k / kPer] |= (unsigned long long)k << ((k % kPer) * kBits);
+  }
+  __device__ __forceinline__ int get(int k) const {
+    const int q = k / kPer, r = (k - q * kPer) * kBits;
+    unsigned long long x = w[0];
+#pragma unroll
+    for (int i = 1; i < kWords; ++i)
+      if (q == i) x = w[i];
+    return (int)((x >> r) & kMask);
+  }
+  __device__ __forceinline__ void set(int k, int v) {
+    const int q = k / kPer, r = (k - q * kPer) * kBits;
+#pragma unroll
+    for (int i = 0; i < kWords; ++i)
+      if (q == i) w[i] = (w[i] & ~(kMask << r)) | ((unsigned long long)v << r);
+  }
+};
+
 // Out-of-line hot routines of the thread-per-cell integrator.  They touch only
 // the cell's shared-memory arrays (passed as the two base pointers), so the
 // register-resident vectors are never forced to local memory by the call.
@@ -81,7 +113,7 @@ __device__ __noinline__ void nl_rhs(double* d, LUT* f);
 template <int N, int R, typename LUT, int BS, int SPEC>
 __device__ __noinline__ void nl_analytic_matrix(double* d, LUT* f, double factor);
 template <int N, int R, typename LUT, int BS, bool RECIP>
-__device__ __noinline__ unsigned long long nl_dgefa(double* d, LUT* f, int* info);
+__device__ __noinline__ RowPerm<N> nl_dgefa(double* d, LUT* f, int* info);
 template <int N, int R, typename LUT, int BS>
 __device__ __noinline__ void nl_rate_constants(double* d, LUT* f, double T);
 
@@ -94,10 +126,9 @@ struct CellState : SmemStore<N, R, LUT, BS> {
   static constexpr int kNF = NF;
   static constexpr int kSpec = SPEC;
   double y[N], ywt[N], s1[N], s2[N], fac[N];
-  unsigned long long piv;  // ipvt, 4 bits per row
+  RowPerm<N> piv;  // row i of the factors is row piv.get(i) of the matrix
   double h, t, tout, rc, rmax, trend, eps;
   int nq, nwait, jtask, nstep, nfe, nje, nsolve, jstepl, nstepl, convrg, ier;
-  __device__ __forceinline__ int ipvt(int k) const { return (int)((piv >> (4 * k)) & 15ull); }
 };
 
 // Register-array element with a runtime index (select chain, no local memory).
@@ -449,16 +480,21 @@ __device__ __forceinline__ double step_norm(const double (&dx)[N]) {
   }
 }
 
-// dgefa.f90:60-117 on the shared-memory matrix (column-major a(j, i) = A(i, j)).
-// RECIP: each pivot is replaced by its reciprocal (the -1/pivot the
-// elimination forms anyway, negated), so that dgesl<RECIP> multiplies where
-// the reference divides; used by the analytic-Jacobian and mixed modes, whose
-// results agree with the reference's to its tolerance, not bit for bit.
+// dgefa.f90:60-117 on the shared-memory matrix (column-major a(j, i) = A(i, j)):
+// the same pivot choices, eliminations and roundings as LINPACK, with the
+// row interchanges also applied to the multipliers of earlier columns (as
+// LAPACK's getrf stores them), so that dgesl applies the whole permutation
+// once instead of one interchange per column.  RECIP: each pivot is replaced
+// by its reciprocal (the -1/pivot the elimination forms anyway, negated), so
+// that dgesl<RECIP> multiplies where the reference divides; used by the
+// analytic-Jacobian and mixed modes, whose results agree with the reference's
+// to its tolerance, not bit for bit.
 template <int N, bool RECIP, class CS>
-__device__ __forceinline__ int dgefa(CS& c, unsigned long long* piv_out) {
+__device__ __forceinline__ int dgefa(CS& c, RowPerm<N>* perm_out) {
   using LUT = typename std::remove_reference<decltype(c.a(0, 0))>::type;
   int info = 0;
-  unsigned long long piv = 0;
+  RowPerm<N> perm;
+  perm.identity();
 #pragma unroll 1
   for (int k = 0; k < N - 1; ++k) {
     int l = k;
@@ -467,12 +503,19 @@ __device__ __forceinline__ int dgefa(CS& c, unsigned long long* piv_out) {
       const LUT xm = fabs(c.a(k, i));
       if (xm > dmax) { l = i; dmax = xm; }
     }
-    piv |= (unsigned long long)l << (4 * k);
     if (c.a(k, l) == (LUT)0) { info = k + 1; continue; }
     if (l != k) {
       const LUT t = c.a(k, l);
       c.a(k, l) = c.a(k, k);
       c.a(k, k) = t;
+      for (int j = 0; j < k; ++j) {
+        const LUT m = c.a(j, l);
+        c.a(j, l) = c.a(j, k);
+        c.a(j, k) = m;
+      }
+      const int pk = perm.get(k);
+      perm.set(k, perm.get(l));
+      perm.set(l, pk);
     }
     const LUT t = (LUT)-1 / c.a(k, k);
     if (RECIP) c.a(k, k) = -t;
@@ -487,25 +530,26 @@ __device__ __forceinline__ int dgefa(CS& c, unsigned long long* piv_out) {
         for (int i = k + 1; i < N; ++i) c.a(j, i) = c.a(j, i) + tj * c.a(k, i);
     }
   }
-  piv |= (unsigned long long)(N - 1) << (4 * (N - 1));
-  *piv_out = piv;
+  *perm_out = perm;
   if (c.a(N - 1, N - 1) == (LUT)0) info = N;
   else if (RECIP) c.a(N - 1, N - 1) = (LUT)1 / c.a(N - 1, N - 1);
   return info;
 }
 
-// dgesl.f90:71-131, JOB = 0, on the register vector b (RECIP: the factors
-// hold the pivots' reciprocals, see dgefa)
+// dgesl.f90:71-131, JOB = 0, on the register vector b.  The permutation is
+// applied at once through the cell's shared scratch z (free during a solve),
+// then the forward sweep runs without interchanges: each element receives
+// the same updates in the same order as in LINPACK's interleaved form.
+// RECIP: the factors hold the pivots' reciprocals (see dgefa).
 template <int N, bool RECIP, class CS>
 __device__ __forceinline__ void dgesl(CS& c, double (&b)[N]) {
 #pragma unroll
+  for (int i = 0; i < N; ++i) c.z(i) = b[i];
+#pragma unroll
+  for (int i = 0; i < N; ++i) b[i] = c.z(c.piv.get(i));
+#pragma unroll
   for (int k = 0; k < N - 1; ++k) {
-    const int l = c.ipvt(k);
-    const double t = sel(b, l);
-    if (l != k) {
-      put(b, l, b[k]);
-      b[k] = t;
-    }
+    const double t = b[k];
     if (t != 0.0) {
 #pragma unroll
       for (int i = k + 1; i < N; ++i) b[i] = b[i] + t * (double)c.a(k, i);
@@ -549,13 +593,13 @@ __device__ __noinline__ void nl_analytic_matrix(double* d, LUT* f, double factor
 }
 
 template <int N, int R, typename LUT, int BS, bool RECIP>
-__device__ __noinline__ unsigned long long nl_dgefa(double* d, LUT* f, int* info) {
+__device__ __noinline__ RowPerm<N> nl_dgefa(double* d, LUT* f, int* info) {
   SmemStore<N, R, LUT, BS> s;
   s.d = d;
   s.f = f;
-  unsigned long long piv = 0;
-  *info = dgefa<N, RECIP>(s, &piv);
-  return piv;
+  RowPerm<N> perm;
+  *info = dgefa<N, RECIP>(s, &perm);
+  return perm;
 }
 
 template <int N, int R, typename LUT, int BS>
@@ -981,7 +1025,7 @@ __device__ bool cell_begin(CS& c, const StepArgs& a, long cid) {
   c.rmax = 10000.0;
   c.trend = 1.0;
   c.nwait = 3;
-  c.piv = 0;
+  c.piv.identity();
   return true;
 }
 
