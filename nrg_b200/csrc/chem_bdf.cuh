@@ -612,23 +612,42 @@ __device__ __noinline__ void nl_rate_constants(double* d, LUT* f, double T) {
 
 // --------------------------------------------------------- SLATEC pieces
 // ddpsc.f90:22-40 on the Nordsieck array (shared memory only, so one
-// out-of-line copy serves every call site).
+// out-of-line copy serves every call site).  Species do not mix, so each
+// species' column of the array is loaded into registers once, takes the
+// reference's additions in the reference's order, and is stored once.
+template <int N, int Q, class S>
+__device__ __forceinline__ void ddpsc_order(S& c, int ksgn) {
+#pragma unroll 1
+  for (int i = 0; i < N; ++i) {
+    double v[Q + 1];
+#pragma unroll
+    for (int j = 0; j <= Q; ++j) v[j] = c.yh(j, i);
+#pragma unroll
+    for (int j1 = 1; j1 <= Q; ++j1)
+#pragma unroll
+      for (int j2 = j1; j2 <= Q; ++j2) {
+        const int j = Q - j2 + j1;  // 1-based column
+        v[j - 1] = ksgn > 0 ? v[j - 1] + v[j] : v[j - 1] - v[j];
+      }
+#pragma unroll
+    for (int j = 0; j < Q; ++j) c.yh(j, i) = v[j];
+  }
+}
+
 template <int N, int R, typename LUT, int BS>
 __device__ __noinline__ void nl_ddpsc(double* d, LUT* f, int ksgn, int nq) {
   SmemStore<N, R, LUT, BS> c;
   c.d = d;
   c.f = f;
-  for (int j1 = 1; j1 <= nq; ++j1)
-    for (int j2 = j1; j2 <= nq; ++j2) {
-      const int j = nq - j2 + j1;  // 1-based column
-      if (ksgn > 0) {
-#pragma unroll
-        for (int i = 0; i < N; ++i) c.yh(j - 1, i) = c.yh(j - 1, i) + c.yh(j, i);
-      } else {
-#pragma unroll
-        for (int i = 0; i < N; ++i) c.yh(j - 1, i) = c.yh(j - 1, i) - c.yh(j, i);
-      }
-    }
+  static_assert(kMaxOrd == 5, "one unrolled predictor per order");
+  switch (nq) {
+    case 1: ddpsc_order<N, 1>(c, ksgn); break;
+    case 2: ddpsc_order<N, 2>(c, ksgn); break;
+    case 3: ddpsc_order<N, 3>(c, ksgn); break;
+    case 4: ddpsc_order<N, 4>(c, ksgn); break;
+    case 5: ddpsc_order<N, 5>(c, ksgn); break;
+    default: break;
+  }
 }
 
 template <int N, class CS>
