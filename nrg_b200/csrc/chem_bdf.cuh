@@ -439,44 +439,57 @@ __device__ __forceinline__ double dnrm2(const double (&dx)[N]) {
   return dnrm2_nl<N>(t);
 }
 
-// Division by a weight of the step and error norms.  Reference mode: the
-// reference's division.  Analytic-Jacobian and mixed modes: multiplication by
-// a reciprocal from the hardware approximation (rcp.approx.ftz.f64) refined by
-// one Newton step r (1 + (1 - w r)), which squares its relative error (to
-// about 2^-44): these norms only steer step sizes, orders and the error test.
-// Weights are at least the error-weight floor, so w is a positive normal
-// number unless it is not finite (then the division is used).
-template <int JAC>
-__device__ __forceinline__ double wdiv(double x, double w) {
-  if constexpr (JAC == kJacFD) {
-    return ddiv(x, w);
-  } else {
-    if (!(w < 1e300)) return ddiv(x, w);
-    double r;
-    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(w));
-    const double e = fma(-w, r, 1.0);
-    return x * fma(r, e, r);
-  }
-}
-
 // sqrt by Newton's iteration at compile time (constant scale factors).
 __host__ __device__ constexpr double ct_sqrt(double x, double g = 1.0, int it = 0) {
   return it == 64 ? g : ct_sqrt(x, 0.5 * (g + x / g), it + 1);
 }
 
-// Weighted norms of the step and error tests.  Reference mode: dnrm2, for the
-// reference's bits.  Analytic-Jacobian and mixed modes: sqrt of the sum of
-// squares in registers (no divisions, no call), which differs from dnrm2 by
-// rounding only; dnrm2 takes over if the sum leaves the safe range.
-template <int N, int JAC>
-__device__ __forceinline__ double step_norm(const double (&dx)[N]) {
-  if constexpr (JAC == kJacFD) {
-    return dnrm2<N>(dx);
-  } else {
-    double s = 0.0;
+// Weighted two-norm sqrt(sum_i (x_i / max(|y_i|, YWT_i))^2) of the corrector,
+// error and order tests (ddcor.f90, ddstp.f90).  Reference mode: the
+// reference's divisions and dnrm2.  Analytic-Jacobian and mixed modes: one
+// pass over the species with the weights' reciprocals from the hardware
+// approximation (rcp.approx.ftz.f64) refined by one Newton step
+// r (1 + (1 - w r)), which squares its relative error to about 2^-44, and a
+// plain sum of squares: it differs by rounding only, and these norms only
+// steer step sizes, orders and the error test.  Weights are at least the
+// error-weight floor; if one is not finite or the sum leaves the safe range,
+// the reference form (out of line, so the fast path stays compact) is used.
+template <int N>
+__device__ __noinline__ double weighted_norm_ref(const double* x, const double* y, const double* ywt) {
+  double q[N];
 #pragma unroll
-    for (int i = 0; i < N; ++i) s = fma(dx[i], dx[i], s);
-    return s < 1e300 ? sqrt(s) : dnrm2<N>(dx);
+  for (int i = 0; i < N; ++i) q[i] = ddiv(x[i], NRG_FMAX(fabs(y[i]), ywt[i]));
+  return dnrm2_nl<N>(q);
+}
+
+template <int N, int JAC, class CS>
+__device__ __forceinline__ double weighted_norm(const CS& c, const double (&x)[N]) {
+  if constexpr (JAC == kJacFD) {
+    double q[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) q[i] = ddiv(x[i], NRG_FMAX(fabs(c.y[i]), c.ywt[i]));
+    return dnrm2<N>(q);
+  } else {
+    double sum = 0.0;
+    bool ok = true;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      const double w = NRG_FMAX(fabs(c.y[i]), c.ywt[i]);
+      ok = ok && (w < 1e300);
+      double r;
+      asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(w));
+      const double q = x[i] * fma(r, fma(-w, r, 1.0), r);
+      sum = fma(q, q, sum);
+    }
+    if (ok && sum < 1e300) return sqrt(sum);
+    double xs[N], ys[N], ws[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      xs[i] = x[i];
+      ys[i] = c.y[i];
+      ws[i] = c.ywt[i];
+    }
+    return weighted_norm_ref<N>(xs, ys, ws);
   }
 }
 
@@ -790,12 +803,12 @@ __device__ double ddcor(CS& c) {
 #pragma unroll
   for (int i = 0; i < N; ++i) {
     c.s1[i] = c.s1[i] + x[i];
-    c.s2[i] = wdiv<JAC>(x[i], NRG_FMAX(fabs(c.y[i]), c.ywt[i]));
   }
-  if constexpr (JAC == kJacFD) return ddiv(dnrm2<N>(c.s2), sqrt((double)CS::kNF));
-  else {
+  if constexpr (JAC == kJacFD) {
+    return ddiv(weighted_norm<N, JAC>(c, x), sqrt((double)CS::kNF));
+  } else {
     constexpr double kInvSqrtNF = 1.0 / ct_sqrt((double)CS::kNF);
-    return step_norm<N, JAC>(c.s2) * kInvSqrtNF;
+    return weighted_norm<N, JAC>(c, x) * kInvSqrtNF;
   }
 }
 
@@ -865,9 +878,7 @@ L160:
   goto L100;
 L170:
   c.convrg = 1;
-#pragma unroll
-  for (int i = 0; i < N; ++i) c.s2[i] = wdiv<JAC>(c.s1[i], NRG_FMAX(fabs(c.y[i]), c.ywt[i]));
-  etest = ddiv(step_norm<N, JAC>(c.s2), TQ(2, c.nq) * sqn);
+  etest = ddiv(weighted_norm<N, JAC>(c, c.s1), TQ(2, c.nq) * sqn);
   if (etest > eps) {
     c.t = told;
     ddpsc<N>(-1, c);
@@ -876,9 +887,10 @@ L170:
       if (c.jtask != 0 && c.jtask != 2) c.rmax = RMFAIL;
       const double rh2 = ddiv(1.0, BIAS2 * npow(ddiv(etest, eps), ddiv(1.0, (double)(c.nq + 1))));
       if (c.nq > 1) {
+        double v[N];
 #pragma unroll
-        for (int i = 0; i < N; ++i) c.s2[i] = wdiv<JAC>(c.yh(c.nq, i), NRG_FMAX(fabs(c.y[i]), c.ywt[i]));
-        const double erdn = ddiv(step_norm<N, JAC>(c.s2), TQ(1, c.nq) * sqn);
+        for (int i = 0; i < N; ++i) v[i] = c.yh(c.nq, i);
+        const double erdn = ddiv(weighted_norm<N, JAC>(c, v), TQ(1, c.nq) * sqn);
         const double rh1 = ddiv(1.0, NRG_FMAX(1.0, BIAS1 * npow(ddiv(erdn, eps), ddiv(1.0, (double)c.nq))));
         if (rh2 < rh1) {
           c.nq = c.nq - 1;
@@ -924,19 +936,20 @@ L170:
     if (c.nq == 1) {
       rh1 = 0.0;
     } else {
+      double v[N];
 #pragma unroll
-      for (int i = 0; i < N; ++i) c.s2[i] = wdiv<JAC>(c.yh(c.nq, i), NRG_FMAX(fabs(c.y[i]), c.ywt[i]));
-      const double erdn = ddiv(step_norm<N, JAC>(c.s2), TQ(1, c.nq) * sqn);
+      for (int i = 0; i < N; ++i) v[i] = c.yh(c.nq, i);
+      const double erdn = ddiv(weighted_norm<N, JAC>(c, v), TQ(1, c.nq) * sqn);
       rh1 = ddiv(1.0, NRG_FMAX(uround, BIAS1 * npow(ddiv(erdn, eps), ddiv(1.0, (double)c.nq))));
     }
     rh2 = ddiv(1.0, NRG_FMAX(uround, BIAS2 * npow(ddiv(etest, eps), ddiv(1.0, (double)(c.nq + 1)))));
     if (c.nq == kMaxOrd) {
       rh3 = 0.0;
     } else {
+      double v[N];
 #pragma unroll
-      for (int i = 0; i < N; ++i)
-        c.s2[i] = wdiv<JAC>(c.s1[i] - c.yh(kMaxOrd, i), NRG_FMAX(fabs(c.y[i]), c.ywt[i]));
-      const double erup = ddiv(step_norm<N, JAC>(c.s2), TQ(3, c.nq) * sqn);
+      for (int i = 0; i < N; ++i) v[i] = c.s1[i] - c.yh(kMaxOrd, i);
+      const double erup = ddiv(weighted_norm<N, JAC>(c, v), TQ(3, c.nq) * sqn);
       rh3 = ddiv(1.0, NRG_FMAX(uround, BIAS3 * npow(ddiv(erup, eps), ddiv(1.0, (double)(c.nq + 2)))));
     }
     if (rh1 > rh2 && rh1 >= rh3) {
