@@ -42,7 +42,11 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--mode", default="auto", choices=["auto", "surrogate", "fast", "reference", "mixed"])
-    p.add_argument("--n-side", type=int, default=2048)
+    p.add_argument("--field", default="flame", choices=["flame", "wide-range", "ignition"],
+                   help="flame: 2048^2 flame field, dt=1e-6 s (the headline workload); wide-range: 1024^2 cells, "
+                        "T~U[800,2600] K, p~U[0.5,5] atm, dt=1e-5 s; ignition: 512^2 cells, dt=1e-5 s, 20%% of "
+                        "them within 50 K of the 1e-5 s ignition temperature")
+    p.add_argument("--n-side", type=int, default=None, help="cells per side (default: the field's own size)")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--kernel", choices=["thread", "thread_queue", "warp_queue"], default=None,
@@ -62,7 +66,24 @@ def parse():
     p.add_argument("--no-state-eq", dest="state_eq", action="store_false",
                    help="skip timing the sources + state-equation update of the field "
                         "(nrg_chem_apply_state_device)")
-    return p.parse_args()
+    a = p.parse_args()
+    if a.n_side is None:
+        a.n_side = {"flame": 2048, "wide-range": 1024, "ignition": 512}[a.field]
+    return a
+
+
+def make_field(F, W, args):
+    """The workload's synthetic cell field and its one-line description."""
+    if args.field == "wide-range":
+        f = F.wide_range_field(W, n_side=args.n_side)
+        return f, (f"wide-range field {args.n_side}x{args.n_side} ({f.n:,} cells), dt=1e-5 s, "
+                   "T~U[800,2600] K, p~U[0.5,5] atm")
+    if args.field == "ignition":
+        f = F.ignition_field(W, n_side=args.n_side)
+        return f, (f"ignition field {args.n_side}x{args.n_side} ({f.n:,} cells), dt=1e-5 s, p=1 atm, 20% of cells "
+                   "within 50 K of the 1e-5 s ignition temperature")
+    f = F.flame_field(W, n_side=args.n_side)
+    return f, f"flame field {args.n_side}x{args.n_side} ({f.n:,} cells), dt=1e-6 s, p=1 atm"
 
 
 # --------------------------------------------------------------- helpers
@@ -230,7 +251,7 @@ def run_reference(args):
     from nrg_b200.chemistry import mechanism_tables
     decks = keromnes_paths()
     W = mechanism_tables(*decks)["molar_mass"]
-    field = F.flame_field(W, n_side=args.n_side)
+    field, desc = make_field(F, W, args)
     from oracle import oracle_py as op
     m = op.Mechanism(*decks, 1.0, "cal.mol")
     cores = os.cpu_count() or 1
@@ -248,14 +269,13 @@ def run_reference(args):
         m.chem_step(samp.dt, samp.T, samp.rho, samp.Y, threads=cores)
     el = time.perf_counter() - t0
     value = args.steps * n / el
-    sample = (f"{n} cells per step drawn uniformly (seeded) from the {args.n_side}x{args.n_side} flame field; "
+    sample = (f"{n} cells per step drawn uniformly (seeded) from the {desc}; "
               f"C restatement of the reference Fortran + SLATEC DDRIV3 path (no Fortran compiler on the box)")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": {"workload": f"flame field {args.n_side}x{args.n_side} ({field.n:,} cells), "
-                                                    "dt=1e-6 s, p=1 atm, KEROMNES H2/air; CPU sample"},
+        "data": "synthetic", "config": {"workload": f"{desc}, KEROMNES H2/air; CPU sample"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
@@ -381,7 +401,12 @@ def main():
     W = tables["molar_mass"]
     dev = torch.device("cuda", local)
     solver = ChemicalKineticsSolver(None, *decks, E_act_units=units, mode="fast")
-    field = F.flame_field(mechanism_tables(*keromnes_paths())["molar_mass"], n_side=args.n_side)
+    field, desc = make_field(F, mechanism_tables(*keromnes_paths())["molar_mass"], args)
+    if args.field != "flame":
+        # the widened rows are timed on flame blocks only
+        args.predictor = args.diffusivity = args.state_eq = False
+        if args.mechanism != "KEROMNES":
+            raise SystemExit("--field other than flame is for the KEROMNES mechanism")
     if args.mechanism == "ACETYLENE":
         # the same flame geometry with the C2H2/O2/Ar mixture
         field = F.acetylene_flame(solver.species_names[:tables["n_species"]], W, n_side=args.n_side)
@@ -393,6 +418,12 @@ def main():
         args.no_e2e = True
     n = field.n
     T, rho, Y = (torch.tensor(a, device=dev) for a in (field.T, field.rho, field.Y))
+    in_bytes = n * (8 * (2 + Y.shape[0]) + 1)
+    # inputs smaller than L2 (126 MB): a 256 MB buffer is rewritten between
+    # timed steps so that every step reads its inputs from HBM
+    l2_flush = torch.empty(32 << 20, dtype=torch.float64, device=dev) if in_bytes < (126 << 20) else None
+    l2_note = (f"inputs ({in_bytes / 1e6:.0f} MB) larger than L2; no flush" if l2_flush is None else
+               f"inputs ({in_bytes / 1e6:.0f} MB) smaller than L2: 256 MB written between timed steps (in the timed time)")
 
     solver.set_cell_order(args.cell_order == "temperature")
     # launch shape of the FP64 integrator: autotuned on a contiguous block of
@@ -445,6 +476,8 @@ def main():
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
             for _ in range(args.steps):
+                if l2_flush is not None:
+                    l2_flush.fill_(1.0)
                 stats.append(solver.step_device(field.dt, T, rho, Y, Yp, Yp2, Ef, T_after=Ta, status=st))
             e1.record()
             torch.cuda.synchronize()
@@ -588,14 +621,14 @@ def main():
             "warmup": args.warmup, "ms_per_step": el / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64+bf16" if mode == "surrogate" else "f64",
             "data": "synthetic",
-            "config": {"workload": f"flame field {args.n_side}x{args.n_side} ({n:,} cells), dt=1e-6 s, p=1 atm, "
+            "config": {"workload": f"{desc}, "
                                    f"{args.mechanism} {'C2H2/O2/Ar' if args.mechanism == 'ACETYLENE' else 'H2/air'} ({tables['n_species']} species, "
                                    f"{tables['n_reactions']} reactions)",
                        "path": {"fast": "plain FP64 integrator, analytic Jacobian",
                                 "reference": "plain FP64 integrator, reference FD Jacobian",
                                 "mixed": "FP32 LU + FP64 residual/refinement",
                                 "surrogate": "BF16 MLP surrogate + gated FP64 fallback"}[mode],
-                       "launch": launch, "cell_order": args.cell_order, "l2": "inputs (370 MB) larger than L2; no flush",
+                       "launch": launch, "cell_order": args.cell_order, "l2": l2_note,
                        "active_cells": int(ph["cells_active"])},
             "plain_fp64": {"value": plain_value, "ms_per_step": el_plain / args.steps,
                            "ratio_surrogate_over_plain": value / plain_value},
