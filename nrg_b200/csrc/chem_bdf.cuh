@@ -439,6 +439,18 @@ __device__ __forceinline__ double dnrm2(const double (&dx)[N]) {
   return dnrm2_nl<N>(t);
 }
 
+// Power of an error ratio in the step-size and order choices (ddstp.f90).
+// Reference mode: the reference's pow.  Analytic-Jacobian and mixed modes:
+// 2^(p log2 x) in single precision, relative error about 1e-6, which only
+// scales the next step size; outside [1e-30, 1e30] the double pow is used.
+template <int JAC>
+__device__ __forceinline__ double ratio_pow(double x, double p) {
+  if constexpr (JAC != kJacFD) {
+    if (x > 1e-30 && x < 1e30) return (double)exp2f((float)p * __log2f((float)x));
+  }
+  return npow(x, p);
+}
+
 // sqrt by Newton's iteration at compile time (constant scale factors).
 __host__ __device__ constexpr double ct_sqrt(double x, double g = 1.0, int it = 0) {
   return it == 64 ? g : ct_sqrt(x, 0.5 * (g + x / g), it + 1);
@@ -872,7 +884,7 @@ L160:
   ddpsc<N>(-1, c);
   c.nwait = c.nq + 2;
   if (c.jtask != 0 && c.jtask != 2) c.rmax = RMFAIL;
-  rh = (iter == 0) ? 0.3 : 0.9 * npow(ddiv(eps, ctest), 0.2);
+  rh = (iter == 0) ? 0.3 : 0.9 * ratio_pow<JAC>(ddiv(eps, ctest), 0.2);
   if (rh * c.h == 0.0) goto L400;
   ddscl<N>(c, rh);
   goto L100;
@@ -885,13 +897,13 @@ L170:
     nfail = nfail + 1;
     if (nfail < MXFAIL || c.nq == 1) {
       if (c.jtask != 0 && c.jtask != 2) c.rmax = RMFAIL;
-      const double rh2 = ddiv(1.0, BIAS2 * npow(ddiv(etest, eps), ddiv(1.0, (double)(c.nq + 1))));
+      const double rh2 = ddiv(1.0, BIAS2 * ratio_pow<JAC>(ddiv(etest, eps), ddiv(1.0, (double)(c.nq + 1))));
       if (c.nq > 1) {
         double v[N];
 #pragma unroll
         for (int i = 0; i < N; ++i) v[i] = c.yh(c.nq, i);
         const double erdn = ddiv(weighted_norm<N, JAC>(c, v), TQ(1, c.nq) * sqn);
-        const double rh1 = ddiv(1.0, NRG_FMAX(1.0, BIAS1 * npow(ddiv(erdn, eps), ddiv(1.0, (double)c.nq))));
+        const double rh1 = ddiv(1.0, NRG_FMAX(1.0, BIAS1 * ratio_pow<JAC>(ddiv(erdn, eps), ddiv(1.0, (double)c.nq))));
         if (rh2 < rh1) {
           c.nq = c.nq - 1;
           c.rc = ddiv(c.rc * EL(1, c.nq), EL(1, c.nq + 1));
@@ -923,7 +935,7 @@ L170:
 #pragma unroll
   for (int i = 0; i < N; ++i) c.y[i] = c.yh(0, i);
   if (c.jtask == 0 || c.jtask == 2) {
-    rh = ddiv(1.0, NRG_FMAX(uround, BIAS2 * npow(ddiv(etest, eps), ddiv(1.0, (double)(c.nq + 1)))));
+    rh = ddiv(1.0, NRG_FMAX(uround, BIAS2 * ratio_pow<JAC>(ddiv(etest, eps), ddiv(1.0, (double)(c.nq + 1)))));
     if (rh > TRSHLD) ddscl<N>(c, rh);
   } else if (c.nwait > 1) {
     c.nwait = c.nwait - 1;
@@ -940,9 +952,9 @@ L170:
 #pragma unroll
       for (int i = 0; i < N; ++i) v[i] = c.yh(c.nq, i);
       const double erdn = ddiv(weighted_norm<N, JAC>(c, v), TQ(1, c.nq) * sqn);
-      rh1 = ddiv(1.0, NRG_FMAX(uround, BIAS1 * npow(ddiv(erdn, eps), ddiv(1.0, (double)c.nq))));
+      rh1 = ddiv(1.0, NRG_FMAX(uround, BIAS1 * ratio_pow<JAC>(ddiv(erdn, eps), ddiv(1.0, (double)c.nq))));
     }
-    rh2 = ddiv(1.0, NRG_FMAX(uround, BIAS2 * npow(ddiv(etest, eps), ddiv(1.0, (double)(c.nq + 1)))));
+    rh2 = ddiv(1.0, NRG_FMAX(uround, BIAS2 * ratio_pow<JAC>(ddiv(etest, eps), ddiv(1.0, (double)(c.nq + 1)))));
     if (c.nq == kMaxOrd) {
       rh3 = 0.0;
     } else {
@@ -950,7 +962,7 @@ L170:
 #pragma unroll
       for (int i = 0; i < N; ++i) v[i] = c.s1[i] - c.yh(kMaxOrd, i);
       const double erup = ddiv(weighted_norm<N, JAC>(c, v), TQ(3, c.nq) * sqn);
-      rh3 = ddiv(1.0, NRG_FMAX(uround, BIAS3 * npow(ddiv(erup, eps), ddiv(1.0, (double)(c.nq + 2)))));
+      rh3 = ddiv(1.0, NRG_FMAX(uround, BIAS3 * ratio_pow<JAC>(ddiv(erup, eps), ddiv(1.0, (double)(c.nq + 2)))));
     }
     if (rh1 > rh2 && rh1 >= rh3) {
       rh = rh1;
