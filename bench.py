@@ -38,7 +38,7 @@ D2H_BYTES_PER_CELL = 19 * 8 + 1   # 9 Y_prod, 9 Y_prod2, E_f_prod, status
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--mode", default="auto", choices=["auto", "surrogate", "fast", "reference", "mixed"])
@@ -88,9 +88,13 @@ def make_field(F, W, args):
 
 # --------------------------------------------------------------- helpers
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons, kept for the timed region only.
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    The sampler starts before the warm-up steps (nvidia-smi needs a moment
+    before its first sample); begin() and end() mark the timed region and
+    summary() keeps the samples whose nvidia-smi timestamps fall inside it."""
+
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -99,11 +103,12 @@ class ClockSampler:
         self.rows = []
         self._p = None
         self._t = None
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         try:
             self._p = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
-                                        "--format=csv,noheader,nounits", "-lms", "200"],
+                                        "--format=csv,noheader,nounits", "-lms", "100"],
                                        stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self._t = threading.Thread(target=self._read, daemon=True)
             self._t.start()
@@ -115,6 +120,12 @@ class ClockSampler:
         for line in self._p.stdout:
             self.rows.append([x.strip() for x in line.split(",")])
 
+    def begin(self):
+        self.t0 = time.time()
+
+    def end(self):
+        self.t1 = time.time()
+
     def __exit__(self, *a):
         if self._p:
             self._p.terminate()
@@ -123,20 +134,32 @@ class ClockSampler:
             except Exception:
                 self._p.kill()
 
+    @staticmethod
+    def _when(ts: str):
+        import datetime
+        try:
+            return datetime.datetime.strptime(ts, "%Y/%m/%d %H:%M:%S.%f").timestamp()
+        except ValueError:
+            return None
+
     def summary(self) -> dict:
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for r in self.rows:
             try:
-                sm.append(float(r[1]))
-                mx = float(r[2])
+                t = self._when(r[0])
+                if t is None or self.t0 is None or not (self.t0 <= t <= self.t1):
+                    continue
+                sm.append(float(r[2]))
+                mx = float(r[3])
                 for i, nm in enumerate(names):
-                    if r[5 + i].lower().startswith("active"):
+                    if r[6 + i].lower().startswith("active"):
                         reasons.add(nm)
             except (ValueError, IndexError):
                 continue
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "window_s": None if self.t0 is None else round(self.t1 - self.t0, 3)}
 
 
 def flop_model(tables: dict, mode: str) -> dict:
@@ -466,13 +489,14 @@ def main():
     def time_arm(arm_mode):
         Yp, Yp2, Ef, Ta, st = make_out()
         solver.set_mode(arm_mode)
-        for _ in range(args.warmup):
-            solver.step_device(field.dt, T, rho, Y, Yp, Yp2, Ef, T_after=Ta, status=st)
-        torch.cuda.synchronize()
-        dist.barrier()
         stats = []
         with ClockSampler(local) as clk:
+            for _ in range(args.warmup):
+                solver.step_device(field.dt, T, rho, Y, Yp, Yp2, Ef, T_after=Ta, status=st)
             torch.cuda.synchronize()
+            dist.barrier()
+            torch.cuda.synchronize()
+            clk.begin()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
             for _ in range(args.steps):
@@ -481,6 +505,7 @@ def main():
                 stats.append(solver.step_device(field.dt, T, rho, Y, Yp, Yp2, Ef, T_after=Ta, status=st))
             e1.record()
             torch.cuda.synchronize()
+            clk.end()
         el = dist.max_over_ranks(e0.elapsed_time(e1), dev)  # the job's time: its slowest rank
         # one untimed step with per-phase events for the roofline
         solver.set_timing(True)

@@ -340,6 +340,12 @@ NRG_API int nrg_surrogate_train(nrg_chem* h, long n, const void* x_bf16, const f
  * written dY (K); |dT| bound (K). */
 NRG_API int nrg_surrogate_set_gate(nrg_chem* h, double elem_tol, double raw_elem_tol, double dT_tol,
                                    double dT_max);
+/* Longest step (s) whose cells the gate may accept; cells with a longer step
+ * go to the FP64 integrator.  Default 1e-6 s: the gate bounds above were
+ * calibrated on 1e-6 s steps, and on 1e-5 s steps of the wide-range
+ * distribution they let cells through with errors of many kelvin.  No
+ * counterpart in the reference. */
+NRG_API int nrg_surrogate_set_gate_dt(nrg_chem* h, double dt_max);
 /* Inference path of the surrogate step: 1 (default) one fused kernel
  * (features, the five layers on tcgen05 tensor cores with TMEM accumulators,
  * gate); 0 the unfused chain (features, one GEMM per layer, gate kernel). */

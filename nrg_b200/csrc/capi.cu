@@ -1228,6 +1228,12 @@ extern "C" int nrg_surrogate_set_gate(nrg_chem* h, double elem_tol, double raw_e
   return NRG_OK;
 }
 
+extern "C" int nrg_surrogate_set_gate_dt(nrg_chem* h, double dt_max) {
+  if (!h || !(dt_max > 0)) return NRG_ERR_ARG;
+  nrg::surrogate_set_gate_dt(h->sur, dt_max);
+  return NRG_OK;
+}
+
 extern "C" int nrg_surrogate_set_inference(nrg_chem* h, int fused) {
   if (!h) return NRG_ERR_ARG;
   nrg::surrogate_set_fused(h->sur, fused != 0);

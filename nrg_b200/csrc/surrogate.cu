@@ -249,6 +249,7 @@ struct GateCfg {
   double elem_tol;      // element residual of the dY that is written (after projection)
   double raw_elem_tol;  // element residual of the network's own dY
   double dT_tol, dT_max;
+  double dt_max;        // cells with a longer step go to FP64: the bounds above were calibrated up to it
 };
 
 // Element residual max_e |sum_k a_ek (W_e / W_k) dY_k| (element mass fraction)
@@ -318,7 +319,7 @@ __device__ __noinline__ bool gate_active_cell(const StepArgs& a, long c, double 
                                                  const double (&y0)[9], const float (&f)[kMlpIn],
                                                  const float* o, const MlpNorm* nm, const GateCfg& gc,
                                                  const double (*P)[9]) {
-  bool ok = true;
+  bool ok = dt <= gc.dt_max;
 #pragma unroll
   for (int j = 0; j < kMlpIn; ++j) {
     const float span = nm->x_max[j] - nm->x_min[j];
@@ -749,7 +750,7 @@ __global__ void k_standardize(long n, const float* xraw, const float* yraw, cons
 struct Surrogate {
   bool ready = false;
   bool uploaded = false;
-  GateCfg gate{1e-6, 5e-6, 0.2, 5.0};
+  GateCfg gate{1e-6, 5e-6, 0.2, 5.0, 1e-6};
   MlpNorm norm{};
   MlpNorm* d_norm = nullptr;
   // parameters: fp32 master, Adam moments, bf16 working copies, gradients
@@ -868,8 +869,9 @@ bool surrogate_ready(const Surrogate* s) { return s && s->ready && s->uploaded; 
 void surrogate_set_ready(Surrogate* s, bool r) { s->ready = r; }
 void surrogate_set_cell_order(Surrogate* s, bool by_temperature) { s->order_cells = by_temperature; }
 void surrogate_set_gate(Surrogate* s, double elem_tol, double raw_elem_tol, double dT_tol, double dT_max) {
-  s->gate = GateCfg{elem_tol, raw_elem_tol, dT_tol, dT_max};
+  s->gate = GateCfg{elem_tol, raw_elem_tol, dT_tol, dT_max, s->gate.dt_max};
 }
+void surrogate_set_gate_dt(Surrogate* s, double dt_max) { s->gate.dt_max = dt_max; }
 
 static std::string ck(cudaError_t e, const char* what) {
   return e == cudaSuccess ? std::string() : std::string(what) + ": " + cudaGetErrorString(e);

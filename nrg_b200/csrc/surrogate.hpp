@@ -84,5 +84,7 @@ std::string surrogate_infer(Surrogate* s, const StepArgs& a, float* out, cudaStr
 // Reads and clears the fused kernel's error word (after the step's work).
 std::string surrogate_check(Surrogate* s, cudaStream_t st);
 void surrogate_set_gate(Surrogate* s, double elem_tol, double raw_elem_tol, double dT_tol, double dT_max);
+// Longest step (s) whose cells the gate may accept.
+void surrogate_set_gate_dt(Surrogate* s, double dt_max);
 
 }  // namespace nrg

@@ -73,6 +73,11 @@ class Surrogate:
     def set_gate(self, elem_tol=1e-6, raw_elem_tol=5e-6, dT_tol=0.2, dT_max=5.0) -> None:
         _check(lib().nrg_surrogate_set_gate(self.h, elem_tol, raw_elem_tol, dT_tol, dT_max), self.h)
 
+    def set_gate_dt(self, dt_max: float = 1e-6) -> None:
+        """Longest step whose cells the gate may accept (the gate bounds are
+        calibrated on 1e-6 s steps); longer steps go to FP64."""
+        _check(lib().nrg_surrogate_set_gate_dt(self.h, dt_max), self.h)
+
     def set_inference(self, fused: bool = True) -> None:
         """Fused tcgen05 kernel (default) or the unfused GEMM chain + gate."""
         _check(lib().nrg_surrogate_set_inference(self.h, int(fused)), self.h)

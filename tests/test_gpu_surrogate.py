@@ -196,3 +196,33 @@ def test_fallback_order_changes_no_result(decks, W):
     for k in ("cells_active", "cells_surrogate", "cells_fallback", "steps", "solves"):
         assert sb[k] == sa[k], (k, sa, sb)
     assert 0 < sb["cells_fallback"] < sb["cells_active"]
+
+
+def test_gate_sends_longer_steps_to_fp64(decks, W):
+    """The gate bounds were calibrated on 1e-6 s steps.  On 1e-5 s steps of
+    the wide-range distribution every cell goes to the FP64 integrator by
+    default (results bit-equal to the plain step), and a flame sample with
+    1e-6 s steps is answered by the network only while the bound admits
+    1e-6 s."""
+    from nrg_b200.chemistry import ChemicalKineticsSolver
+    from nrg_b200.surrogate import DEFAULT_MODEL, RECIPE, Surrogate
+    wide = fields.slice_field(fields.wide_range_field(W, n_side=256), 16384, stride=3)
+    flame = fields.slice_field(fields.flame_field(W), 8 * 2048, offset=1000 * 2048)
+    s = ChemicalKineticsSolver(None, *decks, mode="fast")
+    try:
+        s.set_launch(kernel="thread", block=32)
+        sur = Surrogate(s)
+        sur.load(DEFAULT_MODEL)
+        sur.set_gate(*RECIPE["gate"])
+        plain, _ = run_device(s, wide, "fast")
+        sg, st = run_device(s, wide, "surrogate")
+        fl, st_fl = run_device(s, flame, "surrogate")
+        sur.set_gate_dt(5e-7)
+        fl2, st_fl2 = run_device(s, flame, "surrogate")
+    finally:
+        s.close()
+    assert st["cells_surrogate"] == 0 and st["cells_fallback"] == wide.n
+    for k in ("Y_prod", "E_f_prod", "T_after"):
+        np.testing.assert_array_equal(sg[k], plain[k])
+    assert st_fl["cells_surrogate"] > 0
+    assert st_fl2["cells_surrogate"] == 0 and np.all(fl2["status"][fl2["status"] != 0] == 1)
