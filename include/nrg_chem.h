@@ -88,8 +88,9 @@ typedef struct {
   double device_ms;          /* device time of the step (CUDA events) */
   /* per-phase device time when phase timing is on (nrg_chem_set_timing):
    * [0] surrogate inference (fused path: features + MLP + gate in one kernel;
-   * unfused: features + MLP), [1] compaction (unfused: gate + compaction),
-   * [2] FP64 integrator, [3] unused */
+   * unfused: features + MLP), [1] the rejected cells' list (temperature
+   * order, or compaction in cell order; unfused: the gate too), [2] FP64
+   * integrator (with the plain step's temperature order), [3] unused */
   double phase_ms[4];
 } nrg_chem_stats;
 
