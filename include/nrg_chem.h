@@ -132,7 +132,11 @@ NRG_API int nrg_chem_step_device(nrg_chem* h, double time_step, long n, long ld,
  * NRG_ERR_ARG.  The first call on each device looks up the array's address
  * (set-up), so make that first call before any stream capture.  All calls on
  * a device share the array: calls that overlap on the GPU (several streams or
- * host threads at once) race on it.  Surrogate mode is not available here. */
+ * host threads at once) race on it.  The array's address is looked up once
+ * per device and kept for the life of the process; a device reset
+ * (cudaDeviceReset) invalidates it, so do not call this entry point again on
+ * a device after resetting it in the same process.  Surrogate mode is not
+ * available here. */
 NRG_API int nrg_chem_step_device_noalloc(nrg_chem* h, double time_step, long n, long ld, const double* T,
                                          const double* rho, const double* Y, const signed char* bc,
                                          double* Y_prod, double* Y_prod2, double* E_f_prod, double* T_after,

@@ -6,7 +6,8 @@ nrg_b200.build     -- in-tree nvcc build of libnrg_chem.so (sm_100a)
 """
 import os
 
-MECH_DIR = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "tests", "golden", "mechanism")
+# the reference's input decks (task_setup/chemical_mechanisms, task_setup/thermophysical_data)
+MECH_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "mechanism")
 
 
 # the reference's H2/air mechanisms (task_setup/chemical_mechanisms)

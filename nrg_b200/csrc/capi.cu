@@ -92,6 +92,29 @@ int cuda_fail(nrg_chem* h, cudaError_t e, const char* where) {
     if (e_ != cudaSuccess) return cuda_fail(h, e_, #call); \
   } while (0)
 
+// Makes the handle's device current for the rest of an entry point and gives
+// the calling thread its own current device back when the entry point
+// returns, so a host code that drives several GPUs from one thread may call
+// any handle at any time.
+struct DeviceScope {
+  int prev = -1;
+  cudaError_t enter(int dev) {
+    cudaError_t e = cudaGetDevice(&prev);
+    if (e != cudaSuccess) {
+      prev = -1;
+      return e;
+    }
+    return prev == dev ? cudaSuccess : cudaSetDevice(dev);
+  }
+  ~DeviceScope() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+#define ON_DEVICE(h)         \
+  DeviceScope device_scope_; \
+  CK(h, device_scope_.enter((h)->device))
+
 // Gear coefficients EL(13,12), TQ(3,12) (ddcst.f90:35-106, MINT = 2).
 void gear_coefficients(double* el, double* tq) {
   const int maxord = nrg::kMaxOrd;
@@ -533,8 +556,10 @@ extern "C" int nrg_chem_create(const char* mechanism_path, const char* thermo_pa
 }
 
 extern "C" int nrg_chem_destroy(nrg_chem* h) {
-  if (h) release_tables(h);
   if (!h) return NRG_ERR_ARG;
+  release_tables(h);
+  DeviceScope device_scope;  // frees on the handle's device whatever device is current
+  device_scope.enter(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
   nrg::surrogate_destroy(h->sur);
@@ -629,7 +654,7 @@ extern "C" int nrg_chem_step_device(nrg_chem* h, double time_step, long n, long 
   if (n > 0 && (!T || !rho || !Y || !Y_prod || !Y_prod2 || !E_f_prod))
     return fail(h, NRG_ERR_ARG, "null field pointer");
   if (n > 0x7fffffffL / 2) return fail(h, NRG_ERR_ARG, "too many cells for one call");
-  CK(h, cudaSetDevice(h->device));
+  ON_DEVICE(h);
   CK(h, use_tables(h));
   StepArgs a;
   a.n = n;
@@ -663,6 +688,7 @@ extern "C" int nrg_chem_step_device(nrg_chem* h, double time_step, long n, long 
 
 extern "C" int nrg_chem_step(nrg_chem* h, double time_step, const nrg_field_desc* f, nrg_chem_stats* stats) {
   if (!h || !f) return NRG_ERR_ARG;
+  ON_DEVICE(h);
   const int N = h->mech.n();
   long ext[3], cnt[3];
   for (int d = 0; d < 3; ++d) {
@@ -790,7 +816,7 @@ extern "C" int nrg_chem_autotune(nrg_chem* h, double time_step, long n, long ld,
   if (!h) return NRG_ERR_ARG;
   if (n <= 0 || ld < n || !T || !rho || !Y || !Y_prod || !Y_prod2 || !E_f_prod)
     return fail(h, NRG_ERR_ARG, "autotune needs device inputs with n > 0");
-  CK(h, cudaSetDevice(h->device));
+  ON_DEVICE(h);
   CK(h, use_tables(h));
   if (int rc = ensure_order(h, n)) return rc;
   StepArgs a;
@@ -867,7 +893,7 @@ extern "C" int nrg_chem_apply_state_device(nrg_chem* h, double time_step, long n
   if (n < 0 || ld < n || dims < 0 || dims > 3 || (dims > 0 && !v) ||
       (n > 0 && (!rho || !Y || !E_f || !T || !p || !gamma)) || ((Y_prod || E_f_prod) && !(time_step > 0.0)))
     return fail(h, NRG_ERR_ARG, "bad arguments to nrg_chem_apply_state_device");
-  CK(h, cudaSetDevice(h->device));
+  ON_DEVICE(h);
   CK(h, use_tables(h));
   CK(h, cudaEventRecord(h->ev_in, (cudaStream_t)stream));
   CK(h, cudaStreamWaitEvent(h->stream, h->ev_in, 0));
@@ -916,7 +942,7 @@ extern "C" int nrg_species_predictor_device(nrg_chem* h, double time_step, const
   for (int p = 0; p < n_particle_phases; ++p) a.Y_prod_part[p] = Y_prod_particles[p];
   a.rho_old = rho_old; a.Y_old = Y_old; a.rho_int = rho_int; a.Y_int = Y_int;
   a.rho_out = rho; a.Y_out = Y;
-  CK(h, cudaSetDevice(h->device));
+  ON_DEVICE(h);
   CK(h, cudaEventRecord(h->ev_in, (cudaStream_t)stream));
   CK(h, cudaStreamWaitEvent(h->stream, h->ev_in, 0));
   const cudaError_t e = nrg::launch_species_predictor(N, a, h->stream);
@@ -982,7 +1008,7 @@ extern "C" int nrg_mixture_diffusivity_device(nrg_chem* h, long n, long ld, cons
     return fail(h, NRG_ERR_ARG, "bad arguments to nrg_mixture_diffusivity_device");
   nrg::DiffusivityArgs a = h->diff;
   a.n = n; a.ld = ld; a.T = T; a.p = p; a.Y = Y; a.m_mix = mix_mol_mass; a.bc = (const int8_t*)bc; a.D = D;
-  CK(h, cudaSetDevice(h->device));
+  ON_DEVICE(h);
   CK(h, cudaEventRecord(h->ev_in, (cudaStream_t)stream));
   CK(h, cudaStreamWaitEvent(h->stream, h->ev_in, 0));
   const cudaError_t e = nrg::launch_mixture_diffusivity(a, h->stream);
@@ -1133,18 +1159,20 @@ extern "C" int nrg_surrogate_norm_count(void) { return kNormFloats; }
 
 extern "C" int nrg_surrogate_init(nrg_chem* h, unsigned long long seed) {
   if (!h) return NRG_ERR_ARG;
-  CK(h, cudaSetDevice(h->device));
+  ON_DEVICE(h);
   CK(h, use_tables(h));
   return sfail(h, nrg::surrogate_init(h->sur, seed, h->stream));
 }
 
 extern "C" int nrg_surrogate_get_params(nrg_chem* h, float* params) {
   if (!h || !params) return NRG_ERR_ARG;
+  ON_DEVICE(h);
   return sfail(h, nrg::surrogate_get_params(h->sur, params, h->stream));
 }
 
 extern "C" int nrg_surrogate_set_params(nrg_chem* h, const float* params) {
   if (!h || !params) return NRG_ERR_ARG;
+  ON_DEVICE(h);
   return sfail(h, nrg::surrogate_set_params(h->sur, params, h->stream));
 }
 
@@ -1156,6 +1184,7 @@ extern "C" int nrg_surrogate_get_norm(nrg_chem* h, float* norm) {
 
 extern "C" int nrg_surrogate_set_norm(nrg_chem* h, const float* norm) {
   if (!h || !norm) return NRG_ERR_ARG;
+  ON_DEVICE(h);
   return sfail(h, nrg::surrogate_set_norm(h->sur, floats_to_norm(norm)));
 }
 
@@ -1167,7 +1196,7 @@ extern "C" int nrg_surrogate_prepare(nrg_chem* h, long n, long ld, double dt, co
     return fail(h, NRG_ERR_ARG, "bad arguments to nrg_surrogate_prepare");
   if (!(opts->hull_margin >= 0.f) || !(opts->log_eps > 0.f) || (opts->log_mask >> 9))
     return fail(h, NRG_ERR_ARG, "bad nrg_surrogate_opts (hull_margin >= 0, log_eps > 0, log_mask < 512)");
-  CK(h, cudaSetDevice(h->device));
+  ON_DEVICE(h);
   CK(h, use_tables(h));
   int rc = order_after_legacy(h);
   if (rc) return rc;
@@ -1180,7 +1209,7 @@ extern "C" int nrg_surrogate_features(nrg_chem* h, long n, long ld, double dt, c
                                       const double* T, const double* rho, const double* Y, float* xraw,
                                       void* x_bf16) {
   if (!h || n < 0 || ld < n || (n > 0 && (!T || !rho || !Y))) return fail(h, NRG_ERR_ARG, "bad features args");
-  CK(h, cudaSetDevice(h->device));
+  ON_DEVICE(h);
   CK(h, use_tables(h));
   int rc = order_after_legacy(h);
   if (rc) return rc;
@@ -1193,7 +1222,7 @@ extern "C" int nrg_surrogate_features(nrg_chem* h, long n, long ld, double dt, c
 
 extern "C" int nrg_surrogate_forward(nrg_chem* h, long n, const void* x_bf16, float* out) {
   if (!h || n <= 0 || !x_bf16 || !out) return fail(h, NRG_ERR_ARG, "bad forward args");
-  CK(h, cudaSetDevice(h->device));
+  ON_DEVICE(h);
   CK(h, use_tables(h));
   int rc = order_after_legacy(h);
   if (rc) return rc;
@@ -1203,7 +1232,7 @@ extern "C" int nrg_surrogate_forward(nrg_chem* h, long n, const void* x_bf16, fl
 extern "C" int nrg_surrogate_grad(nrg_chem* h, long n, const void* x_bf16, const float* y, float* grads_host,
                                   double* loss_host) {
   if (!h || n <= 0 || !x_bf16 || !y) return fail(h, NRG_ERR_ARG, "bad grad args");
-  CK(h, cudaSetDevice(h->device));
+  ON_DEVICE(h);
   CK(h, use_tables(h));
   int rc = order_after_legacy(h);
   if (rc) return rc;
@@ -1213,7 +1242,7 @@ extern "C" int nrg_surrogate_grad(nrg_chem* h, long n, const void* x_bf16, const
 extern "C" int nrg_surrogate_train(nrg_chem* h, long n, const void* x_bf16, const float* y, int epochs, int batch,
                                    float lr, unsigned long long seed, float* loss_per_epoch) {
   if (!h || n <= 0 || !x_bf16 || !y || epochs <= 0 || !(lr > 0.f)) return fail(h, NRG_ERR_ARG, "bad train args");
-  CK(h, cudaSetDevice(h->device));
+  ON_DEVICE(h);
   CK(h, use_tables(h));
   int rc = order_after_legacy(h);
   if (rc) return rc;
@@ -1244,7 +1273,7 @@ extern "C" int nrg_surrogate_infer(nrg_chem* h, long n, long ld, double dt, cons
                                    const double* rho, const double* Y, float* out) {
   if (!h || n < 0 || ld < n || (n > 0 && (!T || !rho || !Y || !out)) || (!(dt > 0.0) && !dt_cells))
     return fail(h, NRG_ERR_ARG, "bad arguments to nrg_surrogate_infer");
-  CK(h, cudaSetDevice(h->device));
+  ON_DEVICE(h);
   CK(h, use_tables(h));
   int rc = order_after_legacy(h);
   if (rc) return rc;
@@ -1310,7 +1339,7 @@ extern "C" int nrg_chem_integrate(nrg_chem* h, long n, long ld, double dt, const
     h->mode = saved;
     return fail(h, NRG_ERR_ARG, "null field pointer");
   }
-  CK(h, cudaSetDevice(h->device));
+  ON_DEVICE(h);
   CK(h, use_tables(h));
   StepArgs a{};
   a.n = n; a.ld = ld; a.dt = dt > 0.0 ? dt : 1.0; a.T = T; a.rho = rho; a.Y = Y; a.bc = (const int8_t*)bc;
@@ -1384,13 +1413,9 @@ unsigned char* noalloc_scratch(int dev, std::string* err) {
 __global__ void k_na_flag(StepArgs a, int n_species, unsigned char* flag) {
   for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < a.n; c += (long)gridDim.x * blockDim.x) {
     const double Tc = a.T[c];
-    const bool active = (Tc >= 305.0) && (a.bc == nullptr || a.bc[c] == 0);
+    const bool active = nrg::reference_cell_active(Tc, a.bc, c);
     flag[c] = active ? 1 : 0;
-    if (!active) {  // skip rule of the reference: zero sources, Y_prod2 untouched
-      for (int k = 0; k < n_species; ++k) a.Y_prod[k * a.ld + c] = 0.0;
-      a.E_f_prod[c] = 0.0;
-      if (a.status) a.status[c] = nrg::kCellSkipped;
-    }
+    if (!active) nrg::write_skipped_cell(a, c, n_species, Tc);
   }
 }
 
@@ -1468,7 +1493,7 @@ extern "C" int nrg_chem_step_device_noalloc(nrg_chem* h, double time_step, long 
     if (stats) std::memset(stats, 0, sizeof(*stats));
     return NRG_OK;
   }
-  CK(h, cudaSetDevice(h->device));
+  ON_DEVICE(h);
   CK(h, use_tables(h));
   std::string err;
   unsigned char* base = noalloc_scratch(h->device, &err);

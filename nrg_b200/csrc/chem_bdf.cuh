@@ -1012,12 +1012,8 @@ template <int N, int R, class CS>
 __device__ bool cell_begin(CS& c, const StepArgs& a, long cid) {
   constexpr int NF = CS::kNF;
   const double Tc = a.T[cid];
-  const bool active = (Tc >= 305.0) && (a.bc == nullptr || a.bc[cid] == 0);
-  if (!active) {
-#pragma unroll
-    for (int k = 0; k < NF; ++k) a.Y_prod[k * a.ld + cid] = 0.0;
-    a.E_f_prod[cid] = 0.0;
-    if (a.status) a.status[cid] = kCellSkipped;
+  if (!reference_cell_active(Tc, a.bc, cid)) {
+    write_skipped_cell(a, cid, NF, Tc);
     return false;
   }
   const double rho = a.rho[cid];

@@ -9,6 +9,8 @@
 
 #include <cstdint>
 
+#include "chem_kernels.hpp"
+
 namespace nrg {
 
 constexpr int kMaxSpecies = 24;
@@ -69,5 +71,25 @@ enum CellStatus : uint8_t {
   kCellNonfinite = 4, // non-finite input or output
   kCellSurrogate = 5  // accepted surrogate prediction (gated path)
 };
+
+// Skip rule of the reference (chemical_kinetics_solver.f90:228-231): a cell
+// colder than 305 K, or one carrying a boundary marker, is not integrated.
+// A NaN temperature counts as cold.
+constexpr double kSkipBelowK = 305.0;
+
+__device__ __forceinline__ bool reference_cell_active(double T, const int8_t* bc, long c) {
+  return (T >= kSkipBelowK) && (bc == nullptr || bc[c] == 0);
+}
+
+// Outputs of a skipped cell (:341-346): zero species and energy sources,
+// Y_prod2 left as the caller had it, the temperature after the step equal to
+// the one before.  Every path of the step (integrators, surrogate, the
+// no-allocation step) writes skipped cells through this one function.
+__device__ __forceinline__ void write_skipped_cell(const StepArgs& a, long c, int n_species, double T) {
+  for (int k = 0; k < n_species; ++k) a.Y_prod[k * a.ld + c] = 0.0;
+  a.E_f_prod[c] = 0.0;
+  if (a.T_after) a.T_after[c] = T;
+  if (a.status) a.status[c] = kCellSkipped;
+}
 
 }  // namespace nrg

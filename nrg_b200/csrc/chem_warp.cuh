@@ -651,13 +651,8 @@ L420:
 template <int N, int R, typename LUT>
 __device__ bool warp_cell_begin(WarpCell<N, R, LUT>& c, const StepArgs& a, long cid) {
   const double Tc = a.T[cid];
-  const bool active = (Tc >= 305.0) && (a.bc == nullptr || a.bc[cid] == 0);
-  if (!active) {
-    if (c.lane < N) a.Y_prod[c.lane * a.ld + cid] = 0.0;
-    if (c.lane == 0) {
-      a.E_f_prod[cid] = 0.0;
-      if (a.status) a.status[cid] = kCellSkipped;
-    }
+  if (!reference_cell_active(Tc, a.bc, cid)) {
+    if (c.lane == 0) write_skipped_cell(a, cid, N, Tc);
     return false;
   }
   const double rho = a.rho[cid];

@@ -5,6 +5,7 @@
 // Small HBM-bound kernels next to the integrator's step.
 #include <climits>
 
+#include "chem_device.cuh"
 #include "order.hpp"
 
 namespace nrg {
@@ -19,8 +20,8 @@ static_assert(kDigits <= kThreads, "one thread per digit in the column scans");
 static_assert(kOrderKeyBits % kOrderDigitBits == 0, "whole digits");
 
 __device__ __forceinline__ uint32_t order_key(double T, int8_t bcv) {
-  if (!(T >= 305.0) || bcv != 0) return 0u;  // skipped by the step (also NaN T)
-  return 1u + (uint32_t)fmin((T - 305.0) * 1024.0, (double)((1u << kOrderKeyBits) - 2u));
+  if (!(T >= kSkipBelowK) || bcv != 0) return 0u;  // skipped by the step (also NaN T)
+  return 1u + (uint32_t)fmin((T - kSkipBelowK) * 1024.0, (double)((1u << kOrderKeyBits) - 2u));
 }
 
 // Items of one pass: the cells themselves (first pass; keys computed from T,

@@ -303,12 +303,8 @@ __device__ void element_projector(double (*P)[9]) {
 // Skip rule of the reference (T < 305 K or a boundary marker): zero sources,
 // T unchanged.  Returns true for a skipped cell.
 __device__ __forceinline__ bool write_if_skipped(const StepArgs& a, long c, double T0) {
-  if ((T0 >= 305.0) && (a.bc == nullptr || a.bc[c] == 0)) return false;
-#pragma unroll
-  for (int k = 0; k < 9; ++k) a.Y_prod[k * a.ld + c] = 0.0;
-  a.E_f_prod[c] = 0.0;
-  if (a.T_after) a.T_after[c] = T0;
-  if (a.status) a.status[c] = kCellSkipped;
+  if (reference_cell_active(T0, a.bc, c)) return false;
+  write_skipped_cell(a, c, 9, T0);
   return true;
 }
 

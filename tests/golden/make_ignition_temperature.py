@@ -15,7 +15,7 @@ sys.path.insert(0, ROOT)
 from oracle import oracle_py as op  # noqa: E402
 from nrg_b200 import fields  # noqa: E402
 
-D = os.path.join(ROOT, "tests", "golden", "mechanism")
+D = os.path.join(ROOT, "nrg_b200", "data", "mechanism")
 
 
 def peak_oh_time(m, W, T, t_end=4e-5, n_out=400):

@@ -13,13 +13,33 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
+# Runs the reference arm in this interpreter, then prints which shared
+# objects of the repository the process mapped.
+_RUN_AND_LIST_MAPS = """
+import runpy, sys
+sys.argv = sys.argv[1:]
+try:
+    runpy.run_path("bench.py", run_name="__main__")
+except SystemExit as e:
+    assert not e.code, e.code
+with open("/proc/self/maps") as fh:
+    libs = sorted({l.split()[-1] for l in fh if l.rstrip().endswith(".so")})
+print("MAPPED " + " ".join(x for x in libs if "nrg" in x.rsplit("/", 1)[-1] or "oracle" in x.rsplit("/", 1)[-1]))
+"""
+
+
 @pytest.mark.parametrize("field", ["flame", "ignition"])
 def test_reference_arm_json_line(field):
-    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--field", field,
-                        "--steps", "1", "--warmup", "0", "--cpu-seconds", "0.2"],
+    r = subprocess.run([sys.executable, "-c", _RUN_AND_LIST_MAPS, "bench.py", "--impl", "reference",
+                        "--field", field, "--steps", "1", "--warmup", "0", "--cpu-seconds", "0.2"],
                        capture_output=True, text=True, timeout=600, cwd=ROOT)
     assert r.returncode == 0, r.stderr[-2000:]
-    line = json.loads(r.stdout.strip().splitlines()[-1])
+    out = r.stdout.strip().splitlines()
+    mapped = out[-1].split()[1:]
+    # the reference arm runs the oracle only: no library of the product is mapped
+    assert any(m.endswith("oracle/liboracle.so") for m in mapped), mapped
+    assert not any("libnrg_chem" in m for m in mapped), mapped
+    line = json.loads(out[-2])
     assert line["impl"] == "reference" and line["value"] > 0 and line["unit"] == "cell-updates/s"
     assert line["higher_is_better"] is True and line["steps"] == 1 and line["warmup"] == 0
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1

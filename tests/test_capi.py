@@ -38,3 +38,21 @@ def test_create_error_is_reported_without_gpu(decks, tmp_path):
     assert rc == -2 and b"cannot open" in L.nrg_chem_last_error(None)
     with pytest.raises(chemistry.NrgError):
         chemistry.ChemicalKineticsSolver(None, str(tmp_path / "missing.txt"), *decks[1:])
+
+
+def build_c_driver(out_dir) -> str:
+    """Compiles tests/c_abi_driver.c against include/nrg_chem.h and links it
+    with libnrg_chem.so, as a C (or Fortran bind(C)) host code would."""
+    import subprocess
+    exe = os.path.join(str(out_dir), "c_abi_driver")
+    libdir = os.path.dirname(chemistry.LIB_PATH)
+    r = subprocess.run(["gcc", "-std=c11", "-O2", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                        os.path.join(ROOT, "tests", "c_abi_driver.c"), "-L", libdir, "-lnrg_chem",
+                        "-Wl,-rpath," + libdir, "-o", exe], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    return exe
+
+
+def test_c_driver_compiles_and_links_against_the_header(tmp_path):
+    chemistry.lib()  # builds the library if needed
+    assert os.path.exists(build_c_driver(tmp_path))

@@ -46,3 +46,31 @@ def test_two_gloo_ranks_step_disjoint_rows(tmp_path, oracle_mech, W):
     ref = oracle_mech.chem_step(f.dt, f.T, f.rho, f.Y, threads=1)["Y_prod"]
     np.testing.assert_array_equal(got, ref)
     assert float((tmp_path / "max.txt").read_text()) == 2.0
+
+
+@pytest.mark.gpu
+def test_two_ranks_step_row_blocks_through_the_product(tmp_path, W):
+    """Two processes (gloo for the plumbing) step their row blocks of one
+    field through nrg_chem_step_device on the one GPU: the blocks put
+    together equal a single-process step of the whole field bit for bit."""
+    import torch
+    from nrg_b200 import keromnes_paths
+    from nrg_b200.chemistry import ChemicalKineticsSolver
+    cmd = ["timeout", "-k", "30", "600", sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           "--nproc-per-node=2", "--master-addr=127.0.0.1", f"--master-port={_free_port()}",
+           os.path.join(ROOT, "tests", "dist_worker.py"), str(tmp_path), "product"]
+    r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=700)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    got = np.concatenate([np.load(tmp_path / f"rank{k}.npy") for k in range(2)], axis=1)
+    f = fields.random_field(W)
+    dev = torch.device("cuda:0")
+    T, rho, Y = (torch.tensor(a, device=dev) for a in (f.T, f.rho, f.Y))
+    Yp, Yp2, Ef = torch.zeros_like(Y), torch.zeros_like(Y), torch.zeros_like(T)
+    s = ChemicalKineticsSolver(None, *keromnes_paths(), mode="fast")
+    try:
+        s.step_device(f.dt, T, rho, Y, Yp, Yp2, Ef)
+        torch.cuda.synchronize()
+    finally:
+        s.close()
+    np.testing.assert_array_equal(got, Yp.cpu().numpy())
+    assert float((tmp_path / "max.txt").read_text()) == 2.0

@@ -183,6 +183,39 @@ def test_host_layout_drop_in(decks, oracle_mech, W):
     s.close()
 
 
+def test_host_step_runs_on_the_handles_device_and_keeps_the_callers(decks, oracle_mech, W):
+    """A handle created on device 0 steps host arrays while another device is
+    current: the work runs on device 0 and the caller's current device is
+    still current afterwards."""
+    import torch
+    if torch.cuda.device_count() < 2:
+        pytest.skip("needs two visible GPUs")
+    from nrg_b200.chemistry import DataManager, chemical_kinetics_solver_c
+    f = fields.slice_field(fields.random_field(W), 1024)
+    nx, ny = 32, 32
+    m = DataManager.block(nx, ny)
+    T = m.create_scalar_field("temperature")
+    m.create_scalar_field("pressure")
+    rho = m.create_scalar_field("density")
+    Y = m.create_vector_field("specie_mass_fraction", 9)
+    m.interior(T)[...] = f.T.reshape(ny, nx).T[:, :, None]
+    m.interior(rho)[...] = f.rho.reshape(ny, nx).T[:, :, None]
+    for k in range(9):
+        m.interior(Y[k])[...] = f.Y[k].reshape(ny, nx).T[:, :, None]
+    torch.cuda.set_device(0)
+    s = chemical_kinetics_solver_c(m, *decks, mode="fast")
+    try:
+        torch.cuda.set_device(1)
+        s.solve_chemical_kinetics(f.dt)
+        assert torch.cuda.current_device() == 1
+    finally:
+        s.close()
+        torch.cuda.set_device(0)
+    o = oracle_mech.chem_step(f.dt, f.T, f.rho, f.Y)
+    yp = np.stack([m.interior(a)[:, :, 0].T.reshape(-1) for a in m.fields["specie_production_chemistry"]])
+    np.testing.assert_allclose(yp * f.dt / f.rho, o["Y_prod"] * f.dt / f.rho, rtol=0, atol=TOL_Y)
+
+
 def test_mixed_precision_wide_range_error_per_species(solver, oracle_mech, W):
     """Config 2 (T ~ U[800, 2600] K, p ~ U[0.5, 5] atm, dt = 1e-5 s): the FP32
     LU with FP64 residual and one refinement sweep against the FP64 oracle,
