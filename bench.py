@@ -41,7 +41,7 @@ def parse():
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--mode", default="auto", choices=["auto", "surrogate", "fast", "reference", "mixed"])
+    p.add_argument("--mode", default="auto", choices=["auto", "surrogate", "fast", "reference", "mixed", "table"])
     p.add_argument("--field", default="flame", choices=["flame", "wide-range", "ignition"],
                    help="flame: 2048^2 flame field, dt=1e-6 s (the headline workload); wide-range: 1024^2 cells, "
                         "T~U[800,2600] K, p~U[0.5,5] atm, dt=1e-5 s; ignition: 512^2 cells, dt=1e-5 s, 20%% of "
@@ -66,6 +66,9 @@ def parse():
     p.add_argument("--no-state-eq", dest="state_eq", action="store_false",
                    help="skip timing the sources + state-equation update of the field "
                         "(nrg_chem_apply_state_device)")
+    p.add_argument("--no-table", dest="table", action="store_false",
+                   help="skip timing the table_approximated mode on the field (a table of the flame's first "
+                        "row, made by the plain integrator)")
     a = p.parse_args()
     if a.n_side is None:
         a.n_side = {"flame": 2048, "wide-range": 1024, "ignition": 512}[a.field]
@@ -454,6 +457,78 @@ def time_diffusivity(solver, tables, args, dev, field, T, Y) -> dict:
                     "of every species, every cell of the field"}
 
 
+def table_bytes(n: int, active: int, N: int) -> int:
+    """Algorithmic HBM bytes of one table-mode step without T_after or bc:
+    every cell reads T and writes Y_prod, E_f_prod and its status byte;
+    an active cell also reads Y and writes Y_prod2."""
+    return n * (8 + 8 * N + 8 + 1) + active * (8 * N + 8 * N)
+
+
+def make_flame_table(solver, W, path, n_side: int = 2048) -> None:
+    """The table of the reference's table_approximated mode, made as the
+    reference makes one: the first row of the flame field (a 1-D flame,
+    300 K to 2400 K) stepped by the plain FP64 integrator, its T and Y_prod2
+    written with the table writer (nrg_table_write)."""
+    import torch
+    from nrg_b200 import fields as F
+    from nrg_b200.chemistry import DataManager, write_table
+    row = F.slice_field(F.flame_field(W, n_side=n_side), n_side)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    T, rho, Y = (torch.tensor(a, device=dev) for a in (row.T, row.rho, row.Y))
+    Yp, Yp2, Ef = torch.zeros_like(Y), torch.zeros_like(Y), torch.zeros_like(T)
+    solver.set_mode("fast")
+    solver.step_device(row.dt, T, rho, Y, Yp, Yp2, Ef)
+    torch.cuda.synchronize()
+    m = DataManager((0, 1, 1), (n_side + 1, 1, 1), (1, 1, 1), (n_side, 1, 1))
+    Tf = m.create_scalar_field("temperature")
+    y2 = m.create_vector_field("specie_production_chemistry2", Y.shape[0])
+    m.interior(Tf)[:, 0, 0] = row.T
+    Yp2h = Yp2.cpu().numpy()
+    for k in range(Y.shape[0]):
+        m.interior(y2[k])[:, 0, 0] = Yp2h[k]
+    write_table(path, solver.species_names, m)
+
+
+def time_table(solver, W, args, dev, field, T, rho, Y, peaks, table_path, decks, units) -> dict:
+    """The table_approximated mode over the whole field (nrg_chem_step_device,
+    no T_after): device time, algorithmic HBM rate, and its sources against
+    the oracle's table step on a sample of the field (bit for bit)."""
+    import torch
+    if not os.path.exists(table_path):
+        make_flame_table(solver, W, table_path)
+    solver.read_chemical_kinetics_table(table_path)
+    solver.set_mode("table")
+    n, N = field.n, Y.shape[0]
+    Yp, Yp2, Ef = torch.zeros_like(Y), torch.zeros_like(Y), torch.zeros_like(T)
+    st = torch.zeros(n, dtype=torch.uint8, device=dev)
+    for _ in range(args.warmup):
+        solver.step_device(field.dt, T, rho, Y, Yp, Yp2, Ef, status=st)
+    torch.cuda.synchronize()
+    times, stats = [], None
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        stats = solver.step_device(field.dt, T, rho, Y, Yp, Yp2, Ef, status=st)
+        times.append(stats["device_ms"])
+    ms = statistics.median(times)
+    active = int(stats["cells_active"])
+    nbytes = table_bytes(n, active, N)
+    gbs = nbytes / (ms * 1e-3) * 1e-9
+    from oracle import oracle_py as op
+    idx = oracle_sample_index(field)
+    samp = F_slice(field, idx)
+    om = op.Mechanism(*decks, 1.0, units)
+    T_t, Y_t = op.table_read(table_path, N)
+    o = om.table_step(T_t, Y_t, samp.dt, samp.T, samp.Y)
+    same = bool(np.array_equal(Yp[:, idx].cpu().numpy(), o["Y_prod"]) and
+                np.array_equal(Ef[idx].cpu().numpy(), o["E_f_prod"]))
+    solver.set_mode("fast")
+    return {"ms": ms, "cells_per_s": n / (ms * 1e-3), "table_rows": int(T_t.size), "active_cells": active,
+            "bytes_per_launch": nbytes, "algorithmic_GB_s": gbs, "frac_of_measured_hbm": gbs / peaks["hbm_gbs"],
+            "sources_equal_oracle_on_sample": same, "sample_cells": int(idx.size),
+            "what": "NRG_MODE_TABLE (ODE_solver = 'table_approximated'): Y_prod2 interpolated in T from a table of "
+                    "the flame's first row (k_table_step; reads T and Y, writes Y_prod, Y_prod2, E_f_prod, status)"}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -563,6 +638,11 @@ def main():
         solver.set_timing(False)
         return el, stats, ph, clk.summary(), (Yp, Yp2, Ef, Ta, st)
 
+    import tempfile
+    table_path = os.path.join(tempfile.mkdtemp(prefix="nrg_table_"), "flame_table(T).dat")
+    if mode == "table":
+        make_flame_table(solver, W, table_path)
+        solver.read_chemical_kinetics_table(table_path)
     el_plain, st_plain, ph_plain, clk_plain, out_plain = time_arm("fast")
     if mode == "surrogate":
         el, stats, ph, clocks, out = time_arm("surrogate")
@@ -625,6 +705,10 @@ def main():
     if args.predictor:
         predictor = time_predictor(solver, tables, args, dev, load_peaks())
 
+    table_leg = None
+    if args.table and args.mechanism == "KEROMNES":
+        table_leg = time_table(solver, W, args, dev, field, T, rho, Y, load_peaks(), table_path, decks, units)
+
     diffusivity = None
     if args.diffusivity:
         diffusivity = time_diffusivity(solver, tables, args, dev, field, T, Y)
@@ -647,6 +731,8 @@ def main():
             hs = Surrogate(host)
             hs.load(DEFAULT_MODEL)
             hs.set_gate(*RECIPE["gate"])
+        if mode == "table":
+            host.read_chemical_kinetics_table(table_path)
         host.set_mode(mode)
         host.solve_chemical_kinetics(field.dt)
         dist.barrier()
@@ -706,7 +792,8 @@ def main():
                        "path": {"fast": "plain FP64 integrator, analytic Jacobian",
                                 "reference": "plain FP64 integrator, reference FD Jacobian",
                                 "mixed": "FP32 LU + FP64 residual/refinement",
-                                "surrogate": "BF16 MLP surrogate + gated FP64 fallback"}[mode],
+                                "surrogate": "BF16 MLP surrogate + gated FP64 fallback",
+                                "table": "table_approximated: Y_prod2 interpolated in T"}[mode],
                        "launch": launch, "cell_order": args.cell_order, "l2": l2_note,
                        "active_cells": int(ph["cells_active"])},
             # long per-kernel blocks first; the headline figures close the line
@@ -717,6 +804,7 @@ def main():
             "state_equation": state_eq,
             "species_predictor": predictor,
             "mixture_diffusivity": diffusivity,
+            "table_mode": table_leg,
             "peaks_file": {k: peaks.get(k) for k in ("hbm_gbs", "bf16_tflops", "bf16_tflops_sustained")},
             "accuracy_vs_oracle": acc_oracle,
             "roofline": roof,

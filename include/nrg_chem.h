@@ -44,7 +44,9 @@ enum nrg_mode {
   NRG_MODE_REFERENCE = 0, /* FP64, finite-difference Jacobian exactly as the reference (DDPST MITER=2) */
   NRG_MODE_FAST = 1,      /* FP64, analytic Jacobian */
   NRG_MODE_MIXED = 2,     /* analytic Jacobian, FP32 LU + FP64 residual and refinement */
-  NRG_MODE_SURROGATE = 3  /* gated BF16 MLP surrogate with FP64 fallback (needs a trained model) */
+  NRG_MODE_SURROGATE = 3, /* gated BF16 MLP surrogate with FP64 fallback (needs a trained model) */
+  NRG_MODE_TABLE = 4      /* ODE_solver = 'table_approximated': Y_prod2 interpolated in T from a table
+                             (needs nrg_chem_load_table or nrg_chem_set_table) */
 };
 
 /* Per-cell status byte (nrg_chem_step_device status output). */
@@ -135,12 +137,44 @@ NRG_API int nrg_chem_step_device(nrg_chem* h, double time_step, long n, long ld,
  * host threads at once) race on it.  The array's address is looked up once
  * per device and kept for the life of the process; a device reset
  * (cudaDeviceReset) invalidates it, so do not call this entry point again on
- * a device after resetting it in the same process.  Surrogate mode is not
- * available here. */
+ * a device after resetting it in the same process.  The surrogate and table
+ * modes are not available here. */
 NRG_API int nrg_chem_step_device_noalloc(nrg_chem* h, double time_step, long n, long ld, const double* T,
                                          const double* rho, const double* Y, const signed char* bc,
                                          double* Y_prod, double* Y_prod2, double* E_f_prod, double* T_after,
                                          unsigned char* status, void* stream, nrg_chem_stats* stats);
+
+/* The table_approximated mode (ODE_solver = 'table_approximated',
+ * chemical_kinetics_solver.f90:91,168-170).  A table holds, per row, a
+ * temperature and the N per-step concentration changes Y_prod2 of a
+ * tabulated 1-D flame.  In NRG_MODE_TABLE every active cell takes its values
+ * from the table by linear interpolation in T (the last row interval
+ * holding T; 0 below the first row, the last row above it;
+ * interpolate_chemical_kinetics, :651-685), and the step writes
+ * Y_prod = value * W / dt, Y_prod2 = value - Y and
+ * E_f_prod = -sum h_k(T_ref) * value / dt (:256-262, :314-315, :318-340).
+ * Table arrays: T_t[i], Y_t[k * stride + i] (stride = rows, or capacity in
+ * nrg_table_read). */
+
+/* Replaces read_chemical_kinetics_table (:608-650): reads a table file of
+ * n_species species -- one header record, then one record per row in the
+ * Fortran edit format (n_species+1)E14.7.  Host only (no GPU, no handle).
+ * With T_t == NULL only *rows is set; otherwise capacity >= *rows. */
+NRG_API int nrg_table_read(const char* path, int n_species, long capacity, double* T_t, double* Y_t, long* rows);
+
+/* Replaces write_chemical_kinetics_table (:542-607): writes the table of
+ * the row j = 1, k = 1 of the host arrays f->T and f->Y_prod2 (reference
+ * layout), from the first interior cell between 300.5 and 310 K to the first
+ * cell of the largest temperature.  Host only. */
+NRG_API int nrg_table_write(const char* path, int n_species, const char* const* species_names,
+                            const nrg_field_desc* f);
+
+/* The handle's table for NRG_MODE_TABLE (copied to the device). */
+NRG_API int nrg_chem_set_table(nrg_chem* h, long rows, const double* T_t, const double* Y_t);
+
+/* nrg_table_read + nrg_chem_set_table: the constructor's
+ * read_chemical_kinetics_table call (:168-170). */
+NRG_API int nrg_chem_load_table(nrg_chem* h, const char* path);
 
 /* The chemistry sources applied to the flow state and the state equation,
  * on device arrays (same layout as nrg_chem_step_device), for cells with

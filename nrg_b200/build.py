@@ -29,6 +29,7 @@ SOURCES = {
     "order.cu": [],
     "transport.cu": ["--fmad=false"],  # species predictor in the reference's operation order
     "diffusion.cu": ["--fmad=false"],
+    "table.cu": ["--fmad=false"],  # table mode: the reference's interpolation and source expressions
     "mechanism.cpp": [],
 }
 

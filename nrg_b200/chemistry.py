@@ -25,7 +25,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libnrg_chem.so")
 NRG_MAX_SPECIES = 24
 
-MODES = {"reference": 0, "fast": 1, "mixed": 2, "surrogate": 3}
+MODES = {"reference": 0, "fast": 1, "mixed": 2, "surrogate": 3, "table": 4}
 EACT_UNITS = {"J.mol": 0, "kJ.mol": 1, "cal.mol": 2, "kcal.mol": 3}
 CELL_STATUS = {0: "skipped", 1: "ok", 2: "mxstep", 3: "fatal", 4: "nonfinite", 5: "surrogate"}
 
@@ -116,6 +116,10 @@ SIGNATURES = {
     "nrg_chem_integrate": (_I, [_VP, _L, _L, _D, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP,
                                 ctypes.POINTER(Stats)]),
     "nrg_fp64_peak_tflops": (_I, [ctypes.POINTER(_D)]),
+    "nrg_table_read": (_I, [_CP, _I, _L, _VP, _VP, ctypes.POINTER(_L)]),
+    "nrg_table_write": (_I, [_CP, _I, _VP, ctypes.POINTER(FieldDesc)]),
+    "nrg_chem_set_table": (_I, [_VP, _L, _VP, _VP]),
+    "nrg_chem_load_table": (_I, [_VP, _CP]),
     "nrg_selftest_bounded_wait": (_I, [ctypes.c_longlong, ctypes.POINTER(_I), ctypes.POINTER(_D)]),
     "nrg_chem_load_transport": (_I, [_VP, _CP]),
     "nrg_mech_transport_tables": (_I, [_CP] * 4 + [_VP] * 3),
@@ -354,36 +358,29 @@ class ChemicalKineticsSolver:
         m = self.manager
         if m is None:
             raise NrgError("no data manager attached")
-        N = self.species_number
-        d = FieldDesc()
-        for i in range(3):
-            d.lb[i], d.ub[i], d.lo[i], d.hi[i] = m.lb[i], m.ub[i], m.lo[i], m.hi[i]
-        keep = []
-
-        def fptr(a):
-            if not (a.flags.f_contiguous and a.dtype == np.float64):
-                raise NrgError("fields must be float64 Fortran-ordered arrays")
-            keep.append(a)
-            return a.ctypes.data
-
-        f = m.fields
-        d.T = fptr(f["temperature"])
-        d.rho = fptr(f["density"])
-        d.p = fptr(f["pressure"]) if "pressure" in f else None
-        for k in range(N):
-            d.Y[k] = fptr(f["specie_mass_fraction"][k])
-            d.Y_prod[k] = fptr(f["specie_production_chemistry"][k])
-            d.Y_prod2[k] = fptr(f["specie_production_chemistry2"][k])
-        d.E_f_prod = fptr(f["energy_production_chemistry"])
-        if "bc_markers" in f:
-            bc = f["bc_markers"]
-            if bc.dtype != np.int8 or not bc.flags.f_contiguous:
-                raise NrgError("bc_markers must be int8 Fortran-ordered")
-            keep.append(bc)
-            d.bc_markers = bc.ctypes.data
+        d, keep = field_desc(m, self.species_number)
         st = Stats()
         _check(lib().nrg_chem_step(self._h, float(time_step), ctypes.byref(d), ctypes.byref(st)), self._h)
+        del keep
         return st.as_dict()
+
+    # -- table_approximated mode --------------------------------------------
+    def set_table(self, T_t, Y_t) -> None:
+        """Table of the table mode: T_t (rows,), Y_t (N, rows)."""
+        T_t = np.ascontiguousarray(T_t, dtype=np.float64)
+        Y_t = np.ascontiguousarray(Y_t, dtype=np.float64).reshape(self.species_number, T_t.shape[0])
+        _check(lib().nrg_chem_set_table(self._h, T_t.shape[0], _ptr(T_t), _ptr(Y_t)), self._h)
+
+    def read_chemical_kinetics_table(self, table_file) -> None:
+        """read_chemical_kinetics_table (chemical_kinetics_solver.f90:608-650)."""
+        _check(lib().nrg_chem_load_table(self._h, str(table_file).encode()), self._h)
+
+    def write_chemical_kinetics_table(self, table_file) -> None:
+        """write_chemical_kinetics_table (chemical_kinetics_solver.f90:542-607)
+        from the attached data manager's temperature and Y_prod2 fields."""
+        if self.manager is None:
+            raise NrgError("no data manager attached")
+        write_table(table_file, self.species_names, self.manager)
 
     # -- device-resident step (torch CUDA tensors) ---------------------------
     def step_device(self, time_step, T, rho, Y, Y_prod, Y_prod2, E_f_prod, bc=None, T_after=None,
@@ -439,9 +436,82 @@ class ChemicalKineticsSolver:
         return ms.value
 
 
-def chemical_kinetics_solver_c(manager: DataManager, mechanism, thermo, molar_masses, **kw) -> ChemicalKineticsSolver:
-    """Constructor with the reference's name (chemical_kinetics_solver.f90:105-107)."""
+def chemical_kinetics_solver_c(manager: DataManager, mechanism, thermo, molar_masses, ODE_solver: str = "slatec",
+                               table_file=None, **kw) -> ChemicalKineticsSolver:
+    """Constructor with the reference's name (chemical_kinetics_solver.f90:105-107,
+    111-173).  ODE_solver 'table_approximated' reads table_file and steps in
+    table mode (:168-170); 'slatec' (the reference's default) integrates."""
+    if ODE_solver not in ("slatec", "table_approximated"):
+        raise NrgError(f"unknown ODE_solver {ODE_solver!r}")
+    if ODE_solver == "table_approximated":
+        if table_file is None:
+            raise NrgError("table_approximated needs a table_file")
+        s = ChemicalKineticsSolver(manager, mechanism, thermo, molar_masses, **dict(kw, mode="fast"))
+        try:
+            s.read_chemical_kinetics_table(table_file)
+            s.set_mode("table")
+        except Exception:
+            s.close()
+            raise
+        return s
     return ChemicalKineticsSolver(manager, mechanism, thermo, molar_masses, **kw)
+
+
+def field_desc(m: DataManager, N: int):
+    """nrg_field_desc of a data manager's fields (and the arrays it points
+    into, which the caller keeps alive while the descriptor is used)."""
+    d = FieldDesc()
+    for i in range(3):
+        d.lb[i], d.ub[i], d.lo[i], d.hi[i] = m.lb[i], m.ub[i], m.lo[i], m.hi[i]
+    keep = []
+
+    def fptr(a):
+        if not (a.flags.f_contiguous and a.dtype == np.float64):
+            raise NrgError("fields must be float64 Fortran-ordered arrays")
+        keep.append(a)
+        return a.ctypes.data
+
+    f = m.fields
+    d.T = fptr(f["temperature"])
+    if "density" in f:
+        d.rho = fptr(f["density"])
+    d.p = fptr(f["pressure"]) if "pressure" in f else None
+    for k in range(N):
+        if "specie_mass_fraction" in f:
+            d.Y[k] = fptr(f["specie_mass_fraction"][k])
+        if "specie_production_chemistry" in f:
+            d.Y_prod[k] = fptr(f["specie_production_chemistry"][k])
+        d.Y_prod2[k] = fptr(f["specie_production_chemistry2"][k])
+    if "energy_production_chemistry" in f:
+        d.E_f_prod = fptr(f["energy_production_chemistry"])
+    if "bc_markers" in f:
+        bc = f["bc_markers"]
+        if bc.dtype != np.int8 or not bc.flags.f_contiguous:
+            raise NrgError("bc_markers must be int8 Fortran-ordered")
+        keep.append(bc)
+        d.bc_markers = bc.ctypes.data
+    return d, keep
+
+
+def table_read(path, n_species: int):
+    """A chemistry table file as the library reads it (host only, no GPU):
+    (T_t (rows,), Y_t (N, rows))."""
+    rows = ctypes.c_long()
+    _check(lib().nrg_table_read(str(path).encode(), n_species, 0, None, None, ctypes.byref(rows)))
+    M = rows.value
+    T_t, Y_t = np.zeros(M), np.zeros((n_species, M))
+    _check(lib().nrg_table_read(str(path).encode(), n_species, M, _ptr(T_t), _ptr(Y_t), ctypes.byref(rows)))
+    return T_t, Y_t
+
+
+def write_table(path, species_names, m: DataManager) -> None:
+    """write_chemical_kinetics_table on a data manager's 'temperature' and
+    'specie_production_chemistry2' fields (host only, no GPU)."""
+    N = len(species_names)
+    d, keep = field_desc(m, N)
+    names = (ctypes.c_char_p * N)(*[n.encode() for n in species_names])
+    _check(lib().nrg_table_write(str(path).encode(), N, ctypes.cast(names, ctypes.c_void_p), ctypes.byref(d)))
+    del keep
 
 
 def fp64_peak_tflops() -> float:

@@ -21,6 +21,7 @@
 #include "transport.hpp"
 #include "diffusion.hpp"
 #include "order.hpp"
+#include "table.hpp"
 
 using nrg::DevMech;
 using nrg::LaunchCfg;
@@ -69,6 +70,10 @@ struct nrg_chem {
   int *d_order_list = nullptr, *d_order_count = nullptr;
   // graph cache
   cudaGraphExec_t gexec = nullptr;
+  // table of the table_approximated mode (nrg_chem_set_table / nrg_chem_load_table)
+  double *d_tab_T = nullptr, *d_tab_Y = nullptr;
+  long tab_rows = 0;
+  bool tab_sorted = false;
   // surrogate state (owned by surrogate.cu)
   nrg::Surrogate* sur = nullptr;
   std::string err;
@@ -340,6 +345,13 @@ cudaError_t enqueue_integrator(nrg_chem* h, const StepArgs& a, const LaunchCfg& 
 // The step's kernels on stream s, adding to the device counters; ph: the
 // phase events (or nullptr).
 cudaError_t enqueue_step_body(nrg_chem* h, const StepArgs& a, cudaStream_t s, cudaEvent_t* ph) {
+  if (h->mode == NRG_MODE_TABLE) {
+    const nrg::TableArgs t{h->tab_rows, h->d_tab_T, h->d_tab_Y, h->tab_sorted ? 1 : 0};
+    if (ph) cudaEventRecord(ph[2], s);
+    cudaError_t e = nrg::launch_table_step(h->mech.n(), a, t, h->d_counters, s);
+    if (ph) cudaEventRecord(ph[3], s);
+    return e;
+  }
   if (h->mode == NRG_MODE_SURROGATE)
     return nrg::surrogate_step(h->sur, a, h->cfg, h->d_queue, h->d_counters, s,
                                [h, ph](const StepArgs& fa, cudaStream_t fs) {
@@ -409,6 +421,8 @@ int ensure_order(nrg_chem* h, long n) {
 
 int step_prepare(nrg_chem* h, long n) {
   CK(h, use_tables(h));
+  if (h->mode == NRG_MODE_TABLE && h->tab_rows < 1)
+    return fail(h, NRG_ERR_STATE, "table mode selected but no table is loaded (nrg_chem_load_table)");
   int rc = ensure_order(h, n);
   if (rc) return rc;
   if (h->mode == NRG_MODE_SURROGATE) {
@@ -563,6 +577,8 @@ extern "C" int nrg_chem_destroy(nrg_chem* h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
   nrg::surrogate_destroy(h->sur);
+  cudaFree(h->d_tab_T);
+  cudaFree(h->d_tab_Y);
   free_staging(h);
   cudaFree(h->d_queue);
   cudaFree(h->d_mech);
@@ -588,7 +604,7 @@ extern "C" int nrg_chem_destroy(nrg_chem* h) {
 
 extern "C" int nrg_chem_set_mode(nrg_chem* h, int mode) {
   if (!h) return NRG_ERR_ARG;
-  if (mode < NRG_MODE_REFERENCE || mode > NRG_MODE_SURROGATE) return fail(h, NRG_ERR_ARG, "unknown mode");
+  if (mode < NRG_MODE_REFERENCE || mode > NRG_MODE_TABLE) return fail(h, NRG_ERR_ARG, "unknown mode");
   h->mode = mode;
   return NRG_OK;
 }
@@ -1117,6 +1133,85 @@ extern "C" int nrg_fp64_peak_tflops(double* tflops) {
   return NRG_OK;
 }
 
+// ---------------------------------------------------------------- table
+extern "C" int nrg_table_read(const char* path, int n_species, long capacity, double* T_t, double* Y_t,
+                              long* rows) {
+  if (!path || !rows || n_species < 1 || n_species > NRG_MAX_SPECIES || (T_t && (!Y_t || capacity < 1)))
+    return fail(nullptr, NRG_ERR_ARG, "bad arguments to nrg_table_read");
+  nrg::ChemTable t;
+  const std::string e = nrg::read_chem_table(path, n_species, &t);
+  if (!e.empty()) return fail(nullptr, NRG_ERR_IO, e);
+  *rows = t.rows;
+  if (!T_t) return NRG_OK;
+  if (capacity < t.rows) return fail(nullptr, NRG_ERR_ARG, "nrg_table_read: capacity below the table's rows");
+  std::copy(t.T.begin(), t.T.end(), T_t);
+  for (int k = 0; k < n_species; ++k)
+    std::copy(t.Y.begin() + (size_t)k * t.rows, t.Y.begin() + (size_t)(k + 1) * t.rows, Y_t + (size_t)k * capacity);
+  return NRG_OK;
+}
+
+extern "C" int nrg_table_write(const char* path, int n_species, const char* const* species_names,
+                               const nrg_field_desc* f) {
+  if (!path || !species_names || !f || !f->T || n_species < 1 || n_species > NRG_MAX_SPECIES)
+    return fail(nullptr, NRG_ERR_ARG, "bad arguments to nrg_table_write");
+  for (int k = 0; k < n_species; ++k)
+    if (!f->Y_prod2[k] || !species_names[k]) return fail(nullptr, NRG_ERR_ARG, "null Y_prod2 array or species name");
+  for (int d = 1; d < 3; ++d)
+    if (f->lb[d] > 1 || f->ub[d] < 1)
+      return fail(nullptr, NRG_ERR_ARG, "the table is written from the row j = 1, k = 1, which the arrays must hold");
+  if (f->lo[0] < f->lb[0] || f->hi[0] > f->ub[0]) return fail(nullptr, NRG_ERR_ARG, "interior outside the arrays");
+  const long e0 = (long)f->ub[0] - f->lb[0] + 1, e1 = (long)f->ub[1] - f->lb[1] + 1;
+  const long row = ((long)(1 - f->lb[2]) * e1 + (1 - f->lb[1])) * e0;  // cells(lb0, 1, 1)
+  auto at = [&](int i) { return row + (i - f->lb[0]); };
+  // write_chemical_kinetics_table (chemical_kinetics_solver.f90:574-582):
+  // first interior cell between 300.5 and 310 K, first cell of the largest T
+  double max_T = 0.0;
+  int first = 0, last = 0;
+  for (int i = f->lo[0]; i <= f->hi[0]; ++i) {
+    const double t = f->T[at(i)];
+    if (t > 300.5 && t < 310.0 && first == 0) first = i;
+    if (t > max_T) {
+      last = i;
+      max_T = t;
+    }
+  }
+  if (first <= last && (first < f->lb[0] || last > f->ub[0]))
+    return fail(nullptr, NRG_ERR_ARG, "the tabulated rows reach outside the arrays (no cell between 300.5 and 310 K)");
+  std::vector<std::string> names;
+  for (int k = 0; k < n_species; ++k) names.emplace_back(species_names[k]);
+  const std::string e = nrg::write_chem_table(
+      path, names, first, last, [&](int i) { return f->T[at(i)]; },
+      [&](int k, int i) { return f->Y_prod2[k][at(i)]; });
+  return e.empty() ? NRG_OK : fail(nullptr, NRG_ERR_IO, e);
+}
+
+extern "C" int nrg_chem_set_table(nrg_chem* h, long rows, const double* T_t, const double* Y_t) {
+  if (!h) return NRG_ERR_ARG;
+  if (rows < 1 || !T_t || !Y_t) return fail(h, NRG_ERR_ARG, "a table needs at least one row");
+  ON_DEVICE(h);
+  CK(h, cudaStreamSynchronize(h->stream));
+  cudaFree(h->d_tab_T);
+  cudaFree(h->d_tab_Y);
+  h->d_tab_T = h->d_tab_Y = nullptr;
+  h->tab_rows = 0;
+  const size_t N = (size_t)h->mech.n();
+  CK(h, cudaMalloc(&h->d_tab_T, sizeof(double) * (size_t)rows));
+  CK(h, cudaMalloc(&h->d_tab_Y, sizeof(double) * (size_t)rows * N));
+  CK(h, cudaMemcpy(h->d_tab_T, T_t, sizeof(double) * (size_t)rows, cudaMemcpyHostToDevice));
+  CK(h, cudaMemcpy(h->d_tab_Y, Y_t, sizeof(double) * (size_t)rows * N, cudaMemcpyHostToDevice));
+  h->tab_sorted = nrg::table_nodes_sorted(std::vector<double>(T_t, T_t + rows));
+  h->tab_rows = rows;
+  return NRG_OK;
+}
+
+extern "C" int nrg_chem_load_table(nrg_chem* h, const char* path) {
+  if (!h || !path) return NRG_ERR_ARG;
+  nrg::ChemTable t;
+  const std::string e = nrg::read_chem_table(path, h->mech.n(), &t);
+  if (!e.empty()) return fail(h, NRG_ERR_IO, e);
+  return nrg_chem_set_table(h, t.rows, t.T.data(), t.Y.data());
+}
+
 // ------------------------------------------------------------- surrogate
 namespace {
 int order_after_legacy(nrg_chem* h) {
@@ -1487,8 +1582,9 @@ extern "C" int nrg_chem_step_device_noalloc(nrg_chem* h, double time_step, long 
   if (!(time_step > 0.0) || !std::isfinite(time_step)) return fail(h, NRG_ERR_ARG, "time_step must be > 0");
   if (n > 0 && (!T || !rho || !Y || !Y_prod || !Y_prod2 || !E_f_prod))
     return fail(h, NRG_ERR_ARG, "null field pointer");
-  if (h->mode == NRG_MODE_SURROGATE)
-    return fail(h, NRG_ERR_STATE, "the surrogate needs buffers sized to the field; use nrg_chem_step_device");
+  if (h->mode == NRG_MODE_SURROGATE || h->mode == NRG_MODE_TABLE)
+    return fail(h, NRG_ERR_STATE,
+                "the no-allocation step integrates (reference, fast or mixed mode); use nrg_chem_step_device");
   if (n == 0) {
     if (stats) std::memset(stats, 0, sizeof(*stats));
     return NRG_OK;

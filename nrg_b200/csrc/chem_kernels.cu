@@ -6,6 +6,7 @@
 
 #include "chem_bdf.cuh"
 #include "chem_kernels.hpp"
+#include "table.hpp"
 
 namespace nrg {
 
@@ -152,6 +153,7 @@ void upload_mechanism(const DevMech& full, const DevMech& reduced, cudaStream_t 
   upload_mechanism_ref(full, s);
   upload_mechanism_fast(reduced, s);
   upload_mechanism_mixed(reduced, s);
+  upload_mechanism_table(full, s);
 }
 
 cudaError_t launch_chem(int n_species, int n_int, int spec, int n_reactions, int jac, bool mixed,

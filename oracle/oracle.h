@@ -12,7 +12,7 @@
  * hand-checked parser values instead.
  *
  * Reference files restated (paths inside yakovenko-ivan/NRG):
- *   computing_module/src/current_build/chemical_kinetics_solver.f90:175-540
+ *   computing_module/src/current_build/chemical_kinetics_solver.f90:175-685
  *   package_library/src/chemical_properties_class.f90:117-181,289-768
  *   package_library/src/thermophysical_properties_class.f90:225-452,876-881,1226-1341
  *   package_library/src/global_data.f90:35-44
@@ -135,6 +135,17 @@ int orc_species_predictor(int N, const double *W, int dims, const int n_cells[3]
                           const double *Y_prod_diff, const double *Y_prod_chem, int n_part,
                           const double *const *Y_prod_part, double *rho, double *Y, double *rho_old,
                           double *Y_old, double *rho_int, double *Y_int);
+
+/* table_approximated mode (orc_table.c; chemical_kinetics_solver.f90:542-685
+ * and the mode's branches of :228-346).  Table rows: T_t[i], Y_t[k*M + i]. */
+void orc_format_e14_7(double x, char out[15]);
+int orc_parse_e14_7(const char *field, int len, double *value);
+int orc_table_read(const char *path, int n_species, long capacity, double *T_t, double *Y_t, long *rows);
+int orc_table_write(const char *path, int n_species, const char (*names)[21], int lb, int ub, int lo, int hi,
+                    const double *T_row, const double *Y_prod2_row);
+int orc_table_step(const orc_mech *m, long M, const double *T_t, const double *Y_t, long n, double dt,
+                   const double *T, const double *Y, const signed char *bc, double *Y_prod, double *Y_prod2,
+                   double *E_f_prod, int n_threads);
 
 #ifdef __cplusplus
 }

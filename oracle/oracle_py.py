@@ -108,6 +108,18 @@ def lib():
         L.orc_dnrm2.restype = ctypes.c_double
         L.orc_ddcst.argtypes = [ctypes.c_int, dp, dp]
         L.orc_ddcst.restype = None
+        L.orc_format_e14_7.argtypes = [ctypes.c_double, ctypes.c_char_p]
+        L.orc_format_e14_7.restype = None
+        L.orc_parse_e14_7.argtypes = [ctypes.c_char_p, ctypes.c_int, dp]
+        L.orc_parse_e14_7.restype = ctypes.c_int
+        L.orc_table_read.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_long, ctypes.c_void_p,
+                                     ctypes.c_void_p, ctypes.POINTER(ctypes.c_long)]
+        L.orc_table_read.restype = ctypes.c_int
+        L.orc_table_write.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_void_p] + [ctypes.c_int] * 4 + [dp, dp]
+        L.orc_table_write.restype = ctypes.c_int
+        L.orc_table_step.argtypes = [ctypes.POINTER(OrcMech), ctypes.c_long, dp, dp, ctypes.c_long, ctypes.c_double,
+                                     dp, dp, ctypes.c_void_p, dp, dp, dp, ctypes.c_int]
+        L.orc_table_step.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -176,6 +188,42 @@ class Mechanism:
         c = np.frombuffer(cnt, dtype=np.int32).reshape(n, 4)
         return dict(Y_prod=Yp, Y_prod2=Yp2, E_f_prod=Ef, nstate=c[:, 0].copy(), nstep=c[:, 1].copy(),
                     nfe=c[:, 2].copy(), nje=c[:, 3].copy())
+
+    def table_step(self, T_t, Y_t, dt, T, Y, bc=None, Y_prod2_init=None, threads=0):
+        """table_approximated mode (orc_table_step): T_t (M,), Y_t (N, M)."""
+        n = T.shape[0]
+        N = self.m.n_species
+        T_t = np.ascontiguousarray(T_t, dtype=np.float64)
+        Y_t = np.ascontiguousarray(Y_t, dtype=np.float64).reshape(N, T_t.shape[0])
+        T = np.ascontiguousarray(T, dtype=np.float64)
+        Y = np.ascontiguousarray(Y, dtype=np.float64).reshape(N, n)
+        Yp = np.zeros((N, n))
+        Yp2 = np.zeros((N, n)) if Y_prod2_init is None else np.array(Y_prod2_init, dtype=np.float64)
+        Ef = np.zeros(n)
+        bcp = None
+        if bc is not None:
+            bc = np.ascontiguousarray(bc, dtype=np.int8)
+            bcp = bc.ctypes.data_as(ctypes.c_void_p)
+        rc = lib().orc_table_step(ctypes.byref(self.m), T_t.shape[0], _dp(T_t), _dp(Y_t), n, float(dt), _dp(T),
+                                  _dp(Y), bcp, _dp(Yp), _dp(Yp2), _dp(Ef), int(threads))
+        if rc != 0:
+            raise RuntimeError(f"orc_table_step: {rc}")
+        return dict(Y_prod=Yp, Y_prod2=Yp2, E_f_prod=Ef)
+
+    def table_write(self, path, lb, ub, lo, hi, T_row, Y_prod2_row):
+        """write_chemical_kinetics_table on one row (orc_table_write):
+        T_row (ub-lb+1,), Y_prod2_row (N, ub-lb+1), Fortran indices."""
+        N = self.m.n_species
+        T_row = np.ascontiguousarray(T_row, dtype=np.float64)
+        Y2 = np.ascontiguousarray(Y_prod2_row, dtype=np.float64).reshape(N, T_row.shape[0])
+        rc = lib().orc_table_write(str(path).encode(), N, ctypes.cast(self.m.species_names, ctypes.c_void_p),
+                                   lb, ub, lo, hi, _dp(T_row), _dp(Y2))
+        if rc != 0:
+            raise RuntimeError(f"orc_table_write: {rc}")
+
+    def table_read(self, path):
+        """read_chemical_kinetics_table (orc_table_read): (T_t, Y_t (N, M))."""
+        return table_read(path, self.m.n_species)
 
     def temperature_after(self, dt, T, rho, Y, Y_prod, E_f_prod, threads=0):
         n = T.shape[0]
@@ -311,3 +359,35 @@ def species_predictor(W, dims, n_cells, coord, dx, dt, v_f, rho, Y, rho_int, Y_i
     if rc != 0:
         raise ValueError(f"orc_species_predictor: bad arguments ({rc})")
     return out
+
+
+def format_e14_7(x: float) -> str:
+    """Fortran E14.7 output of one value."""
+    buf = ctypes.create_string_buffer(15)
+    lib().orc_format_e14_7(float(x), buf)
+    return buf.value.decode()
+
+
+def parse_e14_7(field: str) -> float:
+    """Fortran E14.7 input of one field."""
+    v = ctypes.c_double()
+    raw = field.encode()
+    if lib().orc_parse_e14_7(raw, len(raw), ctypes.byref(v)) != 0:
+        raise ValueError(f"malformed E14.7 field {field!r}")
+    return v.value
+
+
+def table_read(path, n_species: int):
+    """read_chemical_kinetics_table (orc_table_read): (T_t, Y_t (N, M))."""
+    rows = ctypes.c_long()
+    rc = lib().orc_table_read(str(path).encode(), n_species, 0, None, None, ctypes.byref(rows))
+    if rc != 0:
+        raise RuntimeError(f"orc_table_read: {rc}")
+    M = rows.value
+    T_t = np.zeros(M)
+    Y_t = np.zeros((n_species, M))
+    rc = lib().orc_table_read(str(path).encode(), n_species, M, T_t.ctypes.data, Y_t.ctypes.data,
+                              ctypes.byref(rows))
+    if rc != 0:
+        raise RuntimeError(f"orc_table_read: {rc}")
+    return T_t, Y_t
