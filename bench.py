@@ -519,8 +519,8 @@ def time_table(solver, W, args, dev, field, T, rho, Y, peaks, table_path, decks,
     om = op.Mechanism(*decks, 1.0, units)
     T_t, Y_t = op.table_read(table_path, N)
     o = om.table_step(T_t, Y_t, samp.dt, samp.T, samp.Y)
-    same = bool(np.array_equal(Yp[:, idx].cpu().numpy(), o["Y_prod"]) and
-                np.array_equal(Ef[idx].cpu().numpy(), o["E_f_prod"]))
+    same = bool(np.array_equal(Yp[:, idx].cpu().numpy(), o["Y_prod"], equal_nan=True) and
+                np.array_equal(Ef[idx].cpu().numpy(), o["E_f_prod"], equal_nan=True))
     solver.set_mode("fast")
     return {"ms": ms, "cells_per_s": n / (ms * 1e-3), "table_rows": int(T_t.size), "active_cells": active,
             "bytes_per_launch": nbytes, "algorithmic_GB_s": gbs, "frac_of_measured_hbm": gbs / peaks["hbm_gbs"],
