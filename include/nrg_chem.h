@@ -89,9 +89,8 @@ typedef struct {
   long long steps, rhs_evals, jacobians, solves;
   double device_ms;          /* device time of the step (CUDA events) */
   /* per-phase device time when phase timing is on (nrg_chem_set_timing):
-   * [0] surrogate inference (fused path: features + MLP + gate in one kernel;
-   * unfused: features + MLP), [1] the rejected cells' list (temperature
-   * order, or compaction in cell order; unfused: the gate too), [2] FP64
+   * [0] surrogate inference (features + MLP, then the FP64 gate), [1] the
+   * rejected cells' list (temperature order, or compaction in cell order), [2] FP64
    * integrator (with the plain step's temperature order), [3] unused */
   double phase_ms[4];
 } nrg_chem_stats;
@@ -385,9 +384,10 @@ NRG_API int nrg_surrogate_set_gate(nrg_chem* h, double elem_tol, double raw_elem
  * distribution they let cells through with errors of many kelvin.  No
  * counterpart in the reference. */
 NRG_API int nrg_surrogate_set_gate_dt(nrg_chem* h, double dt_max);
-/* Inference path of the surrogate step: 1 (default) one fused kernel
- * (features, the five layers on tcgen05 tensor cores with TMEM accumulators,
- * gate); 0 the unfused chain (features, one GEMM per layer, gate kernel). */
+/* Inference path of the surrogate step: 1 (default) the tensor-core kernel
+ * (features and the five layers on tcgen05 with TMEM accumulators) followed
+ * by the wide FP64 gate kernel; 0 the GEMM chain (features, one mma.sync
+ * GEMM per layer) followed by the same gate kernel. */
 NRG_API int nrg_surrogate_set_inference(nrg_chem* h, int fused);
 /* Network outputs (n x 16 fp32, normalised units) of the fused kernel for
  * every cell, no gate (device arrays, same layout as nrg_chem_step_device). */

@@ -1117,9 +1117,12 @@ __device__ int cell_advance(CS& c, int mxstep) {
 // Energy closure at constant density: the temperature the reference EOS
 // computes after the sources are added (cpm_solver.f90:517,549 ->
 // table_approximated_real_gas.f90:404-440 -> calculate_temperature,
-// thermophysical_properties_class.f90:409-452).
+// thermophysical_properties_class.f90:409-452).  The reference starts the
+// Newton iteration (frozen cp) at the temperature before the step; T_start
+// lets a caller that already has an estimate of the result start there.
 template <int N>
-__device__ __noinline__ double temperature_after_nl(double T0, const double* Y0, const double* dY, double dE) {
+__device__ __noinline__ double temperature_after_nl(double T0, double T_start, const double* Y0, const double* dY,
+                                                    double dE) {
   const double RG = 8.31446261815324;
   double X[N], avg = 0.0;
 #pragma unroll 1
@@ -1143,7 +1146,7 @@ __device__ __noinline__ double temperature_after_nl(double T0, const double* Y0,
   }
   const double W1 = ddiv(1.0, avg);
   double hc = 0.0, cp = 0.0;
-  double temp = NRG_FMIN(T0, 6000.0);
+  double temp = NRG_FMIN(T_start, 6000.0);
 #pragma unroll 1
   for (int k = 0; k < N; ++k) {
     X[k] = ddiv(Y1[k], c_mech.W[k]) * W1;
@@ -1165,14 +1168,20 @@ __device__ __noinline__ double temperature_after_nl(double T0, const double* Y0,
 
 template <int N>
 __device__ __forceinline__ double temperature_after(double T0, const double (&Y0)[N], const double (&dY)[N],
-                                                    double dE) {
+                                                    double dE, double T_start) {
   double a[N], b[N];
 #pragma unroll
   for (int k = 0; k < N; ++k) {
     a[k] = Y0[k];
     b[k] = dY[k];
   }
-  return temperature_after_nl<N>(T0, a, b, dE);
+  return temperature_after_nl<N>(T0, T_start, a, b, dE);
+}
+
+template <int N>
+__device__ __forceinline__ double temperature_after(double T0, const double (&Y0)[N], const double (&dY)[N],
+                                                    double dE) {
+  return temperature_after<N>(T0, Y0, dY, dE, T0);
 }
 
 // Outputs of a finished cell (chemical_kinetics_solver.f90:318-340); inert

@@ -308,50 +308,142 @@ __device__ __forceinline__ bool write_if_skipped(const StepArgs& a, long c, doub
   return true;
 }
 
+// Per-block copy of what the gate's energy closure reads: NASA-7 enthalpy
+// coefficients pre-divided by their powers (b_i = a_i / (i + 1), i < 5, and
+// a_5), cp coefficients a_0..a_4, both sets of each species, and 1 / W.
+struct GateThermo {
+  double h[9][2][6];
+  double cp[9][2][5];
+  double invW[9];
+};
+
+__device__ void gate_thermo_init(GateThermo* g) {
+  for (int i = threadIdx.x; i < 9 * 2; i += blockDim.x) {
+    const int k = i >> 1, set = i & 1;
+    const double* a = c_mech.a[k][set];
+    for (int j = 0; j < 5; ++j) {
+      g->h[k][set][j] = a[j] / (double)(j + 1);
+      g->cp[k][set][j] = a[j];
+    }
+    g->h[k][set][5] = a[5];
+    if (set == 0) g->invW[k] = c_mech.invW[k];
+  }
+}
+
+// h_k(T) * ... as the reference's specie_enthalpy (per mole, times R in the
+// tables): t (b0 + t (b1 + t (b2 + t (b3 + t b4)))) + a5, t = min(T, 6000 K).
+__device__ __forceinline__ double gate_enthalpy(const GateThermo& g, int k, double T) {
+  const double t = fmin(T, 6000.0);
+  const double* b = g.h[k][t >= 1000.0 ? 1 : 0];
+  return fma(t, fma(t, fma(t, fma(t, fma(t, b[4], b[3]), b[2]), b[1]), b[0]), b[5]);
+}
+
+// Energy closure of the gate: the reference's constant-density closure
+// (cpm_solver.f90:517,549; calculate_temperature, thermophysical_properties_
+// class.f90:409-452 -- Newton with cp frozen at the start temperature, at
+// most 1000 iterations, |step| < 1e-8 K) unrolled over the nine species in
+// registers, started at T_start (the network's temperature).  The gate
+// compares its result with the network's temperature change within dT_tol,
+// so it agrees with the integrator's closure to far below that tolerance
+// rather than to its last bit.
+__device__ __forceinline__ double gate_closure(const GateThermo& g, double T0, double T_start,
+                                               const double (&Y0)[9], const double (&dY)[9], double dE) {
+  const double RG = 8.31446261815324;
+  double X[9], s0 = 0.0, s1 = 0.0;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) s0 += Y0[k] * g.invW[k];
+  const double W0 = 1.0 / s0;
+  double e0 = 0.0, h0 = 0.0;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    const double x = Y0[k] * g.invW[k] * W0;
+    e0 += gate_enthalpy(g, k, T0) * x;
+    h0 += c_mech.h_ref[k] * x;
+  }
+  e0 -= RG * T0;
+  const double e1 = (e0 - h0) / W0 + dE;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    X[k] = Y0[k] + dY[k];
+    s1 += X[k] * g.invW[k];
+  }
+  const double W1 = 1.0 / s1;
+  double hc = 0.0, cp = 0.0;
+  double temp = fmin(T_start, 6000.0);
+  const int set = temp >= 1000.0 ? 1 : 0;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    X[k] = X[k] * g.invW[k] * W1;
+    hc += c_mech.h_ref[k] * X[k];
+    const double* a = g.cp[k][set];
+    cp += fma(temp, fma(temp, fma(temp, fma(temp, a[4], a[3]), a[2]), a[1]), a[0]) * X[k];
+  }
+  const double ei = e1 * W1, rcp = 1.0 / cp;
+  for (int it = 0; it < 1000; ++it) {
+    double e = 0.0;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) e += gate_enthalpy(g, k, temp) * X[k];
+    e -= RG * temp;
+    const double res = (ei - (e - hc)) * rcp;
+    temp += res;
+    if (fabs(res) < (double)1e-08f) break;
+  }
+  return temp;
+}
+
 // Gate of one active cell on its network outputs o (normalised units): hull
 // of the raw features f, element residuals, FP64 projection, energy closure.
 // Writes the sources of an accepted cell and returns whether it was accepted.
-__device__ __noinline__ bool gate_active_cell(const StepArgs& a, long c, double T0, double rho, double dt,
-                                                 const double (&y0)[9], const float (&f)[kMlpIn],
-                                                 const float* o, const MlpNorm* nm, const GateCfg& gc,
-                                                 const double (*P)[9]) {
-  bool ok = dt <= gc.dt_max;
+// Each test returns as soon as it fails; the cell's mass fractions are read
+// again (from cache) for the closure rather than kept live across the tests.
+__device__ __forceinline__ bool gate_active_cell(const StepArgs& a, long c, double T0, double rho, double dt,
+                                                 const float (&f)[kMlpIn], const float (&o)[kMlpOut],
+                                                 const MlpNorm* nm, const GateCfg& gc, const double (*P)[9],
+                                                 const GateThermo& th) {
+  if (!(dt <= gc.dt_max)) return false;
+  bool in = true;
+  const float margin = nm->hull_margin;
 #pragma unroll
   for (int j = 0; j < kMlpIn; ++j) {
-    const float span = nm->x_max[j] - nm->x_min[j];
-    const float lo = nm->x_min[j] - nm->hull_margin * span, hi = nm->x_max[j] + nm->hull_margin * span;
-    ok = ok && (f[j] >= lo) && (f[j] <= hi);
+    const float lo0 = nm->x_min[j], hi0 = nm->x_max[j], span = hi0 - lo0;
+    in = in && (f[j] >= lo0 - margin * span) && (f[j] <= hi0 + margin * span);
   }
+  if (!in) return false;
   const double sc = (double)target_scale(f[11], nm->dt_pow);
   double dYn[9];
+  bool fin = true;
 #pragma unroll
   for (int k = 0; k < 9; ++k) {
     dYn[k] = (double)o[k] * (double)nm->y_sd[k] * sc;
-    ok = ok && isfinite(dYn[k]);
+    fin = fin && isfinite(dYn[k]);
   }
   const double dT_net = (double)o[9] * (double)nm->y_sd[9] * sc;
-  ok = ok && isfinite(dT_net) && fabs(dT_net) <= gc.dT_max;
-  ok = ok && element_residual(dYn) <= gc.raw_elem_tol;
-  if (!ok) return false;
+  if (!fin || !isfinite(dT_net) || !(fabs(dT_net) <= gc.dT_max)) return false;
+  if (!(element_residual(dYn) <= gc.raw_elem_tol)) return false;
   // the written increment conserves H, O and N: projection in FP64
   double dY[9];
 #pragma unroll
   for (int i = 0; i < 9; ++i) {
     double x = 0.0;
 #pragma unroll
-    for (int j = 0; j < 9; ++j) x += P[i][j] * dYn[j];
+    for (int j = 0; j < 9; ++j) x = fma(P[i][j], dYn[j], x);
     dY[i] = x;
   }
   if (!(element_residual(dY) <= gc.elem_tol)) return false;
+  const double rho_dt = rho / dt;
   double E = 0.0;
 #pragma unroll
-  for (int k = 0; k < 9; ++k) E = E - c_mech.h_ref[k] * (dY[k] * rho / c_mech.W[k]) / dt;
-  const double T1 = temperature_after<9>(T0, y0, dY, E * dt / rho);
+  for (int k = 0; k < 9; ++k) E -= c_mech.h_ref[k] * (dY[k] * th.invW[k]) * rho_dt;
+  double y0[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) y0[k] = a.Y[k * a.ld + c];
+  // the Newton iteration of the closure starts at the network's temperature
+  const double T1 = gate_closure(th, T0, T0 + dT_net, y0, dY, E * dt / rho);
   if (!(fabs((T1 - T0) - dT_net) <= gc.dT_tol)) return false;
 #pragma unroll
   for (int k = 0; k < 9; ++k) {
-    a.Y_prod[k * a.ld + c] = dY[k] * rho / dt;
-    a.Y_prod2[k * a.ld + c] = dY[k] * rho / c_mech.W[k];
+    a.Y_prod[k * a.ld + c] = dY[k] * rho_dt;
+    a.Y_prod2[k * a.ld + c] = dY[k] * rho * th.invW[k];
   }
   a.E_f_prod[c] = E;
   if (a.T_after) a.T_after[c] = T1;
@@ -365,10 +457,14 @@ __device__ __forceinline__ void count_surrogate(unsigned long long n_sur, unsign
   if ((threadIdx.x & 31) == 0 && n_sur) atomicAdd(&counters[6], n_sur);
 }
 
-__global__ void k_gate(StepArgs a, const float* O, const MlpNorm* nm, GateCfg gc, unsigned char* flag,
-                       unsigned long long* counters) {
+// O: the network outputs of every active cell, output j of cell c at
+// O[j * o_ld + c] (o_ld > 0) or O[c * 16 + j] (o_ld == 0).
+__global__ void __launch_bounds__(128, 3) k_gate(StepArgs a, const float* O, long o_ld, const MlpNorm* nm, GateCfg gc,
+                                              unsigned char* flag, unsigned long long* counters) {
   __shared__ double P[9][9];
+  __shared__ GateThermo th;
   if (threadIdx.x == 0) element_projector(P);
+  gate_thermo_init(&th);
   __syncthreads();
   unsigned long long n_sur = 0;
   for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < a.n; c += (long)gridDim.x * blockDim.x) {
@@ -379,54 +475,64 @@ __global__ void k_gate(StepArgs a, const float* O, const MlpNorm* nm, GateCfg gc
     }
     const double rho = a.rho[c];
     const double dt = a.dt_cells ? a.dt_cells[c] : a.dt;
-    double y0[9];
+    float f[kMlpIn], o[kMlpOut];
+    {
+      double y0[9];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) y0[k] = a.Y[k * a.ld + c];
-    float f[kMlpIn];
-    cell_features<9>(T0, rho, y0, dt, f);
-    const bool acc = gate_active_cell(a, c, T0, rho, dt, y0, f, O + c * kMlpOutPad, nm, gc, P);
+      for (int k = 0; k < 9; ++k) y0[k] = a.Y[k * a.ld + c];
+      cell_features<9>(T0, rho, y0, dt, f);
+    }
+#pragma unroll
+    for (int j = 0; j < kMlpOut; ++j) o[j] = o_ld > 0 ? O[j * o_ld + c] : O[c * kMlpOutPad + j];
+    const bool acc = gate_active_cell(a, c, T0, rho, dt, f, o, nm, gc, P, th);
     n_sur += acc;
     flag[c] = acc ? 0 : 1;
   }
   count_surrogate(n_sur, counters);
 }
 
-// ------------------------------------------------- fused tcgen05 inference
-// One kernel per step for features -> 5 MLP layers -> gate.  Persistent CTAs
-// of two warpgroups; each warpgroup streams its own 128-cell tiles (thread t
-// of the group owns cell t of the tile, which is TMEM lane t).  Per tile:
-// features are standardised into a bf16 K-major operand in shared memory,
-// one thread issues the layer's tcgen05.mma (M = 128, A = activations,
-// B = weights, both in shared memory; FP32 accumulator in this group's 128
-// TMEM columns) and commits to the group's mbarrier; the epilogue reads the
-// thread's accumulator row with tcgen05.ld, adds the bias, applies GELU and
-// writes the next layer's bf16 operand.  The weights (104 KB) stay in shared
-// memory for the kernel's lifetime.  While one group runs its epilogue the
-// other group's MMAs run.  Every wait is bounded: on a timeout the group
-// stops issuing MMAs, sends its remaining cells to the FP64 fallback and
-// records the event in *err.
-constexpr int kTcGroups = 2;
+// ------------------------------------------------- tcgen05 inference
+// The network of the surrogate step runs in its own kernel, k_mlp_tc, and the
+// FP64 gate in a wide grid after it (k_gate, above), so that the gate's
+// latency-bound FP64 work (energy-closure Newton, element projection) runs
+// with many warps per SM instead of inside the tensor-core kernel.
+//
+// k_mlp_tc: persistent CTAs of three warpgroups; each warpgroup streams its
+// own 128-cell tiles (thread t of the group owns cell t of the tile, which is
+// TMEM lane t).  Per tile: features are standardised into a bf16 K-major
+// operand in shared memory, one thread issues the layer's tcgen05.mma
+// (M = 128, A = activations, B = weights, both in shared memory; FP32
+// accumulator in this group's 128 TMEM columns) and commits to the group's
+// mbarrier; the epilogue reads the thread's accumulator row with tcgen05.ld,
+// adds the bias, applies GELU and writes the next layer's bf16 operand.  The
+// weights (104 KB) stay in shared memory for the kernel's lifetime; while one
+// group runs its epilogue the others' MMAs run.  Tiles without an active cell
+// skip the network.  Every wait is bounded: on a timeout the group stops
+// issuing MMAs, writes NaN outputs for its remaining cells (the gate sends
+// them to the FP64 integrator) and records the event in *err.
+constexpr int kTcGroups = 3;
 constexpr uint32_t kTcW0 = 0;                             // layer 0: 128 x 16
 constexpr uint32_t kTcW1 = 4096;                          // layers 1-3: 128 x 128
 constexpr uint32_t kTcW4 = kTcW1 + 3 * 32768;             // layer 4: 16 x 128
 constexpr uint32_t kTcAct = kTcW4 + 4096;                 // per group 128 x 128 bf16
 constexpr uint32_t kTcBias = kTcAct + kTcGroups * 32768;  // fp32, 4 x 128 + 16
 constexpr uint32_t kTcMisc = kTcBias + (4 * kMlpHid + kMlpOutPad) * 4;
-constexpr uint32_t kTcSmem = kTcMisc + 1024;
+constexpr uint32_t kTcSmem = kTcMisc + 256;
+constexpr uint32_t kTcTmemCols = 512;  // a power of two holding 128 columns per group
+static_assert(kTcGroups * 128 <= (int)kTcTmemCols, "TMEM columns of the groups");
+static_assert(kTcSmem <= 227u * 1024u, "shared memory of one CTA");
 constexpr uint64_t kTcWaitNs = 1000000000ull;  // 1 s per MMA wait
 
 struct TcArgs {
   StepArgs a;
   const MlpNorm* nm;
-  GateCfg gc;
   const __nv_bfloat16* wb;  // bf16 parameters (per layer W[out][in_pad], then b)
   const float* w;           // fp32 parameters (biases read from here)
   long offW[kMlpLayers], offb[kMlpLayers];
-  unsigned char* flag;          // gate: 1 = FP64 fallback
-  unsigned long long* counters;
-  float* out;                   // optional: network outputs, n x 16 (normalised units)
-  int gate;                     // 0: outputs only, every cell
-  unsigned int* err;            // bit 0: an MMA wait timed out
+  float* out;    // network outputs (normalised units)
+  long out_ld;   // > 0: output j of cell c at out[j * out_ld + c] (kMlpOut values); 0: out[c * 16 + j]
+  int active;    // 1: only the cells the step integrates (skip rule); 0: every cell
+  unsigned int* err;  // bit 0: an MMA wait timed out
 };
 
 __device__ __forceinline__ uint4 pack8(const float* v) {
@@ -438,14 +544,24 @@ __device__ __forceinline__ uint4 pack8(const float* v) {
   return r;
 }
 
-__global__ void __launch_bounds__(128 * kTcGroups, 1) k_mlp_gate_tc(TcArgs p) {
+__device__ __forceinline__ void store_outputs(const TcArgs& p, long c, const float* o, bool valid) {
+  const float nan = __int_as_float(0x7fc00000);
+  if (p.out_ld > 0) {
+#pragma unroll
+    for (int j = 0; j < kMlpOut; ++j) p.out[j * p.out_ld + c] = valid ? o[j] : nan;
+  } else {
+#pragma unroll
+    for (int j = 0; j < kMlpOutPad; ++j) p.out[c * kMlpOutPad + j] = !valid ? nan : (j < kMlpOut ? o[j] : 0.f);
+  }
+}
+
+__global__ void __launch_bounds__(128 * kTcGroups, 1) k_mlp_tc(TcArgs p) {
   extern __shared__ __align__(1024) unsigned char sm[];
   const StepArgs& a = p.a;
   const int tid = threadIdx.x, g = tid >> 7, t = tid & 127, wq = t >> 5;
   uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + kTcMisc);         // [kTcGroups]
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kTcMisc + 16);
-  uint32_t* vote = reinterpret_cast<uint32_t*>(sm + kTcMisc + 32);    // [group][parity][warp]
-  double(*P)[9] = reinterpret_cast<double(*)[9]>(sm + kTcMisc + 128);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kTcMisc + 32);
+  uint32_t* vote = reinterpret_cast<uint32_t*>(sm + kTcMisc + 64);    // [group][parity][warp]
   float* bias = reinterpret_cast<float*>(sm + kTcBias);
 
   // weights into the K-major canonical layout, biases, barriers, TMEM
@@ -470,9 +586,8 @@ __global__ void __launch_bounds__(128 * kTcGroups, 1) k_mlp_gate_tc(TcArgs p) {
   if (tid == 0) {
     for (int i = 0; i < kTcGroups; ++i) tc::mbar_init(tc::smem_u32(&mbar[i]), 1);
     tc::mbar_init_fence();
-    element_projector(P);
   }
-  if (tid < 32) tc::tmem_alloc(tc::smem_u32(tslot), 128 * kTcGroups);
+  if (tid < 32) tc::tmem_alloc(tc::smem_u32(tslot), kTcTmemCols);
   tc::fence_async_smem();
   tc::fence_before_sync();
   __syncthreads();
@@ -489,32 +604,27 @@ __global__ void __launch_bounds__(128 * kTcGroups, 1) k_mlp_gate_tc(TcArgs p) {
   constexpr uint32_t kIdHid = tc::idesc_bf16_f32(128, 128), kIdOut = tc::idesc_bf16_f32(128, 16);
   uint32_t phase = 0;
   bool aborted = false;
-  unsigned long long n_sur = 0;
   const long ntiles = (a.n + 127) / 128;
   int par = 0;
   for (long tile = (long)blockIdx.x * kTcGroups + g; tile < ntiles; tile += (long)gridDim.x * kTcGroups, par ^= 1) {
     const long c = tile * 128 + t;
     bool need = false;
-    double T0 = 0.0, rho = 0.0, dt = 1.0, y0[9];
     float f[kMlpIn];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) y0[k] = 0.0;
 #pragma unroll
     for (int j = 0; j < kMlpIn; ++j) f[j] = 0.f;
     if (c < a.n) {
-      T0 = a.T[c];
-      need = p.gate ? !write_if_skipped(a, c, T0) : true;
-      if (p.gate && !need) p.flag[c] = 0;
+      const double T0 = a.T[c];
+      need = p.active ? reference_cell_active(T0, a.bc, c) : true;
       if (need) {
-        rho = a.rho[c];
-        dt = a.dt_cells ? a.dt_cells[c] : a.dt;
+        double y0[9];
 #pragma unroll
         for (int k = 0; k < 9; ++k) y0[k] = a.Y[k * a.ld + c];
-        cell_features<9>(T0, rho, y0, dt, f);
+        cell_features<9>(T0, a.rho[c], y0, a.dt_cells ? a.dt_cells[c] : a.dt, f);
       }
     }
+    float o[kMlpOutPad];
     if (aborted) {
-      if (need && p.gate) p.flag[c] = 1;
+      if (need) store_outputs(p, c, o, false);
       continue;
     }
     const unsigned bal = __ballot_sync(0xffffffffu, need);
@@ -574,7 +684,6 @@ __global__ void __launch_bounds__(128 * kTcGroups, 1) k_mlp_gate_tc(TcArgs p) {
         tc::commit(mb);
       }
     }
-    float o[kMlpOutPad];
     if (ok) {
       ok = __all_sync(0xffffffffu, tc::mbar_wait(mb, phase, kTcWaitNs));
       phase ^= 1u;
@@ -592,27 +701,14 @@ __global__ void __launch_bounds__(128 * kTcGroups, 1) k_mlp_gate_tc(TcArgs p) {
     if (!ok) {
       aborted = true;
       if (t == 0) atomicOr(p.err, 1u);
-      if (need && p.gate) p.flag[c] = 1;
-      continue;
     }
-    if (need) {
-      if (p.out) {
-#pragma unroll
-        for (int j = 0; j < kMlpOutPad; ++j) p.out[c * kMlpOutPad + j] = j < kMlpOut ? o[j] : 0.f;
-      }
-      if (p.gate) {
-        const bool acc = gate_active_cell(a, c, T0, rho, dt, y0, f, o, p.nm, p.gc, P);
-        n_sur += acc;
-        p.flag[c] = acc ? 0 : 1;
-      }
-    }
+    if (need) store_outputs(p, c, o, ok);
   }
-  count_surrogate(n_sur, p.counters);
   tc::fence_before_sync();
   __syncthreads();
   if (tid < 32) {
     tc::fence_after_sync();
-    tc::tmem_dealloc(tbase, 128 * kTcGroups);
+    tc::tmem_dealloc(tbase, kTcTmemCols);
   }
 }
 
@@ -770,13 +866,15 @@ struct Surrogate {
   long icap = 0;
   __nv_bfloat16 *iX = nullptr, *iH[2] = {nullptr, nullptr};
   float* iO = nullptr;
-  // fused tcgen05 inference (default) or the unfused GEMM chain + gate
+  // tcgen05 inference (default) or the mma.sync GEMM chain, then the gate
   bool fused = true;
   int num_sms = 0;
-  unsigned int* d_err = nullptr;  // bit 0: an MMA wait of the fused kernel timed out
+  unsigned int* d_err = nullptr;  // bit 0: an MMA wait of the tensor-core kernel timed out
   unsigned int* h_err = nullptr;  // pinned
-  // gate / compaction buffers
+  // gate / compaction buffers; gO: network outputs of the tensor-core kernel
+  // (kMlpOut planes of gcap floats)
   long gcap = 0;
+  float* gO = nullptr;
   unsigned char* flag = nullptr;
   int *block_count = nullptr, *block_off = nullptr, *list = nullptr, *n_list = nullptr;
   // fallback cells in temperature order (order.hpp) or in cell order
@@ -823,7 +921,7 @@ Surrogate* surrogate_create(const DevMech& dm) {
   int dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaFuncSetAttribute(k_mlp_gate_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
+  cudaFuncSetAttribute(k_mlp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
   cudaMemset(s->w, 0, P * 4);
   cudaMemset(s->m, 0, P * 4);
   cudaMemset(s->v, 0, P * 4);
@@ -853,7 +951,8 @@ void surrogate_destroy(Surrogate* s) {
   free_act(s);
   cudaFree(s->w); cudaFree(s->m); cudaFree(s->v); cudaFree(s->gr); cudaFree(s->wb); cudaFree(s->d_norm);
   cudaFree(s->iX); cudaFree(s->iH[0]); cudaFree(s->iH[1]); cudaFree(s->iO);
-  cudaFree(s->d_loss); cudaFree(s->flag); cudaFree(s->block_count); cudaFree(s->block_off); cudaFree(s->list);
+  cudaFree(s->d_loss); cudaFree(s->flag); cudaFree(s->gO); cudaFree(s->block_count); cudaFree(s->block_off);
+  cudaFree(s->list);
   cudaFree(s->n_list);
   order_free(&s->order);
   cudaFree(s->d_err);
@@ -915,8 +1014,11 @@ static std::string ensure_infer(Surrogate* s, long n) {
 static std::string ensure_gate(Surrogate* s, long n) {
   if (n <= s->gcap) return "";
   cudaFree(s->flag); cudaFree(s->block_count); cudaFree(s->block_off); cudaFree(s->list); cudaFree(s->n_list);
+  cudaFree(s->gO);
+  s->gO = nullptr;
   const long nb = (n + kCompactBlock - 1) / kCompactBlock;
   std::string e;
+  if ((e = ck(cudaMalloc(&s->gO, sizeof(float) * kMlpOut * (size_t)n), "alloc outputs")).size()) return e;
   if ((e = ck(cudaMalloc(&s->flag, n), "alloc flag")).size()) return e;
   if ((e = ck(cudaMalloc(&s->block_count, nb * 4), "alloc counts")).size()) return e;
   if ((e = ck(cudaMalloc(&s->block_off, nb * 4), "alloc offsets")).size()) return e;
@@ -1219,21 +1321,19 @@ std::string surrogate_reserve(Surrogate* s, long n) {
   return ensure_gate(s, n);
 }
 
-static TcArgs tc_args(Surrogate* s, const StepArgs& a, unsigned long long* counters, float* out, int gate) {
+static TcArgs tc_args(Surrogate* s, const StepArgs& a, float* out, long out_ld, int active) {
   TcArgs p{};
   p.a = a;
   p.nm = s->d_norm;
-  p.gc = s->gate;
   p.wb = s->wb;
   p.w = s->w;
   for (int l = 0; l < kMlpLayers; ++l) {
     p.offW[l] = s->offW[l];
     p.offb[l] = s->offb[l];
   }
-  p.flag = s->flag;
-  p.counters = counters;
   p.out = out;
-  p.gate = gate;
+  p.out_ld = out_ld;
+  p.active = active;
   p.err = s->d_err;
   return p;
 }
@@ -1242,15 +1342,24 @@ static cudaError_t launch_tc(Surrogate* s, const TcArgs& p, cudaStream_t st) {
   const long ntiles = (p.a.n + 127) / 128;
   const int grid = (int)std::max<long>(1, std::min<long>(s->num_sms > 0 ? s->num_sms : 148,
                                                          (ntiles + kTcGroups - 1) / kTcGroups));
-  k_mlp_gate_tc<<<grid, 128 * kTcGroups, kTcSmem, st>>>(p);
+  k_mlp_tc<<<grid, 128 * kTcGroups, kTcSmem, st>>>(p);
+  return cudaGetLastError();
+}
+
+// The FP64 gate over the n cells of a, in a grid of 128-thread blocks.
+static cudaError_t launch_gate(Surrogate* s, const StepArgs& a, const float* O, long o_ld,
+                               unsigned long long* counters, cudaStream_t st) {
+  const int sms = s->num_sms > 0 ? s->num_sms : 148;
+  const long grid = std::min<long>((a.n + 127) / 128, (long)sms * 16);
+  k_gate<<<(unsigned)std::max<long>(grid, 1), 128, 0, st>>>(a, O, o_ld, s->d_norm, s->gate, s->flag, counters);
   return cudaGetLastError();
 }
 
 std::string surrogate_infer(Surrogate* s, const StepArgs& a, float* out, cudaStream_t st) {
   if (a.n <= 0) return "";
-  std::string e = ck(launch_tc(s, tc_args(s, a, nullptr, out, 0), st), "fused inference");
+  std::string e = ck(launch_tc(s, tc_args(s, a, out, 0, 0), st), "tensor-core inference");
   if (!e.empty()) return e;
-  if ((e = ck(cudaStreamSynchronize(st), "fused inference")).size()) return e;
+  if ((e = ck(cudaStreamSynchronize(st), "tensor-core inference")).size()) return e;
   return surrogate_check(s, st);
 }
 
@@ -1261,7 +1370,7 @@ std::string surrogate_check(Surrogate* s, cudaStream_t st) {
   if (*s->h_err) {
     cudaMemsetAsync(s->d_err, 0, 4, st);
     cudaStreamSynchronize(st);
-    return "a tensor-core wait of the fused MLP kernel timed out; the affected cells were integrated in FP64";
+    return "a tensor-core wait of the MLP kernel timed out; the affected cells were integrated in FP64";
   }
   return "";
 }
@@ -1278,15 +1387,16 @@ cudaError_t surrogate_step(Surrogate* s, const StepArgs& a, const LaunchCfg& cfg
   const long n = a.n;
   cudaError_t e;
   if (s->fused) {
-    if ((e = launch_tc(s, tc_args(s, a, counters, nullptr, 1), st)) != cudaSuccess) return e;
+    // network outputs of the active cells, planar, then the wide FP64 gate
+    if ((e = launch_tc(s, tc_args(s, a, s->gO, n, 1), st)) != cudaSuccess) return e;
+    if ((e = launch_gate(s, a, s->gO, n, counters, st)) != cudaSuccess) return e;
     if (ph) cudaEventRecord(ph[1], st);
   } else {
     k_features<<<std::min<long>((n + 255) / 256, 148 * 16), 256, 0, st>>>(n, a.ld, a.dt, a.dt_cells, a.T, a.rho,
                                                                         a.Y, s->d_norm, nullptr, s->iX);
     if ((e = forward_infer(s, n, s->iX, s->iO, st)) != cudaSuccess) return e;
+    if ((e = launch_gate(s, a, s->iO, 0, counters, st)) != cudaSuccess) return e;
     if (ph) cudaEventRecord(ph[1], st);
-    k_gate<<<std::min<long>((n + 255) / 256, 148 * 16), 256, 0, st>>>(a, s->iO, s->d_norm, s->gate, s->flag,
-                                                                    counters);
   }
   if (s->order_cells) {
     // rejected cells grouped by temperature: the fallback's warps then hold

@@ -33,8 +33,8 @@ std::string bounded_wait_probe(unsigned long long limit_ns, int* timed_out, doub
 // on the cells the gate rejects.  counters[6] / [7] receive surrogate /
 // fallback cell counts.
 // ph (may be null): events recorded at phase boundaries: ph[1] after the
-// fused MLP + gate kernel (unfused path: after the last GEMM, before the gate
-// kernel); the fallback callback records ph[2] / ph[3] around the integrator.
+// network and the gate kernel; the fallback callback records ph[2] / ph[3]
+// around the integrator.
 cudaError_t surrogate_step(Surrogate* s, const StepArgs& a, const LaunchCfg& cfg, int* queue,
                            unsigned long long* counters, cudaStream_t st, const FallbackFn& fallback,
                            cudaEvent_t* ph);
@@ -75,13 +75,13 @@ std::string surrogate_prepare(Surrogate* s, long n, long ld, double dt, const do
 void surrogate_set_ready(Surrogate* s, bool ready);
 // Fallback cells grouped by temperature (default) or in cell order.
 void surrogate_set_cell_order(Surrogate* s, bool by_temperature);
-// Inference path of surrogate_step: fused tcgen05 kernel (default) or the
-// unfused GEMM chain followed by the gate kernel.
+// Inference path of surrogate_step: the tcgen05 kernel (default) or the
+// mma.sync GEMM chain, either followed by the gate kernel.
 void surrogate_set_fused(Surrogate* s, bool fused);
-// Fused features + MLP over the n cells of a (no gate): out is n x 16 fp32
-// network outputs in normalised units; synchronises.
+// Features + MLP on tcgen05 over the n cells of a (no gate): out is n x 16
+// fp32 network outputs in normalised units; synchronises.
 std::string surrogate_infer(Surrogate* s, const StepArgs& a, float* out, cudaStream_t st);
-// Reads and clears the fused kernel's error word (after the step's work).
+// Reads and clears the tensor-core kernel's error word (after the step's work).
 std::string surrogate_check(Surrogate* s, cudaStream_t st);
 void surrogate_set_gate(Surrogate* s, double elem_tol, double raw_elem_tol, double dT_tol, double dT_max);
 // Longest step (s) whose cells the gate may accept.
