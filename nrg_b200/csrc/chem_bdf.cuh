@@ -114,7 +114,7 @@ template <int N, int R, typename LUT, int BS, int SPEC>
 __device__ __noinline__ void nl_analytic_matrix(double* d, LUT* f, double factor);
 template <int N, int R, typename LUT, int BS, bool RECIP>
 __device__ __noinline__ RowPerm<N> nl_dgefa(double* d, LUT* f, int* info);
-template <int N, int R, typename LUT, int BS>
+template <int N, int R, typename LUT, int BS, bool FAST>
 __device__ __noinline__ void nl_rate_constants(double* d, LUT* f, double T);
 
 // N integrated species (vectors, Nordsieck rows, LU), NF mechanism species
@@ -274,6 +274,86 @@ __device__ void rate_constants(CS& c, double Tin) {
       const double Kp = nexp(ddiv(d_s, RG) - ddiv(ddiv(d_h, RG), T));
       kr = ddiv(k, Kp * int_pow(conc_ref, c_mech.dnu[r]));
     }
+    c.kf(r) = m_left ? k * mc : k;
+    c.kr(r) = m_right ? kr * mc : kr;
+  }
+}
+
+// calculate_rate_constants for the analytic-Jacobian and mixed modes, whose
+// results agree with the reference's to its tolerance rather than bit for
+// bit: each Arrhenius rate as one exponential, A exp(beta ln T - E / (R T)),
+// the reverse rate as the forward one times one exponential of
+// -dS/R + dH/(R T) - dnu ln(p_atm / (R T)), the Troe blending power as an
+// exponential, and the reactions four at a time with the libm calls inline,
+// so that their long-latency chains overlap.  The same temperature caps as
+// the reference (1e4 K for the rates, 6000 K for the thermochemistry).
+template <int N, int R, class CS>
+__device__ void rate_constants_fast(CS& c, double Tin) {
+  const double RG = 8.31446261815324, PATM = 101325.0;
+  const double T = NRG_FMIN(Tin, 10000.0);
+  const double tt = NRG_FMIN(T, 6000.0);
+  const double logt = log(tt), lnT = log(T), rT = 1.0 / T, rRT = rT / RG;
+  const int set = nasa_set(tt);
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    const double* a = c_mech.a[c_mech.full_of[k]][set];
+    // entropy and enthalpy as d_entropy / d_enthalpy
+    const double sp = fma(fma(fma(a[4] * 0.25, tt, a[3] * (1.0 / 3.0)), tt, a[2] * 0.5), tt, a[1]);
+    c.z(k) = fma(sp, tt, fma(a[0], logt, a[6]));
+    const double hp = fma(fma(fma(fma(a[4] * 0.2, tt, a[3] * 0.25), tt, a[2] * (1.0 / 3.0)), tt, a[1] * 0.5), tt, a[0]);
+    c.zd(k) = fma(hp, tt, a[5]);
+  }
+  const double ln_conc_ref = log(PATM / RG) - lnT;
+#pragma unroll 4
+  for (int r = 0; r < R; ++r) {
+    const double mc = c.kr(r);
+    double d_s = 0.0, d_h = 0.0;
+    bool m_left = false, m_right = false;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      if (i < c_mech.nr[r]) {
+        const int sp = c_mech.right[r][i];
+        if (sp < 0) m_right = true;
+        else {
+          d_s += c.z(sp);
+          d_h += c.zd(sp);
+        }
+      }
+      if (i < c_mech.nl[r]) {
+        const int sp = c_mech.left[r][i];
+        if (sp < 0) m_left = true;
+        else {
+          d_s -= c.z(sp);
+          d_h -= c.zd(sp);
+        }
+      }
+    }
+    const int type = c_mech.type[r];
+    const double kinf = c_mech.A[r] * exp(c_mech.beta[r] * lnT - c_mech.E[r] * rRT);
+    double k = kinf;
+    if (type == 2 || type == 3 || type == 7) {
+      const double k0 = c_mech.A_low[r] * exp(c_mech.beta_low[r] * lnT - c_mech.E_low[r] * rRT);
+      const double rp = k0 * mc / kinf;
+      k = kinf * (rp / (1.0 + rp));
+      if (type == 3) {
+        const double al = c_mech.troe[r][0];
+        const double Fc = (1.0 - al) * exp(-T / c_mech.troe[r][1]) + al * exp(-T / c_mech.troe[r][2]) +
+                          exp(-c_mech.troe[r][3] * rT);
+        const double lnFc = log(Fc), lf = lnFc * 0.43429448190325182765;
+        const double cc = -0.4 - 0.67 * lf, nn = 0.75 - 1.27 * lf;
+        double expo;
+        if (rp != 0.0) {
+          const double lr = log10(rp);
+          const double x = (lr + cc) / (nn - 0.14 * (lr + cc));
+          expo = 1.0 / (1.0 + x * x);
+        } else {
+          expo = -1.0 / 0.14;
+        }
+        k = k * exp(expo * lnFc);
+      }
+    }
+    double kr = 0.0;
+    if (type < 5) kr = k * exp(d_h * rRT - d_s / RG - c_mech.dnu[r] * ln_conc_ref);
     c.kf(r) = m_left ? k * mc : k;
     c.kr(r) = m_right ? kr * mc : kr;
   }
@@ -451,6 +531,27 @@ __device__ __forceinline__ double ratio_pow(double x, double p) {
   return npow(x, p);
 }
 
+// Division in the step-size and order control of DDSTP.  Reference mode: the
+// correctly rounded division (out of line).  Analytic-Jacobian and mixed
+// modes: inline, from the hardware reciprocal approximation refined by one
+// Newton step and one correction of the quotient (within an ulp or two);
+// these quotients only steer step sizes and orders.  Divisors that are zero,
+// not finite or outside [1e-300, 1e300] take the correctly rounded path.
+template <int JAC>
+__device__ __forceinline__ double sdiv(double a, double b) {
+  if constexpr (JAC != kJacFD) {
+    const double ab = fabs(b);
+    if (ab > 1e-300 && ab < 1e300) {
+      double r;
+      asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(b));
+      r = fma(r, fma(-b, r, 1.0), r);
+      const double q = a * r;
+      return fma(r, fma(-b, q, a), q);
+    }
+  }
+  return ddiv(a, b);
+}
+
 // sqrt by Newton's iteration at compile time (constant scale factors).
 __host__ __device__ constexpr double ct_sqrt(double x, double g = 1.0, int it = 0) {
   return it == 64 ? g : ct_sqrt(x, 0.5 * (g + x / g), it + 1);
@@ -514,13 +615,25 @@ __device__ __forceinline__ double weighted_norm(const CS& c, const double (&x)[N
 // that dgesl<RECIP> multiplies where the reference divides; used by the
 // analytic-Jacobian and mixed modes, whose results agree with the reference's
 // to its tolerance, not bit for bit.
+// x + t * y of the elimination.  The analytic-Jacobian modes (RECIP) with
+// double factors fuse it into one FMA; the reference mode keeps the
+// reference's separately rounded multiply and add.
+template <typename LUT, bool RECIP>
+__device__ __forceinline__ LUT lu_axpy(LUT x, LUT t, LUT y) {
+  if constexpr (RECIP && std::is_same<LUT, double>::value) return fma(t, y, x);
+  else return x + t * y;
+}
+
 template <int N, bool RECIP, class CS>
 __device__ __forceinline__ int dgefa(CS& c, RowPerm<N>* perm_out) {
   using LUT = typename std::remove_reference<decltype(c.a(0, 0))>::type;
   int info = 0;
   RowPerm<N> perm;
   perm.identity();
-#pragma unroll 1
+  // up to 9 integrated species the elimination is unrolled: every index but
+  // the pivot row is a compile-time constant and the updates of the columns
+  // right of the pivot are independent instructions
+#pragma unroll(N <= 9 ? N : 1)
   for (int k = 0; k < N - 1; ++k) {
     int l = k;
     LUT dmax = fabs(c.a(k, k));
@@ -552,7 +665,7 @@ __device__ __forceinline__ int dgefa(CS& c, RowPerm<N>* perm_out) {
         c.a(j, k) = tj;
       }
       if (tj != (LUT)0)
-        for (int i = k + 1; i < N; ++i) c.a(j, i) = c.a(j, i) + tj * c.a(k, i);
+        for (int i = k + 1; i < N; ++i) c.a(j, i) = lu_axpy<LUT, RECIP>(c.a(j, i), tj, c.a(k, i));
     }
   }
   *perm_out = perm;
@@ -627,12 +740,13 @@ __device__ __noinline__ RowPerm<N> nl_dgefa(double* d, LUT* f, int* info) {
   return perm;
 }
 
-template <int N, int R, typename LUT, int BS>
+template <int N, int R, typename LUT, int BS, bool FAST>
 __device__ __noinline__ void nl_rate_constants(double* d, LUT* f, double T) {
   SmemStore<N, R, LUT, BS> s;
   s.d = d;
   s.f = f;
-  rate_constants<N, R>(s, T);
+  if constexpr (FAST) rate_constants_fast<N, R>(s, T);
+  else rate_constants<N, R>(s, T);
 }
 
 // --------------------------------------------------------- SLATEC pieces
@@ -642,7 +756,9 @@ __device__ __noinline__ void nl_rate_constants(double* d, LUT* f, double T) {
 // reference's additions in the reference's order, and is stored once.
 template <int N, int Q, class S>
 __device__ __forceinline__ void ddpsc_order(S& c, int ksgn) {
-#pragma unroll 1
+  // species are independent: up to 9 of them are unrolled, so that their
+  // addition chains overlap
+#pragma unroll(N <= 9 ? N : 1)
   for (int i = 0; i < N; ++i) {
     double v[Q + 1];
 #pragma unroll
@@ -682,7 +798,7 @@ __device__ __forceinline__ void ddpsc(int ksgn, CS& c) {
 
 // ddscl.f90:20-37: limits rh, rescales columns 1..nq of the Nordsieck array;
 // returns the rh applied.
-template <int N, int R, typename LUT, int BS>
+template <int N, int R, typename LUT, int BS, int JAC>
 __device__ __noinline__ double nl_ddscl(double* d, LUT* f, int nq, double h, double rmax, double rh) {
   SmemStore<N, R, LUT, BS> c;
   c.d = d;
@@ -690,9 +806,9 @@ __device__ __noinline__ double nl_ddscl(double* d, LUT* f, int nq, double h, dou
   const double hmax = c_mech.hmax;
   if (h < 1.0) {
     const double ah = fabs(h);
-    rh = ddiv(NRG_FMIN(NRG_FMIN(ah * rh, ah * rmax), hmax), ah);
+    rh = sdiv<JAC>(NRG_FMIN(NRG_FMIN(ah * rh, ah * rmax), hmax), ah);
   } else {
-    rh = NRG_FMIN(NRG_FMIN(rh, rmax), ddiv(hmax, fabs(h)));
+    rh = NRG_FMIN(NRG_FMIN(rh, rmax), sdiv<JAC>(hmax, fabs(h)));
   }
   double r1 = 1.0;
   for (int j = 1; j <= nq; ++j) {
@@ -703,9 +819,9 @@ __device__ __noinline__ double nl_ddscl(double* d, LUT* f, int nq, double h, dou
   return rh;
 }
 
-template <int N, class CS>
+template <int N, int JAC, class CS>
 __device__ __forceinline__ void ddscl(CS& c, double rh) {
-  rh = nl_ddscl<N, CS::kR, typename CS::lut_t, CS::kBS>(c.d, c.f, c.nq, c.h, c.rmax, rh);
+  rh = nl_ddscl<N, CS::kR, typename CS::lut_t, CS::kBS, JAC>(c.d, c.f, c.nq, c.h, c.rmax, rh);
   c.h = c.h * rh;
   c.rc = c.rc * rh;
 }
@@ -862,7 +978,7 @@ L110:
   for (int i = 0; i < N; ++i) c.s1[i] = 0.0;
 L130:
   d = ddcor<N, R, JAC, LUT>(c);
-  if (iter > 0) c.trend = NRG_FMAX(0.9 * c.trend, ddiv(d, d1));
+  if (iter > 0) c.trend = NRG_FMAX(0.9 * c.trend, sdiv<JAC>(d, d1));
   d1 = d;
   ctest = NRG_FMIN(2.0 * c.trend, 1.0) * d;
   if (ctest <= eps) goto L170;
@@ -884,29 +1000,29 @@ L160:
   ddpsc<N>(-1, c);
   c.nwait = c.nq + 2;
   if (c.jtask != 0 && c.jtask != 2) c.rmax = RMFAIL;
-  rh = (iter == 0) ? 0.3 : 0.9 * ratio_pow<JAC>(ddiv(eps, ctest), 0.2);
+  rh = (iter == 0) ? 0.3 : 0.9 * ratio_pow<JAC>(sdiv<JAC>(eps, ctest), 0.2);
   if (rh * c.h == 0.0) goto L400;
-  ddscl<N>(c, rh);
+  ddscl<N, JAC>(c, rh);
   goto L100;
 L170:
   c.convrg = 1;
-  etest = ddiv(weighted_norm<N, JAC>(c, c.s1), TQ(2, c.nq) * sqn);
+  etest = sdiv<JAC>(weighted_norm<N, JAC>(c, c.s1), TQ(2, c.nq) * sqn);
   if (etest > eps) {
     c.t = told;
     ddpsc<N>(-1, c);
     nfail = nfail + 1;
     if (nfail < MXFAIL || c.nq == 1) {
       if (c.jtask != 0 && c.jtask != 2) c.rmax = RMFAIL;
-      const double rh2 = ddiv(1.0, BIAS2 * ratio_pow<JAC>(ddiv(etest, eps), ddiv(1.0, (double)(c.nq + 1))));
+      const double rh2 = sdiv<JAC>(1.0, BIAS2 * ratio_pow<JAC>(sdiv<JAC>(etest, eps), sdiv<JAC>(1.0, (double)(c.nq + 1))));
       if (c.nq > 1) {
         double v[N];
 #pragma unroll
         for (int i = 0; i < N; ++i) v[i] = c.yh(c.nq, i);
-        const double erdn = ddiv(weighted_norm<N, JAC>(c, v), TQ(1, c.nq) * sqn);
-        const double rh1 = ddiv(1.0, NRG_FMAX(1.0, BIAS1 * ratio_pow<JAC>(ddiv(erdn, eps), ddiv(1.0, (double)c.nq))));
+        const double erdn = sdiv<JAC>(weighted_norm<N, JAC>(c, v), TQ(1, c.nq) * sqn);
+        const double rh1 = sdiv<JAC>(1.0, NRG_FMAX(1.0, BIAS1 * ratio_pow<JAC>(sdiv<JAC>(erdn, eps), sdiv<JAC>(1.0, (double)c.nq))));
         if (rh2 < rh1) {
           c.nq = c.nq - 1;
-          c.rc = ddiv(c.rc * EL(1, c.nq), EL(1, c.nq + 1));
+          c.rc = sdiv<JAC>(c.rc * EL(1, c.nq), EL(1, c.nq + 1));
           rh = rh1;
         } else {
           rh = rh2;
@@ -916,7 +1032,7 @@ L170:
       }
       c.nwait = c.nq + 2;
       if (rh * c.h == 0.0) goto L400;
-      ddscl<N>(c, rh);
+      ddscl<N, JAC>(c, rh);
       goto L100;
     }
     nfail = 0;
@@ -935,8 +1051,8 @@ L170:
 #pragma unroll
   for (int i = 0; i < N; ++i) c.y[i] = c.yh(0, i);
   if (c.jtask == 0 || c.jtask == 2) {
-    rh = ddiv(1.0, NRG_FMAX(uround, BIAS2 * ratio_pow<JAC>(ddiv(etest, eps), ddiv(1.0, (double)(c.nq + 1)))));
-    if (rh > TRSHLD) ddscl<N>(c, rh);
+    rh = sdiv<JAC>(1.0, NRG_FMAX(uround, BIAS2 * ratio_pow<JAC>(sdiv<JAC>(etest, eps), sdiv<JAC>(1.0, (double)(c.nq + 1)))));
+    if (rh > TRSHLD) ddscl<N, JAC>(c, rh);
   } else if (c.nwait > 1) {
     c.nwait = c.nwait - 1;
     if (c.nwait == 1 && c.nq < kMaxOrd) {
@@ -951,24 +1067,24 @@ L170:
       double v[N];
 #pragma unroll
       for (int i = 0; i < N; ++i) v[i] = c.yh(c.nq, i);
-      const double erdn = ddiv(weighted_norm<N, JAC>(c, v), TQ(1, c.nq) * sqn);
-      rh1 = ddiv(1.0, NRG_FMAX(uround, BIAS1 * ratio_pow<JAC>(ddiv(erdn, eps), ddiv(1.0, (double)c.nq))));
+      const double erdn = sdiv<JAC>(weighted_norm<N, JAC>(c, v), TQ(1, c.nq) * sqn);
+      rh1 = sdiv<JAC>(1.0, NRG_FMAX(uround, BIAS1 * ratio_pow<JAC>(sdiv<JAC>(erdn, eps), sdiv<JAC>(1.0, (double)c.nq))));
     }
-    rh2 = ddiv(1.0, NRG_FMAX(uround, BIAS2 * ratio_pow<JAC>(ddiv(etest, eps), ddiv(1.0, (double)(c.nq + 1)))));
+    rh2 = sdiv<JAC>(1.0, NRG_FMAX(uround, BIAS2 * ratio_pow<JAC>(sdiv<JAC>(etest, eps), sdiv<JAC>(1.0, (double)(c.nq + 1)))));
     if (c.nq == kMaxOrd) {
       rh3 = 0.0;
     } else {
       double v[N];
 #pragma unroll
       for (int i = 0; i < N; ++i) v[i] = c.s1[i] - c.yh(kMaxOrd, i);
-      const double erup = ddiv(weighted_norm<N, JAC>(c, v), TQ(3, c.nq) * sqn);
-      rh3 = ddiv(1.0, NRG_FMAX(uround, BIAS3 * ratio_pow<JAC>(ddiv(erup, eps), ddiv(1.0, (double)(c.nq + 2)))));
+      const double erup = sdiv<JAC>(weighted_norm<N, JAC>(c, v), TQ(3, c.nq) * sqn);
+      rh3 = sdiv<JAC>(1.0, NRG_FMAX(uround, BIAS3 * ratio_pow<JAC>(sdiv<JAC>(erup, eps), sdiv<JAC>(1.0, (double)(c.nq + 2)))));
     }
     if (rh1 > rh2 && rh1 >= rh3) {
       rh = rh1;
       if (rh <= TRSHLD) goto L380;
       c.nq = c.nq - 1;
-      c.rc = ddiv(c.rc * EL(1, c.nq), EL(1, c.nq + 1));
+      c.rc = sdiv<JAC>(c.rc * EL(1, c.nq), EL(1, c.nq + 1));
     } else if (rh2 >= rh1 && rh2 >= rh3) {
       rh = rh2;
       if (rh <= TRSHLD) goto L380;
@@ -977,11 +1093,11 @@ L170:
       if (rh <= TRSHLD) goto L380;
       const double e = EL(c.nq + 1, c.nq);
 #pragma unroll
-      for (int i = 0; i < N; ++i) c.yh(c.nq + 1, i) = ddiv(c.s1[i] * e, (double)(c.nq + 1));
+      for (int i = 0; i < N; ++i) c.yh(c.nq + 1, i) = sdiv<JAC>(c.s1[i] * e, (double)(c.nq + 1));
       c.nq = c.nq + 1;
-      c.rc = ddiv(c.rc * EL(1, c.nq), EL(1, c.nq - 1));
+      c.rc = sdiv<JAC>(c.rc * EL(1, c.nq), EL(1, c.nq - 1));
     }
-    ddscl<N>(c, rh);
+    ddscl<N, JAC>(c, rh);
     c.rmax = RMNORM;
   L380:
     c.nwait = c.nq + 2;
@@ -1008,7 +1124,7 @@ L420:
 // Cell set-up: skip rule (chemical_kinetics_solver.f90:228-231), third-body
 // sums (:238-248), rate constants (:251), DDRIV3 init (ddriv3.f90:930-978).
 // Returns false when the cell is passed through (outputs already written).
-template <int N, int R, class CS>
+template <int N, int R, int JAC, class CS>
 __device__ bool cell_begin(CS& c, const StepArgs& a, long cid) {
   constexpr int NF = CS::kNF;
   const double Tc = a.T[cid];
@@ -1017,17 +1133,20 @@ __device__ bool cell_begin(CS& c, const StepArgs& a, long cid) {
     return false;
   }
   const double rho = a.rho[cid];
-  double yk[NF];
+  double yk[NF], conc[NF];
 #pragma unroll
-  for (int k = 0; k < NF; ++k) yk[k] = a.Y[k * a.ld + cid];
+  for (int k = 0; k < NF; ++k) {
+    yk[k] = a.Y[k * a.ld + cid];
+    conc[k] = yk[k] * rho / c_mech.W[k];  // the reference's Y*rho/W, formed once
+  }
 #pragma unroll 1
   for (int r = 0; r < R; ++r) {
     double s = 0.0;
 #pragma unroll
-    for (int k = 0; k < NF; ++k) s = s + yk[k] * rho / c_mech.W[k] * c_mech.eff_t[k][r];
+    for (int k = 0; k < NF; ++k) s = s + conc[k] * c_mech.eff_t[k][r];
     c.kr(r) = s;  // third-body sum, consumed by rate_constants
   }
-  nl_rate_constants<N, R, typename CS::lut_t, CS::kBS>(c.d, c.f, Tc);
+  nl_rate_constants<N, R, typename CS::lut_t, CS::kBS, JAC != kJacFD>(c.d, c.f, Tc);
   if (NF == N) {
 #pragma unroll
     for (int k = 0; k < N; ++k) {
@@ -1105,7 +1224,7 @@ __device__ int cell_advance(CS& c, int mxstep) {
   if (c.t < c.tout) return 0;
 #pragma unroll
   for (int i = 0; i < N; ++i) c.y[i] = c.yh(c.nq, i);
-  const double r = ddiv(c.tout - c.t, c.h);
+  const double r = sdiv<JAC>(c.tout - c.t, c.h);
   for (int jj = 1; jj <= c.nq; ++jj) {
     const int j = c.nq - jj;
 #pragma unroll
@@ -1184,9 +1303,68 @@ __device__ __forceinline__ double temperature_after(double T0, const double (&Y0
   return temperature_after<N>(T0, Y0, dY, dE, T0);
 }
 
+// The same energy closure for the analytic-Jacobian and mixed modes, whose
+// temperatures agree with the reference's to its tolerance rather than bit
+// for bit: unrolled over the species in registers, with the reciprocal molar
+// masses and one reciprocal of the frozen cp, inline (it runs once per cell,
+// after the integration, when the integrator's registers are free).
+__device__ __forceinline__ double nasa_enthalpy_fast(int k, double T) {
+  const double t = NRG_FMIN(T, 6000.0);
+  const double* a = c_mech.a[k][nasa_set(t)];
+  const double hp = fma(fma(fma(fma(a[4] * 0.2, t, a[3] * 0.25), t, a[2] * (1.0 / 3.0)), t, a[1] * 0.5), t, a[0]);
+  return fma(hp, t, a[5]);
+}
+
+template <int N>
+__device__ __forceinline__ double temperature_after_fast(double T0, const double (&Y0)[N], const double (&dY)[N],
+                                                         double dE) {
+  const double RG = 8.31446261815324;
+  double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+  for (int k = 0; k < N; ++k) s0 += Y0[k] * c_mech.invW[k];
+  const double W0 = 1.0 / s0;
+  double e0 = 0.0, h0 = 0.0;
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    const double x = Y0[k] * c_mech.invW[k] * W0;
+    e0 += nasa_enthalpy_fast(k, T0) * x;
+    h0 += c_mech.h_ref[k] * x;
+  }
+  e0 -= RG * T0;
+  const double e1 = (e0 - h0) / W0 + dE;
+  double X[N];
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    X[k] = Y0[k] + dY[k];
+    s1 += X[k] * c_mech.invW[k];
+  }
+  const double W1 = 1.0 / s1;
+  double hc = 0.0, cp = 0.0;
+  double temp = NRG_FMIN(T0, 6000.0);
+  const int set = nasa_set(temp);
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    X[k] = X[k] * c_mech.invW[k] * W1;
+    hc += c_mech.h_ref[k] * X[k];
+    const double* a = c_mech.a[k][set];
+    cp += fma(fma(fma(fma(a[4], temp, a[3]), temp, a[2]), temp, a[1]), temp, a[0]) * X[k];
+  }
+  const double ei = e1 * W1, rcp = 1.0 / cp;
+  for (int it = 0; it < 1000; ++it) {
+    double e = 0.0;
+#pragma unroll
+    for (int k = 0; k < N; ++k) e += nasa_enthalpy_fast(k, temp) * X[k];
+    e -= RG * temp;
+    const double res = (ei - (e - hc)) * rcp;
+    temp += res;
+    if (fabs(res) < (double)1e-08f) break;
+  }
+  return temp;
+}
+
 // Outputs of a finished cell (chemical_kinetics_solver.f90:318-340); inert
 // species keep their concentration, so their sources are exactly zero.
-template <int N, class CS>
+template <int N, int JAC, class CS>
 __device__ void cell_finish(const CS& c, const StepArgs& a, long cid, int st) {
   constexpr int NF = CS::kNF;
   const double dt = c.tout;
@@ -1219,7 +1397,10 @@ __device__ void cell_finish(const CS& c, const StepArgs& a, long cid, int st) {
     dYm[k] = yp * dt / rho;
   }
   a.E_f_prod[cid] = E;
-  if (a.T_after) a.T_after[cid] = temperature_after<NF>(a.T[cid], Y0, dYm, E * dt / rho);
+  if (a.T_after) {
+    if constexpr (JAC == kJacFD) a.T_after[cid] = temperature_after<NF>(a.T[cid], Y0, dYm, E * dt / rho);
+    else a.T_after[cid] = temperature_after_fast<NF>(a.T[cid], Y0, dYm, E * dt / rho);
+  }
   if (a.status) a.status[cid] = finite ? (uint8_t)st : (uint8_t)kCellNonfinite;
 }
 

@@ -49,11 +49,11 @@ __global__ void __launch_bounds__(BS, 1) k_chem_plain(StepArgs a, unsigned long 
   CellState<N, R, LUT, BS, NF, SPEC> c;
   c.bind(smem, threadIdx.x);
   if (li < nl) {
-    if (cell_begin<N, R>(c, a, cid)) {
+    if (cell_begin<N, R, JAC>(c, a, cid)) {
       int st;
       while ((st = cell_advance<N, R, JAC, LUT>(c, a.mxstep)) == 0) {
       }
-      cell_finish<N>(c, a, cid, st);
+      cell_finish<N, JAC>(c, a, cid, st);
       v[kCntCells] = 1;
       v[kCntSteps] = c.nstep;
       v[kCntRhs] = c.nfe;
@@ -91,12 +91,12 @@ __global__ void __launch_bounds__(BS, 1) k_chem_queue(StepArgs a, int* queue, in
       --left;
       if (cur >= nl) break;
       cid = a.cell_list ? (long)a.cell_list[cur] : cur;
-      have = cell_begin<N, R>(c, a, cid);
+      have = cell_begin<N, R, JAC>(c, a, cid);
       if (!have) continue;
     }
     const int st = cell_advance<N, R, JAC, LUT>(c, a.mxstep);
     if (st) {
-      cell_finish<N>(c, a, cid, st);
+      cell_finish<N, JAC>(c, a, cid, st);
       v[kCntCells] += 1;
       v[kCntSteps] += c.nstep;
       v[kCntRhs] += c.nfe;
