@@ -542,7 +542,7 @@ def main():
         dist.init("nccl", timeout_s=600)
     from nrg_b200 import eact_units, fields as F, keromnes_paths, mechanism_paths
     from nrg_b200.chemistry import ChemicalKineticsSolver, DataManager, fp64_peak_tflops, mechanism_tables
-    from nrg_b200.surrogate import DEFAULT_MODEL, RECIPE, Surrogate, train_default
+    from nrg_b200.surrogate import DEFAULT_MODEL, PREHEAT_MODEL, RECIPE, Surrogate, load_default, train_default
     decks = mechanism_paths(args.mechanism)
     units = eact_units(args.mechanism)
     tables = mechanism_tables(*decks, 1.0, units)
@@ -592,13 +592,16 @@ def main():
         mode = "fast"
     train_info = None
     if mode in ("auto", "surrogate"):
-        sur = Surrogate(solver)
         if os.path.exists(DEFAULT_MODEL):
-            sur.load(DEFAULT_MODEL)
-            sur.set_gate(*RECIPE["gate"])
+            nets = load_default(solver)
             train_info = {"model": os.path.relpath(DEFAULT_MODEL, ROOT), "trained": "loaded",
                           "gate": list(RECIPE["gate"])}
+            if len(nets) > 1:
+                from nrg_b200.surrogate import RECIPE_PREHEAT
+                train_info["preheat_model"] = os.path.relpath(PREHEAT_MODEL, ROOT)
+                train_info["preheat_gate"] = list(RECIPE_PREHEAT["gate"])
         else:
+            sur = Surrogate(solver)
             info = train_default(solver, W)
             sur.save(DEFAULT_MODEL)
             train_info = {"trained": "in this run", "pairs": info["n"], "epochs": info["recipe"]["epochs"],
@@ -728,9 +731,7 @@ def main():
         host.set_launch(**launch)
         host.set_cell_order(args.cell_order == "temperature")
         if mode == "surrogate":
-            hs = Surrogate(host)
-            hs.load(DEFAULT_MODEL)
-            hs.set_gate(*RECIPE["gate"])
+            load_default(host)
         if mode == "table":
             host.read_chemical_kinetics_table(table_path)
         host.set_mode(mode)

@@ -342,6 +342,15 @@ NRG_API const char* nrg_chem_last_error(nrg_chem* h);
  * features, y arrays n x 10 fp32 standardised targets (device memory). */
 NRG_API int nrg_surrogate_param_count(void);
 NRG_API int nrg_surrogate_norm_count(void);
+/* A handle holds two networks: 0, the main one (its training hull starts at
+ * 800 K), and 1, an optional one for a flame's preheat band.  A surrogate
+ * step needs network 0; each active cell goes to network 0 from the bottom of
+ * that network's hull up, to network 1 (when enabled) between the bottom of
+ * its own hull and there, and to the FP64 integrator otherwise; each network
+ * has its own standardisation and gate settings.  The set-up calls below
+ * (init, parameters, norm, training, gate, enable, save, load, inference)
+ * act on the network selected here (0 by default). */
+NRG_API int nrg_surrogate_select(nrg_chem* h, int net);
 NRG_API int nrg_surrogate_init(nrg_chem* h, unsigned long long seed);
 NRG_API int nrg_surrogate_get_params(nrg_chem* h, float* params);
 NRG_API int nrg_surrogate_set_params(nrg_chem* h, const float* params);

@@ -94,6 +94,7 @@ SIGNATURES = {
     "nrg_chem_last_error": (ctypes.c_char_p, [_VP]),
     "nrg_surrogate_param_count": (_I, []),
     "nrg_surrogate_norm_count": (_I, []),
+    "nrg_surrogate_select": (_I, [_VP, _I]),
     "nrg_surrogate_init": (_I, [_VP, ctypes.c_ulonglong]),
     "nrg_surrogate_get_params": (_I, [_VP, _VP]),
     "nrg_surrogate_set_params": (_I, [_VP, _VP]),

@@ -74,8 +74,11 @@ struct nrg_chem {
   double *d_tab_T = nullptr, *d_tab_Y = nullptr;
   long tab_rows = 0;
   bool tab_sorted = false;
-  // surrogate state (owned by surrogate.cu)
-  nrg::Surrogate* sur = nullptr;
+  // surrogate state (owned by surrogate.cu): the main network and a second
+  // one for the flame's preheat band; the nrg_surrogate_* set-up calls act on
+  // network sur_sel (nrg_surrogate_select)
+  nrg::Surrogate* sur_net[2] = {nullptr, nullptr};
+  int sur_sel = 0;
   std::string err;
 };
 
@@ -353,7 +356,7 @@ cudaError_t enqueue_step_body(nrg_chem* h, const StepArgs& a, cudaStream_t s, cu
     return e;
   }
   if (h->mode == NRG_MODE_SURROGATE)
-    return nrg::surrogate_step(h->sur, a, h->cfg, h->d_queue, h->d_counters, s,
+    return nrg::surrogate_step(h->sur_net[0], h->sur_net[1], a, h->cfg, h->d_queue, h->d_counters, s,
                                [h, ph](const StepArgs& fa, cudaStream_t fs) {
                                  if (ph) cudaEventRecord(ph[2], fs);
                                  LaunchCfg c = h->cfg;
@@ -428,9 +431,9 @@ int step_prepare(nrg_chem* h, long n) {
   if (h->mode == NRG_MODE_SURROGATE) {
     if (!(h->mech.n() == 9 && h->mech.r() == 24))
       return fail(h, NRG_ERR_UNSUPPORTED, "the surrogate is built for the 9-species, 24-reaction mechanism");
-    if (!nrg::surrogate_ready(h->sur))
+    if (!nrg::surrogate_ready(h->sur_net[0]))
       return fail(h, NRG_ERR_STATE, "surrogate mode selected but no trained model is loaded");
-    const std::string e = nrg::surrogate_reserve(h->sur, n);
+    const std::string e = nrg::surrogate_reserve(h->sur_net[0], n);
     if (!e.empty()) return fail(h, NRG_ERR_CUDA, e);
   }
   return NRG_OK;
@@ -470,7 +473,8 @@ int step_finish(nrg_chem* h, cudaStream_t s, long n, nrg_chem_stats* stats) {
     }
   }
   if (h->mode == NRG_MODE_SURROGATE) {
-    const std::string e = nrg::surrogate_check(h->sur, s);
+    std::string e = nrg::surrogate_check(h->sur_net[0], s);
+    if (e.empty()) e = nrg::surrogate_check(h->sur_net[1], s);
     if (!e.empty()) return fail(h, NRG_ERR_CUDA, e);
   }
   return NRG_OK;
@@ -555,7 +559,8 @@ extern "C" int nrg_chem_create(const char* mechanism_path, const char* thermo_pa
   }
   reduce_dev_mech(h->dm, &h->dmr);
   h->spec = nrg::match_specialised(h->dmr);
-  h->sur = nrg::surrogate_create(h->dm);
+  h->sur_net[0] = nrg::surrogate_create(h->dm);
+  h->sur_net[1] = nrg::surrogate_create(h->dm);
   if ((ce = use_tables(h)) != cudaSuccess) {
     std::string msg = std::string("mechanism upload failed: ") + cudaGetErrorString(ce);
     nrg_chem_destroy(h);
@@ -576,7 +581,8 @@ extern "C" int nrg_chem_destroy(nrg_chem* h) {
   device_scope.enter(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
-  nrg::surrogate_destroy(h->sur);
+  nrg::surrogate_destroy(h->sur_net[0]);
+  nrg::surrogate_destroy(h->sur_net[1]);
   cudaFree(h->d_tab_T);
   cudaFree(h->d_tab_Y);
   free_staging(h);
@@ -650,7 +656,7 @@ extern "C" int nrg_chem_set_graph(nrg_chem* h, int enable) {
 extern "C" int nrg_chem_set_cell_order(nrg_chem* h, int enable) {
   if (!h) return NRG_ERR_ARG;
   h->order_cells = enable != 0;
-  if (h->sur) nrg::surrogate_set_cell_order(h->sur, h->order_cells);
+  if (h->sur_net[0]) nrg::surrogate_set_cell_order(h->sur_net[0], h->order_cells);
   return NRG_OK;
 }
 
@@ -1250,37 +1256,44 @@ nrg::MlpNorm floats_to_norm(const float* f) {
 }  // namespace
 
 extern "C" int nrg_surrogate_param_count(void) { return nrg::surrogate_param_count(); }
+
+extern "C" int nrg_surrogate_select(nrg_chem* h, int net) {
+  if (!h) return NRG_ERR_ARG;
+  if (net < 0 || net > 1) return fail(h, NRG_ERR_ARG, "network index must be 0 (main) or 1 (preheat band)");
+  h->sur_sel = net;
+  return NRG_OK;
+}
 extern "C" int nrg_surrogate_norm_count(void) { return kNormFloats; }
 
 extern "C" int nrg_surrogate_init(nrg_chem* h, unsigned long long seed) {
   if (!h) return NRG_ERR_ARG;
   ON_DEVICE(h);
   CK(h, use_tables(h));
-  return sfail(h, nrg::surrogate_init(h->sur, seed, h->stream));
+  return sfail(h, nrg::surrogate_init(h->sur_net[h->sur_sel], seed, h->stream));
 }
 
 extern "C" int nrg_surrogate_get_params(nrg_chem* h, float* params) {
   if (!h || !params) return NRG_ERR_ARG;
   ON_DEVICE(h);
-  return sfail(h, nrg::surrogate_get_params(h->sur, params, h->stream));
+  return sfail(h, nrg::surrogate_get_params(h->sur_net[h->sur_sel], params, h->stream));
 }
 
 extern "C" int nrg_surrogate_set_params(nrg_chem* h, const float* params) {
   if (!h || !params) return NRG_ERR_ARG;
   ON_DEVICE(h);
-  return sfail(h, nrg::surrogate_set_params(h->sur, params, h->stream));
+  return sfail(h, nrg::surrogate_set_params(h->sur_net[h->sur_sel], params, h->stream));
 }
 
 extern "C" int nrg_surrogate_get_norm(nrg_chem* h, float* norm) {
   if (!h || !norm) return NRG_ERR_ARG;
-  norm_to_floats(nrg::surrogate_get_norm(h->sur), norm);
+  norm_to_floats(nrg::surrogate_get_norm(h->sur_net[h->sur_sel]), norm);
   return NRG_OK;
 }
 
 extern "C" int nrg_surrogate_set_norm(nrg_chem* h, const float* norm) {
   if (!h || !norm) return NRG_ERR_ARG;
   ON_DEVICE(h);
-  return sfail(h, nrg::surrogate_set_norm(h->sur, floats_to_norm(norm)));
+  return sfail(h, nrg::surrogate_set_norm(h->sur_net[h->sur_sel], floats_to_norm(norm)));
 }
 
 extern "C" int nrg_surrogate_prepare(nrg_chem* h, long n, long ld, double dt, const double* dt_cells,
@@ -1296,7 +1309,7 @@ extern "C" int nrg_surrogate_prepare(nrg_chem* h, long n, long ld, double dt, co
   int rc = order_after_legacy(h);
   if (rc) return rc;
   const nrg::PrepareOpts o{opts->hull_margin, opts->dt_pow, opts->log_mask, opts->log_eps, opts->common_dY_scale};
-  return sfail(h, nrg::surrogate_prepare(h->sur, n, ld, dt, dt_cells, T, rho, Y, Y_prod, T_after, o,
+  return sfail(h, nrg::surrogate_prepare(h->sur_net[h->sur_sel], n, ld, dt, dt_cells, T, rho, Y, Y_prod, T_after, o,
                                          (__nv_bfloat16*)x_bf16, y, h->stream));
 }
 
@@ -1308,7 +1321,7 @@ extern "C" int nrg_surrogate_features(nrg_chem* h, long n, long ld, double dt, c
   CK(h, use_tables(h));
   int rc = order_after_legacy(h);
   if (rc) return rc;
-  std::string e = nrg::surrogate_features(h->sur, n, ld, dt, dt_cells, T, rho, Y, xraw, (__nv_bfloat16*)x_bf16,
+  std::string e = nrg::surrogate_features(h->sur_net[h->sur_sel], n, ld, dt, dt_cells, T, rho, Y, xraw, (__nv_bfloat16*)x_bf16,
                                           h->stream);
   if (!e.empty()) return sfail(h, e);
   CK(h, cudaStreamSynchronize(h->stream));
@@ -1321,7 +1334,7 @@ extern "C" int nrg_surrogate_forward(nrg_chem* h, long n, const void* x_bf16, fl
   CK(h, use_tables(h));
   int rc = order_after_legacy(h);
   if (rc) return rc;
-  return sfail(h, nrg::surrogate_forward(h->sur, n, (const __nv_bfloat16*)x_bf16, out, h->stream));
+  return sfail(h, nrg::surrogate_forward(h->sur_net[h->sur_sel], n, (const __nv_bfloat16*)x_bf16, out, h->stream));
 }
 
 extern "C" int nrg_surrogate_grad(nrg_chem* h, long n, const void* x_bf16, const float* y, float* grads_host,
@@ -1331,7 +1344,7 @@ extern "C" int nrg_surrogate_grad(nrg_chem* h, long n, const void* x_bf16, const
   CK(h, use_tables(h));
   int rc = order_after_legacy(h);
   if (rc) return rc;
-  return sfail(h, nrg::surrogate_grad(h->sur, n, (const __nv_bfloat16*)x_bf16, y, grads_host, loss_host, h->stream));
+  return sfail(h, nrg::surrogate_grad(h->sur_net[h->sur_sel], n, (const __nv_bfloat16*)x_bf16, y, grads_host, loss_host, h->stream));
 }
 
 extern "C" int nrg_surrogate_train(nrg_chem* h, long n, const void* x_bf16, const float* y, int epochs, int batch,
@@ -1341,26 +1354,26 @@ extern "C" int nrg_surrogate_train(nrg_chem* h, long n, const void* x_bf16, cons
   CK(h, use_tables(h));
   int rc = order_after_legacy(h);
   if (rc) return rc;
-  return sfail(h, nrg::surrogate_train(h->sur, n, (const __nv_bfloat16*)x_bf16, y, epochs, batch, lr, seed,
+  return sfail(h, nrg::surrogate_train(h->sur_net[h->sur_sel], n, (const __nv_bfloat16*)x_bf16, y, epochs, batch, lr, seed,
                                        loss_per_epoch, h->stream));
 }
 
 extern "C" int nrg_surrogate_set_gate(nrg_chem* h, double elem_tol, double raw_elem_tol, double dT_tol,
                                       double dT_max) {
   if (!h || !(elem_tol >= 0) || !(raw_elem_tol >= 0) || !(dT_tol >= 0) || !(dT_max >= 0)) return NRG_ERR_ARG;
-  nrg::surrogate_set_gate(h->sur, elem_tol, raw_elem_tol, dT_tol, dT_max);
+  nrg::surrogate_set_gate(h->sur_net[h->sur_sel], elem_tol, raw_elem_tol, dT_tol, dT_max);
   return NRG_OK;
 }
 
 extern "C" int nrg_surrogate_set_gate_dt(nrg_chem* h, double dt_max) {
   if (!h || !(dt_max > 0)) return NRG_ERR_ARG;
-  nrg::surrogate_set_gate_dt(h->sur, dt_max);
+  nrg::surrogate_set_gate_dt(h->sur_net[h->sur_sel], dt_max);
   return NRG_OK;
 }
 
 extern "C" int nrg_surrogate_set_inference(nrg_chem* h, int fused) {
   if (!h) return NRG_ERR_ARG;
-  nrg::surrogate_set_fused(h->sur, fused != 0);
+  nrg::surrogate_set_fused(h->sur_net[0], fused != 0);
   return NRG_OK;
 }
 
@@ -1375,12 +1388,12 @@ extern "C" int nrg_surrogate_infer(nrg_chem* h, long n, long ld, double dt, cons
   StepArgs a{};
   a.n = n; a.ld = ld; a.dt = dt > 0.0 ? dt : 1.0; a.dt_cells = dt_cells; a.T = T; a.rho = rho; a.Y = Y;
   a.mech = h->d_mech;
-  return sfail(h, nrg::surrogate_infer(h->sur, a, out, h->stream));
+  return sfail(h, nrg::surrogate_infer(h->sur_net[h->sur_sel], a, out, h->stream));
 }
 
 extern "C" int nrg_surrogate_enable(nrg_chem* h, int enable) {
   if (!h) return NRG_ERR_ARG;
-  nrg::surrogate_set_ready(h->sur, enable != 0);
+  nrg::surrogate_set_ready(h->sur_net[h->sur_sel], enable != 0);
   return NRG_OK;
 }
 
@@ -1390,7 +1403,7 @@ extern "C" int nrg_surrogate_save(nrg_chem* h, const char* path) {
   std::vector<float> p((size_t)P), nm(kNormFloats);
   int rc = nrg_surrogate_get_params(h, p.data());
   if (rc) return rc;
-  norm_to_floats(nrg::surrogate_get_norm(h->sur), nm.data());
+  norm_to_floats(nrg::surrogate_get_norm(h->sur_net[h->sur_sel]), nm.data());
   FILE* f = std::fopen(path, "wb");
   if (!f) return fail(h, NRG_ERR_IO, std::string("cannot write ") + path);
   const char magic[8] = {'N', 'R', 'G', 'S', 'U', 'R', '3', '\0'};
@@ -1418,7 +1431,7 @@ extern "C" int nrg_surrogate_load(nrg_chem* h, const char* path) {
   if (rc) return rc;
   rc = nrg_surrogate_set_norm(h, nm.data());
   if (rc) return rc;
-  nrg::surrogate_set_ready(h->sur, true);
+  nrg::surrogate_set_ready(h->sur_net[h->sur_sel], true);
   return NRG_OK;
 }
 

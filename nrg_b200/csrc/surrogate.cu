@@ -459,7 +459,28 @@ __device__ __forceinline__ void count_surrogate(unsigned long long n_sur, unsign
 
 // O: the network outputs of every active cell, output j of cell c at
 // O[j * o_ld + c] (o_ld > 0) or O[c * 16 + j] (o_ld == 0).
-__global__ void __launch_bounds__(128, 3) k_gate(StepArgs a, const float* O, long o_ld, const MlpNorm* nm, GateCfg gc,
+// The networks of one step: each answers the active cells whose temperature
+// lies in its routing band [lo, hi) (bands do not overlap) with its own
+// standardisation and gate settings.
+struct GateNet {
+  const MlpNorm* nm;
+  GateCfg gc;
+  double lo, hi;
+  int on;
+};
+constexpr int kMaxNets = 2;
+struct GateNets {
+  GateNet net[kMaxNets];
+};
+
+__device__ __forceinline__ int route_of(const GateNets& g, double T) {
+#pragma unroll
+  for (int i = 0; i < kMaxNets; ++i)
+    if (g.net[i].on && T >= g.net[i].lo && T < g.net[i].hi) return i;
+  return -1;
+}
+
+__global__ void __launch_bounds__(128, 3) k_gate(StepArgs a, const float* O, long o_ld, GateNets nets,
                                               unsigned char* flag, unsigned long long* counters) {
   __shared__ double P[9][9];
   __shared__ GateThermo th;
@@ -473,6 +494,11 @@ __global__ void __launch_bounds__(128, 3) k_gate(StepArgs a, const float* O, lon
       flag[c] = 0;
       continue;
     }
+    const int net = route_of(nets, T0);
+    if (net < 0) {  // no network for this temperature: FP64
+      flag[c] = 1;
+      continue;
+    }
     const double rho = a.rho[c];
     const double dt = a.dt_cells ? a.dt_cells[c] : a.dt;
     float f[kMlpIn], o[kMlpOut];
@@ -484,7 +510,7 @@ __global__ void __launch_bounds__(128, 3) k_gate(StepArgs a, const float* O, lon
     }
 #pragma unroll
     for (int j = 0; j < kMlpOut; ++j) o[j] = o_ld > 0 ? O[j * o_ld + c] : O[c * kMlpOutPad + j];
-    const bool acc = gate_active_cell(a, c, T0, rho, dt, f, o, nm, gc, P, th);
+    const bool acc = gate_active_cell(a, c, T0, rho, dt, f, o, nets.net[net].nm, nets.net[net].gc, P, th);
     n_sur += acc;
     flag[c] = acc ? 0 : 1;
   }
@@ -531,7 +557,8 @@ struct TcArgs {
   long offW[kMlpLayers], offb[kMlpLayers];
   float* out;    // network outputs (normalised units)
   long out_ld;   // > 0: output j of cell c at out[j * out_ld + c] (kMlpOut values); 0: out[c * 16 + j]
-  int active;    // 1: only the cells the step integrates (skip rule); 0: every cell
+  int active;    // 1: only the cells the step integrates (skip rule) whose T is in [route_lo, route_hi); 0: every cell
+  double route_lo, route_hi;
   unsigned int* err;  // bit 0: an MMA wait timed out
 };
 
@@ -614,7 +641,7 @@ __global__ void __launch_bounds__(128 * kTcGroups, 1) k_mlp_tc(TcArgs p) {
     for (int j = 0; j < kMlpIn; ++j) f[j] = 0.f;
     if (c < a.n) {
       const double T0 = a.T[c];
-      need = p.active ? reference_cell_active(T0, a.bc, c) : true;
+      need = p.active ? reference_cell_active(T0, a.bc, c) && T0 >= p.route_lo && T0 < p.route_hi : true;
       if (need) {
         double y0[9];
 #pragma unroll
@@ -1321,8 +1348,11 @@ std::string surrogate_reserve(Surrogate* s, long n) {
   return ensure_gate(s, n);
 }
 
-static TcArgs tc_args(Surrogate* s, const StepArgs& a, float* out, long out_ld, int active) {
+static TcArgs tc_args(Surrogate* s, const StepArgs& a, float* out, long out_ld, int active, double route_lo = -1e300,
+                      double route_hi = 1e300) {
   TcArgs p{};
+  p.route_lo = route_lo;
+  p.route_hi = route_hi;
   p.a = a;
   p.nm = s->d_norm;
   p.wb = s->wb;
@@ -1347,12 +1377,18 @@ static cudaError_t launch_tc(Surrogate* s, const TcArgs& p, cudaStream_t st) {
 }
 
 // The FP64 gate over the n cells of a, in a grid of 128-thread blocks.
-static cudaError_t launch_gate(Surrogate* s, const StepArgs& a, const float* O, long o_ld,
+static cudaError_t launch_gate(Surrogate* s, const StepArgs& a, const float* O, long o_ld, const GateNets& nets,
                                unsigned long long* counters, cudaStream_t st) {
   const int sms = s->num_sms > 0 ? s->num_sms : 148;
   const long grid = std::min<long>((a.n + 127) / 128, (long)sms * 16);
-  k_gate<<<(unsigned)std::max<long>(grid, 1), 128, 0, st>>>(a, O, o_ld, s->d_norm, s->gate, s->flag, counters);
+  k_gate<<<(unsigned)std::max<long>(grid, 1), 128, 0, st>>>(a, O, o_ld, nets, s->flag, counters);
   return cudaGetLastError();
+}
+
+// Lowest temperature of a network's training hull (widened by its margin).
+static double hull_T_lo(const Surrogate* s) {
+  const double lo = s->norm.x_min[0], hi = s->norm.x_max[0];
+  return lo - (double)s->norm.hull_margin * (hi - lo);
 }
 
 std::string surrogate_infer(Surrogate* s, const StepArgs& a, float* out, cudaStream_t st) {
@@ -1364,6 +1400,7 @@ std::string surrogate_infer(Surrogate* s, const StepArgs& a, float* out, cudaStr
 }
 
 std::string surrogate_check(Surrogate* s, cudaStream_t st) {
+  if (!s) return "";
   cudaMemcpyAsync(s->h_err, s->d_err, 4, cudaMemcpyDeviceToHost, st);
   std::string e = ck(cudaStreamSynchronize(st), "surrogate error word");
   if (!e.empty()) return e;
@@ -1377,7 +1414,7 @@ std::string surrogate_check(Surrogate* s, cudaStream_t st) {
 
 void surrogate_set_fused(Surrogate* s, bool fused) { s->fused = fused; }
 
-cudaError_t surrogate_step(Surrogate* s, const StepArgs& a, const LaunchCfg& cfg, int* queue,
+cudaError_t surrogate_step(Surrogate* s, Surrogate* s2, const StepArgs& a, const LaunchCfg& cfg, int* queue,
                            unsigned long long* counters, cudaStream_t st, const FallbackFn& fallback,
                            cudaEvent_t* ph) {
   (void)cfg;
@@ -1386,16 +1423,29 @@ cudaError_t surrogate_step(Surrogate* s, const StepArgs& a, const LaunchCfg& cfg
   if (a.n > s->gcap || (!s->fused && a.n > s->icap)) return cudaErrorMemoryAllocation;
   const long n = a.n;
   cudaError_t e;
+  GateNets nets{};
+  nets.net[0] = GateNet{s->d_norm, s->gate, -1e300, 1e300, 1};
   if (s->fused) {
-    // network outputs of the active cells, planar, then the wide FP64 gate
-    if ((e = launch_tc(s, tc_args(s, a, s->gO, n, 1), st)) != cudaSuccess) return e;
-    if ((e = launch_gate(s, a, s->gO, n, counters, st)) != cudaSuccess) return e;
+    // Routing: the main network takes the cells from the bottom of its hull
+    // up; a second network (the preheat band) those between the bottom of
+    // its own hull and that temperature.
+    const bool two = s2 && surrogate_ready(s2);
+    const double lo0 = hull_T_lo(s);
+    if (two) {
+      nets.net[0].lo = lo0;
+      nets.net[1] = GateNet{s2->d_norm, s2->gate, hull_T_lo(s2), lo0, 1};
+    }
+    // network outputs of the routed cells, planar, then the wide FP64 gate
+    if ((e = launch_tc(s, tc_args(s, a, s->gO, n, 1, nets.net[0].lo, nets.net[0].hi), st)) != cudaSuccess) return e;
+    if (two && (e = launch_tc(s2, tc_args(s2, a, s->gO, n, 1, nets.net[1].lo, nets.net[1].hi), st)) != cudaSuccess)
+      return e;
+    if ((e = launch_gate(s, a, s->gO, n, nets, counters, st)) != cudaSuccess) return e;
     if (ph) cudaEventRecord(ph[1], st);
   } else {
     k_features<<<std::min<long>((n + 255) / 256, 148 * 16), 256, 0, st>>>(n, a.ld, a.dt, a.dt_cells, a.T, a.rho,
                                                                         a.Y, s->d_norm, nullptr, s->iX);
     if ((e = forward_infer(s, n, s->iX, s->iO, st)) != cudaSuccess) return e;
-    if ((e = launch_gate(s, a, s->iO, 0, counters, st)) != cudaSuccess) return e;
+    if ((e = launch_gate(s, a, s->iO, 0, nets, counters, st)) != cudaSuccess) return e;
     if (ph) cudaEventRecord(ph[1], st);
   }
   if (s->order_cells) {

@@ -30,12 +30,15 @@ std::string surrogate_reserve(Surrogate* s, long n);
 std::string bounded_wait_probe(unsigned long long limit_ns, int* timed_out, double* waited_ms);
 
 // Enqueues features -> MLP -> gate/outputs -> compaction -> FP64 fallback
-// on the cells the gate rejects.  counters[6] / [7] receive surrogate /
+// on the cells the gate rejects.  s2 (may be null or not ready): a second
+// network for the temperatures between the bottom of its own training hull
+// and the bottom of s's (the flame's preheat band); s owns the step's
+// buffers.  counters[6] / [7] receive surrogate /
 // fallback cell counts.
 // ph (may be null): events recorded at phase boundaries: ph[1] after the
 // network and the gate kernel; the fallback callback records ph[2] / ph[3]
 // around the integrator.
-cudaError_t surrogate_step(Surrogate* s, const StepArgs& a, const LaunchCfg& cfg, int* queue,
+cudaError_t surrogate_step(Surrogate* s, Surrogate* s2, const StepArgs& a, const LaunchCfg& cfg, int* queue,
                            unsigned long long* counters, cudaStream_t st, const FallbackFn& fallback,
                            cudaEvent_t* ph);
 

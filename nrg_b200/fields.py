@@ -111,12 +111,14 @@ def wide_range_field(W: np.ndarray, n_side: int = 1024, seed: int = 2) -> Field:
     return _finish("wide_range_field", T, p, Y, W, 1e-5, (n_side, n_side))
 
 
-def training_states(W: np.ndarray, n: int, seed: int = 3, coupled: float = 0.0, T_lo: float = 800.0) -> Field:
+def training_states(W: np.ndarray, n: int, seed: int = 3, coupled: float = 0.0, T_lo: float = 800.0,
+                    T_hi: float = 2600.0) -> Field:
     """Training states: the wide-range distribution with dt ~ log-U[1e-7, 1e-5]
-    (radicals shared in a fraction `coupled` of the states; T_lo < 800 K
-    widens the temperature range down to a flame's preheat zone)."""
+    (radicals shared in a fraction `coupled` of the states); [T_lo, T_hi]
+    is [800, 2600] K for the wide-range distribution itself and [305, 800] K
+    for a flame's preheat zone."""
     rng = np.random.Generator(np.random.PCG64(seed))
-    T, p, Y = random_state(n, rng, W, T_lo, 2600.0, 0.5, 5.0, coupled)
+    T, p, Y = random_state(n, rng, W, T_lo, T_hi, 0.5, 5.0, coupled)
     dts = 10.0 ** rng.uniform(-7.0, -5.0, n)
     return _finish("training_states", T, p, Y, W, float("nan"), (n,), dts)
 

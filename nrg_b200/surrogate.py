@@ -20,6 +20,7 @@ from .chemistry import ChemicalKineticsSolver, _check, _ptr, lib
 
 MODEL_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "models")
 DEFAULT_MODEL = os.path.join(MODEL_DIR, "keromnes_surrogate.bin")
+PREHEAT_MODEL = os.path.join(MODEL_DIR, "keromnes_preheat.bin")
 
 
 def param_count() -> int:
@@ -43,47 +44,63 @@ def unflatten(p: np.ndarray):
 
 
 class Surrogate:
-    """Owns the MLP state of a ChemicalKineticsSolver handle."""
+    """One network of a ChemicalKineticsSolver handle: net 0 is the main
+    network, net 1 the optional one for a flame's preheat band (see
+    nrg_surrogate_select).  Every call selects this network first."""
 
-    def __init__(self, solver: ChemicalKineticsSolver):
+    def __init__(self, solver: ChemicalKineticsSolver, net: int = 0):
         self.solver = solver
         self.h = solver.handle
+        self.net = int(net)
+        self._select()
+
+    def _select(self) -> None:
+        _check(lib().nrg_surrogate_select(self.h, self.net), self.h)
 
     def init(self, seed: int = 0) -> None:
+        self._select()
         _check(lib().nrg_surrogate_init(self.h, ctypes.c_ulonglong(seed)), self.h)
 
     def params(self) -> np.ndarray:
+        self._select()
         p = np.zeros(param_count(), np.float32)
         _check(lib().nrg_surrogate_get_params(self.h, p.ctypes.data), self.h)
         return p
 
     def set_params(self, p: np.ndarray) -> None:
+        self._select()
         p = np.ascontiguousarray(p, np.float32)
         _check(lib().nrg_surrogate_set_params(self.h, p.ctypes.data), self.h)
 
     def norm(self) -> np.ndarray:
+        self._select()
         v = np.zeros(lib().nrg_surrogate_norm_count(), np.float32)
         _check(lib().nrg_surrogate_get_norm(self.h, v.ctypes.data), self.h)
         return v
 
     def set_norm(self, v: np.ndarray) -> None:
+        self._select()
         v = np.ascontiguousarray(v, np.float32)
         _check(lib().nrg_surrogate_set_norm(self.h, v.ctypes.data), self.h)
 
     def set_gate(self, elem_tol=1e-6, raw_elem_tol=5e-6, dT_tol=0.2, dT_max=5.0) -> None:
+        self._select()
         _check(lib().nrg_surrogate_set_gate(self.h, elem_tol, raw_elem_tol, dT_tol, dT_max), self.h)
 
     def set_gate_dt(self, dt_max: float = 1e-6) -> None:
         """Longest step whose cells the gate may accept (the gate bounds are
         calibrated on 1e-6 s steps); longer steps go to FP64."""
+        self._select()
         _check(lib().nrg_surrogate_set_gate_dt(self.h, dt_max), self.h)
 
     def set_inference(self, fused: bool = True) -> None:
         """Fused tcgen05 kernel (default) or the unfused GEMM chain + gate."""
+        self._select()
         _check(lib().nrg_surrogate_set_inference(self.h, int(fused)), self.h)
 
     def infer(self, f: fields.Field):
         """Network outputs (n x 16, normalised units) of the fused kernel."""
+        self._select()
         import torch
         dev = torch.device("cuda")
         T, rho, Y = (torch.tensor(a, device=dev) for a in (f.T, f.rho, f.Y))
@@ -95,17 +112,21 @@ class Surrogate:
         return out
 
     def enable(self, on: bool = True) -> None:
+        self._select()
         _check(lib().nrg_surrogate_enable(self.h, int(on)), self.h)
 
     def save(self, path: str) -> None:
+        self._select()
         os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
         _check(lib().nrg_surrogate_save(self.h, path.encode()), self.h)
 
     def load(self, path: str) -> None:
+        self._select()
         _check(lib().nrg_surrogate_load(self.h, path.encode()), self.h)
 
     # ---- device-level pieces (torch tensors as buffers)
     def forward(self, x_bf16):
+        self._select()
         import torch
         out = torch.empty((x_bf16.shape[0], 16), dtype=torch.float32, device=x_bf16.device)
         torch.cuda.synchronize()
@@ -113,6 +134,7 @@ class Surrogate:
         return out
 
     def grad(self, x_bf16, y):
+        self._select()
         import torch
         g = np.zeros(param_count(), np.float32)
         loss = ctypes.c_double()
@@ -122,6 +144,7 @@ class Surrogate:
         return g, loss.value
 
     def train(self, x_bf16, y, epochs=10, batch=4096, lr=1e-3, seed=0):
+        self._select()
         import torch
         losses = np.zeros(epochs, np.float32)
         torch.cuda.synchronize()
@@ -130,6 +153,7 @@ class Surrogate:
         return losses
 
     def features(self, f: fields.Field, xraw=True):
+        self._select()
         import torch
         dev = torch.device("cuda")
         T, rho, Y = (torch.tensor(a, device=dev) for a in (f.T, f.rho, f.Y))
@@ -153,19 +177,86 @@ class PrepareOpts(ctypes.Structure):
 # a validation flame field (flame_field geometry, seed 5) as the widest setting
 # whose accepted cells stay within 0.8 K and 8e-5 of the FP64 result.
 RECIPE = dict(n_train=4_000_000, epochs=150, batch=4096, lr=2e-3, coupled=0.5, hull_margin=0.02, dt_pow=1.0,
-              log_mask=0, log_eps=1e-7, common_dY_scale=0, T_lo=800.0,
+              log_mask=0, log_eps=1e-7, common_dY_scale=0, T_lo=800.0, T_hi=2600.0,
               gate=(1e-6, 5e-6, 0.2, 5.0))
+
+
+# The second network, for a flame's preheat band: the same state distribution
+# with T ~ U[305, 800] K (its own standardisation and hull), 4,000,000 pairs
+# drawn with seed 13, 150 epochs (final loss 3.2e-5); gate settings chosen by
+# calibrate_gate on every 8th row of the validation flame field (seed 5):
+# of 150 settings, the one answering the most preheat-band cells (18,186 of
+# 30,573) with every answered cell within 0.8 K and 8e-5 of the FP64 step
+# (observed 0.49 K and 2.2e-5).
+RECIPE_PREHEAT = dict(RECIPE, T_lo=305.0, T_hi=800.0, pair_seed=13, gate=(1e-6, 5e-6, 0.2, 80.0))
+
+
+def load_default(solver: ChemicalKineticsSolver) -> list:
+    """The committed networks on the solver's handle, each with its gate:
+    the main one (net 0) and, when its file exists, the preheat one (net 1)."""
+    nets = []
+    for net, path, recipe in ((0, DEFAULT_MODEL, RECIPE), (1, PREHEAT_MODEL, RECIPE_PREHEAT)):
+        if not os.path.exists(path):
+            continue
+        sur = Surrogate(solver, net)
+        sur.load(path)
+        sur.set_gate(*recipe["gate"])
+        nets.append(sur)
+    return nets
+
+
+def hull_T_lo(sur: "Surrogate") -> float:
+    """Bottom of a network's training hull in T (widened by its margin): the
+    lower end of its routing band."""
+    nm = sur.norm()
+    lo, hi, margin = float(nm[24]), float(nm[36]), float(nm[58])
+    return lo - margin * (hi - lo)
+
+
+def calibrate_gate(solver: ChemicalKineticsSolver, sur: "Surrogate", field: fields.Field, settings,
+                   T_band=(0.0, 1e9), tol_T: float = 0.8, tol_Y: float = 8e-5) -> dict:
+    """Gate setting of one network: of `settings` (tuples of set_gate's
+    arguments), the one under which the most cells of `field` with T in
+    T_band (the network's routing band) are answered while every answered
+    cell stays within tol_T (K) and tol_Y (mass fraction) of the plain FP64
+    step of the same cell.  Returns the choice and the sweep; leaves the
+    chosen setting in place."""
+    import torch
+    dev = torch.device("cuda")
+    T, rho, Y = (torch.tensor(a, device=dev) for a in (field.T, field.rho, field.Y))
+    outs = [torch.zeros_like(Y), torch.zeros_like(Y), torch.zeros_like(T), torch.zeros_like(T),
+            torch.zeros(field.n, dtype=torch.uint8, device=dev)]
+    solver.set_mode("fast")
+    solver.step_device(field.dt, T, rho, Y, outs[0], outs[1], outs[2], T_after=outs[3], status=outs[4])
+    ref_Yp, ref_Ta = outs[0].cpu().numpy(), outs[3].cpu().numpy()
+    sweep = []
+    solver.set_mode("surrogate")
+    for g in settings:
+        sur.set_gate(*g)
+        solver.step_device(field.dt, T, rho, Y, outs[0], outs[1], outs[2], T_after=outs[3], status=outs[4])
+        st = outs[4].cpu().numpy()
+        acc = (st == 5) & (field.T >= T_band[0]) & (field.T < T_band[1])
+        dY = (np.abs(outs[0].cpu().numpy() - ref_Yp) * field.dt / field.rho[None, :])[:, acc]
+        dT = np.abs(outs[3].cpu().numpy() - ref_Ta)[acc]
+        sweep.append({"gate": list(g), "accepted": int(acc.sum()), "max_dY": float(dY.max()) if acc.any() else 0.0,
+                      "max_dT": float(dT.max()) if acc.any() else 0.0})
+    solver.set_mode("fast")
+    ok = [r for r in sweep if r["max_dY"] <= tol_Y and r["max_dT"] <= tol_T]
+    best = max(ok, key=lambda r: r["accepted"]) if ok else None
+    if best:
+        sur.set_gate(*best["gate"])
+    return {"choice": best, "sweep": sweep}
 
 
 def training_pairs(solver: ChemicalKineticsSolver, W: np.ndarray, n: int, seed: int = 3,
                    hull_margin: float = RECIPE["hull_margin"], dt_pow: float = RECIPE["dt_pow"],
                    coupled: float = RECIPE["coupled"], log_mask: int = RECIPE["log_mask"],
                    log_eps: float = RECIPE["log_eps"], common_dY_scale: int = RECIPE["common_dY_scale"],
-                   T_lo: float = RECIPE["T_lo"]):
+                   T_lo: float = RECIPE["T_lo"], T_hi: float = RECIPE["T_hi"]):
     """Integrates n training states with their own dt (FP64 integrator) and
     returns standardised (x_bf16, y) device tensors plus timing."""
     import torch
-    f = fields.training_states(W, n, seed=seed, coupled=coupled, T_lo=T_lo)
+    f = fields.training_states(W, n, seed=seed, coupled=coupled, T_lo=T_lo, T_hi=T_hi)
     # neighbouring lanes take similar paths when states are sorted by (dt, T)
     order = np.lexsort((f.T, np.round(np.log10(f.dt_cells) * 8)))
     f = fields.Field(f.name, f.T[order], f.rho[order], f.p[order], np.ascontiguousarray(f.Y[:, order]), f.dt,
@@ -188,15 +279,16 @@ def training_pairs(solver: ChemicalKineticsSolver, W: np.ndarray, n: int, seed: 
     return x, y, {"integrate_s": t_int, "integrator_stats": stats, "n": n}
 
 
-def train_default(solver: ChemicalKineticsSolver, W: np.ndarray, seed: int = 0, **overrides) -> dict:
-    """Full recipe (RECIPE, with overrides): pairs -> Adam training -> gate
-    settings -> enabled."""
-    r = dict(RECIPE, **overrides)
-    sur = Surrogate(solver)
+def train_default(solver: ChemicalKineticsSolver, W: np.ndarray, seed: int = 0, net: int = 0, **overrides) -> dict:
+    """Full recipe (RECIPE for net 0, RECIPE_PREHEAT for net 1, with
+    overrides): pairs -> Adam training -> gate settings -> enabled."""
+    r = dict(RECIPE if net == 0 else RECIPE_PREHEAT, **overrides)
+    sur = Surrogate(solver, net)
     t0 = time.perf_counter()
-    x, y, info = training_pairs(solver, W, r["n_train"], hull_margin=r["hull_margin"], dt_pow=r["dt_pow"],
+    x, y, info = training_pairs(solver, W, r["n_train"], seed=r.get("pair_seed", 3), hull_margin=r["hull_margin"],
+                                dt_pow=r["dt_pow"],
                                 coupled=r["coupled"], log_mask=r["log_mask"], log_eps=r["log_eps"],
-                                common_dY_scale=r["common_dY_scale"], T_lo=r["T_lo"])
+                                common_dY_scale=r["common_dY_scale"], T_lo=r["T_lo"], T_hi=r["T_hi"])
     sur.init(seed)
     t1 = time.perf_counter()
     losses = sur.train(x, y, epochs=r["epochs"], batch=r["batch"], lr=r["lr"], seed=seed + 1)

@@ -86,12 +86,16 @@ def test_flame_field_sample_plain_fp64_parity(solver, flame, capsys):
 
 
 def test_flame_field_sample_surrogate_against_oracle(solver, flame, capsys):
-    from nrg_b200.surrogate import DEFAULT_MODEL, RECIPE, Surrogate
+    """Both committed networks (the main one and the preheat band's), each
+    with its calibrated gate, against the oracle; the preheat band is
+    answered too."""
+    from nrg_b200.surrogate import hull_T_lo, load_default
     f, o = flame
-    sur = Surrogate(solver)
-    sur.load(DEFAULT_MODEL)
-    sur.set_gate(*RECIPE["gate"])
+    nets = load_default(solver)
+    assert len(nets) == 2
     g, st = run_device(solver, f, "surrogate")
+    lo0 = hull_T_lo(nets[0])
+    assert ((g["status"] == 5) & (f.T >= 305.0) & (f.T < lo0)).sum() > 0
     act = f.T >= 305.0
     acc = g["status"] == 5
     assert acc.sum() > 0 and np.array_equal(g["status"] != 0, act)
