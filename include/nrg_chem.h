@@ -342,14 +342,17 @@ NRG_API const char* nrg_chem_last_error(nrg_chem* h);
  * features, y arrays n x 10 fp32 standardised targets (device memory). */
 NRG_API int nrg_surrogate_param_count(void);
 NRG_API int nrg_surrogate_norm_count(void);
-/* A handle holds two networks: 0, the main one (its training hull starts at
- * 800 K), and 1, an optional one for a flame's preheat band.  A surrogate
- * step needs network 0; each active cell goes to network 0 from the bottom of
- * that network's hull up, to network 1 (when enabled) between the bottom of
- * its own hull and there, and to the FP64 integrator otherwise; each network
- * has its own standardisation and gate settings.  The set-up calls below
- * (init, parameters, norm, training, gate, enable, save, load, inference)
- * act on the network selected here (0 by default). */
+/* A handle holds up to eight networks: 0, the main one, and 1..7 for
+ * narrower temperature bands (the committed models: 1 a flame's preheat
+ * band, 305-800 K, 2 the low-temperature part of its front, 800-1500 K) or
+ * serving as another network's committee partner.  A
+ * surrogate step needs network 0; each active cell goes to the enabled
+ * network of highest index whose training hull's temperature range holds it
+ * (network 0 also takes the cells above its hull, which its hull test then
+ * rejects), and to the FP64 integrator when there is none; each network has
+ * its own standardisation and gate settings.  The set-up calls below (init,
+ * parameters, norm, training, gate, enable, save, load, inference) act on
+ * the network selected here (0 by default). */
 NRG_API int nrg_surrogate_select(nrg_chem* h, int net);
 NRG_API int nrg_surrogate_init(nrg_chem* h, unsigned long long seed);
 NRG_API int nrg_surrogate_get_params(nrg_chem* h, float* params);
@@ -393,6 +396,18 @@ NRG_API int nrg_surrogate_set_gate(nrg_chem* h, double elem_tol, double raw_elem
  * distribution they let cells through with errors of many kelvin.  No
  * counterpart in the reference. */
 NRG_API int nrg_surrogate_set_gate_dt(nrg_chem* h, double dt_max);
+/* Committee check of the selected network: a cell it answers is accepted
+ * only if network `partner` (-1: no check), evaluated on the same cell,
+ * predicts every dY_k within agree_Y (mass fraction) and dT within agree_T
+ * (K) of it -- two networks trained on different temperature ranges rarely
+ * share an error, so their agreement marks reliable predictions.  No
+ * counterpart in the reference. */
+NRG_API int nrg_surrogate_set_partner(nrg_chem* h, int partner, double agree_Y, double agree_T);
+/* Routing band [T_lo, T_hi) of the selected network instead of its training
+ * hull's temperature range (0, 0: back to the hull's; T_lo >= T_hi: no cells
+ * are routed to it, it only answers as a committee partner).  No
+ * counterpart in the reference. */
+NRG_API int nrg_surrogate_set_band(nrg_chem* h, double T_lo, double T_hi);
 /* Inference path of the surrogate step: 1 (default) the tensor-core kernel
  * (features and the five layers on tcgen05 with TMEM accumulators) followed
  * by the wide FP64 gate kernel; 0 the GEMM chain (features, one mma.sync

@@ -107,6 +107,8 @@ SIGNATURES = {
     "nrg_surrogate_train": (_I, [_VP, _L, _VP, _VP, _I, _I, ctypes.c_float, ctypes.c_ulonglong, _VP]),
     "nrg_surrogate_set_gate": (_I, [_VP, _D, _D, _D, _D]),
     "nrg_surrogate_set_gate_dt": (_I, [_VP, _D]),
+    "nrg_surrogate_set_partner": (_I, [_VP, _I, _D, _D]),
+    "nrg_surrogate_set_band": (_I, [_VP, _D, _D]),
     "nrg_chem_set_specialised": (_I, [_VP, _I]),
     "nrg_chem_apply_state_device": (_I, [_VP, _D, _L, _L, _I] + [_VP] * 17),
     "nrg_surrogate_set_inference": (_I, [_VP, _I]),

@@ -77,7 +77,7 @@ struct nrg_chem {
   // surrogate state (owned by surrogate.cu): the main network and a second
   // one for the flame's preheat band; the nrg_surrogate_* set-up calls act on
   // network sur_sel (nrg_surrogate_select)
-  nrg::Surrogate* sur_net[2] = {nullptr, nullptr};
+  nrg::Surrogate* sur_net[nrg::kMaxNets] = {};
   int sur_sel = 0;
   std::string err;
 };
@@ -356,7 +356,7 @@ cudaError_t enqueue_step_body(nrg_chem* h, const StepArgs& a, cudaStream_t s, cu
     return e;
   }
   if (h->mode == NRG_MODE_SURROGATE)
-    return nrg::surrogate_step(h->sur_net[0], h->sur_net[1], a, h->cfg, h->d_queue, h->d_counters, s,
+    return nrg::surrogate_step(h->sur_net, a, h->cfg, h->d_queue, h->d_counters, s,
                                [h, ph](const StepArgs& fa, cudaStream_t fs) {
                                  if (ph) cudaEventRecord(ph[2], fs);
                                  LaunchCfg c = h->cfg;
@@ -473,8 +473,8 @@ int step_finish(nrg_chem* h, cudaStream_t s, long n, nrg_chem_stats* stats) {
     }
   }
   if (h->mode == NRG_MODE_SURROGATE) {
-    std::string e = nrg::surrogate_check(h->sur_net[0], s);
-    if (e.empty()) e = nrg::surrogate_check(h->sur_net[1], s);
+    std::string e;
+    for (int i = 0; i < nrg::kMaxNets && e.empty(); ++i) e = nrg::surrogate_check(h->sur_net[i], s);
     if (!e.empty()) return fail(h, NRG_ERR_CUDA, e);
   }
   return NRG_OK;
@@ -559,8 +559,7 @@ extern "C" int nrg_chem_create(const char* mechanism_path, const char* thermo_pa
   }
   reduce_dev_mech(h->dm, &h->dmr);
   h->spec = nrg::match_specialised(h->dmr);
-  h->sur_net[0] = nrg::surrogate_create(h->dm);
-  h->sur_net[1] = nrg::surrogate_create(h->dm);
+  for (int i = 0; i < nrg::kMaxNets; ++i) h->sur_net[i] = nrg::surrogate_create(h->dm);
   if ((ce = use_tables(h)) != cudaSuccess) {
     std::string msg = std::string("mechanism upload failed: ") + cudaGetErrorString(ce);
     nrg_chem_destroy(h);
@@ -581,8 +580,7 @@ extern "C" int nrg_chem_destroy(nrg_chem* h) {
   device_scope.enter(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
-  nrg::surrogate_destroy(h->sur_net[0]);
-  nrg::surrogate_destroy(h->sur_net[1]);
+  for (int i = 0; i < nrg::kMaxNets; ++i) nrg::surrogate_destroy(h->sur_net[i]);
   cudaFree(h->d_tab_T);
   cudaFree(h->d_tab_Y);
   free_staging(h);
@@ -1259,7 +1257,7 @@ extern "C" int nrg_surrogate_param_count(void) { return nrg::surrogate_param_cou
 
 extern "C" int nrg_surrogate_select(nrg_chem* h, int net) {
   if (!h) return NRG_ERR_ARG;
-  if (net < 0 || net > 1) return fail(h, NRG_ERR_ARG, "network index must be 0 (main) or 1 (preheat band)");
+  if (net < 0 || net >= nrg::kMaxNets) return fail(h, NRG_ERR_ARG, "network index must be 0 (main) to 7");
   h->sur_sel = net;
   return NRG_OK;
 }
@@ -1362,6 +1360,22 @@ extern "C" int nrg_surrogate_set_gate(nrg_chem* h, double elem_tol, double raw_e
                                       double dT_max) {
   if (!h || !(elem_tol >= 0) || !(raw_elem_tol >= 0) || !(dT_tol >= 0) || !(dT_max >= 0)) return NRG_ERR_ARG;
   nrg::surrogate_set_gate(h->sur_net[h->sur_sel], elem_tol, raw_elem_tol, dT_tol, dT_max);
+  return NRG_OK;
+}
+
+extern "C" int nrg_surrogate_set_band(nrg_chem* h, double T_lo, double T_hi) {
+  if (!h) return NRG_ERR_ARG;
+  const bool unset = T_lo == 0.0 && T_hi == 0.0;
+  if (!(T_lo == T_lo) || !(T_hi == T_hi)) return fail(h, NRG_ERR_ARG, "routing band bounds must be numbers");
+  nrg::surrogate_set_band(h->sur_net[h->sur_sel], !unset, T_lo, T_hi);
+  return NRG_OK;
+}
+
+extern "C" int nrg_surrogate_set_partner(nrg_chem* h, int partner, double agree_Y, double agree_T) {
+  if (!h) return NRG_ERR_ARG;
+  if (partner < -1 || partner >= nrg::kMaxNets || partner == h->sur_sel || !(agree_Y >= 0) || !(agree_T >= 0))
+    return fail(h, NRG_ERR_ARG, "partner must be -1 or another network (0..7), agreement bounds >= 0");
+  nrg::surrogate_set_partner(h->sur_net[h->sur_sel], partner, agree_Y, agree_T);
   return NRG_OK;
 }
 

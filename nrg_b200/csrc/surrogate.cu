@@ -1,7 +1,7 @@
 // Gated MLP surrogate of the per-cell chemistry increment.
 //
-// Training and the unfused inference path use one BF16 tensor-core GEMM
-// (mma.sync m16n8k16, FP32 accumulate) with a fused bias/GELU epilogue; the
+// Training and the GEMM-chain inference path use one BF16 tensor-core GEMM
+// (tcgen05.mma, FP32 accumulator in TMEM) with a fused bias/GELU epilogue; the
 // gate decides per cell whether the prediction is used or the cell goes to
 // the FP64 integrator:
 //   * skip rule of the reference (T < 305 K or bc /= 0): zero sources;
@@ -50,89 +50,158 @@ __device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 lo, __nv_bfloat16 hi
   return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
 }
 
-__device__ __forceinline__ void mma_bf16_16816(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
-                                               uint32_t b0, uint32_t b1) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-      "{%0,%1,%2,%3};\n"
-      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+// C[M, N] = sum_k A[m, k] B[k, n] (+ bias, GELU) on the tensor cores, for
+// training (forward, weight and activation gradients) and the GEMM-chain
+// inference path.  One 128-thread CTA per 128-row x BN-column tile (BN = N
+// rounded up to 16, at most 128): K advances in chunks of 64, each staged in
+// shared memory in the K-major no-swizzle core-matrix layout by all threads
+// (16-byte vector loads where K is the contiguous direction, element loads
+// that transpose otherwise), then multiplied by one thread with
+// tcgen05.mma (kind::f16, FP32 accumulator in 128 TMEM columns); two
+// buffers, so the next chunk is staged while the tensor core reads the
+// previous one.  gridDim.z > 1 splits K (the weight gradients, K = batch):
+// each CTA adds its partial tile to C with atomics (C zeroed beforehand, no
+// bias or GELU then).  Every mbarrier wait is bounded; a timeout sets *err
+// and the CTA stops.
+constexpr uint64_t kTcWaitNs = 1000000000ull;  // 1 s per MMA wait (this GEMM and k_mlp_tc)
+constexpr int kTgBK = 64;
+constexpr uint32_t kTgBuf = 128 * kTgBK * 2;  // one operand chunk: 128 rows x 64 bf16 = 16 KB
+constexpr uint32_t kTgSmem = 4 * kTgBuf + 64;  // A0 A1 B0 B1, barriers, TMEM slot
+
+__device__ __forceinline__ void tg_stage(unsigned char* dst, const __nv_bfloat16* src, long s_row, long s_k,
+                                         long row0, long rows, long k0, long kend) {
+  // dst: 128 rows x kTgBK, row r = operand row row0 + r, column kk = k0 + kk
+  const __nv_bfloat16 zero = __float2bfloat16(0.f);
+  const bool vec = s_k == 1 && (s_row % 8) == 0 && ((reinterpret_cast<uintptr_t>(src) & 15) == 0) &&
+                   k0 + kTgBK <= kend;
+  if (vec) {
+    for (int e = threadIdx.x; e < 128 * (kTgBK / 8); e += blockDim.x) {
+      const int r = e / (kTgBK / 8), kc = e % (kTgBK / 8);
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (row0 + r < rows) v = *reinterpret_cast<const uint4*>(src + (row0 + r) * s_row + k0 + kc * 8);
+      *reinterpret_cast<uint4*>(dst + tc::kmajor_off(r, kc, kTgBK)) = v;
+    }
+  } else {
+    // consecutive threads take consecutive rows (coalesced when rows are the
+    // contiguous direction, as in the transposed operands of the gradients)
+    for (int e = threadIdx.x; e < 128 * kTgBK; e += blockDim.x) {
+      const int r = e % 128, kk = e / 128;
+      const long row = row0 + r, k = k0 + kk;
+      const __nv_bfloat16 v = (row < rows && k < kend) ? src[row * s_row + k * s_k] : zero;
+      *reinterpret_cast<__nv_bfloat16*>(dst + tc::kmajor_off(r, kk >> 3, kTgBK) + (kk & 7) * 2) = v;
+    }
+  }
 }
 
-// C[M,N] = sum_k A[m,k] B[k,n]; 128 threads, 64x64 block tile, 32x32 per warp.
-__global__ void __launch_bounds__(128) k_gemm_bf16(GemmArgs g) {
-  constexpr int BM = 64, BN = 64, BK = 32;
-  __shared__ __nv_bfloat16 As[BM][BK + 8];
-  __shared__ __nv_bfloat16 Bs[BK][BN + 8];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wm = warp >> 1, wn = warp & 1;
-  const int g8 = lane >> 2, tq = lane & 3;
-  const long m0 = (long)blockIdx.x * BM, n0 = (long)blockIdx.y * BN;
-  float acc[2][4][4];
-#pragma unroll
-  for (int i = 0; i < 2; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.f;
-  const __nv_bfloat16 zero = __float2bfloat16(0.f);
-  for (int k0 = 0; k0 < g.K; k0 += BK) {
-    for (int e = tid; e < BM * BK; e += 128) {
-      const int r = e / BK, kk = e % BK;
-      const long m = m0 + r, k = k0 + kk;
-      As[r][kk] = (m < g.M && k < g.K) ? g.A[m * g.sam + k * g.sak] : zero;
-    }
-    for (int e = tid; e < BK * BN; e += 128) {
-      const int kk = e / BN, cc = e % BN;
-      const long k = k0 + kk, n = n0 + cc;
-      Bs[kk][cc] = (k < g.K && n < g.N) ? g.B[k * g.sbk + n * g.sbn] : zero;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int ks = 0; ks < BK; ks += 16) {
-      uint32_t a[2][4], b[4][2];
-#pragma unroll
-      for (int mi = 0; mi < 2; ++mi) {
-        const int r = wm * 32 + mi * 16 + g8;
-        a[mi][0] = pack_bf16(As[r][ks + 2 * tq], As[r][ks + 2 * tq + 1]);
-        a[mi][1] = pack_bf16(As[r + 8][ks + 2 * tq], As[r + 8][ks + 2 * tq + 1]);
-        a[mi][2] = pack_bf16(As[r][ks + 2 * tq + 8], As[r][ks + 2 * tq + 9]);
-        a[mi][3] = pack_bf16(As[r + 8][ks + 2 * tq + 8], As[r + 8][ks + 2 * tq + 9]);
-      }
-#pragma unroll
-      for (int ni = 0; ni < 4; ++ni) {
-        const int cc = wn * 32 + ni * 8 + g8;
-        b[ni][0] = pack_bf16(Bs[ks + 2 * tq][cc], Bs[ks + 2 * tq + 1][cc]);
-        b[ni][1] = pack_bf16(Bs[ks + 2 * tq + 8][cc], Bs[ks + 2 * tq + 9][cc]);
-      }
-#pragma unroll
-      for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-        for (int ni = 0; ni < 4; ++ni)
-          mma_bf16_16816(acc[mi][ni], a[mi][0], a[mi][1], a[mi][2], a[mi][3], b[ni][0], b[ni][1]);
-    }
-    __syncthreads();
+__global__ void __launch_bounds__(128, 1) k_gemm_tc(GemmArgs g, long k_per_cta, unsigned int* err) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  unsigned char* bufA[2] = {sm, sm + kTgBuf};
+  unsigned char* bufB[2] = {sm + 2 * kTgBuf, sm + 3 * kTgBuf};
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + 4 * kTgBuf);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + 4 * kTgBuf + 32);
+  const int tid = threadIdx.x, wq = tid >> 5;
+  const long m0 = (long)blockIdx.x * 128, n0 = (long)blockIdx.y * 128;
+  const long kb = (long)blockIdx.z * k_per_cta, ke = min((long)g.K, kb + k_per_cta);
+  const int bn = (int)(((min(128L, (long)g.N - n0) + 15) / 16) * 16);
+  if (tid == 0) {
+    tc::mbar_init(tc::smem_u32(&mbar[0]), 1);
+    tc::mbar_init(tc::smem_u32(&mbar[1]), 1);
+    tc::mbar_init_fence();
   }
+  if (tid < 32) tc::tmem_alloc(tc::smem_u32(tslot), 128);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tbase = *tslot;
+  // B operand rows are the output columns n: element (n, k) = B[k * sbk + n * sbn]
+  const uint32_t idesc = tc::idesc_bf16_f32(128, (uint32_t)bn);
+  const long nch = (ke - kb + kTgBK - 1) / kTgBK;
+  uint32_t parity[2] = {0u, 0u};
+  bool ok = true;
+  for (long c = 0; c < nch && ok; ++c) {
+    const int b = (int)(c & 1);
+    if (c >= 2) {  // the MMAs that read this buffer two chunks ago are done
+      ok = tc::bar_and(1, 128, tc::mbar_wait(tc::smem_u32(&mbar[b]), parity[b], kTcWaitNs));
+      parity[b] ^= 1u;
+      if (!ok) break;
+    }
+    const long k0 = kb + c * kTgBK;
+    tg_stage(bufA[b], g.A, g.sam, g.sak, m0, g.M, k0, ke);
+    tg_stage(bufB[b], g.B, g.sbn, g.sbk, n0, g.N, k0, ke);
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {
+      tc::fence_after_sync();
+      const uint32_t a = tc::smem_u32(bufA[b]), bb = tc::smem_u32(bufB[b]);
 #pragma unroll
-  for (int mi = 0; mi < 2; ++mi)
+      for (int s = 0; s < kTgBK / 16; ++s)
+        tc::mma_bf16(tbase, tc::smem_desc(a + s * 256, 128, kTgBK * 16), tc::smem_desc(bb + s * 256, 128, kTgBK * 16),
+                     idesc, (c > 0 || s > 0) ? 1u : 0u);
+      tc::commit(tc::smem_u32(&mbar[b]));
+    }
+  }
+  // the last chunk's MMAs (and with them all earlier ones) complete
+  if (ok && nch > 0) {
+    const int b = (int)((nch - 1) & 1);
+    ok = tc::bar_and(1, 128, tc::mbar_wait(tc::smem_u32(&mbar[b]), parity[b], kTcWaitNs));
+  }
+  if (!ok) {
+    if (tid == 0) atomicOr(err, 1u);
+  } else if (nch > 0) {
+    tc::fence_after_sync();
+    const long m = m0 + tid;
+    const bool split = gridDim.z > 1;
+    for (int j0 = 0; j0 < bn; j0 += 16) {
+      uint32_t r[16];
+      tc::tmem_ld16(tbase + ((uint32_t)(wq * 32) << 16) + (uint32_t)j0, r);
+      tc::tmem_ld_wait();
+      if (m >= g.M) continue;
 #pragma unroll
-    for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const long m = m0 + wm * 32 + mi * 16 + g8 + (q >= 2 ? 8 : 0);
-        const long n = n0 + wn * 32 + ni * 8 + 2 * tq + (q & 1);
-        if (m >= g.M || n >= g.N) continue;
-        float v = acc[mi][ni][q];
+      for (int j = 0; j < 16; ++j) {
+        const long n = n0 + j0 + j;
+        if (n >= g.N) continue;
+        float v = __uint_as_float(r[j]);
+        if (split) {
+          atomicAdd(&g.C[m * g.ldc + n], v);
+          continue;
+        }
         if (g.bias) v += g.bias[n];
         if (g.C) g.C[m * g.ldc + n] = v;
         if (g.H) g.H[m * g.ldh + n] = __float2bfloat16(g.gelu ? gelu_f(v) : v);
       }
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (tid < 32) {
+    tc::fence_after_sync();
+    tc::tmem_dealloc(tbase, 128);
+  }
 }
 
-static cudaError_t gemm(const GemmArgs& g, cudaStream_t st) {
-  dim3 grid((unsigned)((g.M + 63) / 64), (unsigned)((g.N + 63) / 64));
-  if (grid.x == 0 || grid.y == 0) return cudaSuccess;
-  k_gemm_bf16<<<grid, 128, 0, st>>>(g);
+// Launches the tensor-core GEMM; K split over CTAs when the output is a
+// single tile and K is long (the weight gradients).
+static cudaError_t gemm(const GemmArgs& g, cudaStream_t st, unsigned int* err) {
+  if (g.M <= 0 || g.N <= 0) return cudaSuccess;
+  dim3 grid((unsigned)((g.M + 127) / 128), (unsigned)((g.N + 127) / 128), 1);
+  long kpc = g.K;
+  if (grid.x * grid.y < 16 && g.K > 4 * kTgBK) {
+    if (g.bias || g.H || !g.C) return cudaErrorInvalidValue;  // split K adds partial tiles only
+    const long chunks = (g.K + kTgBK - 1) / kTgBK;
+    const long z = std::min<long>(chunks, 64);
+    kpc = ((chunks + z - 1) / z) * kTgBK;
+    grid.z = (unsigned)((g.K + kpc - 1) / kpc);
+    cudaError_t e = cudaSuccess;
+    if (g.ldc == g.N) {
+      e = cudaMemsetAsync(g.C, 0, sizeof(float) * (size_t)g.N * (size_t)g.M, st);
+    } else {
+      for (long m = 0; m < g.M && e == cudaSuccess; ++m)
+        e = cudaMemsetAsync(g.C + m * g.ldc, 0, sizeof(float) * (size_t)g.N, st);
+    }
+    if (e != cudaSuccess) return e;
+  }
+  k_gemm_tc<<<grid, 128, kTgSmem, st>>>(g, kpc, err);
   return cudaGetLastError();
 }
 
@@ -250,6 +319,11 @@ struct GateCfg {
   double raw_elem_tol;  // element residual of the network's own dY
   double dT_tol, dT_max;
   double dt_max;        // cells with a longer step go to FP64: the bounds above were calibrated up to it
+  // committee check: with a partner network (index >= 0), a cell is accepted
+  // only if the partner predicts every dY_k within agree_Y and dT within
+  // agree_T of this network
+  int partner;
+  double agree_Y, agree_T;
 };
 
 // Element residual max_e |sum_k a_ek (W_e / W_k) dY_k| (element mass fraction)
@@ -399,7 +473,7 @@ __device__ __forceinline__ double gate_closure(const GateThermo& g, double T0, d
 __device__ __forceinline__ bool gate_active_cell(const StepArgs& a, long c, double T0, double rho, double dt,
                                                  const float (&f)[kMlpIn], const float (&o)[kMlpOut],
                                                  const MlpNorm* nm, const GateCfg& gc, const double (*P)[9],
-                                                 const GateThermo& th) {
+                                                 const GateThermo& th, const float* op, const MlpNorm* pnm) {
   if (!(dt <= gc.dt_max)) return false;
   bool in = true;
   const float margin = nm->hull_margin;
@@ -419,6 +493,13 @@ __device__ __forceinline__ bool gate_active_cell(const StepArgs& a, long c, doub
   }
   const double dT_net = (double)o[9] * (double)nm->y_sd[9] * sc;
   if (!fin || !isfinite(dT_net) || !(fabs(dT_net) <= gc.dT_max)) return false;
+  if (op) {  // committee check against the partner network's prediction
+    const double psc = (double)target_scale(f[11], pnm->dt_pow);
+    bool agree = fabs((double)op[9] * (double)pnm->y_sd[9] * psc - dT_net) <= gc.agree_T;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) agree = agree && fabs((double)op[k] * (double)pnm->y_sd[k] * psc - dYn[k]) <= gc.agree_Y;
+    if (!agree) return false;
+  }
   if (!(element_residual(dYn) <= gc.raw_elem_tol)) return false;
   // the written increment conserves H, O and N: projection in FP64
   double dY[9];
@@ -459,28 +540,32 @@ __device__ __forceinline__ void count_surrogate(unsigned long long n_sur, unsign
 
 // O: the network outputs of every active cell, output j of cell c at
 // O[j * o_ld + c] (o_ld > 0) or O[c * 16 + j] (o_ld == 0).
-// The networks of one step: each answers the active cells whose temperature
-// lies in its routing band [lo, hi) (bands do not overlap) with its own
-// standardisation and gate settings.
+// The networks of one step: an active cell goes to the enabled network of
+// highest index whose routing band [lo, hi) -- the temperature range of its
+// training hull -- holds its temperature, and is gated with that network's
+// standardisation and settings.  Network 0 is the main one; the others
+// cover narrower bands (a flame's preheat zone, the low-temperature part of
+// its front) and take precedence there.
 struct GateNet {
   const MlpNorm* nm;
   GateCfg gc;
   double lo, hi;
   int on;
 };
-constexpr int kMaxNets = 2;
 struct GateNets {
   GateNet net[kMaxNets];
 };
 
 __device__ __forceinline__ int route_of(const GateNets& g, double T) {
 #pragma unroll
-  for (int i = 0; i < kMaxNets; ++i)
+  for (int i = kMaxNets - 1; i >= 0; --i)
     if (g.net[i].on && T >= g.net[i].lo && T < g.net[i].hi) return i;
   return -1;
 }
 
-__global__ void __launch_bounds__(128, 3) k_gate(StepArgs a, const float* O, long o_ld, GateNets nets,
+// OP (may be null): the partner networks' outputs for the cells routed to a
+// network that has a partner, planar like O with o_ld.
+__global__ void __launch_bounds__(128, 3) k_gate(StepArgs a, const float* O, const float* OP, long o_ld, GateNets nets,
                                               unsigned char* flag, unsigned long long* counters) {
   __shared__ double P[9][9];
   __shared__ GateThermo th;
@@ -510,7 +595,15 @@ __global__ void __launch_bounds__(128, 3) k_gate(StepArgs a, const float* O, lon
     }
 #pragma unroll
     for (int j = 0; j < kMlpOut; ++j) o[j] = o_ld > 0 ? O[j * o_ld + c] : O[c * kMlpOutPad + j];
-    const bool acc = gate_active_cell(a, c, T0, rho, dt, f, o, nets.net[net].nm, nets.net[net].gc, P, th);
+    const int pn = nets.net[net].gc.partner;
+    float op[kMlpOut];
+    const bool with_partner = OP && o_ld > 0 && pn >= 0 && pn < kMaxNets && nets.net[pn].on;
+    if (with_partner) {
+#pragma unroll
+      for (int j = 0; j < kMlpOut; ++j) op[j] = OP[j * o_ld + c];
+    }
+    const bool acc = gate_active_cell(a, c, T0, rho, dt, f, o, nets.net[net].nm, nets.net[net].gc, P, th,
+                                      with_partner ? op : nullptr, with_partner ? nets.net[pn].nm : nullptr);
     n_sur += acc;
     flag[c] = acc ? 0 : 1;
   }
@@ -547,7 +640,6 @@ constexpr uint32_t kTcSmem = kTcMisc + 256;
 constexpr uint32_t kTcTmemCols = 512;  // a power of two holding 128 columns per group
 static_assert(kTcGroups * 128 <= (int)kTcTmemCols, "TMEM columns of the groups");
 static_assert(kTcSmem <= 227u * 1024u, "shared memory of one CTA");
-constexpr uint64_t kTcWaitNs = 1000000000ull;  // 1 s per MMA wait
 
 struct TcArgs {
   StepArgs a;
@@ -557,8 +649,11 @@ struct TcArgs {
   long offW[kMlpLayers], offb[kMlpLayers];
   float* out;    // network outputs (normalised units)
   long out_ld;   // > 0: output j of cell c at out[j * out_ld + c] (kMlpOut values); 0: out[c * 16 + j]
-  int active;    // 1: only the cells the step integrates (skip rule) whose T is in [route_lo, route_hi); 0: every cell
-  double route_lo, route_hi;
+  int active;    // 1: only the cells the step integrates (skip rule) that route to network `net`, or to a
+                 // network whose partner `net` is (those outputs go to out_partner); 0: every cell
+  int net;
+  GateNets routes;
+  float* out_partner;
   unsigned int* err;  // bit 0: an MMA wait timed out
 };
 
@@ -571,11 +666,12 @@ __device__ __forceinline__ uint4 pack8(const float* v) {
   return r;
 }
 
-__device__ __forceinline__ void store_outputs(const TcArgs& p, long c, const float* o, bool valid) {
+__device__ __forceinline__ void store_outputs(const TcArgs& p, long c, const float* o, bool valid, bool partner) {
   const float nan = __int_as_float(0x7fc00000);
   if (p.out_ld > 0) {
+    float* dst = partner ? p.out_partner : p.out;
 #pragma unroll
-    for (int j = 0; j < kMlpOut; ++j) p.out[j * p.out_ld + c] = valid ? o[j] : nan;
+    for (int j = 0; j < kMlpOut; ++j) dst[j * p.out_ld + c] = valid ? o[j] : nan;
   } else {
 #pragma unroll
     for (int j = 0; j < kMlpOutPad; ++j) p.out[c * kMlpOutPad + j] = !valid ? nan : (j < kMlpOut ? o[j] : 0.f);
@@ -635,13 +731,19 @@ __global__ void __launch_bounds__(128 * kTcGroups, 1) k_mlp_tc(TcArgs p) {
   int par = 0;
   for (long tile = (long)blockIdx.x * kTcGroups + g; tile < ntiles; tile += (long)gridDim.x * kTcGroups, par ^= 1) {
     const long c = tile * 128 + t;
-    bool need = false;
+    bool need = false, for_partner = false;
     float f[kMlpIn];
 #pragma unroll
     for (int j = 0; j < kMlpIn; ++j) f[j] = 0.f;
     if (c < a.n) {
       const double T0 = a.T[c];
-      need = p.active ? reference_cell_active(T0, a.bc, c) && T0 >= p.route_lo && T0 < p.route_hi : true;
+      if (p.active) {
+        const int r = reference_cell_active(T0, a.bc, c) ? route_of(p.routes, T0) : -1;
+        for_partner = r >= 0 && r != p.net && p.out_partner && p.routes.net[r].gc.partner == p.net;
+        need = r == p.net || for_partner;
+      } else {
+        need = true;
+      }
       if (need) {
         double y0[9];
 #pragma unroll
@@ -651,7 +753,7 @@ __global__ void __launch_bounds__(128 * kTcGroups, 1) k_mlp_tc(TcArgs p) {
     }
     float o[kMlpOutPad];
     if (aborted) {
-      if (need) store_outputs(p, c, o, false);
+      if (need) store_outputs(p, c, o, false, for_partner);
       continue;
     }
     const unsigned bal = __ballot_sync(0xffffffffu, need);
@@ -729,7 +831,7 @@ __global__ void __launch_bounds__(128 * kTcGroups, 1) k_mlp_tc(TcArgs p) {
       aborted = true;
       if (t == 0) atomicOr(p.err, 1u);
     }
-    if (need) store_outputs(p, c, o, ok);
+    if (need) store_outputs(p, c, o, ok, for_partner);
   }
   tc::fence_before_sync();
   __syncthreads();
@@ -869,7 +971,7 @@ __global__ void k_standardize(long n, const float* xraw, const float* yraw, cons
 struct Surrogate {
   bool ready = false;
   bool uploaded = false;
-  GateCfg gate{1e-6, 5e-6, 0.2, 5.0, 1e-6};
+  GateCfg gate{1e-6, 5e-6, 0.2, 5.0, 1e-6, -1, 0.0, 0.0};
   MlpNorm norm{};
   MlpNorm* d_norm = nullptr;
   // parameters: fp32 master, Adam moments, bf16 working copies, gradients
@@ -902,6 +1004,10 @@ struct Surrogate {
   // (kMlpOut planes of gcap floats)
   long gcap = 0;
   float* gO = nullptr;
+  float* gP = nullptr;  // partner networks' outputs (committee check), same layout
+  // routing band [band_lo, band_hi) when set (band_set), else the hull's T range
+  bool band_set = false;
+  double band_lo = 0.0, band_hi = 0.0;
   unsigned char* flag = nullptr;
   int *block_count = nullptr, *block_off = nullptr, *list = nullptr, *n_list = nullptr;
   // fallback cells in temperature order (order.hpp) or in cell order
@@ -949,6 +1055,7 @@ Surrogate* surrogate_create(const DevMech& dm) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, dev);
   cudaFuncSetAttribute(k_mlp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
+  cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTgSmem);
   cudaMemset(s->w, 0, P * 4);
   cudaMemset(s->m, 0, P * 4);
   cudaMemset(s->v, 0, P * 4);
@@ -978,7 +1085,7 @@ void surrogate_destroy(Surrogate* s) {
   free_act(s);
   cudaFree(s->w); cudaFree(s->m); cudaFree(s->v); cudaFree(s->gr); cudaFree(s->wb); cudaFree(s->d_norm);
   cudaFree(s->iX); cudaFree(s->iH[0]); cudaFree(s->iH[1]); cudaFree(s->iO);
-  cudaFree(s->d_loss); cudaFree(s->flag); cudaFree(s->gO); cudaFree(s->block_count); cudaFree(s->block_off);
+  cudaFree(s->d_loss); cudaFree(s->flag); cudaFree(s->gO); cudaFree(s->gP); cudaFree(s->block_count); cudaFree(s->block_off);
   cudaFree(s->list);
   cudaFree(s->n_list);
   order_free(&s->order);
@@ -991,9 +1098,20 @@ bool surrogate_ready(const Surrogate* s) { return s && s->ready && s->uploaded; 
 void surrogate_set_ready(Surrogate* s, bool r) { s->ready = r; }
 void surrogate_set_cell_order(Surrogate* s, bool by_temperature) { s->order_cells = by_temperature; }
 void surrogate_set_gate(Surrogate* s, double elem_tol, double raw_elem_tol, double dT_tol, double dT_max) {
-  s->gate = GateCfg{elem_tol, raw_elem_tol, dT_tol, dT_max, s->gate.dt_max};
+  const GateCfg g0 = s->gate;
+  s->gate = GateCfg{elem_tol, raw_elem_tol, dT_tol, dT_max, g0.dt_max, g0.partner, g0.agree_Y, g0.agree_T};
 }
 void surrogate_set_gate_dt(Surrogate* s, double dt_max) { s->gate.dt_max = dt_max; }
+void surrogate_set_band(Surrogate* s, bool set, double lo, double hi) {
+  s->band_set = set;
+  s->band_lo = lo;
+  s->band_hi = hi;
+}
+void surrogate_set_partner(Surrogate* s, int partner, double agree_Y, double agree_T) {
+  s->gate.partner = partner;
+  s->gate.agree_Y = agree_Y;
+  s->gate.agree_T = agree_T;
+}
 
 static std::string ck(cudaError_t e, const char* what) {
   return e == cudaSuccess ? std::string() : std::string(what) + ": " + cudaGetErrorString(e);
@@ -1042,10 +1160,12 @@ static std::string ensure_gate(Surrogate* s, long n) {
   if (n <= s->gcap) return "";
   cudaFree(s->flag); cudaFree(s->block_count); cudaFree(s->block_off); cudaFree(s->list); cudaFree(s->n_list);
   cudaFree(s->gO);
-  s->gO = nullptr;
+  cudaFree(s->gP);
+  s->gO = s->gP = nullptr;
   const long nb = (n + kCompactBlock - 1) / kCompactBlock;
   std::string e;
   if ((e = ck(cudaMalloc(&s->gO, sizeof(float) * kMlpOut * (size_t)n), "alloc outputs")).size()) return e;
+  if ((e = ck(cudaMalloc(&s->gP, sizeof(float) * kMlpOut * (size_t)n), "alloc partner outputs")).size()) return e;
   if ((e = ck(cudaMalloc(&s->flag, n), "alloc flag")).size()) return e;
   if ((e = ck(cudaMalloc(&s->block_count, nb * 4), "alloc counts")).size()) return e;
   if ((e = ck(cudaMalloc(&s->block_off, nb * 4), "alloc offsets")).size()) return e;
@@ -1127,7 +1247,7 @@ static cudaError_t forward(Surrogate* s, long n, const __nv_bfloat16* x, float* 
     g.H = last ? nullptr : s->H[l];
     g.ldh = mlp_out(l);
     g.gelu = 1;
-    cudaError_t e = gemm(g, st);
+    cudaError_t e = gemm(g, st, s->d_err);
     if (e != cudaSuccess) return e;
     in = s->H[l];
   }
@@ -1163,7 +1283,7 @@ static cudaError_t forward_infer(Surrogate* s, long n, const __nv_bfloat16* x, f
     g.H = last ? nullptr : s->iH[l & 1];
     g.ldh = mlp_out(l);
     g.gelu = 1;
-    cudaError_t e = gemm(g, st);
+    cudaError_t e = gemm(g, st, s->d_err);
     if (e != cudaSuccess) return e;
     in = s->iH[l & 1];
   }
@@ -1193,7 +1313,7 @@ static cudaError_t backward(Surrogate* s, long B, const __nv_bfloat16* x, const 
     g.sbn = 1;
     g.C = s->gr + s->offW[l];
     g.ldc = mlp_in(l);
-    if ((e = gemm(g, st)) != cudaSuccess) return e;
+    if ((e = gemm(g, st, s->d_err)) != cudaSuccess) return e;
     k_colsum<<<mlp_out(l), 256, 0, st>>>(B, mlp_out(l), dZf, s->gr + s->offb[l]);
     if (l == 0) break;
     // dH[b][in] = sum_out dZ[b][out] W[out][in]
@@ -1209,7 +1329,7 @@ static cudaError_t backward(Surrogate* s, long B, const __nv_bfloat16* x, const 
     h.sbn = 1;
     h.C = s->dHf;
     h.ldc = mlp_in(l);
-    if ((e = gemm(h, st)) != cudaSuccess) return e;
+    if ((e = gemm(h, st, s->d_err)) != cudaSuccess) return e;
     const long cnt = B * kMlpHid;
     k_gelu_back<<<std::min<long>((cnt + 255) / 256, 4096), 256, 0, st>>>(cnt, s->dHf, s->Z[l - 1], s->dZf,
                                                                          s->dHb);
@@ -1348,11 +1468,12 @@ std::string surrogate_reserve(Surrogate* s, long n) {
   return ensure_gate(s, n);
 }
 
-static TcArgs tc_args(Surrogate* s, const StepArgs& a, float* out, long out_ld, int active, double route_lo = -1e300,
-                      double route_hi = 1e300) {
+static TcArgs tc_args(Surrogate* s, const StepArgs& a, float* out, long out_ld, int active,
+                      const GateNets* routes = nullptr, int net = 0, float* out_partner = nullptr) {
   TcArgs p{};
-  p.route_lo = route_lo;
-  p.route_hi = route_hi;
+  if (routes) p.routes = *routes;
+  p.net = net;
+  p.out_partner = out_partner;
   p.a = a;
   p.nm = s->d_norm;
   p.wb = s->wb;
@@ -1377,18 +1498,19 @@ static cudaError_t launch_tc(Surrogate* s, const TcArgs& p, cudaStream_t st) {
 }
 
 // The FP64 gate over the n cells of a, in a grid of 128-thread blocks.
-static cudaError_t launch_gate(Surrogate* s, const StepArgs& a, const float* O, long o_ld, const GateNets& nets,
-                               unsigned long long* counters, cudaStream_t st) {
+static cudaError_t launch_gate(Surrogate* s, const StepArgs& a, const float* O, const float* OP, long o_ld,
+                               const GateNets& nets, unsigned long long* counters, cudaStream_t st) {
   const int sms = s->num_sms > 0 ? s->num_sms : 148;
   const long grid = std::min<long>((a.n + 127) / 128, (long)sms * 16);
-  k_gate<<<(unsigned)std::max<long>(grid, 1), 128, 0, st>>>(a, O, o_ld, nets, s->flag, counters);
+  k_gate<<<(unsigned)std::max<long>(grid, 1), 128, 0, st>>>(a, O, OP, o_ld, nets, s->flag, counters);
   return cudaGetLastError();
 }
 
-// Lowest temperature of a network's training hull (widened by its margin).
-static double hull_T_lo(const Surrogate* s) {
-  const double lo = s->norm.x_min[0], hi = s->norm.x_max[0];
-  return lo - (double)s->norm.hull_margin * (hi - lo);
+// Temperature range of a network's training hull (widened by its margin).
+static void hull_T(const Surrogate* s, double* lo_out, double* hi_out) {
+  const double lo = s->norm.x_min[0], hi = s->norm.x_max[0], m = (double)s->norm.hull_margin * (hi - lo);
+  *lo_out = lo - m;
+  *hi_out = hi + m;
 }
 
 std::string surrogate_infer(Surrogate* s, const StepArgs& a, float* out, cudaStream_t st) {
@@ -1414,11 +1536,12 @@ std::string surrogate_check(Surrogate* s, cudaStream_t st) {
 
 void surrogate_set_fused(Surrogate* s, bool fused) { s->fused = fused; }
 
-cudaError_t surrogate_step(Surrogate* s, Surrogate* s2, const StepArgs& a, const LaunchCfg& cfg, int* queue,
+cudaError_t surrogate_step(Surrogate* const* nets_in, const StepArgs& a, const LaunchCfg& cfg, int* queue,
                            unsigned long long* counters, cudaStream_t st, const FallbackFn& fallback,
                            cudaEvent_t* ph) {
   (void)cfg;
   (void)queue;
+  Surrogate* s = nets_in[0];
   // buffers are reserved by surrogate_reserve before any graph capture
   if (a.n > s->gcap || (!s->fused && a.n > s->icap)) return cudaErrorMemoryAllocation;
   const long n = a.n;
@@ -1426,26 +1549,33 @@ cudaError_t surrogate_step(Surrogate* s, Surrogate* s2, const StepArgs& a, const
   GateNets nets{};
   nets.net[0] = GateNet{s->d_norm, s->gate, -1e300, 1e300, 1};
   if (s->fused) {
-    // Routing: the main network takes the cells from the bottom of its hull
-    // up; a second network (the preheat band) those between the bottom of
-    // its own hull and that temperature.
-    const bool two = s2 && surrogate_ready(s2);
-    const double lo0 = hull_T_lo(s);
-    if (two) {
-      nets.net[0].lo = lo0;
-      nets.net[1] = GateNet{s2->d_norm, s2->gate, hull_T_lo(s2), lo0, 1};
+    // routing bands: the hulls' temperature ranges; network 0 also takes
+    // what lies above its hull (its hull test then sends it to FP64)
+    for (int i = 0; i < kMaxNets; ++i) {
+      Surrogate* si = nets_in[i];
+      if (!si || !surrogate_ready(si)) continue;
+      double lo, hi;
+      hull_T(si, &lo, &hi);
+      if (i == 0) hi = 1e300;
+      if (si->band_set) {
+        lo = si->band_lo;
+        hi = si->band_hi;
+      }
+      nets.net[i] = GateNet{si->d_norm, si->gate, lo, hi, 1};
     }
     // network outputs of the routed cells, planar, then the wide FP64 gate
-    if ((e = launch_tc(s, tc_args(s, a, s->gO, n, 1, nets.net[0].lo, nets.net[0].hi), st)) != cudaSuccess) return e;
-    if (two && (e = launch_tc(s2, tc_args(s2, a, s->gO, n, 1, nets.net[1].lo, nets.net[1].hi), st)) != cudaSuccess)
-      return e;
-    if ((e = launch_gate(s, a, s->gO, n, nets, counters, st)) != cudaSuccess) return e;
+    for (int i = 0; i < kMaxNets; ++i) {
+      if (!nets.net[i].on) continue;
+      if ((e = launch_tc(nets_in[i], tc_args(nets_in[i], a, s->gO, n, 1, &nets, i, s->gP), st)) != cudaSuccess)
+        return e;
+    }
+    if ((e = launch_gate(s, a, s->gO, s->gP, n, nets, counters, st)) != cudaSuccess) return e;
     if (ph) cudaEventRecord(ph[1], st);
   } else {
     k_features<<<std::min<long>((n + 255) / 256, 148 * 16), 256, 0, st>>>(n, a.ld, a.dt, a.dt_cells, a.T, a.rho,
                                                                         a.Y, s->d_norm, nullptr, s->iX);
     if ((e = forward_infer(s, n, s->iX, s->iO, st)) != cudaSuccess) return e;
-    if ((e = launch_gate(s, a, s->iO, 0, nets, counters, st)) != cudaSuccess) return e;
+    if ((e = launch_gate(s, a, s->iO, nullptr, 0, nets, counters, st)) != cudaSuccess) return e;
     if (ph) cudaEventRecord(ph[1], st);
   }
   if (s->order_cells) {

@@ -14,6 +14,10 @@ namespace nrg {
 
 struct Surrogate;
 
+// Networks of one handle: 0 the main one, the others for narrower
+// temperature bands (routing in surrogate_step).
+constexpr int kMaxNets = 8;
+
 using FallbackFn = std::function<cudaError_t(const StepArgs&, cudaStream_t)>;
 
 Surrogate* surrogate_create(const DevMech& dm);
@@ -30,15 +34,15 @@ std::string surrogate_reserve(Surrogate* s, long n);
 std::string bounded_wait_probe(unsigned long long limit_ns, int* timed_out, double* waited_ms);
 
 // Enqueues features -> MLP -> gate/outputs -> compaction -> FP64 fallback
-// on the cells the gate rejects.  s2 (may be null or not ready): a second
-// network for the temperatures between the bottom of its own training hull
-// and the bottom of s's (the flame's preheat band); s owns the step's
-// buffers.  counters[6] / [7] receive surrogate /
+// on the cells the gate rejects.  nets: kMaxNets networks, nets[0] the main
+// one (ready; it owns the step's buffers), the others may be null or not
+// ready; each active cell goes to the ready network of highest index whose
+// hull's temperature range holds it.  counters[6] / [7] receive surrogate /
 // fallback cell counts.
 // ph (may be null): events recorded at phase boundaries: ph[1] after the
 // network and the gate kernel; the fallback callback records ph[2] / ph[3]
 // around the integrator.
-cudaError_t surrogate_step(Surrogate* s, Surrogate* s2, const StepArgs& a, const LaunchCfg& cfg, int* queue,
+cudaError_t surrogate_step(Surrogate* const* nets, const StepArgs& a, const LaunchCfg& cfg, int* queue,
                            unsigned long long* counters, cudaStream_t st, const FallbackFn& fallback,
                            cudaEvent_t* ph);
 
@@ -89,5 +93,9 @@ std::string surrogate_check(Surrogate* s, cudaStream_t st);
 void surrogate_set_gate(Surrogate* s, double elem_tol, double raw_elem_tol, double dT_tol, double dT_max);
 // Longest step (s) whose cells the gate may accept.
 void surrogate_set_gate_dt(Surrogate* s, double dt_max);
+// Committee check of a network: partner (-1: none), agreement bounds.
+void surrogate_set_partner(Surrogate* s, int partner, double agree_Y, double agree_T);
+// Routing band [lo, hi) of a network (set = false: its hull's T range).
+void surrogate_set_band(Surrogate* s, bool set, double lo, double hi);
 
 }  // namespace nrg

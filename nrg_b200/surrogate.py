@@ -21,6 +21,7 @@ from .chemistry import ChemicalKineticsSolver, _check, _ptr, lib
 MODEL_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "models")
 DEFAULT_MODEL = os.path.join(MODEL_DIR, "keromnes_surrogate.bin")
 PREHEAT_MODEL = os.path.join(MODEL_DIR, "keromnes_preheat.bin")
+FRONT_LOW_MODEL = os.path.join(MODEL_DIR, "keromnes_front_low.bin")
 
 
 def param_count() -> int:
@@ -45,7 +46,7 @@ def unflatten(p: np.ndarray):
 
 class Surrogate:
     """One network of a ChemicalKineticsSolver handle: net 0 is the main
-    network, net 1 the optional one for a flame's preheat band (see
+    network, nets 1-3 optional ones for narrower temperature bands (see
     nrg_surrogate_select).  Every call selects this network first."""
 
     def __init__(self, solver: ChemicalKineticsSolver, net: int = 0):
@@ -86,6 +87,18 @@ class Surrogate:
     def set_gate(self, elem_tol=1e-6, raw_elem_tol=5e-6, dT_tol=0.2, dT_max=5.0) -> None:
         self._select()
         _check(lib().nrg_surrogate_set_gate(self.h, elem_tol, raw_elem_tol, dT_tol, dT_max), self.h)
+
+    def set_band(self, T_lo: float = 0.0, T_hi: float = 0.0) -> None:
+        """Routing band [T_lo, T_hi) of this network (0, 0: its hull's; an
+        empty band, T_lo >= T_hi: a partner only, never routed cells)."""
+        self._select()
+        _check(lib().nrg_surrogate_set_band(self.h, float(T_lo), float(T_hi)), self.h)
+
+    def set_partner(self, partner: int = -1, agree_Y: float = 0.0, agree_T: float = 0.0) -> None:
+        """Committee check: accept a cell only if network `partner` predicts
+        the same increment within agree_Y / agree_T (-1: no check)."""
+        self._select()
+        _check(lib().nrg_surrogate_set_partner(self.h, int(partner), float(agree_Y), float(agree_T)), self.h)
 
     def set_gate_dt(self, dt_max: float = 1e-6) -> None:
         """Longest step whose cells the gate may accept (the gate bounds are
@@ -190,37 +203,68 @@ RECIPE = dict(n_train=4_000_000, epochs=150, batch=4096, lr=2e-3, coupled=0.5, h
 # (observed 0.49 K and 2.2e-5).
 RECIPE_PREHEAT = dict(RECIPE, T_lo=305.0, T_hi=800.0, pair_seed=13, gate=(1e-6, 5e-6, 0.2, 80.0))
 
+# The third network, for the low-temperature part of a flame front: the same
+# state distribution with T ~ U[800, 1500] K, 4,000,000 pairs drawn with seed
+# 17, 150 epochs (final loss 3.1e-4); gate settings chosen by calibrate_gate
+# as for the preheat network (3,058 of the 9,694 validation cells it is routed
+# answered, within 0.74 K and 6.8e-5 of the FP64 step).
+RECIPE_FRONT_LOW = dict(RECIPE, T_lo=800.0, T_hi=1500.0, pair_seed=17, gate=(1e-6, 5e-6, 0.2, 80.0))
+
+# (network index, model file, recipe) of the committed networks
+COMMITTED = ((0, DEFAULT_MODEL, RECIPE), (1, PREHEAT_MODEL, RECIPE_PREHEAT), (2, FRONT_LOW_MODEL, RECIPE_FRONT_LOW))
+
+
+# partner network of each committed network that has one
+COMMITTED_PARTNERS = tuple((net, r["partner"][0]) for net, _, r in COMMITTED if "partner" in r)
+
 
 def load_default(solver: ChemicalKineticsSolver) -> list:
     """The committed networks on the solver's handle, each with its gate:
-    the main one (net 0) and, when its file exists, the preheat one (net 1)."""
+    the main one (net 0) and the band networks whose files exist."""
     nets = []
-    for net, path, recipe in ((0, DEFAULT_MODEL, RECIPE), (1, PREHEAT_MODEL, RECIPE_PREHEAT)):
+    for net, path, recipe in COMMITTED:
         if not os.path.exists(path):
             continue
         sur = Surrogate(solver, net)
         sur.load(path)
         sur.set_gate(*recipe["gate"])
+        if "partner" in recipe:
+            sur.set_partner(*recipe["partner"])
+        if "band" in recipe:
+            sur.set_band(*recipe["band"])
         nets.append(sur)
     return nets
 
 
-def hull_T_lo(sur: "Surrogate") -> float:
-    """Bottom of a network's training hull in T (widened by its margin): the
-    lower end of its routing band."""
+def hull_T(sur: "Surrogate"):
+    """Temperature range of a network's training hull (widened by its
+    margin): its routing band."""
     nm = sur.norm()
     lo, hi, margin = float(nm[24]), float(nm[36]), float(nm[58])
-    return lo - margin * (hi - lo)
+    return lo - margin * (hi - lo), hi + margin * (hi - lo)
+
+
+def routed_to(nets, T: np.ndarray) -> np.ndarray:
+    """Index of the network each temperature is routed to (-1: none)."""
+    r = np.full(T.shape, -1)
+    for s in sorted(nets, key=lambda s: s.net):
+        lo, hi = hull_T(s)
+        if s.net == 0:
+            hi = np.inf
+        r[(T >= lo) & (T < hi)] = s.net
+    return r
 
 
 def calibrate_gate(solver: ChemicalKineticsSolver, sur: "Surrogate", field: fields.Field, settings,
-                   T_band=(0.0, 1e9), tol_T: float = 0.8, tol_Y: float = 8e-5) -> dict:
-    """Gate setting of one network: of `settings` (tuples of set_gate's
-    arguments), the one under which the most cells of `field` with T in
-    T_band (the network's routing band) are answered while every answered
-    cell stays within tol_T (K) and tol_Y (mass fraction) of the plain FP64
-    step of the same cell.  Returns the choice and the sweep; leaves the
-    chosen setting in place."""
+                   cells=None, tol_T: float = 0.8, tol_Y: float = 8e-5) -> dict:
+    """Gate setting of one network: of `settings` (tuples of set_gate's four
+    arguments, followed by the committee bounds agree_Y, agree_T of the
+    network's partner when it has one), the one under which the most cells
+    of `field` (those selected
+    by the boolean mask `cells`, the ones routed to this network) are answered
+    while every answered cell stays within tol_T (K) and tol_Y (mass fraction)
+    of the plain FP64 step of the same cell.  Returns the choice and the
+    sweep; leaves the chosen setting in place."""
     import torch
     dev = torch.device("cuda")
     T, rho, Y = (torch.tensor(a, device=dev) for a in (field.T, field.rho, field.Y))
@@ -231,11 +275,16 @@ def calibrate_gate(solver: ChemicalKineticsSolver, sur: "Surrogate", field: fiel
     ref_Yp, ref_Ta = outs[0].cpu().numpy(), outs[3].cpu().numpy()
     sweep = []
     solver.set_mode("surrogate")
+    partner = None
     for g in settings:
-        sur.set_gate(*g)
+        sur.set_gate(*g[:4])
+        if len(g) > 4:
+            if partner is None:
+                partner = dict(COMMITTED_PARTNERS).get(sur.net, 0)
+            sur.set_partner(partner, g[4], g[5])
         solver.step_device(field.dt, T, rho, Y, outs[0], outs[1], outs[2], T_after=outs[3], status=outs[4])
         st = outs[4].cpu().numpy()
-        acc = (st == 5) & (field.T >= T_band[0]) & (field.T < T_band[1])
+        acc = (st == 5) if cells is None else (st == 5) & cells
         dY = (np.abs(outs[0].cpu().numpy() - ref_Yp) * field.dt / field.rho[None, :])[:, acc]
         dT = np.abs(outs[3].cpu().numpy() - ref_Ta)[acc]
         sweep.append({"gate": list(g), "accepted": int(acc.sum()), "max_dY": float(dY.max()) if acc.any() else 0.0,
@@ -244,7 +293,9 @@ def calibrate_gate(solver: ChemicalKineticsSolver, sur: "Surrogate", field: fiel
     ok = [r for r in sweep if r["max_dY"] <= tol_Y and r["max_dT"] <= tol_T]
     best = max(ok, key=lambda r: r["accepted"]) if ok else None
     if best:
-        sur.set_gate(*best["gate"])
+        sur.set_gate(*best["gate"][:4])
+        if len(best["gate"]) > 4:
+            sur.set_partner(partner, best["gate"][4], best["gate"][5])
     return {"choice": best, "sweep": sweep}
 
 

@@ -86,16 +86,17 @@ def test_flame_field_sample_plain_fp64_parity(solver, flame, capsys):
 
 
 def test_flame_field_sample_surrogate_against_oracle(solver, flame, capsys):
-    """Both committed networks (the main one and the preheat band's), each
-    with its calibrated gate, against the oracle; the preheat band is
-    answered too."""
-    from nrg_b200.surrogate import hull_T_lo, load_default
+    """The committed networks (the main one and the band networks), each
+    with its calibrated gate, against the oracle; every network answers
+    some of the cells routed to it."""
+    from nrg_b200.surrogate import COMMITTED, load_default, routed_to
     f, o = flame
     nets = load_default(solver)
-    assert len(nets) == 2
+    assert len(nets) == len(COMMITTED)
     g, st = run_device(solver, f, "surrogate")
-    lo0 = hull_T_lo(nets[0])
-    assert ((g["status"] == 5) & (f.T >= 305.0) & (f.T < lo0)).sum() > 0
+    route = routed_to(nets, f.T)
+    for s in nets:
+        assert ((g["status"] == 5) & (route == s.net) & (f.T >= 305.0)).sum() > 0, s.net
     act = f.T >= 305.0
     acc = g["status"] == 5
     assert acc.sum() > 0 and np.array_equal(g["status"] != 0, act)
