@@ -32,7 +32,8 @@ sys.path.insert(0, ROOT)
 METRIC = "chem cell-updates/s: surrogate+fallback vs plain FP64, same GPU, |ΔT|≤1 K"
 UNIT = "cell-updates/s"
 H2D_BYTES_PER_CELL = 11 * 8 + 1   # T, rho, 9 Y, bc
-D2H_BYTES_PER_CELL = 19 * 8 + 1   # 9 Y_prod, 9 Y_prod2, E_f_prod, status
+D2H_BYTES_PER_CELL = 10 * 8 + 1   # 9 Y_prod2, E_f_prod, status (the host rebuilds Y_prod = Y_prod2 W / dt)
+D2H_BYTES_PER_CELL_TABLE = 19 * 8 + 1  # table mode: 9 Y_prod as well
 
 
 def parse():
@@ -52,6 +53,8 @@ def parse():
     p.add_argument("--kernel", choices=["thread", "thread_queue", "warp_queue"], default=None,
                    help="fix the integrator launch instead of autotuning it (with --block)")
     p.add_argument("--block", type=int, default=32)
+    p.add_argument("--fallback-eps", type=float, default=None,
+                   help="integrator tolerance of the surrogate's rejected cells (default: FALLBACK_EPS; 0: 1e-9)")
     p.add_argument("--cell-order", choices=["temperature", "cell"], default="temperature",
                    help="order in which the FP64 integrator takes the cells (same results)")
     p.add_argument("--mechanism", default="KEROMNES", choices=["KEROMNES", "ZHANG", "TEREZA", "KONNOV", "ACETYLENE"],
@@ -542,7 +545,8 @@ def main():
         dist.init("nccl", timeout_s=600)
     from nrg_b200 import eact_units, fields as F, keromnes_paths, mechanism_paths
     from nrg_b200.chemistry import ChemicalKineticsSolver, DataManager, fp64_peak_tflops, mechanism_tables
-    from nrg_b200.surrogate import DEFAULT_MODEL, PREHEAT_MODEL, RECIPE, Surrogate, load_default, train_default
+    from nrg_b200.surrogate import (DEFAULT_MODEL, FALLBACK_EPS, PREHEAT_MODEL, RECIPE, Surrogate, load_default,
+                                    train_default)
     decks = mechanism_paths(args.mechanism)
     units = eact_units(args.mechanism)
     tables = mechanism_tables(*decks, 1.0, units)
@@ -593,9 +597,10 @@ def main():
     train_info = None
     if mode in ("auto", "surrogate"):
         if os.path.exists(DEFAULT_MODEL):
-            nets = load_default(solver)
+            nets = load_default(solver, args.fallback_eps)
             train_info = {"model": os.path.relpath(DEFAULT_MODEL, ROOT), "trained": "loaded",
-                          "gate": list(RECIPE["gate"])}
+                          "gate": list(RECIPE["gate"]),
+                          "fallback_eps": FALLBACK_EPS if args.fallback_eps is None else args.fallback_eps}
             if len(nets) > 1:
                 from nrg_b200.surrogate import RECIPE_PREHEAT
                 train_info["preheat_model"] = os.path.relpath(PREHEAT_MODEL, ROOT)
@@ -669,6 +674,11 @@ def main():
                "max_abs_dY": float(dYk.max()), "max_abs_dY_per_species": [float(v) for v in dYk.max(1)],
                "accepted_cells": int((st_s == 5).sum()), "fallback_cells": int(ph["cells_fallback"]),
                "fallback_fraction_of_active": float(ph["cells_fallback"]) / max(1, int(act.sum()))}
+        if mode == "surrogate":
+            # the integrated (rejected) cells alone: the fallback tolerance's share
+            fb = (st_s[act] != 5)
+            acc["fallback_max_abs_dT_K"] = float(dT[fb].max()) if fb.any() else 0.0
+            acc["fallback_max_abs_dY"] = float(dYk[:, fb].max()) if fb.any() else 0.0
 
     state_eq = None
     if args.state_eq:
@@ -731,7 +741,7 @@ def main():
         host.set_launch(**launch)
         host.set_cell_order(args.cell_order == "temperature")
         if mode == "surrogate":
-            load_default(host)
+            load_default(host, args.fallback_eps)
         if mode == "table":
             host.read_chemical_kinetics_table(table_path)
         host.set_mode(mode)
@@ -742,8 +752,9 @@ def main():
             host.solve_chemical_kinetics(field.dt)
         el2 = dist.max_over_ranks(time.perf_counter() - t0, dev)
         e2e = {"value": args.steps * n * world / el2, "unit": UNIT,
-               "h2d_bytes_per_step": n * H2D_BYTES_PER_CELL, "d2h_bytes_per_step": n * D2H_BYTES_PER_CELL,
-               "path": "nrg_chem_step (host Fortran-layout arrays, gather/H2D/step/D2H/scatter)"}
+               "h2d_bytes_per_step": n * H2D_BYTES_PER_CELL, "d2h_bytes_per_step": n * (D2H_BYTES_PER_CELL_TABLE if mode == "table" else D2H_BYTES_PER_CELL),
+               "path": "nrg_chem_step (host Fortran-layout arrays: chunks gathered and copied in while the "
+                       "networks and gate run per chunk; FP64 fallback per half of the field; copied out and scattered)"}
         host.close()
 
     if rank == 0:

@@ -91,7 +91,11 @@ typedef struct {
   /* per-phase device time when phase timing is on (nrg_chem_set_timing):
    * [0] surrogate inference (features + MLP, then the FP64 gate), [1] the
    * rejected cells' list (temperature order, or compaction in cell order), [2] FP64
-   * integrator (with the plain step's temperature order), [3] unused */
+   * integrator (with the plain step's temperature order), [3] unused.
+   * nrg_chem_step (host arrays) reports host wall times instead: [0] the
+   * gather of the inputs into pinned staging, [1] the chunks' scatter with
+   * its waits for their copies, [2] the rejected cells' read-back and
+   * scatter (surrogate mode), [3] the whole call */
   double phase_ms[4];
 } nrg_chem_stats;
 
@@ -138,6 +142,11 @@ NRG_API int nrg_chem_step_device(nrg_chem* h, double time_step, long n, long ld,
  * (cudaDeviceReset) invalidates it, so do not call this entry point again on
  * a device after resetting it in the same process.  The surrogate and table
  * modes are not available here. */
+/* Relative tolerance EPS of the FP64 integrator (DDRIV3's EPS; the
+ * reference fixes it at 1e-9, chemical_kinetics_solver.f90:282).  0 restores
+ * 1e-9; any other value departs from the reference's results. */
+NRG_API int nrg_chem_set_eps(nrg_chem* h, double eps);
+
 NRG_API int nrg_chem_step_device_noalloc(nrg_chem* h, double time_step, long n, long ld, const double* T,
                                          const double* rho, const double* Y, const signed char* bc,
                                          double* Y_prod, double* Y_prod2, double* E_f_prod, double* T_after,
@@ -408,9 +417,16 @@ NRG_API int nrg_surrogate_set_partner(nrg_chem* h, int partner, double agree_Y, 
  * are routed to it, it only answers as a committee partner).  No
  * counterpart in the reference. */
 NRG_API int nrg_surrogate_set_band(nrg_chem* h, double T_lo, double T_hi);
+/* Relative tolerance EPS of the FP64 integration of the cells the gate
+ * rejects (0, the default: the handle's EPS, nrg_chem_set_eps).  The
+ * surrogate mode is an approximation to |dT| <= 1 K, |dY_k| <= 1e-4; an EPS
+ * of 1e-5 keeps the fallback cells' error below 1e-6 in Y on the flame
+ * field while taking about 40% fewer BDF steps than 1e-9.  Per handle, for
+ * every network.  No counterpart in the reference. */
+NRG_API int nrg_surrogate_set_fallback_eps(nrg_chem* h, double eps);
 /* Inference path of the surrogate step: 1 (default) the tensor-core kernel
  * (features and the five layers on tcgen05 with TMEM accumulators) followed
- * by the wide FP64 gate kernel; 0 the GEMM chain (features, one mma.sync
+ * by the wide FP64 gate kernel; 0 the GEMM chain (features, one tcgen05
  * GEMM per layer) followed by the same gate kernel. */
 NRG_API int nrg_surrogate_set_inference(nrg_chem* h, int fused);
 /* Network outputs (n x 16 fp32, normalised units) of the fused kernel for

@@ -87,6 +87,8 @@ SIGNATURES = {
     "nrg_chem_set_graph": (_I, [_VP, _I]),
     "nrg_chem_set_cell_order": (_I, [_VP, _I]),
     "nrg_chem_set_timing": (_I, [_VP, _I]),
+    "nrg_chem_set_eps": (_I, [_VP, _D]),
+    "nrg_surrogate_set_fallback_eps": (_I, [_VP, _D]),
     "nrg_chem_info": (_I, [_VP, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "nrg_chem_tables": (_I, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "nrg_chem_species_name": (_I, [_VP, _I, ctypes.c_char_p, _I]),
@@ -348,6 +350,10 @@ class ChemicalKineticsSolver:
         """Generated mechanism-specialised RHS / iteration matrix (default when
         the mechanism matches) or the table-driven loops."""
         _check(lib().nrg_chem_set_specialised(self._h, int(enable)), self._h)
+
+    def set_eps(self, eps: float = 0.0) -> None:
+        """Integrator tolerance EPS (0: the reference's 1e-9)."""
+        _check(lib().nrg_chem_set_eps(self._h, float(eps)), self._h)
 
     def set_timing(self, enable: bool) -> None:
         _check(lib().nrg_chem_set_timing(self._h, int(enable)), self._h)

@@ -8,8 +8,16 @@
 #include <climits>
 #include <cmath>
 #include <cstring>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <functional>
 #include <mutex>
 #include <thread>
+#include <unistd.h>
+#if defined(__SSE2__)
+#include <emmintrin.h>
+#endif
 #include <string>
 #include <vector>
 
@@ -46,6 +54,8 @@ struct nrg_chem {
   int mode = NRG_MODE_FAST;
   LaunchCfg cfg;
   bool use_graph = true;
+  double eps = 0.0;           // integrator tolerance override (0: the reference's EPS)
+  double fallback_eps = 0.0;  // tolerance of the surrogate's FP64 fallback (0: eps)
   bool timing = false;
   cudaEvent_t ph[4] = {nullptr, nullptr, nullptr, nullptr};
   int* d_queue = nullptr;
@@ -63,6 +73,12 @@ struct nrg_chem {
          *h_Ef = nullptr;
   int8_t* h_bc = nullptr;
   uint8_t* h_status = nullptr;
+  // host path, surrogate mode: the rejected cells' outputs packed in cell
+  // order for the read-back after the fallback (surrogate_pack_rejected)
+  size_t pk_cap = 0;
+  int *d_pk_idx = nullptr, *d_pk_count = nullptr, *h_pk_idx = nullptr, *h_pk_count = nullptr;
+  double *d_pk_vals = nullptr, *h_pk_vals = nullptr;
+  uint8_t *d_pk_st = nullptr, *h_pk_st = nullptr;
   // temperature order of the plain integrator's cells (order.hpp)
   bool order_cells = true;
   long order_cap = 0;
@@ -274,24 +290,187 @@ void free_staging(nrg_chem* h) {
   h->d_bc = h->h_bc = nullptr;
   h->d_status = h->h_status = nullptr;
   h->cap = 0;
+  cudaFree(h->d_pk_idx); cudaFree(h->d_pk_count); cudaFree(h->d_pk_vals); cudaFree(h->d_pk_st);
+  cudaFreeHost(h->h_pk_idx); cudaFreeHost(h->h_pk_count); cudaFreeHost(h->h_pk_vals); cudaFreeHost(h->h_pk_st);
+  h->d_pk_idx = h->d_pk_count = h->h_pk_idx = h->h_pk_count = nullptr;
+  h->d_pk_vals = h->h_pk_vals = nullptr;
+  h->d_pk_st = h->h_pk_st = nullptr;
+  h->pk_cap = 0;
 }
 
-// Runs f(r) for every r in [r0, r1) on the host's hardware threads (contiguous
-// blocks of rows per thread).
+int ensure_pack(nrg_chem* h, size_t n) {
+  if (n <= h->pk_cap) return NRG_OK;
+  const size_t N = (size_t)h->mech.n();
+  CK(h, cudaMalloc(&h->d_pk_idx, n * 4));
+  CK(h, cudaMalloc(&h->d_pk_count, 4));
+  CK(h, cudaMalloc(&h->d_pk_vals, (N + 1) * n * 8));
+  CK(h, cudaMalloc(&h->d_pk_st, n));
+  CK(h, cudaMallocHost(&h->h_pk_idx, n * 4));
+  CK(h, cudaMallocHost(&h->h_pk_count, 4));
+  CK(h, cudaMallocHost(&h->h_pk_vals, (N + 1) * n * 8));
+  CK(h, cudaMallocHost(&h->h_pk_st, n));
+  h->pk_cap = n;
+  return NRG_OK;
+}
+
+// Host threads for the gather and scatter of the host path: started once per
+// process and kept (a step runs up to 16 parallel loops; starting threads for
+// each cost more than the loops' own work on small chunks).  run(nt, f) calls
+// f(0..nt-1) on the workers and the calling thread and returns when all are
+// done; calls from several host threads are serialised.  A child process
+// made by fork() starts its own pool (the parent's workers do not exist
+// there).  The pool is never destroyed: its workers wait on a condition
+// variable until the process ends.
+class HostPool {
+ public:
+  static HostPool& get() {
+    static std::mutex mu;
+    static HostPool* pool = nullptr;
+    static pid_t owner = 0;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!pool || owner != getpid()) {
+      pool = new HostPool();
+      owner = getpid();
+    }
+    return *pool;
+  }
+  long size() const { return (long)workers_.size() + 1; }
+  void run(long nt, const std::function<void(long)>& f) {
+    if (nt <= 0) return;
+    std::lock_guard<std::mutex> run_lk(run_mu_);
+    if (workers_.empty() || nt == 1) {
+      for (long i = 0; i < nt; ++i) f(i);
+      return;
+    }
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      job_ = &f;
+      ntasks_ = nt;
+      next_.store(0);
+      busy_ = (long)workers_.size();
+      ++gen_;
+    }
+    cv_.notify_all();
+    work();
+    std::unique_lock<std::mutex> lk(mu_);
+    done_.wait(lk, [&] { return busy_ == 0; });
+    job_ = nullptr;
+  }
+
+ private:
+  HostPool() {
+    const unsigned hw = std::thread::hardware_concurrency();
+    const long nw = std::max(0L, std::min(31L, (long)hw - 1));
+    for (long i = 0; i < nw; ++i) {
+      workers_.emplace_back([this] {
+        unsigned long long seen = 0;
+        for (;;) {
+          {
+            std::unique_lock<std::mutex> lk(mu_);
+            cv_.wait(lk, [&] { return gen_ != seen; });
+            seen = gen_;
+          }
+          work();
+          std::lock_guard<std::mutex> lk(mu_);
+          if (--busy_ == 0) done_.notify_one();
+        }
+      });
+      workers_.back().detach();
+    }
+  }
+  void work() {
+    for (;;) {
+      const long i = next_.fetch_add(1);
+      if (i >= ntasks_) break;
+      (*job_)(i);
+    }
+  }
+  std::mutex run_mu_, mu_;
+  std::condition_variable cv_, done_;
+  std::vector<std::thread> workers_;
+  const std::function<void(long)>* job_ = nullptr;
+  long ntasks_ = 0, busy_ = 0;
+  std::atomic<long> next_{0};
+  unsigned long long gen_ = 0;
+};
+
+// Runs f(i) for every i in [r0, r1) on the host's hardware threads
+// (contiguous blocks of indices per task).  Each task ends with a store
+// fence, so the streaming stores below are visible before the loop returns
+// (and before a copy engine reads what they wrote).
 template <class F>
 void parallel_rows(long r0, long r1, F f) {
   const long n = r1 - r0;
   if (n <= 0) return;
-  long T = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-  T = std::min(T, n);
-  auto body = [&](long t) {
+  HostPool& pool = HostPool::get();
+  const long T = std::min(pool.size(), n);
+  pool.run(T, [&](long t) {
     for (long r = r0 + n * t / T; r < r0 + n * (t + 1) / T; ++r) f(r);
-  };
-  std::vector<std::thread> th;
-  th.reserve((size_t)T - 1);
-  for (long t = 1; t < T; ++t) th.emplace_back(body, t);
-  body(0);
-  for (std::thread& x : th) x.join();
+#if defined(__SSE2__)
+    _mm_sfence();
+#endif
+  });
+}
+
+// The host path's gather and scatter are bound by host memory bandwidth.
+// Destinations that are written whole go through streaming (non-temporal)
+// stores: a plain store first reads the destination's cache line, a third
+// more traffic on a copy.
+inline void stream_copy(double* dst, const double* src, long n) {
+#if defined(__SSE2__)
+  long i = 0;
+  if (n > 0 && ((uintptr_t)dst & 15) != 0) {
+    dst[0] = src[0];
+    i = 1;
+  }
+  for (; i + 1 < n; i += 2) _mm_stream_pd(dst + i, _mm_loadu_pd(src + i));
+  if (i < n) dst[i] = src[i];
+#else
+  std::memcpy(dst, src, (size_t)n * 8);
+#endif
+}
+
+// y2[i] = src[i] in the cells the step did not skip (the reference leaves
+// Y_prod2 as it was in skipped cells); streaming stores where both cells of
+// an aligned pair are written.
+inline void masked_y_prod2(double* y2, const double* src, const uint8_t* st, long n) {
+#if defined(__SSE2__)
+  long i = 0;
+  if (n > 0 && ((uintptr_t)y2 & 15) != 0) {
+    if (st[0] != NRG_CELL_SKIPPED) y2[0] = src[0];
+    i = 1;
+  }
+  for (; i + 1 < n; i += 2) {
+    const bool a = st[i] != NRG_CELL_SKIPPED, b = st[i + 1] != NRG_CELL_SKIPPED;
+    if (a && b) {
+      _mm_stream_pd(y2 + i, _mm_loadu_pd(src + i));
+    } else {
+      if (a) y2[i] = src[i];
+      if (b) y2[i + 1] = src[i + 1];
+    }
+  }
+  if (i < n && st[i] != NRG_CELL_SKIPPED) y2[i] = src[i];
+#else
+  for (long i = 0; i < n; ++i)
+    if (st[i] != NRG_CELL_SKIPPED) y2[i] = src[i];
+#endif
+}
+
+// yp[i] = Y_prod2 W / dt (the two IEEE operations the kernels evaluate), 0 in
+// skipped cells.
+inline void stream_y_prod(double* yp, const double* y2, const uint8_t* st, long n, double W, double dt) {
+  auto v = [&](long i) { return st[i] == NRG_CELL_SKIPPED ? 0.0 : y2[i] * W / dt; };
+#if defined(__SSE2__)
+  long i = 0;
+  if (n > 0 && ((uintptr_t)yp & 15) != 0) {
+    yp[0] = v(0);
+    i = 1;
+  }
+  for (; i + 1 < n; i += 2) _mm_stream_pd(yp + i, _mm_set_pd(v(i + 1), v(i)));
+  if (i < n) yp[i] = v(i);
+#else
+  for (long i = 0; i < n; ++i) yp[i] = v(i);
+#endif
 }
 
 int ensure_staging(nrg_chem* h, size_t n) {
@@ -330,6 +509,7 @@ cudaError_t enqueue_integrator(nrg_chem* h, const StepArgs& a, const LaunchCfg& 
   LaunchCfg c = cfg;
   if (c.kernel == nrg::kKernelThreadQueue && c.grid <= 0) c.grid = h->num_sms;
   StepArgs b = a;
+  b.eps = a.eps > 0.0 ? a.eps : h->eps;
   // a whole field with one dt: its cells in temperature order (lanes of a
   // warp then take similar BDF paths); lists built by the caller and the
   // per-cell-dt training states keep their own order
@@ -345,6 +525,19 @@ cudaError_t enqueue_integrator(nrg_chem* h, const StepArgs& a, const LaunchCfg& 
                           h->d_queue, h->d_counters, s);
 }
 
+// The surrogate's FP64 fallback: the plain integrator at the fallback
+// tolerance on the rejected cells' list.
+nrg::FallbackFn integrator_fallback(nrg_chem* h, cudaEvent_t* ph) {
+  return [h, ph](const StepArgs& fa, cudaStream_t fs) {
+    if (ph) cudaEventRecord(ph[2], fs);
+    StepArgs fb = fa;
+    fb.eps = h->fallback_eps;
+    cudaError_t e = enqueue_integrator(h, fb, h->cfg, fs);
+    if (ph) cudaEventRecord(ph[3], fs);
+    return e;
+  };
+}
+
 // The step's kernels on stream s, adding to the device counters; ph: the
 // phase events (or nullptr).
 cudaError_t enqueue_step_body(nrg_chem* h, const StepArgs& a, cudaStream_t s, cudaEvent_t* ph) {
@@ -356,14 +549,7 @@ cudaError_t enqueue_step_body(nrg_chem* h, const StepArgs& a, cudaStream_t s, cu
     return e;
   }
   if (h->mode == NRG_MODE_SURROGATE)
-    return nrg::surrogate_step(h->sur_net, a, h->cfg, h->d_queue, h->d_counters, s,
-                               [h, ph](const StepArgs& fa, cudaStream_t fs) {
-                                 if (ph) cudaEventRecord(ph[2], fs);
-                                 LaunchCfg c = h->cfg;
-                                 cudaError_t e = enqueue_integrator(h, fa, c, fs);
-                                 if (ph) cudaEventRecord(ph[3], fs);
-                                 return e;
-                               },
+    return nrg::surrogate_step(h->sur_net, a, h->cfg, h->d_queue, h->d_counters, s, integrator_fallback(h, ph),
                                ph);
   if (ph) cudaEventRecord(ph[2], s);
   cudaError_t e2 = enqueue_integrator(h, a, h->cfg, s);
@@ -441,7 +627,7 @@ int step_prepare(nrg_chem* h, long n) {
 
 // After the step's work was queued on s between h->ev0 and h->ev1: waits for
 // it, fills stats (may be NULL) and checks the surrogate's error word.
-int step_finish(nrg_chem* h, cudaStream_t s, long n, nrg_chem_stats* stats) {
+int step_finish(nrg_chem* h, cudaStream_t s, long n, nrg_chem_stats* stats, bool phases = true) {
   CK(h, cudaMemcpyAsync(h->h_counters, h->d_counters, sizeof(unsigned long long) * 8,
                         cudaMemcpyDeviceToHost, s));
   CK(h, cudaStreamSynchronize(s));
@@ -460,7 +646,7 @@ int step_finish(nrg_chem* h, cudaStream_t s, long n, nrg_chem_stats* stats) {
     stats->cells_fallback = (long long)h->h_counters[7];
     if (h->mode == NRG_MODE_SURROGATE) stats->cells_active += stats->cells_surrogate;
     stats->device_ms = ms;
-    if (h->timing) {
+    if (h->timing && phases) {
       float p = 0.f;
       if (h->mode == NRG_MODE_SURROGATE) {
         cudaEventElapsedTime(&p, h->ev0, h->ph[1]);  // features + MLP (ph[1] = gate start)
@@ -658,6 +844,13 @@ extern "C" int nrg_chem_set_cell_order(nrg_chem* h, int enable) {
   return NRG_OK;
 }
 
+extern "C" int nrg_chem_set_eps(nrg_chem* h, double eps) {
+  if (!h) return NRG_ERR_ARG;
+  if (!(eps >= 0.0) || !(eps < 1.0)) return fail(h, NRG_ERR_ARG, "eps must be in [0, 1); 0 restores the reference's 1e-9");
+  h->eps = eps;
+  return NRG_OK;
+}
+
 extern "C" int nrg_chem_set_timing(nrg_chem* h, int enable) {
   if (!h) return NRG_ERR_ARG;
   h->timing = enable != 0;
@@ -736,13 +929,27 @@ extern "C" int nrg_chem_step(nrg_chem* h, double time_step, const nrg_field_desc
   }
   rc = step_prepare(h, n);
   if (rc) return rc;
+  const bool sur = h->mode == NRG_MODE_SURROGATE, table = h->mode == NRG_MODE_TABLE;
+  if (sur && (rc = ensure_pack(h, (size_t)n))) return rc;
   // The interior is handled as rows along i (contiguous in the reference's
-  // column-major arrays), split into up to eight chunks of rows.  Per chunk:
-  // gather on all host threads into pinned staging, H2D on copy_in, the step
-  // on the compute stream, D2H on copy_out, scatter on all host threads.  The
-  // host gathers chunk p + 1 while chunk p is copied and stepped, copy_in runs
-  // ahead of the steps, and chunk p is copied out and scattered while later
-  // chunks are stepped.
+  // column-major arrays), split into up to eight chunks of rows.  Per chunk
+  // the host gathers on all its threads into pinned staging and copies in on
+  // copy_in; the host gathers chunk p + 1 while chunk p is copied.
+  // * integrator and table modes: each chunk is stepped as it arrives,
+  //   copied out on copy_out and scattered while later chunks are stepped
+  //   (on the 2048 x 2048 flame field this beats one launch over the whole
+  //   field after the last chunk: 90 against 96 ms);
+  // * surrogate mode: each chunk goes through the networks and the gate as
+  //   it arrives (its accepted and skipped cells are then final) and is
+  //   copied out and scattered while later chunks arrive.  The FP64
+  //   fallback runs twice, on the rejected cells of the first half of the
+  //   chunks (while the host gathers the second half) and on those of the
+  //   second half (two launches: each pays the integrator's tail of slow
+  //   cells once); the rejected cells' outputs alone are then packed,
+  //   copied out and scattered.
+  // Every mode but the table writes Y_prod = Y_prod2 W / dt: only Y_prod2
+  // crosses PCIe and the host rebuilds Y_prod with the same two operations.
+  const bool derive_yp = !table;
   const long rowlen = cnt[0], nrow = cnt[1] * cnt[2];
   auto row_base = [&](long r) {
     const int j = f->lo[1] + (int)(r % cnt[1]), k = f->lo[2] + (int)(r / cnt[1]);
@@ -756,29 +963,7 @@ extern "C" int nrg_chem_step(nrg_chem* h, double time_step, const nrg_field_desc
     *c0 = r0 * rowlen;
     *nc = (r1 - r0) * rowlen;
   };
-  CK(h, cudaMemsetAsync(h->d_counters, 0, sizeof(unsigned long long) * 8, s));
-  CK(h, cudaEventRecord(h->ev0, s));
-  for (int p = 0; p < P; ++p) {
-    long c0, nc;
-    chunk_cells(p, &c0, &nc);
-    parallel_rows(nrow * p / P, nrow * (p + 1) / P, [&](long r) {
-      const long L = row_base(r), c = r * rowlen;
-      std::memcpy(h->h_T + c, f->T + L, rb);
-      std::memcpy(h->h_rho + c, f->rho + L, rb);
-      if (f->bc_markers)
-        std::memcpy(h->h_bc + c, f->bc_markers + L, (size_t)rowlen);
-      else
-        std::memset(h->h_bc + c, 0, (size_t)rowlen);
-      for (int sp = 0; sp < N; ++sp) std::memcpy(h->h_Y + (size_t)sp * n + c, f->Y[sp] + L, rb);
-    });
-    CK(h, cudaMemcpyAsync(h->d_T + c0, h->h_T + c0, nc * 8, cudaMemcpyHostToDevice, ci));
-    CK(h, cudaMemcpyAsync(h->d_rho + c0, h->h_rho + c0, nc * 8, cudaMemcpyHostToDevice, ci));
-    CK(h, cudaMemcpyAsync(h->d_bc + c0, h->h_bc + c0, nc, cudaMemcpyHostToDevice, ci));
-    for (int sp = 0; sp < N; ++sp)
-      CK(h, cudaMemcpyAsync(h->d_Y + (size_t)sp * n + c0, h->h_Y + (size_t)sp * n + c0, nc * 8,
-                            cudaMemcpyHostToDevice, ci));
-    CK(h, cudaEventRecord(h->ev_h2d[p], ci));
-    CK(h, cudaStreamWaitEvent(s, h->ev_h2d[p], 0));
+  auto args_of = [&](long c0, long nc) {
     StepArgs a;
     a.n = nc;
     a.ld = n;
@@ -798,36 +983,136 @@ extern "C" int nrg_chem_step(nrg_chem* h, double time_step, const nrg_field_desc
     a.cell_list = nullptr;
     a.n_list = 0;
     a.n_list_dev = nullptr;
-    const cudaError_t e = enqueue_step_body(h, a, s, nullptr);
-    if (e != cudaSuccess) return cuda_fail(h, e, "enqueue_step");
-    CK(h, cudaEventRecord(h->ev_step[p], s));
-    CK(h, cudaStreamWaitEvent(co, h->ev_step[p], 0));
+    return a;
+  };
+  // chunk p's outputs back to the host once event `ready` has fired on s
+  auto copy_out = [&](int p, cudaEvent_t ready) -> int {
+    long c0, nc;
+    chunk_cells(p, &c0, &nc);
+    CK(h, cudaStreamWaitEvent(co, ready, 0));
     for (int sp = 0; sp < N; ++sp) {
-      CK(h, cudaMemcpyAsync(h->h_Yp + (size_t)sp * n + c0, h->d_Yp + (size_t)sp * n + c0, nc * 8,
-                            cudaMemcpyDeviceToHost, co));
+      if (!derive_yp)
+        CK(h, cudaMemcpyAsync(h->h_Yp + (size_t)sp * n + c0, h->d_Yp + (size_t)sp * n + c0, nc * 8,
+                              cudaMemcpyDeviceToHost, co));
       CK(h, cudaMemcpyAsync(h->h_Yp2 + (size_t)sp * n + c0, h->d_Yp2 + (size_t)sp * n + c0, nc * 8,
                             cudaMemcpyDeviceToHost, co));
     }
     CK(h, cudaMemcpyAsync(h->h_Ef + c0, h->d_Ef + c0, nc * 8, cudaMemcpyDeviceToHost, co));
     CK(h, cudaMemcpyAsync(h->h_status + c0, h->d_status + c0, nc, cudaMemcpyDeviceToHost, co));
     CK(h, cudaEventRecord(h->ev_chunk[p], co));
+    return NRG_OK;
+  };
+  using clk = std::chrono::steady_clock;
+  auto ms_since = [](clk::time_point t0) { return std::chrono::duration<double, std::milli>(clk::now() - t0).count(); };
+  const clk::time_point t_call = clk::now();
+  double host_ms[3] = {0.0, 0.0, 0.0};  // gather, chunk scatter (with its waits), rejected cells' read-back
+  CK(h, cudaMemsetAsync(h->d_counters, 0, sizeof(unsigned long long) * 8, s));
+  CK(h, cudaEventRecord(h->ev0, s));
+  for (int p = 0; p < P; ++p) {
+    long c0, nc;
+    chunk_cells(p, &c0, &nc);
+    const clk::time_point tg = clk::now();
+    parallel_rows(nrow * p / P, nrow * (p + 1) / P, [&](long r) {
+      const long L = row_base(r), c = r * rowlen;
+      stream_copy(h->h_T + c, f->T + L, rowlen);
+      stream_copy(h->h_rho + c, f->rho + L, rowlen);
+      if (f->bc_markers)
+        std::memcpy(h->h_bc + c, f->bc_markers + L, (size_t)rowlen);
+      else
+        std::memset(h->h_bc + c, 0, (size_t)rowlen);
+      for (int sp = 0; sp < N; ++sp) stream_copy(h->h_Y + (size_t)sp * n + c, f->Y[sp] + L, rowlen);
+    });
+    host_ms[0] += ms_since(tg);
+    CK(h, cudaMemcpyAsync(h->d_T + c0, h->h_T + c0, nc * 8, cudaMemcpyHostToDevice, ci));
+    CK(h, cudaMemcpyAsync(h->d_rho + c0, h->h_rho + c0, nc * 8, cudaMemcpyHostToDevice, ci));
+    CK(h, cudaMemcpyAsync(h->d_bc + c0, h->h_bc + c0, nc, cudaMemcpyHostToDevice, ci));
+    for (int sp = 0; sp < N; ++sp)
+      CK(h, cudaMemcpyAsync(h->d_Y + (size_t)sp * n + c0, h->h_Y + (size_t)sp * n + c0, nc * 8,
+                            cudaMemcpyHostToDevice, ci));
+    CK(h, cudaEventRecord(h->ev_h2d[p], ci));
+    CK(h, cudaStreamWaitEvent(s, h->ev_h2d[p], 0));
+    const cudaError_t e = sur ? nrg::surrogate_gate(h->sur_net, args_of(c0, nc), c0, h->d_counters, s, nullptr)
+                              : enqueue_step_body(h, args_of(c0, nc), s, nullptr);
+    if (e != cudaSuccess) return cuda_fail(h, e, sur ? "surrogate_gate" : "enqueue_step");
+    CK(h, cudaEventRecord(h->ev_step[p], s));
+    if ((rc = copy_out(p, h->ev_step[p]))) return rc;
+    if (sur && (p == P / 2 - 1 || p == P - 1)) {
+      // the rejected cells of the chunks since the last fallback: the first
+      // half's run while the host still gathers and copies in the second
+      const int p0 = p == P - 1 && P / 2 >= 1 ? P / 2 : 0;
+      long f0, fn, l0, ln;
+      chunk_cells(p0, &f0, &fn);
+      chunk_cells(p, &l0, &ln);
+      const cudaError_t ef = nrg::surrogate_fallback(h->sur_net, args_of(f0, l0 + ln - f0), f0, h->d_counters, s,
+                                                     integrator_fallback(h, nullptr));
+      if (ef != cudaSuccess) return cuda_fail(h, ef, "surrogate_fallback");
+    }
+  }
+  if (sur) {
+    cudaError_t e = nrg::surrogate_pack_rejected(h->sur_net[0], n, N, n, h->d_Yp2, h->d_Ef, h->d_status, h->d_pk_idx,
+                                     h->d_pk_count, h->d_pk_vals, h->d_pk_st, s);
+    if (e != cudaSuccess) return cuda_fail(h, e, "surrogate_pack_rejected");
+    CK(h, cudaMemcpyAsync(h->h_pk_count, h->d_pk_count, 4, cudaMemcpyDeviceToHost, s));
   }
   CK(h, cudaEventRecord(h->ev1, s));
+  const double* W = h->mech.molar_mass.data();
+  const clk::time_point ts = clk::now();
   for (int p = 0; p < P; ++p) {
     CK(h, cudaEventSynchronize(h->ev_chunk[p]));
     parallel_rows(nrow * p / P, nrow * (p + 1) / P, [&](long r) {
       const long L = row_base(r), c = r * rowlen;
-      std::memcpy(f->E_f_prod + L, h->h_Ef + c, rb);
+      stream_copy(f->E_f_prod + L, h->h_Ef + c, rowlen);
+      const uint8_t* stc = h->h_status + c;
       for (int sp = 0; sp < N; ++sp) {
-        std::memcpy(f->Y_prod[sp] + L, h->h_Yp + (size_t)sp * n + c, rb);
         double* y2 = f->Y_prod2[sp] + L;
         const double* src = h->h_Yp2 + (size_t)sp * n + c;
-        for (long i = 0; i < rowlen; ++i)
-          if (h->h_status[c + i] != NRG_CELL_SKIPPED) y2[i] = src[i];  // the reference leaves it in skipped cells
+        if (derive_yp) {
+          stream_y_prod(f->Y_prod[sp] + L, src, stc, rowlen, W[sp], time_step);
+          masked_y_prod2(y2, src, stc, rowlen);
+        } else {
+          std::memcpy(f->Y_prod[sp] + L, h->h_Yp + (size_t)sp * n + c, rb);
+          for (long i = 0; i < rowlen; ++i)
+            if (stc[i] != NRG_CELL_SKIPPED) y2[i] = src[i];
+        }
       }
     });
   }
-  return step_finish(h, s, n, stats);
+  host_ms[1] = ms_since(ts);
+  const clk::time_point tr = clk::now();
+  if (sur) {
+    // the rejected cells' outputs (the chunks carried their values before
+    // the fallback): read back packed, scattered over the chunks' values
+    CK(h, cudaEventSynchronize(h->ev1));
+    const long m = *h->h_pk_count;
+    if (m < 0 || m > n) return fail(h, NRG_ERR_CUDA, "rejected-cell count out of range");
+    if (m > 0) {
+      CK(h, cudaMemcpyAsync(h->h_pk_idx, h->d_pk_idx, (size_t)m * 4, cudaMemcpyDeviceToHost, s));
+      CK(h, cudaMemcpyAsync(h->h_pk_vals, h->d_pk_vals, (size_t)m * (N + 1) * 8, cudaMemcpyDeviceToHost, s));
+      CK(h, cudaMemcpyAsync(h->h_pk_st, h->d_pk_st, (size_t)m, cudaMemcpyDeviceToHost, s));
+      CK(h, cudaStreamSynchronize(s));
+      const long tasks = std::min<long>(HostPool::get().size() * 4, m);
+      parallel_rows(0, tasks, [&](long t) {
+        for (long j = m * t / tasks; j < m * (t + 1) / tasks; ++j) {
+          const long c = h->h_pk_idx[j];
+          const long L = row_base(c / rowlen) + c % rowlen;
+          const bool skip = h->h_pk_st[j] == NRG_CELL_SKIPPED;
+          f->E_f_prod[L] = h->h_pk_vals[(size_t)N * m + j];
+          for (int sp = 0; sp < N; ++sp) {
+            const double v = h->h_pk_vals[(size_t)sp * m + j];
+            f->Y_prod[sp][L] = skip ? 0.0 : v * W[sp] / time_step;
+            if (!skip) f->Y_prod2[sp][L] = v;
+          }
+        }
+      });
+    }
+  }
+  host_ms[2] = ms_since(tr);
+  rc = step_finish(h, s, n, stats, false);  // host times instead of the phase events
+  if (rc == NRG_OK && stats && h->timing) {
+    for (int i = 0; i < 3; ++i) stats->phase_ms[i] = host_ms[i];
+    stats->phase_ms[3] = ms_since(t_call);
+  }
+  return rc;
 }
 
 extern "C" int nrg_chem_autotune(nrg_chem* h, double time_step, long n, long ld, const double* T,
@@ -1376,6 +1661,13 @@ extern "C" int nrg_surrogate_set_partner(nrg_chem* h, int partner, double agree_
   if (partner < -1 || partner >= nrg::kMaxNets || partner == h->sur_sel || !(agree_Y >= 0) || !(agree_T >= 0))
     return fail(h, NRG_ERR_ARG, "partner must be -1 or another network (0..7), agreement bounds >= 0");
   nrg::surrogate_set_partner(h->sur_net[h->sur_sel], partner, agree_Y, agree_T);
+  return NRG_OK;
+}
+
+extern "C" int nrg_surrogate_set_fallback_eps(nrg_chem* h, double eps) {
+  if (!h) return NRG_ERR_ARG;
+  if (!(eps >= 0.0) || !(eps < 1.0)) return fail(h, NRG_ERR_ARG, "fallback eps must be in [0, 1)");
+  h->fallback_eps = eps;
   return NRG_OK;
 }
 

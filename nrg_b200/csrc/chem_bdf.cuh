@@ -1169,7 +1169,7 @@ __device__ bool cell_begin(CS& c, const StepArgs& a, long cid) {
   c.t = 0.0;
   const double h = (c.tout - c.t) * (1.0 - 4.0 * c_mech.uround);
   c.h = copysign(NRG_FMIN(fabs(h), c_mech.hmax), h);
-  c.eps = c_mech.eps;
+  c.eps = a.eps > 0.0 ? a.eps : c_mech.eps;
   c.jtask = 0;
   c.nstep = 0;
   c.nstepl = 0;

@@ -30,6 +30,7 @@ struct StepArgs {
   const int* cell_list;    // integrate only these cells (gated fallback); null: 0..n-1
   int n_list;              // number of entries in cell_list (grid bound when n_list_dev is set)
   const int* n_list_dev;   // device-side entry count of cell_list (may be null)
+  double eps = 0.0;        // relative tolerance of the integrator; 0: the mechanism's (the reference's 1e-9)
 };
 
 // Chemistry sources applied to the state, then the state equation.

@@ -672,7 +672,7 @@ __device__ bool warp_cell_begin(WarpCell<N, R, LUT>& c, const StepArgs& a, long 
   c.t = 0.0;
   const double h = (c.tout - c.t) * (1.0 - 4.0 * c.M->uround);
   c.h = copysign(NRG_FMIN(fabs(h), c.M->hmax), h);
-  c.eps = c.M->eps;
+  c.eps = a.eps > 0.0 ? a.eps : c.M->eps;
   c.jtask = 0;
   c.nstep = 0;
   c.nstepl = 0;

@@ -523,8 +523,11 @@ __device__ __forceinline__ bool gate_active_cell(const StepArgs& a, long c, doub
   if (!(fabs((T1 - T0) - dT_net) <= gc.dT_tol)) return false;
 #pragma unroll
   for (int k = 0; k < 9; ++k) {
-    a.Y_prod[k * a.ld + c] = dY[k] * rho_dt;
-    a.Y_prod2[k * a.ld + c] = dY[k] * rho * th.invW[k];
+    // the integrator's relation Y_prod = Y_prod2 W / dt, evaluated the same
+    // way, so that a host can rebuild Y_prod from Y_prod2 bit for bit
+    const double y2 = dY[k] * rho * th.invW[k];
+    a.Y_prod2[k * a.ld + c] = y2;
+    a.Y_prod[k * a.ld + c] = y2 * c_mech.W[k] / dt;
   }
   a.E_f_prod[c] = E;
   if (a.T_after) a.T_after[c] = T1;
@@ -1499,10 +1502,11 @@ static cudaError_t launch_tc(Surrogate* s, const TcArgs& p, cudaStream_t st) {
 
 // The FP64 gate over the n cells of a, in a grid of 128-thread blocks.
 static cudaError_t launch_gate(Surrogate* s, const StepArgs& a, const float* O, const float* OP, long o_ld,
-                               const GateNets& nets, unsigned long long* counters, cudaStream_t st) {
+                               const GateNets& nets, unsigned long long* counters, cudaStream_t st,
+                               unsigned char* flag) {
   const int sms = s->num_sms > 0 ? s->num_sms : 148;
   const long grid = std::min<long>((a.n + 127) / 128, (long)sms * 16);
-  k_gate<<<(unsigned)std::max<long>(grid, 1), 128, 0, st>>>(a, O, OP, o_ld, nets, s->flag, counters);
+  k_gate<<<(unsigned)std::max<long>(grid, 1), 128, 0, st>>>(a, O, OP, o_ld, nets, flag, counters);
   return cudaGetLastError();
 }
 
@@ -1536,15 +1540,13 @@ std::string surrogate_check(Surrogate* s, cudaStream_t st) {
 
 void surrogate_set_fused(Surrogate* s, bool fused) { s->fused = fused; }
 
-cudaError_t surrogate_step(Surrogate* const* nets_in, const StepArgs& a, const LaunchCfg& cfg, int* queue,
-                           unsigned long long* counters, cudaStream_t st, const FallbackFn& fallback,
-                           cudaEvent_t* ph) {
-  (void)cfg;
-  (void)queue;
+cudaError_t surrogate_gate(Surrogate* const* nets_in, const StepArgs& a, long flag_off,
+                           unsigned long long* counters, cudaStream_t st, cudaEvent_t* ph) {
   Surrogate* s = nets_in[0];
   // buffers are reserved by surrogate_reserve before any graph capture
-  if (a.n > s->gcap || (!s->fused && a.n > s->icap)) return cudaErrorMemoryAllocation;
+  if (flag_off < 0 || flag_off + a.n > s->gcap || (!s->fused && a.n > s->icap)) return cudaErrorMemoryAllocation;
   const long n = a.n;
+  unsigned char* flag = s->flag + flag_off;
   cudaError_t e;
   GateNets nets{};
   nets.net[0] = GateNet{s->d_norm, s->gate, -1e300, 1e300, 1};
@@ -1569,26 +1571,35 @@ cudaError_t surrogate_step(Surrogate* const* nets_in, const StepArgs& a, const L
       if ((e = launch_tc(nets_in[i], tc_args(nets_in[i], a, s->gO, n, 1, &nets, i, s->gP), st)) != cudaSuccess)
         return e;
     }
-    if ((e = launch_gate(s, a, s->gO, s->gP, n, nets, counters, st)) != cudaSuccess) return e;
-    if (ph) cudaEventRecord(ph[1], st);
+    if ((e = launch_gate(s, a, s->gO, s->gP, n, nets, counters, st, flag)) != cudaSuccess) return e;
   } else {
     k_features<<<std::min<long>((n + 255) / 256, 148 * 16), 256, 0, st>>>(n, a.ld, a.dt, a.dt_cells, a.T, a.rho,
                                                                         a.Y, s->d_norm, nullptr, s->iX);
     if ((e = forward_infer(s, n, s->iX, s->iO, st)) != cudaSuccess) return e;
-    if ((e = launch_gate(s, a, s->iO, nullptr, 0, nets, counters, st)) != cudaSuccess) return e;
-    if (ph) cudaEventRecord(ph[1], st);
+    if ((e = launch_gate(s, a, s->iO, nullptr, 0, nets, counters, st, flag)) != cudaSuccess) return e;
   }
+  if (ph) cudaEventRecord(ph[1], st);
+  return cudaSuccess;
+}
+
+cudaError_t surrogate_fallback(Surrogate* const* nets_in, const StepArgs& a, long flag_off,
+                               unsigned long long* counters, cudaStream_t st, const FallbackFn& fallback) {
+  Surrogate* s = nets_in[0];
+  if (flag_off < 0 || flag_off + a.n > s->gcap) return cudaErrorMemoryAllocation;
+  const long n = a.n;
+  const unsigned char* flag = s->flag + flag_off;
+  cudaError_t e;
   if (s->order_cells) {
     // rejected cells grouped by temperature: the fallback's warps then hold
     // cells with similar BDF paths
-    if ((e = order_cells_by_temperature(n, a.T, a.bc, s->flag, &s->order, s->list, s->n_list,
+    if ((e = order_cells_by_temperature(n, a.T, a.bc, flag, &s->order, s->list, s->n_list,
                                         counters ? counters + 7 : nullptr, st)) != cudaSuccess)
       return e;
   } else {
     const int nb = (int)((n + kCompactBlock - 1) / kCompactBlock);
-    k_flag_count<<<nb, kCompactBlock, 0, st>>>(n, s->flag, s->block_count);
+    k_flag_count<<<nb, kCompactBlock, 0, st>>>(n, flag, s->block_count);
     k_scan_counts<<<1, 1024, 0, st>>>(nb, s->block_count, s->block_off, s->n_list, counters);
-    k_compact<<<nb, kCompactBlock, 0, st>>>(n, s->flag, s->block_off, s->list);
+    k_compact<<<nb, kCompactBlock, 0, st>>>(n, flag, s->block_off, s->list);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   StepArgs fa = a;
@@ -1596,6 +1607,43 @@ cudaError_t surrogate_step(Surrogate* const* nets_in, const StepArgs& a, const L
   fa.n_list_dev = s->n_list;
   fa.n_list = (int)n;  // upper bound for the grid; the kernel reads the device count
   return fallback(fa, st);
+}
+
+cudaError_t surrogate_step(Surrogate* const* nets_in, const StepArgs& a, const LaunchCfg& cfg, int* queue,
+                           unsigned long long* counters, cudaStream_t st, const FallbackFn& fallback,
+                           cudaEvent_t* ph) {
+  (void)cfg;
+  (void)queue;
+  cudaError_t e = surrogate_gate(nets_in, a, 0, counters, st, ph);
+  if (e != cudaSuccess) return e;
+  return surrogate_fallback(nets_in, a, 0, counters, st, fallback);
+}
+
+// The rejected cells' outputs, packed in cell order: idx[j] the cell, then
+// vals[k * m + j] = Y_prod2_k and vals[N * m + j] = E_f_prod, st_out[j] the
+// status, m = *count the number of rejected cells.
+__global__ void k_pack_rejected(int N, long ld, const int* idx, const int* count, const double* Yp2,
+                                const double* Ef, const uint8_t* status, double* vals, uint8_t* st_out) {
+  const long m = *count;
+  for (long j = blockIdx.x * (long)blockDim.x + threadIdx.x; j < m; j += (long)gridDim.x * blockDim.x) {
+    const long c = idx[j];
+    for (int k = 0; k < N; ++k) vals[k * m + j] = Yp2[k * ld + c];
+    vals[N * m + j] = Ef[c];
+    st_out[j] = status[c];
+  }
+}
+
+cudaError_t surrogate_pack_rejected(Surrogate* s, long n, int N, long ld, const double* Yp2, const double* Ef,
+                                    const uint8_t* status, int* idx, int* count, double* vals, uint8_t* st_out,
+                                    cudaStream_t st) {
+  if (n > s->gcap) return cudaErrorMemoryAllocation;
+  const int nb = (int)((n + kCompactBlock - 1) / kCompactBlock);
+  k_flag_count<<<nb, kCompactBlock, 0, st>>>(n, s->flag, s->block_count);
+  k_scan_counts<<<1, 1024, 0, st>>>(nb, s->block_count, s->block_off, count, nullptr);
+  k_compact<<<nb, kCompactBlock, 0, st>>>(n, s->flag, s->block_off, idx);
+  const int sms = s->num_sms > 0 ? s->num_sms : 148;
+  k_pack_rejected<<<sms * 8, 256, 0, st>>>(N, ld, idx, count, Yp2, Ef, status, vals, st_out);
+  return cudaGetLastError();
 }
 
 // Bounded-wait probe: one warp waits on an mbarrier that nothing arrives at,

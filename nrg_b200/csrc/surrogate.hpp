@@ -45,6 +45,24 @@ std::string bounded_wait_probe(unsigned long long limit_ns, int* timed_out, doub
 cudaError_t surrogate_step(Surrogate* const* nets, const StepArgs& a, const LaunchCfg& cfg, int* queue,
                            unsigned long long* counters, cudaStream_t st, const FallbackFn& fallback,
                            cudaEvent_t* ph);
+// The two halves of surrogate_step, for callers that stream a field in
+// chunks: surrogate_gate runs the networks and the gate on a.n cells whose
+// accept/reject flags go to positions [flag_off, flag_off + a.n) of the
+// step's flag array (accepted and skipped cells are final after it);
+// surrogate_fallback then integrates the a.n cells at a's pointers whose
+// flags sit at [flag_off, flag_off + a.n) and were set by surrogate_gate
+// calls before it.
+cudaError_t surrogate_gate(Surrogate* const* nets, const StepArgs& a, long flag_off,
+                           unsigned long long* counters, cudaStream_t st, cudaEvent_t* ph);
+cudaError_t surrogate_fallback(Surrogate* const* nets, const StepArgs& a, long flag_off,
+                               unsigned long long* counters, cudaStream_t st, const FallbackFn& fallback);
+// After surrogate_fallback over n cells: the rejected cells' Y_prod2,
+// E_f_prod and status packed in cell order (idx[j], vals[k * m + j] for
+// species k, vals[N * m + j] for E_f_prod, st_out[j]; *count = m), so that a
+// host reads back only those cells.
+cudaError_t surrogate_pack_rejected(Surrogate* s, long n, int N, long ld, const double* Yp2, const double* Ef,
+                                    const uint8_t* status, int* idx, int* count, double* vals, uint8_t* st_out,
+                                    cudaStream_t st);
 
 // ---- training / inspection (device pointers unless stated)
 std::string surrogate_init(Surrogate* s, unsigned long long seed, cudaStream_t st);

@@ -17,6 +17,7 @@ import numpy as np
 import pytest
 
 from nrg_b200 import fields
+from nrg_b200.surrogate import FALLBACK_EPS
 from tests.gpu_util import dY, run_device
 
 pytestmark = pytest.mark.gpu
@@ -25,6 +26,9 @@ TOL_Y = 1e-9
 TOL_T = 1e-6
 SUR_TOL_T_K = 1.0
 SUR_TOL_Y = 1e-4
+# cells the gate rejects, integrated in FP64 at EPS 1e-5
+FALLBACK_TOL_Y = 1e-6
+FALLBACK_TOL_T_K = 0.01
 
 # (T_lo, T_hi, cells drawn) per band of the flame field
 FLAME_BANDS = [(0.0, 305.0, 2048), (305.0, 800.0, 8192), (800.0, 2380.0, 14336), (2380.0, 2399.9, 4096),
@@ -110,6 +114,78 @@ def test_flame_field_sample_surrogate_against_oracle(solver, flame, capsys):
             print(f"  band {lo:.0f}-{min(hi, 2400):.0f} K: {int((acc & b).sum())} of {int(b.sum())} accepted")
     assert dT.max() <= SUR_TOL_T_K, dT.max()
     assert e.max() <= SUR_TOL_Y, e
+    # the rejected cells, integrated at the fallback tolerance (1e-5)
+    fb = act & ~acc
+    assert fb.sum() > 0
+    assert np.abs(dY(g, f) - dY(o, f))[:, fb].max() <= FALLBACK_TOL_Y
+    assert np.abs(g["T_after"] - o["T_after"])[fb].max() <= FALLBACK_TOL_T_K
+
+
+def test_surrogate_fallback_at_the_reference_eps_gives_the_plain_bits(solver, flame):
+    """With the fallback at the reference's EPS (1e-9) the rejected cells are
+    the plain integrator's cells bit for bit; the accepted ones are the
+    network's either way."""
+    from nrg_b200.surrogate import load_default
+    f, _ = flame
+    plain, _ = run_device(solver, f, "fast")
+    nets = load_default(solver, fallback_eps=0.0)
+    try:
+        g, st = run_device(solver, f, "surrogate")
+    finally:
+        nets[0].set_fallback_eps(FALLBACK_EPS)
+    g5, _ = run_device(solver, f, "surrogate")
+    fb = (g["status"] != 5) & (g["status"] != 0)
+    assert fb.sum() > 0
+    for k in ("Y_prod", "Y_prod2"):
+        np.testing.assert_array_equal(g[k][:, fb], plain[k][:, fb])
+    for k in ("E_f_prod", "T_after", "status"):
+        np.testing.assert_array_equal(g[k][fb], plain[k][fb])
+    acc = g["status"] == 5
+    np.testing.assert_array_equal(g5["status"] == 5, acc)
+    np.testing.assert_array_equal(g5["Y_prod"][:, acc], g["Y_prod"][:, acc])
+
+
+def test_surrogate_host_layout_equals_the_device_step(decks, W):
+    """solve_chemical_kinetics in surrogate mode on Fortran-layout host arrays
+    (only Y_prod2 crosses PCIe; the host rebuilds Y_prod = Y_prod2 W / dt)
+    gives the device entry point's bits, skipped cells included."""
+    from nrg_b200.chemistry import ChemicalKineticsSolver, DataManager, chemical_kinetics_solver_c
+    from nrg_b200.surrogate import load_default
+    full = fields.flame_field(W)
+    nx, ny = 2048, 6
+    f = fields.slice_field(full, nx * ny, offset=1021 * 2048)
+    assert (f.T < 305.0).any() and (f.T > 2000.0).any()
+    m = DataManager.block(nx, ny)
+    for name in ("temperature", "pressure", "density"):
+        m.create_scalar_field(name)
+    Y = m.create_vector_field("specie_mass_fraction", 9)
+    m.interior(m.fields["temperature"])[...] = f.T.reshape(ny, nx).T[:, :, None]
+    m.interior(m.fields["density"])[...] = f.rho.reshape(ny, nx).T[:, :, None]
+    for k in range(9):
+        m.interior(Y[k])[...] = f.Y[k].reshape(ny, nx).T[:, :, None]
+    host = chemical_kinetics_solver_c(m, *decks)
+    for k in range(9):
+        m.fields["specie_production_chemistry2"][k][...] = -1.0
+    try:
+        load_default(host)
+        host.set_mode("surrogate")
+        st = host.solve_chemical_kinetics(f.dt)
+    finally:
+        host.close()
+    d = ChemicalKineticsSolver(None, *decks, mode="fast")
+    try:
+        load_default(d)
+        g, _ = run_device(d, f, "surrogate", y_prod2_init=np.full((9, f.n), -1.0))
+    finally:
+        d.close()
+    flat = lambda a: m.interior(a)[:, :, 0].T.reshape(-1)
+    yp = np.stack([flat(a) for a in m.fields["specie_production_chemistry"]])
+    yp2 = np.stack([flat(a) for a in m.fields["specie_production_chemistry2"]])
+    assert (g["status"] == 5).sum() > 0 and (g["status"] == 0).sum() > 0
+    np.testing.assert_array_equal(yp, g["Y_prod"])
+    np.testing.assert_array_equal(yp2, g["Y_prod2"])
+    np.testing.assert_array_equal(flat(m.fields["energy_production_chemistry"]), g["E_f_prod"])
+    assert st["cells"] == f.n
 
 
 @pytest.mark.parametrize("mode", ["reference", "fast"])

@@ -401,3 +401,35 @@ def test_host_layout_shapes_match_the_device_step(decks, W, shape):
     ghost = np.ones(m.shape, bool)
     ghost[tuple(slice(lo - l, hi - l + 1) for lo, hi, l in zip(m.lo, m.hi, m.lb))] = False
     assert np.all(m.fields["specie_production_chemistry2"][0][ghost] == -1.0)
+
+
+def test_integrator_eps_override_and_restore(solver, oracle_mech, W):
+    """nrg_chem_set_eps, in the warp-per-cell and the thread-per-cell
+    kernels: a looser EPS takes fewer BDF steps and stays within its own
+    bound of the oracle; 0 restores the reference's 1e-9 bits."""
+    f = fields.slice_field(fields.random_field(W), 2048)
+    for launch in (dict(kernel="warp_queue", block=256, grid=0, chunk=1), dict(kernel="thread", block=32)):
+        _check_eps(solver, oracle_mech, f, launch)
+
+
+def _check_eps(solver, oracle_mech, f, launch):
+    from nrg_b200.chemistry import NrgError
+    solver.set_launch(**launch)
+    base, st0 = run_device(solver, f, "fast")
+    try:
+        solver.set_eps(1e-5)
+        loose, st1 = run_device(solver, f, "fast")
+        with pytest.raises(NrgError):
+            solver.set_eps(-1.0)
+        with pytest.raises(NrgError):
+            solver.set_eps(1.5)
+    finally:
+        solver.set_eps(0.0)
+    again, _ = run_device(solver, f, "fast")
+    assert st1["steps"] < st0["steps"]
+    o = oracle_run(oracle_mech, f)
+    act = f.T >= 305.0
+    # the random field's states are harsher than the flame's: 1.3e-6 measured
+    assert np.abs(dY(loose, f) - dY(o, f))[:, act].max() <= 1e-5
+    for k in ("Y_prod", "Y_prod2", "E_f_prod", "T_after", "status"):
+        np.testing.assert_array_equal(again[k], base[k])
