@@ -355,6 +355,11 @@ class ChemicalKineticsSolver:
         """Integrator tolerance EPS (0: the reference's 1e-9)."""
         _check(lib().nrg_chem_set_eps(self._h, float(eps)), self._h)
 
+    def set_fallback_eps(self, eps: float = 0.0) -> None:
+        """Integrator tolerance of the surrogate's rejected cells (0: the
+        handle's EPS)."""
+        _check(lib().nrg_surrogate_set_fallback_eps(self._h, float(eps)), self._h)
+
     def set_timing(self, enable: bool) -> None:
         _check(lib().nrg_chem_set_timing(self._h, int(enable)), self._h)
 

@@ -658,6 +658,10 @@ struct TcArgs {
   GateNets routes;
   float* out_partner;
   unsigned int* err;  // bit 0: an MMA wait timed out
+  // when set: the kernel's cells are list[0 .. *list_count) (indices into a)
+  // instead of every cell of a
+  const int* list;
+  const int* list_count;
 };
 
 __device__ __forceinline__ uint4 pack8(const float* v) {
@@ -730,15 +734,17 @@ __global__ void __launch_bounds__(128 * kTcGroups, 1) k_mlp_tc(TcArgs p) {
   constexpr uint32_t kIdHid = tc::idesc_bf16_f32(128, 128), kIdOut = tc::idesc_bf16_f32(128, 16);
   uint32_t phase = 0;
   bool aborted = false;
-  const long ntiles = (a.n + 127) / 128;
+  const long nitems = p.list ? (long)*p.list_count : a.n;
+  const long ntiles = (nitems + 127) / 128;
   int par = 0;
   for (long tile = (long)blockIdx.x * kTcGroups + g; tile < ntiles; tile += (long)gridDim.x * kTcGroups, par ^= 1) {
-    const long c = tile * 128 + t;
+    const long idx = tile * 128 + t;
+    const long c = p.list ? (idx < nitems ? (long)p.list[idx] : -1L) : idx;
     bool need = false, for_partner = false;
     float f[kMlpIn];
 #pragma unroll
     for (int j = 0; j < kMlpIn; ++j) f[j] = 0.f;
-    if (c < a.n) {
+    if (c >= 0 && c < a.n) {
       const double T0 = a.T[c];
       if (p.active) {
         const int r = reference_cell_active(T0, a.bc, c) ? route_of(p.routes, T0) : -1;
@@ -855,8 +861,10 @@ __global__ void k_flag_count(long n, const unsigned char* flag, int* block_count
   if (threadIdx.x == 0) block_count[blockIdx.x] = cnt;
 }
 
-__global__ void k_scan_counts(int nb, const int* block_count, int* block_off, int* total,
-                              unsigned long long* counters) {
+// Exclusive scan of nb block counts by one block (any multiple of 32 threads up
+// to 1024); the total goes to *total (and is added to counters[7]).
+__device__ void scan_counts_body(int nb, const int* block_count, int* block_off, int* total,
+                                 unsigned long long* counters) {
   __shared__ int carry;
   if (threadIdx.x == 0) carry = 0;
   __syncthreads();
@@ -891,6 +899,61 @@ __global__ void k_scan_counts(int nb, const int* block_count, int* block_off, in
   if (threadIdx.x == 0) {
     *total = carry;
     if (counters) counters[7] += (unsigned long long)carry;
+  }
+}
+
+__global__ void k_scan_counts(int nb, const int* block_count, int* block_off, int* total,
+                              unsigned long long* counters) {
+  scan_counts_body(nb, block_count, block_off, total, counters);
+}
+
+// ------------------------------------------------ per-network cell lists
+// The tensor-core kernel of network i runs over the list of the cells it has
+// to answer, so its tiles are full and a network with a narrow band does not
+// scan the whole field.  Bit i of a cell's mask: the cell routes to network
+// i, or to a network whose committee partner i is.
+__device__ __forceinline__ unsigned route_mask(const StepArgs& a, const GateNets& nets, long c) {
+  const double T0 = a.T[c];
+  if (!reference_cell_active(T0, a.bc, c)) return 0u;
+  const int r = route_of(nets, T0);
+  if (r < 0) return 0u;
+  unsigned m = 1u << r;
+  const int q = nets.net[r].gc.partner;
+  if (q >= 0 && q < kMaxNets && q != r && nets.net[q].on) m |= 1u << q;
+  return m;
+}
+
+__global__ void k_route_count(StepArgs a, GateNets nets, unsigned char* mask, int nb, int* block_count) {
+  const long c = (long)blockIdx.x * kCompactBlock + threadIdx.x;
+  const unsigned m = c < a.n ? route_mask(a, nets, c) : 0u;
+  if (c < a.n) mask[c] = (unsigned char)m;
+  for (int i = 0; i < kMaxNets; ++i) {
+    const int cnt = __syncthreads_count((int)((m >> i) & 1u));
+    if (threadIdx.x == 0) block_count[i * nb + blockIdx.x] = cnt;
+  }
+}
+
+__global__ void k_route_scan(int nb, const int* block_count, int* block_off, int* total) {
+  scan_counts_body(nb, block_count + (long)blockIdx.x * nb, block_off + (long)blockIdx.x * nb, total + blockIdx.x,
+                   nullptr);
+}
+
+// list[i * cap + j]: the j-th cell (in cell order) of network i's list
+__global__ void k_route_scatter(long n, const unsigned char* mask, int nb, const int* block_off, long cap,
+                                int* list) {
+  const long c = (long)blockIdx.x * kCompactBlock + threadIdx.x;
+  const unsigned m = c < n ? mask[c] : 0u;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __shared__ int wcount[kCompactBlock / 32];
+  for (int i = 0; i < kMaxNets; ++i) {
+    const int f = (int)((m >> i) & 1u);
+    if (!__syncthreads_or(f)) continue;
+    const unsigned bal = __ballot_sync(0xffffffffu, f);
+    if (lane == 0) wcount[w] = __popc(bal);
+    __syncthreads();
+    int before = 0;
+    for (int q = 0; q < w; ++q) before += wcount[q];
+    if (f) list[(long)i * cap + block_off[i * nb + blockIdx.x] + before + __popc(bal & ((1u << lane) - 1u))] = (int)c;
   }
 }
 
@@ -1013,6 +1076,9 @@ struct Surrogate {
   double band_lo = 0.0, band_hi = 0.0;
   unsigned char* flag = nullptr;
   int *block_count = nullptr, *block_off = nullptr, *list = nullptr, *n_list = nullptr;
+  // per-network cell lists of the tensor-core kernel (kMaxNets lists of gcap)
+  unsigned char* rmask = nullptr;
+  int *rlist = nullptr, *rblock_count = nullptr, *rblock_off = nullptr, *rcount = nullptr;
   // fallback cells in temperature order (order.hpp) or in cell order
   bool order_cells = true;
   OrderScratch order;
@@ -1091,6 +1157,7 @@ void surrogate_destroy(Surrogate* s) {
   cudaFree(s->d_loss); cudaFree(s->flag); cudaFree(s->gO); cudaFree(s->gP); cudaFree(s->block_count); cudaFree(s->block_off);
   cudaFree(s->list);
   cudaFree(s->n_list);
+  cudaFree(s->rmask); cudaFree(s->rlist); cudaFree(s->rblock_count); cudaFree(s->rblock_off); cudaFree(s->rcount);
   order_free(&s->order);
   cudaFree(s->d_err);
   cudaFreeHost(s->h_err);
@@ -1162,6 +1229,9 @@ static std::string ensure_infer(Surrogate* s, long n) {
 static std::string ensure_gate(Surrogate* s, long n) {
   if (n <= s->gcap) return "";
   cudaFree(s->flag); cudaFree(s->block_count); cudaFree(s->block_off); cudaFree(s->list); cudaFree(s->n_list);
+  cudaFree(s->rmask); cudaFree(s->rlist); cudaFree(s->rblock_count); cudaFree(s->rblock_off); cudaFree(s->rcount);
+  s->rmask = nullptr;
+  s->rlist = s->rblock_count = s->rblock_off = s->rcount = nullptr;
   cudaFree(s->gO);
   cudaFree(s->gP);
   s->gO = s->gP = nullptr;
@@ -1174,6 +1244,11 @@ static std::string ensure_gate(Surrogate* s, long n) {
   if ((e = ck(cudaMalloc(&s->block_off, nb * 4), "alloc offsets")).size()) return e;
   if ((e = ck(cudaMalloc(&s->list, n * 4), "alloc list")).size()) return e;
   if ((e = ck(cudaMalloc(&s->n_list, 4), "alloc count")).size()) return e;
+  if ((e = ck(cudaMalloc(&s->rmask, n), "alloc route masks")).size()) return e;
+  if ((e = ck(cudaMalloc(&s->rlist, sizeof(int) * kMaxNets * (size_t)n), "alloc network lists")).size()) return e;
+  if ((e = ck(cudaMalloc(&s->rblock_count, sizeof(int) * kMaxNets * nb), "alloc network counts")).size()) return e;
+  if ((e = ck(cudaMalloc(&s->rblock_off, sizeof(int) * kMaxNets * nb), "alloc network offsets")).size()) return e;
+  if ((e = ck(cudaMalloc(&s->rcount, sizeof(int) * kMaxNets), "alloc network totals")).size()) return e;
   if ((e = order_reserve(&s->order, n)).size()) return e;
   s->gcap = n;
   return "";
@@ -1565,11 +1640,21 @@ cudaError_t surrogate_gate(Surrogate* const* nets_in, const StepArgs& a, long fl
       }
       nets.net[i] = GateNet{si->d_norm, si->gate, lo, hi, 1};
     }
-    // network outputs of the routed cells, planar, then the wide FP64 gate
+    // each network's cells listed once, then the network outputs of the
+    // listed cells, planar, then the wide FP64 gate
+    const int nb = (int)((n + kCompactBlock - 1) / kCompactBlock);
+    if (n > 0) {
+      k_route_count<<<nb, kCompactBlock, 0, st>>>(a, nets, s->rmask, nb, s->rblock_count);
+      k_route_scan<<<kMaxNets, 1024, 0, st>>>(nb, s->rblock_count, s->rblock_off, s->rcount);
+      k_route_scatter<<<nb, kCompactBlock, 0, st>>>(n, s->rmask, nb, s->rblock_off, s->gcap, s->rlist);
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
     for (int i = 0; i < kMaxNets; ++i) {
       if (!nets.net[i].on) continue;
-      if ((e = launch_tc(nets_in[i], tc_args(nets_in[i], a, s->gO, n, 1, &nets, i, s->gP), st)) != cudaSuccess)
-        return e;
+      TcArgs p = tc_args(nets_in[i], a, s->gO, n, 1, &nets, i, s->gP);
+      p.list = s->rlist + (size_t)i * s->gcap;
+      p.list_count = s->rcount + i;
+      if ((e = launch_tc(nets_in[i], p, st)) != cudaSuccess) return e;
     }
     if ((e = launch_gate(s, a, s->gO, s->gP, n, nets, counters, st, flag)) != cudaSuccess) return e;
   } else {
