@@ -1579,8 +1579,10 @@ static cudaError_t launch_tc(Surrogate* s, const TcArgs& p, cudaStream_t st) {
 static cudaError_t launch_gate(Surrogate* s, const StepArgs& a, const float* O, const float* OP, long o_ld,
                                const GateNets& nets, unsigned long long* counters, cudaStream_t st,
                                unsigned char* flag) {
+  // one resident wave of blocks (three per SM), each looping over cells: the
+  // block's set-up (projector, thermo tables) is paid once per block
   const int sms = s->num_sms > 0 ? s->num_sms : 148;
-  const long grid = std::min<long>((a.n + 127) / 128, (long)sms * 16);
+  const long grid = std::min<long>((a.n + 127) / 128, (long)sms * 3);
   k_gate<<<(unsigned)std::max<long>(grid, 1), 128, 0, st>>>(a, O, OP, o_ld, nets, flag, counters);
   return cudaGetLastError();
 }
