@@ -424,6 +424,14 @@ NRG_API int nrg_surrogate_set_band(nrg_chem* h, double T_lo, double T_hi);
  * field while taking about 40% fewer BDF steps than 1e-9.  Per handle, for
  * every network.  No counterpart in the reference. */
 NRG_API int nrg_surrogate_set_fallback_eps(nrg_chem* h, double eps);
+/* Gate bounds of the selected network for longer steps: band 1..3 applies to
+ * steps in (the previous band's dt_max, dt_max], band 0 being
+ * nrg_surrogate_set_gate with nrg_surrogate_set_gate_dt's bound; the bounds
+ * mean what they mean in nrg_surrogate_set_gate.  dt_max 0 leaves the band
+ * unused.  Steps above every band go to FP64.  No counterpart in the
+ * reference. */
+NRG_API int nrg_surrogate_set_gate_band(nrg_chem* h, int band, double dt_max, double elem_tol,
+                                        double raw_elem_tol, double dT_tol, double dT_max);
 /* Inference path of the surrogate step: 1 (default) the tensor-core kernel
  * (features and the five layers on tcgen05 with TMEM accumulators) followed
  * by the wide FP64 gate kernel; 0 the GEMM chain (features, one tcgen05

@@ -1671,6 +1671,16 @@ extern "C" int nrg_surrogate_set_fallback_eps(nrg_chem* h, double eps) {
   return NRG_OK;
 }
 
+extern "C" int nrg_surrogate_set_gate_band(nrg_chem* h, int band, double dt_max, double elem_tol,
+                                           double raw_elem_tol, double dT_tol, double dT_max) {
+  if (!h) return NRG_ERR_ARG;
+  if (band < 1 || band >= nrg::kGateBands || !(dt_max >= 0.0) || !(elem_tol >= 0.0) || !(raw_elem_tol >= 0.0) ||
+      !(dT_tol >= 0.0) || !(dT_max >= 0.0))
+    return fail(h, NRG_ERR_ARG, "gate band must be 1..3 with non-negative bounds");
+  nrg::surrogate_set_gate_band(h->sur_net[h->sur_sel], band, dt_max, elem_tol, raw_elem_tol, dT_tol, dT_max);
+  return NRG_OK;
+}
+
 extern "C" int nrg_surrogate_set_gate_dt(nrg_chem* h, double dt_max) {
   if (!h || !(dt_max > 0)) return NRG_ERR_ARG;
   nrg::surrogate_set_gate_dt(h->sur_net[h->sur_sel], dt_max);

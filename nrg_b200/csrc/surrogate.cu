@@ -549,12 +549,35 @@ __device__ __forceinline__ void count_surrogate(unsigned long long n_sur, unsign
 // standardisation and settings.  Network 0 is the main one; the others
 // cover narrower bands (a flame's preheat zone, the low-temperature part of
 // its front) and take precedence there.
+// gc: the gate for steps up to gc.dt_max (and the committee partner); xb:
+// bounds for longer steps, band b for dt in (previous band's dt_max,
+// xb[b].dt_max] (dt_max 0: unused).
 struct GateNet {
   const MlpNorm* nm;
   GateCfg gc;
   double lo, hi;
   int on;
+  GateCfg xb[kGateBands - 1];
 };
+
+// The gate settings for a step of length dt (the committee fields are gc's).
+__device__ __forceinline__ GateCfg gate_for_dt(const GateNet& g, double dt) {
+  if (dt <= g.gc.dt_max) return g.gc;
+  double prev = g.gc.dt_max;
+#pragma unroll
+  for (int b = 0; b < kGateBands - 1; ++b) {
+    const GateCfg& x = g.xb[b];
+    if (x.dt_max > prev && dt <= x.dt_max) {
+      GateCfg r = x;
+      r.partner = g.gc.partner;
+      r.agree_Y = g.gc.agree_Y;
+      r.agree_T = g.gc.agree_T;
+      return r;
+    }
+    if (x.dt_max > prev) prev = x.dt_max;
+  }
+  return g.gc;  // dt above every band: gate_active_cell rejects it
+}
 struct GateNets {
   GateNet net[kMaxNets];
 };
@@ -605,7 +628,8 @@ __global__ void __launch_bounds__(128, 3) k_gate(StepArgs a, const float* O, con
 #pragma unroll
       for (int j = 0; j < kMlpOut; ++j) op[j] = OP[j * o_ld + c];
     }
-    const bool acc = gate_active_cell(a, c, T0, rho, dt, f, o, nets.net[net].nm, nets.net[net].gc, P, th,
+    const GateCfg gc = gate_for_dt(nets.net[net], dt);
+    const bool acc = gate_active_cell(a, c, T0, rho, dt, f, o, nets.net[net].nm, gc, P, th,
                                       with_partner ? op : nullptr, with_partner ? nets.net[pn].nm : nullptr);
     n_sur += acc;
     flag[c] = acc ? 0 : 1;
@@ -1038,6 +1062,7 @@ struct Surrogate {
   bool ready = false;
   bool uploaded = false;
   GateCfg gate{1e-6, 5e-6, 0.2, 5.0, 1e-6, -1, 0.0, 0.0};
+  GateCfg xgate[kGateBands - 1] = {};  // bounds for longer steps (dt_max 0: unused)
   MlpNorm norm{};
   MlpNorm* d_norm = nullptr;
   // parameters: fp32 master, Adam moments, bf16 working copies, gradients
@@ -1172,6 +1197,22 @@ void surrogate_set_gate(Surrogate* s, double elem_tol, double raw_elem_tol, doub
   s->gate = GateCfg{elem_tol, raw_elem_tol, dT_tol, dT_max, g0.dt_max, g0.partner, g0.agree_Y, g0.agree_T};
 }
 void surrogate_set_gate_dt(Surrogate* s, double dt_max) { s->gate.dt_max = dt_max; }
+void surrogate_set_gate_band(Surrogate* s, int band, double dt_max, double elem_tol, double raw_elem_tol,
+                             double dT_tol, double dT_max) {
+  if (band < 1 || band >= kGateBands) return;
+  s->xgate[band - 1] = GateCfg{elem_tol, raw_elem_tol, dT_tol, dT_max, dt_max, -1, 0.0, 0.0};
+}
+
+static GateNet gate_net(const Surrogate* s, double lo, double hi) {
+  GateNet g{};
+  g.nm = s->d_norm;
+  g.gc = s->gate;
+  g.lo = lo;
+  g.hi = hi;
+  g.on = 1;
+  for (int b = 0; b < kGateBands - 1; ++b) g.xb[b] = s->xgate[b];
+  return g;
+}
 void surrogate_set_band(Surrogate* s, bool set, double lo, double hi) {
   s->band_set = set;
   s->band_lo = lo;
@@ -1626,7 +1667,7 @@ cudaError_t surrogate_gate(Surrogate* const* nets_in, const StepArgs& a, long fl
   unsigned char* flag = s->flag + flag_off;
   cudaError_t e;
   GateNets nets{};
-  nets.net[0] = GateNet{s->d_norm, s->gate, -1e300, 1e300, 1};
+  nets.net[0] = gate_net(s, -1e300, 1e300);
   if (s->fused) {
     // routing bands: the hulls' temperature ranges; network 0 also takes
     // what lies above its hull (its hull test then sends it to FP64)
@@ -1640,7 +1681,7 @@ cudaError_t surrogate_gate(Surrogate* const* nets_in, const StepArgs& a, long fl
         lo = si->band_lo;
         hi = si->band_hi;
       }
-      nets.net[i] = GateNet{si->d_norm, si->gate, lo, hi, 1};
+      nets.net[i] = gate_net(si, lo, hi);
     }
     // each network's cells listed once, then the network outputs of the
     // listed cells, planar, then the wide FP64 gate

@@ -17,6 +17,9 @@ struct Surrogate;
 // Networks of one handle: 0 the main one, the others for narrower
 // temperature bands (routing in surrogate_step).
 constexpr int kMaxNets = 8;
+// gate settings per network: one for steps up to its dt bound and up to
+// kGateBands - 1 more for longer steps
+constexpr int kGateBands = 4;
 
 using FallbackFn = std::function<cudaError_t(const StepArgs&, cudaStream_t)>;
 
@@ -111,6 +114,11 @@ std::string surrogate_check(Surrogate* s, cudaStream_t st);
 void surrogate_set_gate(Surrogate* s, double elem_tol, double raw_elem_tol, double dT_tol, double dT_max);
 // Longest step (s) whose cells the gate may accept.
 void surrogate_set_gate_dt(Surrogate* s, double dt_max);
+// Gate bounds of band b (1 .. kGateBands - 1) for steps in (the previous
+// band's dt_max, dt_max]; band 0 is surrogate_set_gate / surrogate_set_gate_dt.
+// dt_max 0 leaves the band unused.
+void surrogate_set_gate_band(Surrogate* s, int band, double dt_max, double elem_tol, double raw_elem_tol,
+                             double dT_tol, double dT_max);
 // Committee check of a network: partner (-1: none), agreement bounds.
 void surrogate_set_partner(Surrogate* s, int partner, double agree_Y, double agree_T);
 // Routing band [lo, hi) of a network (set = false: its hull's T range).

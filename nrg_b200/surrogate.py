@@ -105,6 +105,14 @@ class Surrogate:
         handle's, by default the reference's 1e-9); one value per handle."""
         _check(lib().nrg_surrogate_set_fallback_eps(self.h, float(eps)), self.h)
 
+    def set_gate_band(self, band: int, dt_max: float, elem_tol: float = 1e-6, raw_elem_tol: float = 5e-6,
+                      dT_tol: float = 0.2, dT_max: float = 5.0) -> None:
+        """Gate bounds for steps in (the previous band's dt_max, dt_max]
+        (band 1..3; band 0 is set_gate with set_gate_dt; dt_max 0: unused)."""
+        self._select()
+        _check(lib().nrg_surrogate_set_gate_band(self.h, int(band), float(dt_max), float(elem_tol),
+                                                 float(raw_elem_tol), float(dT_tol), float(dT_max)), self.h)
+
     def set_gate_dt(self, dt_max: float = 1e-6) -> None:
         """Longest step whose cells the gate may accept (the gate bounds are
         calibrated on 1e-6 s steps); longer steps go to FP64."""

@@ -226,3 +226,42 @@ def test_gate_sends_longer_steps_to_fp64(decks, W):
         np.testing.assert_array_equal(sg[k], plain[k])
     assert st_fl["cells_surrogate"] > 0
     assert st_fl2["cells_surrogate"] == 0 and np.all(fl2["status"][fl2["status"] != 0] == 1)
+
+
+def test_gate_bands_by_step_length(decks, W):
+    """nrg_surrogate_set_gate_band: a band admits steps up to its dt_max
+    with its own bounds; steps above every band, and a band with dt_max 0 or
+    with zero bounds, answer nothing (those cells get the plain step's bits)."""
+    from nrg_b200.chemistry import ChemicalKineticsSolver, NrgError
+    from nrg_b200.surrogate import DEFAULT_MODEL, RECIPE, Surrogate
+    wide = fields.slice_field(fields.wide_range_field(W, n_side=256), 16384, stride=3)
+    mid = fields.Field("mid", wide.T, wide.rho, wide.p, wide.Y, 3e-6, wide.shape)
+    s = ChemicalKineticsSolver(None, *decks, mode="fast")
+    try:
+        s.set_launch(kernel="thread", block=32)
+        sur = Surrogate(s)
+        sur.load(DEFAULT_MODEL)
+        sur.set_gate(*RECIPE["gate"])
+        plain, _ = run_device(s, mid, "fast")
+        _, st_none = run_device(s, mid, "surrogate")
+        sur.set_gate_band(1, 5e-6, 1e-6, 5e-6, 0.2, 80.0)
+        got, st_band = run_device(s, mid, "surrogate")
+        sur.set_gate_band(2, 2e-6, 1e-6, 5e-6, 0.2, 80.0)  # not above band 1's bound: unused
+        _, st_band2 = run_device(s, mid, "surrogate")
+        sur.set_gate_band(1, 5e-6, 0.0, 0.0, 0.0, 0.0)
+        _, st_zero = run_device(s, mid, "surrogate")
+        sur.set_gate_band(1, 2e-6, 1e-6, 5e-6, 0.2, 80.0)
+        _, st_short = run_device(s, mid, "surrogate")
+        with pytest.raises(NrgError):
+            sur.set_gate_band(4, 1e-5)
+        with pytest.raises(NrgError):
+            sur.set_gate_band(1, -1.0)
+    finally:
+        s.close()
+    assert st_none["cells_surrogate"] == 0
+    assert st_band["cells_surrogate"] > 0
+    assert st_band2["cells_surrogate"] == st_band["cells_surrogate"]
+    assert st_zero["cells_surrogate"] == 0 and st_short["cells_surrogate"] == 0
+    rej = (got["status"] != 5) & (got["status"] != 0)
+    for k in ("Y_prod", "Y_prod2"):
+        np.testing.assert_array_equal(got[k][:, rej], plain[k][:, rej])
