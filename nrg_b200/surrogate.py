@@ -223,13 +223,30 @@ RECIPE_PREHEAT = dict(RECIPE, T_lo=305.0, T_hi=800.0, pair_seed=13, gate=(1e-6, 
 # answered, within 0.74 K and 6.8e-5 of the FP64 step).
 RECIPE_FRONT_LOW = dict(RECIPE, T_lo=800.0, T_hi=1500.0, pair_seed=17, gate=(1e-6, 5e-6, 0.2, 80.0))
 
-# (network index, model file, recipe) of the committed networks
 # Tolerance of the FP64 integration of rejected cells.  On the flame field
 # an EPS of 1e-5 moves Y by at most 1.1e-7 and T by 1e-3 K from the 1e-9
 # integration (three orders inside the mode's 1e-4 / 1 K bounds) while
 # taking 1.6 to 3.2 times fewer BDF steps per cell.
 FALLBACK_EPS = 1e-5
 
+# Gate bands for wide-range states: calibrate_gate_bands over GATE_SWEEP on
+# 65,536 held-out states (seed 12; the test set is seed 11, the training
+# pairs seeds 3, 13, 17), each band calibrated at its longest step, tolerance
+# 0.8 K and 8e-5.  Answered / routed cells at the calibration steps:
+#   net 0 (T >= 1500 K): 19,041 / 39,522 at 1.5e-7 s, 8,495 at 2.5e-7 s,
+#     773 at 4e-7 s, no setting within bounds at 6.3e-7 s or longer;
+#   net 2 (800-1500 K): 24,340 / 26,014 at 1.5e-7 s, 22,091 at 2.5e-7 s,
+#     17,578 at 4e-7 s, 829 at 1e-6 s, 3 at 2e-6 s.
+# Steps above 1e-6 s go to FP64.  Network 1 (305-800 K) routes no
+# wide-range state and keeps its flame bounds.
+WIDE_RANGE_GATES = {
+    0: ((1.5e-7, (1e-6, 5e-7, 0.2, 2.0)), (2.5e-7, (1e-6, 2e-6, 0.02, 2.0)), (4e-7, (1e-6, 1e-6, 0.005, 80.0)),
+        (1e-6, None)),
+    2: ((1.5e-7, (1e-6, 5e-6, 0.2, 10.0)), (2.5e-7, (1e-6, 5e-6, 0.2, 5.0)), (4e-7, (1e-6, 5e-6, 0.2, 2.0)),
+        (1e-6, (1e-6, 5e-6, 0.005, 2.0))),
+}
+
+# (network index, model file, recipe) of the committed networks
 COMMITTED = ((0, DEFAULT_MODEL, RECIPE), (1, PREHEAT_MODEL, RECIPE_PREHEAT), (2, FRONT_LOW_MODEL, RECIPE_FRONT_LOW))
 
 
@@ -237,10 +254,66 @@ COMMITTED = ((0, DEFAULT_MODEL, RECIPE), (1, PREHEAT_MODEL, RECIPE_PREHEAT), (2,
 COMMITTED_PARTNERS = tuple((net, r["partner"][0]) for net, _, r in COMMITTED if "partner" in r)
 
 
-def load_default(solver: ChemicalKineticsSolver, fallback_eps: float = None) -> list:
+# Gate settings (set_gate's four bounds) swept by calibrate_gate_bands
+GATE_SWEEP = tuple((e, r, t, m) for e in (1e-6, 3e-7, 1e-7) for r in (5e-6, 2e-6, 1e-6, 5e-7)
+                   for t in (0.2, 0.05, 0.02, 0.01, 0.005) for m in (80.0, 20.0, 10.0, 5.0, 2.0))
+
+# Step bounds of the gate bands for states of the wide-range distribution
+# (T ~ U[800, 2600] K, p ~ U[0.5, 5] atm, dt ~ log-U[1e-7, 1e-5] s).
+WIDE_RANGE_DT = (1.5e-7, 2.5e-7, 4e-7, 1e-6)
+
+
+def calibrate_gate_bands(solver: ChemicalKineticsSolver, nets, W: np.ndarray, dts=WIDE_RANGE_DT, n: int = 65536,
+                         seed: int = 12, settings=GATE_SWEEP, tol_T: float = 0.8, tol_Y: float = 8e-5) -> dict:
+    """Per network and step band, the gate setting (calibrate_gate over
+    `settings`) that answers the most cells of a held-out set of
+    wide-range states (seed `seed`, not a training seed) stepped with the
+    band's longest dt, every answered cell within tol_T / tol_Y of the FP64
+    step.  Returns {net: [(dt_max, setting or None, answered, routed)]};
+    None: no setting keeps every answered cell within the bounds."""
+    states = fields.training_states(W, n, seed=seed, coupled=0.0)
+    out = {s.net: [] for s in nets}
+    for dt in dts:
+        f = fields.Field("held_out", states.T, states.rho, states.p, states.Y, float(dt), (n,))
+        route = routed_to(nets, f.T)
+        for sur in nets:
+            cells = (route == sur.net) & (f.T >= 305.0)
+            if not cells.any():
+                out[sur.net].append((float(dt), None, 0, 0))
+                continue
+            sur.set_gate_dt(float(dt))
+            r = calibrate_gate(solver, sur, f, settings, cells=cells, tol_T=tol_T, tol_Y=tol_Y)
+            best = r["choice"]
+            out[sur.net].append((float(dt), tuple(best["gate"][:4]) if best else None,
+                                 best["accepted"] if best else 0, int(cells.sum())))
+    return out
+
+
+def apply_gate_bands(nets, bands: dict) -> None:
+    """Gate bands of each network from calibrate_gate_bands' result: band 0
+    through set_gate / set_gate_dt, the longer bands through set_gate_band;
+    a band without a setting answers nothing."""
+    none = (0.0, 0.0, 0.0, 0.0)
+    for sur in nets:
+        rows = bands.get(sur.net, ())
+        for b, (dt, g, *_rest) in enumerate(rows):
+            g = tuple(g) if g else none
+            if b == 0:
+                sur.set_gate(*g)
+                sur.set_gate_dt(dt)
+            else:
+                sur.set_gate_band(b, dt, *g)
+
+
+def load_default(solver: ChemicalKineticsSolver, fallback_eps: float = None, gates: str = "flame") -> list:
     """The committed networks on the solver's handle, each with its gate:
     the main one (net 0) and the band networks whose files exist; the
-    rejected cells integrated at FALLBACK_EPS (or `fallback_eps`)."""
+    rejected cells integrated at FALLBACK_EPS (or `fallback_eps`).  gates:
+    "flame" (the bounds calibrated on the validation flame, dt = 1e-6 s) or
+    "wide-range" (WIDE_RANGE_GATES, per step band, calibrated on held-out
+    wide-range states)."""
+    if gates not in ("flame", "wide-range"):
+        raise ValueError("gates must be 'flame' or 'wide-range'")
     nets = []
     for net, path, recipe in COMMITTED:
         if not os.path.exists(path):
@@ -255,6 +328,8 @@ def load_default(solver: ChemicalKineticsSolver, fallback_eps: float = None) -> 
         nets.append(sur)
     if nets:
         nets[0].set_fallback_eps(FALLBACK_EPS if fallback_eps is None else fallback_eps)
+    if gates == "wide-range":
+        apply_gate_bands(nets, WIDE_RANGE_GATES)
     return nets
 
 
