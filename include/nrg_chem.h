@@ -94,8 +94,7 @@ typedef struct {
    * integrator (with the plain step's temperature order), [3] unused.
    * nrg_chem_step (host arrays) reports host wall times instead: [0] the
    * gather of the inputs into pinned staging, [1] the chunks' scatter with
-   * its waits for their copies, [2] the rejected cells' read-back and
-   * scatter (surrogate mode), [3] the whole call */
+   * its waits for their copies, [2] unused, [3] the whole call */
   double phase_ms[4];
 } nrg_chem_stats;
 

@@ -73,12 +73,6 @@ struct nrg_chem {
          *h_Ef = nullptr;
   int8_t* h_bc = nullptr;
   uint8_t* h_status = nullptr;
-  // host path, surrogate mode: the rejected cells' outputs packed in cell
-  // order for the read-back after the fallback (surrogate_pack_rejected)
-  size_t pk_cap = 0;
-  int *d_pk_idx = nullptr, *d_pk_count = nullptr, *h_pk_idx = nullptr, *h_pk_count = nullptr;
-  double *d_pk_vals = nullptr, *h_pk_vals = nullptr;
-  uint8_t *d_pk_st = nullptr, *h_pk_st = nullptr;
   // temperature order of the plain integrator's cells (order.hpp)
   bool order_cells = true;
   long order_cap = 0;
@@ -290,27 +284,6 @@ void free_staging(nrg_chem* h) {
   h->d_bc = h->h_bc = nullptr;
   h->d_status = h->h_status = nullptr;
   h->cap = 0;
-  cudaFree(h->d_pk_idx); cudaFree(h->d_pk_count); cudaFree(h->d_pk_vals); cudaFree(h->d_pk_st);
-  cudaFreeHost(h->h_pk_idx); cudaFreeHost(h->h_pk_count); cudaFreeHost(h->h_pk_vals); cudaFreeHost(h->h_pk_st);
-  h->d_pk_idx = h->d_pk_count = h->h_pk_idx = h->h_pk_count = nullptr;
-  h->d_pk_vals = h->h_pk_vals = nullptr;
-  h->d_pk_st = h->h_pk_st = nullptr;
-  h->pk_cap = 0;
-}
-
-int ensure_pack(nrg_chem* h, size_t n) {
-  if (n <= h->pk_cap) return NRG_OK;
-  const size_t N = (size_t)h->mech.n();
-  CK(h, cudaMalloc(&h->d_pk_idx, n * 4));
-  CK(h, cudaMalloc(&h->d_pk_count, 4));
-  CK(h, cudaMalloc(&h->d_pk_vals, (N + 1) * n * 8));
-  CK(h, cudaMalloc(&h->d_pk_st, n));
-  CK(h, cudaMallocHost(&h->h_pk_idx, n * 4));
-  CK(h, cudaMallocHost(&h->h_pk_count, 4));
-  CK(h, cudaMallocHost(&h->h_pk_vals, (N + 1) * n * 8));
-  CK(h, cudaMallocHost(&h->h_pk_st, n));
-  h->pk_cap = n;
-  return NRG_OK;
 }
 
 // Host threads for the gather and scatter of the host path: started once per
@@ -930,7 +903,6 @@ extern "C" int nrg_chem_step(nrg_chem* h, double time_step, const nrg_field_desc
   rc = step_prepare(h, n);
   if (rc) return rc;
   const bool sur = h->mode == NRG_MODE_SURROGATE, table = h->mode == NRG_MODE_TABLE;
-  if (sur && (rc = ensure_pack(h, (size_t)n))) return rc;
   // The interior is handled as rows along i (contiguous in the reference's
   // column-major arrays), split into up to eight chunks of rows.  Per chunk
   // the host gathers on all its threads into pinned staging and copies in on
@@ -939,14 +911,11 @@ extern "C" int nrg_chem_step(nrg_chem* h, double time_step, const nrg_field_desc
   //   copied out on copy_out and scattered while later chunks are stepped
   //   (on the 2048 x 2048 flame field this beats one launch over the whole
   //   field after the last chunk: 90 against 96 ms);
-  // * surrogate mode: each chunk goes through the networks and the gate as
-  //   it arrives (its accepted and skipped cells are then final) and is
-  //   copied out and scattered while later chunks arrive.  The FP64
-  //   fallback runs twice, on the rejected cells of the first half of the
-  //   chunks (while the host gathers the second half) and on those of the
-  //   second half (two launches: each pays the integrator's tail of slow
-  //   cells once); the rejected cells' outputs alone are then packed,
-  //   copied out and scattered.
+  // * surrogate mode: each chunk goes through the networks, the gate and
+  //   the FP64 fallback of its rejected cells as it arrives, and is copied
+  //   out and scattered while later chunks arrive (one fallback launch per
+  //   chunk: 17.4 ms per flame step, against 19.7 ms with two fallbacks over
+  //   half the field each and a packed read-back of the rejected cells).
   // Every mode but the table writes Y_prod = Y_prod2 W / dt: only Y_prod2
   // crosses PCIe and the host rebuilds Y_prod with the same two operations.
   const bool derive_yp = !table;
@@ -1005,7 +974,7 @@ extern "C" int nrg_chem_step(nrg_chem* h, double time_step, const nrg_field_desc
   using clk = std::chrono::steady_clock;
   auto ms_since = [](clk::time_point t0) { return std::chrono::duration<double, std::milli>(clk::now() - t0).count(); };
   const clk::time_point t_call = clk::now();
-  double host_ms[3] = {0.0, 0.0, 0.0};  // gather, chunk scatter (with its waits), rejected cells' read-back
+  double host_ms[2] = {0.0, 0.0};  // gather, scatter (with its waits for the chunks)
   CK(h, cudaMemsetAsync(h->d_counters, 0, sizeof(unsigned long long) * 8, s));
   CK(h, cudaEventRecord(h->ev0, s));
   for (int p = 0; p < P; ++p) {
@@ -1034,25 +1003,15 @@ extern "C" int nrg_chem_step(nrg_chem* h, double time_step, const nrg_field_desc
     const cudaError_t e = sur ? nrg::surrogate_gate(h->sur_net, args_of(c0, nc), c0, h->d_counters, s, nullptr)
                               : enqueue_step_body(h, args_of(c0, nc), s, nullptr);
     if (e != cudaSuccess) return cuda_fail(h, e, sur ? "surrogate_gate" : "enqueue_step");
-    CK(h, cudaEventRecord(h->ev_step[p], s));
-    if ((rc = copy_out(p, h->ev_step[p]))) return rc;
-    if (sur && (p == P / 2 - 1 || p == P - 1)) {
-      // the rejected cells of the chunks since the last fallback: the first
-      // half's run while the host still gathers and copies in the second
-      const int p0 = p == P - 1 && P / 2 >= 1 ? P / 2 : 0;
-      long f0, fn, l0, ln;
-      chunk_cells(p0, &f0, &fn);
-      chunk_cells(p, &l0, &ln);
-      const cudaError_t ef = nrg::surrogate_fallback(h->sur_net, args_of(f0, l0 + ln - f0), f0, h->d_counters, s,
+    if (sur) {
+      // the chunk's rejected cells right after its gate, so that its outputs
+      // are final when it is copied out
+      const cudaError_t ef = nrg::surrogate_fallback(h->sur_net, args_of(c0, nc), c0, h->d_counters, s,
                                                      integrator_fallback(h, nullptr));
       if (ef != cudaSuccess) return cuda_fail(h, ef, "surrogate_fallback");
     }
-  }
-  if (sur) {
-    cudaError_t e = nrg::surrogate_pack_rejected(h->sur_net[0], n, N, n, h->d_Yp2, h->d_Ef, h->d_status, h->d_pk_idx,
-                                     h->d_pk_count, h->d_pk_vals, h->d_pk_st, s);
-    if (e != cudaSuccess) return cuda_fail(h, e, "surrogate_pack_rejected");
-    CK(h, cudaMemcpyAsync(h->h_pk_count, h->d_pk_count, 4, cudaMemcpyDeviceToHost, s));
+    CK(h, cudaEventRecord(h->ev_step[p], s));
+    if ((rc = copy_out(p, h->ev_step[p]))) return rc;
   }
   CK(h, cudaEventRecord(h->ev1, s));
   const double* W = h->mech.molar_mass.data();
@@ -1078,38 +1037,9 @@ extern "C" int nrg_chem_step(nrg_chem* h, double time_step, const nrg_field_desc
     });
   }
   host_ms[1] = ms_since(ts);
-  const clk::time_point tr = clk::now();
-  if (sur) {
-    // the rejected cells' outputs (the chunks carried their values before
-    // the fallback): read back packed, scattered over the chunks' values
-    CK(h, cudaEventSynchronize(h->ev1));
-    const long m = *h->h_pk_count;
-    if (m < 0 || m > n) return fail(h, NRG_ERR_CUDA, "rejected-cell count out of range");
-    if (m > 0) {
-      CK(h, cudaMemcpyAsync(h->h_pk_idx, h->d_pk_idx, (size_t)m * 4, cudaMemcpyDeviceToHost, s));
-      CK(h, cudaMemcpyAsync(h->h_pk_vals, h->d_pk_vals, (size_t)m * (N + 1) * 8, cudaMemcpyDeviceToHost, s));
-      CK(h, cudaMemcpyAsync(h->h_pk_st, h->d_pk_st, (size_t)m, cudaMemcpyDeviceToHost, s));
-      CK(h, cudaStreamSynchronize(s));
-      const long tasks = std::min<long>(HostPool::get().size() * 4, m);
-      parallel_rows(0, tasks, [&](long t) {
-        for (long j = m * t / tasks; j < m * (t + 1) / tasks; ++j) {
-          const long c = h->h_pk_idx[j];
-          const long L = row_base(c / rowlen) + c % rowlen;
-          const bool skip = h->h_pk_st[j] == NRG_CELL_SKIPPED;
-          f->E_f_prod[L] = h->h_pk_vals[(size_t)N * m + j];
-          for (int sp = 0; sp < N; ++sp) {
-            const double v = h->h_pk_vals[(size_t)sp * m + j];
-            f->Y_prod[sp][L] = skip ? 0.0 : v * W[sp] / time_step;
-            if (!skip) f->Y_prod2[sp][L] = v;
-          }
-        }
-      });
-    }
-  }
-  host_ms[2] = ms_since(tr);
   rc = step_finish(h, s, n, stats, false);  // host times instead of the phase events
   if (rc == NRG_OK && stats && h->timing) {
-    for (int i = 0; i < 3; ++i) stats->phase_ms[i] = host_ms[i];
+    for (int i = 0; i < 2; ++i) stats->phase_ms[i] = host_ms[i];
     stats->phase_ms[3] = ms_since(t_call);
   }
   return rc;

@@ -1747,33 +1747,6 @@ cudaError_t surrogate_step(Surrogate* const* nets_in, const StepArgs& a, const L
   return surrogate_fallback(nets_in, a, 0, counters, st, fallback);
 }
 
-// The rejected cells' outputs, packed in cell order: idx[j] the cell, then
-// vals[k * m + j] = Y_prod2_k and vals[N * m + j] = E_f_prod, st_out[j] the
-// status, m = *count the number of rejected cells.
-__global__ void k_pack_rejected(int N, long ld, const int* idx, const int* count, const double* Yp2,
-                                const double* Ef, const uint8_t* status, double* vals, uint8_t* st_out) {
-  const long m = *count;
-  for (long j = blockIdx.x * (long)blockDim.x + threadIdx.x; j < m; j += (long)gridDim.x * blockDim.x) {
-    const long c = idx[j];
-    for (int k = 0; k < N; ++k) vals[k * m + j] = Yp2[k * ld + c];
-    vals[N * m + j] = Ef[c];
-    st_out[j] = status[c];
-  }
-}
-
-cudaError_t surrogate_pack_rejected(Surrogate* s, long n, int N, long ld, const double* Yp2, const double* Ef,
-                                    const uint8_t* status, int* idx, int* count, double* vals, uint8_t* st_out,
-                                    cudaStream_t st) {
-  if (n > s->gcap) return cudaErrorMemoryAllocation;
-  const int nb = (int)((n + kCompactBlock - 1) / kCompactBlock);
-  k_flag_count<<<nb, kCompactBlock, 0, st>>>(n, s->flag, s->block_count);
-  k_scan_counts<<<1, 1024, 0, st>>>(nb, s->block_count, s->block_off, count, nullptr);
-  k_compact<<<nb, kCompactBlock, 0, st>>>(n, s->flag, s->block_off, idx);
-  const int sms = s->num_sms > 0 ? s->num_sms : 148;
-  k_pack_rejected<<<sms * 8, 256, 0, st>>>(N, ld, idx, count, Yp2, Ef, status, vals, st_out);
-  return cudaGetLastError();
-}
-
 // Bounded-wait probe: one warp waits on an mbarrier that nothing arrives at,
 // with the same bounded wait the tensor-core kernel uses, and reports that the
 // wait gave up (and after how long) instead of hanging.

@@ -59,13 +59,6 @@ cudaError_t surrogate_gate(Surrogate* const* nets, const StepArgs& a, long flag_
                            unsigned long long* counters, cudaStream_t st, cudaEvent_t* ph);
 cudaError_t surrogate_fallback(Surrogate* const* nets, const StepArgs& a, long flag_off,
                                unsigned long long* counters, cudaStream_t st, const FallbackFn& fallback);
-// After surrogate_fallback over n cells: the rejected cells' Y_prod2,
-// E_f_prod and status packed in cell order (idx[j], vals[k * m + j] for
-// species k, vals[N * m + j] for E_f_prod, st_out[j]; *count = m), so that a
-// host reads back only those cells.
-cudaError_t surrogate_pack_rejected(Surrogate* s, long n, int N, long ld, const double* Yp2, const double* Ef,
-                                    const uint8_t* status, int* idx, int* count, double* vals, uint8_t* st_out,
-                                    cudaStream_t st);
 
 // ---- training / inspection (device pointers unless stated)
 std::string surrogate_init(Surrogate* s, unsigned long long seed, cudaStream_t st);
