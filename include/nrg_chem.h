@@ -416,6 +416,11 @@ NRG_API int nrg_surrogate_set_partner(nrg_chem* h, int partner, double agree_Y, 
  * are routed to it, it only answers as a committee partner).  No
  * counterpart in the reference. */
 NRG_API int nrg_surrogate_set_band(nrg_chem* h, double T_lo, double T_hi);
+/* Step band (dt_lo, dt_hi] of the selected network (default (0, 1e300]):
+ * only cells whose step lies in it are routed to the network, so a network
+ * trained on long steps answers those alone.  No counterpart in the
+ * reference. */
+NRG_API int nrg_surrogate_set_dt_band(nrg_chem* h, double dt_lo, double dt_hi);
 /* Relative tolerance EPS of the FP64 integration of the cells the gate
  * rejects (0, the default: the handle's EPS, nrg_chem_set_eps).  The
  * surrogate mode is an approximation to |dT| <= 1 K, |dY_k| <= 1e-4; an EPS

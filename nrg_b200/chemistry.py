@@ -89,6 +89,7 @@ SIGNATURES = {
     "nrg_chem_set_timing": (_I, [_VP, _I]),
     "nrg_chem_set_eps": (_I, [_VP, _D]),
     "nrg_surrogate_set_fallback_eps": (_I, [_VP, _D]),
+    "nrg_surrogate_set_dt_band": (_I, [_VP, _D, _D]),
     "nrg_surrogate_set_gate_band": (_I, [_VP, _I, _D, _D, _D, _D, _D]),
     "nrg_chem_info": (_I, [_VP, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "nrg_chem_tables": (_I, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),

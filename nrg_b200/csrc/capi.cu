@@ -1611,6 +1611,13 @@ extern "C" int nrg_surrogate_set_gate_band(nrg_chem* h, int band, double dt_max,
   return NRG_OK;
 }
 
+extern "C" int nrg_surrogate_set_dt_band(nrg_chem* h, double dt_lo, double dt_hi) {
+  if (!h) return NRG_ERR_ARG;
+  if (!(dt_lo >= 0.0) || !(dt_hi > dt_lo)) return fail(h, NRG_ERR_ARG, "step band needs 0 <= dt_lo < dt_hi");
+  nrg::surrogate_set_dt_band(h->sur_net[h->sur_sel], dt_lo, dt_hi);
+  return NRG_OK;
+}
+
 extern "C" int nrg_surrogate_set_gate_dt(nrg_chem* h, double dt_max) {
   if (!h || !(dt_max > 0)) return NRG_ERR_ARG;
   nrg::surrogate_set_gate_dt(h->sur_net[h->sur_sel], dt_max);

@@ -558,6 +558,7 @@ struct GateNet {
   double lo, hi;
   int on;
   GateCfg xb[kGateBands - 1];
+  double dt_lo, dt_hi;  // routing step band (dt_lo, dt_hi]
 };
 
 // The gate settings for a step of length dt (the committee fields are gc's).
@@ -582,10 +583,12 @@ struct GateNets {
   GateNet net[kMaxNets];
 };
 
-__device__ __forceinline__ int route_of(const GateNets& g, double T) {
+// The enabled network of highest index whose temperature band [lo, hi) and
+// step band (dt_lo, dt_hi] hold the cell, or -1.
+__device__ __forceinline__ int route_of(const GateNets& g, double T, double dt) {
 #pragma unroll
   for (int i = kMaxNets - 1; i >= 0; --i)
-    if (g.net[i].on && T >= g.net[i].lo && T < g.net[i].hi) return i;
+    if (g.net[i].on && T >= g.net[i].lo && T < g.net[i].hi && dt > g.net[i].dt_lo && dt <= g.net[i].dt_hi) return i;
   return -1;
 }
 
@@ -605,8 +608,8 @@ __global__ void __launch_bounds__(128, 3) k_gate(StepArgs a, const float* O, con
       flag[c] = 0;
       continue;
     }
-    const int net = route_of(nets, T0);
-    if (net < 0) {  // no network for this temperature: FP64
+    const int net = route_of(nets, T0, a.dt_cells ? a.dt_cells[c] : a.dt);
+    if (net < 0) {  // no network for this temperature and step: FP64
       flag[c] = 1;
       continue;
     }
@@ -771,7 +774,8 @@ __global__ void __launch_bounds__(128 * kTcGroups, 1) k_mlp_tc(TcArgs p) {
     if (c >= 0 && c < a.n) {
       const double T0 = a.T[c];
       if (p.active) {
-        const int r = reference_cell_active(T0, a.bc, c) ? route_of(p.routes, T0) : -1;
+        const int r = reference_cell_active(T0, a.bc, c) ? route_of(p.routes, T0, a.dt_cells ? a.dt_cells[c] : a.dt)
+                                                         : -1;
         for_partner = r >= 0 && r != p.net && p.out_partner && p.routes.net[r].gc.partner == p.net;
         need = r == p.net || for_partner;
       } else {
@@ -939,7 +943,7 @@ __global__ void k_scan_counts(int nb, const int* block_count, int* block_off, in
 __device__ __forceinline__ unsigned route_mask(const StepArgs& a, const GateNets& nets, long c) {
   const double T0 = a.T[c];
   if (!reference_cell_active(T0, a.bc, c)) return 0u;
-  const int r = route_of(nets, T0);
+  const int r = route_of(nets, T0, a.dt_cells ? a.dt_cells[c] : a.dt);
   if (r < 0) return 0u;
   unsigned m = 1u << r;
   const int q = nets.net[r].gc.partner;
@@ -1099,6 +1103,8 @@ struct Surrogate {
   // routing band [band_lo, band_hi) when set (band_set), else the hull's T range
   bool band_set = false;
   double band_lo = 0.0, band_hi = 0.0;
+  // routing step band (dt_band_lo, dt_band_hi]
+  double dt_band_lo = 0.0, dt_band_hi = 1e300;
   unsigned char* flag = nullptr;
   int *block_count = nullptr, *block_off = nullptr, *list = nullptr, *n_list = nullptr;
   // per-network cell lists of the tensor-core kernel (kMaxNets lists of gcap)
@@ -1197,6 +1203,10 @@ void surrogate_set_gate(Surrogate* s, double elem_tol, double raw_elem_tol, doub
   s->gate = GateCfg{elem_tol, raw_elem_tol, dT_tol, dT_max, g0.dt_max, g0.partner, g0.agree_Y, g0.agree_T};
 }
 void surrogate_set_gate_dt(Surrogate* s, double dt_max) { s->gate.dt_max = dt_max; }
+void surrogate_set_dt_band(Surrogate* s, double dt_lo, double dt_hi) {
+  s->dt_band_lo = dt_lo;
+  s->dt_band_hi = dt_hi;
+}
 void surrogate_set_gate_band(Surrogate* s, int band, double dt_max, double elem_tol, double raw_elem_tol,
                              double dT_tol, double dT_max) {
   if (band < 1 || band >= kGateBands) return;
@@ -1211,6 +1221,8 @@ static GateNet gate_net(const Surrogate* s, double lo, double hi) {
   g.hi = hi;
   g.on = 1;
   for (int b = 0; b < kGateBands - 1; ++b) g.xb[b] = s->xgate[b];
+  g.dt_lo = s->dt_band_lo;
+  g.dt_hi = s->dt_band_hi;
   return g;
 }
 void surrogate_set_band(Surrogate* s, bool set, double lo, double hi) {

@@ -107,6 +107,9 @@ std::string surrogate_check(Surrogate* s, cudaStream_t st);
 void surrogate_set_gate(Surrogate* s, double elem_tol, double raw_elem_tol, double dT_tol, double dT_max);
 // Longest step (s) whose cells the gate may accept.
 void surrogate_set_gate_dt(Surrogate* s, double dt_max);
+// Routing step band (dt_lo, dt_hi] of a network (default (0, 1e300]): cells
+// whose step lies outside it are not routed to it.
+void surrogate_set_dt_band(Surrogate* s, double dt_lo, double dt_hi);
 // Gate bounds of band b (1 .. kGateBands - 1) for steps in (the previous
 // band's dt_max, dt_max]; band 0 is surrogate_set_gate / surrogate_set_gate_dt.
 // dt_max 0 leaves the band unused.

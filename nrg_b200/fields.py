@@ -112,14 +112,14 @@ def wide_range_field(W: np.ndarray, n_side: int = 1024, seed: int = 2) -> Field:
 
 
 def training_states(W: np.ndarray, n: int, seed: int = 3, coupled: float = 0.0, T_lo: float = 800.0,
-                    T_hi: float = 2600.0) -> Field:
-    """Training states: the wide-range distribution with dt ~ log-U[1e-7, 1e-5]
-    (radicals shared in a fraction `coupled` of the states); [T_lo, T_hi]
-    is [800, 2600] K for the wide-range distribution itself and [305, 800] K
-    for a flame's preheat zone."""
+                    T_hi: float = 2600.0, dt_lo: float = 1e-7, dt_hi: float = 1e-5) -> Field:
+    """Training states: the wide-range distribution with dt ~ log-U[dt_lo,
+    dt_hi] (default [1e-7, 1e-5] s; radicals shared in a fraction `coupled`
+    of the states); [T_lo, T_hi] is [800, 2600] K for the wide-range
+    distribution itself and [305, 800] K for a flame's preheat zone."""
     rng = np.random.Generator(np.random.PCG64(seed))
     T, p, Y = random_state(n, rng, W, T_lo, T_hi, 0.5, 5.0, coupled)
-    dts = 10.0 ** rng.uniform(-7.0, -5.0, n)
+    dts = 10.0 ** rng.uniform(np.log10(dt_lo), np.log10(dt_hi), n)
     return _finish("training_states", T, p, Y, W, float("nan"), (n,), dts)
 
 

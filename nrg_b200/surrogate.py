@@ -113,6 +113,12 @@ class Surrogate:
         _check(lib().nrg_surrogate_set_gate_band(self.h, int(band), float(dt_max), float(elem_tol),
                                                  float(raw_elem_tol), float(dT_tol), float(dT_max)), self.h)
 
+    def set_dt_band(self, dt_lo: float = 0.0, dt_hi: float = 1e300) -> None:
+        """Routing step band (dt_lo, dt_hi] of this network."""
+        self._select()
+        _check(lib().nrg_surrogate_set_dt_band(self.h, float(dt_lo), float(dt_hi)), self.h)
+        self.dt_band = (float(dt_lo), float(dt_hi))
+
     def set_gate_dt(self, dt_max: float = 1e-6) -> None:
         """Longest step whose cells the gate may accept (the gate bounds are
         calibrated on 1e-6 s steps); longer steps go to FP64."""
@@ -223,6 +229,15 @@ RECIPE_PREHEAT = dict(RECIPE, T_lo=305.0, T_hi=800.0, pair_seed=13, gate=(1e-6, 
 # answered, within 0.74 K and 6.8e-5 of the FP64 step).
 RECIPE_FRONT_LOW = dict(RECIPE, T_lo=800.0, T_hi=1500.0, pair_seed=17, gate=(1e-6, 5e-6, 0.2, 80.0))
 
+# A network for long steps, measured and not committed: the wide-range
+# distribution with dt ~ log-U[1e-6, 1e-5] s (seed 19, 150 epochs, final
+# loss 1.8e-4), routed only the cells whose step lies in (1e-6, 1e-5] s
+# (train_default(solver, W, net=3, ...) with this recipe, then set_dt_band).
+# calibrate_gate_bands on the held-out states of seed 12 found it answering
+# 41 of 65,536 cells within 0.8 K and 8e-5 at 2e-6 s, none at 4e-6 s and one
+# at 1e-5 s.
+RECIPE_LONG_DT = dict(RECIPE, pair_seed=19, dt_lo=1e-6, dt_hi=1e-5, dt_band=(1e-6, 1e-5), gate_dt=1e-5)
+
 # Tolerance of the FP64 integration of rejected cells.  On the flame field
 # an EPS of 1e-5 moves Y by at most 1.1e-7 and T by 1e-3 K from the 1e-9
 # integration (three orders inside the mode's 1e-4 / 1 K bounds) while
@@ -275,7 +290,7 @@ def calibrate_gate_bands(solver: ChemicalKineticsSolver, nets, W: np.ndarray, dt
     out = {s.net: [] for s in nets}
     for dt in dts:
         f = fields.Field("held_out", states.T, states.rho, states.p, states.Y, float(dt), (n,))
-        route = routed_to(nets, f.T)
+        route = routed_to(nets, f.T, float(dt))
         for sur in nets:
             cells = (route == sur.net) & (f.T >= 305.0)
             if not cells.any():
@@ -325,6 +340,10 @@ def load_default(solver: ChemicalKineticsSolver, fallback_eps: float = None, gat
             sur.set_partner(*recipe["partner"])
         if "band" in recipe:
             sur.set_band(*recipe["band"])
+        if "dt_band" in recipe:
+            sur.set_dt_band(*recipe["dt_band"])
+        if "gate_dt" in recipe:
+            sur.set_gate_dt(recipe["gate_dt"])
         nets.append(sur)
     if nets:
         nets[0].set_fallback_eps(FALLBACK_EPS if fallback_eps is None else fallback_eps)
@@ -341,14 +360,17 @@ def hull_T(sur: "Surrogate"):
     return lo - margin * (hi - lo), hi + margin * (hi - lo)
 
 
-def routed_to(nets, T: np.ndarray) -> np.ndarray:
-    """Index of the network each temperature is routed to (-1: none)."""
+def routed_to(nets, T: np.ndarray, dt: float = 1e-6) -> np.ndarray:
+    """Index of the network each temperature (at step dt) is routed to
+    (-1: none)."""
     r = np.full(T.shape, -1)
     for s in sorted(nets, key=lambda s: s.net):
         lo, hi = hull_T(s)
         if s.net == 0:
             hi = np.inf
-        r[(T >= lo) & (T < hi)] = s.net
+        d_lo, d_hi = getattr(s, "dt_band", (0.0, np.inf))
+        if d_lo < dt <= d_hi:
+            r[(T >= lo) & (T < hi)] = s.net
     return r
 
 
@@ -400,11 +422,12 @@ def training_pairs(solver: ChemicalKineticsSolver, W: np.ndarray, n: int, seed: 
                    hull_margin: float = RECIPE["hull_margin"], dt_pow: float = RECIPE["dt_pow"],
                    coupled: float = RECIPE["coupled"], log_mask: int = RECIPE["log_mask"],
                    log_eps: float = RECIPE["log_eps"], common_dY_scale: int = RECIPE["common_dY_scale"],
-                   T_lo: float = RECIPE["T_lo"], T_hi: float = RECIPE["T_hi"]):
+                   T_lo: float = RECIPE["T_lo"], T_hi: float = RECIPE["T_hi"], dt_lo: float = 1e-7,
+                   dt_hi: float = 1e-5):
     """Integrates n training states with their own dt (FP64 integrator) and
     returns standardised (x_bf16, y) device tensors plus timing."""
     import torch
-    f = fields.training_states(W, n, seed=seed, coupled=coupled, T_lo=T_lo, T_hi=T_hi)
+    f = fields.training_states(W, n, seed=seed, coupled=coupled, T_lo=T_lo, T_hi=T_hi, dt_lo=dt_lo, dt_hi=dt_hi)
     # neighbouring lanes take similar paths when states are sorted by (dt, T)
     order = np.lexsort((f.T, np.round(np.log10(f.dt_cells) * 8)))
     f = fields.Field(f.name, f.T[order], f.rho[order], f.p[order], np.ascontiguousarray(f.Y[:, order]), f.dt,
@@ -436,7 +459,8 @@ def train_default(solver: ChemicalKineticsSolver, W: np.ndarray, seed: int = 0, 
     x, y, info = training_pairs(solver, W, r["n_train"], seed=r.get("pair_seed", 3), hull_margin=r["hull_margin"],
                                 dt_pow=r["dt_pow"],
                                 coupled=r["coupled"], log_mask=r["log_mask"], log_eps=r["log_eps"],
-                                common_dY_scale=r["common_dY_scale"], T_lo=r["T_lo"], T_hi=r["T_hi"])
+                                common_dY_scale=r["common_dY_scale"], T_lo=r["T_lo"], T_hi=r["T_hi"],
+                                dt_lo=r.get("dt_lo", 1e-7), dt_hi=r.get("dt_hi", 1e-5))
     sur.init(seed)
     t1 = time.perf_counter()
     losses = sur.train(x, y, epochs=r["epochs"], batch=r["batch"], lr=r["lr"], seed=seed + 1)

@@ -265,3 +265,33 @@ def test_gate_bands_by_step_length(decks, W):
     rej = (got["status"] != 5) & (got["status"] != 0)
     for k in ("Y_prod", "Y_prod2"):
         np.testing.assert_array_equal(got[k][:, rej], plain[k][:, rej])
+
+
+def test_step_band_routing(decks, W):
+    """nrg_surrogate_set_dt_band: a network is routed only the cells whose
+    step lies in its band (dt_lo, dt_hi]; outside it the cells go to FP64
+    with the plain step's bits."""
+    from nrg_b200.chemistry import ChemicalKineticsSolver, NrgError
+    from nrg_b200.surrogate import DEFAULT_MODEL, RECIPE, Surrogate
+    flame = fields.slice_field(fields.flame_field(W), 4 * 2048, offset=1000 * 2048)
+    s = ChemicalKineticsSolver(None, *decks, mode="fast")
+    try:
+        s.set_launch(kernel="thread", block=32)
+        sur = Surrogate(s)
+        sur.load(DEFAULT_MODEL)
+        sur.set_gate(*RECIPE["gate"])
+        plain, _ = run_device(s, flame, "fast")
+        _, st_in = run_device(s, flame, "surrogate")
+        sur.set_dt_band(1e-6, 1e-5)  # the flame's 1e-6 s step is outside (1e-6, 1e-5]
+        out, st_out = run_device(s, flame, "surrogate")
+        sur.set_dt_band(5e-7, 1e-6)
+        _, st_back = run_device(s, flame, "surrogate")
+        with pytest.raises(NrgError):
+            sur.set_dt_band(1e-5, 1e-6)
+    finally:
+        s.close()
+    assert st_in["cells_surrogate"] > 0
+    assert st_out["cells_surrogate"] == 0
+    assert st_back["cells_surrogate"] == st_in["cells_surrogate"]
+    for k in ("Y_prod", "Y_prod2", "E_f_prod", "T_after"):
+        np.testing.assert_array_equal(out[k], plain[k])
