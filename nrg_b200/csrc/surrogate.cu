@@ -1090,7 +1090,8 @@ struct Surrogate {
   long icap = 0;
   __nv_bfloat16 *iX = nullptr, *iH[2] = {nullptr, nullptr};
   float* iO = nullptr;
-  // tcgen05 inference (default) or the mma.sync GEMM chain, then the gate
+  // the tensor-core network kernel (default) or the GEMM chain (one k_gemm_tc
+  // launch per layer), then the gate
   bool fused = true;
   int num_sms = 0;
   unsigned int* d_err = nullptr;  // bit 0: an MMA wait of the tensor-core kernel timed out

@@ -96,8 +96,9 @@ std::string surrogate_prepare(Surrogate* s, long n, long ld, double dt, const do
 void surrogate_set_ready(Surrogate* s, bool ready);
 // Fallback cells grouped by temperature (default) or in cell order.
 void surrogate_set_cell_order(Surrogate* s, bool by_temperature);
-// Inference path of surrogate_step: the tcgen05 kernel (default) or the
-// mma.sync GEMM chain, either followed by the gate kernel.
+// Inference path of surrogate_step: the tensor-core network kernel (default)
+// or the GEMM chain (one tcgen05 GEMM launch per layer), either followed by
+// the gate kernel.
 void surrogate_set_fused(Surrogate* s, bool fused);
 // Features + MLP on tcgen05 over the n cells of a (no gate): out is n x 16
 // fp32 network outputs in normalised units; synchronises.
