@@ -138,8 +138,8 @@ __global__ void __launch_bounds__(kDigits) k_rs_scan_digits(int* digit_base, int
 }
 
 // Stable scatter of one tile: an item's slot is its tile's offset for its
-// digit, plus the items of that digit in earlier rounds, earlier warps of
-// this round and earlier lanes of its warp.
+// digit, plus the items of that digit in earlier iterations of the tile
+// loop, earlier warps of this iteration and earlier lanes of its warp.
 __global__ void __launch_bounds__(kThreads) k_rs_scatter(PassIn p, const int* offsets, const int* digit_base,
                                                          int tiles, uint32_t* keys_out, int* vals_out) {
   __shared__ int s_off[kDigits];
