@@ -50,6 +50,10 @@ struct nrg_chem {
   // host path: H2D and D2H copy streams and per-chunk events (copied in,
   // stepped, copied out), so that transfers and host work overlap the steps
   cudaStream_t copy_in = nullptr, copy_out = nullptr;
+  // host path, surrogate mode: a second compute stream (odd chunks) and the
+  // event that joins it back into the compute stream
+  cudaStream_t stream2 = nullptr;
+  cudaEvent_t ev_join = nullptr;
   cudaEvent_t ev_h2d[8] = {}, ev_step[8] = {}, ev_chunk[8] = {};
   int mode = NRG_MODE_FAST;
   LaunchCfg cfg;
@@ -758,6 +762,8 @@ extern "C" int nrg_chem_destroy(nrg_chem* h) {
   if (h->stream) cudaStreamDestroy(h->stream);
   if (h->copy_in) cudaStreamDestroy(h->copy_in);
   if (h->copy_out) cudaStreamDestroy(h->copy_out);
+  if (h->stream2) cudaStreamDestroy(h->stream2);
+  if (h->ev_join) cudaEventDestroy(h->ev_join);
   for (cudaEvent_t* arr : {h->ev_h2d, h->ev_step, h->ev_chunk})
     for (int i = 0; i < 8; ++i)
       if (arr[i]) cudaEventDestroy(arr[i]);
@@ -897,6 +903,8 @@ extern "C" int nrg_chem_step(nrg_chem* h, double time_step, const nrg_field_desc
   if (!h->copy_in) {
     CK(h, cudaStreamCreateWithFlags(&h->copy_in, cudaStreamNonBlocking));
     CK(h, cudaStreamCreateWithFlags(&h->copy_out, cudaStreamNonBlocking));
+    CK(h, cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking));
+    CK(h, cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
     for (cudaEvent_t* arr : {h->ev_h2d, h->ev_step, h->ev_chunk})
       for (int i = 0; i < 8; ++i) CK(h, cudaEventCreateWithFlags(&arr[i], cudaEventDisableTiming));
   }
@@ -915,7 +923,9 @@ extern "C" int nrg_chem_step(nrg_chem* h, double time_step, const nrg_field_desc
   //   the FP64 fallback of its rejected cells as it arrives, and is copied
   //   out and scattered while later chunks arrive (one fallback launch per
   //   chunk: 17.4 ms per flame step, against 19.7 ms with two fallbacks over
-  //   half the field each and a packed read-back of the rejected cells).
+  //   half the field each and a packed read-back of the rejected cells);
+  //   odd chunks run on a second stream with their own scratch, so that the
+  //   chunks' tails of slow cells overlap (15.7 ms).
   // Every mode but the table writes Y_prod = Y_prod2 W / dt: only Y_prod2
   // crosses PCIe and the host rebuilds Y_prod with the same two operations.
   const bool derive_yp = !table;
@@ -977,6 +987,24 @@ extern "C" int nrg_chem_step(nrg_chem* h, double time_step, const nrg_field_desc
   double host_ms[2] = {0.0, 0.0};  // gather, scatter (with its waits for the chunks)
   CK(h, cudaMemsetAsync(h->d_counters, 0, sizeof(unsigned long long) * 8, s));
   CK(h, cudaEventRecord(h->ev0, s));
+  // surrogate mode: even chunks on the compute stream, odd ones on a second
+  // stream with their own scratch (lane 1), so that one chunk's networks,
+  // gate and fallback fill the other's tail of slow cells.  The plain
+  // integrator's queue kernels share a queue head, so only the grid kernel
+  // takes part.
+  const bool two_lanes = sur && P > 1 && nrg::surrogate_fused(h->sur_net[0]) &&
+                         h->cfg.kernel == nrg::kKernelThreadGrid;
+  if (two_lanes) {
+    long max_nc = 0;
+    for (int p = 0; p < P; ++p) {
+      long a0, an;
+      chunk_cells(p, &a0, &an);
+      max_nc = std::max(max_nc, an);
+    }
+    const std::string le = nrg::surrogate_reserve_lane1(h->sur_net[0], max_nc);
+    if (!le.empty()) return fail(h, NRG_ERR_CUDA, le);
+    CK(h, cudaStreamWaitEvent(h->stream2, h->ev0, 0));  // after the counters are cleared
+  }
   for (int p = 0; p < P; ++p) {
     long c0, nc;
     chunk_cells(p, &c0, &nc);
@@ -999,19 +1027,25 @@ extern "C" int nrg_chem_step(nrg_chem* h, double time_step, const nrg_field_desc
       CK(h, cudaMemcpyAsync(h->d_Y + (size_t)sp * n + c0, h->h_Y + (size_t)sp * n + c0, nc * 8,
                             cudaMemcpyHostToDevice, ci));
     CK(h, cudaEventRecord(h->ev_h2d[p], ci));
-    CK(h, cudaStreamWaitEvent(s, h->ev_h2d[p], 0));
-    const cudaError_t e = sur ? nrg::surrogate_gate(h->sur_net, args_of(c0, nc), c0, h->d_counters, s, nullptr)
+    const int lane = two_lanes ? (p & 1) : 0;
+    cudaStream_t sp = lane ? h->stream2 : s;
+    CK(h, cudaStreamWaitEvent(sp, h->ev_h2d[p], 0));
+    const cudaError_t e = sur ? nrg::surrogate_gate(h->sur_net, args_of(c0, nc), c0, h->d_counters, sp, nullptr, lane)
                               : enqueue_step_body(h, args_of(c0, nc), s, nullptr);
     if (e != cudaSuccess) return cuda_fail(h, e, sur ? "surrogate_gate" : "enqueue_step");
     if (sur) {
       // the chunk's rejected cells right after its gate, so that its outputs
       // are final when it is copied out
-      const cudaError_t ef = nrg::surrogate_fallback(h->sur_net, args_of(c0, nc), c0, h->d_counters, s,
-                                                     integrator_fallback(h, nullptr));
+      const cudaError_t ef = nrg::surrogate_fallback(h->sur_net, args_of(c0, nc), c0, h->d_counters, sp,
+                                                     integrator_fallback(h, nullptr), lane);
       if (ef != cudaSuccess) return cuda_fail(h, ef, "surrogate_fallback");
     }
-    CK(h, cudaEventRecord(h->ev_step[p], s));
+    CK(h, cudaEventRecord(h->ev_step[p], sp));
     if ((rc = copy_out(p, h->ev_step[p]))) return rc;
+  }
+  if (two_lanes) {
+    CK(h, cudaEventRecord(h->ev_join, h->stream2));
+    CK(h, cudaStreamWaitEvent(s, h->ev_join, 0));
   }
   CK(h, cudaEventRecord(h->ev1, s));
   const double* W = h->mech.molar_mass.data();

@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(kDigits) k_rs_scan_digits(int* digit_base, int
   if (threadIdx.x == 0) {
     *total = sum;
     if (total2) *total2 = sum;
-    if (counter) *counter += (unsigned long long)sum;
+    if (counter) atomicAdd(counter, (unsigned long long)sum);  // orders on two streams may add at once
   }
 }
 

@@ -926,7 +926,7 @@ __device__ void scan_counts_body(int nb, const int* block_count, int* block_off,
   }
   if (threadIdx.x == 0) {
     *total = carry;
-    if (counters) counters[7] += (unsigned long long)carry;
+    if (counters) atomicAdd(&counters[7], (unsigned long long)carry);  // steps of two streams may add at once
   }
 }
 
@@ -1114,7 +1114,50 @@ struct Surrogate {
   // fallback cells in temperature order (order.hpp) or in cell order
   bool order_cells = true;
   OrderScratch order;
+  // a second set of the per-step scratch above (lists, outputs, order), so
+  // that two chunks of a field go through surrogate_gate / surrogate_fallback
+  // at once on two streams (surrogate_reserve_lane1)
+  struct Lane {
+    long cap = 0;
+    float *gO = nullptr, *gP = nullptr;
+    int *block_count = nullptr, *block_off = nullptr, *list = nullptr, *n_list = nullptr;
+    unsigned char* rmask = nullptr;
+    int *rlist = nullptr, *rblock_count = nullptr, *rblock_off = nullptr, *rcount = nullptr;
+    OrderScratch order;
+  } lane1;
 };
+
+// The scratch of lane 0 (the fields of Surrogate) or lane 1 (Surrogate::lane1).
+struct LaneRef {
+  long cap;
+  float *gO, *gP;
+  int *block_count, *block_off, *list, *n_list;
+  unsigned char* rmask;
+  int *rlist, *rblock_count, *rblock_off, *rcount;
+  OrderScratch* order;
+};
+
+static LaneRef lane_ref(Surrogate* s, int lane) {
+  if (lane == 1) {
+    Surrogate::Lane& L = s->lane1;
+    return LaneRef{L.cap, L.gO, L.gP, L.block_count, L.block_off, L.list, L.n_list, L.rmask, L.rlist,
+                   L.rblock_count, L.rblock_off, L.rcount, &L.order};
+  }
+  return LaneRef{s->gcap, s->gO, s->gP, s->block_count, s->block_off, s->list, s->n_list, s->rmask, s->rlist,
+                 s->rblock_count, s->rblock_off, s->rcount, &s->order};
+}
+
+static void free_lane1(Surrogate* s) {
+  Surrogate::Lane& L = s->lane1;
+  cudaFree(L.gO); cudaFree(L.gP); cudaFree(L.block_count); cudaFree(L.block_off); cudaFree(L.list);
+  cudaFree(L.n_list); cudaFree(L.rmask); cudaFree(L.rlist); cudaFree(L.rblock_count); cudaFree(L.rblock_off);
+  cudaFree(L.rcount);
+  order_free(&L.order);
+  L.gO = L.gP = nullptr;
+  L.block_count = L.block_off = L.list = L.n_list = L.rlist = L.rblock_count = L.rblock_off = L.rcount = nullptr;
+  L.rmask = nullptr;
+  L.cap = 0;
+}
 
 static long param_layout(Surrogate* s) {
   long off = 0;
@@ -1191,6 +1234,7 @@ void surrogate_destroy(Surrogate* s) {
   cudaFree(s->n_list);
   cudaFree(s->rmask); cudaFree(s->rlist); cudaFree(s->rblock_count); cudaFree(s->rblock_off); cudaFree(s->rcount);
   order_free(&s->order);
+  free_lane1(s);
   cudaFree(s->d_err);
   cudaFreeHost(s->h_err);
   delete s;
@@ -1671,11 +1715,38 @@ std::string surrogate_check(Surrogate* s, cudaStream_t st) {
 
 void surrogate_set_fused(Surrogate* s, bool fused) { s->fused = fused; }
 
+std::string surrogate_reserve_lane1(Surrogate* s, long n) {
+  Surrogate::Lane& L = s->lane1;
+  if (n <= L.cap) return "";
+  free_lane1(s);
+  const long nb = (n + kCompactBlock - 1) / kCompactBlock;
+  std::string e;
+  if ((e = ck(cudaMalloc(&L.gO, sizeof(float) * kMlpOut * (size_t)n), "alloc outputs")).size()) return e;
+  if ((e = ck(cudaMalloc(&L.gP, sizeof(float) * kMlpOut * (size_t)n), "alloc partner outputs")).size()) return e;
+  if ((e = ck(cudaMalloc(&L.block_count, nb * 4), "alloc counts")).size()) return e;
+  if ((e = ck(cudaMalloc(&L.block_off, nb * 4), "alloc offsets")).size()) return e;
+  if ((e = ck(cudaMalloc(&L.list, n * 4), "alloc list")).size()) return e;
+  if ((e = ck(cudaMalloc(&L.n_list, 4), "alloc count")).size()) return e;
+  if ((e = ck(cudaMalloc(&L.rmask, n), "alloc route masks")).size()) return e;
+  if ((e = ck(cudaMalloc(&L.rlist, sizeof(int) * kMaxNets * (size_t)n), "alloc network lists")).size()) return e;
+  if ((e = ck(cudaMalloc(&L.rblock_count, sizeof(int) * kMaxNets * nb), "alloc network counts")).size()) return e;
+  if ((e = ck(cudaMalloc(&L.rblock_off, sizeof(int) * kMaxNets * nb), "alloc network offsets")).size()) return e;
+  if ((e = ck(cudaMalloc(&L.rcount, sizeof(int) * kMaxNets), "alloc network totals")).size()) return e;
+  if ((e = order_reserve(&L.order, n)).size()) return e;
+  L.cap = n;
+  return "";
+}
+
+bool surrogate_fused(const Surrogate* s) { return s && s->fused; }
+
 cudaError_t surrogate_gate(Surrogate* const* nets_in, const StepArgs& a, long flag_off,
-                           unsigned long long* counters, cudaStream_t st, cudaEvent_t* ph) {
+                           unsigned long long* counters, cudaStream_t st, cudaEvent_t* ph, int lane) {
   Surrogate* s = nets_in[0];
-  // buffers are reserved by surrogate_reserve before any graph capture
-  if (flag_off < 0 || flag_off + a.n > s->gcap || (!s->fused && a.n > s->icap)) return cudaErrorMemoryAllocation;
+  const LaneRef R = lane_ref(s, lane);
+  // buffers are reserved by surrogate_reserve (lane 1: surrogate_reserve_lane1)
+  // before any graph capture
+  if (flag_off < 0 || flag_off + a.n > s->gcap || a.n > R.cap || (!s->fused && (lane != 0 || a.n > s->icap)))
+    return cudaErrorMemoryAllocation;
   const long n = a.n;
   unsigned char* flag = s->flag + flag_off;
   cudaError_t e;
@@ -1700,19 +1771,19 @@ cudaError_t surrogate_gate(Surrogate* const* nets_in, const StepArgs& a, long fl
     // listed cells, planar, then the wide FP64 gate
     const int nb = (int)((n + kCompactBlock - 1) / kCompactBlock);
     if (n > 0) {
-      k_route_count<<<nb, kCompactBlock, 0, st>>>(a, nets, s->rmask, nb, s->rblock_count);
-      k_route_scan<<<kMaxNets, 1024, 0, st>>>(nb, s->rblock_count, s->rblock_off, s->rcount);
-      k_route_scatter<<<nb, kCompactBlock, 0, st>>>(n, s->rmask, nb, s->rblock_off, s->gcap, s->rlist);
+      k_route_count<<<nb, kCompactBlock, 0, st>>>(a, nets, R.rmask, nb, R.rblock_count);
+      k_route_scan<<<kMaxNets, 1024, 0, st>>>(nb, R.rblock_count, R.rblock_off, R.rcount);
+      k_route_scatter<<<nb, kCompactBlock, 0, st>>>(n, R.rmask, nb, R.rblock_off, R.cap, R.rlist);
       if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     for (int i = 0; i < kMaxNets; ++i) {
       if (!nets.net[i].on) continue;
-      TcArgs p = tc_args(nets_in[i], a, s->gO, n, 1, &nets, i, s->gP);
-      p.list = s->rlist + (size_t)i * s->gcap;
-      p.list_count = s->rcount + i;
+      TcArgs p = tc_args(nets_in[i], a, R.gO, n, 1, &nets, i, R.gP);
+      p.list = R.rlist + (size_t)i * R.cap;
+      p.list_count = R.rcount + i;
       if ((e = launch_tc(nets_in[i], p, st)) != cudaSuccess) return e;
     }
-    if ((e = launch_gate(s, a, s->gO, s->gP, n, nets, counters, st, flag)) != cudaSuccess) return e;
+    if ((e = launch_gate(s, a, R.gO, R.gP, n, nets, counters, st, flag)) != cudaSuccess) return e;
   } else {
     k_features<<<std::min<long>((n + 255) / 256, 148 * 16), 256, 0, st>>>(n, a.ld, a.dt, a.dt_cells, a.T, a.rho,
                                                                         a.Y, s->d_norm, nullptr, s->iX);
@@ -1724,28 +1795,29 @@ cudaError_t surrogate_gate(Surrogate* const* nets_in, const StepArgs& a, long fl
 }
 
 cudaError_t surrogate_fallback(Surrogate* const* nets_in, const StepArgs& a, long flag_off,
-                               unsigned long long* counters, cudaStream_t st, const FallbackFn& fallback) {
+                               unsigned long long* counters, cudaStream_t st, const FallbackFn& fallback, int lane) {
   Surrogate* s = nets_in[0];
-  if (flag_off < 0 || flag_off + a.n > s->gcap) return cudaErrorMemoryAllocation;
+  const LaneRef R = lane_ref(s, lane);
+  if (flag_off < 0 || flag_off + a.n > s->gcap || a.n > R.cap) return cudaErrorMemoryAllocation;
   const long n = a.n;
   const unsigned char* flag = s->flag + flag_off;
   cudaError_t e;
   if (s->order_cells) {
     // rejected cells grouped by temperature: the fallback's warps then hold
     // cells with similar BDF paths
-    if ((e = order_cells_by_temperature(n, a.T, a.bc, flag, &s->order, s->list, s->n_list,
+    if ((e = order_cells_by_temperature(n, a.T, a.bc, flag, R.order, R.list, R.n_list,
                                         counters ? counters + 7 : nullptr, st)) != cudaSuccess)
       return e;
   } else {
     const int nb = (int)((n + kCompactBlock - 1) / kCompactBlock);
-    k_flag_count<<<nb, kCompactBlock, 0, st>>>(n, flag, s->block_count);
-    k_scan_counts<<<1, 1024, 0, st>>>(nb, s->block_count, s->block_off, s->n_list, counters);
-    k_compact<<<nb, kCompactBlock, 0, st>>>(n, flag, s->block_off, s->list);
+    k_flag_count<<<nb, kCompactBlock, 0, st>>>(n, flag, R.block_count);
+    k_scan_counts<<<1, 1024, 0, st>>>(nb, R.block_count, R.block_off, R.n_list, counters);
+    k_compact<<<nb, kCompactBlock, 0, st>>>(n, flag, R.block_off, R.list);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   StepArgs fa = a;
-  fa.cell_list = s->list;
-  fa.n_list_dev = s->n_list;
+  fa.cell_list = R.list;
+  fa.n_list_dev = R.n_list;
   fa.n_list = (int)n;  // upper bound for the grid; the kernel reads the device count
   return fallback(fa, st);
 }
@@ -1755,9 +1827,9 @@ cudaError_t surrogate_step(Surrogate* const* nets_in, const StepArgs& a, const L
                            cudaEvent_t* ph) {
   (void)cfg;
   (void)queue;
-  cudaError_t e = surrogate_gate(nets_in, a, 0, counters, st, ph);
+  cudaError_t e = surrogate_gate(nets_in, a, 0, counters, st, ph, 0);
   if (e != cudaSuccess) return e;
-  return surrogate_fallback(nets_in, a, 0, counters, st, fallback);
+  return surrogate_fallback(nets_in, a, 0, counters, st, fallback, 0);
 }
 
 // Bounded-wait probe: one warp waits on an mbarrier that nothing arrives at,

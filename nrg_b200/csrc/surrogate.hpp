@@ -55,10 +55,18 @@ cudaError_t surrogate_step(Surrogate* const* nets, const StepArgs& a, const Laun
 // surrogate_fallback then integrates the a.n cells at a's pointers whose
 // flags sit at [flag_off, flag_off + a.n) and were set by surrogate_gate
 // calls before it.
+// lane: which of the two sets of per-step scratch the call uses (0 always
+// exists; 1 after surrogate_reserve_lane1, fused inference only), so that
+// calls on two streams with different lanes may run at once.
 cudaError_t surrogate_gate(Surrogate* const* nets, const StepArgs& a, long flag_off,
-                           unsigned long long* counters, cudaStream_t st, cudaEvent_t* ph);
+                           unsigned long long* counters, cudaStream_t st, cudaEvent_t* ph, int lane = 0);
 cudaError_t surrogate_fallback(Surrogate* const* nets, const StepArgs& a, long flag_off,
-                               unsigned long long* counters, cudaStream_t st, const FallbackFn& fallback);
+                               unsigned long long* counters, cudaStream_t st, const FallbackFn& fallback,
+                               int lane = 0);
+// Scratch of lane 1 for chunks of up to n cells (before any graph capture).
+std::string surrogate_reserve_lane1(Surrogate* s, long n);
+// Whether the tensor-core inference path is selected (the default).
+bool surrogate_fused(const Surrogate* s);
 
 // ---- training / inspection (device pointers unless stated)
 std::string surrogate_init(Surrogate* s, unsigned long long seed, cudaStream_t st);
