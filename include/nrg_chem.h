@@ -281,6 +281,13 @@ NRG_API int nrg_chem_set_mode(nrg_chem* h, int mode);
  * chunk: cells reserved per queue fetch (1..64). */
 NRG_API int nrg_chem_set_launch(nrg_chem* h, int kernel, int block, int grid, int chunk);
 NRG_API int nrg_chem_get_launch(nrg_chem* h, int* kernel, int* block, int* grid, int* chunk);
+/* Form of the LU factorisation in the thread-per-cell kernels: 0 (default)
+ * unrolled over the integrated species, 1 a loop.  Same results; the
+ * unrolled form is faster where neighbouring cells take alike BDF paths
+ * (the flame field), the loop, with a quarter of the code, where they vary
+ * (ignition and wide-range fields).  nrg_chem_autotune tries both. */
+NRG_API int nrg_chem_set_lu_form(nrg_chem* h, int rolled);
+NRG_API int nrg_chem_get_lu_form(nrg_chem* h, int* rolled);
 
 /* Times candidate launch shapes on the given device-resident inputs (outputs
  * are scratch) and keeps the fastest for this handle.  ms_best may be NULL. */

@@ -89,6 +89,8 @@ SIGNATURES = {
     "nrg_chem_set_timing": (_I, [_VP, _I]),
     "nrg_chem_set_eps": (_I, [_VP, _D]),
     "nrg_surrogate_set_fallback_eps": (_I, [_VP, _D]),
+    "nrg_chem_set_lu_form": (_I, [_VP, _I]),
+    "nrg_chem_get_lu_form": (_I, [_VP, ctypes.POINTER(_I)]),
     "nrg_surrogate_set_dt_band": (_I, [_VP, _D, _D]),
     "nrg_surrogate_set_gate_band": (_I, [_VP, _I, _D, _D, _D, _D, _D]),
     "nrg_chem_info": (_I, [_VP, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
@@ -284,17 +286,23 @@ class ChemicalKineticsSolver:
 
     KERNELS = {"thread": 0, "thread_queue": 1, "warp_queue": 2}
 
-    def set_launch(self, kernel="warp_queue", block=256, grid=0, chunk=1) -> None:
+    def set_launch(self, kernel="warp_queue", block=256, grid=0, chunk=1, lu_rolled=None) -> None:
         """kernel: 'thread' (one thread per cell), 'thread_queue' (thread per
-        cell with a work queue) or 'warp_queue' (warp per cell, work queue)."""
+        cell with a work queue) or 'warp_queue' (warp per cell, work queue);
+        lu_rolled: the thread kernels' LU as a loop (None: unchanged)."""
         k = self.KERNELS[kernel] if isinstance(kernel, str) else int(kernel)
         _check(lib().nrg_chem_set_launch(self._h, k, block, grid, chunk), self._h)
+        if lu_rolled is not None:
+            _check(lib().nrg_chem_set_lu_form(self._h, int(bool(lu_rolled))), self._h)
 
     def get_launch(self) -> dict:
         v = [ctypes.c_int() for _ in range(4)]
         _check(lib().nrg_chem_get_launch(self._h, *[ctypes.byref(x) for x in v]), self._h)
         d = dict(zip(("kernel", "block", "grid", "chunk"), [x.value for x in v]))
         d["kernel"] = {v: k for k, v in self.KERNELS.items()}[d["kernel"]]
+        r = ctypes.c_int()
+        _check(lib().nrg_chem_get_lu_form(self._h, ctypes.byref(r)), self._h)
+        d["lu_rolled"] = bool(r.value)
         return d
 
     def set_graph(self, enable: bool) -> None:

@@ -487,6 +487,7 @@ cudaError_t enqueue_integrator(nrg_chem* h, const StepArgs& a, const LaunchCfg& 
   if (c.kernel == nrg::kKernelThreadQueue && c.grid <= 0) c.grid = h->num_sms;
   StepArgs b = a;
   b.eps = a.eps > 0.0 ? a.eps : h->eps;
+  b.lu_rolled = c.lu_rolled;
   // a whole field with one dt: its cells in temperature order (lanes of a
   // warp then take similar BDF paths); lists built by the caller and the
   // per-cell-dt training states keep their own order
@@ -801,6 +802,18 @@ extern "C" int nrg_chem_set_launch(nrg_chem* h, int kernel, int block, int grid,
   return NRG_OK;
 }
 
+extern "C" int nrg_chem_set_lu_form(nrg_chem* h, int rolled) {
+  if (!h) return NRG_ERR_ARG;
+  h->cfg.lu_rolled = rolled != 0;
+  return NRG_OK;
+}
+
+extern "C" int nrg_chem_get_lu_form(nrg_chem* h, int* rolled) {
+  if (!h || !rolled) return NRG_ERR_ARG;
+  *rolled = h->cfg.lu_rolled;
+  return NRG_OK;
+}
+
 extern "C" int nrg_chem_get_launch(nrg_chem* h, int* kernel, int* block, int* grid, int* chunk) {
   if (!h) return NRG_ERR_ARG;
   if (kernel) *kernel = h->cfg.kernel;
@@ -1099,7 +1112,8 @@ extern "C" int nrg_chem_autotune(nrg_chem* h, double time_step, long n, long ld,
   a.n_list_dev = nullptr;
   // candidate shapes: warp per cell (occupancy-derived persistent grid),
   // thread per cell from the work queue (1 or 2 blocks of 64 per SM, chunk 1
-  // or 2) and thread per cell over the plain grid (32- or 64-thread blocks)
+  // or 2) and thread per cell over the plain grid (32- or 64-thread blocks, LU
+  // unrolled or as a loop)
   std::vector<LaunchCfg> cands;
   for (int block : {128, 256}) {
     LaunchCfg c;
@@ -1118,12 +1132,14 @@ extern "C" int nrg_chem_autotune(nrg_chem* h, double time_step, long n, long ld,
       c.chunk = chunk;
       cands.push_back(c);
     }
-  for (int block : {32, 64}) {
-    LaunchCfg c;
-    c.kernel = nrg::kKernelThreadGrid;
-    c.block = block;
-    cands.push_back(c);
-  }
+  for (int block : {32, 64})
+    for (int rolled : {0, 1}) {
+      LaunchCfg c;
+      c.kernel = nrg::kKernelThreadGrid;
+      c.block = block;
+      c.lu_rolled = rolled;
+      cands.push_back(c);
+    }
   cudaStream_t s = h->stream;
   float best = 1e30f;
   LaunchCfg best_cfg = h->cfg;

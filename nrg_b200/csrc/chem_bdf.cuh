@@ -113,7 +113,7 @@ __device__ __noinline__ void nl_rhs(double* d, LUT* f);
 template <int N, int R, typename LUT, int BS, int SPEC>
 __device__ __noinline__ void nl_analytic_matrix(double* d, LUT* f, double factor);
 template <int N, int R, typename LUT, int BS, bool RECIP>
-__device__ __noinline__ RowPerm<N> nl_dgefa(double* d, LUT* f, int* info);
+__device__ __noinline__ RowPerm<N> nl_dgefa(double* d, LUT* f, int* info, int rolled);
 template <int N, int R, typename LUT, int BS, bool FAST>
 __device__ __noinline__ void nl_rate_constants(double* d, LUT* f, double T);
 
@@ -129,6 +129,7 @@ struct CellState : SmemStore<N, R, LUT, BS> {
   RowPerm<N> piv;  // row i of the factors is row piv.get(i) of the matrix
   double h, t, tout, rc, rmax, trend, eps;
   int nq, nwait, jtask, nstep, nfe, nje, nsolve, jstepl, nstepl, convrg, ier;
+  int lu_rolled;  // LU factorisation as a loop (StepArgs::lu_rolled)
 };
 
 // Register-array element with a runtime index (select chain, no local memory).
@@ -531,24 +532,13 @@ __device__ __forceinline__ double ratio_pow(double x, double p) {
   return npow(x, p);
 }
 
-// Division in the step-size and order control of DDSTP.  Reference mode: the
-// correctly rounded division (out of line).  Analytic-Jacobian and mixed
-// modes: inline, from the hardware reciprocal approximation refined by one
-// Newton step and one correction of the quotient (within an ulp or two);
-// these quotients only steer step sizes and orders.  Divisors that are zero,
-// not finite or outside [1e-300, 1e300] take the correctly rounded path.
+// Division in the step-size and order control of DDSTP: the correctly
+// rounded division (out of line) in every mode.  An inline quotient from the
+// hardware reciprocal approximation (one Newton step and a correction) in
+// the analytic-Jacobian and mixed modes measured no faster on the flame
+// field and 7 % slower on the ignition and wide-range fields (larger code).
 template <int JAC>
 __device__ __forceinline__ double sdiv(double a, double b) {
-  if constexpr (JAC != kJacFD) {
-    const double ab = fabs(b);
-    if (ab > 1e-300 && ab < 1e300) {
-      double r;
-      asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(b));
-      r = fma(r, fma(-b, r, 1.0), r);
-      const double q = a * r;
-      return fma(r, fma(-b, q, a), q);
-    }
-  }
   return ddiv(a, b);
 }
 
@@ -624,49 +614,65 @@ __device__ __forceinline__ LUT lu_axpy(LUT x, LUT t, LUT y) {
   else return x + t * y;
 }
 
+// One elimination step k of dgefa (pivot search, interchange, scaling,
+// column updates).
+template <int N, bool RECIP, class CS, class LUT>
+__device__ __forceinline__ void dgefa_step(CS& c, int k, RowPerm<N>& perm, int& info) {
+  int l = k;
+  LUT dmax = fabs(c.a(k, k));
+  for (int i = k + 1; i < N; ++i) {
+    const LUT xm = fabs(c.a(k, i));
+    if (xm > dmax) { l = i; dmax = xm; }
+  }
+  if (c.a(k, l) == (LUT)0) {
+    info = k + 1;
+    return;
+  }
+  if (l != k) {
+    const LUT t = c.a(k, l);
+    c.a(k, l) = c.a(k, k);
+    c.a(k, k) = t;
+    for (int j = 0; j < k; ++j) {
+      const LUT m = c.a(j, l);
+      c.a(j, l) = c.a(j, k);
+      c.a(j, k) = m;
+    }
+    const int pk = perm.get(k);
+    perm.set(k, perm.get(l));
+    perm.set(l, pk);
+  }
+  const LUT t = (LUT)-1 / c.a(k, k);
+  if (RECIP) c.a(k, k) = -t;
+  for (int i = k + 1; i < N; ++i) c.a(k, i) = t * c.a(k, i);
+  for (int j = k + 1; j < N; ++j) {
+    const LUT tj = c.a(j, l);
+    if (l != k) {
+      c.a(j, l) = c.a(j, k);
+      c.a(j, k) = tj;
+    }
+    if (tj != (LUT)0)
+      for (int i = k + 1; i < N; ++i) c.a(j, i) = lu_axpy<LUT, RECIP>(c.a(j, i), tj, c.a(k, i));
+  }
+}
+
+// rolled: the elimination as a loop over k; otherwise, up to 9 integrated
+// species, unrolled (every index but the pivot row a compile-time constant,
+// the updates of the columns right of the pivot independent instructions).
+// The two forms give the same bits; the unrolled one is faster where the
+// cells' BDF paths are alike (the flame), the rolled one, a quarter of the
+// code, where they vary (instruction cache): the autotuner picks.
 template <int N, bool RECIP, class CS>
-__device__ __forceinline__ int dgefa(CS& c, RowPerm<N>* perm_out) {
+__device__ __forceinline__ int dgefa(CS& c, RowPerm<N>* perm_out, bool rolled) {
   using LUT = typename std::remove_reference<decltype(c.a(0, 0))>::type;
   int info = 0;
   RowPerm<N> perm;
   perm.identity();
-  // up to 9 integrated species the elimination is unrolled: every index but
-  // the pivot row is a compile-time constant and the updates of the columns
-  // right of the pivot are independent instructions
+  if (rolled) {
+#pragma unroll 1
+    for (int k = 0; k < N - 1; ++k) dgefa_step<N, RECIP, CS, LUT>(c, k, perm, info);
+  } else {
 #pragma unroll(N <= 9 ? N : 1)
-  for (int k = 0; k < N - 1; ++k) {
-    int l = k;
-    LUT dmax = fabs(c.a(k, k));
-    for (int i = k + 1; i < N; ++i) {
-      const LUT xm = fabs(c.a(k, i));
-      if (xm > dmax) { l = i; dmax = xm; }
-    }
-    if (c.a(k, l) == (LUT)0) { info = k + 1; continue; }
-    if (l != k) {
-      const LUT t = c.a(k, l);
-      c.a(k, l) = c.a(k, k);
-      c.a(k, k) = t;
-      for (int j = 0; j < k; ++j) {
-        const LUT m = c.a(j, l);
-        c.a(j, l) = c.a(j, k);
-        c.a(j, k) = m;
-      }
-      const int pk = perm.get(k);
-      perm.set(k, perm.get(l));
-      perm.set(l, pk);
-    }
-    const LUT t = (LUT)-1 / c.a(k, k);
-    if (RECIP) c.a(k, k) = -t;
-    for (int i = k + 1; i < N; ++i) c.a(k, i) = t * c.a(k, i);
-    for (int j = k + 1; j < N; ++j) {
-      const LUT tj = c.a(j, l);
-      if (l != k) {
-        c.a(j, l) = c.a(j, k);
-        c.a(j, k) = tj;
-      }
-      if (tj != (LUT)0)
-        for (int i = k + 1; i < N; ++i) c.a(j, i) = lu_axpy<LUT, RECIP>(c.a(j, i), tj, c.a(k, i));
-    }
+    for (int k = 0; k < N - 1; ++k) dgefa_step<N, RECIP, CS, LUT>(c, k, perm, info);
   }
   *perm_out = perm;
   if (c.a(N - 1, N - 1) == (LUT)0) info = N;
@@ -731,12 +737,12 @@ __device__ __noinline__ void nl_analytic_matrix(double* d, LUT* f, double factor
 }
 
 template <int N, int R, typename LUT, int BS, bool RECIP>
-__device__ __noinline__ RowPerm<N> nl_dgefa(double* d, LUT* f, int* info) {
+__device__ __noinline__ RowPerm<N> nl_dgefa(double* d, LUT* f, int* info, int rolled) {
   SmemStore<N, R, LUT, BS> s;
   s.d = d;
   s.f = f;
   RowPerm<N> perm;
-  *info = dgefa<N, RECIP>(s, &perm);
+  *info = dgefa<N, RECIP>(s, &perm, rolled != 0);
   return perm;
 }
 
@@ -756,9 +762,10 @@ __device__ __noinline__ void nl_rate_constants(double* d, LUT* f, double T) {
 // reference's additions in the reference's order, and is stored once.
 template <int N, int Q, class S>
 __device__ __forceinline__ void ddpsc_order(S& c, int ksgn) {
-  // species are independent: up to 9 of them are unrolled, so that their
-  // addition chains overlap
-#pragma unroll(N <= 9 ? N : 1)
+  // one species at a time (unrolling the species, so that their addition
+  // chains overlap, measured slower: 73.2 against 70.0 ms per flame step,
+  // 122 against 103 ms on the ignition field, from the larger code)
+#pragma unroll 1
   for (int i = 0; i < N; ++i) {
     double v[Q + 1];
 #pragma unroll
@@ -909,7 +916,7 @@ __device__ void ddpst(CS& c) {
     nl_analytic_matrix<N, R, typename CS::lut_t, CS::kBS, CS::kSpec>(c.d, c.f, -el1h);
   }
   int info = 0;
-  c.piv = nl_dgefa<N, R, typename CS::lut_t, CS::kBS, JAC != kJacFD>(c.d, c.f, &info);
+  c.piv = nl_dgefa<N, R, typename CS::lut_t, CS::kBS, JAC != kJacFD>(c.d, c.f, &info, c.lu_rolled);
   if (info != 0) c.ier = 1;
 }
 
@@ -1171,6 +1178,7 @@ __device__ bool cell_begin(CS& c, const StepArgs& a, long cid) {
   c.h = copysign(NRG_FMIN(fabs(h), c_mech.hmax), h);
   c.eps = a.eps > 0.0 ? a.eps : c_mech.eps;
   c.jtask = 0;
+  c.lu_rolled = a.lu_rolled;
   c.nstep = 0;
   c.nstepl = 0;
   c.jstepl = 0;

@@ -31,6 +31,7 @@ struct StepArgs {
   int n_list;              // number of entries in cell_list (grid bound when n_list_dev is set)
   const int* n_list_dev;   // device-side entry count of cell_list (may be null)
   double eps = 0.0;        // relative tolerance of the integrator; 0: the mechanism's (the reference's 1e-9)
+  int lu_rolled = 0;       // thread-per-cell kernels: the LU factorisation as a loop (same bits)
 };
 
 // Chemistry sources applied to the state, then the state equation.
@@ -64,6 +65,7 @@ struct LaunchCfg {
   int block = 32;                  // threads per block
   int grid = 0;                   // persistent grid (0: fill the GPU)
   int chunk = 1;                  // cells reserved per queue fetch (per lane or per warp)
+  int lu_rolled = 0;              // thread-per-cell kernels: LU as a loop instead of unrolled
 };
 
 // full: tables over all species; reduced: the same with reaction lists
