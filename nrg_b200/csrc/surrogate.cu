@@ -1534,8 +1534,10 @@ std::string surrogate_train(Surrogate* s, long n, const __nv_bfloat16* x, const 
   std::vector<int> perm((size_t)n);
   for (long i = 0; i < n; ++i) perm[i] = (int)i;
   std::mt19937_64 rng(seed);
+  // two permutation buffers: the next epoch's order is drawn on the host
+  // and copied in while the GPU still runs the current epoch
   int* d_perm = nullptr;
-  if ((e = ck(cudaMalloc(&d_perm, n * 4), "alloc perm")).size()) return e;
+  if ((e = ck(cudaMalloc(&d_perm, 2 * n * 4), "alloc perm")).size()) return e;
   __nv_bfloat16* Xb = nullptr;
   if ((e = ck(cudaMalloc(&Xb, (long)batch * kMlpInPad * 2), "alloc batch")).size()) {
     cudaFree(d_perm);
@@ -1544,12 +1546,13 @@ std::string surrogate_train(Surrogate* s, long n, const __nv_bfloat16* x, const 
   const long steps = n / batch;
   const double total = (double)steps * epochs;
   long t_local = 0;
+  std::shuffle(perm.begin(), perm.end(), rng);
+  cudaMemcpyAsync(d_perm, perm.data(), n * 4, cudaMemcpyHostToDevice, st);
   for (int ep = 0; ep < epochs; ++ep) {
-    std::shuffle(perm.begin(), perm.end(), rng);
-    cudaMemcpyAsync(d_perm, perm.data(), n * 4, cudaMemcpyHostToDevice, st);
+    const int* cur = d_perm + (ep & 1) * n;
     cudaMemsetAsync(s->d_loss, 0, sizeof(double), st);
     for (long it = 0; it < steps; ++it) {
-      k_gather_rows<<<(batch + 255) / 256, 256, 0, st>>>(batch, d_perm + it * batch, x, y, Xb, s->Yb);
+      k_gather_rows<<<(batch + 255) / 256, 256, 0, st>>>(batch, cur + it * batch, x, y, Xb, s->Yb);
       cudaError_t ce = backward(s, batch, Xb, s->Yb, st);
       if (ce != cudaSuccess) {
         cudaFree(d_perm);
@@ -1563,6 +1566,10 @@ std::string surrogate_train(Surrogate* s, long n, const __nv_bfloat16* x, const 
       const float b1 = 0.9f, b2 = 0.999f;
       const float bc1 = 1.f - std::pow(b1, (float)s->step), bc2 = 1.f - std::pow(b2, (float)s->step);
       k_adam<<<64, 256, 0, st>>>(s->n_params, s->w, s->gr, s->m, s->v, s->wb, lr_t, b1, b2, 1e-8f, bc1, bc2);
+    }
+    if (ep + 1 < epochs) {  // the next epoch's order, drawn while this one runs
+      std::shuffle(perm.begin(), perm.end(), rng);
+      cudaMemcpyAsync(d_perm + ((ep + 1) & 1) * n, perm.data(), n * 4, cudaMemcpyHostToDevice, st);
     }
     double L = 0.0;
     cudaMemcpyAsync(&L, s->d_loss, sizeof(double), cudaMemcpyDeviceToHost, st);
