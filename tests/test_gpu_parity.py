@@ -433,3 +433,21 @@ def _check_eps(solver, oracle_mech, f, launch):
     assert np.abs(dY(loose, f) - dY(o, f))[:, act].max() <= 1e-5
     for k in ("Y_prod", "Y_prod2", "E_f_prod", "T_after", "status"):
         np.testing.assert_array_equal(again[k], base[k])
+
+
+@pytest.mark.parametrize("mode", ["reference", "fast", "mixed"])
+def test_lu_forms_give_identical_results(solver, W, mode):
+    """nrg_chem_set_lu_form: the unrolled and the looped LU factorisation of
+    the thread-per-cell kernels take the same operations in the same order."""
+    f = fields.slice_field(fields.ignition_field(W, n_side=128), 4000, stride=3)
+    try:
+        outs = [run_device(solver, f, mode, launch=dict(kernel="thread", block=32, grid=0, chunk=1, lu_rolled=r))
+                for r in (False, True)]
+    finally:
+        solver.set_launch(kernel="warp_queue", block=256, grid=0, chunk=1, lu_rolled=False)
+    (a, sa), (b, sb) = outs
+    for key in ("Y_prod", "Y_prod2", "E_f_prod", "T_after", "status"):
+        np.testing.assert_array_equal(a[key], b[key], err_msg=key)
+    for key in ("steps", "rhs_evals", "jacobians", "solves"):
+        assert sa[key] == sb[key], key
+    assert solver.get_launch()["lu_rolled"] is False
