@@ -86,6 +86,8 @@ struct nrg_chem {
   cudaGraphExec_t gexec = nullptr;
   // table of the table_approximated mode (nrg_chem_set_table / nrg_chem_load_table)
   double *d_tab_T = nullptr, *d_tab_Y = nullptr;
+  int2* d_tab_idx = nullptr;  // bucket index of sorted nodes (nrg::TableIndex)
+  nrg::TableIndex tab_idx;
   long tab_rows = 0;
   bool tab_sorted = false;
   // surrogate state (owned by surrogate.cu): the main network and a second
@@ -520,7 +522,8 @@ nrg::FallbackFn integrator_fallback(nrg_chem* h, cudaEvent_t* ph) {
 // phase events (or nullptr).
 cudaError_t enqueue_step_body(nrg_chem* h, const StepArgs& a, cudaStream_t s, cudaEvent_t* ph) {
   if (h->mode == NRG_MODE_TABLE) {
-    const nrg::TableArgs t{h->tab_rows, h->d_tab_T, h->d_tab_Y, h->tab_sorted ? 1 : 0};
+    const nrg::TableArgs t{h->tab_rows, h->d_tab_T, h->d_tab_Y, h->tab_sorted ? 1 : 0, h->d_tab_idx,
+                           (int)h->tab_idx.lo.size(), h->tab_idx.t0, h->tab_idx.inv_w};
     if (ph) cudaEventRecord(ph[2], s);
     cudaError_t e = nrg::launch_table_step(h->mech.n(), a, t, h->d_counters, s);
     if (ph) cudaEventRecord(ph[3], s);
@@ -747,6 +750,7 @@ extern "C" int nrg_chem_destroy(nrg_chem* h) {
   for (int i = 0; i < nrg::kMaxNets; ++i) nrg::surrogate_destroy(h->sur_net[i]);
   cudaFree(h->d_tab_T);
   cudaFree(h->d_tab_Y);
+  cudaFree(h->d_tab_idx);
   free_staging(h);
   cudaFree(h->d_queue);
   cudaFree(h->d_mech);
@@ -1461,14 +1465,28 @@ extern "C" int nrg_chem_set_table(nrg_chem* h, long rows, const double* T_t, con
   CK(h, cudaStreamSynchronize(h->stream));
   cudaFree(h->d_tab_T);
   cudaFree(h->d_tab_Y);
+  cudaFree(h->d_tab_idx);
   h->d_tab_T = h->d_tab_Y = nullptr;
+  h->d_tab_idx = nullptr;
+  h->tab_idx = nrg::TableIndex();
   h->tab_rows = 0;
   const size_t N = (size_t)h->mech.n();
   CK(h, cudaMalloc(&h->d_tab_T, sizeof(double) * (size_t)rows));
   CK(h, cudaMalloc(&h->d_tab_Y, sizeof(double) * (size_t)rows * N));
   CK(h, cudaMemcpy(h->d_tab_T, T_t, sizeof(double) * (size_t)rows, cudaMemcpyHostToDevice));
   CK(h, cudaMemcpy(h->d_tab_Y, Y_t, sizeof(double) * (size_t)rows * N, cudaMemcpyHostToDevice));
-  h->tab_sorted = nrg::table_nodes_sorted(std::vector<double>(T_t, T_t + rows));
+  const std::vector<double> nodes(T_t, T_t + rows);
+  h->tab_sorted = nrg::table_nodes_sorted(nodes);
+  // Sorted nodes: a bucket index of 4,096 buckets (32 KB) narrows each
+  // cell's bisection to the few nodes of its bucket.
+  if (h->tab_sorted && nrg::build_table_index(nodes, 4096, &h->tab_idx)) {
+    std::vector<int2> pairs(h->tab_idx.lo.size());
+    for (size_t j = 0; j < pairs.size(); ++j) pairs[j] = make_int2(h->tab_idx.lo[j], h->tab_idx.hi[j]);
+    CK(h, cudaMalloc(&h->d_tab_idx, sizeof(int2) * pairs.size()));
+    CK(h, cudaMemcpy(h->d_tab_idx, pairs.data(), sizeof(int2) * pairs.size(), cudaMemcpyHostToDevice));
+  } else {
+    h->tab_idx = nrg::TableIndex();
+  }
   h->tab_rows = rows;
   return NRG_OK;
 }

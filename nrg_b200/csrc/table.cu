@@ -150,6 +150,29 @@ bool table_nodes_sorted(const std::vector<double>& T) {
   return true;
 }
 
+bool build_table_index(const std::vector<double>& T, int n_buckets, TableIndex* out) {
+  const size_t M = T.size();
+  if (M < 2 || M > 2147483647u || n_buckets < 1 || !(T.front() < T.back())) return false;
+  const double t0 = T.front(), span = T.back() - T.front();
+  const double inv_w = (double)n_buckets / span;
+  if (!std::isfinite(inv_w) || !std::isfinite(span)) return false;
+  // The device's bucket (T - t0) * inv_w carries at most a few roundings
+  // relative to its value (at most n_buckets); these bounds are wider by a
+  // millionth of a bucket plus 2^-40 of the largest node.
+  const double w = span / (double)n_buckets;
+  const double margin = w * 1e-6 + std::ldexp(std::max(std::fabs(T.front()), std::fabs(T.back())), -40);
+  out->lo.assign((size_t)n_buckets, 0);
+  out->hi.assign((size_t)n_buckets, 0);
+  out->t0 = t0;
+  out->inv_w = inv_w;
+  const auto count_le = [&](double x) { return (int)(std::upper_bound(T.begin(), T.end(), x) - T.begin()); };
+  for (int j = 0; j < n_buckets; ++j) {
+    out->lo[(size_t)j] = j == 0 ? 0 : count_le(t0 + (double)j * w - margin);
+    out->hi[(size_t)j] = j == n_buckets - 1 ? (int)M : count_le(t0 + (double)(j + 1) * w + margin);
+  }
+  return true;
+}
+
 // --------------------------------------------------------------- device
 void upload_mechanism_table(const DevMech& m, cudaStream_t s) {
   cudaMemcpyToSymbolAsync(c_mech, &m, sizeof(DevMech), 0, cudaMemcpyHostToDevice, s);
@@ -165,6 +188,13 @@ __device__ __forceinline__ long table_interval(const TableArgs& t, double T) {
   const long M = t.rows;
   if (t.sorted) {
     long lo = 0, hi = M;
+    if (t.idx) {  // the bucket's range of node counts (TableIndex); NaN falls in bucket 0
+      const double x = (T - t.t0) * t.inv_w;
+      const int j = x >= 0.0 ? (x < (double)t.nb ? (int)x : t.nb - 1) : 0;
+      const int2 b = __ldg(t.idx + j);
+      lo = b.x;
+      hi = b.y;
+    }
     while (lo < hi) {
       const long mid = (lo + hi) >> 1;
       if (__ldg(t.T + mid) <= T) lo = mid + 1;
@@ -181,9 +211,11 @@ __device__ __forceinline__ long table_interval(const TableArgs& t, double T) {
 }
 
 // TA: the temperature after the step is written (the energy closure's
-// Newton iteration); without it the kernel is a lean streaming pass.
+// Newton iteration); without it the kernel is a lean streaming pass.  Six
+// 128-thread blocks per SM (at most 85 registers): the kernel waits on HBM
+// latency, and more warps keep more loads in flight.
 template <int N, bool TA>
-__global__ void __launch_bounds__(256) k_table_step(StepArgs a, TableArgs t, unsigned long long* counters) {
+__global__ void __launch_bounds__(128, 6) k_table_step(StepArgs a, TableArgs t, unsigned long long* counters) {
   unsigned active = 0, bad = 0;
   const long M = t.rows;
   for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < a.n; c += (long)gridDim.x * blockDim.x) {
@@ -259,12 +291,16 @@ cudaError_t launch_table_step(int n_species, const StepArgs& a, const TableArgs&
   if (a.n <= 0) return cudaSuccess;
   if (t.rows < 1 || !t.T || !t.Y) return cudaErrorInvalidValue;
   if (a.T_after && !a.rho) return cudaErrorInvalidValue;
-  const unsigned grid = (unsigned)std::min<long>((a.n + 255) / 256, 148L * 8);
+  // a block per 128 cells: the block scheduler keeps every SM's six slots
+  // busy to the end (measured faster than eight or sixteen blocks per SM
+  // striding over the cells, than one resident wave, and than 256-thread
+  // blocks)
+  const unsigned grid = (unsigned)std::min<long>((a.n + 127) / 128, 2147483647L);
   const bool ta = a.T_after != nullptr;
 #define NRG_TABLE_CASE(NS)                                                           \
   case NS:                                                                           \
-    if (ta) k_table_step<NS, true><<<grid, 256, 0, s>>>(a, t, counters);             \
-    else k_table_step<NS, false><<<grid, 256, 0, s>>>(a, t, counters);               \
+    if (ta) k_table_step<NS, true><<<grid, 128, 0, s>>>(a, t, counters);             \
+    else k_table_step<NS, false><<<grid, 128, 0, s>>>(a, t, counters);               \
     break;
   switch (n_species) {
     NRG_TABLE_CASE(9)

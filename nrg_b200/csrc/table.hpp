@@ -41,12 +41,30 @@ void format_e14_7(double x, char out[15]);
 // interval holding a temperature is found by bisection.
 bool table_nodes_sorted(const std::vector<double>& T);
 
+// Bucket index of sorted nodes: the range [T_0, T_{rows-1}] cut into nb equal
+// buckets; a temperature T in bucket j = floor((T - T_0) * inv_w) (clamped to
+// [0, nb - 1]) has between lo[j] and hi[j] nodes <= T, so the bisection for
+// its interval starts from that range instead of the whole table.
+struct TableIndex {
+  std::vector<int> lo, hi;
+  double t0 = 0.0, inv_w = 0.0;
+};
+
+// Builds the index of sorted nodes (false, and no index, for fewer than two
+// distinct nodes or more than 2^31 - 1 rows).  The bucket bounds are widened
+// by a millionth of a bucket, more than the rounding of the device's bucket
+// arithmetic, so the true node count always lies in [lo[j], hi[j]].
+bool build_table_index(const std::vector<double>& T, int n_buckets, TableIndex* out);
+
 // Device copy of a table for the step kernel.
 struct TableArgs {
   long rows;
   const double* T;   // rows
   const double* Y;   // N x rows, species-major
   int sorted;        // table_nodes_sorted
+  const int2* idx;   // TableIndex as (lo, hi) pairs, or null
+  int nb;            // buckets of idx
+  double t0, inv_w;  // TableIndex::t0, inv_w
 };
 
 // One chemistry step in table mode over a.n cells (a.cell_list unused):

@@ -117,6 +117,53 @@ def test_interpolation_edge_cases_equal_the_oracle(solver, oracle_mech, W, nodes
     assert np.array_equal(g["status"] == 4, ~fin & ~skipped)
 
 
+def test_bucket_search_and_sources_on_hard_operands_equal_the_oracle(solver, oracle_mech, W):
+    """The kernel finds a cell's interval by bisection inside one bucket of a
+    4,096-bucket index over the sorted nodes; the interval and the sources
+    must be the reference's bit for bit.  Operands that stress them: a
+    cluster of 500 nodes inside one bucket, node gaps of one ulp (~2e-13 K),
+    repeated nodes (0 / 0), cell temperatures exactly at nodes, at the host's
+    bucket edges and one ulp either side, table values over the whole double
+    range (zeros, subnormals, values near the overflow threshold), and an odd
+    step length."""
+    rng = np.random.default_rng(23)
+    nodes = np.concatenate([
+        rng.uniform(400.0, 2600.0, 300),
+        1200.0 + rng.uniform(0.0, 1e-3, 500),                      # one bucket
+        1800.0 + np.arange(40) * 2.2737367544323206e-13,            # 1 ulp of 1800 K apart
+        np.repeat(rng.uniform(500.0, 2500.0, 5), 2),                # repeated nodes
+        [400.0, 2600.0]])
+    T_t = np.sort(nodes)
+    M = T_t.size
+    mag = 10.0 ** rng.uniform(-320.0, 305.0, (9, M))
+    Y_t = np.where(rng.random((9, M)) < 0.5, -1.0, 1.0) * mag
+    Y_t[:, ::17] = 0.0
+    Y_t[:, 5::41] = 5e-324
+    w = (T_t[-1] - T_t[0]) / 4096
+    edges = T_t[0] + np.arange(4097) * w
+    probes = np.concatenate([
+        T_t, np.nextafter(T_t, np.inf), np.nextafter(T_t, -np.inf),
+        edges, np.nextafter(edges, np.inf), np.nextafter(edges, -np.inf),
+        rng.uniform(305.0, 3000.0, 20000),
+        1200.0 + rng.uniform(-1e-4, 1.1e-3, 8000),
+        1800.0 + rng.uniform(-1e-12, 1e-11, 2000)])
+    base = fields.random_field(W, n_side=256)
+    f = fields.slice_field(base, probes.size)
+    f.T[:] = probes
+    f.dt = 3.7e-7
+    solver.set_table(T_t, Y_t)
+    g, st = run_device(solver, f, "table")
+    o = _oracle_table(oracle_mech, T_t, Y_t, f)
+    for k in ("Y_prod", "Y_prod2", "E_f_prod"):
+        np.testing.assert_array_equal(g[k], o[k], err_msg=k)
+    skipped = f.T < 305.0
+    fin = np.isfinite(o["E_f_prod"]) & np.all(np.isfinite(o["Y_prod"]) & np.isfinite(o["Y_prod2"]), axis=0)
+    assert np.array_equal(g["status"] == 4, ~fin & ~skipped)
+    # finite sources and overflows both occur
+    ok = np.isfinite(o["Y_prod"]) & (o["Y_prod"] != 0.0)
+    assert ok.sum() > 100000 and (~np.isfinite(o["Y_prod"])).sum() > 0
+
+
 def test_host_layout_table_mode_through_the_reference_constructor(decks, oracle_mech, flame, table_file):
     """chemical_kinetics_solver_c(..., ODE_solver='table_approximated') on
     Fortran-layout host arrays with a ghost layer."""
