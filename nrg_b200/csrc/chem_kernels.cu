@@ -134,7 +134,9 @@ __global__ void k_apply_state(ApplyStateArgs a) {
 
 cudaError_t launch_apply_state(int n_species, const ApplyStateArgs& a, cudaStream_t s) {
   if (a.n <= 0) return cudaSuccess;
-  const long grid = std::min<long>((a.n + 127) / 128, 148L * 16);
+  // a block per 128 cells (not a capped grid striding over the cells): the
+  // block scheduler keeps every SM's slots busy to the end
+  const long grid = std::min<long>((a.n + 127) / 128, 2147483647L);
   switch (n_species) {
     case 9: k_apply_state<9><<<(unsigned)grid, 128, 0, s>>>(a); break;
     case 10: k_apply_state<10><<<(unsigned)grid, 128, 0, s>>>(a); break;

@@ -316,11 +316,8 @@ static cudaError_t launch_n(const PredictorArgs& a, cudaStream_t s) {
   kern<<<grid, dim3(32, TY), smem, s>>>(a);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const long total = nx * ny * nz;
-  const long blocks = std::min<long>((total + 255) / 256, (long)sms * 8);
+  const long blocks = std::min<long>((total + 255) / 256, 2147483647L);  // a block per 256 cells
   k_predictor_commit<N><<<(unsigned)std::max<long>(blocks, 1), 256, 0, s>>>(a);
   return cudaGetLastError();
 }
